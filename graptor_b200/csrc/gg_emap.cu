@@ -1,0 +1,969 @@
+// gg_emap.cu -- edgemap traversal kernels, the variant dispatcher, and the
+// BFS-level / BFS-parent / connected-components drivers.
+//
+// Reference behaviour (include/graptor/api.h:2143-2415): one edgemap call
+// evaluates relax(s,d) over the edges leaving the active (src-filtered)
+// vertices into dst-filtered vertices and records the output frontier; the
+// traversal is chosen per call by the sparse/dense threshold
+// (api.h:130-222): sparse => CSR push (dsl/edgemap.h:1397-1740 with
+// edge-balanced chunks, dsl/emap/edgechunk.h:315-620), dense => CSC pull with
+// per-vertex early exit (dsl/emap/GraptorCSCDataParCached.h:60-302, 348-496).
+//
+// B200 design
+//   * push_sparse : the frontier list is kept in three degree bins (produced
+//     directly by the kernel that made the frontier); one launch processes
+//     large-degree sources with a CTA each, medium ones with a warp each and
+//     small ones with a thread each (warp-uniform loops).
+//   * push_merge  : edge-balanced push: degree prefix sum over the frontier,
+//     each CTA takes an equal slice of edges and finds its sources by binary
+//     search (merge-path partitioning).
+//   * pull_dense  : one warp owns 32 consecutive destinations (one frontier
+//     bitmap word); each lane first scans up to K in-edges of its own vertex,
+//     then the warp cooperatively scans the remaining long rows 32 edges at a
+//     time (coalesced), exiting as soon as the dst filter turns false.  The
+//     output bitmap word is written with a single store, counts reduced per
+//     CTA, and the output list is appended warp-aggregated.
+//   * push_dense  : push from a frontier bitmap with the same two-phase warp
+//     scheme, for large frontiers whose operator does not early-exit.
+// Records: NE_PREV (a[d] != prev[d], then prev[d] = a[d]) is detected without
+// a dedup pass: in push the thread whose atomic moved a[d] away from prev[d]
+// records d; in pull the owner of d does.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <type_traits>
+
+#include "gg_internal.cuh"
+
+namespace gg {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+struct EmapArgs {
+    const uint64_t *off;      // CSR (push, out-degree)
+    const uint32_t *adj;
+    const uint64_t *in_off;   // CSC (pull)
+    const uint32_t *in_adj;
+    uint32_t n;
+    int record;
+    // input frontier
+    const uint32_t *in_bits;  // bitmap or nullptr (all vertices)
+    const uint32_t *in_b0, *in_b1, *in_b2;
+    uint32_t c0, c1, c2;
+    // output frontier
+    uint32_t *out_bits;       // pull: every word written; push: test-and-set dedup (pre-cleared)
+    uint32_t *out_b0, *out_b1, *out_b2;
+    unsigned long long *out_cnt;
+    uint32_t smax, mmax;
+    int K;
+};
+
+template <int R>
+struct Op {
+    using V = typename std::conditional<R == GG_RELAX_MIN_PLUS1_I32, int32_t, uint32_t>::type;
+    V *a;
+    V *prev;
+    int filter;
+    int64_t fk;
+
+    __device__ __forceinline__ V load(uint32_t v) const { return a[v]; }
+    __device__ __forceinline__ static V none() {
+        if constexpr (R == GG_RELAX_MIN_PLUS1_I32) return INT_MAX;
+        else return 0xFFFFFFFFu;
+    }
+    __device__ __forceinline__ bool dst_ok(V cur) const {
+        switch (filter) {
+        case GG_FILTER_GT_CONST: return (int64_t)cur > fk;
+        case GG_FILTER_NE_ZERO: return cur != 0;
+        case GG_FILTER_MSB_SET: return ((uint32_t)cur >> 31) != 0;
+        default: return true;
+        }
+    }
+    // value offered along an edge s->d
+    __device__ __forceinline__ V src_val(uint32_t s) const {
+        if constexpr (R == GG_RELAX_MIN_PLUS1_I32) return a[s] + 1;
+        else if constexpr (R == GG_RELAX_MIN_U32) return a[s];
+        else return (V)s;
+    }
+    __device__ __forceinline__ bool better(V x, V best) const {
+        if constexpr (R == GG_RELAX_SETIF_U32) return ((uint32_t)best >> 31) != 0;
+        else return x < best;
+    }
+    // among the lanes with ok set (mask okm) pick the winner's value
+    __device__ __forceinline__ V warp_pick(bool ok, V x, unsigned okm) const {
+        if constexpr (R == GG_RELAX_SETIF_U32) {
+            return __shfl_sync(FULL, x, __ffs(okm) - 1);
+        } else {
+            V mine = ok ? x : none();
+            return __reduce_min_sync(FULL, mine);
+        }
+    }
+    // push: offer sv to d; true iff this thread records d
+    __device__ __forceinline__ bool offer(uint32_t d, V sv, int record, uint32_t *dedup) const {
+        V cur = a[d];
+        if (!dst_ok(cur)) return false;
+        V old;
+        if constexpr (R == GG_RELAX_SETIF_U32) {
+            if (((uint32_t)cur >> 31) == 0) return false;
+            old = atomicCAS(a + d, cur, sv);
+            if (old != cur) return false;
+        } else {
+            if (!(sv < cur)) return false;
+            old = atomicMin(a + d, sv);
+            if (!(sv < old)) return false;
+        }
+        if (record == GG_RECORD_NE_PREV) return old == prev[d];
+        if (record == GG_RECORD_REDUCTION) {
+            uint32_t bit = 1u << (d & 31);
+            return (atomicOr(dedup + (d >> 5), bit) & bit) == 0;
+        }
+        return false;
+    }
+};
+
+__device__ __forceinline__ void emit_out(const EmapArgs &A, bool rec, uint32_t d,
+                                         unsigned long long &nv, unsigned long long &ne) {
+    uint64_t deg = 0;
+    if (rec) {
+        deg = A.off[d + 1] - A.off[d];
+        nv++;
+        ne += deg;
+    }
+    uint32_t bin = deg <= A.smax ? 0u : (deg <= A.mmax ? 1u : 2u);
+    // warp-aggregated append (see gg_core.cu emit_binned)
+    const unsigned am = __activemask();
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (uint32_t b = 0; b < NBINS; ++b) {
+        unsigned mk = __ballot_sync(am, rec && bin == b);
+        if (mk == 0) continue;
+        int leader = __ffs(mk) - 1;
+        unsigned long long base = 0;
+        if ((int)lane == leader) base = atomicAdd(A.out_cnt + FC_BIN0 + b, (unsigned long long)__popc(mk));
+        base = __shfl_sync(am, base, leader);
+        if (rec && bin == b) {
+            uint32_t *dst = b == 0 ? A.out_b0 : (b == 1 ? A.out_b1 : A.out_b2);
+            dst[base + __popc(mk & ((1u << lane) - 1u))] = d;
+        }
+    }
+}
+
+template <int BLOCK>
+__device__ __forceinline__ void flush_counts(const EmapArgs &A, unsigned long long nv,
+                                             unsigned long long ne, unsigned long long sc) {
+    nv = dev::block_sum<unsigned long long, BLOCK>(nv);
+    ne = dev::block_sum<unsigned long long, BLOCK>(ne);
+    sc = dev::block_sum<unsigned long long, BLOCK>(sc);
+    if (threadIdx.x == 0) {
+        if (nv) atomicAdd(A.out_cnt + FC_NACTV, nv);
+        if (ne) atomicAdd(A.out_cnt + FC_NACTE, ne);
+        if (sc) atomicAdd(A.out_cnt + FC_SCANNED, sc);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Dense pull over the CSC
+// ---------------------------------------------------------------------------
+template <int R, bool SRCF, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_pull(EmapArgs A, Op<R> op) {
+    using V = typename Op<R>::V;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwords = (A.n + 31u) >> 5;
+    const uint32_t nw = (gridDim.x * BLOCK) >> 5;
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    for (uint32_t w = (blockIdx.x * BLOCK + threadIdx.x) >> 5; w < nwords; w += nw) {
+        const uint32_t d = (w << 5) + lane;
+        const bool valid = d < A.n;
+        V best = valid ? op.load(d) : Op<R>::none();
+        bool act = valid && op.dst_ok(best);
+        bool changed = false;
+        uint64_t e = 0, end = 0;
+        if (act) {
+            e = A.in_off[d];
+            end = A.in_off[d + 1];
+        }
+        const uint64_t beg = e;
+        const uint64_t lim = min(end, e + (uint64_t)A.K);
+        while (act && e < lim) {
+            const uint32_t s = __ldg(A.in_adj + e);
+            ++e;
+            if (!SRCF || dev::bit_test(A.in_bits, s)) {
+                V x = op.src_val(s);
+                if (op.better(x, best)) {
+                    best = x;
+                    changed = true;
+                    if (!op.dst_ok(best)) act = false;
+                }
+            }
+        }
+        sc += e - beg;
+        unsigned pend = __ballot_sync(FULL, act && e < end);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint64_t ej = __shfl_sync(FULL, e, j);
+            const uint64_t endj = __shfl_sync(FULL, end, j);
+            V bj = __shfl_sync(FULL, best, j);
+            bool chj = false;
+            for (uint64_t base = ej; base < endj; base += 32) {
+                const uint64_t idx = base + lane;
+                bool ok = false;
+                V x = Op<R>::none();
+                if (idx < endj) {
+                    const uint32_t s = __ldg(A.in_adj + idx);
+                    if (!SRCF || dev::bit_test(A.in_bits, s)) {
+                        x = op.src_val(s);
+                        ok = op.better(x, bj);
+                    }
+                }
+                if (lane == 0) sc += min((uint64_t)32, endj - base);
+                const unsigned okm = __ballot_sync(FULL, ok);
+                if (okm) {
+                    bj = op.warp_pick(ok, x, okm);
+                    chj = true;
+                    if (!op.dst_ok(bj)) break;
+                }
+            }
+            if ((int)lane == j) {
+                best = bj;
+                changed = changed || chj;
+            }
+        }
+        bool rec = false;
+        if (changed) {
+            op.a[d] = best;
+            if (A.record == GG_RECORD_NE_PREV) {
+                if (best != op.prev[d]) {
+                    op.prev[d] = best;
+                    rec = true;
+                }
+            } else if (A.record == GG_RECORD_REDUCTION) {
+                rec = true;
+            }
+        }
+        if (A.out_bits) {
+            const unsigned bits = __ballot_sync(FULL, rec);
+            if (lane == 0) A.out_bits[w] = bits;
+        }
+        if (A.out_b0) emit_out(A, rec, d, nv, ne);
+    }
+    if (A.out_cnt) flush_counts<BLOCK>(A, nv, ne, sc);
+}
+
+// ---------------------------------------------------------------------------
+// Degree-binned sparse push
+// ---------------------------------------------------------------------------
+template <int R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uint32_t nb_large,
+                                                       uint32_t nb_med) {
+    using V = typename Op<R>::V;
+    const uint32_t lane = threadIdx.x & 31u;
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    if (blockIdx.x < nb_large) {
+        // large bin: a CTA per source vertex
+        for (uint32_t i = blockIdx.x; i < A.c2; i += nb_large) {
+            const uint32_t s = A.in_b2[i];
+            const V sv = op.src_val(s);
+            const uint64_t beg = A.off[s], end = A.off[s + 1];
+            if (threadIdx.x == 0) sc += end - beg;
+            for (uint64_t base = beg; base < end; base += BLOCK) {
+                const uint64_t e = base + threadIdx.x;
+                bool rec = false;
+                uint32_t d = 0;
+                if (e < end) {
+                    d = __ldg(A.adj + e);
+                    rec = op.offer(d, sv, A.record, A.out_bits);
+                }
+                emit_out(A, rec, d, nv, ne);
+            }
+        }
+    } else if (blockIdx.x < nb_large + nb_med) {
+        // medium bin: a warp per source vertex
+        const uint32_t wpb = BLOCK / 32;
+        const uint32_t nwm = nb_med * wpb;
+        const uint32_t wid = (blockIdx.x - nb_large) * wpb + (threadIdx.x >> 5);
+        for (uint32_t i = wid; i < A.c1; i += nwm) {
+            const uint32_t s = A.in_b1[i];
+            const V sv = op.src_val(s);
+            const uint64_t beg = A.off[s], end = A.off[s + 1];
+            if (lane == 0) sc += end - beg;
+            for (uint64_t base = beg; base < end; base += 32) {
+                const uint64_t e = base + lane;
+                bool rec = false;
+                uint32_t d = 0;
+                if (e < end) {
+                    d = __ldg(A.adj + e);
+                    rec = op.offer(d, sv, A.record, A.out_bits);
+                }
+                emit_out(A, rec, d, nv, ne);
+            }
+        }
+    } else {
+        // small bin: a thread per source vertex, warp-uniform edge loop
+        const uint32_t wpb = BLOCK / 32;
+        const uint32_t nws = (gridDim.x - nb_large - nb_med) * wpb;
+        const uint32_t wid = (blockIdx.x - nb_large - nb_med) * wpb + (threadIdx.x >> 5);
+        for (uint64_t base = (uint64_t)wid * 32; base < A.c0; base += (uint64_t)nws * 32) {
+            const uint64_t i = base + lane;
+            const bool have = i < A.c0;
+            uint32_t s = 0;
+            uint64_t beg = 0, end = 0;
+            V sv = Op<R>::none();
+            if (have) {
+                s = A.in_b0[i];
+                beg = A.off[s];
+                end = A.off[s + 1];
+                sv = op.src_val(s);
+            }
+            const uint32_t deg = (uint32_t)(end - beg);
+            sc += deg;
+            const uint32_t maxd = __reduce_max_sync(FULL, deg);
+            for (uint32_t k = 0; k < maxd; ++k) {
+                bool rec = false;
+                uint32_t d = 0;
+                if (k < deg) {
+                    d = __ldg(A.adj + beg + k);
+                    rec = op.offer(d, sv, A.record, A.out_bits);
+                }
+                emit_out(A, rec, d, nv, ne);
+            }
+        }
+    }
+    flush_counts<BLOCK>(A, nv, ne, sc);
+}
+
+// ---------------------------------------------------------------------------
+// Edge-balanced (merge-path) push over a contiguous frontier list
+// ---------------------------------------------------------------------------
+// Gather the three bins into one list with out-degrees.
+__global__ void k_concat_bins(const uint32_t *b0, const uint32_t *b1, const uint32_t *b2,
+                              const uint64_t *cnt, const uint64_t *off, uint32_t *list,
+                              uint64_t *deg) {
+    const uint64_t c0 = cnt[FC_BIN0], c1 = cnt[FC_BIN1], c2 = cnt[FC_BIN2];
+    const uint64_t tot = c0 + c1 + c2;
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (; i < tot; i += stride) {
+        uint32_t v = i < c0 ? b0[i] : (i < c0 + c1 ? b1[i - c0] : b2[i - c0 - c1]);
+        list[i] = v;
+        deg[i] = off[v + 1] - off[v];
+    }
+}
+
+// pre: exclusive prefix of degrees (k+1 entries, pre[k] = total edges).
+template <int R, int BLOCK, int TILE>
+__global__ void __launch_bounds__(BLOCK) k_push_merge(EmapArgs A, Op<R> op, const uint32_t *list,
+                                                      const uint64_t *pre, uint64_t k) {
+    using V = typename Op<R>::V;
+    __shared__ uint64_t s_lo;
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    const uint64_t total = pre[k];
+    const uint64_t ntiles = (total + TILE - 1) / TILE;
+    for (uint64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const uint64_t t0 = t * TILE;
+        if (threadIdx.x == 0) {
+            // last source i with pre[i] <= t0
+            uint64_t lo = 0, hi = k;
+            while (hi - lo > 1) {
+                uint64_t mid = (lo + hi) / 2;
+                if (pre[mid] <= t0) lo = mid; else hi = mid;
+            }
+            s_lo = lo;
+        }
+        __syncthreads();
+        const uint64_t lo = s_lo;
+        __syncthreads();
+        for (uint64_t e0 = t0; e0 < min(t0 + TILE, total); e0 += BLOCK) {
+            const uint64_t e = e0 + threadIdx.x;
+            bool rec = false;
+            uint32_t d = 0;
+            if (e < total && e < t0 + TILE) {
+                // source index: last i >= lo with pre[i] <= e (search a short range)
+                uint64_t a = lo, b = k;
+                uint64_t step = 1;
+                while (a + step < b && pre[a + step] <= e) { a += step; step <<= 1; }
+                b = min(b, a + step);
+                while (b - a > 1) {
+                    uint64_t mid = (a + b) / 2;
+                    if (pre[mid] <= e) a = mid; else b = mid;
+                }
+                const uint32_t s = list[a];
+                const uint64_t pos = A.off[s] + (e - pre[a]);
+                d = __ldg(A.adj + pos);
+                rec = op.offer(d, op.src_val(s), A.record, A.out_bits);
+                sc++;
+            }
+            emit_out(A, rec, d, nv, ne);
+        }
+    }
+    flush_counts<BLOCK>(A, nv, ne, sc);
+}
+
+// ---------------------------------------------------------------------------
+// Dense push from a frontier bitmap
+// ---------------------------------------------------------------------------
+template <int R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_push_dense(EmapArgs A, Op<R> op) {
+    using V = typename Op<R>::V;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwords = (A.n + 31u) >> 5;
+    const uint32_t nw = (gridDim.x * BLOCK) >> 5;
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    for (uint32_t w = (blockIdx.x * BLOCK + threadIdx.x) >> 5; w < nwords; w += nw) {
+        const uint32_t s = (w << 5) + lane;
+        const uint32_t word = A.in_bits ? A.in_bits[w] : FULL;
+        const bool act = s < A.n && ((word >> lane) & 1u);
+        uint64_t beg = 0, end = 0;
+        V sv = Op<R>::none();
+        if (act) {
+            beg = A.off[s];
+            end = A.off[s + 1];
+            sv = op.src_val(s);
+        }
+        // phase 1: up to K edges per lane
+        const uint32_t k1 = (uint32_t)min(end - beg, (uint64_t)A.K);
+        const uint32_t maxk = __reduce_max_sync(FULL, k1);
+        for (uint32_t k = 0; k < maxk; ++k) {
+            bool rec = false;
+            uint32_t d = 0;
+            if (k < k1) {
+                d = __ldg(A.adj + beg + k);
+                rec = op.offer(d, sv, A.record, A.out_bits);
+            }
+            emit_out(A, rec, d, nv, ne);
+        }
+        sc += k1;
+        // phase 2: warp-cooperative over long rows
+        unsigned pend = __ballot_sync(FULL, act && beg + k1 < end);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint64_t ej = __shfl_sync(FULL, beg + k1, j);
+            const uint64_t endj = __shfl_sync(FULL, end, j);
+            const V svj = __shfl_sync(FULL, sv, j);
+            if (lane == 0) sc += endj - ej;
+            for (uint64_t base = ej; base < endj; base += 32) {
+                const uint64_t e = base + lane;
+                bool rec = false;
+                uint32_t d = 0;
+                if (e < endj) {
+                    d = __ldg(A.adj + e);
+                    rec = op.offer(d, svj, A.record, A.out_bits);
+                }
+                emit_out(A, rec, d, nv, ne);
+            }
+        }
+    }
+    flush_counts<BLOCK>(A, nv, ne, sc);
+}
+
+// prev[v] = a[v] over the output list (maintain_copies, vertexmap.h:2515-2535)
+template <typename V>
+__global__ void k_copy_prev(const uint32_t *b0, const uint32_t *b1, const uint32_t *b2,
+                            const uint64_t *cnt, const V *a, V *prev) {
+    const uint64_t c0 = cnt[FC_BIN0], c1 = cnt[FC_BIN1], c2 = cnt[FC_BIN2];
+    const uint64_t tot = c0 + c1 + c2;
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (; i < tot; i += stride) {
+        uint32_t v = i < c0 ? b0[i] : (i < c0 + c1 ? b1[i - c0] : b2[i - c0 - c1]);
+        prev[v] = a[v];
+    }
+}
+
+__global__ void k_iota_u32(uint32_t *a, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t stride = gridDim.x * blockDim.x;
+    for (; i < n; i += stride) a[i] = i;
+}
+
+// neighbours of vertex z get label 0 in both copies (CCv PRESET_ZERO,
+// bench/CCv.C:262-291, applied to vertex 0 whose component minimum is 0)
+__global__ void k_preset_zero(const uint64_t *off, const uint32_t *adj, uint32_t z, uint32_t *lab,
+                              uint32_t *prev) {
+    for (uint64_t e = off[z] + blockIdx.x * blockDim.x + threadIdx.x; e < off[z + 1];
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        lab[adj[e]] = 0;
+        prev[adj[e]] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+constexpr int kBlock = 256;
+
+static unsigned persistent_grid(gg_ctx *ctx, uint64_t warps_needed) {
+    uint64_t blocks = (warps_needed + (kBlock / 32) - 1) / (kBlock / 32);
+    uint64_t cap = (uint64_t)ctx->sm_count * tuning().blocks_per_sm;
+    if (blocks > cap) blocks = cap;
+    return (unsigned)std::max<uint64_t>(blocks, 1);
+}
+
+static bool threshold_sparse(int kind, int k, uint64_t nactv, uint64_t nacte, uint64_t m) {
+    switch (kind) {
+    case GG_THRESH_ALWAYS_SPARSE: return true;
+    case GG_THRESH_ALWAYS_DENSE: return false;
+    case GG_THRESH_FRAC:
+        // api.h:137-140: float(nactv+nacte) <= float(m) / (100.0/(float)k)
+        return (float)(nactv + nacte) <= (float)m / (float)(100.0 / (float)k);
+    default:
+        return (nactv + nacte) <= (m / 20);  // api.h:154-156
+    }
+}
+
+int learned_select(gg_graph *g, uint64_t nactv, uint64_t nacte, int iter, bool can_early_exit);
+
+template <int R>
+static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier *in,
+                                gg_frontier *out, int variant) {
+    gg_ctx *ctx = g->ctx;
+    cudaStream_t st = ctx->stream;
+    const Tuning &t = tuning();
+    Op<R> op;
+    op.a = (typename Op<R>::V *)d->a->d;
+    op.prev = d->prev ? (typename Op<R>::V *)d->prev->d : nullptr;
+    op.filter = d->dst_filter;
+    op.fk = d->dst_filter_k;
+
+    EmapArgs A;
+    memset(&A, 0, sizeof(A));
+    A.off = g->off;
+    A.adj = g->adj;
+    A.in_off = g->in_off;
+    A.in_adj = g->in_adj;
+    A.n = g->n;
+    A.record = d->record;
+    A.smax = t.bin_small_max;
+    A.mmax = t.bin_medium_max;
+    A.K = variant == GG_VAR_PULL_DENSE ? t.pull_k : t.push_k;
+    const bool have_out = out != nullptr && d->record != GG_RECORD_NONE;
+    if (have_out) {
+        GG_CHECK(frontier_alloc_bins(out));
+        GG_CHECK(frontier_reset_counts(out));
+        A.out_b0 = out->bins[0];
+        A.out_b1 = out->bins[1];
+        A.out_b2 = out->bins[2];
+        A.out_cnt = (unsigned long long *)out->d_cnt;
+    }
+    const size_t words = ((size_t)g->n + 31) / 32;
+    bool out_bitmap_valid = false;
+    if (variant == GG_VAR_PULL_DENSE) {
+        if (have_out) {
+            GG_CHECK(frontier_alloc_bitmap(out));
+            A.out_bits = out->bitmap;
+            out_bitmap_valid = true;
+        }
+    } else if (have_out && d->record == GG_RECORD_REDUCTION) {
+        GG_CHECK(frontier_alloc_bitmap(out));
+        GG_CUDA(ctx, cudaMemsetAsync(out->bitmap, 0, words * 4, st));
+        A.out_bits = out->bitmap;
+        out_bitmap_valid = true;
+    }
+    if (!have_out && d->record != GG_RECORD_NONE) return set_error(ctx, GG_ERR_ARG, "record without output frontier");
+    if (!have_out) {
+        // counts still wanted for the scanned-edge statistic
+        if (!g->aux_cnt) GG_CUDA(ctx, cudaMalloc(&g->aux_cnt, FC_WORDS * 8));
+        GG_CUDA(ctx, cudaMemsetAsync(g->aux_cnt, 0, FC_WORDS * 8, st));
+        A.out_cnt = (unsigned long long *)g->aux_cnt;
+    }
+
+    const bool all_in = in == nullptr || in->all;
+    switch (variant) {
+    case GG_VAR_PULL_DENSE: {
+        if (!all_in) {
+            GG_CHECK(frontier_ensure_bitmap(in));
+            A.in_bits = in->bitmap;
+        }
+        unsigned grid = persistent_grid(ctx, words);
+        if (all_in) k_pull<R, false, kBlock><<<grid, kBlock, 0, st>>>(A, op);
+        else k_pull<R, true, kBlock><<<grid, kBlock, 0, st>>>(A, op);
+        GG_LAUNCHED(ctx);
+        break;
+    }
+    case GG_VAR_PUSH_DENSE: {
+        if (!all_in) {
+            GG_CHECK(frontier_ensure_bitmap(in));
+            A.in_bits = in->bitmap;
+        }
+        unsigned grid = persistent_grid(ctx, words);
+        k_push_dense<R, kBlock><<<grid, kBlock, 0, st>>>(A, op);
+        GG_LAUNCHED(ctx);
+        break;
+    }
+    case GG_VAR_PUSH_SPARSE: {
+        if (all_in) {
+            if (!in) return set_error(ctx, GG_ERR_ARG, "sparse push needs a frontier");
+        }
+        GG_CHECK(frontier_ensure_list(in));
+        GG_CHECK(frontier_fetch_counts(in));
+        A.in_b0 = in->bins[0];
+        A.in_b1 = in->bins[1];
+        A.in_b2 = in->bins[2];
+        A.c0 = (uint32_t)in->h_cnt[FC_BIN0];
+        A.c1 = (uint32_t)in->h_cnt[FC_BIN1];
+        A.c2 = (uint32_t)in->h_cnt[FC_BIN2];
+        const uint32_t cap = ctx->sm_count * t.blocks_per_sm;
+        uint32_t nb_large = std::min<uint32_t>(A.c2, cap);
+        uint32_t nb_med = std::min<uint32_t>((A.c1 + kBlock / 32 - 1) / (kBlock / 32), cap);
+        uint32_t nb_small = std::min<uint32_t>((A.c0 + kBlock - 1) / kBlock, cap);
+        uint32_t grid = nb_large + nb_med + nb_small;
+        if (grid == 0) break;
+        k_push_binned<R, kBlock><<<grid, kBlock, 0, st>>>(A, op, nb_large, nb_med);
+        GG_LAUNCHED(ctx);
+        break;
+    }
+    case GG_VAR_PUSH_MERGE: {
+        if (!in) return set_error(ctx, GG_ERR_ARG, "merge push needs a frontier");
+        GG_CHECK(frontier_ensure_list(in));
+        GG_CHECK(frontier_fetch_counts(in));
+        uint64_t k = in->h_cnt[FC_BIN0] + in->h_cnt[FC_BIN1] + in->h_cnt[FC_BIN2];
+        if (k == 0) break;
+        // scratch: list[k] u32, deg[k+1] u64, pre[k+1] u64, cub temp
+        size_t cub_bytes = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (uint64_t *)nullptr, (uint64_t *)nullptr, (int64_t)(k + 1), st);
+        size_t lb = ((k * 4 + 255) / 256) * 256, db = (((k + 1) * 8 + 255) / 256) * 256;
+        void *p;
+        GG_CHECK(graph_scratch(g, lb + 2 * db + cub_bytes, &p));
+        uint32_t *list = (uint32_t *)p;
+        uint64_t *deg = (uint64_t *)((char *)p + lb);
+        uint64_t *pre = (uint64_t *)((char *)p + lb + db);
+        void *cub_tmp = (char *)p + lb + 2 * db;
+        GG_CUDA(ctx, cudaMemsetAsync(deg + k, 0, 8, st));
+        k_concat_bins<<<persistent_grid(ctx, (k + 31) / 32), kBlock, 0, st>>>(
+            in->bins[0], in->bins[1], in->bins[2], in->d_cnt, g->off, list, deg);
+        GG_LAUNCHED(ctx);
+        GG_CUDA(ctx, cub::DeviceScan::ExclusiveSum(cub_tmp, cub_bytes, deg, pre, (int64_t)(k + 1), st));
+        ctx->launches++;
+        constexpr int TILE = 4096;
+        uint64_t edges = in->h_cnt[FC_NACTE];
+        unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((edges + TILE - 1) / TILE,
+                                                                            (uint64_t)ctx->sm_count * t.blocks_per_sm));
+        k_push_merge<R, kBlock, TILE><<<grid, kBlock, 0, st>>>(A, op, list, pre, k);
+        GG_LAUNCHED(ctx);
+        break;
+    }
+    default:
+        return set_error(ctx, GG_ERR_ARG, "unknown variant");
+    }
+    if (have_out) {
+        if (d->record == GG_RECORD_NE_PREV && variant != GG_VAR_PULL_DENSE) {
+            if (!d->prev) return set_error(ctx, GG_ERR_ARG, "NE_PREV record needs prev");
+            k_copy_prev<<<persistent_grid(ctx, words), kBlock, 0, st>>>(
+                out->bins[0], out->bins[1], out->bins[2], out->d_cnt, op.a, op.prev);
+            GG_LAUNCHED(ctx);
+        }
+        out->all = false;
+        out->has_list = true;
+        out->has_bitmap = out_bitmap_valid;
+        out->host_valid = false;
+    }
+    return GG_OK;
+}
+
+gg_status pr_edgemap_gather(gg_graph *g, const gg_emap_desc *d, gg_frontier *in);
+
+gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_frontier *out,
+                       gg_emap_stats *stats) {
+    gg_ctx *ctx = g->ctx;
+    if (!d->a || d->a->g != g) return set_error(ctx, GG_ERR_ARG, "edgemap: relaxed property missing or of another graph");
+    if (in && in->g != g) return set_error(ctx, GG_ERR_ARG, "edgemap: input frontier of another graph");
+    if (out && out->g != g) return set_error(ctx, GG_ERR_ARG, "edgemap: output frontier of another graph");
+    if (out && out == in) return set_error(ctx, GG_ERR_ARG, "edgemap: input and output frontier must differ");
+    if (d->relax == GG_RELAX_ADD_GATHER) {
+        if (d->record != GG_RECORD_NONE) return set_error(ctx, GG_ERR_UNSUPPORTED, "ADD_GATHER records no frontier");
+        GG_CHECK(pr_edgemap_gather(g, d, in));
+        if (stats) {
+            memset(stats, 0, sizeof(*stats));
+            stats->variant = GG_VAR_PULL_DENSE;
+            stats->nactv_in = g->n;
+            stats->nacte_in = g->m;
+            stats->scanned = g->m;
+        }
+        return GG_OK;
+    }
+    const gg_dtype want = d->relax == GG_RELAX_MIN_PLUS1_I32 ? GG_I32 : GG_U32;
+    if (d->relax < 0 || d->relax > GG_RELAX_SETIF_U32) return set_error(ctx, GG_ERR_ARG, "unknown relax kind");
+    if (d->a->t != want) return set_error(ctx, GG_ERR_ARG, "relaxed property has the wrong dtype");
+    if (d->prev && (d->prev->t != want || d->prev->g != g)) return set_error(ctx, GG_ERR_ARG, "prev property mismatch");
+    if (d->record == GG_RECORD_NE_PREV && !d->prev) return set_error(ctx, GG_ERR_ARG, "NE_PREV record needs prev");
+    if (d->dst_filter < GG_FILTER_NONE || d->dst_filter > GG_FILTER_MSB_SET) return set_error(ctx, GG_ERR_ARG, "unknown dst filter");
+    if (d->dst_filter != GG_FILTER_NONE && d->dst_filter_prop && d->dst_filter_prop != d->a)
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "dst filter on a property other than the relaxed one");
+    if (d->threshold == GG_THRESH_FRAC && d->threshold_k <= 0) return set_error(ctx, GG_ERR_ARG, "frac threshold needs k > 0");
+
+    uint64_t nactv = g->n, nacte = g->m;
+    const bool all_in = in == nullptr || in->all;
+    if (!all_in) {
+        GG_CHECK(frontier_fetch_counts(in));
+        nactv = in->h_cnt[FC_NACTV];
+        nacte = in->h_cnt[FC_NACTE];
+    }
+    int variant = d->variant;
+    if (variant == GG_VAR_AUTO) {
+        bool can_exit = d->dst_filter != GG_FILTER_NONE;
+        if (all_in) {
+            variant = GG_VAR_PULL_DENSE;
+        } else if (d->threshold == GG_THRESH_LEARNED) {
+            variant = learned_select(g, nactv, nacte, 0, can_exit);
+        } else {
+            variant = threshold_sparse(d->threshold, d->threshold_k, nactv, nacte, g->m)
+                          ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+        }
+    }
+    if (all_in && (variant == GG_VAR_PUSH_SPARSE || variant == GG_VAR_PUSH_MERGE) && !in)
+        variant = GG_VAR_PUSH_DENSE;
+    if (!all_in && nactv == 0) {
+        // empty input: empty output, nothing to launch
+        if (out) GG_CHECK(gg_frontier_clear(out));
+        if (stats) {
+            memset(stats, 0, sizeof(*stats));
+            stats->variant = variant;
+        }
+        return GG_OK;
+    }
+    gg_status s;
+    switch (d->relax) {
+    case GG_RELAX_MIN_PLUS1_I32: s = launch_variant<GG_RELAX_MIN_PLUS1_I32>(g, d, in, out, variant); break;
+    case GG_RELAX_MIN_U32: s = launch_variant<GG_RELAX_MIN_U32>(g, d, in, out, variant); break;
+    default: s = launch_variant<GG_RELAX_SETIF_U32>(g, d, in, out, variant); break;
+    }
+    GG_CHECK(s);
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->variant = variant;
+        stats->nactv_in = nactv;
+        stats->nacte_in = nacte;
+        if (out && d->record != GG_RECORD_NONE) {
+            GG_CHECK(frontier_fetch_counts(out));
+            stats->scanned = out->h_cnt[FC_SCANNED];
+            stats->nactv_out = out->h_cnt[FC_NACTV];
+            stats->nacte_out = out->h_cnt[FC_NACTE];
+        }
+    }
+    return GG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Drivers
+// ---------------------------------------------------------------------------
+struct RunTimer {
+    gg_ctx *ctx;
+    explicit RunTimer(gg_ctx *c) : ctx(c) { cudaEventRecord(ctx->ev0, ctx->stream); }
+    double stop() {
+        cudaEventRecord(ctx->ev1, ctx->stream);
+        cudaEventSynchronize(ctx->ev1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        return ms;
+    }
+};
+
+static gg_status get_tmp_frontiers(gg_graph *g, gg_frontier **a, gg_frontier **b) {
+    for (auto &f : g->tmp_front)
+        if (!f) GG_CHECK(gg_frontier_create(g, &f));
+    *a = g->tmp_front[0];
+    *b = g->tmp_front[1];
+    return GG_OK;
+}
+
+struct TmpProp {
+    gg_prop *p = nullptr;
+    ~TmpProp() { if (p) gg_prop_destroy(p); }
+};
+
+static void record_iter(gg_run_stats *st, int it, const gg_emap_stats &es) {
+    if (!st || it >= GG_MAX_ITERS) return;
+    st->variant[it] = es.variant;
+    st->nactv[it] = es.nactv_in;
+    st->nacte[it] = es.nacte_in;
+    st->scanned[it] = es.scanned;
+    st->scanned_edges += es.scanned;
+}
+
+static void default_opts(const gg_run_opts *o, gg_run_opts *r, int thresh, int k) {
+    if (o) {
+        *r = *o;
+    } else {
+        r->threshold = thresh;
+        r->threshold_k = k;
+        r->variant = GG_VAR_AUTO;
+        r->collect_stats = 0;
+    }
+}
+
+// Generic frontier loop shared by the three analytics.
+static gg_status frontier_loop(gg_graph *g, gg_emap_desc &desc, gg_frontier *F, gg_frontier *O,
+                               const gg_run_opts &opt, gg_run_stats *st, bool level_k,
+                               int *iters_out) {
+    int iter = 0;
+    for (;;) {
+        GG_CHECK(frontier_fetch_counts(F));
+        if (F->h_cnt[FC_NACTV] == 0 && !F->all) break;
+        if (level_k) desc.dst_filter_k = iter + 1;
+        gg_emap_stats es;
+        GG_CHECK(edgemap_impl(g, &desc, F, O, opt.collect_stats ? &es : nullptr));
+        if (opt.collect_stats) record_iter(st, iter, es);
+        std::swap(F, O);
+        ++iter;
+        if (iter > (int)g->n + 2) return set_error(g->ctx, GG_ERR_STATE, "frontier loop did not converge");
+    }
+    *iters_out = iter;
+    return GG_OK;
+}
+
+}  // namespace gg
+
+using namespace gg;
+
+extern "C" {
+
+gg_status gg_edgemap(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_frontier *out,
+                     gg_emap_stats *stats) {
+    if (!g || !d) return GG_ERR_ARG;
+    return edgemap_impl(g, d, in, out, stats);
+}
+
+gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop *level,
+                       int32_t *host_level, gg_run_stats *st) {
+    if (!g || root >= g->n) return GG_ERR_ARG;
+    if (level && (level->g != g || level->t != GG_I32)) return set_error(g->ctx, GG_ERR_ARG, "level must be an I32 property of g");
+    gg_run_opts opt;
+    default_opts(o, &opt, GG_THRESH_DEFAULT, 0);
+    TmpProp tl, tp;
+    if (!level) { GG_CHECK(gg_prop_create(g, GG_I32, &tl.p)); level = tl.p; }
+    GG_CHECK(gg_prop_create(g, GG_I32, &tp.p));
+    gg_prop *prev = tp.p;
+    if (st) memset(st, 0, sizeof(*st));
+    uint64_t k0 = g->ctx->launches;
+    RunTimer tm(g->ctx);
+    // BFSLVLv.C:117-129: level = prev = n+1, level[start] = prev[start] = 0
+    int32_t inf = (int32_t)g->n + 1, zero = 0;
+    GG_CHECK(gg_prop_fill(level, &inf));
+    GG_CHECK(gg_prop_fill(prev, &inf));
+    GG_CHECK(gg_prop_set(level, root, &zero));
+    GG_CHECK(gg_prop_set(prev, root, &zero));
+    gg_frontier *F, *O;
+    GG_CHECK(get_tmp_frontiers(g, &F, &O));
+    GG_CHECK(gg_frontier_set_single(F, root));
+    gg_emap_desc desc;
+    memset(&desc, 0, sizeof(desc));
+    desc.relax = GG_RELAX_MIN_PLUS1_I32;
+    desc.a = level;
+    desc.dst_filter = GG_FILTER_GT_CONST;  // level[d] > iter+1   (BFSLVLv.C:190-194)
+    desc.record = GG_RECORD_NE_PREV;       // level[d] != prev[d]  (BFSLVLv.C:168-172)
+    desc.prev = prev;
+    desc.threshold = opt.threshold;
+    desc.threshold_k = opt.threshold_k;
+    desc.variant = opt.variant;
+    int iters = 0;
+    GG_CHECK(frontier_loop(g, desc, F, O, opt, st, true, &iters));
+    double ms = tm.stop();
+    if (st) {
+        st->iterations = iters;
+        st->total_ms = ms;
+        st->kernels = g->ctx->launches - k0;
+    }
+    if (host_level) GG_CHECK(gg_prop_download(level, host_level));
+    return gg_ctx_sync(g->ctx);
+}
+
+gg_status gg_bfs_parent(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop *parent,
+                        uint32_t *host_parent, gg_run_stats *st) {
+    if (!g || root >= g->n) return GG_ERR_ARG;
+    if (parent && (parent->g != g || parent->t != GG_U32)) return set_error(g->ctx, GG_ERR_ARG, "parent must be a U32 property of g");
+    gg_run_opts opt;
+    default_opts(o, &opt, GG_THRESH_DEFAULT, 0);
+    TmpProp tl, tp;
+    if (!parent) { GG_CHECK(gg_prop_create(g, GG_U32, &tl.p)); parent = tl.p; }
+    GG_CHECK(gg_prop_create(g, GG_U32, &tp.p));
+    gg_prop *prev = tp.p;
+    if (st) memset(st, 0, sizeof(*st));
+    uint64_t k0 = g->ctx->launches;
+    RunTimer tm(g->ctx);
+    // BFSv.C:105-113: parent = prev = ~0, parent[start] = prev[start] = start
+    uint32_t unset = 0xFFFFFFFFu;
+    GG_CHECK(gg_prop_fill(parent, &unset));
+    GG_CHECK(gg_prop_fill(prev, &unset));
+    GG_CHECK(gg_prop_set(parent, root, &root));
+    GG_CHECK(gg_prop_set(prev, root, &root));
+    gg_frontier *F, *O;
+    GG_CHECK(get_tmp_frontiers(g, &F, &O));
+    GG_CHECK(gg_frontier_set_single(F, root));
+    gg_emap_desc desc;
+    memset(&desc, 0, sizeof(desc));
+    desc.relax = GG_RELAX_SETIF_U32;       // parent[d].setif(s)   (BFSv.C:144-146)
+    desc.a = parent;
+    desc.dst_filter = GG_FILTER_MSB_SET;   // msbset(parent[d])    (BFSv.C:139-142)
+    desc.src_strong = 1;
+    desc.record = GG_RECORD_NE_PREV;
+    desc.prev = prev;
+    desc.threshold = opt.threshold;
+    desc.threshold_k = opt.threshold_k;
+    desc.variant = opt.variant;
+    int iters = 0;
+    GG_CHECK(frontier_loop(g, desc, F, O, opt, st, false, &iters));
+    double ms = tm.stop();
+    if (st) {
+        st->iterations = iters;
+        st->total_ms = ms;
+        st->kernels = g->ctx->launches - k0;
+    }
+    if (host_parent) GG_CHECK(gg_prop_download(parent, host_parent));
+    return gg_ctx_sync(g->ctx);
+}
+
+gg_status gg_cc(gg_graph *g, const gg_run_opts *o, gg_prop *label, uint32_t *host_label,
+                gg_run_stats *st) {
+    if (!g) return GG_ERR_ARG;
+    if (label && (label->g != g || label->t != GG_U32)) return set_error(g->ctx, GG_ERR_ARG, "label must be a U32 property of g");
+    gg_run_opts opt;
+    default_opts(o, &opt, GG_THRESH_FRAC, 5);  // CCv.C:309 emap_step(F, 5)
+    TmpProp tl, tp;
+    if (!label) { GG_CHECK(gg_prop_create(g, GG_U32, &tl.p)); label = tl.p; }
+    GG_CHECK(gg_prop_create(g, GG_U32, &tp.p));
+    gg_prop *prev = tp.p;
+    if (st) memset(st, 0, sizeof(*st));
+    gg_ctx *ctx = g->ctx;
+    uint64_t k0 = ctx->launches;
+    RunTimer tm(ctx);
+    if (g->n) {
+        // IDs[v] = v (CCv.C:246-248), prevIDs = IDs
+        k_iota_u32<<<persistent_grid(ctx, (g->n + 31) / 32), kBlock, 0, ctx->stream>>>((uint32_t *)label->d, g->n);
+        GG_LAUNCHED(ctx);
+        k_iota_u32<<<persistent_grid(ctx, (g->n + 31) / 32), kBlock, 0, ctx->stream>>>((uint32_t *)prev->d, g->n);
+        GG_LAUNCHED(ctx);
+        if (g->symmetric) {
+            k_preset_zero<<<ctx->sm_count, kBlock, 0, ctx->stream>>>(g->off, g->adj, 0, (uint32_t *)label->d,
+                                                                     (uint32_t *)prev->d);
+            GG_LAUNCHED(ctx);
+        }
+    }
+    gg_frontier *F, *O;
+    GG_CHECK(get_tmp_frontiers(g, &F, &O));
+    GG_CHECK(gg_frontier_set_all(F));
+    gg_emap_desc desc;
+    memset(&desc, 0, sizeof(desc));
+    desc.relax = GG_RELAX_MIN_U32;         // IDs[d].min(IDs[s])   (CCv.C:575-581)
+    desc.a = label;
+    desc.dst_filter = GG_FILTER_NE_ZERO;   // IDs[d] != 0          (CCv.C:566-570)
+    desc.record = GG_RECORD_NE_PREV;       // IDs[d] != prevIDs[d] (CCv.C:546-551)
+    desc.prev = prev;
+    desc.threshold = opt.threshold;
+    desc.threshold_k = opt.threshold_k;
+    desc.variant = opt.variant;
+    int iters = 0;
+    GG_CHECK(frontier_loop(g, desc, F, O, opt, st, false, &iters));
+    double ms = tm.stop();
+    if (st) {
+        st->iterations = iters;
+        st->total_ms = ms;
+        st->kernels = ctx->launches - k0;
+    }
+    if (host_label) GG_CHECK(gg_prop_download(label, host_label));
+    return gg_ctx_sync(ctx);
+}
+
+}  // extern "C"

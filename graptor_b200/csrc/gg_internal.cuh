@@ -1,0 +1,175 @@
+// gg_internal.cuh -- internal types and device helpers of libgg.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "gg.h"
+
+namespace gg {
+
+// ---------------------------------------------------------------------------
+// Errors
+// ---------------------------------------------------------------------------
+gg_status set_error(gg_ctx *ctx, gg_status s, const std::string &msg);
+gg_status cuda_error(gg_ctx *ctx, cudaError_t e, const char *what);
+
+#define GG_CUDA(ctx, expr)                                              \
+    do {                                                                \
+        cudaError_t _e = (expr);                                        \
+        if (_e != cudaSuccess) return ::gg::cuda_error((ctx), _e, #expr); \
+    } while (0)
+
+#define GG_CHECK(expr)                          \
+    do {                                        \
+        gg_status _s = (expr);                  \
+        if (_s != GG_OK) return _s;             \
+    } while (0)
+
+// After a launch: count it and surface launch-configuration errors.
+#define GG_LAUNCHED(ctx)                                                   \
+    do {                                                                   \
+        (ctx)->launches++;                                                 \
+        cudaError_t _e = cudaGetLastError();                               \
+        if (_e != cudaSuccess) return ::gg::cuda_error((ctx), _e, "kernel launch"); \
+    } while (0)
+
+// Device error word bits (set by kernels with bounds checks / bounded waits).
+enum : uint32_t {
+    DEV_ERR_BOUNDS = 1u,
+    DEV_ERR_TIMEOUT = 2u,
+    DEV_ERR_OVERFLOW = 4u,
+};
+
+}  // namespace gg
+
+// ---------------------------------------------------------------------------
+// Handles
+// ---------------------------------------------------------------------------
+struct gg_ctx {
+    int device = 0;
+    int sm_count = 148;
+    size_t l2_bytes = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string err;
+    uint64_t launches = 0;
+    uint32_t *d_err = nullptr;  // device error word
+    uint64_t *h_pinned = nullptr;  // small pinned staging buffer (counts)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+// Frontier counters live on the device in this layout.
+enum {
+    FC_NACTV = 0,   // active vertices
+    FC_NACTE = 1,   // sum of out-degrees of active vertices
+    FC_BIN0 = 2,    // list bin sizes (small / medium / large out-degree)
+    FC_BIN1 = 3,
+    FC_BIN2 = 4,
+    FC_SCANNED = 5, // edges examined by the step that produced this frontier
+    FC_WORDS = 8
+};
+
+enum { NBINS = 3 };
+
+struct gg_graph;
+
+struct gg_frontier {
+    gg_graph *g = nullptr;
+    bool all = false;         // every vertex active (frontier::all_true)
+    bool has_list = false;    // bins valid
+    bool has_bitmap = false;  // bitmap valid
+    uint32_t *bins[NBINS] = {nullptr, nullptr, nullptr};  // each n entries
+    uint32_t *bitmap = nullptr;                            // ceil(n/32) words
+    uint64_t *d_cnt = nullptr;                             // FC_WORDS counters
+    // host copy of counters (valid when host_valid)
+    uint64_t h_cnt[FC_WORDS] = {0};
+    bool host_valid = false;
+};
+
+struct gg_graph {
+    gg_ctx *ctx = nullptr;
+    uint32_t n = 0;
+    uint64_t m = 0;
+    int symmetric = 0;
+    uint64_t *off = nullptr;     // CSR offsets [n+1]
+    uint32_t *adj = nullptr;     // CSR targets [m]
+    uint64_t *in_off = nullptr;  // CSC (== off when symmetric)
+    uint32_t *in_adj = nullptr;
+    uint32_t maxdeg_v = 0, maxdeg = 0;
+    // scratch owned by the graph (grown on demand)
+    void *scratch = nullptr;
+    size_t scratch_bytes = 0;
+    gg_frontier *tmp_front[2] = {nullptr, nullptr};
+    uint64_t *aux_cnt = nullptr;  // counters of steps that record no frontier
+};
+
+struct gg_prop {
+    gg_graph *g = nullptr;
+    gg_dtype t = GG_I32;
+    size_t esz = 4;
+    void *d = nullptr;
+};
+
+namespace gg {
+
+size_t dtype_size(gg_dtype t);
+gg_status graph_scratch(gg_graph *g, size_t bytes, void **p);
+gg_status frontier_alloc_bins(gg_frontier *f);
+gg_status frontier_alloc_bitmap(gg_frontier *f);
+gg_status frontier_fetch_counts(gg_frontier *f);     // device -> host (syncs)
+gg_status frontier_ensure_bitmap(gg_frontier *f);    // from list
+gg_status frontier_ensure_list(gg_frontier *f);      // from bitmap / all
+gg_status frontier_reset_counts(gg_frontier *f);     // async zero of d_cnt
+uint32_t bin_of_degree(uint64_t deg);
+
+// Degree-bin thresholds of the sparse push (tunable by the autotuner).
+struct Tuning {
+    uint32_t bin_small_max = 32;    // deg <= this: thread per vertex
+    uint32_t bin_medium_max = 2048; // deg <= this: warp per vertex, else CTA
+    int pull_k = 8;                 // per-lane edges before warp cooperation (pull)
+    int push_k = 8;
+    int block = 256;
+    int blocks_per_sm = 8;
+};
+Tuning &tuning();
+
+}  // namespace gg
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+namespace gg {
+namespace dev {
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ bool bit_test(const uint32_t *__restrict__ bm, uint32_t v) {
+    return (__ldg(bm + (v >> 5)) >> (v & 31u)) & 1u;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// Block-wide sum of a per-thread value; result valid in thread 0.
+template <typename T, int BLOCK>
+__device__ __forceinline__ T block_sum(T x) {
+    __shared__ T sh[BLOCK / 32];
+    x = warp_sum(x);
+    if (lane_id() == 0) sh[threadIdx.x >> 5] = x;
+    __syncthreads();
+    T r = 0;
+    if (threadIdx.x < 32) {
+        r = (threadIdx.x < BLOCK / 32) ? sh[threadIdx.x] : T(0);
+        r = warp_sum(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+}  // namespace dev
+}  // namespace gg

@@ -1,0 +1,407 @@
+// gg_pr.cu -- PageRank power iteration (PRv / PR_vary) and the ADD_GATHER
+// edgemap.
+//
+// Reference loop (bench/PRv.C:115-290, bench/PR_vary.C:247-447), per
+// iteration:
+//   y[d]  = sum_{s->d} contrib[s]                  dense pull, PRv.C:202-212
+//   s     = sum y                                   (double)   PRv.C:227-231
+//   y    += (1-s)/n                                 dangling + teleport mass
+//   s     = sum y ; y *= 1/s                        renormalise
+//   delta = sum |x-y| (double); x = y; y = 0; contrib = d*x/outdeg
+// until iter == maxiter or delta <= tol.
+//
+// B200 design: two kernels per iteration plus a one-thread bookkeeping
+// kernel, all enqueued up front; a device-resident state block carries the
+// sums and a "done" flag that makes later iterations return immediately once
+// the residual test passes, so the host never synchronises inside the loop.
+//   k_pr_gather : warp owns 32 destinations; short rows summed per lane, long
+//                 rows by the whole warp with 4 independent coalesced loads in
+//                 flight per lane; contributions decoded from the storage
+//                 format (FP32, BF16, FP16, FP8-E4M3 with scale, customfp<6,10>,
+//                 BF16-by-truncation); accumulation in float or double; the
+//                 block sums of y (double) are folded in with one atomic per CTA.
+//   k_pr_update : y += w, y *= 1/s, delta, x = y, contrib = d*x/deg encoded,
+//                 one pass.  The second sum of the reference (sum of the
+//                 rounded y+w) is taken as s + n*w in double: equal in exact
+//                 arithmetic, different by at most n/2 float ulps of 1/n.
+//   k_pr_finish : residual test, iteration count, FP8 scale for the next
+//                 encode (from this iteration's max with 2x headroom).
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_fp8.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "gg_internal.cuh"
+
+namespace gg {
+
+// ---------------------------------------------------------------------------
+// Storage formats
+// ---------------------------------------------------------------------------
+template <int DT> struct Store;
+template <> struct Store<GG_F32> {
+    using T = float;
+    __device__ static float dec(T v) { return v; }
+    __device__ static T enc(float f) { return f; }
+};
+template <> struct Store<GG_BF16> {
+    using T = __nv_bfloat16;
+    __device__ static float dec(T v) { return __bfloat162float(v); }
+    __device__ static T enc(float f) { return __float2bfloat16_rn(f); }
+};
+template <> struct Store<GG_F16> {
+    using T = __half;
+    __device__ static float dec(T v) { return __half2float(v); }
+    __device__ static T enc(float f) { return __float2half_rn(f); }
+};
+template <> struct Store<GG_FP8E4M3> {
+    using T = __nv_fp8_storage_t;
+    __device__ static float dec(T v) {
+        __half_raw h = __nv_cvt_fp8_to_halfraw(v, __NV_E4M3);
+        return __half2float(__half(h));
+    }
+    __device__ static T enc(float f) { return __nv_cvt_float_to_fp8(f, __NV_SATFINITE, __NV_E4M3); }
+};
+// Graptor customfp<6,10> (include/graptor/customfp.h:97-166): low 6 exponent
+// bits + top 10 mantissa bits, truncated; decoding restores exponent bit 6.
+template <> struct Store<GG_CFP_6_10> {
+    using T = uint16_t;
+    __device__ static float dec(T v) { return __uint_as_float(((uint32_t)v | (1u << 16)) << 13); }
+    __device__ static T enc(float f) { return (T)((__float_as_uint(f) >> 13) & 0xFFFFu); }
+};
+// Graptor scustomfp<true,8,7>: bfloat16 by truncation.
+template <> struct Store<GG_BF16_TRUNC> {
+    using T = uint16_t;
+    __device__ static float dec(T v) { return __uint_as_float((uint32_t)v << 16); }
+    __device__ static T enc(float f) { return (T)(__float_as_uint(f) >> 16); }
+};
+
+struct PrState {
+    double s1;        // sum of y after the gather
+    double delta;     // L1 residual of this iteration
+    float cmax;       // max contribution written by the update (for FP8 scaling)
+    float scale;      // encode multiplier of the stored contributions
+    float scale_inv;  // decode multiplier
+    int done;
+    int iters;
+    int maxiter;
+    double tol;
+    double deltas[GG_MAX_ITERS];
+};
+
+constexpr unsigned FULL = 0xffffffffu;
+
+template <int DT, bool ACC64, bool ADD_OLD, int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_pr_gather(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj,
+            const typename Store<DT>::T *__restrict__ contrib, uint32_t n, float *y_f32,
+            double *y_f64, PrState *st, float scale_inv_arg, int K) {
+    using S = Store<DT>;
+    using Acc = typename std::conditional<ACC64, double, float>::type;
+    if (st && st->done) return;
+    const float sinv = st ? st->scale_inv : scale_inv_arg;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwords = (n + 31u) >> 5;
+    const uint32_t nw = (gridDim.x * BLOCK) >> 5;
+    double ysum = 0;
+    for (uint32_t w = (blockIdx.x * BLOCK + threadIdx.x) >> 5; w < nwords; w += nw) {
+        const uint32_t d = (w << 5) + lane;
+        const bool valid = d < n;
+        uint64_t beg = 0, end = 0;
+        if (valid) {
+            beg = in_off[d];
+            end = in_off[d + 1];
+        }
+        Acc acc = 0;
+        const bool shortrow = end - beg <= (uint64_t)K;
+        if (valid && shortrow) {
+            for (uint64_t e = beg; e < end; ++e) acc += (Acc)S::dec(contrib[__ldg(in_adj + e)]);
+        }
+        unsigned pend = __ballot_sync(FULL, valid && !shortrow);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint64_t bj = __shfl_sync(FULL, beg, j);
+            const uint64_t ej = __shfl_sync(FULL, end, j);
+            Acc part = 0;
+            uint64_t base = bj;
+            for (; base + 128 <= ej; base += 128) {
+                uint32_t s0 = __ldg(in_adj + base + lane);
+                uint32_t s1 = __ldg(in_adj + base + 32 + lane);
+                uint32_t s2 = __ldg(in_adj + base + 64 + lane);
+                uint32_t s3 = __ldg(in_adj + base + 96 + lane);
+                part += (Acc)S::dec(contrib[s0]) + (Acc)S::dec(contrib[s1]) +
+                        (Acc)S::dec(contrib[s2]) + (Acc)S::dec(contrib[s3]);
+            }
+            for (; base < ej; base += 32) {
+                uint64_t e = base + lane;
+                if (e < ej) part += (Acc)S::dec(contrib[__ldg(in_adj + e)]);
+            }
+            part = dev::warp_sum(part);
+            if ((int)lane == j) acc = part;
+        }
+        if (valid) {
+            if (DT == GG_FP8E4M3) acc *= (Acc)sinv;
+            if (y_f64) {
+                double v = ADD_OLD ? y_f64[d] + (double)acc : (double)acc;
+                y_f64[d] = v;
+                ysum += v;
+            } else {
+                float v = ADD_OLD ? (float)((double)y_f32[d] + (double)acc) : (float)acc;
+                y_f32[d] = v;
+                ysum += (double)v;
+            }
+        }
+    }
+    if (st) {
+        ysum = dev::block_sum<double, BLOCK>(ysum);
+        if (threadIdx.x == 0) atomicAdd(&st->s1, ysum);
+    }
+}
+
+template <int DT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_pr_update(const float *__restrict__ y, float *__restrict__ x, typename Store<DT>::T *contrib,
+            const uint64_t *__restrict__ off, uint32_t n, float damp, int renorm_f32, PrState *st) {
+    using S = Store<DT>;
+    if (st->done) return;
+    const double s1 = st->s1;
+    const double w = (1.0 - s1) / (double)n;
+    const double s2 = s1 + (double)n * w;
+    const float wf32 = 1.0f / (float)s2;
+    const double wf64 = 1.0 / s2;
+    const float enc_scale = st->scale;
+    double dl = 0;
+    float cm = 0.0f;
+    const uint32_t stride = gridDim.x * BLOCK;
+    for (uint32_t v = blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
+        float yv = (float)((double)y[v] + w);
+        yv = renorm_f32 ? yv * wf32 : (float)((double)yv * wf64);
+        const float xv = x[v];
+        dl += (double)fabsf(xv - yv);
+        x[v] = yv;
+        const uint64_t deg = off[v + 1] - off[v];
+        const float c = damp * yv / (float)deg;
+        contrib[v] = S::enc(DT == GG_FP8E4M3 ? c * enc_scale : c);
+        if (deg && c > cm) cm = c;
+    }
+    dl = dev::block_sum<double, BLOCK>(dl);
+    // max of non-negative floats: integer order of the bit patterns
+    __shared__ float sh[BLOCK / 32];
+    for (int o = 16; o > 0; o >>= 1) cm = fmaxf(cm, __shfl_xor_sync(FULL, cm, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = cm;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float b = 0.0f;
+        for (int i = 0; i < BLOCK / 32; ++i) b = fmaxf(b, sh[i]);
+        atomicAdd(&st->delta, dl);
+        atomicMax((int *)&st->cmax, __float_as_int(b));
+    }
+}
+
+// Largest power of two p with cmax * p * 2 <= 448 (2x headroom).
+__device__ __host__ inline float fp8_scale_for(float cmax) {
+    if (!(cmax > 0.0f)) return 1.0f;
+    int e;
+    frexpf(224.0f / cmax, &e);
+    return ldexpf(1.0f, e - 1);
+}
+
+__global__ void k_pr_finish(PrState *st) {
+    if (st->done) return;
+    const int it = st->iters;
+    if (it < GG_MAX_ITERS) st->deltas[it] = st->delta;
+    st->iters = it + 1;
+    if (st->iters >= st->maxiter || !(st->delta > st->tol)) st->done = 1;
+    st->scale_inv = 1.0f / st->scale;  // decode of what the update just wrote
+    st->scale = fp8_scale_for(st->cmax);  // next encode
+    st->s1 = 0;
+    st->delta = 0;
+    st->cmax = 0.0f;
+}
+
+// Initial x = 1/n, contrib = d*x/deg (PRv.C:155-182); first pass finds the max.
+template <int DT, int BLOCK>
+__global__ void k_pr_init(float *x, typename Store<DT>::T *contrib, const uint64_t *off, uint32_t n,
+                          float damp, PrState *st, int pass) {
+    using S = Store<DT>;
+    const float x0 = 1.0f / (float)n;
+    float cm = 0.0f;
+    const uint32_t stride = gridDim.x * BLOCK;
+    const float scale = pass == 1 ? fp8_scale_for(st->cmax) : 1.0f;
+    for (uint32_t v = blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
+        const uint64_t deg = off[v + 1] - off[v];
+        const float c = damp * x0 / (float)deg;
+        if (pass == 0) {
+            if (deg && c > cm) cm = c;
+        } else {
+            x[v] = x0;
+            contrib[v] = S::enc(DT == GG_FP8E4M3 ? c * scale : c);
+        }
+    }
+    if (pass == 0) {
+        for (int o = 16; o > 0; o >>= 1) cm = fmaxf(cm, __shfl_xor_sync(FULL, cm, o));
+        if ((threadIdx.x & 31) == 0) atomicMax((int *)&st->cmax, __float_as_int(cm));
+    } else if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->scale = scale;
+        st->scale_inv = 1.0f / scale;
+        st->cmax = 0.0f;
+    }
+}
+
+constexpr int kBlock = 256;
+
+static unsigned pr_grid(gg_ctx *ctx, uint64_t work) {
+    uint64_t b = (work + kBlock - 1) / kBlock;
+    uint64_t cap = (uint64_t)ctx->sm_count * tuning().blocks_per_sm;
+    if (b > cap) b = cap;
+    return (unsigned)(b ? b : 1);
+}
+
+template <int DT>
+static gg_status pr_run(gg_graph *g, const gg_pr_params *p, float *x, float *y, void *contrib,
+                        PrState *st) {
+    gg_ctx *ctx = g->ctx;
+    cudaStream_t s = ctx->stream;
+    using T = typename Store<DT>::T;
+    const uint32_t n = g->n;
+    const unsigned gw = pr_grid(ctx, (uint64_t)((n + 31) / 32) * 32);
+    const unsigned gv = pr_grid(ctx, n);
+    k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, n, p->damping, st, 0);
+    GG_LAUNCHED(ctx);
+    k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, n, p->damping, st, 1);
+    GG_LAUNCHED(ctx);
+    const int K = tuning().pull_k;
+    for (int it = 0; it < p->maxiter; ++it) {
+        if (p->accum_f64)
+            k_pr_gather<DT, true, false, kBlock><<<gw, kBlock, 0, s>>>(g->in_off, g->in_adj, (const T *)contrib, n,
+                                                                      y, nullptr, st, 1.0f, K);
+        else
+            k_pr_gather<DT, false, false, kBlock><<<gw, kBlock, 0, s>>>(g->in_off, g->in_adj, (const T *)contrib, n,
+                                                                       y, nullptr, st, 1.0f, K);
+        GG_LAUNCHED(ctx);
+        k_pr_update<DT, kBlock><<<gv, kBlock, 0, s>>>(y, x, (T *)contrib, g->off, n, p->damping, p->renorm_f32, st);
+        GG_LAUNCHED(ctx);
+        k_pr_finish<<<1, 1, 0, s>>>(st);
+        GG_LAUNCHED(ctx);
+    }
+    return GG_OK;
+}
+
+// ADD_GATHER edgemap: y[d] += sum_{s in in(d), s active} dec(contrib[s]) * scale.
+template <int DT>
+static gg_status gather_api(gg_graph *g, const gg_emap_desc *d) {
+    gg_ctx *ctx = g->ctx;
+    using T = typename Store<DT>::T;
+    const unsigned gw = pr_grid(ctx, (uint64_t)((g->n + 31) / 32) * 32);
+    float *yf = d->a->t == GG_F32 ? (float *)d->a->d : nullptr;
+    double *yd = d->a->t == GG_F64 ? (double *)d->a->d : nullptr;
+    const float sc = d->src_scale != 0.0f ? d->src_scale : 1.0f;
+    if (d->accum_f64)
+        k_pr_gather<DT, true, true, kBlock><<<gw, kBlock, 0, ctx->stream>>>(
+            g->in_off, g->in_adj, (const T *)d->src->d, g->n, yf, yd, nullptr, sc, tuning().pull_k);
+    else
+        k_pr_gather<DT, false, true, kBlock><<<gw, kBlock, 0, ctx->stream>>>(
+            g->in_off, g->in_adj, (const T *)d->src->d, g->n, yf, yd, nullptr, sc, tuning().pull_k);
+    GG_LAUNCHED(ctx);
+    return GG_OK;
+}
+
+gg_status pr_edgemap_gather(gg_graph *g, const gg_emap_desc *d, gg_frontier *in) {
+    gg_ctx *ctx = g->ctx;
+    if (in && !in->all) return set_error(ctx, GG_ERR_UNSUPPORTED, "ADD_GATHER runs over all vertices (no src filter)");
+    if (!d->src || d->src->g != g) return set_error(ctx, GG_ERR_ARG, "ADD_GATHER needs a contribution property of g");
+    if (d->a->t != GG_F32 && d->a->t != GG_F64) return set_error(ctx, GG_ERR_ARG, "ADD_GATHER accumulator must be F32 or F64");
+    if (d->dst_filter != GG_FILTER_NONE) return set_error(ctx, GG_ERR_UNSUPPORTED, "ADD_GATHER takes no dst filter");
+    if (d->src_scale != 0.0f && d->src->t != GG_FP8E4M3)
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "src_scale applies to FP8 contributions only");
+    switch (d->src->t) {
+    case GG_F32: return gather_api<GG_F32>(g, d);
+    case GG_BF16: return gather_api<GG_BF16>(g, d);
+    case GG_F16: return gather_api<GG_F16>(g, d);
+    case GG_FP8E4M3: return gather_api<GG_FP8E4M3>(g, d);
+    case GG_CFP_6_10: return gather_api<GG_CFP_6_10>(g, d);
+    case GG_BF16_TRUNC: return gather_api<GG_BF16_TRUNC>(g, d);
+    default: return set_error(ctx, GG_ERR_UNSUPPORTED, "contribution dtype");
+    }
+}
+
+}  // namespace gg
+
+using namespace gg;
+
+extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x, float *host_x,
+                                 gg_run_stats *stats) {
+    if (!g || !p) return GG_ERR_ARG;
+    gg_ctx *ctx = g->ctx;
+    if (p->maxiter < 0 || p->maxiter > GG_MAX_ITERS) return set_error(ctx, GG_ERR_ARG, "maxiter out of range");
+    if (x && (x->g != g || x->t != GG_F32)) return set_error(ctx, GG_ERR_ARG, "x must be an F32 property of g");
+    const int dt = p->contrib_dtype;
+    if (dt != GG_F32 && dt != GG_BF16 && dt != GG_F16 && dt != GG_FP8E4M3 && dt != GG_CFP_6_10 &&
+        dt != GG_BF16_TRUNC)
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "contribution dtype");
+    if (g->n == 0) return GG_OK;
+    gg_prop *xp = x, *tmpx = nullptr;
+    if (!xp) {
+        GG_CHECK(gg_prop_create(g, GG_F32, &tmpx));
+        xp = tmpx;
+    }
+    // scratch: y (f32), contrib (up to 4 B), state
+    const size_t nb = (((size_t)g->n + 1) * 4 + 255) / 256 * 256;
+    void *base = nullptr;
+    gg_status s = graph_scratch(g, 2 * nb + sizeof(PrState), &base);
+    if (s != GG_OK) { if (tmpx) gg_prop_destroy(tmpx); return s; }
+    float *y = (float *)base;
+    void *contrib = (char *)base + nb;
+    PrState *st = (PrState *)((char *)base + 2 * nb);
+    PrState init;
+    memset(&init, 0, sizeof(init));
+    init.maxiter = p->maxiter;
+    init.tol = p->tol;
+    init.scale = 1.0f;
+    init.scale_inv = 1.0f;
+    init.done = p->maxiter == 0;
+    uint64_t k0 = ctx->launches;
+    cudaEventRecord(ctx->ev0, ctx->stream);
+    cudaError_t e = cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) {
+        switch (dt) {
+        case GG_F32: s = pr_run<GG_F32>(g, p, (float *)xp->d, y, contrib, st); break;
+        case GG_BF16: s = pr_run<GG_BF16>(g, p, (float *)xp->d, y, contrib, st); break;
+        case GG_F16: s = pr_run<GG_F16>(g, p, (float *)xp->d, y, contrib, st); break;
+        case GG_FP8E4M3: s = pr_run<GG_FP8E4M3>(g, p, (float *)xp->d, y, contrib, st); break;
+        case GG_CFP_6_10: s = pr_run<GG_CFP_6_10>(g, p, (float *)xp->d, y, contrib, st); break;
+        default: s = pr_run<GG_BF16_TRUNC>(g, p, (float *)xp->d, y, contrib, st); break;
+        }
+    } else {
+        s = cuda_error(ctx, e, "gg_pagerank state upload");
+    }
+    cudaEventRecord(ctx->ev1, ctx->stream);
+    PrState fin;
+    if (s == GG_OK) {
+        e = cudaMemcpyAsync(&fin, st, sizeof(fin), cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) s = cuda_error(ctx, e, "gg_pagerank");
+    }
+    if (s == GG_OK && stats) {
+        memset(stats, 0, sizeof(*stats));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        stats->total_ms = ms;
+        stats->iterations = fin.iters;
+        stats->kernels = ctx->launches - k0;
+        for (int i = 0; i < fin.iters && i < GG_MAX_ITERS; ++i) {
+            stats->delta[i] = fin.deltas[i];
+            stats->variant[i] = GG_VAR_PULL_DENSE;
+            stats->scanned[i] = g->m;
+            stats->nactv[i] = g->n;
+            stats->nacte[i] = g->m;
+        }
+        stats->scanned_edges = (uint64_t)fin.iters * g->m;
+    }
+    if (s == GG_OK && host_x) s = gg_prop_download(xp, host_x);
+    if (tmpx) gg_prop_destroy(tmpx);
+    return s;
+}

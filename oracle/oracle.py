@@ -1,0 +1,300 @@
+"""Python handle on the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/liboracle.so`` (built from ``oracle/oracle.c`` by
+``oracle/Makefile``) and the reference-built programs under ``oracle/_ref/``.
+Only the test suite, the smoke check and the benchmark's CPU-baseline leg
+import this module; the GPU library never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+# contribution storage formats of orc_pr_vary (must match oracle.c)
+F32, F64, BF16, F16, FP8, CFP_6_10, BF16_TRUNC = range(7)
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"oracle library missing: {LIB_PATH} (run make -C oracle)")
+        L = C.CDLL(LIB_PATH)
+        u64p = C.POINTER(C.c_uint64)
+        u32p = C.POINTER(C.c_uint32)
+        L.orc_gen_rmat.argtypes = [C.c_int, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                                   C.c_uint64, C.c_int, u32p, u64p,
+                                   C.POINTER(u64p), C.POINTER(u32p)]
+        L.orc_gen_er.argtypes = [C.c_uint32, C.c_double, C.c_uint32, C.c_uint64, C.c_int,
+                                 u32p, u64p, C.POINTER(u64p), C.POINTER(u32p)]
+        L.orc_gen_grid.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                   u32p, u64p, C.POINTER(u64p), C.POINTER(u32p)]
+        L.orc_transpose.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p,
+                                    C.POINTER(u64p), C.POINTER(u32p)]
+        L.orc_write_bin.argtypes = [C.c_char_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p]
+        L.orc_read_bin.argtypes = [C.c_char_p, u32p, u64p, C.POINTER(u64p), C.POINTER(u32p)]
+        L.orc_bfs_level.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        L.orc_reached_edges.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p]
+        L.orc_reached_edges.restype = C.c_uint64
+        L.orc_check_parents.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
+                                        C.c_void_p, C.c_void_p]
+        L.orc_check_parents.restype = C.c_uint64
+        L.orc_cc.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_pr_f32.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                 C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_pr_f64.argtypes = L.orc_pr_f32.argtypes
+        L.orc_pr_vary.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                  C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_cfp_from_float.argtypes = [C.c_float, C.c_int, C.c_int, C.c_int]
+        L.orc_cfp_from_float.restype = C.c_uint32
+        L.orc_cfp_to_float.argtypes = [C.c_uint32, C.c_int, C.c_int, C.c_int]
+        L.orc_cfp_to_float.restype = C.c_float
+        L.orc_free.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+@dataclass
+class Graph:
+    """Host CSR: off uint64[n+1], adj uint32[m]."""
+    n: int
+    off: np.ndarray
+    adj: np.ndarray
+
+    @property
+    def m(self) -> int:
+        return int(self.off[-1])
+
+    def outdeg(self) -> np.ndarray:
+        return np.diff(self.off).astype(np.uint32)
+
+    def transpose(self) -> "Graph":
+        L = lib()
+        po, pa = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+        if L.orc_transpose(self.n, _p(self.off), _p(self.adj), C.byref(po), C.byref(pa)):
+            raise MemoryError("orc_transpose")
+        return _take(self.n, self.m, po, pa)
+
+
+def _take(n, m, po, pa) -> Graph:
+    L = lib()
+    off = np.ctypeslib.as_array(po, shape=(n + 1,)).copy()
+    adj = np.ctypeslib.as_array(pa, shape=(max(m, 1),))[:m].copy()
+    L.orc_free(C.cast(po, C.c_void_p))
+    L.orc_free(C.cast(pa, C.c_void_p))
+    return Graph(n, off, adj)
+
+
+def _gen(fn, *args) -> Graph:
+    n, m = C.c_uint32(), C.c_uint64()
+    po, pa = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+    rc = fn(*args, C.byref(n), C.byref(m), C.byref(po), C.byref(pa))
+    if rc:
+        raise RuntimeError(f"generator failed ({rc})")
+    return _take(n.value, m.value, po, pa)
+
+
+def rmat(scale: int, nedges: int, seed: int, a=0.57, b=0.19, c=0.19, symmetric=True) -> Graph:
+    return _gen(lib().orc_gen_rmat, scale, nedges, a, b, c, seed, int(symmetric))
+
+
+def er(n: int, avgdeg: float, seed: int, dangling_bp: int = 0, symmetric=True) -> Graph:
+    return _gen(lib().orc_gen_er, n, avgdeg, dangling_bp, seed, int(symmetric))
+
+
+def grid(rows: int, cols: int, seed: int, del_bp: int = 0) -> Graph:
+    return _gen(lib().orc_gen_grid, rows, cols, del_bp, seed)
+
+
+def from_edges(n: int, edges, symmetric=True) -> Graph:
+    """Small hand-made graphs for edge-case tests (dedup, no self-loops)."""
+    e = np.asarray(edges, dtype=np.int64).reshape(-1, 2)
+    if symmetric and len(e):
+        e = np.concatenate([e, e[:, ::-1]])
+    e = e[e[:, 0] != e[:, 1]] if len(e) else e
+    if len(e):
+        e = np.unique(e, axis=0)
+    off = np.zeros(n + 1, dtype=np.uint64)
+    if len(e):
+        np.add.at(off, e[:, 0] + 1, 1)
+    off = np.cumsum(off).astype(np.uint64)
+    adj = e[:, 1].astype(np.uint32) if len(e) else np.zeros(0, dtype=np.uint32)
+    return Graph(n, off, adj)
+
+
+def write_bin(g: Graph, path: str) -> None:
+    if lib().orc_write_bin(path.encode(), g.n, g.m, _p(g.off), _p(g.adj)):
+        raise OSError(f"write_bin {path}")
+
+
+def read_bin(path: str) -> Graph:
+    n, m = C.c_uint32(), C.c_uint64()
+    po, pa = C.POINTER(C.c_uint64)(), C.POINTER(C.c_uint32)()
+    rc = lib().orc_read_bin(path.encode(), C.byref(n), C.byref(m), C.byref(po), C.byref(pa))
+    if rc:
+        raise OSError(f"read_bin {path}: {rc}")
+    return _take(n.value, m.value, po, pa)
+
+
+def bfs_level(g: Graph, root: int) -> np.ndarray:
+    lv = np.empty(g.n, dtype=np.int32)
+    lib().orc_bfs_level(g.n, _p(g.off), _p(g.adj), root, _p(lv))
+    return lv
+
+
+def reached_edges(g: Graph, level: np.ndarray) -> int:
+    level = np.ascontiguousarray(level, dtype=np.int32)
+    return int(lib().orc_reached_edges(g.n, _p(g.off), _p(level)))
+
+
+def check_parents(g: Graph, root: int, parent: np.ndarray, level: np.ndarray) -> int:
+    parent = np.ascontiguousarray(parent, dtype=np.uint32)
+    level = np.ascontiguousarray(level, dtype=np.int32)
+    return int(lib().orc_check_parents(g.n, _p(g.off), _p(g.adj), root, _p(parent), _p(level)))
+
+
+def cc(g: Graph) -> np.ndarray:
+    lab = np.empty(g.n, dtype=np.uint32)
+    lib().orc_cc(g.n, _p(g.off), _p(g.adj), _p(lab))
+    return lab
+
+
+def pagerank(g: Graph, maxiter: int = 20, tol: float = 1e-7, f64: bool = False,
+             csc: Graph | None = None):
+    """PRv-style power iteration; returns (x, iters, deltas)."""
+    csc = csc if csc is not None else g.transpose()
+    outdeg = g.outdeg()
+    x = np.empty(g.n, dtype=np.float64 if f64 else np.float32)
+    deltas = np.zeros(max(maxiter, 1), dtype=np.float64)
+    fn = lib().orc_pr_f64 if f64 else lib().orc_pr_f32
+    it = fn(g.n, _p(csc.off), _p(csc.adj), _p(outdeg), maxiter, tol, _p(x), _p(deltas))
+    return x, it, deltas[:it]
+
+
+def pagerank_vary(g: Graph, fmt: int, accum_f64: bool, maxiter: int = 100, tol: float = 1e-7,
+                  csc: Graph | None = None):
+    csc = csc if csc is not None else g.transpose()
+    outdeg = g.outdeg()
+    x = np.empty(g.n, dtype=np.float32)
+    deltas = np.zeros(max(maxiter, 1), dtype=np.float64)
+    it = lib().orc_pr_vary(g.n, _p(csc.off), _p(csc.adj), _p(outdeg), fmt, int(accum_f64),
+                           maxiter, tol, _p(x), _p(deltas))
+    return x, it, deltas[:it]
+
+
+def cfp_from_float(f: float, S: int, E: int, M: int) -> int:
+    return int(lib().orc_cfp_from_float(f, S, E, M))
+
+
+def cfp_to_float(c: int, S: int, E: int, M: int) -> float:
+    return float(lib().orc_cfp_to_float(c, S, E, M))
+
+
+# ---------------------------------------------------------------------------
+# The reference's own programs, built from its sources by oracle/Makefile.
+# ---------------------------------------------------------------------------
+
+def ref_variant() -> str:
+    """Pick the reference build the host CPU can execute (AVX-512 or AVX2)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = f.read()
+    except OSError:
+        flags = ""
+    return "avx512" if " avx512f" in flags and " avx512bw" in flags else "avx2"
+
+
+def ref_prog(name: str) -> str | None:
+    p = os.path.join(REF_DIR, ref_variant(), name)
+    return p if os.path.exists(p) else None
+
+
+def ref_available(name: str = "ref_bfslvl") -> bool:
+    return ref_prog(name) is not None
+
+
+def _run(args, threads: int | None = None, timeout: int = 1800) -> str:
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    r = subprocess.run(args, capture_output=True, text=True, env=env, timeout=timeout)
+    if r.returncode != 0:
+        raise RuntimeError(f"{args[0]} failed rc={r.returncode}: {r.stderr[-2000:]}")
+    return r.stdout
+
+
+class PaddedGraph(RuntimeError):
+    """The reference's VEBO layout padded the vertex set (VEBOReorder.h:700-712);
+    its PageRank then runs over the padded count and is not comparable."""
+
+
+def ref_bfs(bin_path: str, roots, out_prefix: str | None = None, parents: bool = False,
+            threads: int | None = None):
+    """Run the reference BFSLVLv (or BFSv) from each root.
+
+    Returns a list of (root, seconds, reached, per-vertex int32 array or None)."""
+    prog = ref_prog("ref_bfsv" if parents else "ref_bfslvl")
+    if prog is None:
+        raise RuntimeError("reference BFS harness not built")
+    outp = out_prefix or "-"
+    txt = _run([prog, bin_path, outp] + [str(r) for r in roots], threads)
+    res = []
+    for line in txt.splitlines():
+        if line.startswith("n "):
+            f = line.split()
+            if int(f[1]) != int(f[3]):
+                raise PaddedGraph(f"reference padded {f[1]} vertices to {f[3]}")
+        if not line.startswith("root "):
+            continue
+        f = line.split()
+        r, t, k = int(f[1]), float(f[3]), int(f[5])
+        arr = None
+        if out_prefix:
+            arr = np.fromfile(f"{out_prefix}.{r}.i32", dtype=np.int32)
+        res.append((r, t, k, arr))
+    return res
+
+
+def _running_times(txt: str):
+    return [float(l.split(":")[1]) for l in txt.splitlines() if l.startswith("Running")]
+
+
+def ref_cc(bin_path: str, out_path: str, threads: int | None = None, rounds: int = 1):
+    """Reference CCv: returns (labels uint32 in original order, [round seconds])."""
+    prog = ref_prog("CCv")
+    txt = _run([prog, "-s", "-b", "-rounds", str(rounds), "-c", "256",
+                "-cc:outfile", out_path, bin_path], threads)
+    lab = np.loadtxt(out_path, dtype=np.uint64).astype(np.uint32)
+    n = int(np.fromfile(bin_path, dtype=np.uint64, count=3)[2])
+    if len(lab) != n:
+        raise PaddedGraph(f"reference padded {n} vertices to {len(lab)}")
+    return lab, _running_times(txt)
+
+
+def ref_pr(bin_path: str, out_path: str, maxiter: int = 20, threads: int | None = None,
+           prog_name: str = "PRv", symmetric: bool = True, rounds: int = 1):
+    """Reference PRv / PR_vary: returns (x float64 array, [round seconds])."""
+    prog = ref_prog(prog_name)
+    args = [prog] + (["-s"] if symmetric else []) + [
+        "-b", "-rounds", str(rounds), "-c", "256", "-pr:maxiter", str(maxiter),
+        "-pr:outfile", out_path, bin_path]
+    txt = _run(args, threads)
+    x = np.loadtxt(out_path, dtype=np.float64)
+    n = int(np.fromfile(bin_path, dtype=np.uint64, count=3)[2])
+    if len(x) != n:
+        raise PaddedGraph(f"reference padded {n} vertices to {len(x)}")
+    return x, _running_times(txt)

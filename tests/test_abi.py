@@ -1,0 +1,66 @@
+"""CPU checks of the C ABI: the library loads and exports every entry point
+that include/*.h declares (no compute calls: there may be no GPU here)."""
+import ctypes as C
+import glob
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "graptor_b200", "libgg.so")
+
+
+def declared():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        txt = open(h).read()
+        names |= set(re.findall(r"GG_API\s+[\w\s\*]+?\b(gg_\w+)\s*\(", txt))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    for must in ["gg_ctx_create", "gg_graph_upload", "gg_edgemap", "gg_vertexmap",
+                 "gg_bfs_level", "gg_cc", "gg_pagerank", "gg_frontier_create", "gg_prop_create"]:
+        assert must in names
+
+
+def test_library_exports_all_declared():
+    if not os.path.exists(LIB):
+        from graptor_b200 import build
+        build.build()
+    L = C.CDLL(LIB)
+    missing = [n for n in sorted(declared()) if not hasattr(L, n)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", LIB], capture_output=True, text=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l}
+    assert declared() <= exported
+    # nothing but the C ABI leaks out of the shared object
+    assert all(n.startswith("gg_") for n in exported), sorted(n for n in exported if not n.startswith("gg_"))
+
+
+def test_status_strings_and_sizes():
+    from graptor_b200 import gg
+    L = gg.lib()
+    assert L.gg_status_string(gg.GG_ERR_TIMEOUT) == b"GG_ERR_TIMEOUT"
+    assert L.gg_dtype_size(gg.BF16) == 2 and L.gg_dtype_size(gg.F64) == 8
+    assert L.gg_dtype_size(gg.FP8E4M3) == 1
+
+
+def test_null_arguments_rejected_without_gpu():
+    from graptor_b200 import gg
+    L = gg.lib()
+    assert L.gg_ctx_create(0, None) == gg.GG_ERR_ARG
+    assert L.gg_edgemap(None, None, None, None, None) == gg.GG_ERR_ARG
+    assert L.gg_graph_destroy(None) == gg.GG_ERR_ARG
+
+
+def test_ctx_create_reports_missing_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from graptor_b200 import gg
+    h = C.c_void_p()
+    assert gg.lib().gg_ctx_create(0, C.byref(h)) == gg.GG_ERR_NOT_FOUND

@@ -1,0 +1,283 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle and the
+reference's golden outputs.  BFS levels and CC labels bit-exact, BFS parents
+a valid BFS tree, PageRank within stated L1 tolerances."""
+import glob
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from graptor_b200 import gg
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+VARIANTS = [gg.VAR_PUSH_SPARSE, gg.VAR_PUSH_MERGE, gg.VAR_PULL_DENSE, gg.VAR_PUSH_DENSE]
+
+# PageRank tolerances (L1 over all vertices, ranks sum to 1)
+PR_L1_VS_REF_F32 = 1e-6    # FP32 GPU run vs the reference FP32 run (PRv)
+PR_L1_VS_F64 = {gg.F32: 1e-6, gg.BF16: 1e-4, gg.F16: 1e-4, gg.FP8E4M3: 3e-2,
+                gg.CFP_6_10: 2e-3, gg.BF16_TRUNC: 2e-3}
+
+
+def golden(name):
+    return np.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def upload(ctx, g, symmetric=True):
+    return ctx.upload(g.off, g.adj, symmetric)
+
+
+def golden_names():
+    return [os.path.basename(p)[:-4] for p in sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+            if "config1" not in p]
+
+
+def test_generator_matches_oracle(ctx):
+    for (scale, ef, seed) in [(10, 8, 3), (12, 16, 5)]:
+        dg = ctx.rmat(scale, ef << scale, seed)
+        og = O.rmat(scale, ef << scale, seed)
+        off, adj = dg.download()
+        assert np.array_equal(off, og.off) and np.array_equal(adj, og.adj)
+    dg = ctx.grid(17, 23, seed=9, del_bp=300)
+    og = O.grid(17, 23, seed=9, del_bp=300)
+    off, adj = dg.download()
+    assert np.array_equal(off, og.off) and np.array_equal(adj, og.adj)
+    dg = ctx.er(3000, 12.0, seed=4, dangling_bp=100, symmetric=False)
+    og = O.er(3000, 12.0, seed=4, dangling_bp=100, symmetric=False)
+    off, adj = dg.download()
+    assert np.array_equal(off, og.off) and np.array_equal(adj, og.adj)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_golden_bfs_cc_pr(ctx, name):
+    z = golden(name)
+    g = ctx.upload(z["off"], z["adj"], True)
+    og = O.Graph(int(z["n"]), z["off"], z["adj"])
+    for r, lv in zip(z["bfs_roots"], z["bfs_levels"]):
+        assert np.array_equal(g.bfs_level(int(r)), lv)
+        pa = g.bfs_parent(int(r))
+        assert O.check_parents(og, int(r), pa, lv) == 0
+    assert np.array_equal(g.cc(), z["cc"])
+    x = g.pagerank(maxiter=int(z["pr_iters"]), contrib=gg.F32, accum_f64=True, renorm_f32=True)
+    assert np.abs(x.astype(np.float64) - z["pr"]).sum() <= PR_L1_VS_REF_F32
+
+
+def test_config1_rmat16(ctx):
+    """The small configuration end to end: R-MAT 16 generated on the device,
+    CSR hash and BFS/CC/PR outputs against the reference's own run."""
+    z = golden("config1_rmat16")
+    g = ctx.rmat(int(z["scale"]), int(z["nedges"]), int(z["seed"]))
+    off, adj = g.download()
+    h = hashlib.sha256()
+    h.update(off.tobytes())
+    h.update(adj.tobytes())
+    assert h.hexdigest() == str(z["sha256"])
+    root, _ = g.max_degree_vertex()
+    assert root == int(z["bfs_roots"][0])
+    assert np.array_equal(g.bfs_level(root), z["bfs_levels"][0])
+    og = O.Graph(g.n, off, adj)
+    assert O.check_parents(og, root, g.bfs_parent(root), z["bfs_levels"][0]) == 0
+    assert np.array_equal(g.cc(), z["cc"])
+    x = g.pagerank(maxiter=20)
+    assert np.abs(x.astype(np.float64) - z["pr"]).sum() <= PR_L1_VS_REF_F32
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_bfs_every_variant(ctx, variant):
+    og = O.rmat(13, 16 << 13, seed=21)
+    g = upload(ctx, og)
+    deg = og.outdeg()
+    rng = np.random.default_rng(0)
+    roots = [int(np.argmax(deg))] + [int(x) for x in rng.choice(np.flatnonzero(deg), 3)] + [
+        int(np.flatnonzero(deg == 0)[0])]
+    opts = gg.default_opts(variant=variant)
+    for r in roots:
+        ref = O.bfs_level(og, r)
+        assert np.array_equal(g.bfs_level(r, opts=opts), ref)
+        assert O.check_parents(og, r, g.bfs_parent(r, opts=opts), ref) == 0
+    assert np.array_equal(g.cc(opts=opts), O.cc(og))
+
+
+@pytest.mark.parametrize("thresh,k", [(gg.THRESH_DEFAULT, 0), (gg.THRESH_FRAC, 5),
+                                      (gg.THRESH_FRAC, 200), (gg.THRESH_ALWAYS_SPARSE, 0),
+                                      (gg.THRESH_ALWAYS_DENSE, 0)])
+def test_thresholds_same_fixed_point(ctx, thresh, k):
+    og = O.grid(64, 96, seed=2, del_bp=100)
+    g = upload(ctx, og)
+    opts = gg.default_opts(threshold=thresh, k=k)
+    assert np.array_equal(g.bfs_level(5, opts=opts), O.bfs_level(og, 5))
+    assert np.array_equal(g.cc(opts=opts), O.cc(og))
+
+
+def test_edge_cases(ctx):
+    # single vertex, no edges
+    g = ctx.upload(np.zeros(2, dtype=np.uint64), np.zeros(0, dtype=np.uint32))
+    assert list(g.bfs_level(0)) == [0]
+    assert list(g.cc()) == [0]
+    assert list(g.bfs_parent(0)) == [0]
+    # isolated root in a larger graph
+    og = O.from_edges(40, [(1, 2), (2, 3), (5, 6)])
+    g = upload(ctx, og)
+    lv = g.bfs_level(0)
+    assert lv[0] == 0 and np.all(lv[1:] == 41)
+    assert np.array_equal(g.cc(), O.cc(og))
+    # star: one hub with a huge row (CTA bin) and leaves (thread bin)
+    n = 50000
+    og = O.from_edges(n, [(0, i) for i in range(1, n)])
+    g = upload(ctx, og)
+    for v in VARIANTS:
+        o = gg.default_opts(variant=v)
+        assert np.array_equal(g.bfs_level(7, opts=o), O.bfs_level(og, 7))
+    assert np.array_equal(g.cc(), O.cc(og))
+    # long path (high diameter, many sparse iterations)
+    n = 3000
+    og = O.from_edges(n, [(i, i + 1) for i in range(n - 1)])
+    g = upload(ctx, og)
+    assert np.array_equal(g.bfs_level(n // 2), O.bfs_level(og, n // 2))
+    assert np.array_equal(g.cc(), O.cc(og))
+
+
+def test_directed_graph_csc(ctx):
+    og = O.er(4096, 8.0, seed=7, dangling_bp=100, symmetric=False)
+    g = ctx.upload(og.off, og.adj, symmetric=False)
+    for v in VARIANTS:
+        o = gg.default_opts(variant=v)
+        assert np.array_equal(g.bfs_level(3, opts=o), O.bfs_level(og, 3))
+    x = g.pagerank(maxiter=50, tol=0)
+    xo, _, _ = O.pagerank(og, maxiter=50, tol=0)
+    assert np.abs(x.astype(np.float64) - xo).sum() <= 1e-6
+
+
+@pytest.mark.parametrize("fmt", list(PR_L1_VS_F64))
+def test_pagerank_precision(ctx, fmt):
+    og = O.rmat(14, 16 << 14, seed=31)
+    g = upload(ctx, og)
+    x64, it64, _ = O.pagerank(og, maxiter=100, tol=1e-7, f64=True)
+    st = gg.RunStats()
+    x = g.pagerank(maxiter=100, tol=1e-7, contrib=fmt, accum_f64=(fmt == gg.F32),
+                   renorm_f32=False, stats=st)
+    err = np.abs(x.astype(np.float64) - x64).sum()
+    assert err <= PR_L1_VS_F64[fmt], (fmt, err)
+    assert 1 <= st.iterations <= 100
+
+
+def test_pr_cfp_matches_restatement(ctx):
+    """customfp<6,10> storage against the restated PR_vary variant 46 loop."""
+    og = O.rmat(12, 16 << 12, seed=8)
+    g = upload(ctx, og)
+    xo, _, _ = O.pagerank_vary(og, O.CFP_6_10, accum_f64=False, maxiter=30, tol=0)
+    x = g.pagerank(maxiter=30, tol=0, contrib=gg.CFP_6_10, accum_f64=False, renorm_f32=False)
+    assert np.abs(x.astype(np.float64) - xo).sum() <= 1e-5
+
+
+def test_edgemap_api_bfs_step(ctx):
+    """One BFSLVLv step through gg_edgemap with explicit frontiers."""
+    og = O.rmat(11, 8 << 11, seed=5)
+    g = upload(ctx, og)
+    n = g.n
+    lvl, prev = g.prop(gg.I32), g.prop(gg.I32)
+    lvl.fill(n + 1); prev.fill(n + 1); lvl.set(0, 0); prev.set(0, 0)
+    F, O2 = g.frontier(), g.frontier()
+    F.set_single(0)
+    ref = O.bfs_level(og, 0)
+    it = 0
+    while F.counts()[0]:
+        d = gg.EmapDesc(relax=gg.RELAX_MIN_PLUS1_I32, a=lvl.h, dst_filter=gg.FILTER_GT_CONST,
+                        dst_filter_k=it + 1, record=gg.RECORD_NE_PREV, prev=prev.h,
+                        variant=gg.VAR_AUTO)
+        st = g.edgemap(d, F, O2, stats=True)
+        got = O2.download()
+        assert np.array_equal(got, np.flatnonzero(ref == it + 1))
+        assert st.nactv_out == len(got)
+        F, O2 = O2, F
+        it += 1
+    assert np.array_equal(lvl.download(), ref)
+
+
+def test_vertexmap_program(ctx):
+    """PRv's normalisation chain as one fused vertex pass."""
+    og = O.rmat(10, 8 << 10, seed=2)
+    g = upload(ctx, og)
+    y, x = g.prop(gg.F32), g.prop(gg.F32)
+    yv = np.random.default_rng(1).random(g.n).astype(np.float32)
+    xv = np.random.default_rng(2).random(g.n).astype(np.float32)
+    y.upload(yv); x.upload(xv)
+    d = gg.VmapDesc()
+    prog = [(gg.VM_LOAD, 0), (gg.VM_CONST, 0), (gg.VM_MUL, 0), (gg.VM_STORE, 0),   # y *= w
+            (gg.VM_LOAD, 1), (gg.VM_LOAD, 0), (gg.VM_SUB, 0), (gg.VM_ABS, 0),
+            (gg.VM_REDUCE_ADD, 0),                                                   # delta
+            (gg.VM_LOAD, 0), (gg.VM_STORE, 1)]                                       # x = y
+    d.ncode = len(prog)
+    for i, (c, a) in enumerate(prog):
+        d.code[i], d.arg[i] = c, a
+    d.props[0], d.props[1] = y.h, x.h
+    d.consts[0] = 0.5
+    d.nreduce = 1
+    red = g.vertexmap(d)
+    ynew = (yv.astype(np.float64) * 0.5).astype(np.float32)
+    assert np.array_equal(y.download(), ynew)
+    assert np.array_equal(x.download(), ynew)
+    assert abs(red[0] - np.abs(xv.astype(np.float64) - ynew).sum()) < 1e-6 * g.n
+
+
+def test_vertex_filter(ctx):
+    og = O.rmat(10, 8 << 10, seed=2)
+    g = upload(ctx, og)
+    lab = g.prop(gg.U32)
+    labels = O.cc(og)
+    lab.upload(labels)
+    d = gg.VmapDesc()
+    prog = [(gg.VM_LOAD, 0), (gg.VM_CONST, 0), (gg.VM_EQ, 0), (gg.VM_FILTER, 0)]
+    d.ncode = len(prog)
+    for i, (c, a) in enumerate(prog):
+        d.code[i], d.arg[i] = c, a
+    d.props[0] = lab.h
+    d.consts[0] = 0.0
+    out = g.frontier()
+    g.vertexmap(d, None, out)
+    assert np.array_equal(out.download(), np.flatnonzero(labels == 0))
+    assert out.counts() == (int((labels == 0).sum()), int(og.outdeg()[labels == 0].sum()))
+
+
+def test_errors_are_status_codes(ctx):
+    og = O.rmat(8, 8 << 8, seed=1)
+    g = upload(ctx, og)
+    with pytest.raises(gg.GGError) as e:
+        g.bfs_level(g.n + 5)
+    assert e.value.status == gg.GG_ERR_ARG
+    p = g.prop(gg.F32)
+    d = gg.EmapDesc(relax=gg.RELAX_MIN_U32, a=p.h, record=gg.RECORD_NONE)
+    with pytest.raises(gg.GGError):
+        g.edgemap(d)
+    bad = np.array([0, 2, 1], dtype=np.uint64)
+    with pytest.raises(gg.GGError):
+        ctx.upload(bad, np.array([1, 0], dtype=np.uint32))
+    with pytest.raises(gg.GGError) as e:
+        ctx.read_bin("/nonexistent/graph.bin")
+    assert e.value.status == gg.GG_ERR_IO
+
+
+def test_bin_file_roundtrip(ctx, tmp_path):
+    og = O.rmat(11, 8 << 11, seed=3)
+    p = str(tmp_path / "g.bin")
+    O.write_bin(og, p)
+    g = ctx.read_bin(p)
+    off, adj = g.download()
+    assert np.array_equal(off, og.off) and np.array_equal(adj, og.adj)
+    q = str(tmp_path / "h.bin")
+    g.write_bin(q)
+    h = O.read_bin(q)
+    assert np.array_equal(h.off, og.off) and np.array_equal(h.adj, og.adj)
+
+
+def test_repeat_runs_deterministic(ctx):
+    """Atomics-order stress: repeated runs give identical exact outputs."""
+    og = O.rmat(14, 16 << 14, seed=77)
+    g = upload(ctx, og)
+    a = g.bfs_level(0)
+    c = g.cc()
+    for _ in range(3):
+        assert np.array_equal(g.bfs_level(0), a)
+        assert np.array_equal(g.cc(), c)

@@ -1,0 +1,156 @@
+"""CPU tests of the oracle: generator invariants, file format, and the
+restatement against the committed golden fixtures made by the reference."""
+import glob
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def check_csr(g, symmetric=True):
+    off, adj = g.off, g.adj
+    assert off[0] == 0 and off[-1] == len(adj)
+    assert np.all(np.diff(off.astype(np.int64)) >= 0)
+    assert np.all(adj < g.n)
+    src = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(off).astype(np.int64))
+    assert not np.any(src == adj), "self-loop"
+    key = src * g.n + adj
+    assert np.all(np.diff(key) > 0), "rows not sorted / duplicates"
+    if symmetric:
+        rkey = np.sort(adj.astype(np.int64) * g.n + src)
+        assert np.array_equal(rkey, key), "not symmetric"
+
+
+@pytest.mark.parametrize("scale,ef", [(8, 8), (10, 16), (12, 4)])
+def test_rmat_invariants(scale, ef):
+    g = O.rmat(scale, ef << scale, seed=7)
+    check_csr(g)
+    g2 = O.rmat(scale, ef << scale, seed=7)
+    assert np.array_equal(g.off, g2.off) and np.array_equal(g.adj, g2.adj)
+    g3 = O.rmat(scale, ef << scale, seed=8)
+    assert not np.array_equal(g.adj[: min(len(g.adj), len(g3.adj))], g3.adj[: min(len(g.adj), len(g3.adj))])
+
+
+def test_rmat_skew():
+    # quadrant a dominates: low ids collect most edges, vertex 0 is the hub
+    g = O.rmat(14, 16 << 14, seed=1)
+    deg = g.outdeg()
+    assert int(np.argmax(deg)) < 16
+    assert deg[: 1 << 10].sum() > deg[-(1 << 10):].sum() * 20
+
+
+def test_er_directed_dangling():
+    g = O.er(1 << 12, 32.0, seed=3, dangling_bp=100, symmetric=False)
+    check_csr(g, symmetric=False)
+    zero = (g.outdeg() == 0).mean()
+    assert 0.003 < zero < 0.03
+    gs = O.er(1 << 12, 16.0, seed=3)
+    check_csr(gs)
+
+
+def test_grid():
+    g = O.grid(32, 48, seed=5, del_bp=100)
+    check_csr(g)
+    full = O.grid(32, 48, seed=5)
+    assert full.m == 2 * (31 * 48 + 32 * 47)
+    assert g.m < full.m
+
+
+def test_bin_roundtrip(tmp_path):
+    g = O.rmat(10, 8 << 10, seed=2)
+    p = str(tmp_path / "g.bin")
+    O.write_bin(g, p)
+    hdr = np.fromfile(p, dtype=np.uint64, count=8)
+    assert list(hdr) == [2, 1, g.n, g.m, 4, 8, 0, 0]
+    h = O.read_bin(p)
+    assert np.array_equal(h.off, g.off) and np.array_equal(h.adj, g.adj)
+
+
+def test_bin_rejects_corrupt(tmp_path):
+    p = str(tmp_path / "bad.bin")
+    np.array([9, 1, 4, 0, 4, 8, 0, 0], dtype=np.uint64).tofile(p)
+    with pytest.raises(OSError):
+        O.read_bin(p)
+    q = str(tmp_path / "short.bin")
+    np.array([2, 1, 100, 1000, 4, 8, 0, 0], dtype=np.uint64).tofile(q)
+    with pytest.raises(OSError):
+        O.read_bin(q)
+
+
+def test_bfs_small_known():
+    # path 0-1-2-3 plus isolated 4: levels 0,1,2,3,n+1
+    g = O.from_edges(5, [(0, 1), (1, 2), (2, 3)])
+    assert list(O.bfs_level(g, 0)) == [0, 1, 2, 3, 6]
+    assert list(O.bfs_level(g, 2)) == [2, 1, 0, 1, 6]
+    lab = O.cc(g)
+    assert list(lab) == [0, 0, 0, 0, 4]
+
+
+def test_check_parents_detects_bad():
+    g = O.from_edges(4, [(0, 1), (1, 2), (0, 3)])
+    lv = O.bfs_level(g, 0)
+    good = np.array([0, 0, 1, 0], dtype=np.uint32)
+    assert O.check_parents(g, 0, good, lv) == 0
+    bad = np.array([0, 0, 3, 0], dtype=np.uint32)  # 3 is not a neighbour of 2
+    assert O.check_parents(g, 0, bad, lv) == 1
+
+
+def test_cfp_restatement():
+    # customfp<6,10>: exponent field keeps its low 6 bits, mantissa its top 10
+    for f in [0.5, 0.25, 1.0 / 3, 1e-5, 0.9999, 1.5]:
+        c = O.cfp_from_float(f, 0, 6, 10)
+        back = O.cfp_to_float(c, 0, 6, 10)
+        if 2.0 ** -63 <= f < 2.0:
+            assert abs(back - f) <= f * 2.0 ** -10
+            assert back <= f  # truncation
+    # scustomfp<true,8,7> is bf16 by truncation
+    for f in [1.0, -2.5, 3.14159, 1e-30]:
+        c = O.cfp_from_float(f, 1, 8, 7)
+        u = np.array([f], dtype=np.float32).view(np.uint32)[0]
+        assert c == (u >> 16)
+
+
+def test_pr_sums_to_one():
+    g = O.rmat(10, 8 << 10, seed=4)
+    x, it, d = O.pagerank(g, maxiter=30)
+    assert it == 30 or d[-1] <= 1e-7
+    assert abs(float(x.astype(np.float64).sum()) - 1.0) < 1e-4
+    x64, _, _ = O.pagerank(g, maxiter=30, f64=True)
+    assert np.abs(x - x64).sum() < 1e-5
+
+
+def golden_files():
+    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+@pytest.mark.parametrize("path", golden_files(), ids=lambda p: os.path.basename(p))
+def test_oracle_matches_reference_golden(path):
+    """Pins the restatement: the fixtures hold outputs of the reference's own
+    build (BFSLVLv, BFSv, CCv, PRv) on seeded graphs."""
+    z = np.load(path)
+    if "off" in z:
+        g = O.Graph(int(z["n"]), z["off"], z["adj"])
+    else:  # large workload stored by generator parameters + CSR hash
+        g = O.rmat(int(z["scale"]), int(z["nedges"]), int(z["seed"]))
+        h = hashlib.sha256()
+        h.update(g.off.tobytes())
+        h.update(g.adj.tobytes())
+        assert h.hexdigest() == str(z["sha256"])
+    for r, lv in zip(z["bfs_roots"], z["bfs_levels"]):
+        assert np.array_equal(O.bfs_level(g, int(r)), lv)
+    if "bfsv_parents" in z:
+        for r, pa in zip(z["bfs_roots"], z["bfsv_parents"]):
+            lv = O.bfs_level(g, int(r))
+            assert O.check_parents(g, int(r), pa.astype(np.uint32), lv) == 0
+    assert np.array_equal(O.cc(g), z["cc"])
+    x, _, _ = O.pagerank(g, maxiter=int(z["pr_iters"]))
+    assert np.abs(x.astype(np.float64) - z["pr"]).sum() <= 1e-6
+
+
+def test_golden_present():
+    assert len(golden_files()) >= 4
