@@ -1,0 +1,457 @@
+#!/usr/bin/env python3
+"""Benchmark of the edgemap/vertexmap hot path on one B200 (or N replicas).
+
+Workload (the large single-GPU configuration): R-MAT scale 24, edge factor 16
+(2^28 generated edges, a,b,c,d = .57,.19,.19,.05, seed 1), symmetrised, self
+loops and duplicate edges removed, uint32 vertex ids / uint64 offsets, built on
+the device.  One step = one BFSLVLv run (BFS levels, sparse push / dense pull
+switched by the m/20 threshold) from the next of 64 seeded non-isolated
+roots.  The graph (2.3 GB) is far larger than the 126 MB L2, so no flush is
+needed between steps.
+
+Headline `value`: BFS GTEPS over the timed steps, Graph500 convention
+(m_c/2 per run, m_c = directed edges incident to the reached vertices),
+inputs resident in HBM.  The same JSON line also carries CC (CCv to
+convergence) and PageRank (PRv, 20 iterations) throughput, the reduced
+precision PageRank speed-ups, `e2e` (the public C-ABI call returning levels
+to pinned host memory), the roofline of the dominant kernel, and the
+reference CPU build timed on this host (`cpu_baseline`).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With --gpus N under torchrun every rank runs its own replica on its own
+roots (no collective on the data path; "replicas only"); time is the max
+over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BFS/CC GTEPS, PR GEdges/s/iter @RMAT-24, %HBM peak; BF16/learned vs plain"
+SCALE, EDGE_FACTOR, GRAPH_SEED, ROOT_SEED, NROOTS = 24, 16, 1, 12345, 64
+WORKLOAD = ("BFSLVLv levels from 64 seeded non-isolated roots, R-MAT scale 24 edge factor 16 "
+            "(a,b,c=.57,.19,.19, seed 1), symmetrised, deduplicated, no self-loops")
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread is not None:
+            self.thread.join(timeout=5)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for i, nm in enumerate(names):
+                if len(r) > 5 + i and r[5 + i].lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def pick_roots(deg: np.ndarray) -> np.ndarray:
+    nz = np.flatnonzero(deg)
+    rng = np.random.default_rng(ROOT_SEED)
+    return rng.choice(nz, size=NROOTS, replace=False).astype(np.uint32)
+
+
+def bfs_bytes(n: int, st, it: int) -> float:
+    """Algorithmic bytes of BFS iteration `it` (per-unit figures: 8-byte
+    offsets, 4-byte ids and levels).  Sparse push: 4F + 16F + 4E + 4E + 4N.
+    Dense pull: 8(n+1) + 4n + 4S + 4N + 2n/8."""
+    from graptor_b200 import gg
+    F, E, S = st.nactv[it], st.nacte[it], st.scanned[it]
+    N = st.nactv[it + 1] if it + 1 < st.iterations else 0
+    if st.variant[it] == gg.VAR_PULL_DENSE:
+        return 8.0 * (n + 1) + 4.0 * n + 4.0 * S + 4.0 * N + 2.0 * n / 8
+    return 20.0 * F + 8.0 * E + 4.0 * N
+
+
+# ---------------------------------------------------------------------------
+# reference CPU arm / baseline
+# ---------------------------------------------------------------------------
+def reference_bfs(bin_path: str, roots, threads: int):
+    from oracle import oracle as O
+    return O.ref_bfs(bin_path, [int(r) for r in roots], threads=threads)
+
+
+def cpu_info():
+    cores = os.cpu_count() or 1
+    model = ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return cores, model
+
+
+def run_reference_arm(args, ws, rank):
+    """The reference's own BFSLVLv (compiled from its sources, OpenMP backend)
+    on this host's cores, same graph, roots, metric and unit."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    if not O.ref_available("ref_bfslvl"):
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference build oracle/_ref missing (needs the reference sources to compile)"}))
+        return 0
+    cores, model = cpu_info()
+    t0 = time.time()
+    g = O.rmat(args.scale, EDGE_FACTOR << args.scale, GRAPH_SEED)
+    roots = pick_roots(g.outdeg())
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "rmat.bin")
+        O.write_bin(g, path)
+        prep = time.time() - t0
+        seq = [roots[i % NROOTS] for i in range(args.warmup + args.steps)]
+        res = reference_bfs(path, seq, cores)
+    res = res[args.warmup:]
+    tot_t, tot_e = 0.0, 0.0
+    gteps = []
+    for r, t, _, _ in res:
+        lv = O.bfs_level(g, int(r))
+        mc = O.reached_edges(g, lv)
+        tot_t += t
+        tot_e += mc / 2
+        gteps.append(mc / 2 / t / 1e9)
+    val = tot_e / tot_t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "GTEPS",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(tot_t / len(res) * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "scale": args.scale, "edge_factor": EDGE_FACTOR,
+                   "n": g.n, "m": g.m, "roots": NROOTS},
+        "cpu_baseline": {"value": round(val, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                         "sample": f"{len(res)} BFSLVLv runs, reference build (OpenMP, {model})"},
+        "e2e": {"value": round(val, 4), "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "bfs": {"gteps_mean": round(float(np.mean(gteps)), 4),
+                "gteps_hmean": round(float(len(gteps) / np.sum(1.0 / np.array(gteps))), 4)},
+        "input_prep_s": round(prep, 1),
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, ws, rank, local):
+    from graptor_b200 import gg
+    import torch
+
+    hbm_peak, peak_kind = peaks()
+    ctx = gg.Context(local)
+    t0 = time.time()
+    g = ctx.rmat(args.scale, EDGE_FACTOR << args.scale, GRAPH_SEED)
+    gen_s = time.time() - t0
+    off, adj = g.download()
+    deg = np.diff(off).astype(np.int64)
+    roots = pick_roots(deg)
+    n, m = g.n, g.m
+
+    lvl = g.prop(gg.I32)
+    opts = gg.default_opts(collect=True)
+    seq = [int(roots[(k * ws + rank) % NROOTS]) for k in range(args.warmup + args.steps)]
+
+    # ---- warm-up ----
+    for k in range(args.warmup):
+        g.bfs_level(seq[k], level=lvl, host=False, opts=opts)
+    ctx.sync()
+
+    # ---- timed BFS steps (device time, CUDA events on the library's stream) ----
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler = ClockSampler(local)
+    stats = [gg.RunStats() for _ in range(args.steps)]
+    launches0 = ctx.launches
+    barrier(ws)
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0.record(stream)
+    for k in range(args.steps):
+        g.bfs_level(seq[args.warmup + k], level=lvl, host=False, opts=opts, stats=stats[k])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = ctx.launches - launches0
+    t_ms = ev0.elapsed_time(ev1)
+    t_ms_max = max_over_ranks(t_ms, ws)
+    barrier(ws)
+
+    half_edges = sum(st.edges_reached for st in stats) / 2.0
+    total_half_edges = sum_over_ranks(half_edges, ws)
+    value = total_half_edges / (t_ms_max / 1e3) / 1e9
+    per_root = [st.edges_reached / 2.0 / (st.total_ms / 1e3) / 1e9 for st in stats]
+
+    # roofline of the dominant traversal kernel (by summed kernel time)
+    ktime = {}
+    kbytes = {}
+    for st in stats:
+        for it in range(st.iterations):
+            v = st.variant[it]
+            ktime[v] = ktime.get(v, 0.0) + st.iter_ms[it]
+            kbytes[v] = kbytes.get(v, 0.0) + bfs_bytes(n, st, it)
+    dom = max(ktime, key=ktime.get)
+    nlaunch = sum(1 for st in stats for it in range(st.iterations) if st.variant[it] == dom)
+    achieved = kbytes[dom] / (ktime[dom] / 1e3) / 1e9
+    kernel_names = {gg.VAR_PULL_DENSE: "k_pull", gg.VAR_PUSH_SPARSE: "k_push_binned",
+                    gg.VAR_PUSH_MERGE: "k_push_merge", gg.VAR_PUSH_DENSE: "k_push_dense"}
+    bfs_iter_total_ms = sum(ktime.values())
+    bfs_pass_bytes = 8.0 * (n + 1) + 4.0 * m + 8.0 * n
+
+    out = {}
+    if rank == 0:
+        out["bfs"] = {
+            "gteps_mean": round(float(np.mean(per_root)), 3),
+            "gteps_hmean": round(float(len(per_root) / np.sum(1.0 / np.array(per_root))), 3),
+            "ms_per_root_mean": round(float(np.mean([st.total_ms for st in stats])), 4),
+            "iterations_mean": round(float(np.mean([st.iterations for st in stats])), 2),
+            "kernel_share": {kernel_names[v]: round(t / bfs_iter_total_ms, 3) for v, t in ktime.items()},
+            "one_pass_frac_of_hbm": round(bfs_pass_bytes / (np.mean([st.total_ms for st in stats]) / 1e3)
+                                          / 1e9 / hbm_peak, 4),
+        }
+
+    # ---- CC (CCv to convergence) ----
+    if not args.quick:
+        lab = g.prop(gg.U32)
+        g.cc(label=lab, host=False)
+        cc_ms = []
+        cst = gg.RunStats()
+        for _ in range(3):
+            st = gg.RunStats()
+            g.cc(label=lab, host=False, opts=gg.default_opts(gg.THRESH_FRAC, 5), stats=st)
+            cc_ms.append(st.total_ms)
+            cst = st
+        cc_best = float(np.median(cc_ms))
+        out["cc"] = {"ms": round(cc_best, 3), "gedges_per_s": round(m / (cc_best / 1e3) / 1e9, 3),
+                     "iterations": cst.iterations}
+
+        # ---- PageRank (PRv: FP32 storage, double gather accumulation, 20 iterations) ----
+        x = g.prop(gg.F32)
+        prs = {}
+        for name, fmt, acc64 in [("f32", gg.F32, True), ("f32_accf32", gg.F32, False), ("bf16", gg.BF16, False),
+                                 ("f16", gg.F16, False), ("fp8e4m3", gg.FP8E4M3, False),
+                                 ("cfp_6_10", gg.CFP_6_10, False)]:
+            g.pagerank(maxiter=3, tol=0, contrib=fmt, accum_f64=acc64, x=x, host=False)
+            ts = []
+            for _ in range(3):
+                st = gg.RunStats()
+                g.pagerank(maxiter=20, tol=0, contrib=fmt, accum_f64=acc64, renorm_f32=(name == "f32"),
+                           x=x, host=False, stats=st)
+                ts.append(st.total_ms / 20)
+            t_it = float(np.median(ts))
+            prs[name] = {"ms_per_iter": round(t_it, 4), "gedges_per_s_per_iter": round(m / (t_it / 1e3) / 1e9, 3)}
+        base = prs["f32"]["ms_per_iter"]
+        for k, v in prs.items():
+            v["speedup_vs_f32"] = round(base / v["ms_per_iter"], 3)
+        pr_bytes_f32 = 8.0 * (n + 1) + 4.0 * m + 4.0 * m + n * (4 + 4 + 4 + 4)
+        prs["f32"]["frac_of_hbm"] = round(pr_bytes_f32 / (base / 1e3) / 1e9 / hbm_peak, 4)
+        out["pr"] = prs
+
+    # ---- e2e: public C-ABI call, graph uploaded from host memory, levels back to pinned host ----
+    e2e = None
+    if not args.quick:
+        pin = torch.empty(n, dtype=torch.int32, pin_memory=True).numpy()
+        t_up = time.time()
+        gh = ctx.upload(off, adj, symmetric=True)
+        upload_s = time.time() - t_up
+        lv2 = gh.prop(gg.I32)
+        for k in range(min(args.warmup, 3)):
+            gh.bfs_level(seq[k], level=lv2, out=pin)
+        barrier(ws)
+        t1 = time.perf_counter()
+        e2e_edges = 0.0
+        for k in range(args.steps):
+            st = gg.RunStats()
+            gh.bfs_level(seq[args.warmup + k], level=lv2, out=pin, stats=st)
+            e2e_edges += st.edges_reached / 2.0
+        e2e_s = max_over_ranks(time.perf_counter() - t1, ws)
+        e2e_val = sum_over_ranks(e2e_edges, ws) / e2e_s / 1e9
+        e2e = {"value": round(e2e_val, 4), "unit": "GTEPS", "h2d_bytes_per_step": 4,
+               "d2h_bytes_per_step": 4 * n, "graph_upload_s": round(upload_s, 3)}
+        del gh
+
+    # ---- CPU baseline: the reference build on this host, bounded sample ----
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import oracle as O
+            if O.ref_available("ref_bfslvl"):
+                cores, model = cpu_info()
+                sample_roots = [int(r) for r in roots[: args.cpu_roots]]
+                with tempfile.TemporaryDirectory() as tmp:
+                    path = os.path.join(tmp, "rmat.bin")
+                    g.write_bin(path)
+                    tc = time.time()
+                    res = reference_bfs(path, sample_roots, cores)
+                    wall = time.time() - tc
+                tt, ee = 0.0, 0.0
+                for r, t, _, _ in res:
+                    st = gg.RunStats()
+                    g.bfs_level(int(r), level=lvl, host=False, stats=st)
+                    tt += t
+                    ee += st.edges_reached / 2.0
+                cpu = {"value": round(ee / tt / 1e9, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+                       "sample": f"{len(res)} BFSLVLv runs (roots 0..{len(res)-1} of the 64) of the reference "
+                                 f"build, OpenMP, {model}; load+VEBO+runs wall {wall:.0f} s"}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "GTEPS", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"failed: {e}"[:300]}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "GTEPS", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_ms_max / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "scale": args.scale, "edge_factor": EDGE_FACTOR, "n": n, "m": m,
+                       "roots": NROOTS, "parallelism": f"replicas{ws}" if ws > 1 else "single",
+                       "l2": "graph 2.3 GB > 126 MB L2, no flush between steps",
+                       "graph_build_s": round(gen_s, 2)},
+            "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": round(achieved, 1),
+                         "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
+                         "traffic": None, "peak_kind": peak_kind, "launches": nlaunch,
+                         "bytes_per_launch": round(kbytes[dom] / max(nlaunch, 1)),
+                         "ms_per_launch": round(ktime[dom] / max(nlaunch, 1), 4)},
+            "clocks": clocks, "gpu_launches": launches,
+            "e2e": e2e, "cpu_baseline": cpu,
+        }
+        line.update(out)
+        print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scale", type=int, default=SCALE)
+    ap.add_argument("--cpu-roots", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="BFS only (no CC/PR/e2e)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    ws, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            rc = run_reference_arm(args, ws, rank)
+        else:
+            rc = run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    return rc
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -11,6 +11,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -208,6 +209,25 @@ __global__ void k_max_degree(const uint64_t *off, uint32_t n, unsigned long long
     if ((threadIdx.x & 31) == 0) atomicMax(best, b);
 }
 
+// chunks per CSC row (0 for light rows)
+__global__ void k_heavy_count(const uint64_t *in_off, uint32_t n, uint32_t T, uint32_t CH,
+                              uint8_t *flag, uint64_t *nch) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t stride = gridDim.x * blockDim.x;
+    for (; i < n; i += stride) {
+        uint64_t d = in_off[i + 1] - in_off[i];
+        bool h = d > T;
+        flag[i] = h ? 1 : 0;
+        nch[i] = h ? (d + CH - 1) / CH : 0;
+    }
+}
+
+__global__ void k_heavy_gather(const uint32_t *hv, uint32_t nh, const uint64_t *nch, uint64_t *cnt) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nh) cnt[i] = nch[hv[i]];
+    if (i == nh) cnt[i] = 0;
+}
+
 static int ceil_log2(uint64_t x) {
     int l = 0;
     while ((1ull << l) < x) ++l;
@@ -277,6 +297,48 @@ static gg_status build_from_keys(gg_ctx *ctx, uint32_t n, uint64_t *keys, uint64
     return rc;
 }
 
+gg_status build_heavy_rows(gg_graph *g) {
+    gg_ctx *ctx = g->ctx;
+    cudaStream_t st = ctx->stream;
+    HeavyRows &H = g->heavy;
+    H.T = tuning().heavy_deg;
+    H.CH = tuning().heavy_chunk;
+    const uint32_t n = g->n;
+    uint8_t *flag = nullptr;
+    uint64_t *nch = nullptr, *d_num = nullptr;
+    void *tmp = nullptr;
+    size_t tb = 0, tb2 = 0;
+    gg_status rc = GG_OK;
+    auto done = [&](gg_status s) { cudaFree(flag); cudaFree(nch); cudaFree(d_num); cudaFree(tmp); return s; };
+#define HK(expr) do { cudaError_t _e = (expr); if (_e != cudaSuccess) return done(cuda_error(ctx, _e, #expr)); } while (0)
+    HK(cudaMalloc(&flag, n + 1));
+    HK(cudaMalloc(&nch, ((size_t)n + 1) * 8));
+    HK(cudaMalloc(&d_num, 8));
+    HK(cudaMalloc(&H.v, ((size_t)n + 1) * 4));
+    k_heavy_count<<<grid_for(ctx, n), 256, 0, st>>>(g->in_off, n, H.T, H.CH, flag, nch);
+    ctx->launches++;
+    cub::CountingInputIterator<uint32_t> it(0);
+    HK(cub::DeviceSelect::Flagged(nullptr, tb, it, flag, H.v, d_num, (int64_t)n, st));
+    HK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, nch, nch, (int64_t)n + 1, st));
+    HK(cudaMalloc(&tmp, std::max(tb, tb2)));
+    tb = std::max(tb, tb2);
+    HK(cub::DeviceSelect::Flagged(tmp, tb, it, flag, H.v, d_num, (int64_t)n, st));
+    ctx->launches++;
+    uint64_t nh = 0;
+    HK(cudaMemcpyAsync(&nh, d_num, 8, cudaMemcpyDeviceToHost, st));
+    HK(cudaStreamSynchronize(st));
+    H.nheavy = (uint32_t)nh;
+    HK(cudaMalloc(&H.first, (nh + 1) * 8));
+    k_heavy_gather<<<(unsigned)((nh + 256) / 256), 256, 0, st>>>(H.v, (uint32_t)nh, nch, H.first);
+    ctx->launches++;
+    HK(cub::DeviceScan::ExclusiveSum(tmp, tb, H.first, H.first, (int64_t)nh + 1, st));
+    ctx->launches++;
+    HK(cudaMemcpyAsync(&H.nchunks, H.first + nh, 8, cudaMemcpyDeviceToHost, st));
+    HK(cudaStreamSynchronize(st));
+#undef HK
+    return done(rc);
+}
+
 static gg_status graph_finish(gg_graph *g) {
     gg_ctx *ctx = g->ctx;
     cudaStream_t st = ctx->stream;
@@ -310,7 +372,7 @@ static gg_status graph_finish(gg_graph *g) {
     cudaFree(d_best);
     g->maxdeg = (uint32_t)(h_best >> 32);
     g->maxdeg_v = g->n ? (uint32_t)(0xFFFFFFFFull - (h_best & 0xFFFFFFFFull)) : 0;
-    return GG_OK;
+    return build_heavy_rows(g);
 }
 
 static void graph_free(gg_graph *g) {
@@ -321,6 +383,8 @@ static void graph_free(gg_graph *g) {
     cudaFree(g->adj);
     cudaFree(g->scratch);
     cudaFree(g->aux_cnt);
+    cudaFree(g->heavy.v);
+    cudaFree(g->heavy.first);
     for (auto *f : g->tmp_front)
         if (f) gg_frontier_destroy(f);
     delete g;
@@ -476,6 +540,8 @@ gg_status gg_ctx_create(int device, gg_ctx **out) {
     if ((e = cudaMallocHost(&c->h_pinned, 64 * sizeof(uint64_t))) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreate(&c->ev0)) != cudaSuccess) return bail(e);
     if ((e = cudaEventCreate(&c->ev1)) != cudaSuccess) return bail(e);
+    if ((e = cudaEventCreate(&c->evk0)) != cudaSuccess) return bail(e);
+    if ((e = cudaEventCreate(&c->evk1)) != cudaSuccess) return bail(e);
     *out = c;
     return GG_OK;
 }
@@ -489,6 +555,8 @@ gg_status gg_ctx_destroy(gg_ctx *ctx) {
     if (ctx->h_pinned) cudaFreeHost(ctx->h_pinned);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->evk0) cudaEventDestroy(ctx->evk0);
+    if (ctx->evk1) cudaEventDestroy(ctx->evk1);
     delete ctx;
     return GG_OK;
 }

@@ -571,6 +571,8 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     }
 
     const bool all_in = in == nullptr || in->all;
+    // kernel timing brackets only the traversal kernel (not conversions)
+    auto tstart = [&]() { if (ctx->time_kernels) cudaEventRecord(ctx->evk0, st); };
     switch (variant) {
     case GG_VAR_PULL_DENSE: {
         if (!all_in) {
@@ -578,6 +580,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
             A.in_bits = in->bitmap;
         }
         unsigned grid = persistent_grid(ctx, words);
+        tstart();
         if (all_in) k_pull<R, false, kBlock><<<grid, kBlock, 0, st>>>(A, op);
         else k_pull<R, true, kBlock><<<grid, kBlock, 0, st>>>(A, op);
         GG_LAUNCHED(ctx);
@@ -589,6 +592,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
             A.in_bits = in->bitmap;
         }
         unsigned grid = persistent_grid(ctx, words);
+        tstart();
         k_push_dense<R, kBlock><<<grid, kBlock, 0, st>>>(A, op);
         GG_LAUNCHED(ctx);
         break;
@@ -610,6 +614,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
         uint32_t nb_med = std::min<uint32_t>((A.c1 + kBlock / 32 - 1) / (kBlock / 32), cap);
         uint32_t nb_small = std::min<uint32_t>((A.c0 + kBlock - 1) / kBlock, cap);
         uint32_t grid = nb_large + nb_med + nb_small;
+        tstart();
         if (grid == 0) break;
         k_push_binned<R, kBlock><<<grid, kBlock, 0, st>>>(A, op, nb_large, nb_med);
         GG_LAUNCHED(ctx);
@@ -632,6 +637,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
         uint64_t *pre = (uint64_t *)((char *)p + lb + db);
         void *cub_tmp = (char *)p + lb + 2 * db;
         GG_CUDA(ctx, cudaMemsetAsync(deg + k, 0, 8, st));
+        tstart();
         k_concat_bins<<<persistent_grid(ctx, (k + 31) / 32), kBlock, 0, st>>>(
             in->bins[0], in->bins[1], in->bins[2], in->d_cnt, g->off, list, deg);
         GG_LAUNCHED(ctx);
@@ -648,6 +654,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     default:
         return set_error(ctx, GG_ERR_ARG, "unknown variant");
     }
+    if (ctx->time_kernels) cudaEventRecord(ctx->evk1, st);
     if (have_out) {
         if (d->record == GG_RECORD_NE_PREV && variant != GG_VAR_PULL_DENSE) {
             if (!d->prev) return set_error(ctx, GG_ERR_ARG, "NE_PREV record needs prev");
@@ -725,14 +732,22 @@ gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_f
         return GG_OK;
     }
     gg_status s;
+    ctx->time_kernels = stats != nullptr;
+    cudaEventRecord(ctx->evk0, ctx->stream);  // defined start even if nothing launches
     switch (d->relax) {
     case GG_RELAX_MIN_PLUS1_I32: s = launch_variant<GG_RELAX_MIN_PLUS1_I32>(g, d, in, out, variant); break;
     case GG_RELAX_MIN_U32: s = launch_variant<GG_RELAX_MIN_U32>(g, d, in, out, variant); break;
     default: s = launch_variant<GG_RELAX_SETIF_U32>(g, d, in, out, variant); break;
     }
+    if (stats && s == GG_OK) cudaEventRecord(ctx->evk1, ctx->stream);
+    ctx->time_kernels = false;
     GG_CHECK(s);
     if (stats) {
         memset(stats, 0, sizeof(*stats));
+        GG_CUDA(ctx, cudaEventSynchronize(ctx->evk1));
+        float kms = 0;
+        cudaEventElapsedTime(&kms, ctx->evk0, ctx->evk1);
+        stats->kernel_ms = kms;
         stats->variant = variant;
         stats->nactv_in = nactv;
         stats->nacte_in = nacte;
@@ -780,6 +795,7 @@ static void record_iter(gg_run_stats *st, int it, const gg_emap_stats &es) {
     st->nactv[it] = es.nactv_in;
     st->nacte[it] = es.nacte_in;
     st->scanned[it] = es.scanned;
+    st->iter_ms[it] = es.kernel_ms;
     st->scanned_edges += es.scanned;
 }
 
@@ -802,6 +818,10 @@ static gg_status frontier_loop(gg_graph *g, gg_emap_desc &desc, gg_frontier *F, 
     for (;;) {
         GG_CHECK(frontier_fetch_counts(F));
         if (F->h_cnt[FC_NACTV] == 0 && !F->all) break;
+        if (st) {
+            st->vertices_reached += F->h_cnt[FC_NACTV];
+            st->edges_reached += F->h_cnt[FC_NACTE];
+        }
         if (level_k) desc.dst_filter_k = iter + 1;
         gg_emap_stats es;
         GG_CHECK(edgemap_impl(g, &desc, F, O, opt.collect_stats ? &es : nullptr));

@@ -56,7 +56,9 @@ struct gg_ctx {
     uint64_t launches = 0;
     uint32_t *d_err = nullptr;  // device error word
     uint64_t *h_pinned = nullptr;  // small pinned staging buffer (counts)
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;    // whole-run timing
+    cudaEvent_t evk0 = nullptr, evk1 = nullptr;  // traversal-kernel timing
+    bool time_kernels = false;                   // record evk0/evk1 around the next traversal kernel
 };
 
 // Frontier counters live on the device in this layout.
@@ -73,6 +75,17 @@ enum {
 enum { NBINS = 3 };
 
 struct gg_graph;
+
+// In-rows of the CSC longer than `T` edges ("heavy" rows: R-MAT hubs, all
+// at low ids) are cut into chunks of `CH` edges so that no warp walks a hub
+// row alone.  first[h]..first[h+1] are the chunks of heavy vertex v[h].
+struct HeavyRows {
+    uint32_t *v = nullptr;      // heavy vertices, ascending
+    uint64_t *first = nullptr;  // [nheavy + 1] chunk prefix
+    uint32_t nheavy = 0;
+    uint64_t nchunks = 0;
+    uint32_t T = 0, CH = 0;
+};
 
 struct gg_frontier {
     gg_graph *g = nullptr;
@@ -102,6 +115,7 @@ struct gg_graph {
     size_t scratch_bytes = 0;
     gg_frontier *tmp_front[2] = {nullptr, nullptr};
     uint64_t *aux_cnt = nullptr;  // counters of steps that record no frontier
+    HeavyRows heavy;              // chunked long rows of the CSC (pull / gather)
 };
 
 struct gg_prop {
@@ -122,6 +136,7 @@ gg_status frontier_ensure_bitmap(gg_frontier *f);    // from list
 gg_status frontier_ensure_list(gg_frontier *f);      // from bitmap / all
 gg_status frontier_reset_counts(gg_frontier *f);     // async zero of d_cnt
 uint32_t bin_of_degree(uint64_t deg);
+gg_status build_heavy_rows(gg_graph *g);
 
 // Degree-bin thresholds of the sparse push (tunable by the autotuner).
 struct Tuning {
@@ -131,6 +146,8 @@ struct Tuning {
     int push_k = 8;
     int block = 256;
     int blocks_per_sm = 8;
+    uint32_t heavy_deg = 256;    // CSC rows longer than this are chunked
+    uint32_t heavy_chunk = 1024; // edges per chunk
 };
 Tuning &tuning();
 

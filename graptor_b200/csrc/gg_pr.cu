@@ -25,7 +25,9 @@
 //                 rounded y+w) is taken as s + n*w in double: equal in exact
 //                 arithmetic, different by at most n/2 float ulps of 1/n.
 //   k_pr_finish : residual test, iteration count, FP8 scale for the next
-//                 encode (from this iteration's max with 2x headroom).
+//                 encode (from this iteration's max with 2x headroom); FP16
+//                 is scaled the same way, since contributions of order 1/n
+//                 fall below its normal range.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_fp8.h>
@@ -93,11 +95,23 @@ struct PrState {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Scaled formats: FP8-E4M3 (max 448) and FP16 (max 65504, min normal 2^-14)
+// store contrib * scale with scale a power of two chosen so that the
+// largest contribution lands at half the format's range (2x headroom).
+__device__ __host__ inline bool scaled_format(int dt) { return dt == GG_FP8E4M3 || dt == GG_F16; }
+__device__ __host__ inline float scale_for(int dt, float cmax) {
+    if (!scaled_format(dt) || !(cmax > 0.0f)) return 1.0f;
+    const float half_range = dt == GG_FP8E4M3 ? 224.0f : 32768.0f;
+    int e;
+    frexpf(half_range / cmax, &e);
+    return ldexpf(1.0f, e - 1);
+}
+
 template <int DT, bool ACC64, bool ADD_OLD, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_pr_gather(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj,
             const typename Store<DT>::T *__restrict__ contrib, uint32_t n, float *y_f32,
-            double *y_f64, PrState *st, float scale_inv_arg, int K) {
+            double *y_f64, PrState *st, float scale_inv_arg, int K, uint32_t T) {
     using S = Store<DT>;
     using Acc = typename std::conditional<ACC64, double, float>::type;
     if (st && st->done) return;
@@ -114,12 +128,14 @@ k_pr_gather(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in
             beg = in_off[d];
             end = in_off[d + 1];
         }
+        // heavy rows are summed by k_pr_heavy_chunks / k_pr_heavy_finalize
+        const bool mine = valid && end - beg <= (uint64_t)T;
         Acc acc = 0;
         const bool shortrow = end - beg <= (uint64_t)K;
-        if (valid && shortrow) {
+        if (mine && shortrow) {
             for (uint64_t e = beg; e < end; ++e) acc += (Acc)S::dec(contrib[__ldg(in_adj + e)]);
         }
-        unsigned pend = __ballot_sync(FULL, valid && !shortrow);
+        unsigned pend = __ballot_sync(FULL, mine && !shortrow);
         while (pend) {
             const int j = __ffs(pend) - 1;
             pend &= pend - 1;
@@ -142,8 +158,8 @@ k_pr_gather(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in
             part = dev::warp_sum(part);
             if ((int)lane == j) acc = part;
         }
-        if (valid) {
-            if (DT == GG_FP8E4M3) acc *= (Acc)sinv;
+        if (mine) {
+            if (DT == GG_FP8E4M3 || DT == GG_F16) acc *= (Acc)sinv;
             if (y_f64) {
                 double v = ADD_OLD ? y_f64[d] + (double)acc : (double)acc;
                 y_f64[d] = v;
@@ -153,6 +169,78 @@ k_pr_gather(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in
                 y_f32[d] = v;
                 ysum += (double)v;
             }
+        }
+    }
+    if (st) {
+        ysum = dev::block_sum<double, BLOCK>(ysum);
+        if (threadIdx.x == 0) atomicAdd(&st->s1, ysum);
+    }
+}
+
+// One warp per chunk of a heavy row: partial[c] = sum of the chunk's
+// decoded contributions (4 independent coalesced loads per lane in flight).
+template <int DT, bool ACC64>
+__global__ void __launch_bounds__(256)
+k_pr_heavy_chunks(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj,
+                  const typename Store<DT>::T *__restrict__ contrib, HeavyRows H,
+                  typename std::conditional<ACC64, double, float>::type *partial, const PrState *st) {
+    using S = Store<DT>;
+    using Acc = typename std::conditional<ACC64, double, float>::type;
+    if (st && st->done) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < H.nchunks; c += nw) {
+        // heavy row owning chunk c: last h with first[h] <= c
+        uint32_t lo = 0, hi = H.nheavy;
+        while (hi - lo > 1) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (H.first[mid] <= c) lo = mid; else hi = mid;
+        }
+        const uint32_t v = H.v[lo];
+        const uint64_t rb = in_off[v], re = in_off[v + 1];
+        const uint64_t e0 = rb + (c - H.first[lo]) * H.CH;
+        const uint64_t e1 = min(e0 + H.CH, re);
+        Acc part = 0;
+        uint64_t base = e0;
+        for (; base + 128 <= e1; base += 128) {
+            uint32_t s0 = __ldg(in_adj + base + lane);
+            uint32_t s1 = __ldg(in_adj + base + 32 + lane);
+            uint32_t s2 = __ldg(in_adj + base + 64 + lane);
+            uint32_t s3 = __ldg(in_adj + base + 96 + lane);
+            part += (Acc)S::dec(contrib[s0]) + (Acc)S::dec(contrib[s1]) +
+                    (Acc)S::dec(contrib[s2]) + (Acc)S::dec(contrib[s3]);
+        }
+        for (; base < e1; base += 32) {
+            uint64_t e = base + lane;
+            if (e < e1) part += (Acc)S::dec(contrib[__ldg(in_adj + e)]);
+        }
+        part = dev::warp_sum(part);
+        if (lane == 0) partial[c] = part;
+    }
+}
+
+// Heavy row totals, partials summed in chunk order (deterministic).
+template <int DT, bool ACC64, bool ADD_OLD, int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+k_pr_heavy_finalize(HeavyRows H, const typename std::conditional<ACC64, double, float>::type *partial,
+                    float *y_f32, double *y_f64, PrState *st, float scale_inv_arg) {
+    using Acc = typename std::conditional<ACC64, double, float>::type;
+    if (st && st->done) return;
+    const float sinv = st ? st->scale_inv : scale_inv_arg;
+    double ysum = 0;
+    for (uint32_t h = blockIdx.x * BLOCK + threadIdx.x; h < H.nheavy; h += gridDim.x * BLOCK) {
+        Acc acc = 0;
+        for (uint64_t c = H.first[h]; c < H.first[h + 1]; ++c) acc += partial[c];
+        if (DT == GG_FP8E4M3 || DT == GG_F16) acc *= (Acc)sinv;
+        const uint32_t d = H.v[h];
+        if (y_f64) {
+            double v = ADD_OLD ? y_f64[d] + (double)acc : (double)acc;
+            y_f64[d] = v;
+            ysum += v;
+        } else {
+            float v = ADD_OLD ? (float)((double)y_f32[d] + (double)acc) : (float)acc;
+            y_f32[d] = v;
+            ysum += (double)v;
         }
     }
     if (st) {
@@ -184,7 +272,7 @@ k_pr_update(const float *__restrict__ y, float *__restrict__ x, typename Store<D
         x[v] = yv;
         const uint64_t deg = off[v + 1] - off[v];
         const float c = damp * yv / (float)deg;
-        contrib[v] = S::enc(DT == GG_FP8E4M3 ? c * enc_scale : c);
+        contrib[v] = S::enc(scaled_format(DT) ? c * enc_scale : c);
         if (deg && c > cm) cm = c;
     }
     dl = dev::block_sum<double, BLOCK>(dl);
@@ -201,22 +289,14 @@ k_pr_update(const float *__restrict__ y, float *__restrict__ x, typename Store<D
     }
 }
 
-// Largest power of two p with cmax * p * 2 <= 448 (2x headroom).
-__device__ __host__ inline float fp8_scale_for(float cmax) {
-    if (!(cmax > 0.0f)) return 1.0f;
-    int e;
-    frexpf(224.0f / cmax, &e);
-    return ldexpf(1.0f, e - 1);
-}
-
-__global__ void k_pr_finish(PrState *st) {
+__global__ void k_pr_finish(PrState *st, int dt) {
     if (st->done) return;
     const int it = st->iters;
     if (it < GG_MAX_ITERS) st->deltas[it] = st->delta;
     st->iters = it + 1;
     if (st->iters >= st->maxiter || !(st->delta > st->tol)) st->done = 1;
     st->scale_inv = 1.0f / st->scale;  // decode of what the update just wrote
-    st->scale = fp8_scale_for(st->cmax);  // next encode
+    st->scale = scale_for(dt, st->cmax);  // next encode
     st->s1 = 0;
     st->delta = 0;
     st->cmax = 0.0f;
@@ -230,7 +310,7 @@ __global__ void k_pr_init(float *x, typename Store<DT>::T *contrib, const uint64
     const float x0 = 1.0f / (float)n;
     float cm = 0.0f;
     const uint32_t stride = gridDim.x * BLOCK;
-    const float scale = pass == 1 ? fp8_scale_for(st->cmax) : 1.0f;
+    const float scale = pass == 1 ? scale_for(DT, st->cmax) : 1.0f;
     for (uint32_t v = blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
         const uint64_t deg = off[v + 1] - off[v];
         const float c = damp * x0 / (float)deg;
@@ -238,7 +318,7 @@ __global__ void k_pr_init(float *x, typename Store<DT>::T *contrib, const uint64
             if (deg && c > cm) cm = c;
         } else {
             x[v] = x0;
-            contrib[v] = S::enc(DT == GG_FP8E4M3 ? c * scale : c);
+            contrib[v] = S::enc(scaled_format(DT) ? c * scale : c);
         }
     }
     if (pass == 0) {
@@ -260,9 +340,39 @@ static unsigned pr_grid(gg_ctx *ctx, uint64_t work) {
     return (unsigned)(b ? b : 1);
 }
 
+// gather of one iteration / one API call: light rows, heavy chunks, heavy totals
+template <int DT, bool ACC64, bool ADD_OLD>
+static gg_status gather_launch(gg_graph *g, const typename Store<DT>::T *contrib, float *yf,
+                               double *yd, PrState *st, float sinv, void *partial) {
+    gg_ctx *ctx = g->ctx;
+    cudaStream_t s = ctx->stream;
+    using Acc = typename std::conditional<ACC64, double, float>::type;
+    const HeavyRows &H = g->heavy;
+    const uint64_t warps = (uint64_t)((g->n + 31) / 32);
+    uint64_t blocks = (warps * 32 + 255) / 256;
+    const uint64_t cap = (uint64_t)ctx->sm_count * tuning().blocks_per_sm;
+    if (blocks > cap) blocks = cap;
+    k_pr_gather<DT, ACC64, ADD_OLD, 256><<<(unsigned)(blocks ? blocks : 1), 256, 0, s>>>(
+        g->in_off, g->in_adj, contrib, g->n, yf, yd, st, sinv, tuning().pull_k, H.T);
+    GG_LAUNCHED(ctx);
+    if (H.nchunks) {
+        uint64_t cb = (H.nchunks * 32 + 255) / 256;
+        if (cb > cap) cb = cap;
+        k_pr_heavy_chunks<DT, ACC64><<<(unsigned)cb, 256, 0, s>>>(g->in_off, g->in_adj, contrib, H,
+                                                                  (Acc *)partial, st);
+        GG_LAUNCHED(ctx);
+        uint64_t fb = (H.nheavy + 255) / 256;
+        if (fb > cap) fb = cap;
+        k_pr_heavy_finalize<DT, ACC64, ADD_OLD, 256><<<(unsigned)fb, 256, 0, s>>>(H, (const Acc *)partial, yf, yd,
+                                                                                 st, sinv);
+        GG_LAUNCHED(ctx);
+    }
+    return GG_OK;
+}
+
 template <int DT>
 static gg_status pr_run(gg_graph *g, const gg_pr_params *p, float *x, float *y, void *contrib,
-                        PrState *st) {
+                        PrState *st, void *partial) {
     gg_ctx *ctx = g->ctx;
     cudaStream_t s = ctx->stream;
     using T = typename Store<DT>::T;
@@ -273,18 +383,15 @@ static gg_status pr_run(gg_graph *g, const gg_pr_params *p, float *x, float *y, 
     GG_LAUNCHED(ctx);
     k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, n, p->damping, st, 1);
     GG_LAUNCHED(ctx);
-    const int K = tuning().pull_k;
+    (void)gw;
     for (int it = 0; it < p->maxiter; ++it) {
         if (p->accum_f64)
-            k_pr_gather<DT, true, false, kBlock><<<gw, kBlock, 0, s>>>(g->in_off, g->in_adj, (const T *)contrib, n,
-                                                                      y, nullptr, st, 1.0f, K);
+            GG_CHECK((gather_launch<DT, true, false>(g, (const T *)contrib, y, nullptr, st, 1.0f, partial)));
         else
-            k_pr_gather<DT, false, false, kBlock><<<gw, kBlock, 0, s>>>(g->in_off, g->in_adj, (const T *)contrib, n,
-                                                                       y, nullptr, st, 1.0f, K);
-        GG_LAUNCHED(ctx);
+            GG_CHECK((gather_launch<DT, false, false>(g, (const T *)contrib, y, nullptr, st, 1.0f, partial)));
         k_pr_update<DT, kBlock><<<gv, kBlock, 0, s>>>(y, x, (T *)contrib, g->off, n, p->damping, p->renorm_f32, st);
         GG_LAUNCHED(ctx);
-        k_pr_finish<<<1, 1, 0, s>>>(st);
+        k_pr_finish<<<1, 1, 0, s>>>(st, DT);
         GG_LAUNCHED(ctx);
     }
     return GG_OK;
@@ -295,18 +402,14 @@ template <int DT>
 static gg_status gather_api(gg_graph *g, const gg_emap_desc *d) {
     gg_ctx *ctx = g->ctx;
     using T = typename Store<DT>::T;
-    const unsigned gw = pr_grid(ctx, (uint64_t)((g->n + 31) / 32) * 32);
     float *yf = d->a->t == GG_F32 ? (float *)d->a->d : nullptr;
     double *yd = d->a->t == GG_F64 ? (double *)d->a->d : nullptr;
     const float sc = d->src_scale != 0.0f ? d->src_scale : 1.0f;
+    void *partial = nullptr;
+    GG_CHECK(graph_scratch(g, (g->heavy.nchunks + 1) * 8, &partial));
     if (d->accum_f64)
-        k_pr_gather<DT, true, true, kBlock><<<gw, kBlock, 0, ctx->stream>>>(
-            g->in_off, g->in_adj, (const T *)d->src->d, g->n, yf, yd, nullptr, sc, tuning().pull_k);
-    else
-        k_pr_gather<DT, false, true, kBlock><<<gw, kBlock, 0, ctx->stream>>>(
-            g->in_off, g->in_adj, (const T *)d->src->d, g->n, yf, yd, nullptr, sc, tuning().pull_k);
-    GG_LAUNCHED(ctx);
-    return GG_OK;
+        return gather_launch<DT, true, true>(g, (const T *)d->src->d, yf, yd, nullptr, sc, partial);
+    return gather_launch<DT, false, true>(g, (const T *)d->src->d, yf, yd, nullptr, sc, partial);
 }
 
 gg_status pr_edgemap_gather(gg_graph *g, const gg_emap_desc *d, gg_frontier *in) {
@@ -350,12 +453,14 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
     }
     // scratch: y (f32), contrib (up to 4 B), state
     const size_t nb = (((size_t)g->n + 1) * 4 + 255) / 256 * 256;
+    const size_t sb = (sizeof(PrState) + 255) / 256 * 256;
     void *base = nullptr;
-    gg_status s = graph_scratch(g, 2 * nb + sizeof(PrState), &base);
+    gg_status s = graph_scratch(g, 2 * nb + sb + (g->heavy.nchunks + 1) * 8, &base);
     if (s != GG_OK) { if (tmpx) gg_prop_destroy(tmpx); return s; }
     float *y = (float *)base;
     void *contrib = (char *)base + nb;
     PrState *st = (PrState *)((char *)base + 2 * nb);
+    void *partial = (char *)base + 2 * nb + sb;
     PrState init;
     memset(&init, 0, sizeof(init));
     init.maxiter = p->maxiter;
@@ -368,12 +473,12 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
     cudaError_t e = cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
         switch (dt) {
-        case GG_F32: s = pr_run<GG_F32>(g, p, (float *)xp->d, y, contrib, st); break;
-        case GG_BF16: s = pr_run<GG_BF16>(g, p, (float *)xp->d, y, contrib, st); break;
-        case GG_F16: s = pr_run<GG_F16>(g, p, (float *)xp->d, y, contrib, st); break;
-        case GG_FP8E4M3: s = pr_run<GG_FP8E4M3>(g, p, (float *)xp->d, y, contrib, st); break;
-        case GG_CFP_6_10: s = pr_run<GG_CFP_6_10>(g, p, (float *)xp->d, y, contrib, st); break;
-        default: s = pr_run<GG_BF16_TRUNC>(g, p, (float *)xp->d, y, contrib, st); break;
+        case GG_F32: s = pr_run<GG_F32>(g, p, (float *)xp->d, y, contrib, st, partial); break;
+        case GG_BF16: s = pr_run<GG_BF16>(g, p, (float *)xp->d, y, contrib, st, partial); break;
+        case GG_F16: s = pr_run<GG_F16>(g, p, (float *)xp->d, y, contrib, st, partial); break;
+        case GG_FP8E4M3: s = pr_run<GG_FP8E4M3>(g, p, (float *)xp->d, y, contrib, st, partial); break;
+        case GG_CFP_6_10: s = pr_run<GG_CFP_6_10>(g, p, (float *)xp->d, y, contrib, st, partial); break;
+        default: s = pr_run<GG_BF16_TRUNC>(g, p, (float *)xp->d, y, contrib, st, partial); break;
         }
     } else {
         s = cuda_error(ctx, e, "gg_pagerank state upload");

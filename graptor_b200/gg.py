@@ -53,7 +53,8 @@ class EmapDesc(C.Structure):
 
 class EmapStats(C.Structure):
     _fields_ = [("variant", C.c_int), ("nactv_in", C.c_uint64), ("nacte_in", C.c_uint64),
-                ("scanned", C.c_uint64), ("nactv_out", C.c_uint64), ("nacte_out", C.c_uint64)]
+                ("scanned", C.c_uint64), ("nactv_out", C.c_uint64), ("nacte_out", C.c_uint64),
+                ("kernel_ms", C.c_double)]
 
 
 class VmapDesc(C.Structure):
@@ -63,9 +64,11 @@ class VmapDesc(C.Structure):
 
 class RunStats(C.Structure):
     _fields_ = [("iterations", C.c_int), ("total_ms", C.c_double), ("kernels", C.c_uint64),
-                ("scanned_edges", C.c_uint64), ("variant", C.c_int * MAX_ITERS),
+                ("scanned_edges", C.c_uint64), ("vertices_reached", C.c_uint64),
+                ("edges_reached", C.c_uint64), ("variant", C.c_int * MAX_ITERS),
                 ("nactv", C.c_uint64 * MAX_ITERS), ("nacte", C.c_uint64 * MAX_ITERS),
-                ("scanned", C.c_uint64 * MAX_ITERS), ("delta", C.c_double * MAX_ITERS)]
+                ("scanned", C.c_uint64 * MAX_ITERS), ("delta", C.c_double * MAX_ITERS),
+                ("iter_ms", C.c_double * MAX_ITERS)]
 
 
 class RunOpts(C.Structure):
@@ -292,8 +295,12 @@ class Graph:
 
     # analytics
     def bfs_level(self, root: int, level: "Prop" = None, host: bool = True, opts: RunOpts = None,
-                  stats: RunStats = None):
-        out = np.empty(self.n, dtype=np.int32) if host else None
+                  stats: RunStats = None, out: np.ndarray = None):
+        if out is not None:
+            assert out.dtype == np.int32 and out.size >= self.n and out.flags.c_contiguous
+            host = True
+        elif host:
+            out = np.empty(self.n, dtype=np.int32)
         self.ctx.check(lib().gg_bfs_level(self.h, root, C.byref(opts) if opts else None,
                                           level.h if level else None,
                                           _p(out) if host else None,

@@ -224,6 +224,7 @@ typedef struct gg_emap_stats {
     uint64_t scanned;   /* S_i (edges examined) when counted, else 0 */
     uint64_t nactv_out; /* N_i */
     uint64_t nacte_out;
+    double kernel_ms;   /* device time of the traversal kernel (CUDA events) */
 } gg_emap_stats;
 
 /* One edgemap step.  in may be NULL (all vertices active: no src filter).
@@ -288,11 +289,14 @@ typedef struct gg_run_stats {
     double total_ms;                  /* device time of the run (CUDA events) */
     uint64_t kernels;                 /* kernels launched */
     uint64_t scanned_edges;           /* sum of S_i */
+    uint64_t vertices_reached;        /* sum of |F_i| over the input frontiers */
+    uint64_t edges_reached;           /* sum of out-degrees over them (BFS: m_c) */
     int variant[GG_MAX_ITERS];        /* per iteration (-itimes) */
     uint64_t nactv[GG_MAX_ITERS];
     uint64_t nacte[GG_MAX_ITERS];
     uint64_t scanned[GG_MAX_ITERS];
     double delta[GG_MAX_ITERS];       /* PageRank L1 residual per iteration */
+    double iter_ms[GG_MAX_ITERS];     /* traversal-kernel device time (collect_stats) */
 } gg_run_stats;
 
 typedef struct gg_run_opts {

@@ -577,7 +577,8 @@ static float q_e4m3(float f) { return q_grid(f, 3, -6, 448.0f); }
  * Unlike PRv, run_prec renormalises by the double 1/s.  For ORC_FP8 the
  * contribution is stored as q(contrib * scale) with scale = 2^k chosen
  * each iteration so that max|contrib|*scale <= 448, and the gather
- * multiplies by 1/scale.  x_out gets the FP32 rank vector. */
+ * multiplies by 1/scale; ORC_F16 is scaled the same way (to 65504).
+ * x_out gets the FP32 rank vector. */
 ORC_API int orc_pr_vary(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj,
                         const uint32_t *outdeg, int fmt, int accum_f64, int maxiter,
                         double tol, float *x_out, double *deltas) {
@@ -598,16 +599,16 @@ ORC_API int orc_pr_vary(uint32_t n, const uint64_t *in_off, const uint32_t *in_a
             if (c > cmax) cmax = c;
         }
         float scale = 1.0f;
-        if (fmt == ORC_FP8 && cmax > 0.0f) {
+        if ((fmt == ORC_FP8 || fmt == ORC_F16) && cmax > 0.0f) {
             int e;
-            frexpf(448.0f / cmax, &e);
+            frexpf((fmt == ORC_FP8 ? 448.0f : 65504.0f) / cmax, &e);
             scale = ldexpf(1.0f, e - 1);
         }
         for (uint32_t v = 0; v < n; ++v) {
             float c = cq[v];
             switch (fmt) {
             case ORC_BF16: c = q_bf16_rne(c); break;
-            case ORC_F16: c = q_f16(c); break;
+            case ORC_F16: c = q_f16(c * scale) / scale; break;
             case ORC_FP8: c = q_e4m3(c * scale) / scale; break;
             case ORC_CFP_6_10: c = orc_cfp_to_float(orc_cfp_from_float(c, 0, 6, 10), 0, 6, 10); break;
             case ORC_BF16_TRUNC: c = orc_cfp_to_float(orc_cfp_from_float(c, 1, 8, 7), 1, 8, 7); break;
