@@ -8,11 +8,14 @@
 // self-loop removal, de-duplication, transposition) runs on the device with a
 // radix sort of packed (row, col) keys.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -44,6 +47,29 @@ size_t dtype_size(gg_dtype t) {
 Tuning &tuning() {
     static Tuning t;
     return t;
+}
+
+int resident_ctas(const void *kernel, int block) {
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto key = std::make_pair(kernel, block);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, 0) != cudaSuccess || nb < 1) {
+        cudaGetLastError();
+        nb = 1;
+    }
+    cache[key] = nb;
+    return nb;
+}
+
+unsigned occ_grid(gg_ctx *ctx, const void *kernel, int block, uint64_t work_threads) {
+    const uint64_t cap = (uint64_t)ctx->sm_count * resident_ctas(kernel, block);
+    uint64_t b = (work_threads + block - 1) / block;
+    if (b > cap) b = cap;
+    return (unsigned)(b ? b : 1);
 }
 
 uint32_t bin_of_degree(uint64_t deg) {
@@ -228,6 +254,14 @@ __global__ void k_heavy_gather(const uint32_t *hv, uint32_t nh, const uint64_t *
     if (i == nh) cnt[i] = 0;
 }
 
+// crow[c] = heavy index owning chunk c
+__global__ void k_heavy_crow(const uint64_t *first, uint32_t nh, uint32_t *crow) {
+    uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t stride = gridDim.x * blockDim.x;
+    for (; h < nh; h += stride)
+        for (uint64_t c = first[h]; c < first[h + 1]; ++c) crow[c] = h;
+}
+
 static int ceil_log2(uint64_t x) {
     int l = 0;
     while ((1ull << l) < x) ++l;
@@ -317,7 +351,7 @@ gg_status build_heavy_rows(gg_graph *g) {
     HK(cudaMalloc(&H.v, ((size_t)n + 1) * 4));
     k_heavy_count<<<grid_for(ctx, n), 256, 0, st>>>(g->in_off, n, H.T, H.CH, flag, nch);
     ctx->launches++;
-    cub::CountingInputIterator<uint32_t> it(0);
+    thrust::counting_iterator<uint32_t> it(0);
     HK(cub::DeviceSelect::Flagged(nullptr, tb, it, flag, H.v, d_num, (int64_t)n, st));
     HK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, nch, nch, (int64_t)n + 1, st));
     HK(cudaMalloc(&tmp, std::max(tb, tb2)));
@@ -335,6 +369,12 @@ gg_status build_heavy_rows(gg_graph *g) {
     ctx->launches++;
     HK(cudaMemcpyAsync(&H.nchunks, H.first + nh, 8, cudaMemcpyDeviceToHost, st));
     HK(cudaStreamSynchronize(st));
+    HK(cudaMalloc(&H.crow, (H.nchunks + 1) * 4));
+    if (nh) {
+        k_heavy_crow<<<grid_for(ctx, nh), 256, 0, st>>>(H.first, (uint32_t)nh, H.crow);
+        ctx->launches++;
+        HK(cudaStreamSynchronize(st));
+    }
 #undef HK
     return done(rc);
 }
@@ -385,8 +425,14 @@ static void graph_free(gg_graph *g) {
     cudaFree(g->aux_cnt);
     cudaFree(g->heavy.v);
     cudaFree(g->heavy.first);
+    cudaFree(g->heavy.crow);
+    cudaFree(g->cand.list[0]);
+    cudaFree(g->cand.list[1]);
+    cudaFree(g->cand.cnt);
     for (auto *f : g->tmp_front)
         if (f) gg_frontier_destroy(f);
+    for (auto *p : g->tmp_prop)
+        if (p) gg_prop_destroy(p);
     delete g;
 }
 
@@ -597,6 +643,41 @@ gg_status gg_ctx_sync(gg_ctx *ctx) {
 const char *gg_last_error(gg_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
 
 uint64_t gg_ctx_launch_count(gg_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+gg_status gg_tuning_set(const char *name, int64_t v) {
+    if (!name || v < 0 || v > (int64_t)1 << 31) return GG_ERR_ARG;
+    Tuning &t = tuning();
+    std::string k(name);
+    if (k == "bin_small_max") t.bin_small_max = (uint32_t)v;
+    else if (k == "bin_medium_max") t.bin_medium_max = (uint32_t)v;
+    else if (k == "pull_k" && v >= 1 && v <= 1024) t.pull_k = (int)v;
+    else if (k == "push_k" && v >= 1 && v <= 1024) t.push_k = (int)v;
+    else if (k == "heavy_deg" && v >= 32) t.heavy_deg = (uint32_t)v;
+    else if (k == "heavy_chunk" && v >= 32) t.heavy_chunk = (uint32_t)v;
+    else if (k == "large_chunk" && v >= 256) t.large_chunk = (uint32_t)v;
+    else if (k == "pr_stream" && v <= 1) t.pr_stream = (int)v;
+    else if (k == "blocks_per_sm" && v >= 1 && v <= 32) t.blocks_per_sm = (int)v;
+    else return GG_ERR_ARG;
+    if (t.bin_small_max > t.bin_medium_max) return GG_ERR_ARG;
+    return GG_OK;
+}
+
+gg_status gg_tuning_get(const char *name, int64_t *v) {
+    if (!name || !v) return GG_ERR_ARG;
+    const Tuning &t = tuning();
+    std::string k(name);
+    if (k == "bin_small_max") *v = t.bin_small_max;
+    else if (k == "bin_medium_max") *v = t.bin_medium_max;
+    else if (k == "pull_k") *v = t.pull_k;
+    else if (k == "push_k") *v = t.push_k;
+    else if (k == "heavy_deg") *v = t.heavy_deg;
+    else if (k == "heavy_chunk") *v = t.heavy_chunk;
+    else if (k == "large_chunk") *v = t.large_chunk;
+    else if (k == "pr_stream") *v = t.pr_stream;
+    else if (k == "blocks_per_sm") *v = t.blocks_per_sm;
+    else return GG_ERR_ARG;
+    return GG_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Graphs

@@ -58,6 +58,14 @@ struct EmapArgs {
     unsigned long long *out_cnt;
     uint32_t smax, mmax;
     int K;
+    const uint64_t *large_first;  // [c2 + 1] chunk prefix of the large bin (push)
+    uint32_t large_ch;            // edges per large-bin chunk
+    // pull candidate lists (drivers only): the destinations that can still
+    // pass the (monotone) dst filter.  cand == nullptr: scan all vertices.
+    const uint32_t *cand;
+    const unsigned long long *cand_n;   // device count of cand
+    uint32_t *cand_out;                 // vertices still passing after this step
+    unsigned long long *cand_out_n;
 };
 
 template <int R>
@@ -166,37 +174,58 @@ __device__ __forceinline__ void flush_counts(const EmapArgs &A, unsigned long lo
 // ---------------------------------------------------------------------------
 // Dense pull over the CSC
 // ---------------------------------------------------------------------------
-template <int R, bool SRCF, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_pull(EmapArgs A, Op<R> op) {
+// One lane owns one destination d.  Full-scan mode walks 32-vertex words
+// (one output bitmap word per warp, plain store); candidate mode walks a
+// list of destinations (output bitmap pre-cleared, bits set with atomicOr).
+// Loads are issued ahead of use: d's value and both offsets together, then
+// up to 4 neighbour ids, then their frontier bits and source values.
+template <int R, bool SRCF, bool CAND, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
     using V = typename Op<R>::V;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t nwords = (A.n + 31u) >> 5;
-    const uint32_t nw = (gridDim.x * BLOCK) >> 5;
+    const uint64_t nitems = CAND ? *A.cand_n : (uint64_t)A.n;
+    const uint64_t nw = (gridDim.x * BLOCK) >> 5;
     unsigned long long nv = 0, ne = 0, sc = 0;
-    for (uint32_t w = (blockIdx.x * BLOCK + threadIdx.x) >> 5; w < nwords; w += nw) {
-        const uint32_t d = (w << 5) + lane;
-        const bool valid = d < A.n;
-        V best = valid ? op.load(d) : Op<R>::none();
-        bool act = valid && op.dst_ok(best);
-        bool changed = false;
+    for (uint64_t w = (blockIdx.x * BLOCK + threadIdx.x) >> 5; (w << 5) < nitems; w += nw) {
+        const uint64_t item = (w << 5) + lane;
+        const bool valid = item < nitems;
+        const uint32_t d = CAND ? (valid ? A.cand[item] : 0u) : (uint32_t)item;
+        V best = Op<R>::none();
         uint64_t e = 0, end = 0;
-        if (act) {
+        if (valid) {
+            best = op.load(d);
             e = A.in_off[d];
             end = A.in_off[d + 1];
         }
+        bool act = valid && op.dst_ok(best);
+        bool changed = false;
         const uint64_t beg = e;
         const uint64_t lim = min(end, e + (uint64_t)A.K);
         while (act && e < lim) {
-            const uint32_t s = __ldg(A.in_adj + e);
-            ++e;
-            if (!SRCF || dev::bit_test(A.in_bits, s)) {
-                V x = op.src_val(s);
-                if (op.better(x, best)) {
-                    best = x;
+            const int cnt = (int)min((uint64_t)4, lim - e);
+            uint32_t sv[4];
+            bool inF[4];
+            V xv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) sv[j] = j < cnt ? __ldg(A.in_adj + e + j) : 0u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                inF[j] = j < cnt && (!SRCF || dev::bit_test(A.in_bits, sv[j]));
+                xv[j] = j < cnt ? op.src_val(sv[j]) : Op<R>::none();
+            }
+            int used = cnt;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (j < cnt && act && inF[j] && op.better(xv[j], best)) {
+                    best = xv[j];
                     changed = true;
-                    if (!op.dst_ok(best)) act = false;
+                    if (!op.dst_ok(best)) {
+                        act = false;
+                        used = j + 1;
+                    }
                 }
             }
+            e += used;
         }
         sc += e - beg;
         unsigned pend = __ballot_sync(FULL, act && e < end);
@@ -206,7 +235,7 @@ __global__ void __launch_bounds__(BLOCK) k_pull(EmapArgs A, Op<R> op) {
             const uint64_t ej = __shfl_sync(FULL, e, j);
             const uint64_t endj = __shfl_sync(FULL, end, j);
             V bj = __shfl_sync(FULL, best, j);
-            bool chj = false;
+            bool chj = false, actj = true;
             for (uint64_t base = ej; base < endj; base += 32) {
                 const uint64_t idx = base + lane;
                 bool ok = false;
@@ -223,12 +252,16 @@ __global__ void __launch_bounds__(BLOCK) k_pull(EmapArgs A, Op<R> op) {
                 if (okm) {
                     bj = op.warp_pick(ok, x, okm);
                     chj = true;
-                    if (!op.dst_ok(bj)) break;
+                    if (!op.dst_ok(bj)) {
+                        actj = false;
+                        break;
+                    }
                 }
             }
             if ((int)lane == j) {
                 best = bj;
                 changed = changed || chj;
+                act = actj;
             }
         }
         bool rec = false;
@@ -244,10 +277,27 @@ __global__ void __launch_bounds__(BLOCK) k_pull(EmapArgs A, Op<R> op) {
             }
         }
         if (A.out_bits) {
-            const unsigned bits = __ballot_sync(FULL, rec);
-            if (lane == 0) A.out_bits[w] = bits;
+            if (CAND) {
+                if (rec) atomicOr(A.out_bits + (d >> 5), 1u << (d & 31));
+            } else {
+                const unsigned bits = __ballot_sync(FULL, rec);
+                if (lane == 0) A.out_bits[w] = bits;
+            }
         }
         if (A.out_b0) emit_out(A, rec, d, nv, ne);
+        if (A.cand_out) {
+            // still a candidate: passes the filter and has in-edges
+            const bool keep = valid && act && end > beg;
+            const unsigned am = __activemask();
+            const unsigned mk = __ballot_sync(am, keep);
+            if (mk) {
+                const int leader = __ffs(mk) - 1;
+                unsigned long long base = 0;
+                if ((int)lane == leader) base = atomicAdd(A.cand_out_n, (unsigned long long)__popc(mk));
+                base = __shfl_sync(am, base, leader);
+                if (keep) A.cand_out[base + __popc(mk & ((1u << lane) - 1u))] = d;
+            }
+        }
     }
     if (A.out_cnt) flush_counts<BLOCK>(A, nv, ne, sc);
 }
@@ -262,11 +312,20 @@ __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uin
     const uint32_t lane = threadIdx.x & 31u;
     unsigned long long nv = 0, ne = 0, sc = 0;
     if (blockIdx.x < nb_large) {
-        // large bin: a CTA per source vertex
-        for (uint32_t i = blockIdx.x; i < A.c2; i += nb_large) {
-            const uint32_t s = A.in_b2[i];
+        // large bin: rows cut into chunks of large_ch edges, a CTA per chunk,
+        // so one hub row is spread over many SMs
+        const uint64_t nch = A.large_first[A.c2];
+        for (uint64_t c = blockIdx.x; c < nch; c += nb_large) {
+            uint32_t lo = 0, hi = A.c2;  // last h with large_first[h] <= c
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (A.large_first[mid] <= c) lo = mid; else hi = mid;
+            }
+            const uint32_t s = A.in_b2[lo];
             const V sv = op.src_val(s);
-            const uint64_t beg = A.off[s], end = A.off[s + 1];
+            const uint64_t rb = A.off[s], re = A.off[s + 1];
+            const uint64_t beg = rb + (c - A.large_first[lo]) * A.large_ch;
+            const uint64_t end = min(beg + A.large_ch, re);
             if (threadIdx.x == 0) sc += end - beg;
             for (uint64_t base = beg; base < end; base += BLOCK) {
                 const uint64_t e = base + threadIdx.x;
@@ -332,6 +391,18 @@ __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uin
         }
     }
     flush_counts<BLOCK>(A, nv, ne, sc);
+}
+
+// chunks of each large-bin vertex's row (first[c2] = 0 before the scan)
+__global__ void k_large_chunks(const uint32_t *b2, uint32_t c2, const uint64_t *off, uint32_t ch,
+                               uint64_t *first) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < c2) {
+        const uint32_t v = b2[i];
+        first[i] = (off[v + 1] - off[v] + ch - 1) / ch;
+    } else if (i == c2) {
+        first[i] = 0;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -579,11 +650,37 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
             GG_CHECK(frontier_ensure_bitmap(in));
             A.in_bits = in->bitmap;
         }
-        unsigned grid = persistent_grid(ctx, words);
+        CandLists *cl = g->cand_active ? &g->cand : nullptr;
+        if (cl) {
+            A.cand_out = cl->list[cl->cur ^ 1];
+            A.cand_out_n = (unsigned long long *)(cl->cnt + (cl->cur ^ 1));
+            GG_CUDA(ctx, cudaMemsetAsync(A.cand_out_n, 0, 8, st));
+            if (cl->valid) {
+                A.cand = cl->list[cl->cur];
+                A.cand_n = (const unsigned long long *)(cl->cnt + cl->cur);
+                if (A.out_bits) GG_CUDA(ctx, cudaMemsetAsync(A.out_bits, 0, words * 4, st));
+            }
+        }
+        const uint64_t items = (A.cand && cl->host_n != UINT64_MAX) ? cl->host_n : (uint64_t)g->n;
+        const void *kp = A.cand ? (all_in ? (const void *)k_pull<R, false, true, kBlock>
+                                          : (const void *)k_pull<R, true, true, kBlock>)
+                                : (all_in ? (const void *)k_pull<R, false, false, kBlock>
+                                          : (const void *)k_pull<R, true, false, kBlock>);
+        const unsigned grid = occ_grid(ctx, kp, kBlock, items);
         tstart();
-        if (all_in) k_pull<R, false, kBlock><<<grid, kBlock, 0, st>>>(A, op);
-        else k_pull<R, true, kBlock><<<grid, kBlock, 0, st>>>(A, op);
+        if (A.cand) {
+            if (all_in) k_pull<R, false, true, kBlock><<<grid, kBlock, 0, st>>>(A, op);
+            else k_pull<R, true, true, kBlock><<<grid, kBlock, 0, st>>>(A, op);
+        } else {
+            if (all_in) k_pull<R, false, false, kBlock><<<grid, kBlock, 0, st>>>(A, op);
+            else k_pull<R, true, false, kBlock><<<grid, kBlock, 0, st>>>(A, op);
+        }
         GG_LAUNCHED(ctx);
+        if (cl) {
+            cl->cur ^= 1;
+            cl->valid = true;
+            cl->host_n = UINT64_MAX;  // known on the device only
+        }
         break;
     }
     case GG_VAR_PUSH_DENSE: {
@@ -610,7 +707,27 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
         A.c1 = (uint32_t)in->h_cnt[FC_BIN1];
         A.c2 = (uint32_t)in->h_cnt[FC_BIN2];
         const uint32_t cap = ctx->sm_count * t.blocks_per_sm;
-        uint32_t nb_large = std::min<uint32_t>(A.c2, cap);
+        uint32_t nb_large = 0;
+        if (A.c2) {
+            // chunk table of the large bin: counts, then an exclusive scan
+            A.large_ch = t.large_chunk;
+            size_t cub_bytes = 0;
+            GG_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (uint64_t *)nullptr,
+                                                       (uint64_t *)nullptr, (int64_t)A.c2 + 1, st));
+            const size_t fb = (((size_t)A.c2 + 1) * 8 + 255) / 256 * 256;
+            void *p;
+            GG_CHECK(graph_scratch(g, fb + cub_bytes, &p));
+            uint64_t *first = (uint64_t *)p;
+            k_large_chunks<<<(A.c2 + 256) / 256, 256, 0, st>>>(A.in_b2, A.c2, g->off, A.large_ch, first);
+            GG_LAUNCHED(ctx);
+            GG_CUDA(ctx, cub::DeviceScan::ExclusiveSum((char *)p + fb, cub_bytes, first, first,
+                                                       (int64_t)A.c2 + 1, st));
+            ctx->launches++;
+            A.large_first = first;
+            // upper bound on the chunk count from the host-known edge total
+            const uint64_t est = in->h_cnt[FC_NACTE] / A.large_ch + A.c2;
+            nb_large = (uint32_t)std::min<uint64_t>(est, cap);
+        }
         uint32_t nb_med = std::min<uint32_t>((A.c1 + kBlock / 32 - 1) / (kBlock / 32), cap);
         uint32_t nb_small = std::min<uint32_t>((A.c0 + kBlock - 1) / kBlock, cap);
         uint32_t grid = nb_large + nb_med + nb_small;
@@ -784,10 +901,18 @@ static gg_status get_tmp_frontiers(gg_graph *g, gg_frontier **a, gg_frontier **b
     return GG_OK;
 }
 
-struct TmpProp {
-    gg_prop *p = nullptr;
-    ~TmpProp() { if (p) gg_prop_destroy(p); }
-};
+// Per-graph cached temporaries (prev copies, default outputs): created on
+// first use, reused by later runs, freed with the graph.
+static gg_status tmp_prop(gg_graph *g, int slot, gg_dtype t, gg_prop **out) {
+    gg_prop *&p = g->tmp_prop[slot];
+    if (p && p->t != t) {
+        gg_prop_destroy(p);
+        p = nullptr;
+    }
+    if (!p) GG_CHECK(gg_prop_create(g, t, &p));
+    *out = p;
+    return GG_OK;
+}
 
 static void record_iter(gg_run_stats *st, int it, const gg_emap_stats &es) {
     if (!st || it >= GG_MAX_ITERS) return;
@@ -811,9 +936,31 @@ static void default_opts(const gg_run_opts *o, gg_run_opts *r, int thresh, int k
 }
 
 // Generic frontier loop shared by the three analytics.
+// Candidate lists live for one driver run.
+struct CandScope {
+    gg_graph *g;
+    explicit CandScope(gg_graph *gr) : g(gr) {}
+    gg_status open() {
+        CandLists &c = g->cand;
+        if (!c.list[0]) {
+            for (auto &l : c.list) GG_CUDA(g->ctx, cudaMalloc(&l, ((size_t)g->n + 1) * 4));
+            GG_CUDA(g->ctx, cudaMalloc(&c.cnt, 2 * sizeof(uint64_t)));
+        }
+        c.cur = 0;
+        c.valid = false;
+        c.host_n = UINT64_MAX;
+        g->cand_active = true;
+        return GG_OK;
+    }
+    ~CandScope() { g->cand_active = false; }
+};
+
+// Generic frontier loop shared by the three analytics.
 static gg_status frontier_loop(gg_graph *g, gg_emap_desc &desc, gg_frontier *F, gg_frontier *O,
                                const gg_run_opts &opt, gg_run_stats *st, bool level_k,
                                int *iters_out) {
+    CandScope cs(g);
+    GG_CHECK(cs.open());
     int iter = 0;
     for (;;) {
         GG_CHECK(frontier_fetch_counts(F));
@@ -852,10 +999,9 @@ gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop
     if (level && (level->g != g || level->t != GG_I32)) return set_error(g->ctx, GG_ERR_ARG, "level must be an I32 property of g");
     gg_run_opts opt;
     default_opts(o, &opt, GG_THRESH_DEFAULT, 0);
-    TmpProp tl, tp;
-    if (!level) { GG_CHECK(gg_prop_create(g, GG_I32, &tl.p)); level = tl.p; }
-    GG_CHECK(gg_prop_create(g, GG_I32, &tp.p));
-    gg_prop *prev = tp.p;
+    if (!level) GG_CHECK(tmp_prop(g, 0, GG_I32, &level));
+    gg_prop *prev;
+    GG_CHECK(tmp_prop(g, 1, GG_I32, &prev));
     if (st) memset(st, 0, sizeof(*st));
     uint64_t k0 = g->ctx->launches;
     RunTimer tm(g->ctx);
@@ -896,10 +1042,9 @@ gg_status gg_bfs_parent(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_pro
     if (parent && (parent->g != g || parent->t != GG_U32)) return set_error(g->ctx, GG_ERR_ARG, "parent must be a U32 property of g");
     gg_run_opts opt;
     default_opts(o, &opt, GG_THRESH_DEFAULT, 0);
-    TmpProp tl, tp;
-    if (!parent) { GG_CHECK(gg_prop_create(g, GG_U32, &tl.p)); parent = tl.p; }
-    GG_CHECK(gg_prop_create(g, GG_U32, &tp.p));
-    gg_prop *prev = tp.p;
+    if (!parent) GG_CHECK(tmp_prop(g, 2, GG_U32, &parent));
+    gg_prop *prev;
+    GG_CHECK(tmp_prop(g, 3, GG_U32, &prev));
     if (st) memset(st, 0, sizeof(*st));
     uint64_t k0 = g->ctx->launches;
     RunTimer tm(g->ctx);
@@ -941,10 +1086,9 @@ gg_status gg_cc(gg_graph *g, const gg_run_opts *o, gg_prop *label, uint32_t *hos
     if (label && (label->g != g || label->t != GG_U32)) return set_error(g->ctx, GG_ERR_ARG, "label must be a U32 property of g");
     gg_run_opts opt;
     default_opts(o, &opt, GG_THRESH_FRAC, 5);  // CCv.C:309 emap_step(F, 5)
-    TmpProp tl, tp;
-    if (!label) { GG_CHECK(gg_prop_create(g, GG_U32, &tl.p)); label = tl.p; }
-    GG_CHECK(gg_prop_create(g, GG_U32, &tp.p));
-    gg_prop *prev = tp.p;
+    if (!label) GG_CHECK(tmp_prop(g, 2, GG_U32, &label));
+    gg_prop *prev;
+    GG_CHECK(tmp_prop(g, 3, GG_U32, &prev));
     if (st) memset(st, 0, sizeof(*st));
     gg_ctx *ctx = g->ctx;
     uint64_t k0 = ctx->launches;

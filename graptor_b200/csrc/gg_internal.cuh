@@ -5,6 +5,7 @@
 #include <string>
 
 #include "gg.h"
+#include "gg_tune.h"
 
 namespace gg {
 
@@ -82,9 +83,20 @@ struct gg_graph;
 struct HeavyRows {
     uint32_t *v = nullptr;      // heavy vertices, ascending
     uint64_t *first = nullptr;  // [nheavy + 1] chunk prefix
+    uint32_t *crow = nullptr;   // [nchunks] heavy index of each chunk
     uint32_t nheavy = 0;
     uint64_t nchunks = 0;
     uint32_t T = 0, CH = 0;
+};
+
+// Pull candidate lists of a driver run: destinations that still pass the
+// dst filter (double-buffered, device counts).
+struct CandLists {
+    uint32_t *list[2] = {nullptr, nullptr};
+    uint64_t *cnt = nullptr;  // [2] device counters
+    int cur = 0;
+    bool valid = false;       // list[cur] holds the candidates
+    uint64_t host_n = 0;      // count of list[cur] if known on the host, else UINT64_MAX
 };
 
 struct gg_frontier {
@@ -116,6 +128,9 @@ struct gg_graph {
     gg_frontier *tmp_front[2] = {nullptr, nullptr};
     uint64_t *aux_cnt = nullptr;  // counters of steps that record no frontier
     HeavyRows heavy;              // chunked long rows of the CSC (pull / gather)
+    gg_prop *tmp_prop[4] = {nullptr, nullptr, nullptr, nullptr};  // cached run temporaries
+    CandLists cand;               // pull candidate lists (driver runs)
+    bool cand_active = false;     // a driver run uses them for its pull steps
 };
 
 struct gg_prop {
@@ -148,8 +163,15 @@ struct Tuning {
     int blocks_per_sm = 8;
     uint32_t heavy_deg = 256;    // CSC rows longer than this are chunked
     uint32_t heavy_chunk = 1024; // edges per chunk
+    uint32_t large_chunk = 2048; // push: edges per chunk of a large-bin row
+    int pr_stream = 1;           // PageRank light rows: warp-streamed segmented gather
 };
 Tuning &tuning();
+
+// Grid of `block`-thread CTAs for a grid-stride kernel: resident CTAs per SM
+// (occupancy query, cached per kernel) x SM count, capped by the work.
+int resident_ctas(const void *kernel, int block);
+unsigned occ_grid(gg_ctx *ctx, const void *kernel, int block, uint64_t work_threads);
 
 }  // namespace gg
 

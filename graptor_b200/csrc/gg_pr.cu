@@ -111,52 +111,95 @@ template <int DT, bool ACC64, bool ADD_OLD, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_pr_gather(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj,
             const typename Store<DT>::T *__restrict__ contrib, uint32_t n, float *y_f32,
-            double *y_f64, PrState *st, float scale_inv_arg, int K, uint32_t T) {
+            double *y_f64, PrState *st, float scale_inv_arg, int K, uint32_t T, int stream) {
     using S = Store<DT>;
     using Acc = typename std::conditional<ACC64, double, float>::type;
+    constexpr int U = 4;  // 32-edge chunks in flight per warp iteration
+    __shared__ Acc sm[BLOCK / 32][33];
     if (st && st->done) return;
     const float sinv = st ? st->scale_inv : scale_inv_arg;
     const uint32_t lane = threadIdx.x & 31u;
+    Acc *row = sm[threadIdx.x >> 5];
     const uint32_t nwords = (n + 31u) >> 5;
     const uint32_t nw = (gridDim.x * BLOCK) >> 5;
+    const uint64_t oend = in_off[n];
     double ysum = 0;
     for (uint32_t w = (blockIdx.x * BLOCK + threadIdx.x) >> 5; w < nwords; w += nw) {
         const uint32_t d = (w << 5) + lane;
         const bool valid = d < n;
-        uint64_t beg = 0, end = 0;
-        if (valid) {
-            beg = in_off[d];
-            end = in_off[d + 1];
-        }
+        const uint64_t beg = valid ? in_off[d] : oend;
+        const uint64_t end = valid ? in_off[d + 1] : oend;
         // heavy rows are summed by k_pr_heavy_chunks / k_pr_heavy_finalize
-        const bool mine = valid && end - beg <= (uint64_t)T;
+        const bool heavy = end - beg > (uint64_t)T;
+        const bool mine = valid && !heavy;
         Acc acc = 0;
-        const bool shortrow = end - beg <= (uint64_t)K;
-        if (mine && shortrow) {
-            for (uint64_t e = beg; e < end; ++e) acc += (Acc)S::dec(contrib[__ldg(in_adj + e)]);
-        }
-        unsigned pend = __ballot_sync(FULL, mine && !shortrow);
-        while (pend) {
-            const int j = __ffs(pend) - 1;
-            pend &= pend - 1;
-            const uint64_t bj = __shfl_sync(FULL, beg, j);
-            const uint64_t ej = __shfl_sync(FULL, end, j);
-            Acc part = 0;
-            uint64_t base = bj;
-            for (; base + 128 <= ej; base += 128) {
-                uint32_t s0 = __ldg(in_adj + base + lane);
-                uint32_t s1 = __ldg(in_adj + base + 32 + lane);
-                uint32_t s2 = __ldg(in_adj + base + 64 + lane);
-                uint32_t s3 = __ldg(in_adj + base + 96 + lane);
-                part += (Acc)S::dec(contrib[s0]) + (Acc)S::dec(contrib[s1]) +
-                        (Acc)S::dec(contrib[s2]) + (Acc)S::dec(contrib[s3]);
+        if (stream && __ballot_sync(FULL, heavy) == 0) {
+            // Streaming: the word's 32 rows are contiguous in in_adj; lanes
+            // take consecutive edges, find their row by a 5-step search over
+            // the lanes' row starts, and sum per row with a segmented scan.
+            const uint64_t o0 = __shfl_sync(FULL, beg, 0);
+            const uint64_t o1 = __shfl_sync(FULL, end, 31);
+            row[lane] = 0;
+            __syncwarp();
+            for (uint64_t base = o0; base < o1; base += 32 * U) {
+                uint32_t sidx[U];
+                Acc val[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t e = base + u * 32 + lane;
+                    sidx[u] = e < o1 ? __ldg(in_adj + e) : 0u;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t e = base + u * 32 + lane;
+                    val[u] = e < o1 ? (Acc)S::dec(contrib[sidx[u]]) : (Acc)0;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const uint64_t e = base + u * 32 + lane;
+                    if (base + u * 32 >= o1) break;  // warp-uniform
+                    const bool ok = e < o1;
+                    uint32_t r = 0;
+#pragma unroll
+                    for (uint32_t step = 16; step >= 1; step >>= 1) {
+                        const uint64_t bc = __shfl_sync(FULL, beg, r + step);
+                        if (bc <= e) r += step;
+                    }
+                    if (!ok) r = 32;
+                    Acc v = val[u];
+#pragma unroll
+                    for (int dd = 1; dd < 32; dd <<= 1) {
+                        const Acc t = __shfl_up_sync(FULL, v, dd);
+                        const uint32_t rr = __shfl_up_sync(FULL, r, dd);
+                        if (lane >= (uint32_t)dd && rr == r) v += t;
+                    }
+                    const uint32_t rn = __shfl_down_sync(FULL, r, 1);
+                    const bool tail = lane == 31 || rn != r;
+                    if (ok && tail) row[r] += v;
+                    __syncwarp();
+                }
             }
-            for (; base < ej; base += 32) {
-                uint64_t e = base + lane;
-                if (e < ej) part += (Acc)S::dec(contrib[__ldg(in_adj + e)]);
+            acc = row[lane];
+            __syncwarp();
+        } else {
+            // words holding a heavy row: per-row sums for the light rows
+            const bool shortrow = end - beg <= (uint64_t)K;
+            if (mine && shortrow)
+                for (uint64_t e = beg; e < end; ++e) acc += (Acc)S::dec(contrib[__ldg(in_adj + e)]);
+            unsigned pend = __ballot_sync(FULL, mine && !shortrow);
+            while (pend) {
+                const int j = __ffs(pend) - 1;
+                pend &= pend - 1;
+                const uint64_t bj = __shfl_sync(FULL, beg, j);
+                const uint64_t ej = __shfl_sync(FULL, end, j);
+                Acc part = 0;
+                for (uint64_t b2 = bj; b2 < ej; b2 += 32) {
+                    const uint64_t e = b2 + lane;
+                    if (e < ej) part += (Acc)S::dec(contrib[__ldg(in_adj + e)]);
+                }
+                part = dev::warp_sum(part);
+                if ((int)lane == j) acc = part;
             }
-            part = dev::warp_sum(part);
-            if ((int)lane == j) acc = part;
         }
         if (mine) {
             if (DT == GG_FP8E4M3 || DT == GG_F16) acc *= (Acc)sinv;
@@ -190,12 +233,7 @@ k_pr_heavy_chunks(const uint64_t *__restrict__ in_off, const uint32_t *__restric
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < H.nchunks; c += nw) {
-        // heavy row owning chunk c: last h with first[h] <= c
-        uint32_t lo = 0, hi = H.nheavy;
-        while (hi - lo > 1) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (H.first[mid] <= c) lo = mid; else hi = mid;
-        }
+        const uint32_t lo = H.crow[c];  // heavy row owning chunk c
         const uint32_t v = H.v[lo];
         const uint64_t rb = in_off[v], re = in_off[v + 1];
         const uint64_t e0 = rb + (c - H.first[lo]) * H.CH;
@@ -353,7 +391,7 @@ static gg_status gather_launch(gg_graph *g, const typename Store<DT>::T *contrib
     const uint64_t cap = (uint64_t)ctx->sm_count * tuning().blocks_per_sm;
     if (blocks > cap) blocks = cap;
     k_pr_gather<DT, ACC64, ADD_OLD, 256><<<(unsigned)(blocks ? blocks : 1), 256, 0, s>>>(
-        g->in_off, g->in_adj, contrib, g->n, yf, yd, st, sinv, tuning().pull_k, H.T);
+        g->in_off, g->in_adj, contrib, g->n, yf, yd, st, sinv, tuning().pull_k, H.T, tuning().pr_stream);
     GG_LAUNCHED(ctx);
     if (H.nchunks) {
         uint64_t cb = (H.nchunks * 32 + 255) / 256;
@@ -400,7 +438,6 @@ static gg_status pr_run(gg_graph *g, const gg_pr_params *p, float *x, float *y, 
 // ADD_GATHER edgemap: y[d] += sum_{s in in(d), s active} dec(contrib[s]) * scale.
 template <int DT>
 static gg_status gather_api(gg_graph *g, const gg_emap_desc *d) {
-    gg_ctx *ctx = g->ctx;
     using T = typename Store<DT>::T;
     float *yf = d->a->t == GG_F32 ? (float *)d->a->d : nullptr;
     double *yd = d->a->t == GG_F64 ? (double *)d->a->d : nullptr;

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from typing import Optional
 
 import numpy as np
@@ -91,6 +92,7 @@ EXPORTS = [
     "gg_frontier_clear", "gg_frontier_set_single", "gg_frontier_set_all", "gg_frontier_set_list",
     "gg_frontier_counts", "gg_frontier_download", "gg_frontier_destroy", "gg_edgemap",
     "gg_vertexmap", "gg_bfs_level", "gg_bfs_parent", "gg_cc", "gg_pagerank",
+    "gg_tuning_set", "gg_tuning_get",
 ]
 
 
@@ -155,6 +157,8 @@ def lib() -> C.CDLL:
     L.gg_bfs_parent.argtypes = [vp, u32, C.POINTER(RunOpts), vp, vp, C.POINTER(RunStats)]
     L.gg_cc.argtypes = [vp, C.POINTER(RunOpts), vp, vp, C.POINTER(RunStats)]
     L.gg_pagerank.argtypes = [vp, C.POINTER(PrParams), vp, vp, C.POINTER(RunStats)]
+    L.gg_tuning_set.argtypes = [C.c_char_p, C.c_int64]
+    L.gg_tuning_get.argtypes = [C.c_char_p, C.POINTER(C.c_int64)]
     special = ("gg_status_string", "gg_dtype_size", "gg_last_error", "gg_ctx_launch_count")
     for name in EXPORTS:
         if name not in special:
@@ -179,6 +183,7 @@ class Context:
 
     def __init__(self, device: int = 0):
         self.h = C.c_void_p()
+        self._children = weakref.WeakSet()  # graphs: destroyed before the context
         s = lib().gg_ctx_create(device, C.byref(self.h))
         if s != GG_OK:
             raise GGError(s, "gg_ctx_create failed")
@@ -189,7 +194,11 @@ class Context:
             raise GGError(s, f"{what}: {msg}")
 
     def close(self):
+        """Destroy the context; graphs (and their properties and frontiers)
+        created from it are destroyed first, so no handle outlives it."""
         if self.h:
+            for g in list(self._children):
+                g.close()
             lib().gg_ctx_destroy(self.h)
             self.h = C.c_void_p()
 
@@ -252,19 +261,23 @@ class Context:
 class Graph:
     def __init__(self, ctx: Context, h: C.c_void_p):
         self.ctx, self.h = ctx, h
+        self._children = weakref.WeakSet()  # props / frontiers: destroyed before the graph
+        ctx._children.add(self)
         n, m, sym = C.c_uint32(), C.c_uint64(), C.c_int()
         ctx.check(lib().gg_graph_info(h, C.byref(n), C.byref(m), C.byref(sym)), "info")
         self.n, self.m, self.symmetric = n.value, m.value, bool(sym.value)
 
     def close(self):
         if self.h:
-            lib().gg_graph_destroy(self.h)
+            for c in list(self._children):
+                c.close()
+            if self.ctx.h:
+                lib().gg_graph_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):
         try:
-            if self.ctx.h:
-                self.close()
+            self.close()
         except Exception:
             pass
 
@@ -357,16 +370,17 @@ class Prop:
         self.g, self.dtype = g, dtype
         self.h = C.c_void_p()
         g.ctx.check(lib().gg_prop_create(g.h, dtype, C.byref(self.h)), "gg_prop_create")
+        g._children.add(self)
 
     def close(self):
         if self.h:
-            lib().gg_prop_destroy(self.h)
+            if self.g.h and self.g.ctx.h:
+                lib().gg_prop_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):
         try:
-            if self.g.h:
-                self.close()
+            self.close()
         except Exception:
             pass
 
@@ -407,16 +421,17 @@ class Frontier:
         self.g = g
         self.h = C.c_void_p()
         g.ctx.check(lib().gg_frontier_create(g.h, C.byref(self.h)), "gg_frontier_create")
+        g._children.add(self)
 
     def close(self):
         if self.h:
-            lib().gg_frontier_destroy(self.h)
+            if self.g.h and self.g.ctx.h:
+                lib().gg_frontier_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):
         try:
-            if self.g.h:
-                self.close()
+            self.close()
         except Exception:
             pass
 
@@ -445,6 +460,20 @@ class Frontier:
         a = np.empty(max(k.value, 1), dtype=np.uint32)
         self.g.ctx.check(lib().gg_frontier_download(self.h, _p(a), len(a), C.byref(k)), "download")
         return np.sort(a[: k.value])
+
+
+def tuning_set(name: str, value: int):
+    s = lib().gg_tuning_set(name.encode(), int(value))
+    if s != GG_OK:
+        raise GGError(s, f"gg_tuning_set({name}, {value})")
+
+
+def tuning_get(name: str) -> int:
+    v = C.c_int64()
+    s = lib().gg_tuning_get(name.encode(), C.byref(v))
+    if s != GG_OK:
+        raise GGError(s, f"gg_tuning_get({name})")
+    return v.value
 
 
 def default_opts(threshold=THRESH_DEFAULT, k=0, variant=VAR_AUTO, collect=False) -> RunOpts:

@@ -64,3 +64,21 @@ def test_ctx_create_reports_missing_device():
     from graptor_b200 import gg
     h = C.c_void_p()
     assert gg.lib().gg_ctx_create(0, C.byref(h)) == gg.GG_ERR_NOT_FOUND
+
+
+def test_tuning_knobs_roundtrip():
+    from graptor_b200 import gg
+    old = gg.tuning_get("pull_k")
+    try:
+        gg.tuning_set("pull_k", 12)
+        assert gg.tuning_get("pull_k") == 12
+    finally:
+        gg.tuning_set("pull_k", old)
+    with pytest.raises(gg.GGError):
+        gg.tuning_set("no_such_knob", 1)
+    with pytest.raises(gg.GGError):
+        gg.tuning_set("pull_k", 0)
+    small = gg.tuning_get("bin_small_max")
+    with pytest.raises(gg.GGError):  # small bin above the medium bin
+        gg.tuning_set("bin_small_max", gg.tuning_get("bin_medium_max") + 1)
+    gg.tuning_set("bin_small_max", small)

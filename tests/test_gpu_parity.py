@@ -168,6 +168,22 @@ def test_pagerank_precision(ctx, fmt):
     assert 1 <= st.iterations <= 100
 
 
+@pytest.mark.parametrize("stream", [0, 1])
+def test_pr_gather_schemes_agree(ctx, stream):
+    """Both light-row gather schemes (per-row, warp-streamed) and the
+    heavy-row chunks give PRv's answer."""
+    og = O.rmat(15, 16 << 15, seed=9)
+    g = upload(ctx, og)
+    old = gg.tuning_get("pr_stream")
+    gg.tuning_set("pr_stream", stream)
+    try:
+        x = g.pagerank(maxiter=20, tol=0)
+    finally:
+        gg.tuning_set("pr_stream", old)
+    xo, _, _ = O.pagerank(og, maxiter=20, tol=0)
+    assert np.abs(x.astype(np.float64) - xo).sum() <= PR_L1_VS_REF_F32
+
+
 def test_pr_cfp_matches_restatement(ctx):
     """customfp<6,10> storage against the restated PR_vary variant 46 loop."""
     og = O.rmat(12, 16 << 12, seed=8)
