@@ -328,6 +328,35 @@ typedef struct gg_pr_params {
 GG_API gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x, float *host_x,
                              gg_run_stats *st);
 
+/* ------------------------------------------------------------------ */
+/* BFS levels without allocation.  This entry point has no counterpart */
+/* in the reference.  It is for callers that cannot let a library call */
+/* cudaMalloc (a fixed device-memory budget owned by the caller's own  */
+/* pool, pipelines that must avoid the implicit device synchronisation */
+/* of cudaMalloc/cudaFree, hosts that forbid allocation by plug-ins).  */
+/* No context is needed and nothing is allocated: the caller passes    */
+/* the device CSR (d_off: n+1 entries, d_adj: d_off[n] entries) and    */
+/* the device output d_level (n entries: level of every vertex, root 0,*/
+/* unreached n+1, as gg_bfs_level).  Work runs on cuda_stream (NULL =  */
+/* the legacy default stream) of the current device.                   */
+/*   - n must not exceed GG_NOALLOC_MAX_VERTICES; larger graphs return */
+/*     GG_ERR_ARG with a message in err (may be NULL) and launch       */
+/*     nothing.                                                        */
+/*   - The frontier queues live in one fixed __device__ array of about */
+/*     8 MiB that every GPU loading the library keeps until exit.      */
+/*     Every call on a device shares it and each call clears what must */
+/*     start at zero; calls that overlap on the GPU (other streams or  */
+/*     host threads) race on it, so the caller must serialise them.    */
+/*   - The first call on a device looks up the array's device address  */
+/*     (cudaGetSymbolAddress, once per device); make that first call   */
+/*     before any stream capture begins.                               */
+/*   - The call synchronises cuda_stream once per BFS level.           */
+/* ------------------------------------------------------------------ */
+#define GG_NOALLOC_MAX_VERTICES (1u << 20)
+GG_API gg_status gg_bfs_level_noalloc(const uint64_t *d_off, const uint32_t *d_adj, uint32_t n,
+                                      uint32_t root, int32_t *d_level, void *cuda_stream,
+                                      int *iterations, char *err, size_t err_len);
+
 #ifdef __cplusplus
 }
 #endif
