@@ -254,6 +254,30 @@ __global__ void k_heavy_gather(const uint32_t *hv, uint32_t nh, const uint64_t *
     if (i == nh) cnt[i] = 0;
 }
 
+__global__ void k_nonzero_flags(const uint64_t *in_off, uint32_t n, uint8_t *flag) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (; i < n; i += stride) flag[i] = in_off[i + 1] > in_off[i] ? 1 : 0;
+}
+
+// per-word work estimates (see HeavyRows)
+__global__ void k_word_costs(const uint64_t *in_off, uint32_t n, uint32_t T, uint64_t *light,
+                             uint64_t *pull) {
+    const uint32_t nwords = (n + 31) / 32;
+    uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (; w < nwords; w += stride) {
+        uint64_t cl = 0, cp = 0;
+        for (uint32_t v = w * 32; v < min(n, w * 32 + 32); ++v) {
+            const uint64_t d = in_off[v + 1] - in_off[v];
+            cl += 4 + (d <= T ? d : 0);
+            cp += 2 + (d < 16 ? d : 16);
+        }
+        light[w] = cl;
+        pull[w] = cp;
+    }
+}
+
 // crow[c] = heavy index owning chunk c
 __global__ void k_heavy_crow(const uint64_t *first, uint32_t nh, uint32_t *crow) {
     uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
@@ -369,6 +393,45 @@ gg_status build_heavy_rows(gg_graph *g) {
     ctx->launches++;
     HK(cudaMemcpyAsync(&H.nchunks, H.first + nh, 8, cudaMemcpyDeviceToHost, st));
     HK(cudaStreamSynchronize(st));
+    {
+        const uint32_t nwords = (n + 31) / 32;
+        HK(cudaMalloc(&H.light_prefix, ((size_t)nwords + 1) * 8));
+        HK(cudaMalloc(&H.pull_prefix, ((size_t)nwords + 1) * 8));
+        k_word_costs<<<grid_for(ctx, nwords), 256, 0, st>>>(g->in_off, n, H.T, H.light_prefix, H.pull_prefix);
+        ctx->launches++;
+        size_t tb3 = 0;
+        HK(cub::DeviceScan::InclusiveSum(nullptr, tb3, H.light_prefix, H.light_prefix, (int64_t)nwords, st));
+        if (tb3 > tb) {
+            cudaFree(tmp);
+            tmp = nullptr;
+            HK(cudaMalloc(&tmp, tb3));
+            tb = tb3;
+        }
+        if (nwords) {
+            HK(cub::DeviceScan::InclusiveSum(tmp, tb, H.light_prefix, H.light_prefix, (int64_t)nwords, st));
+            HK(cub::DeviceScan::InclusiveSum(tmp, tb, H.pull_prefix, H.pull_prefix, (int64_t)nwords, st));
+            ctx->launches += 2;
+        }
+    }
+    {
+        // vertices with in-edges (the first pull's candidates)
+        uint8_t *nz = flag;  // reuse: flag[v] = in-degree > 0
+        k_nonzero_flags<<<grid_for(ctx, n), 256, 0, st>>>(g->in_off, n, nz);
+        ctx->launches++;
+        HK(cudaMalloc(&g->nonisolated, ((size_t)n + 1) * 4));
+        HK(cudaMalloc(&g->nonisolated_n, 8));
+        size_t tb4 = 0;
+        HK(cub::DeviceSelect::Flagged(nullptr, tb4, it, nz, g->nonisolated, g->nonisolated_n, (int64_t)n, st));
+        if (tb4 > tb) {
+            cudaFree(tmp);
+            tmp = nullptr;
+            HK(cudaMalloc(&tmp, tb4));
+            tb = tb4;
+        }
+        HK(cub::DeviceSelect::Flagged(tmp, tb, it, nz, g->nonisolated, g->nonisolated_n, (int64_t)n, st));
+        ctx->launches++;
+        HK(cudaStreamSynchronize(st));
+    }
     HK(cudaMalloc(&H.crow, (H.nchunks + 1) * 4));
     if (nh) {
         k_heavy_crow<<<grid_for(ctx, nh), 256, 0, st>>>(H.first, (uint32_t)nh, H.crow);
@@ -426,6 +489,11 @@ static void graph_free(gg_graph *g) {
     cudaFree(g->heavy.v);
     cudaFree(g->heavy.first);
     cudaFree(g->heavy.crow);
+    cudaFree(g->nonisolated);
+    cudaFree(g->nonisolated_n);
+    cudaFree(g->pstate);
+    cudaFree(g->heavy.light_prefix);
+    cudaFree(g->heavy.pull_prefix);
     cudaFree(g->cand.list[0]);
     cudaFree(g->cand.list[1]);
     cudaFree(g->cand.cnt);
@@ -433,6 +501,9 @@ static void graph_free(gg_graph *g) {
         if (f) gg_frontier_destroy(f);
     for (auto *p : g->tmp_prop)
         if (p) gg_prop_destroy(p);
+    for (auto *b : g->pool_bins) cudaFree(b);
+    for (auto *b : g->pool_bitmaps) cudaFree(b);
+    for (auto *c : g->pool_cnt) cudaFree(c);
     delete g;
 }
 
@@ -491,24 +562,36 @@ __device__ __forceinline__ void emit_binned(bool act, uint32_t v, uint32_t bin, 
     }
 }
 
-// Bitmap (or all vertices when bm == nullptr) -> binned list + counts.
-__global__ void k_bitmap_to_list(const uint32_t *bm, uint32_t n, const uint64_t *off, uint32_t *b0,
-                                 uint32_t *b1, uint32_t *b2, unsigned long long *cnt,
-                                 uint32_t smax, uint32_t mmax) {
-    uint32_t nwords = (n + 31) / 32;
-    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    uint32_t nw = (gridDim.x * blockDim.x) >> 5;
-    uint32_t lane = threadIdx.x & 31;
+// Bitmap (or all vertices when bm == nullptr) -> binned list + counts, the
+// appends staged per warp in shared memory.
+__global__ void __launch_bounds__(256) k_bitmap_to_list(const uint32_t *bm, uint32_t n, const uint64_t *off,
+                                                        uint32_t *b0, uint32_t *b1, uint32_t *b2,
+                                                        unsigned long long *cnt, uint32_t smax, uint32_t mmax) {
+    __shared__ uint32_t sb[3][8][256];
+    const uint32_t wib = threadIdx.x >> 5;
+    gg::dev::WarpAppender<256> ap0{sb[0][wib], 0, b0, cnt + FC_BIN0};
+    gg::dev::WarpAppender<256> ap1{sb[1][wib], 0, b1, cnt + FC_BIN1};
+    gg::dev::WarpAppender<256> ap2{sb[2][wib], 0, b2, cnt + FC_BIN2};
+    const uint32_t nwords = (n + 31) / 32;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
     unsigned long long nv = 0, ne = 0;
     for (uint32_t w = warp; w < nwords; w += nw) {
-        uint32_t v = w * 32 + lane;
-        uint32_t word = bm ? bm[w] : 0xFFFFFFFFu;
-        bool act = v < n && ((word >> lane) & 1u);
-        uint64_t deg = act ? off[v + 1] - off[v] : 0;
-        uint32_t bin = deg <= smax ? 0 : (deg <= mmax ? 1 : 2);
+        const uint32_t word = bm ? bm[w] : 0xFFFFFFFFu;
+        if (word == 0) continue;  // warp-uniform
+        const uint32_t v = w * 32 + lane;
+        const bool act = v < n && ((word >> lane) & 1u);
+        const uint64_t deg = act ? off[v + 1] - off[v] : 0;
+        const uint32_t bin = deg <= smax ? 0 : (deg <= mmax ? 1 : 2);
         if (act) { nv++; ne += deg; }
-        emit_binned(act, v, bin, b0, b1, b2, cnt);
+        ap0.push(act && bin == 0, v);
+        ap1.push(act && bin == 1, v);
+        ap2.push(act && bin == 2, v);
     }
+    ap0.flush();
+    ap1.flush();
+    ap2.flush();
     nv = gg::dev::warp_sum(nv);
     ne = gg::dev::warp_sum(ne);
     if (lane == 0 && nv) {
@@ -645,9 +728,15 @@ const char *gg_last_error(gg_ctx *ctx) { return ctx ? ctx->err.c_str() : "no con
 uint64_t gg_ctx_launch_count(gg_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
 gg_status gg_tuning_set(const char *name, int64_t v) {
-    if (!name || v < 0 || v > (int64_t)1 << 31) return GG_ERR_ARG;
+    if (!name || v < 0) return GG_ERR_ARG;
     Tuning &t = tuning();
     std::string k(name);
+    if (k == "barrier_timeout_ns") {
+        if (v < 1) return GG_ERR_ARG;
+        t.barrier_timeout_ns = (unsigned long long)v;
+        return GG_OK;
+    }
+    if (v > (int64_t)1 << 31) return GG_ERR_ARG;
     if (k == "bin_small_max") t.bin_small_max = (uint32_t)v;
     else if (k == "bin_medium_max") t.bin_medium_max = (uint32_t)v;
     else if (k == "pull_k" && v >= 1 && v <= 1024) t.pull_k = (int)v;
@@ -657,6 +746,8 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "large_chunk" && v >= 256) t.large_chunk = (uint32_t)v;
     else if (k == "pr_stream" && v <= 1) t.pr_stream = (int)v;
     else if (k == "blocks_per_sm" && v >= 1 && v <= 32) t.blocks_per_sm = (int)v;
+    else if (k == "persistent" && v <= 7) t.persistent = (int)v;
+    else if (k == "barrier_timeout_ns" && v >= 1) t.barrier_timeout_ns = (unsigned long long)v;
     else return GG_ERR_ARG;
     if (t.bin_small_max > t.bin_medium_max) return GG_ERR_ARG;
     return GG_OK;
@@ -675,6 +766,8 @@ gg_status gg_tuning_get(const char *name, int64_t *v) {
     else if (k == "large_chunk") *v = t.large_chunk;
     else if (k == "pr_stream") *v = t.pr_stream;
     else if (k == "blocks_per_sm") *v = t.blocks_per_sm;
+    else if (k == "persistent") *v = t.persistent;
+    else if (k == "barrier_timeout_ns") *v = (int64_t)t.barrier_timeout_ns;
     else return GG_ERR_ARG;
     return GG_OK;
 }
@@ -953,7 +1046,13 @@ gg_status gg_frontier_create(gg_graph *g, gg_frontier **out) {
     gg_frontier *f = new (std::nothrow) gg_frontier;
     if (!f) return GG_ERR_OOM;
     f->g = g;
-    cudaError_t e = cudaMalloc(&f->d_cnt, FC_WORDS * sizeof(uint64_t));
+    cudaError_t e = cudaSuccess;
+    if (!g->pool_cnt.empty()) {
+        f->d_cnt = g->pool_cnt.back();
+        g->pool_cnt.pop_back();
+    } else {
+        e = cudaMalloc(&f->d_cnt, FC_WORDS * sizeof(uint64_t));
+    }
     if (e != cudaSuccess) { delete f; return cuda_error(g->ctx, e, "gg_frontier_create"); }
     e = cudaMemsetAsync(f->d_cnt, 0, FC_WORDS * sizeof(uint64_t), g->ctx->stream);
     if (e != cudaSuccess) { cudaFree(f->d_cnt); delete f; return cuda_error(g->ctx, e, "memset"); }
@@ -964,10 +1063,11 @@ gg_status gg_frontier_create(gg_graph *g, gg_frontier **out) {
 
 gg_status gg_frontier_destroy(gg_frontier *f) {
     if (!f) return GG_ERR_ARG;
-    cudaStreamSynchronize(f->g->ctx->stream);
-    for (auto *b : f->bins) cudaFree(b);
-    cudaFree(f->bitmap);
-    cudaFree(f->d_cnt);
+    gg_graph *g = f->g;
+    // buffers go back to the graph's pools (stream-ordered reuse)
+    if (f->bins[0]) g->pool_bins.push_back(f->bins[0]);
+    if (f->bitmap) g->pool_bitmaps.push_back(f->bitmap);
+    if (f->d_cnt) g->pool_cnt.push_back(f->d_cnt);
     delete f;
     return GG_OK;
 }
@@ -1075,17 +1175,35 @@ gg_status gg_frontier_download(gg_frontier *f, uint32_t *host_list, uint64_t cap
 // ---------------------------------------------------------------------------
 namespace gg {
 
+// Frontier buffers come from per-graph pools: analytics create and delete a
+// frontier every iteration (Graptor's frontier::del pattern), and all use of
+// a buffer is ordered on the context's stream, so a released buffer can be
+// handed to the next frontier without a cudaMalloc / cudaFree pair.
 gg_status frontier_alloc_bins(gg_frontier *f) {
     if (f->bins[0]) return GG_OK;
-    size_t cap = (size_t)f->g->n + 1;
-    for (int b = 0; b < NBINS; ++b) GG_CUDA(f->g->ctx, cudaMalloc(&f->bins[b], cap * 4));
+    gg_graph *g = f->g;
+    const size_t cap = (size_t)g->n + 1;
+    uint32_t *blk = nullptr;
+    if (!g->pool_bins.empty()) {
+        blk = g->pool_bins.back();
+        g->pool_bins.pop_back();
+    } else {
+        GG_CUDA(g->ctx, cudaMalloc(&blk, NBINS * cap * 4));
+    }
+    for (int b = 0; b < NBINS; ++b) f->bins[b] = blk + b * cap;
     return GG_OK;
 }
 
 gg_status frontier_alloc_bitmap(gg_frontier *f) {
     if (f->bitmap) return GG_OK;
-    size_t words = ((size_t)f->g->n + 31) / 32 + 1;
-    GG_CUDA(f->g->ctx, cudaMalloc(&f->bitmap, words * 4));
+    gg_graph *g = f->g;
+    if (!g->pool_bitmaps.empty()) {
+        f->bitmap = g->pool_bitmaps.back();
+        g->pool_bitmaps.pop_back();
+        return GG_OK;
+    }
+    size_t words = ((size_t)g->n + 31) / 32 + 1;
+    GG_CUDA(g->ctx, cudaMalloc(&f->bitmap, words * 4));
     return GG_OK;
 }
 

@@ -66,6 +66,7 @@ struct EmapArgs {
     const unsigned long long *cand_n;   // device count of cand
     uint32_t *cand_out;                 // vertices still passing after this step
     unsigned long long *cand_out_n;
+    const uint64_t *word_prefix;        // full-scan pull: per-word cost prefix
 };
 
 template <int R>
@@ -75,6 +76,7 @@ struct Op {
     V *prev;
     int filter;
     int64_t fk;
+    int level_sync;  // MIN_PLUS1: active sources hold fk-1, offer fk without a load
 
     __device__ __forceinline__ V load(uint32_t v) const { return a[v]; }
     __device__ __forceinline__ static V none() {
@@ -91,7 +93,7 @@ struct Op {
     }
     // value offered along an edge s->d
     __device__ __forceinline__ V src_val(uint32_t s) const {
-        if constexpr (R == GG_RELAX_MIN_PLUS1_I32) return a[s] + 1;
+        if constexpr (R == GG_RELAX_MIN_PLUS1_I32) return level_sync ? (V)fk : a[s] + 1;
         else if constexpr (R == GG_RELAX_MIN_U32) return a[s];
         else return (V)s;
     }
@@ -185,8 +187,16 @@ __global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nitems = CAND ? *A.cand_n : (uint64_t)A.n;
     const uint64_t nw = (gridDim.x * BLOCK) >> 5;
+    const uint64_t gw = (blockIdx.x * BLOCK + threadIdx.x) >> 5;
+    // candidate lists: grid-stride over list words; full scan: a contiguous
+    // range of vertex words of equal estimated work per warp
+    uint32_t wlo = 0, whi = 0;
+    if (!CAND) dev::balanced_range(A.word_prefix, (A.n + 31u) >> 5, gw, nw, wlo, whi);
+    const uint64_t wstep = CAND ? nw : 1;
     unsigned long long nv = 0, ne = 0, sc = 0;
-    for (uint64_t w = (blockIdx.x * BLOCK + threadIdx.x) >> 5; (w << 5) < nitems; w += nw) {
+    __shared__ uint32_t s_cand[BLOCK / 32][256];
+    dev::WarpAppender<256> keepers{s_cand[threadIdx.x >> 5], 0, A.cand_out, A.cand_out_n};
+    for (uint64_t w = CAND ? gw : wlo; CAND ? ((w << 5) < nitems) : (w < whi); w += wstep) {
         const uint64_t item = (w << 5) + lane;
         const bool valid = item < nitems;
         const uint32_t d = CAND ? (valid ? A.cand[item] : 0u) : (uint32_t)item;
@@ -278,27 +288,32 @@ __global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
         }
         if (A.out_bits) {
             if (CAND) {
-                if (rec) atomicOr(A.out_bits + (d >> 5), 1u << (d & 31));
+                // lanes holding vertices of the same bitmap word combine
+                // their bits; one atomicOr per word and warp
+                const uint32_t wd = d >> 5;
+                unsigned todo = __ballot_sync(FULL, rec);
+                while (todo) {  // one round per distinct word (list is mostly ascending)
+                    const int leader = __ffs(todo) - 1;
+                    const uint32_t w0 = __shfl_sync(FULL, wd, leader);
+                    const bool mine = rec && wd == w0;
+                    const unsigned bits = __reduce_or_sync(FULL, mine ? (1u << (d & 31)) : 0u);
+                    if ((int)lane == leader) atomicOr(A.out_bits + w0, bits);
+                    todo &= ~__ballot_sync(FULL, mine);
+                }
             } else {
                 const unsigned bits = __ballot_sync(FULL, rec);
                 if (lane == 0) A.out_bits[w] = bits;
             }
         }
-        if (A.out_b0) emit_out(A, rec, d, nv, ne);
-        if (A.cand_out) {
-            // still a candidate: passes the filter and has in-edges
-            const bool keep = valid && act && end > beg;
-            const unsigned am = __activemask();
-            const unsigned mk = __ballot_sync(am, keep);
-            if (mk) {
-                const int leader = __ffs(mk) - 1;
-                unsigned long long base = 0;
-                if ((int)lane == leader) base = atomicAdd(A.cand_out_n, (unsigned long long)__popc(mk));
-                base = __shfl_sync(am, base, leader);
-                if (keep) A.cand_out[base + __popc(mk & ((1u << lane) - 1u))] = d;
-            }
+        if (rec) {
+            // the output list is built from the bitmap only if a push needs it
+            nv++;
+            ne += A.off[d + 1] - A.off[d];
         }
+        // still a candidate: passes the filter and has in-edges
+        if (A.cand_out) keepers.push(valid && act && end > beg, d);
     }
+    if (A.cand_out) keepers.flush();
     if (A.out_cnt) flush_counts<BLOCK>(A, nv, ne, sc);
 }
 
@@ -598,6 +613,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     op.prev = d->prev ? (typename Op<R>::V *)d->prev->d : nullptr;
     op.filter = d->dst_filter;
     op.fk = d->dst_filter_k;
+    op.level_sync = (d->src_level_sync && d->dst_filter == GG_FILTER_GT_CONST) ? 1 : 0;
 
     EmapArgs A;
     memset(&A, 0, sizeof(A));
@@ -610,6 +626,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     A.smax = t.bin_small_max;
     A.mmax = t.bin_medium_max;
     A.K = variant == GG_VAR_PULL_DENSE ? t.pull_k : t.push_k;
+    A.word_prefix = g->heavy.pull_prefix;
     const bool have_out = out != nullptr && d->record != GG_RECORD_NONE;
     if (have_out) {
         GG_CHECK(frontier_alloc_bins(out));
@@ -658,8 +675,12 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
             if (cl->valid) {
                 A.cand = cl->list[cl->cur];
                 A.cand_n = (const unsigned long long *)(cl->cnt + cl->cur);
-                if (A.out_bits) GG_CUDA(ctx, cudaMemsetAsync(A.out_bits, 0, words * 4, st));
+            } else if (g->nonisolated) {
+                // first pull of a run: every vertex with in-edges
+                A.cand = g->nonisolated;
+                A.cand_n = (const unsigned long long *)g->nonisolated_n;
             }
+            if (A.cand && A.out_bits) GG_CUDA(ctx, cudaMemsetAsync(A.out_bits, 0, words * 4, st));
         }
         const uint64_t items = (A.cand && cl->host_n != UINT64_MAX) ? cl->host_n : (uint64_t)g->n;
         const void *kp = A.cand ? (all_in ? (const void *)k_pull<R, false, true, kBlock>
@@ -773,6 +794,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     }
     if (ctx->time_kernels) cudaEventRecord(ctx->evk1, st);
     if (have_out) {
+        const bool list_written = variant != GG_VAR_PULL_DENSE;
         if (d->record == GG_RECORD_NE_PREV && variant != GG_VAR_PULL_DENSE) {
             if (!d->prev) return set_error(ctx, GG_ERR_ARG, "NE_PREV record needs prev");
             k_copy_prev<<<persistent_grid(ctx, words), kBlock, 0, st>>>(
@@ -780,7 +802,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
             GG_LAUNCHED(ctx);
         }
         out->all = false;
-        out->has_list = true;
+        out->has_list = list_written;
         out->has_bitmap = out_bitmap_valid;
         out->host_valid = false;
     }
@@ -935,7 +957,6 @@ static void default_opts(const gg_run_opts *o, gg_run_opts *r, int thresh, int k
     }
 }
 
-// Generic frontier loop shared by the three analytics.
 // Candidate lists live for one driver run.
 struct CandScope {
     gg_graph *g;
@@ -954,6 +975,14 @@ struct CandScope {
     }
     ~CandScope() { g->cand_active = false; }
 };
+
+// Device-driven loop (analytic bit set in the `persistent` knob) unless a
+// variant only the host loop provides is asked for.
+// The learned selector and timing collection run device-driven always.
+static bool use_persistent(const gg_graph *g, const gg_run_opts &opt, int analytic_bit) {
+    if (opt.threshold == GG_THRESH_LEARNED || g->force_iter >= 0) return true;
+    return (tuning().persistent & analytic_bit) != 0;
+}
 
 // Generic frontier loop shared by the three analytics.
 static gg_status frontier_loop(gg_graph *g, gg_emap_desc &desc, gg_frontier *F, gg_frontier *O,
@@ -1019,13 +1048,15 @@ gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop
     desc.relax = GG_RELAX_MIN_PLUS1_I32;
     desc.a = level;
     desc.dst_filter = GG_FILTER_GT_CONST;  // level[d] > iter+1   (BFSLVLv.C:190-194)
+    desc.src_level_sync = 1;               // frontier of iteration i holds level i
     desc.record = GG_RECORD_NE_PREV;       // level[d] != prev[d]  (BFSLVLv.C:168-172)
     desc.prev = prev;
     desc.threshold = opt.threshold;
     desc.threshold_k = opt.threshold_k;
     desc.variant = opt.variant;
     int iters = 0;
-    GG_CHECK(frontier_loop(g, desc, F, O, opt, st, true, &iters));
+    if (use_persistent(g, opt, 1)) GG_CHECK(persistent_traverse(g, desc, 1, false, root, opt, st, &iters));
+    else GG_CHECK(frontier_loop(g, desc, F, O, opt, st, true, &iters));
     double ms = tm.stop();
     if (st) {
         st->iterations = iters;
@@ -1069,7 +1100,8 @@ gg_status gg_bfs_parent(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_pro
     desc.threshold_k = opt.threshold_k;
     desc.variant = opt.variant;
     int iters = 0;
-    GG_CHECK(frontier_loop(g, desc, F, O, opt, st, false, &iters));
+    if (use_persistent(g, opt, 2)) GG_CHECK(persistent_traverse(g, desc, 0, false, root, opt, st, &iters));
+    else GG_CHECK(frontier_loop(g, desc, F, O, opt, st, false, &iters));
     double ms = tm.stop();
     if (st) {
         st->iterations = iters;
@@ -1119,7 +1151,8 @@ gg_status gg_cc(gg_graph *g, const gg_run_opts *o, gg_prop *label, uint32_t *hos
     desc.threshold_k = opt.threshold_k;
     desc.variant = opt.variant;
     int iters = 0;
-    GG_CHECK(frontier_loop(g, desc, F, O, opt, st, false, &iters));
+    if (use_persistent(g, opt, 4)) GG_CHECK(persistent_traverse(g, desc, 0, true, 0, opt, st, &iters));
+    else GG_CHECK(frontier_loop(g, desc, F, O, opt, st, false, &iters));
     double ms = tm.stop();
     if (st) {
         st->iterations = iters;

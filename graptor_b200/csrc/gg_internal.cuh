@@ -3,9 +3,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string>
+#include <vector>
 
 #include "gg.h"
 #include "gg_tune.h"
+#include "gg_select.h"
 
 namespace gg {
 
@@ -84,6 +86,12 @@ struct HeavyRows {
     uint32_t *v = nullptr;      // heavy vertices, ascending
     uint64_t *first = nullptr;  // [nheavy + 1] chunk prefix
     uint32_t *crow = nullptr;   // [nchunks] heavy index of each chunk
+    // Per 32-vertex word work estimates (inclusive prefix over words) used to
+    // give every warp a contiguous range of equal estimated work:
+    //   light_prefix: PageRank light-row gather, light in-edges + 4 per vertex
+    //   pull_prefix : dense pull, min(in-degree, 16) + 2 per vertex
+    uint64_t *light_prefix = nullptr;
+    uint64_t *pull_prefix = nullptr;
     uint32_t nheavy = 0;
     uint64_t nchunks = 0;
     uint32_t T = 0, CH = 0;
@@ -129,8 +137,17 @@ struct gg_graph {
     uint64_t *aux_cnt = nullptr;  // counters of steps that record no frontier
     HeavyRows heavy;              // chunked long rows of the CSC (pull / gather)
     gg_prop *tmp_prop[4] = {nullptr, nullptr, nullptr, nullptr};  // cached run temporaries
+    uint32_t *nonisolated = nullptr;    // vertices with in-edges, ascending
+    uint64_t *nonisolated_n = nullptr;  // its length (device)
     CandLists cand;               // pull candidate lists (driver runs)
     bool cand_active = false;     // a driver run uses them for its pull steps
+    // released frontier buffers, reused in stream order
+    std::vector<uint32_t *> pool_bins, pool_bitmaps;
+    std::vector<uint64_t *> pool_cnt;
+    void *pstate = nullptr;       // device state block of persistent traversals
+    float gini = -1.0f;           // degree Gini coefficient (selector feature), <0: unknown
+    gg_selector *selector = nullptr;  // learned variant selector (GG_THRESH_LEARNED)
+    int force_iter = -1, force_variant = -1;  // timing collection: one forced choice
 };
 
 struct gg_prop {
@@ -152,6 +169,12 @@ gg_status frontier_ensure_list(gg_frontier *f);      // from bitmap / all
 gg_status frontier_reset_counts(gg_frontier *f);     // async zero of d_cnt
 uint32_t bin_of_degree(uint64_t deg);
 gg_status build_heavy_rows(gg_graph *g);
+gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, bool start_all, uint32_t root,
+                              const gg_run_opts &opt, gg_run_stats *stats, int *iters_out,
+                              int force_iter = -1, int force_variant = -1);
+gg_status graph_gini(gg_graph *g, float *out);
+void selector_features(float *x, double nactv, double nacte, double unreached, int iter, double n, double m,
+                       float gini);
 
 // Degree-bin thresholds of the sparse push (tunable by the autotuner).
 struct Tuning {
@@ -163,8 +186,14 @@ struct Tuning {
     int blocks_per_sm = 8;
     uint32_t heavy_deg = 256;    // CSC rows longer than this are chunked
     uint32_t heavy_chunk = 1024; // edges per chunk
-    uint32_t large_chunk = 2048; // push: edges per chunk of a large-bin row
-    int pr_stream = 1;           // PageRank light rows: warp-streamed segmented gather
+    uint32_t large_chunk = 512;  // push: edges per chunk of a large-bin row
+    int pr_stream = 0;           // PageRank light rows: warp-streamed segmented gather
+    // analytics run as one device-driven cooperative launch: bit 0 BFS levels,
+    // bit 1 BFS parents, bit 2 CC (the persistent grid reads values written
+    // during the launch through L2, which costs the big dense phases more
+    // than the per-iteration host round trips it saves on R-MAT BFS)
+    int persistent = 4;
+    unsigned long long barrier_timeout_ns = 5000000000ull;  // grid-barrier wait limit
 };
 Tuning &tuning();
 
@@ -183,6 +212,31 @@ namespace dev {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// Contiguous word range [lo, hi) of warp `wid` of `nw` warps such that every
+// warp gets an equal share of the work estimate.  pre[w] is the inclusive
+// prefix of the per-word costs (nwords entries); word w covers cost units
+// [pre[w-1], pre[w]) and belongs to the warp whose share [t0, t1) holds its
+// first unit.  Binary searches only, no atomics.
+__device__ __forceinline__ uint32_t prefix_lower(const uint64_t *__restrict__ pre, uint32_t nwords,
+                                                 uint64_t target) {
+    uint32_t a = 0, b = nwords;  // smallest w with pre[w] >= target
+    while (a < b) {
+        const uint32_t mid = (a + b) >> 1;
+        if (pre[mid] >= target) b = mid; else a = mid + 1;
+    }
+    return a;
+}
+
+__device__ __forceinline__ void balanced_range(const uint64_t *__restrict__ pre, uint32_t nwords,
+                                               uint64_t wid, uint64_t nw, uint32_t &lo, uint32_t &hi) {
+    if (nwords == 0) { lo = hi = 0; return; }
+    const uint64_t total = pre[nwords - 1];
+    const uint64_t t0 = (total * wid) / nw, t1 = (total * (wid + 1)) / nw;
+    lo = t0 == 0 ? 0u : min(prefix_lower(pre, nwords, t0) + 1, nwords);
+    hi = wid + 1 >= nw ? nwords : (t1 == 0 ? 0u : min(prefix_lower(pre, nwords, t1) + 1, nwords));
+    if (hi < lo) hi = lo;
+}
+
 __device__ __forceinline__ bool bit_test(const uint32_t *__restrict__ bm, uint32_t v) {
     return (__ldg(bm + (v >> 5)) >> (v & 31u)) & 1u;
 }
@@ -193,6 +247,36 @@ __device__ __forceinline__ T warp_sum(T x) {
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     return x;
 }
+
+// Per-warp staging of list appends in shared memory: one global atomic per
+// ~CAP appended items instead of one per 32.  push() and flush() must be
+// called by all 32 lanes together.
+template <int CAP>
+struct WarpAppender {
+    uint32_t *buf;                // this warp's CAP entries of shared memory
+    uint32_t n = 0;               // staged count (same in every lane)
+    uint32_t *dst;
+    unsigned long long *dst_n;
+    __device__ __forceinline__ void push(bool keep, uint32_t v) {
+        const uint32_t lane = threadIdx.x & 31u;
+        const unsigned mk = __ballot_sync(0xffffffffu, keep);
+        if (keep) buf[n + __popc(mk & ((1u << lane) - 1u))] = v;
+        n += __popc(mk);
+        if (n > CAP - 32) flush();
+    }
+    __device__ __forceinline__ void flush() {
+        __syncwarp();
+        if (n) {
+            const uint32_t lane = threadIdx.x & 31u;
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(dst_n, (unsigned long long)n);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            for (uint32_t i = lane; i < n; i += 32) dst[base + i] = buf[i];
+        }
+        __syncwarp();
+        n = 0;
+    }
+};
 
 // Block-wide sum of a per-thread value; result valid in thread 0.
 template <typename T, int BLOCK>

@@ -1,0 +1,925 @@
+// gg_persist.cu -- device-driven frontier traversal: one cooperative launch
+// runs every iteration of a BFS-level, BFS-parent or CC analytic.
+//
+// The host-driven loop (gg_emap.cu) synchronises once per iteration to read
+// the frontier counts that decide between sparse push and dense pull
+// (include/graptor/api.h:2223-2288).  Here every CTA of a persistent grid
+// reads those counts from device memory after a grid barrier and takes the
+// same decision, so a whole traversal is one launch with no host round trip
+// and no per-iteration launch latency.  Phases of an iteration:
+//   [push F->O  or  pull F->O]  barrier  [copy prev / clear old F]  barrier
+// A push writes O's degree-binned list and bitmap; a pull writes O's bitmap
+// (the list is built by a conversion phase only when a push follows).
+//
+// Coherence: data written during the launch (values, frontiers, counters,
+// candidate lists) are read with ld.global.cg (L2), never through the
+// non-coherent L1; the read-only graph uses the read-only path.
+//
+// The grid barrier is the kernel's only wait.  It is bounded by a
+// %globaltimer deadline (timeout_ns); a CTA that gives up sets
+// DEV_ERR_TIMEOUT in the state block and every CTA returns at its next
+// barrier check, so the host sees GG_ERR_TIMEOUT and the context stays
+// usable.  Co-residency of all CTAs is guaranteed by the cooperative launch.
+#include <climits>
+#include <cuda_bf16.h>
+
+#include <cstring>
+#include <type_traits>
+
+#include "gg_internal.cuh"
+#include "gg_mlp.cuh"
+
+namespace gg {
+
+constexpr unsigned FULLP = 0xffffffffu;
+constexpr int kPB = 256;           // threads per CTA
+constexpr uint32_t kLargeScan = 1024;  // large-bin rows chunked when at most this many
+
+struct PFront {
+    uint32_t *bins[NBINS];
+    uint32_t *bitmap;
+    unsigned long long *cnt;  // FC_WORDS
+};
+
+struct PState {
+    unsigned int bar_count;
+    unsigned int bar_gen;
+    unsigned int err;
+    int iterations;
+    int has_list[2];
+    int all[2];
+    unsigned long long cand_n[2];
+    int cand_valid;
+    int cand_cur;
+    int variant[GG_MAX_ITERS];
+    unsigned long long nactv[GG_MAX_ITERS];
+    unsigned long long nacte[GG_MAX_ITERS];
+    unsigned long long scanned[GG_MAX_ITERS];
+    unsigned long long t_ns[GG_MAX_ITERS + 1];
+    unsigned long long reached_v, reached_e;
+};
+
+struct PArgs {
+    const uint64_t *off, *in_off;
+    const uint32_t *adj, *in_adj;
+    uint32_t n;
+    uint64_t m;
+    PFront fr[2];
+    uint32_t *cand[2];
+    const uint32_t *nonisolated;
+    const unsigned long long *nonisolated_n;
+    void *a, *prev;
+    int relax, record, filter, level_k, level_sync;
+    int64_t fk;
+    int threshold, threshold_k, variant;
+    uint32_t smax, mmax, large_ch;
+    int K;
+    int max_iters;
+    unsigned long long timeout_ns;
+    PState *st;
+    unsigned long long *merge;         // merge-path scratch: list length + CTA count
+    const __nv_bfloat16 *sel_w;        // learned selector weights (bfloat16), or null
+    float gini;
+    int force_iter, force_variant;     // timing collection: one forced (iteration, variant)
+};
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <typename T> __device__ __forceinline__ T ldcg(const T *p) { return __ldcg(p); }
+
+// Bounded grid barrier (sense = generation counter).  Returns false when any
+// CTA has flagged an error (timeout): the caller then returns.
+__device__ __forceinline__ bool grid_barrier(PState *st, unsigned long long timeout_ns) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        volatile unsigned int *genp = &st->bar_gen;
+        const unsigned int gen = *genp;
+        if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+            atomicExch(&st->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&st->bar_gen, 1u);
+        } else {
+            const unsigned long long t0 = globaltimer();
+            while (*genp == gen) {
+                if (globaltimer() - t0 > timeout_ns) {
+                    atomicOr(&st->err, DEV_ERR_TIMEOUT);
+                    break;
+                }
+                if (*(volatile unsigned int *)&st->err) break;
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *(volatile unsigned int *)&st->err == 0;
+}
+
+// ---- relax semantics (same table as the host-driven kernels) --------------
+template <int R> struct POp {
+    using V = typename std::conditional<R == GG_RELAX_MIN_PLUS1_I32, int32_t, uint32_t>::type;
+    V *a, *prev;
+    int filter;
+    int64_t fk;
+    int level_sync;
+    __device__ __forceinline__ static V none() {
+        if constexpr (R == GG_RELAX_MIN_PLUS1_I32) return INT_MAX;
+        else return 0xFFFFFFFFu;
+    }
+    __device__ __forceinline__ V load(uint32_t v) const { return ldcg(a + v); }
+    __device__ __forceinline__ bool dst_ok(V cur) const {
+        switch (filter) {
+        case GG_FILTER_GT_CONST: return (int64_t)cur > fk;
+        case GG_FILTER_NE_ZERO: return cur != 0;
+        case GG_FILTER_MSB_SET: return ((uint32_t)cur >> 31) != 0;
+        default: return true;
+        }
+    }
+    __device__ __forceinline__ V src_val(uint32_t s) const {
+        if constexpr (R == GG_RELAX_MIN_PLUS1_I32) return level_sync ? (V)fk : ldcg(a + s) + 1;
+        else if constexpr (R == GG_RELAX_MIN_U32) return ldcg(a + s);
+        else return (V)s;
+    }
+    __device__ __forceinline__ bool better(V x, V best) const {
+        if constexpr (R == GG_RELAX_SETIF_U32) return ((uint32_t)best >> 31) != 0;
+        else return x < best;
+    }
+    __device__ __forceinline__ V warp_pick(bool ok, V x, unsigned okm) const {
+        if constexpr (R == GG_RELAX_SETIF_U32) return __shfl_sync(FULLP, x, __ffs(okm) - 1);
+        else return __reduce_min_sync(FULLP, ok ? x : none());
+    }
+    // push: true iff this thread records d (first change away from prev)
+    __device__ __forceinline__ bool offer(uint32_t d, V sv, int record) const {
+        V cur = ldcg(a + d);
+        if (!dst_ok(cur)) return false;
+        V old;
+        if constexpr (R == GG_RELAX_SETIF_U32) {
+            if (((uint32_t)cur >> 31) == 0) return false;
+            old = atomicCAS(a + d, cur, sv);
+            if (old != cur) return false;
+        } else {
+            if (!(sv < cur)) return false;
+            old = atomicMin(a + d, sv);
+            if (!(sv < old)) return false;
+        }
+        return record == GG_RECORD_NE_PREV ? old == ldcg(prev + d) : true;
+    }
+};
+
+__device__ __forceinline__ bool bit_cg(const uint32_t *bm, uint32_t v) {
+    return (ldcg(bm + (v >> 5)) >> (v & 31u)) & 1u;
+}
+
+// warp-aggregated append into O's degree bins + bitmap bit + counts
+__device__ __forceinline__ void p_emit(const PArgs &P, const PFront &O, bool rec, uint32_t d,
+                                       unsigned long long &nv, unsigned long long &ne) {
+    uint64_t deg = 0;
+    if (rec) {
+        deg = P.off[d + 1] - P.off[d];
+        nv++;
+        ne += deg;
+        atomicOr(O.bitmap + (d >> 5), 1u << (d & 31));
+    }
+    const uint32_t bin = deg <= P.smax ? 0u : (deg <= P.mmax ? 1u : 2u);
+    const unsigned am = __activemask();
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (uint32_t b = 0; b < NBINS; ++b) {
+        const unsigned mk = __ballot_sync(am, rec && bin == b);
+        if (mk == 0) continue;
+        const int leader = __ffs(mk) - 1;
+        unsigned long long base = 0;
+        if ((int)lane == leader) base = atomicAdd(O.cnt + FC_BIN0 + b, (unsigned long long)__popc(mk));
+        base = __shfl_sync(am, base, leader);
+        if (rec && bin == b) O.bins[b][base + __popc(mk & ((1u << lane) - 1u))] = d;
+    }
+}
+
+__device__ __forceinline__ void p_flush(const PFront &O, unsigned long long nv, unsigned long long ne,
+                                        unsigned long long sc) {
+    nv = dev::block_sum<unsigned long long, kPB>(nv);
+    ne = dev::block_sum<unsigned long long, kPB>(ne);
+    sc = dev::block_sum<unsigned long long, kPB>(sc);
+    if (threadIdx.x == 0) {
+        if (nv) atomicAdd(O.cnt + FC_NACTV, nv);
+        if (ne) atomicAdd(O.cnt + FC_NACTE, ne);
+        if (sc) atomicAdd(O.cnt + FC_SCANNED, sc);
+    }
+}
+
+// ---- sparse push F -> O ------------------------------------------------------
+// One shared buffer serves all phases (they never overlap in time).
+constexpr int kSmemWords = 3 * (kPB / 32) * 256;  // 24 KiB
+
+template <int R>
+__device__ void phase_push(const PArgs &P, const POp<R> &op, const PFront &F, const PFront &O,
+                           uint32_t *smem) {
+    using V = typename POp<R>::V;
+    unsigned long long *s_first = reinterpret_cast<unsigned long long *>(smem);  // kLargeScan + 1
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t c0 = (uint32_t)ldcg(F.cnt + FC_BIN0), c1 = (uint32_t)ldcg(F.cnt + FC_BIN1),
+                   c2 = (uint32_t)ldcg(F.cnt + FC_BIN2);
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    // large bin: rows cut into chunks (chunk table built per CTA in shared memory)
+    if (c2 && c2 <= kLargeScan) {
+        for (uint32_t i = threadIdx.x; i < c2; i += kPB) {
+            const uint32_t v = ldcg(F.bins[2] + i);
+            s_first[i + 1] = (P.off[v + 1] - P.off[v] + P.large_ch - 1) / P.large_ch;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_first[0] = 0;
+            for (uint32_t i = 1; i <= c2; ++i) s_first[i] += s_first[i - 1];
+        }
+        __syncthreads();
+        const unsigned long long nch = s_first[c2];
+        for (unsigned long long c = blockIdx.x; c < nch; c += gridDim.x) {
+            uint32_t lo = 0, hi = c2;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (s_first[mid] <= c) lo = mid; else hi = mid;
+            }
+            const uint32_t s = ldcg(F.bins[2] + lo);
+            const V sv = op.src_val(s);
+            const uint64_t beg = P.off[s] + (c - s_first[lo]) * P.large_ch;
+            const uint64_t end = min(beg + P.large_ch, P.off[s + 1]);
+            if (threadIdx.x == 0) sc += end - beg;
+            for (uint64_t base = beg; base < end; base += kPB) {
+                const uint64_t e = base + threadIdx.x;
+                bool rec = false;
+                uint32_t d = 0;
+                if (e < end) {
+                    d = __ldg(P.adj + e);
+                    rec = op.offer(d, sv, P.record);
+                }
+                p_emit(P, O, rec, d, nv, ne);
+            }
+        }
+    } else if (c2) {
+        for (uint32_t i = blockIdx.x; i < c2; i += gridDim.x) {  // a CTA per row
+            const uint32_t s = ldcg(F.bins[2] + i);
+            const V sv = op.src_val(s);
+            const uint64_t beg = P.off[s], end = P.off[s + 1];
+            if (threadIdx.x == 0) sc += end - beg;
+            for (uint64_t base = beg; base < end; base += kPB) {
+                const uint64_t e = base + threadIdx.x;
+                bool rec = false;
+                uint32_t d = 0;
+                if (e < end) {
+                    d = __ldg(P.adj + e);
+                    rec = op.offer(d, sv, P.record);
+                }
+                p_emit(P, O, rec, d, nv, ne);
+            }
+        }
+    }
+    // medium bin: a warp per row
+    const uint64_t gw = ((uint64_t)blockIdx.x * kPB + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * kPB) >> 5;
+    for (uint64_t i = gw; i < c1; i += nw) {
+        const uint32_t s = ldcg(F.bins[1] + i);
+        const V sv = op.src_val(s);
+        const uint64_t beg = P.off[s], end = P.off[s + 1];
+        if (lane == 0) sc += end - beg;
+        for (uint64_t base = beg; base < end; base += 32) {
+            const uint64_t e = base + lane;
+            bool rec = false;
+            uint32_t d = 0;
+            if (e < end) {
+                d = __ldg(P.adj + e);
+                rec = op.offer(d, sv, P.record);
+            }
+            p_emit(P, O, rec, d, nv, ne);
+        }
+    }
+    // small bin: a thread per row, warp-uniform edge loop
+    for (uint64_t base = gw * 32; base < c0; base += nw * 32) {
+        const uint64_t i = base + lane;
+        const bool have = i < c0;
+        uint32_t s = 0;
+        uint64_t beg = 0, end = 0;
+        V sv = POp<R>::none();
+        if (have) {
+            s = ldcg(F.bins[0] + i);
+            beg = P.off[s];
+            end = P.off[s + 1];
+            sv = op.src_val(s);
+        }
+        const uint32_t deg = (uint32_t)(end - beg);
+        sc += deg;
+        const uint32_t maxd = __reduce_max_sync(FULLP, deg);
+        for (uint32_t k = 0; k < maxd; ++k) {
+            bool rec = false;
+            uint32_t d = 0;
+            if (k < deg) {
+                d = __ldg(P.adj + beg + k);
+                rec = op.offer(d, sv, P.record);
+            }
+            p_emit(P, O, rec, d, nv, ne);
+        }
+    }
+    p_flush(O, nv, ne, sc);
+}
+
+// ---- dense pull F -> O over a candidate list -------------------------------
+template <int R, bool SRCF>
+__device__ void phase_pull(const PArgs &P, const POp<R> &op, const PFront &F, const PFront &O,
+                           const uint32_t *cand, unsigned long long ncand, uint32_t *cand_out,
+                           unsigned long long *cand_out_n, uint32_t *smem) {
+    using V = typename POp<R>::V;
+    const uint32_t lane = threadIdx.x & 31u;
+    dev::WarpAppender<256> keepers{smem + (threadIdx.x >> 5) * 256, 0, cand_out, cand_out_n};
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    const uint64_t nw = ((uint64_t)gridDim.x * kPB) >> 5;
+    for (uint64_t w = ((uint64_t)blockIdx.x * kPB + threadIdx.x) >> 5; (w << 5) < ncand; w += nw) {
+        const uint64_t item = (w << 5) + lane;
+        const bool valid = item < ncand;
+        const uint32_t d = valid ? ldcg(cand + item) : 0u;
+        V best = POp<R>::none();
+        uint64_t e = 0, end = 0;
+        if (valid) {
+            best = op.load(d);
+            e = P.in_off[d];
+            end = P.in_off[d + 1];
+        }
+        bool act = valid && op.dst_ok(best);
+        bool changed = false;
+        const uint64_t beg = e;
+        const uint64_t lim = min(end, e + (uint64_t)P.K);
+        while (act && e < lim) {
+            const int cnt = (int)min((uint64_t)4, lim - e);
+            uint32_t sv[4];
+            bool inF[4];
+            V xv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) sv[j] = j < cnt ? __ldg(P.in_adj + e + j) : 0u;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                inF[j] = j < cnt && (!SRCF || bit_cg(F.bitmap, sv[j]));
+                xv[j] = j < cnt ? op.src_val(sv[j]) : POp<R>::none();
+            }
+            int used = cnt;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (j < cnt && act && inF[j] && op.better(xv[j], best)) {
+                    best = xv[j];
+                    changed = true;
+                    if (!op.dst_ok(best)) {
+                        act = false;
+                        used = j + 1;
+                    }
+                }
+            }
+            e += used;
+        }
+        sc += e - beg;
+        unsigned pend = __ballot_sync(FULLP, act && e < end);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint64_t ej = __shfl_sync(FULLP, e, j);
+            const uint64_t endj = __shfl_sync(FULLP, end, j);
+            V bj = __shfl_sync(FULLP, best, j);
+            bool chj = false, actj = true;
+            for (uint64_t base = ej; base < endj; base += 32) {
+                const uint64_t idx = base + lane;
+                bool ok = false;
+                V x = POp<R>::none();
+                if (idx < endj) {
+                    const uint32_t s = __ldg(P.in_adj + idx);
+                    if (!SRCF || bit_cg(F.bitmap, s)) {
+                        x = op.src_val(s);
+                        ok = op.better(x, bj);
+                    }
+                }
+                if (lane == 0) sc += min((uint64_t)32, endj - base);
+                const unsigned okm = __ballot_sync(FULLP, ok);
+                if (okm) {
+                    bj = op.warp_pick(ok, x, okm);
+                    chj = true;
+                    if (!op.dst_ok(bj)) {
+                        actj = false;
+                        break;
+                    }
+                }
+            }
+            if ((int)lane == j) {
+                best = bj;
+                changed = changed || chj;
+                act = actj;
+            }
+        }
+        bool rec = false;
+        if (changed) {
+            op.a[d] = best;
+            if (P.record == GG_RECORD_NE_PREV) {
+                if (best != ldcg(op.prev + d)) {
+                    op.prev[d] = best;
+                    rec = true;
+                }
+            } else if (P.record == GG_RECORD_REDUCTION) {
+                rec = true;
+            }
+        }
+        // O bitmap: one atomicOr per distinct word of the warp
+        unsigned todo = __ballot_sync(FULLP, rec);
+        while (todo) {
+            const int leader = __ffs(todo) - 1;
+            const uint32_t w0 = __shfl_sync(FULLP, d >> 5, leader);
+            const bool mine = rec && (d >> 5) == w0;
+            const unsigned bits = __reduce_or_sync(FULLP, mine ? (1u << (d & 31)) : 0u);
+            if ((int)lane == leader) atomicOr(O.bitmap + w0, bits);
+            todo &= ~__ballot_sync(FULLP, mine);
+        }
+        if (rec) {
+            nv++;
+            ne += P.off[d + 1] - P.off[d];
+        }
+        keepers.push(valid && act && end > beg, d);
+    }
+    keepers.flush();
+    p_flush(O, nv, ne, sc);
+}
+
+// F's bitmap -> F's binned list (only before a push that follows a pull)
+__device__ void phase_bitmap_to_list(const PArgs &P, const PFront &F, uint32_t *smem) {
+    const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    constexpr int per = (kPB / 32) * 256;
+    dev::WarpAppender<256> ap0{smem + 0 * per + wib * 256, 0, F.bins[0], F.cnt + FC_BIN0};
+    dev::WarpAppender<256> ap1{smem + 1 * per + wib * 256, 0, F.bins[1], F.cnt + FC_BIN1};
+    dev::WarpAppender<256> ap2{smem + 2 * per + wib * 256, 0, F.bins[2], F.cnt + FC_BIN2};
+    const uint32_t nwords = (P.n + 31) / 32;
+    const uint64_t nw = ((uint64_t)gridDim.x * kPB) >> 5;
+    for (uint64_t w = ((uint64_t)blockIdx.x * kPB + threadIdx.x) >> 5; w < nwords; w += nw) {
+        const uint32_t word = ldcg(F.bitmap + w);
+        if (word == 0) continue;
+        const uint32_t v = (uint32_t)w * 32 + lane;
+        const bool act = v < P.n && ((word >> lane) & 1u);
+        const uint64_t deg = act ? P.off[v + 1] - P.off[v] : 0;
+        const uint32_t bin = deg <= P.smax ? 0 : (deg <= P.mmax ? 1 : 2);
+        ap0.push(act && bin == 0, v);
+        ap1.push(act && bin == 1, v);
+        ap2.push(act && bin == 2, v);
+    }
+    ap0.flush();
+    ap1.flush();
+    ap2.flush();
+}
+
+// ---- dense push from F's bitmap ----------------------------------------------
+template <int R>
+__device__ void phase_push_dense(const PArgs &P, const POp<R> &op, const PFront &F, const PFront &O, bool all) {
+    using V = typename POp<R>::V;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwords = (P.n + 31) / 32;
+    const uint64_t nw = ((uint64_t)gridDim.x * kPB) >> 5;
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    for (uint64_t w = ((uint64_t)blockIdx.x * kPB + threadIdx.x) >> 5; w < nwords; w += nw) {
+        const uint32_t word = all ? 0xFFFFFFFFu : ldcg(F.bitmap + w);
+        if (word == 0) continue;  // warp-uniform
+        const uint32_t s = (uint32_t)w * 32 + lane;
+        const bool act = s < P.n && ((word >> lane) & 1u);
+        uint64_t beg = 0, end = 0;
+        V sv = POp<R>::none();
+        if (act) {
+            beg = P.off[s];
+            end = P.off[s + 1];
+            sv = op.src_val(s);
+        }
+        const uint32_t k1 = (uint32_t)min(end - beg, (uint64_t)P.K);
+        const uint32_t maxk = __reduce_max_sync(FULLP, k1);
+        for (uint32_t k = 0; k < maxk; ++k) {
+            bool rec = false;
+            uint32_t d = 0;
+            if (k < k1) {
+                d = __ldg(P.adj + beg + k);
+                rec = op.offer(d, sv, P.record);
+            }
+            p_emit(P, O, rec, d, nv, ne);
+        }
+        sc += k1;
+        unsigned pend = __ballot_sync(FULLP, act && beg + k1 < end);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint64_t ej = __shfl_sync(FULLP, beg + k1, j), endj = __shfl_sync(FULLP, end, j);
+            const V svj = __shfl_sync(FULLP, sv, j);
+            if (lane == 0) sc += endj - ej;
+            for (uint64_t base = ej; base < endj; base += 32) {
+                const uint64_t e = base + lane;
+                bool rec = false;
+                uint32_t d = 0;
+                if (e < endj) {
+                    d = __ldg(P.adj + e);
+                    rec = op.offer(d, svj, P.record);
+                }
+                p_emit(P, O, rec, d, nv, ne);
+            }
+        }
+    }
+    p_flush(O, nv, ne, sc);
+}
+
+// ---- edge-balanced ("merge path") push ---------------------------------------
+// Rows of F's list are cut into chunks of kMergeCh edges; a device-wide scan
+// of the chunk counts (M1 per-CTA slice sums, M2 slice prefixes) lets every
+// warp take equal chunk ranges in M3 and find each chunk's row by binary
+// search.  Uses the scratch array P.merge (list length + CTA count entries).
+constexpr uint32_t kMergeCh = 64;
+
+__device__ __forceinline__ uint32_t list_at(const PFront &F, uint64_t i, uint64_t c0, uint64_t c1) {
+    return i < c0 ? ldcg(F.bins[0] + i) : (i < c0 + c1 ? ldcg(F.bins[1] + i - c0) : ldcg(F.bins[2] + i - c0 - c1));
+}
+
+__device__ void phase_merge_count(const PArgs &P, const PFront &F) {
+    const uint64_t c0 = ldcg(F.cnt + FC_BIN0), c1 = ldcg(F.cnt + FC_BIN1), c2 = ldcg(F.cnt + FC_BIN2);
+    const uint64_t L = c0 + c1 + c2, G = gridDim.x;
+    const uint64_t lo = L * blockIdx.x / G, hi = L * (blockIdx.x + 1) / G;
+    unsigned long long sum = 0;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += kPB) {
+        const uint32_t v = list_at(F, i, c0, c1);
+        const unsigned long long ch = (P.off[v + 1] - P.off[v] + kMergeCh - 1) / kMergeCh;
+        P.merge[i] = ch;
+        sum += ch;
+    }
+    sum = dev::block_sum<unsigned long long, kPB>(sum);
+    if (threadIdx.x == 0) P.merge[L + blockIdx.x] = sum;
+}
+
+// Block-wide exclusive scan of one value per thread (kPB threads).
+__device__ __forceinline__ unsigned long long block_exclusive_scan(unsigned long long x, unsigned long long *total) {
+    __shared__ unsigned long long s_w[kPB / 32];
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    unsigned long long inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long t = __shfl_up_sync(FULLP, inc, o);
+        if (lane >= (uint32_t)o) inc += t;
+    }
+    if (lane == 31) s_w[wid] = inc;
+    __syncthreads();
+    unsigned long long wbase = 0, tot = 0;
+    for (int w = 0; w < kPB / 32; ++w) {
+        if (w < (int)wid) wbase += s_w[w];
+        tot += s_w[w];
+    }
+    __syncthreads();
+    *total = tot;
+    return wbase + inc - x;
+}
+
+__device__ void phase_merge_scan(const PArgs &P, const PFront &F) {
+    const uint64_t c0 = ldcg(F.cnt + FC_BIN0), c1 = ldcg(F.cnt + FC_BIN1), c2 = ldcg(F.cnt + FC_BIN2);
+    const uint64_t L = c0 + c1 + c2, G = gridDim.x;
+    const uint64_t lo = L * blockIdx.x / G, hi = L * (blockIdx.x + 1) / G;
+    // offset of this CTA's slice: sum of the earlier CTAs' slice sums
+    unsigned long long o = 0;
+    for (uint64_t b = threadIdx.x; b < blockIdx.x; b += kPB) o += ldcg(P.merge + L + b);
+    o = dev::block_sum<unsigned long long, kPB>(o);
+    __shared__ unsigned long long s_run;
+    if (threadIdx.x == 0) s_run = o;
+    __syncthreads();
+    // exclusive prefix of the slice, kPB entries at a time, in place
+    for (uint64_t base = lo; base < hi; base += kPB) {
+        const uint64_t i = base + threadIdx.x;
+        const unsigned long long c = i < hi ? ldcg(P.merge + i) : 0ull;
+        unsigned long long tot;
+        const unsigned long long ex = block_exclusive_scan(c, &tot);
+        const unsigned long long run = s_run;
+        if (i < hi) P.merge[i] = run + ex;
+        __syncthreads();
+        if (threadIdx.x == 0) s_run = run + tot;
+        __syncthreads();
+    }
+}
+
+template <int R>
+__device__ void phase_merge_push(const PArgs &P, const POp<R> &op, const PFront &F, const PFront &O) {
+    using V = typename POp<R>::V;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t c0 = ldcg(F.cnt + FC_BIN0), c1 = ldcg(F.cnt + FC_BIN1), c2 = ldcg(F.cnt + FC_BIN2);
+    const uint64_t L = c0 + c1 + c2, G = gridDim.x;
+    __shared__ unsigned long long s_total;
+    unsigned long long part = 0;
+    for (uint64_t b = threadIdx.x; b < G; b += kPB) part += ldcg(P.merge + L + b);
+    part = dev::block_sum<unsigned long long, kPB>(part);
+    if (threadIdx.x == 0) s_total = part;
+    __syncthreads();
+    const unsigned long long total = s_total;
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    const uint64_t nw = ((uint64_t)G * kPB) >> 5;
+    for (uint64_t c = ((uint64_t)blockIdx.x * kPB + threadIdx.x) >> 5; c < total; c += nw) {
+        uint64_t a = 0, b = L;  // last row i with prefix[i] <= c
+        while (b - a > 1) {
+            const uint64_t mid = (a + b) >> 1;
+            if (ldcg(P.merge + mid) <= c) a = mid; else b = mid;
+        }
+        const uint32_t s = list_at(F, a, c0, c1);
+        const V sv = op.src_val(s);
+        const uint64_t beg = P.off[s] + (c - ldcg(P.merge + a)) * kMergeCh;
+        const uint64_t end = min(beg + kMergeCh, P.off[s + 1]);
+        if (lane == 0) sc += end - beg;
+        for (uint64_t base = beg; base < end; base += 32) {
+            const uint64_t e = base + lane;
+            bool rec = false;
+            uint32_t d = 0;
+            if (e < end) {
+                d = __ldg(P.adj + e);
+                rec = op.offer(d, sv, P.record);
+            }
+            p_emit(P, O, rec, d, nv, ne);
+        }
+    }
+    p_flush(O, nv, ne, sc);
+}
+
+// Threshold / fixed / learned choice; identical in every CTA (same inputs,
+// same arithmetic).  Returns a gg_variant.
+__device__ int choose_variant(const PArgs &P, int iter, unsigned long long nactv, unsigned long long nacte,
+                              bool f_all, const PState *st, int *s_choice) {
+    if (f_all) return GG_VAR_PULL_DENSE;
+    if (iter == P.force_iter) return P.force_variant;
+    if (P.variant >= 0) return P.variant;
+    switch (P.threshold) {
+    case GG_THRESH_ALWAYS_SPARSE: return GG_VAR_PUSH_SPARSE;
+    case GG_THRESH_ALWAYS_DENSE: return GG_VAR_PULL_DENSE;
+    case GG_THRESH_FRAC:
+        return (float)(nactv + nacte) <= (float)P.m / (float)(100.0 / (float)P.threshold_k) ? GG_VAR_PUSH_SPARSE
+                                                                                            : GG_VAR_PULL_DENSE;
+    case GG_THRESH_LEARNED:
+        if (P.sel_w) {
+            // warp 0 evaluates the network, the CTA reads its choice
+            if (threadIdx.x < 32) {
+                const double n = P.n, m = (double)P.m, fv = (double)nactv, fe = (double)nacte;
+                const double unr = n - (double)ldcg(&st->reached_v);
+                float x[GG_SEL_FEATURES];
+                x[0] = (float)(log2(1.0 + fv) / 32);
+                x[1] = (float)(log2(1.0 + fe) / 40);
+                x[2] = (float)(log2(1.0 + (unr > 0 ? unr : 0)) / 32);
+                x[3] = (float)(min(iter, 255) / 64.0);
+                x[4] = (float)(log2(1.0 + (n > 0 ? m / n : 0)) / 8);
+                x[5] = P.gini;
+                x[6] = (float)(n > 0 ? fv / n : 0);
+                x[7] = (float)(m > 0 ? fe / m : 0);
+                x[8] = (float)fmin(4.0, m > 0 ? (fv + fe) / m : 0.0);
+                x[9] = (float)(log2(n > 1 ? n : 1.0) / 32);
+                float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
+                mlp::warp_forward(P.sel_w, x, o, z1, a1, z2, a2);
+                int best = 0;
+                for (int v = 1; v < GG_SEL_VARIANTS; ++v)
+                    if (o[v] < o[best]) best = v;
+                if (threadIdx.x == 0) *s_choice = best;
+            }
+            __syncthreads();
+            const int c = *s_choice;
+            __syncthreads();
+            return c;
+        }
+        // no network attached: the default threshold
+    default:
+        return (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
+    __shared__ __align__(16) uint32_t smem[kSmemWords];
+    __shared__ int s_choice;
+    static_assert(kSmemWords * 4 >= (kLargeScan + 1) * 8, "chunk table fits the shared buffer");
+    PState *st = P.st;
+    POp<R> op;
+    op.a = (typename POp<R>::V *)P.a;
+    op.prev = (typename POp<R>::V *)P.prev;
+    op.filter = P.filter;
+    op.fk = P.fk;
+    op.level_sync = P.level_sync;
+    const uint64_t tid = (uint64_t)blockIdx.x * kPB + threadIdx.x;
+    const uint64_t nthreads = (uint64_t)gridDim.x * kPB;
+    int cur = 0;
+    int iter = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->t_ns[0] = globaltimer();
+    for (; iter < P.max_iters; ++iter) {
+        const PFront F = P.fr[cur], O = P.fr[cur ^ 1];
+        const unsigned long long nactv = ldcg(F.cnt + FC_NACTV), nacte = ldcg(F.cnt + FC_NACTE);
+        const int f_all = ldcg(&st->all[cur]);
+        if (nactv == 0 && !f_all) break;
+        if (P.level_k) op.fk = iter + 1;
+        const int var = choose_variant(P, iter, nactv, nacte, f_all != 0, st, &s_choice);
+        const bool pushes = var != GG_VAR_PULL_DENSE;
+        if (blockIdx.x == 0 && threadIdx.x == 0 && iter < GG_MAX_ITERS) {
+            st->variant[iter] = var;
+            st->nactv[iter] = nactv;
+            st->nacte[iter] = nacte;
+        }
+        if (var == GG_VAR_PUSH_SPARSE || var == GG_VAR_PUSH_MERGE) {
+            if (!ldcg(&st->has_list[cur])) {
+                __syncthreads();
+                phase_bitmap_to_list(P, F, smem);
+                if (!grid_barrier(st, P.timeout_ns)) return;
+            }
+            __syncthreads();
+            if (var == GG_VAR_PUSH_SPARSE) {
+                phase_push<R>(P, op, F, O, smem);
+            } else {
+                phase_merge_count(P, F);
+                if (!grid_barrier(st, P.timeout_ns)) return;
+                phase_merge_scan(P, F);
+                if (!grid_barrier(st, P.timeout_ns)) return;
+                phase_merge_push<R>(P, op, F, O);
+            }
+        } else if (var == GG_VAR_PUSH_DENSE) {
+            __syncthreads();
+            phase_push_dense<R>(P, op, F, O, f_all != 0);
+        } else {
+            const int cc = ldcg(&st->cand_cur);
+            const bool cv = ldcg(&st->cand_valid) != 0;
+            const uint32_t *cin = cv ? P.cand[cc] : P.nonisolated;
+            const unsigned long long nin = cv ? ldcg(&st->cand_n[cc]) : ldcg(P.nonisolated_n);
+            __syncthreads();
+            if (f_all)
+                phase_pull<R, false>(P, op, F, O, cin, nin, P.cand[cc ^ 1], &st->cand_n[cc ^ 1], smem);
+            else
+                phase_pull<R, true>(P, op, F, O, cin, nin, P.cand[cc ^ 1], &st->cand_n[cc ^ 1], smem);
+        }
+        if (!grid_barrier(st, P.timeout_ns)) return;
+        // post: maintain copies for a push, recycle the old frontier as next output
+        if (pushes && P.record == GG_RECORD_NE_PREV) {
+            const unsigned long long b0 = ldcg(O.cnt + FC_BIN0), b1 = ldcg(O.cnt + FC_BIN1),
+                                     b2 = ldcg(O.cnt + FC_BIN2);
+            for (uint64_t i = tid; i < b0 + b1 + b2; i += nthreads) {
+                const uint32_t v = i < b0 ? ldcg(O.bins[0] + i)
+                                          : (i < b0 + b1 ? ldcg(O.bins[1] + i - b0) : ldcg(O.bins[2] + i - b0 - b1));
+                if (P.relax == GG_RELAX_MIN_PLUS1_I32) ((int32_t *)P.prev)[v] = ldcg((int32_t *)P.a + v);
+                else ((uint32_t *)P.prev)[v] = ldcg((uint32_t *)P.a + v);
+            }
+        }
+        const uint32_t nwords = (P.n + 31) / 32;
+        for (uint64_t w = tid; w < nwords; w += nthreads) F.bitmap[w] = 0u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            // decision inputs change only here, between the two barriers, so
+            // every CTA's next choice reads the same values
+            st->reached_v += nactv;
+            st->reached_e += nacte;
+            for (int i = 0; i < FC_WORDS; ++i) F.cnt[i] = 0;
+            st->has_list[cur ^ 1] = pushes ? 1 : 0;
+            st->all[cur] = 0;
+            st->all[cur ^ 1] = 0;
+            if (!pushes) {
+                st->cand_valid = 1;
+                st->cand_n[ldcg(&st->cand_cur)] = 0;
+                st->cand_cur ^= 1;
+            }
+            if (iter < GG_MAX_ITERS) {
+                st->scanned[iter] = ldcg(O.cnt + FC_SCANNED);
+                st->t_ns[iter + 1] = globaltimer();
+            }
+        }
+        if (!grid_barrier(st, P.timeout_ns)) return;
+        cur ^= 1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->iterations = iter;
+}
+
+__global__ void k_traverse_init(PFront F, uint32_t root, const uint64_t *off, uint32_t smax, uint32_t mmax,
+                                int single) {
+    if (single) {
+        const uint64_t deg = off[root + 1] - off[root];
+        const int b = deg <= smax ? 0 : (deg <= mmax ? 1 : 2);
+        F.bins[b][0] = root;
+        F.cnt[FC_BIN0 + b] = 1;
+        F.cnt[FC_NACTV] = 1;
+        F.cnt[FC_NACTE] = deg;
+        F.bitmap[root >> 5] |= 1u << (root & 31);
+    }
+}
+
+// Host side -----------------------------------------------------------------
+template <int R>
+static const void *traverse_kernel() { return (const void *)k_traverse<R>; }
+
+const void *selector_weights(gg_graph *g);
+
+gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, bool start_all, uint32_t root,
+                              const gg_run_opts &opt, gg_run_stats *stats, int *iters_out, int force_iter,
+                              int force_variant) {
+    gg_ctx *ctx = g->ctx;
+    cudaStream_t s = ctx->stream;
+    const Tuning &t = tuning();
+    // buffers: the graph's two scratch frontiers, candidate lists, state block
+    for (auto &f : g->tmp_front)
+        if (!f) GG_CHECK(gg_frontier_create(g, &f));
+    for (auto *f : g->tmp_front) {
+        GG_CHECK(frontier_alloc_bins(f));
+        GG_CHECK(frontier_alloc_bitmap(f));
+    }
+    CandLists &c = g->cand;
+    if (!c.list[0]) {
+        for (auto &l : c.list) GG_CUDA(ctx, cudaMalloc(&l, ((size_t)g->n + 1) * 4));
+        GG_CUDA(ctx, cudaMalloc(&c.cnt, 2 * sizeof(uint64_t)));
+    }
+    if (!g->pstate) GG_CUDA(ctx, cudaMalloc(&g->pstate, sizeof(PState)));
+    PState *st = (PState *)g->pstate;
+    const size_t words = ((size_t)g->n + 31) / 32 + 1;
+    PArgs P;
+    std::memset(&P, 0, sizeof(P));
+    P.off = g->off;
+    P.adj = g->adj;
+    P.in_off = g->in_off;
+    P.in_adj = g->in_adj;
+    P.n = g->n;
+    P.m = g->m;
+    for (int i = 0; i < 2; ++i) {
+        gg_frontier *f = g->tmp_front[i];
+        for (int b = 0; b < NBINS; ++b) P.fr[i].bins[b] = f->bins[b];
+        P.fr[i].bitmap = f->bitmap;
+        P.fr[i].cnt = (unsigned long long *)f->d_cnt;
+        GG_CUDA(ctx, cudaMemsetAsync(f->bitmap, 0, words * 4, s));
+        GG_CUDA(ctx, cudaMemsetAsync(f->d_cnt, 0, FC_WORDS * 8, s));
+        f->host_valid = false;
+        f->has_list = f->has_bitmap = f->all = false;
+    }
+    P.cand[0] = c.list[0];
+    P.cand[1] = c.list[1];
+    P.nonisolated = g->nonisolated;
+    P.nonisolated_n = (const unsigned long long *)g->nonisolated_n;
+    P.a = d.a->d;
+    P.prev = d.prev ? d.prev->d : nullptr;
+    P.relax = d.relax;
+    P.record = d.record;
+    P.filter = d.dst_filter;
+    P.level_k = level_k;
+    P.level_sync = (d.src_level_sync && d.dst_filter == GG_FILTER_GT_CONST) ? 1 : 0;
+    P.fk = d.dst_filter_k;
+    P.threshold = opt.threshold;
+    P.threshold_k = opt.threshold_k;
+    P.variant = opt.variant;
+    P.smax = t.bin_small_max;
+    P.mmax = t.bin_medium_max;
+    P.large_ch = t.large_chunk;
+    P.K = t.pull_k;
+    P.max_iters = (int)std::min<uint64_t>((uint64_t)g->n + 2, (uint64_t)INT_MAX / 2);
+    P.timeout_ns = t.barrier_timeout_ns;
+    P.st = st;
+    P.force_iter = force_iter >= 0 ? force_iter : g->force_iter;
+    P.force_variant = force_iter >= 0 ? force_variant : g->force_variant;
+    P.sel_w = (const __nv_bfloat16 *)selector_weights(g);
+    P.gini = g->gini < 0 ? 0.0f : g->gini;
+    if (opt.threshold == GG_THRESH_LEARNED && P.sel_w && g->gini < 0) {
+        float gi;
+        GG_CHECK(graph_gini(g, &gi));
+        P.gini = gi;
+    }
+    GG_CUDA(ctx, cudaMemsetAsync(st, 0, sizeof(PState), s));
+    if (start_all) {
+        int one = 1;
+        GG_CUDA(ctx, cudaMemcpyAsync(&st->all[0], &one, sizeof(int), cudaMemcpyHostToDevice, s));
+        // counts of the all-true frontier: n vertices, m edges
+        uint64_t cnt[2] = {g->n, g->m};
+        GG_CUDA(ctx, cudaMemcpyAsync(P.fr[0].cnt, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
+    } else {
+        k_traverse_init<<<1, 1, 0, s>>>(P.fr[0], root, g->off, P.smax, P.mmax, 1);
+        GG_LAUNCHED(ctx);
+        int one = 1;
+        GG_CUDA(ctx, cudaMemcpyAsync(&st->has_list[0], &one, sizeof(int), cudaMemcpyHostToDevice, s));
+    }
+    const void *kfn = d.relax == GG_RELAX_MIN_PLUS1_I32 ? traverse_kernel<GG_RELAX_MIN_PLUS1_I32>()
+                    : d.relax == GG_RELAX_MIN_U32      ? traverse_kernel<GG_RELAX_MIN_U32>()
+                                                        : traverse_kernel<GG_RELAX_SETIF_U32>();
+    const int per_sm = resident_ctas(kfn, kPB);
+    const unsigned grid = (unsigned)(ctx->sm_count * per_sm);
+    // merge-path scratch: one count per list entry (<= n) + one per CTA
+    void *mp;
+    GG_CHECK(graph_scratch(g, ((size_t)g->n + grid + 1) * 8, &mp));
+    P.merge = (unsigned long long *)mp;
+    void *args[] = {&P};
+    GG_CUDA(ctx, cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kPB), args, 0, s));
+    ctx->launches++;
+    PState hs;
+    GG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PState), cudaMemcpyDeviceToHost, s));
+    GG_CUDA(ctx, cudaStreamSynchronize(s));
+    if (hs.err & DEV_ERR_TIMEOUT) return set_error(ctx, GG_ERR_TIMEOUT, "traversal grid barrier timed out");
+    if (hs.err) return set_error(ctx, GG_ERR_STATE, "traversal device error");
+    *iters_out = hs.iterations;
+    if (stats) {
+        stats->vertices_reached = hs.reached_v;
+        stats->edges_reached = hs.reached_e;
+        const int k = std::min(hs.iterations, GG_MAX_ITERS);
+        for (int i = 0; i < k; ++i) {
+            stats->variant[i] = hs.variant[i];
+            stats->nactv[i] = hs.nactv[i];
+            stats->nacte[i] = hs.nacte[i];
+            stats->scanned[i] = hs.scanned[i];
+            stats->iter_ms[i] = (double)(hs.t_ns[i + 1] - hs.t_ns[i]) * 1e-6;
+            stats->scanned_edges += hs.scanned[i];
+        }
+    }
+    // the final frontier is empty; no host state to keep
+    return GG_OK;
+}
+
+}  // namespace gg

@@ -111,7 +111,8 @@ template <int DT, bool ACC64, bool ADD_OLD, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_pr_gather(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj,
             const typename Store<DT>::T *__restrict__ contrib, uint32_t n, float *y_f32,
-            double *y_f64, PrState *st, float scale_inv_arg, int K, uint32_t T, int stream) {
+            double *y_f64, PrState *st, float scale_inv_arg, int K, uint32_t T, int stream,
+            const uint64_t *__restrict__ word_prefix) {
     using S = Store<DT>;
     using Acc = typename std::conditional<ACC64, double, float>::type;
     constexpr int U = 4;  // 32-edge chunks in flight per warp iteration
@@ -124,7 +125,10 @@ k_pr_gather(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in
     const uint32_t nw = (gridDim.x * BLOCK) >> 5;
     const uint64_t oend = in_off[n];
     double ysum = 0;
-    for (uint32_t w = (blockIdx.x * BLOCK + threadIdx.x) >> 5; w < nwords; w += nw) {
+    // a contiguous range of words of equal light-edge work per warp
+    uint32_t wlo, whi;
+    dev::balanced_range(word_prefix, nwords, (blockIdx.x * BLOCK + threadIdx.x) >> 5, nw, wlo, whi);
+    for (uint32_t w = wlo; w < whi; ++w) {
         const uint32_t d = (w << 5) + lane;
         const bool valid = d < n;
         const uint64_t beg = valid ? in_off[d] : oend;
@@ -391,7 +395,8 @@ static gg_status gather_launch(gg_graph *g, const typename Store<DT>::T *contrib
     const uint64_t cap = (uint64_t)ctx->sm_count * tuning().blocks_per_sm;
     if (blocks > cap) blocks = cap;
     k_pr_gather<DT, ACC64, ADD_OLD, 256><<<(unsigned)(blocks ? blocks : 1), 256, 0, s>>>(
-        g->in_off, g->in_adj, contrib, g->n, yf, yd, st, sinv, tuning().pull_k, H.T, tuning().pr_stream);
+        g->in_off, g->in_adj, contrib, g->n, yf, yd, st, sinv, tuning().pull_k, H.T, tuning().pr_stream,
+        H.light_prefix);
     GG_LAUNCHED(ctx);
     if (H.nchunks) {
         uint64_t cb = (H.nchunks * 32 + 255) / 256;

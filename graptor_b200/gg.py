@@ -49,7 +49,7 @@ class EmapDesc(C.Structure):
                 ("accum_f64", C.c_int), ("dst_filter", C.c_int), ("dst_filter_prop", C.c_void_p),
                 ("dst_filter_k", C.c_int64), ("src_strong", C.c_int), ("record", C.c_int),
                 ("prev", C.c_void_p), ("threshold", C.c_int), ("threshold_k", C.c_int),
-                ("variant", C.c_int), ("fusion", C.c_int)]
+                ("variant", C.c_int), ("fusion", C.c_int), ("src_level_sync", C.c_int)]
 
 
 class EmapStats(C.Structure):
@@ -478,3 +478,106 @@ def tuning_get(name: str) -> int:
 
 def default_opts(threshold=THRESH_DEFAULT, k=0, variant=VAR_AUTO, collect=False) -> RunOpts:
     return RunOpts(threshold=threshold, threshold_k=k, variant=variant, collect_stats=int(collect))
+
+
+# ---------------------------------------------------------------------------
+# Learned variant selector (include/gg_select.h)
+# ---------------------------------------------------------------------------
+SEL_FEATURES, SEL_VARIANTS, SEL_NPARAMS = 10, 4, 32 * 10 + 32 + 32 * 32 + 32 + 4 * 32 + 4
+
+
+def _sel_lib():
+    L = lib()
+    if not getattr(L, "_sel_bound", False):
+        vp, fp, ip = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_int)
+        L.gg_selector_create.argtypes = [vp, C.POINTER(vp)]
+        L.gg_selector_destroy.argtypes = [vp]
+        L.gg_selector_set_params.argtypes = [vp, vp, C.c_int]
+        L.gg_selector_get_params.argtypes = [vp, vp, C.c_int]
+        L.gg_selector_forward.argtypes = [vp, vp, C.c_int, vp]
+        L.gg_selector_loss_grad.argtypes = [vp, vp, vp, vp, C.c_int, fp, vp]
+        L.gg_selector_train.argtypes = [vp, vp, vp, vp, C.c_int, C.c_int, C.c_float, fp]
+        L.gg_selector_collect.argtypes = [vp, C.c_int, C.c_uint32, C.c_int, vp, vp, C.c_int, ip]
+        L.gg_graph_set_selector.argtypes = [vp, vp]
+        for n in ["gg_selector_create", "gg_selector_destroy", "gg_selector_set_params",
+                  "gg_selector_get_params", "gg_selector_forward", "gg_selector_loss_grad",
+                  "gg_selector_train", "gg_selector_collect", "gg_graph_set_selector"]:
+            getattr(L, n).restype = C.c_int
+        L._sel_bound = True
+    return L
+
+
+def _f32(a, shape):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    assert a.shape == shape, (a.shape, shape)
+    return a
+
+
+class Selector:
+    """The traversal-variant network: inference, loss gradient, training."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.h = C.c_void_p()
+        ctx.check(_sel_lib().gg_selector_create(ctx.h, C.byref(self.h)), "gg_selector_create")
+        ctx._children.add(self)
+
+    def close(self):
+        if self.h:
+            if self.ctx.h:
+                _sel_lib().gg_selector_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def params(self) -> np.ndarray:
+        p = np.empty(SEL_NPARAMS, dtype=np.float32)
+        self.ctx.check(_sel_lib().gg_selector_get_params(self.h, _p(p), SEL_NPARAMS), "get_params")
+        return p
+
+    @params.setter
+    def params(self, p):
+        p = _f32(p, (SEL_NPARAMS,))
+        self.ctx.check(_sel_lib().gg_selector_set_params(self.h, _p(p), SEL_NPARAMS), "set_params")
+
+    def forward(self, X) -> np.ndarray:
+        X = _f32(X, (len(X), SEL_FEATURES))
+        out = np.empty((len(X), SEL_VARIANTS), dtype=np.float32)
+        self.ctx.check(_sel_lib().gg_selector_forward(self.h, _p(X), len(X), _p(out)), "forward")
+        return out
+
+    def loss_grad(self, X, Y, M):
+        n = len(X)
+        X, Y, M = _f32(X, (n, SEL_FEATURES)), _f32(Y, (n, SEL_VARIANTS)), _f32(M, (n, SEL_VARIANTS))
+        loss = C.c_float()
+        g = np.empty(SEL_NPARAMS, dtype=np.float32)
+        self.ctx.check(_sel_lib().gg_selector_loss_grad(self.h, _p(X), _p(Y), _p(M), n, C.byref(loss), _p(g)),
+                       "loss_grad")
+        return loss.value, g
+
+    def train(self, X, Y, M, epochs=500, lr=3e-3) -> float:
+        n = len(X)
+        X, Y, M = _f32(X, (n, SEL_FEATURES)), _f32(Y, (n, SEL_VARIANTS)), _f32(M, (n, SEL_VARIANTS))
+        loss = C.c_float()
+        self.ctx.check(_sel_lib().gg_selector_train(self.h, _p(X), _p(Y), _p(M), n, epochs, lr, C.byref(loss)),
+                       "train")
+        return loss.value
+
+
+def selector_collect(g: "Graph", analytic: int, root: int = 0, max_samples: int = 8, cap: int = 256):
+    """Per sampled iteration: features X[k][10], measured log2 us Y[k][4]."""
+    X = np.zeros((cap, SEL_FEATURES), dtype=np.float32)
+    Y = np.zeros((cap, SEL_VARIANTS), dtype=np.float32)
+    k = C.c_int()
+    g.ctx.check(_sel_lib().gg_selector_collect(g.h, analytic, root, max_samples, _p(X), _p(Y), cap, C.byref(k)),
+                "gg_selector_collect")
+    return X[: k.value], Y[: k.value]
+
+
+def attach_selector(g: "Graph", sel: "Selector | None"):
+    g.ctx.check(_sel_lib().gg_graph_set_selector(g.h, sel.h if sel else None), "gg_graph_set_selector")

@@ -215,6 +215,9 @@ typedef struct gg_emap_desc {
     int threshold_k;        /* FRAC percentage */
     int variant;            /* gg_variant override (GG_VAR_AUTO = threshold decides) */
     int fusion;             /* api::fusion present: multi-hop push allowed */
+    int src_level_sync;     /* MIN_PLUS1 with GT_CONST filter k: every active source
+                               holds a[s] == k-1 (level-synchronous BFS), so the
+                               relax offers k without loading a[s] */
 } gg_emap_desc;
 
 typedef struct gg_emap_stats {

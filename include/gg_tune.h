@@ -11,7 +11,12 @@
  * pull_k, push_k (edges a lane scans alone before its warp helps),
  * heavy_deg, heavy_chunk (CSC rows chunked for gathers; applies to graphs
  * created afterwards), large_chunk (push: edges per chunk of a hub row),
- * pr_stream (1: warp-streamed segmented PageRank gather, 0: per-row).
+ * pr_stream (1: warp-streamed segmented PageRank gather, 0: per-row),
+ * persistent (bit mask: 1 BFS levels, 2 BFS parents, 4 CC run as one
+ * device-driven cooperative launch; otherwise one launch per iteration from
+ * the host), barrier_timeout_ns
+ * (how long a CTA of a persistent run waits at a grid barrier before it
+ * reports GG_ERR_TIMEOUT).
  */
 #ifndef GG_TUNE_H
 #define GG_TUNE_H

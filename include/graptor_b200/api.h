@@ -1,0 +1,974 @@
+// graptor_b200/api.h -- Graptor's edgemap/vertexmap operator surface over the
+// B200 library (libgg.so, C ABI in gg.h).  Header-only C++17.
+//
+// The reference's analytics are written against include/graptor/api.h:
+//   api::edgemap(GA, api::record(...), api::filter(...), api::relax(λ))  (api.h:2143-2415)
+//   make_lazy_executor(part).vertex_map(λ).vertex_scan(λ).materialize() (dsl/vertexmap.h:2120-2446)
+//   api::vertexprop<T,VID,AID,Enc>                                      (api/vertexprop.h:30-140)
+//   frontier::create / all_true / del / nActiveVertices / ...            (frontier/frontier.h:58-716)
+// and the lambdas return expression trees built from expr::_c, _0, _1, cast,
+// iif, min, setif, ... (dsl/ast).  As in the reference the lambdas run once,
+// on placeholder arguments, to build the tree; here the tree is a run-time
+// object that is lowered to a gg_emap_desc (the enumerated relax/filter/record
+// kinds of the hot path) or compiled to a gg_vmap_desc stack program.  A tree
+// outside the lowering table throws graptor_b200::error(GG_ERR_UNSUPPORTED)
+// naming the expression.
+#ifndef GRAPTOR_B200_API_H
+#define GRAPTOR_B200_API_H
+
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "gg.h"
+
+using VID = uint32_t;
+using EID = uint64_t;
+
+namespace graptor_b200 {
+
+struct error : std::runtime_error {
+    gg_status status;
+    error(gg_status s, const std::string &m) : std::runtime_error(m), status(s) {}
+};
+
+inline gg_ctx *&ctx_slot() {
+    static gg_ctx *c = nullptr;
+    return c;
+}
+
+// Process-wide context on device GG_DEVICE (default 0), created on first use.
+inline gg_ctx *context() {
+    gg_ctx *&c = ctx_slot();
+    if (!c) {
+        const char *dv = std::getenv("GG_DEVICE");
+        gg_status s = gg_ctx_create(dv ? std::atoi(dv) : 0, &c);
+        if (s != GG_OK) throw error(s, std::string("gg_ctx_create: ") + gg_status_string(s));
+    }
+    return c;
+}
+
+inline void check(gg_status s, const char *what) {
+    if (s != GG_OK) {
+        std::string m = std::string(what) + ": " + gg_status_string(s) + ": " + gg_last_error(ctx_slot());
+        throw error(s, m);
+    }
+}
+
+// Device writes bump this epoch; host mirrors of properties refresh on change.
+inline uint64_t &device_epoch() {
+    static uint64_t e = 1;
+    return e;
+}
+
+template <typename T> struct dtype_of;
+template <> struct dtype_of<int32_t> { static constexpr gg_dtype value = GG_I32; };
+template <> struct dtype_of<uint32_t> { static constexpr gg_dtype value = GG_U32; };
+template <> struct dtype_of<float> { static constexpr gg_dtype value = GG_F32; };
+template <> struct dtype_of<double> { static constexpr gg_dtype value = GG_F64; };
+
+// Registry of device arrays by device address, so that expr::array_ro(ptr)
+// (PRv.C:125-150) can find the property behind a raw pointer.
+inline std::map<const void *, gg_prop *> &registry() {
+    static std::map<const void *, gg_prop *> r;
+    return r;
+}
+
+}  // namespace graptor_b200
+
+// ---------------------------------------------------------------------------
+// Graph and partitioner
+// ---------------------------------------------------------------------------
+class GraphGPU;
+
+class partitioner {
+public:
+    partitioner() = default;
+    partitioner(gg_graph *g, VID n) : g_(g), n_(n) {}
+    VID get_num_vertices() const { return n_; }
+    VID get_num_elements() const { return n_; }
+    int get_num_partitions() const { return 1; }
+    gg_graph *graph() const { return g_; }
+
+private:
+    gg_graph *g_ = nullptr;
+    VID n_ = 0;
+};
+
+class GraphGPU {
+public:
+    GraphGPU() = default;
+    explicit GraphGPU(gg_graph *g) : g_(g) { init(); }
+    static GraphGPU read_bin(const std::string &path, bool symmetric) {
+        gg_graph *g = nullptr;
+        graptor_b200::check(gg_graph_read_bin(graptor_b200::context(), path.c_str(), symmetric, &g),
+                            "gg_graph_read_bin");
+        return GraphGPU(g);
+    }
+    static GraphGPU from_csr(VID n, EID m, const EID *off, const VID *adj, bool symmetric) {
+        gg_graph *g = nullptr;
+        graptor_b200::check(gg_graph_upload(graptor_b200::context(), n, m, off, adj, symmetric, &g),
+                            "gg_graph_upload");
+        return GraphGPU(g);
+    }
+    VID numVertices() const { return n_; }
+    EID numEdges() const { return m_; }
+    bool isSymmetric() const { return sym_ != 0; }
+    const partitioner &get_partitioner() const { return part_; }
+    VID getOutDegree(VID v) const {
+        if (!deg_) {
+            std::vector<EID> off((size_t)n_ + 1);
+            graptor_b200::check(gg_graph_download(g_, off.data(), nullptr), "gg_graph_download");
+            deg_ = std::make_shared<std::vector<VID>>(n_);
+            for (VID i = 0; i < n_; ++i) (*deg_)[i] = (VID)(off[i + 1] - off[i]);
+        }
+        return (*deg_)[v];
+    }
+    // no vertex renumbering on the device: ids are the file's ids
+    VID remapID(VID v) const { return v; }
+    VID originalID(VID v) const { return v; }
+    gg_graph *handle() const { return g_; }
+    void del() {
+        if (g_) gg_graph_destroy(g_);
+        g_ = nullptr;
+    }
+
+private:
+    void init() {
+        uint64_t m = 0;
+        graptor_b200::check(gg_graph_info(g_, &n_, &m, &sym_), "gg_graph_info");
+        m_ = m;
+        part_ = partitioner(g_, n_);
+    }
+    gg_graph *g_ = nullptr;
+    VID n_ = 0;
+    EID m_ = 0;
+    int sym_ = 0;
+    partitioner part_;
+    mutable std::shared_ptr<std::vector<VID>> deg_;
+};
+
+// ---------------------------------------------------------------------------
+// Frontier (value handle with manual del(), frontier/frontier.h:58-716)
+// ---------------------------------------------------------------------------
+enum class frontier_type { ft_true = 0, ft_unbacked = 1, ft_bool = 2, ft_bit = 3, ft_logical1 = 4,
+                           ft_logical2 = 5, ft_logical4 = 6, ft_logical8 = 7, ft_sparse = 8,
+                           ft_bit2 = 9, ft_msb4 = 10, ft_N = 11 };
+
+inline std::ostream &operator<<(std::ostream &os, frontier_type t) {
+    static const char *names[] = {"true", "unbacked", "bool", "bit", "logical1", "logical2",
+                                  "logical4", "logical8", "sparse", "bit2", "msb4", "N"};
+    int i = (int)t;
+    return os << names[(i >= 0 && i <= 11) ? i : 11];
+}
+
+class frontier {
+public:
+    frontier() = default;
+    // frontier::create(n, v, deg): one active vertex
+    static frontier create(VID n, VID v, VID deg) {
+        frontier f;
+        f.kind_ = K_SINGLE;
+        f.n_ = n;
+        f.v_ = v;
+        f.nactv_ = 1;
+        f.nacte_ = deg;
+        return f;
+    }
+    static frontier all_true(VID n, EID m) {
+        frontier f;
+        f.kind_ = K_ALL;
+        f.n_ = n;
+        f.nactv_ = n;
+        f.nacte_ = m;
+        return f;
+    }
+    static frontier empty() { return frontier(); }
+    void del() {
+        if (f_) gg_frontier_destroy(f_);
+        f_ = nullptr;
+        kind_ = K_EMPTY;
+    }
+    bool isEmpty() const { return nActiveVertices() == 0; }
+    VID nActiveVertices() const { refresh(); return (VID)nactv_; }
+    EID nActiveEdges() const { refresh(); return nacte_; }
+    float density(EID m) const { return m ? float(double(nActiveVertices() + nActiveEdges()) / double(m)) : 0.f; }
+    frontier_type getType() const {
+        return kind_ == K_ALL ? frontier_type::ft_true : kind_ == K_DEV ? frontier_type::ft_sparse
+                                                                       : frontier_type::ft_unbacked;
+    }
+    bool is_set(VID v) const {
+        if (kind_ == K_ALL) return true;
+        if (kind_ == K_SINGLE) return v == v_;
+        if (kind_ != K_DEV) return false;
+        uint64_t k = 0;
+        graptor_b200::check(gg_frontier_download(f_, nullptr, 0, &k), "gg_frontier_download");
+        std::vector<uint32_t> l(k ? k : 1);
+        graptor_b200::check(gg_frontier_download(f_, l.data(), k, &k), "gg_frontier_download");
+        for (uint64_t i = 0; i < k; ++i)
+            if (l[i] == v) return true;
+        return false;
+    }
+
+    // --- library side ---
+    // Device frontier for graph g (materialises a pending single/all frontier).
+    gg_frontier *bind(gg_graph *g) {
+        if (kind_ == K_DEV) return f_;
+        if (!f_) graptor_b200::check(gg_frontier_create(g, &f_), "gg_frontier_create");
+        if (kind_ == K_SINGLE) graptor_b200::check(gg_frontier_set_single(f_, v_), "gg_frontier_set_single");
+        else if (kind_ == K_ALL) graptor_b200::check(gg_frontier_set_all(f_), "gg_frontier_set_all");
+        else graptor_b200::check(gg_frontier_clear(f_), "gg_frontier_clear");
+        kind_ = K_DEV;
+        stale_ = true;
+        return f_;
+    }
+    // An output frontier written by the device.
+    gg_frontier *output(gg_graph *g) {
+        if (!f_) graptor_b200::check(gg_frontier_create(g, &f_), "gg_frontier_create");
+        kind_ = K_DEV;
+        stale_ = true;
+        return f_;
+    }
+    bool all() const { return kind_ == K_ALL; }
+
+private:
+    enum Kind { K_EMPTY, K_SINGLE, K_ALL, K_DEV };
+    void refresh() const {
+        if (kind_ == K_DEV && stale_) {
+            uint64_t v = 0, e = 0;
+            graptor_b200::check(gg_frontier_counts(f_, &v, &e), "gg_frontier_counts");
+            nactv_ = v;
+            nacte_ = e;
+            stale_ = false;
+        }
+    }
+    Kind kind_ = K_EMPTY;
+    gg_frontier *f_ = nullptr;
+    VID n_ = 0, v_ = 0;
+    mutable uint64_t nactv_ = 0;
+    mutable EID nacte_ = 0;
+    mutable bool stale_ = false;
+};
+
+// ---------------------------------------------------------------------------
+// Expression trees (the meaning of dsl/ast for the hot-path operators)
+// ---------------------------------------------------------------------------
+namespace expr {
+
+enum class NK {
+    VarSrc, VarDst, VarV, VarEdge, Const, Ref, Min, SetIf, Assign, AddAssign, MulAssign,
+    Add, Sub, Mul, Div, Eq, Ne, Lt, Gt, Le, Ge, LAnd, LOr, Cast, Abs, Iif, MsbSet, Noop
+};
+
+struct Node {
+    NK k;
+    std::vector<std::shared_ptr<Node>> c;
+    double cval = 0;       // Const
+    gg_dtype dt = GG_F64;  // Const / Ref / Cast: value type
+    gg_prop *prop = nullptr;  // Ref: device array
+    double *host = nullptr;   // Ref: host scalar accumulator (array_ro over a host variable)
+};
+using NP = std::shared_ptr<Node>;
+
+inline NP mk(NK k, std::vector<NP> c = {}) {
+    auto n = std::make_shared<Node>();
+    n->k = k;
+    n->c = std::move(c);
+    return n;
+}
+
+inline std::string show(const NP &n) {
+    static const char *nm[] = {"s", "d", "v", "e", "const", "ref", "min", "setif", "=", "+=", "*=",
+                               "+", "-", "*", "/", "==", "!=", "<", ">", "<=", ">=", "&&", "||",
+                               "cast", "abs", "iif", "msbset", "noop"};
+    std::ostringstream os;
+    if (n->k == NK::Const) return (os << n->cval, os.str());
+    os << nm[(int)n->k];
+    if (!n->c.empty()) {
+        os << "(";
+        for (size_t i = 0; i < n->c.size(); ++i) os << (i ? "," : "") << show(n->c[i]);
+        os << ")";
+    }
+    return os.str();
+}
+
+class E;
+template <typename T> E _c(T v);
+
+// An expression value.  Copying an E copies the handle, not the tree.
+class E {
+public:
+    E() : n_(mk(NK::Noop)) {}
+    explicit E(NP n) : n_(std::move(n)) {}
+    template <typename T, typename = std::enable_if_t<std::is_arithmetic<T>::value>>
+    E(T v);  // literal operand
+    const NP &node() const { return n_; }
+
+    // a[d].min(x): relax to the minimum, "changed" as value
+    E min(const E &x) const { return E(mk(NK::Min, {n_, x.n_})); }
+    // a[d].setif(x): set when unset (msb set)
+    E setif(const E &x) const { return E(mk(NK::SetIf, {n_, x.n_})); }
+    E operator+=(const E &x) const { return E(mk(NK::AddAssign, {n_, x.n_})); }
+    E operator*=(const E &x) const { return E(mk(NK::MulAssign, {n_, x.n_})); }
+    // assignment builds a node (a[v] = x); E values are never re-seated
+    E operator=(const E &x) const { return E(mk(NK::Assign, {n_, x.n_})); }
+    // _0(vid): the zero index of a scalar accumulator (PRv.C:241)
+    E operator()(const E &) const { return *this; }
+
+private:
+    NP n_;
+};
+
+inline E cst(double v, gg_dtype dt) {
+    auto n = mk(NK::Const);
+    n->cval = v;
+    n->dt = dt;
+    return E(n);
+}
+
+template <typename T>
+inline gg_dtype literal_dtype() {
+    if (std::is_floating_point<T>::value) return sizeof(T) == 4 ? GG_F32 : GG_F64;
+    return std::is_signed<T>::value ? GG_I32 : GG_U32;
+}
+
+template <typename T, typename>
+inline E::E(T v) : n_(cst((double)v, literal_dtype<T>()).node()) {}
+
+template <typename T> inline E _c(T v) { return cst((double)v, literal_dtype<T>()); }
+
+#define GG_BINOP(op, kind)                                                             \
+    inline E operator op(const E &a, const E &b) { return E(mk(NK::kind, {a.node(), b.node()})); }
+GG_BINOP(+, Add)
+GG_BINOP(-, Sub)
+GG_BINOP(*, Mul)
+GG_BINOP(/, Div)
+GG_BINOP(==, Eq)
+GG_BINOP(!=, Ne)
+GG_BINOP(<, Lt)
+GG_BINOP(>, Gt)
+GG_BINOP(<=, Le)
+GG_BINOP(>=, Ge)
+GG_BINOP(&&, LAnd)
+GG_BINOP(||, LOr)
+#undef GG_BINOP
+
+static const E _0 = cst(0, GG_I32);
+static const E _1 = cst(1, GG_I32);
+static const E _1s = cst(-1, GG_I32);
+static const E _true = cst(1, GG_I32);
+static const E _false = cst(0, GG_I32);
+
+inline E zero_val(const E &) { return cst(0, GG_I32); }
+template <typename T> inline E constant_val(const E &, T v) { return cst((double)v, literal_dtype<T>()); }
+template <typename T> inline E cast(const E &a) {
+    auto n = mk(NK::Cast, {a.node()});
+    n->dt = literal_dtype<T>();
+    return E(n);
+}
+inline E make_unop_abs(const E &a) { return E(mk(NK::Abs, {a.node()})); }
+inline E iif(const E &c, const E &a, const E &b) { return E(mk(NK::Iif, {c.node(), a.node(), b.node()})); }
+inline E msbset(const E &a) { return E(mk(NK::MsbSet, {a.node()})); }
+inline E make_noop() { return E(mk(NK::Noop)); }
+
+inline E var(NK k) { return E(mk(k)); }
+
+// Reference to element idx of a device array (or of a host scalar).
+inline E ref(gg_prop *p, double *host, gg_dtype dt, const E &idx) {
+    auto n = mk(NK::Ref, {idx.node()});
+    n->prop = p;
+    n->host = host;
+    n->dt = dt;
+    return E(n);
+}
+
+// expr::array_ro<T,VID,AID,Enc>(ptr): a view over a device array registered
+// by mmap_ptr / vertexprop, or over a host scalar (reduction target).
+template <typename T, typename U = VID, short AID = 0, typename Enc = void>
+class array_ro {
+public:
+    explicit array_ro(T *p) {
+        auto &r = graptor_b200::registry();
+        auto it = r.find((const void *)p);
+        if (it != r.end()) prop_ = it->second;
+        else host_ = reinterpret_cast<double *>(p);
+        static_assert(!std::is_same<T, void>::value, "element type");
+        if (!prop_ && !std::is_same<T, double>::value)
+            throw graptor_b200::error(GG_ERR_UNSUPPORTED, "array_ro over host memory must be a double scalar");
+    }
+    E operator[](const E &i) const { return ref(prop_, host_, graptor_b200::dtype_of<T>::value, i); }
+
+private:
+    gg_prop *prop_ = nullptr;
+    double *host_ = nullptr;
+};
+
+}  // namespace expr
+
+// ---------------------------------------------------------------------------
+// Storage encodings (encoding.h / customfp.h types used as template tags)
+// ---------------------------------------------------------------------------
+template <unsigned short E_, unsigned short M_> struct customfp {};
+template <bool S_, unsigned short E_, unsigned short M_, bool Z_, int B_> struct scustomfp {};
+template <typename T> struct array_encoding { using stored_type = T; };
+template <typename T, bool = false> struct array_encoding_wide { using stored_type = T; };
+
+namespace graptor_b200 {
+template <typename T, typename Enc> struct storage_dtype { static constexpr gg_dtype value = dtype_of<T>::value; };
+template <typename T> struct storage_dtype<T, array_encoding<customfp<6, 10>>> { static constexpr gg_dtype value = GG_CFP_6_10; };
+template <typename T> struct storage_dtype<T, array_encoding_wide<customfp<6, 10>>> { static constexpr gg_dtype value = GG_CFP_6_10; };
+template <typename T> struct storage_dtype<T, array_encoding_wide<scustomfp<true, 8, 7, false, 0>>> { static constexpr gg_dtype value = GG_BF16_TRUNC; };
+template <typename T, typename S> struct storage_dtype<T, array_encoding<S>> { static constexpr gg_dtype value = dtype_of<S>::value; };
+
+// Host-side element proxy: reads/writes one element through the C ABI.
+template <typename T>
+class elem_proxy {
+public:
+    elem_proxy(gg_prop *p, VID v) : p_(p), v_(v) {}
+    elem_proxy &operator=(T x) {
+        check(gg_prop_set(p_, v_, &x), "gg_prop_set");
+        ++device_epoch();
+        return *this;
+    }
+    operator T() const {
+        T x{};
+        check(gg_prop_get(p_, v_, &x), "gg_prop_get");
+        return x;
+    }
+
+private:
+    gg_prop *p_;
+    VID v_;
+};
+
+template <typename T>
+class ptr_proxy {
+public:
+    explicit ptr_proxy(gg_prop *p) : p_(p) {}
+    elem_proxy<T> operator[](VID v) const { return elem_proxy<T>(p_, v); }
+
+private:
+    gg_prop *p_;
+};
+}  // namespace graptor_b200
+
+// mmap_ptr<T>: device array of one element per vertex (mm.h), host access by proxy.
+struct numa_allocation_partitioned {
+    explicit numa_allocation_partitioned(const partitioner &p) : part(p) {}
+    partitioner part;
+};
+
+template <typename T>
+class mmap_ptr {
+public:
+    void allocate(const numa_allocation_partitioned &a) {
+        graptor_b200::check(gg_prop_create(a.part.graph(), graptor_b200::dtype_of<T>::value, &p_),
+                            "gg_prop_create");
+        void *d = nullptr;
+        gg_prop_device_ptr(p_, &d);
+        graptor_b200::registry()[d] = p_;
+        d_ = (T *)d;
+    }
+    T *get() const { return d_; }
+    graptor_b200::elem_proxy<T> operator[](VID v) const { return graptor_b200::elem_proxy<T>(p_, v); }
+    void del() {
+        if (p_) {
+            graptor_b200::registry().erase(d_);
+            gg_prop_destroy(p_);
+        }
+        p_ = nullptr;
+        d_ = nullptr;
+    }
+    gg_prop *handle() const { return p_; }
+
+private:
+    gg_prop *p_ = nullptr;
+    T *d_ = nullptr;
+};
+
+namespace api {
+
+// ---------------------------------------------------------------------------
+// vertexprop (api/vertexprop.h:30-140)
+// ---------------------------------------------------------------------------
+template <typename T, typename U = VID, short AID = 0, typename Enc = array_encoding<T>>
+class vertexprop {
+public:
+    vertexprop(const partitioner &part, const char *name = nullptr) {
+        (void)name;
+        graptor_b200::check(gg_prop_create(part.graph(), graptor_b200::storage_dtype<T, Enc>::value, &p_),
+                            "gg_prop_create");
+        void *d = nullptr;
+        gg_prop_device_ptr(p_, &d);
+        graptor_b200::registry()[d] = p_;
+        n_ = part.get_num_vertices();
+    }
+    static vertexprop create(const partitioner &part, const char *name = nullptr) { return vertexprop(part, name); }
+    void del() {
+        if (p_) {
+            void *d = nullptr;
+            gg_prop_device_ptr(p_, &d);
+            graptor_b200::registry().erase(d);
+            gg_prop_destroy(p_);
+        }
+        p_ = nullptr;
+    }
+    expr::E operator[](const expr::E &i) const {
+        return expr::ref(p_, nullptr, graptor_b200::storage_dtype<T, Enc>::value, i);
+    }
+    // host read (vertexprop::operator[](VID)): served from a host mirror
+    // refreshed when the device has written since the last read
+    T operator[](VID v) const {
+        if (mirror_epoch_ != graptor_b200::device_epoch() || mirror_.size() != n_) {
+            mirror_.resize(n_);
+            graptor_b200::check(gg_prop_download(p_, mirror_.data()), "gg_prop_download");
+            mirror_epoch_ = graptor_b200::device_epoch();
+        }
+        return mirror_[v];
+    }
+    void set(VID v, T t) {
+        graptor_b200::check(gg_prop_set(p_, v, &t), "gg_prop_set");
+        ++graptor_b200::device_epoch();
+    }
+    graptor_b200::ptr_proxy<T> get_ptr() const { return graptor_b200::ptr_proxy<T>(p_); }
+    void fill(const partitioner &, T val) {
+        graptor_b200::check(gg_prop_fill(p_, &val), "gg_prop_fill");
+        ++graptor_b200::device_epoch();
+    }
+    gg_prop *handle() const { return p_; }
+
+private:
+    gg_prop *p_ = nullptr;
+    VID n_ = 0;
+    mutable std::vector<T> mirror_;
+    mutable uint64_t mirror_epoch_ = 0;
+};
+
+// ---------------------------------------------------------------------------
+// Argument tags and argument objects (api.h:130-1985)
+// ---------------------------------------------------------------------------
+enum class filter_strength { weak, strong };
+enum class filter_entity { src, dst };
+enum class frontier_record { frontier_reduction, frontier_method, frontier_reduction_or_method };
+template <filter_strength S> struct filter_strength_argument {};
+template <filter_entity E_> struct filter_entity_argument {};
+template <frontier_record R> struct frontier_record_argument {};
+static constexpr filter_strength_argument<filter_strength::weak> weak{};
+static constexpr filter_strength_argument<filter_strength::strong> strong{};
+static constexpr filter_entity_argument<filter_entity::src> src{};
+static constexpr filter_entity_argument<filter_entity::dst> dst{};
+static constexpr frontier_record_argument<frontier_record::frontier_reduction> reduction{};
+static constexpr frontier_record_argument<frontier_record::frontier_method> method{};
+static constexpr frontier_record_argument<frontier_record::frontier_reduction_or_method> reduction_or_method{};
+
+struct default_threshold {
+    bool is_sparse(VID nactv, EID nacte, EID m) const { return (EID(nactv) + nacte) <= (m / 20); }
+    bool is_sparse(const frontier &F, EID m) const { return is_sparse(F.nActiveVertices(), F.nActiveEdges(), m); }
+};
+class frac_threshold {
+public:
+    explicit frac_threshold(int k) : k_(k) {}
+    bool is_sparse(VID nactv, EID nacte, EID m) const {
+        return float(EID(nactv) + nacte) <= float(m) / (100.0f / (float)k_);
+    }
+    int k() const { return k_; }
+
+private:
+    int k_;
+};
+struct always_sparse_t {};
+struct always_dense_t {};
+struct learned_threshold_t {};
+static constexpr always_sparse_t always_sparse{};
+static constexpr always_dense_t always_dense{};
+static constexpr learned_threshold_t learned_threshold{};
+struct fusion_select { explicit fusion_select(bool e = true) : enable(e) {} bool enable; };
+
+struct arg_config {
+    int threshold = GG_THRESH_DEFAULT;
+    int k = 0;
+    bool fusion = true;
+};
+inline void config_one(arg_config &, const default_threshold &) {}
+inline void config_one(arg_config &c, const frac_threshold &t) { c.threshold = GG_THRESH_FRAC; c.k = t.k(); }
+inline void config_one(arg_config &c, const always_sparse_t &) { c.threshold = GG_THRESH_ALWAYS_SPARSE; }
+inline void config_one(arg_config &c, const always_dense_t &) { c.threshold = GG_THRESH_ALWAYS_DENSE; }
+inline void config_one(arg_config &c, const learned_threshold_t &) { c.threshold = GG_THRESH_LEARNED; }
+inline void config_one(arg_config &c, const fusion_select &f) { c.fusion = f.enable; }
+template <typename... A> arg_config config(const A &... a) {
+    arg_config c;
+    (config_one(c, a), ...);
+    return c;
+}
+
+template <typename Fn> struct arg_relax { Fn fn; };
+template <typename Fn> arg_relax<Fn> relax(Fn fn) { return arg_relax<Fn>{fn}; }
+template <typename Fn> struct arg_fusion { Fn fn; };
+template <typename Fn> arg_fusion<Fn> fusion(Fn fn) { return arg_fusion<Fn>{fn}; }
+
+struct arg_filter_src { frontier *F; bool strong; };
+template <typename Fn> struct arg_filter_dst { Fn fn; bool strong; };
+template <filter_strength S>
+arg_filter_src filter(filter_strength_argument<S>, filter_entity_argument<filter_entity::src>, frontier &F) {
+    return arg_filter_src{&F, S == filter_strength::strong};
+}
+template <filter_strength S, typename Fn>
+arg_filter_dst<Fn> filter(filter_strength_argument<S>, filter_entity_argument<filter_entity::dst>, Fn fn) {
+    return arg_filter_dst<Fn>{fn, S == filter_strength::strong};
+}
+
+struct no_method {};
+template <typename Fn> struct arg_record { frontier *out; frontier_record kind; Fn fn; bool has_fn; };
+template <filter_strength S = filter_strength::strong>
+arg_record<no_method> record(frontier &f, filter_strength_argument<S> = strong) {
+    return arg_record<no_method>{&f, frontier_record::frontier_reduction, no_method{}, false};
+}
+template <frontier_record R, filter_strength S = filter_strength::strong>
+arg_record<no_method> record(frontier &f, frontier_record_argument<R>, filter_strength_argument<S> = strong) {
+    return arg_record<no_method>{&f, R, no_method{}, false};
+}
+template <typename Fn, filter_strength S = filter_strength::strong,
+          typename = std::enable_if_t<std::is_invocable<Fn, expr::E>::value>>
+arg_record<Fn> record(frontier &f, Fn fn, filter_strength_argument<S> = strong) {
+    return arg_record<Fn>{&f, frontier_record::frontier_method, fn, true};
+}
+template <frontier_record R, typename Fn, filter_strength S = filter_strength::strong,
+          typename = std::enable_if_t<std::is_invocable<Fn, expr::E>::value>>
+arg_record<Fn> record(frontier &f, frontier_record_argument<R>, Fn fn, filter_strength_argument<S> = strong) {
+    return arg_record<Fn>{&f, R, fn, true};
+}
+
+}  // namespace api
+
+// ---------------------------------------------------------------------------
+// Lowering: expression trees -> gg_emap_desc / gg_vmap_desc
+// ---------------------------------------------------------------------------
+namespace graptor_b200 {
+using expr::NK;
+using expr::NP;
+
+[[noreturn]] inline void unsupported(const char *what, const NP &n) {
+    throw error(GG_ERR_UNSUPPORTED, std::string(what) + " not on the hot path: " + expr::show(n));
+}
+
+inline bool is_ref_at(const NP &n, NK var) { return n->k == NK::Ref && n->prop && n->c[0]->k == var; }
+inline bool is_const(const NP &n, double v) { return n->k == NK::Const && n->cval == v; }
+inline NP strip_cast(const NP &n) { return n->k == NK::Cast ? n->c[0] : n; }
+
+// relax(s,d,e) -> descriptor fields (SURVEY-documented lowering table)
+inline void lower_relax(const NP &r, gg_emap_desc &d) {
+    if (r->k == NK::Min && is_ref_at(r->c[0], NK::VarDst)) {
+        const NP &a = r->c[0], &x = r->c[1];
+        if (x->k == NK::Add && is_ref_at(x->c[0], NK::VarSrc) && x->c[0]->prop == a->prop && is_const(x->c[1], 1) &&
+            a->dt == GG_I32) {
+            d.relax = GG_RELAX_MIN_PLUS1_I32;  // a[d].min(a[s] + _1)
+            d.a = a->prop;
+            return;
+        }
+        if (is_ref_at(x, NK::VarSrc) && x->prop == a->prop && a->dt == GG_U32) {
+            d.relax = GG_RELAX_MIN_U32;  // a[d].min(a[s])
+            d.a = a->prop;
+            return;
+        }
+    }
+    if (r->k == NK::SetIf && is_ref_at(r->c[0], NK::VarDst) && r->c[1]->k == NK::VarSrc && r->c[0]->dt == GG_U32) {
+        d.relax = GG_RELAX_SETIF_U32;  // a[d].setif(s)
+        d.a = r->c[0]->prop;
+        return;
+    }
+    if (r->k == NK::AddAssign && is_ref_at(r->c[0], NK::VarDst)) {
+        const NP x = strip_cast(r->c[1]);
+        if (is_ref_at(x, NK::VarSrc)) {
+            d.relax = GG_RELAX_ADD_GATHER;  // y[d] += cast(contrib[s])
+            d.a = r->c[0]->prop;
+            d.src = x->prop;
+            d.accum_f64 = r->c[1]->k == NK::Cast ? (r->c[1]->dt == GG_F64) : (r->c[0]->dt == GG_F64);
+            return;
+        }
+    }
+    unsupported("relax", r);
+}
+
+inline void lower_dst_filter(const NP &f, gg_emap_desc &d) {
+    if (f->k == NK::Gt && is_ref_at(f->c[0], NK::VarDst) && f->c[1]->k == NK::Const) {
+        d.dst_filter = GG_FILTER_GT_CONST;
+        d.dst_filter_prop = f->c[0]->prop;
+        d.dst_filter_k = (int64_t)f->c[1]->cval;
+        return;
+    }
+    if (f->k == NK::Ne && is_ref_at(f->c[0], NK::VarDst) && is_const(f->c[1], 0)) {
+        d.dst_filter = GG_FILTER_NE_ZERO;
+        d.dst_filter_prop = f->c[0]->prop;
+        return;
+    }
+    if (f->k == NK::MsbSet && is_ref_at(f->c[0], NK::VarDst)) {
+        d.dst_filter = GG_FILTER_MSB_SET;
+        d.dst_filter_prop = f->c[0]->prop;
+        return;
+    }
+    unsupported("dst filter", f);
+}
+
+inline void lower_record_method(const NP &m, gg_emap_desc &d) {
+    if (m->k == NK::Ne && is_ref_at(m->c[0], NK::VarDst) && is_ref_at(m->c[1], NK::VarDst)) {
+        d.record = GG_RECORD_NE_PREV;  // a[d] != prev[d]
+        d.prev = m->c[1]->prop;
+        return;
+    }
+    unsupported("record method", m);
+}
+
+// Vertex statements -> stack program
+struct VmBuilder {
+    gg_vmap_desc d;
+    std::vector<double *> red_targets;
+    VmBuilder() { std::memset(&d, 0, sizeof(d)); }
+    int prop_slot(gg_prop *p) {
+        for (int i = 0; i < GG_VM_MAX_PROPS; ++i) {
+            if (d.props[i] == p) return i;
+            if (!d.props[i]) { d.props[i] = p; return i; }
+        }
+        return -1;
+    }
+    int const_slot(double v) {
+        for (int i = 0; i < GG_VM_MAX_CONSTS; ++i) {
+            if (i < nconst && d.consts[i] == v) return i;
+        }
+        if (nconst >= GG_VM_MAX_CONSTS) return -1;
+        d.consts[nconst] = v;
+        return nconst++;
+    }
+    int red_slot(double *h) {
+        for (size_t i = 0; i < red_targets.size(); ++i) if (red_targets[i] == h) return (int)i;
+        if (red_targets.size() >= GG_VM_MAX_REDUCE) return -1;
+        red_targets.push_back(h);
+        d.nreduce = (int)red_targets.size();
+        return d.nreduce - 1;
+    }
+    bool emit(int op, int arg = 0) {
+        if (d.ncode >= GG_VM_MAX_CODE) return false;
+        d.code[d.ncode] = (uint8_t)op;
+        d.arg[d.ncode] = (uint8_t)arg;
+        ++d.ncode;
+        return true;
+    }
+    int nconst = 0;
+    int saved_code = 0, saved_const = 0;
+    gg_vmap_desc saved;
+    std::vector<double *> saved_red;
+    void mark() { saved = d; saved_code = d.ncode; saved_const = nconst; saved_red = red_targets; }
+    void undo() { d = saved; nconst = saved_const; red_targets = saved_red; }
+
+    bool value(const NP &n) {
+        switch (n->k) {
+        case NK::Const: { int c = const_slot(n->cval); return c >= 0 && emit(GG_VM_CONST, c); }
+        case NK::VarV: return emit(GG_VM_VID);
+        case NK::Ref: {
+            if (n->c[0]->k != NK::VarV || !n->prop) unsupported("vertex operand", n);
+            int s = prop_slot(n->prop);
+            return s >= 0 && emit(GG_VM_LOAD, s) && (n->dt == GG_F32 ? emit(GG_VM_TOF32) : true);
+        }
+        case NK::Add: case NK::Sub: case NK::Mul: case NK::Div: case NK::Eq: case NK::Ne:
+        case NK::Lt: case NK::Gt: {
+            static const std::map<NK, int> ops = {{NK::Add, GG_VM_ADD}, {NK::Sub, GG_VM_SUB}, {NK::Mul, GG_VM_MUL},
+                                                  {NK::Div, GG_VM_DIV}, {NK::Eq, GG_VM_EQ}, {NK::Ne, GG_VM_NE},
+                                                  {NK::Lt, GG_VM_LT}, {NK::Gt, GG_VM_GT}};
+            if (!value(n->c[0]) || !value(n->c[1]) || !emit(ops.at(n->k))) return false;
+            // float arithmetic on float operands rounds like the reference
+            if (n->c[0]->dt == GG_F32 || n->c[1]->dt == GG_F32) {
+                if (n->k == NK::Add || n->k == NK::Sub || n->k == NK::Mul || n->k == NK::Div) return emit(GG_VM_TOF32);
+            }
+            return true;
+        }
+        case NK::Cast: {
+            if (!value(n->c[0])) return false;
+            return n->dt == GG_F32 ? emit(GG_VM_TOF32) : true;
+        }
+        case NK::Abs: return value(n->c[0]) && emit(GG_VM_ABS);
+        case NK::Iif: return value(n->c[0]) && value(n->c[1]) && value(n->c[2]) && emit(GG_VM_SELECT);
+        default: unsupported("vertex expression", n);
+        }
+    }
+    // one statement; returns false when the program is full
+    bool statement(const NP &s) {
+        mark();
+        bool ok = true;
+        if (s->k == NK::Noop) return true;
+        const NP &lhs = s->c.empty() ? s : s->c[0];
+        if (lhs->k != NK::Ref) unsupported("vertex statement", s);
+        if (lhs->host) {  // scalar accumulator: accum[_0(v)] += x
+            if (s->k != NK::AddAssign) unsupported("scalar statement", s);
+            int r = red_slot(lhs->host);
+            ok = r >= 0 && value(s->c[1]) && emit(GG_VM_REDUCE_ADD, r);
+        } else {
+            if (lhs->c[0]->k != NK::VarV) unsupported("vertex statement", s);
+            int p = prop_slot(lhs->prop);
+            ok = p >= 0;
+            if (ok) {
+                if (s->k == NK::Assign) ok = value(s->c[1]) && emit(GG_VM_STORE, p);
+                else if (s->k == NK::AddAssign) ok = emit(GG_VM_LOAD, p) && value(s->c[1]) && emit(GG_VM_ADD) && emit(GG_VM_STORE, p);
+                else if (s->k == NK::MulAssign) ok = emit(GG_VM_LOAD, p) && value(s->c[1]) && emit(GG_VM_MUL) && emit(GG_VM_STORE, p);
+                else unsupported("vertex statement", s);
+            }
+        }
+        if (!ok) undo();
+        return ok;
+    }
+};
+
+inline void run_vmap(gg_graph *g, VmBuilder &b, gg_frontier *filter, gg_frontier *out) {
+    double red[GG_VM_MAX_REDUCE] = {0, 0, 0, 0};
+    check(gg_vertexmap(g, &b.d, filter, out, red), "gg_vertexmap");
+    ++device_epoch();
+    for (size_t i = 0; i < b.red_targets.size(); ++i) *b.red_targets[i] += red[i];
+}
+
+}  // namespace graptor_b200
+
+// ---------------------------------------------------------------------------
+// Lazy executor (dsl/vertexmap.h:2120-2446): queued steps, merged passes
+// ---------------------------------------------------------------------------
+class lazy_executor {
+public:
+    explicit lazy_executor(const partitioner &part) : part_(part) {}
+
+    template <typename Fn> lazy_executor &vertex_map(Fn fn) {
+        stmts_.push_back(fn(expr::var(expr::NK::VarV)).node());
+        return *this;
+    }
+    template <typename Fn> lazy_executor &vertex_scan(Fn fn) { return vertex_map(fn); }
+    template <typename G, typename Fn>
+    lazy_executor &vertex_filter(const G &GA, frontier &F, frontier &out, Fn fn) {
+        flush();
+        graptor_b200::VmBuilder b;
+        expr::NP c = fn(expr::var(expr::NK::VarV)).node();
+        if (!b.value(c) || !b.emit(GG_VM_FILTER)) graptor_b200::unsupported("vertex filter", c);
+        gg_frontier *fin = F.all() ? nullptr : F.bind(GA.handle());
+        graptor_b200::run_vmap(GA.handle(), b, fin, out.output(GA.handle()));
+        return *this;
+    }
+    // an edgemap step queued by api::edgemap
+    lazy_executor &edge_step(std::function<void()> step) {
+        flush();
+        step();
+        return *this;
+    }
+    void materialize() { flush(); }
+
+private:
+    void flush() {
+        if (stmts_.empty()) return;
+        graptor_b200::VmBuilder b;
+        for (size_t i = 0; i < stmts_.size();) {
+            if (b.statement(stmts_[i])) {
+                ++i;
+                continue;
+            }
+            if (b.d.ncode == 0) graptor_b200::unsupported("vertex statement (too long)", stmts_[i]);
+            graptor_b200::run_vmap(part_.graph(), b, nullptr, nullptr);
+            b = graptor_b200::VmBuilder();
+        }
+        if (b.d.ncode) graptor_b200::run_vmap(part_.graph(), b, nullptr, nullptr);
+        stmts_.clear();
+    }
+    partitioner part_;
+    std::vector<expr::NP> stmts_;
+};
+
+inline lazy_executor make_lazy_executor(const partitioner &part) { return lazy_executor(part); }
+
+// maintain_copies(part, output, prev, cur): prev[v] = cur[v] on the output
+// frontier (dsl/vertexmap.h:2515-2535)
+template <typename P1, typename P2>
+void maintain_copies(const partitioner &part, frontier &output, P1 &prev, P2 &cur) {
+    graptor_b200::VmBuilder b;
+    int s = b.prop_slot(cur.handle()), t = b.prop_slot(prev.handle());
+    b.emit(GG_VM_LOAD, s);
+    b.emit(GG_VM_STORE, t);
+    if (output.isEmpty()) return;
+    graptor_b200::run_vmap(part.graph(), b, output.all() ? nullptr : output.bind(part.graph()), nullptr);
+}
+
+namespace api {
+
+// ---------------------------------------------------------------------------
+// edgemap (api.h:2143-2415)
+// ---------------------------------------------------------------------------
+struct emap_state {
+    gg_emap_desc d;
+    frontier *in = nullptr;
+    frontier *out = nullptr;
+    std::vector<expr::NP> vertexops;
+    emap_state() {
+        std::memset(&d, 0, sizeof(d));
+        d.variant = GG_VAR_AUTO;
+    }
+};
+
+inline void emap_arg(emap_state &s, const arg_config &c) {
+    s.d.threshold = c.threshold;
+    s.d.threshold_k = c.k;
+    s.d.fusion = c.fusion;
+}
+inline void emap_arg(emap_state &s, const arg_filter_src &f) {
+    s.in = f.F;
+    s.d.src_strong = f.strong;
+}
+template <typename Fn> void emap_arg(emap_state &s, const arg_filter_dst<Fn> &f) {
+    graptor_b200::lower_dst_filter(f.fn(expr::var(expr::NK::VarDst)).node(), s.d);
+}
+template <typename Fn> void emap_arg(emap_state &s, const arg_record<Fn> &r) {
+    s.out = r.out;
+    if constexpr (std::is_same<Fn, no_method>::value) {
+        s.d.record = GG_RECORD_REDUCTION;
+    } else {
+        graptor_b200::lower_record_method(r.fn(expr::var(expr::NK::VarDst)).node(), s.d);
+    }
+}
+template <typename Fn> void emap_arg(emap_state &s, const arg_relax<Fn> &r) {
+    graptor_b200::lower_relax(r.fn(expr::var(expr::NK::VarSrc), expr::var(expr::NK::VarDst),
+                                    expr::var(expr::NK::VarEdge)).node(),
+                               s.d);
+}
+template <typename Fn> void emap_arg(emap_state &s, const arg_fusion<Fn> &) {
+    s.d.fusion = 1;  // the library's async push is always min-label/level safe
+}
+inline void emap_arg(emap_state &, int) {}  // unsupported config() forms return 0 in the reference
+
+template <typename GraphType, typename... Args>
+lazy_executor edgemap(const GraphType &GA, Args &&... args) {
+    emap_state s;
+    (emap_arg(s, args), ...);
+    lazy_executor lz(GA.get_partitioner());
+    gg_graph *g = GA.handle();
+    lz.edge_step([=]() mutable {
+        gg_frontier *fin = (s.in && !s.in->all()) ? s.in->bind(g) : nullptr;
+        gg_frontier *fout = s.out ? s.out->output(g) : nullptr;
+        if (!fout) s.d.record = GG_RECORD_NONE;
+        if (s.d.relax == GG_RELAX_ADD_GATHER) s.d.record = GG_RECORD_NONE;
+        if (s.d.record == GG_RECORD_NONE && fout) {
+            // a recorded frontier with a gather relax: nothing is activated
+            graptor_b200::check(gg_frontier_clear(fout), "gg_frontier_clear");
+            fout = nullptr;
+        }
+        graptor_b200::check(gg_edgemap(g, &s.d, fin, fout, nullptr), "gg_edgemap");
+        ++graptor_b200::device_epoch();
+    });
+    return lz;
+}
+
+}  // namespace api
+
+#endif  // GRAPTOR_B200_API_H

@@ -82,3 +82,11 @@ def test_tuning_knobs_roundtrip():
     with pytest.raises(gg.GGError):  # small bin above the medium bin
         gg.tuning_set("bin_small_max", gg.tuning_get("bin_medium_max") + 1)
     gg.tuning_set("bin_small_max", small)
+
+
+def test_tuning_accepts_long_timeouts():
+    from graptor_b200 import gg
+    old = gg.tuning_get("barrier_timeout_ns")
+    gg.tuning_set("barrier_timeout_ns", 10_000_000_000)
+    assert gg.tuning_get("barrier_timeout_ns") == 10_000_000_000
+    gg.tuning_set("barrier_timeout_ns", old)
