@@ -240,6 +240,162 @@ def run_reference_arm(args, ws, rank):
 
 
 # ---------------------------------------------------------------------------
+# learned selector evaluation (held-out graphs)
+# ---------------------------------------------------------------------------
+def selector_eval(ctx, graphs):
+    """Device-driven BFS / CC with the density threshold, the learned selector
+    and each fixed variant; oracle-best = per-iteration minimum over the fixed
+    variants (BFS: every variant walks the same levels)."""
+    from graptor_b200 import gg
+    from graptor_b200.selector_train import load_selector
+    sel = load_selector(ctx)
+    old = gg.tuning_get("persistent")
+    gg.tuning_set("persistent", 7)
+    out = {"weights": "graptor_b200/data/selector.npz" if sel else None}
+    try:
+        for name, g, roots in graphs:
+            if sel:
+                gg.attach_selector(g, sel)
+            res = {}
+            for analytic in ("bfs", "cc"):
+                def run(opts, r):
+                    st = gg.RunStats()
+                    if analytic == "bfs":
+                        g.bfs_level(r, host=False, opts=opts, stats=st)
+                    else:
+                        g.cc(host=False, opts=opts, stats=st)
+                    return st
+                rs = roots if analytic == "bfs" else [0]
+                modes = {"threshold": gg.default_opts(gg.THRESH_DEFAULT if analytic == "bfs" else gg.THRESH_FRAC,
+                                                      0 if analytic == "bfs" else 5, collect=True)}
+                if sel:
+                    modes["learned"] = gg.default_opts(gg.THRESH_LEARNED, collect=True)
+                for v, vn in gg.VARIANT_NAMES.items():
+                    modes["fixed_" + vn] = gg.default_opts(variant=v, collect=True)
+                tot = {k: 0.0 for k in modes}
+                oracle = 0.0
+                for r in rs:
+                    per = {}
+                    for k, o in modes.items():
+                        run(o, r)  # warm
+                        st = run(o, r)
+                        tot[k] += st.total_ms
+                        per[k] = st
+                    fixed = [per["fixed_" + vn] for vn in gg.VARIANT_NAMES.values()]
+                    its = {f.iterations for f in fixed}
+                    if len(its) == 1 and fixed[0].iterations <= gg.MAX_ITERS:
+                        T = fixed[0].iterations
+                        it_min = sum(min(f.iter_ms[i] for f in fixed) for i in range(T))
+                        it_thr = sum(per["threshold"].iter_ms[i] for i in range(T))
+                        # whole-run overheads (launch, setup) as in the threshold run
+                        oracle += it_min + (per["threshold"].total_ms - it_thr)
+                    else:
+                        oracle = float("nan")
+                best_fixed = min(v for k, v in tot.items() if k.startswith("fixed_"))
+                d = {k: round(v / len(rs), 4) for k, v in tot.items()}
+                d["oracle_best_ms"] = round(oracle / len(rs), 4) if oracle == oracle else None
+                d["best_fixed_ms"] = round(best_fixed / len(rs), 4)
+                if sel:
+                    d["learned_vs_threshold"] = round(tot["threshold"] / tot["learned"], 3)
+                    if oracle == oracle:
+                        d["learned_over_oracle"] = round(tot["learned"] / oracle, 3)
+                res[analytic] = d
+            out[name] = res
+            if sel:
+                gg.attach_selector(g, None)
+    finally:
+        gg.tuning_set("persistent", old)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# batched traversals
+# ---------------------------------------------------------------------------
+def small_graph_batch(ctx, count, seed=2000):
+    """`count` graphs, vertex counts log-uniform in [2^10, 2^18]: R-MAT with
+    edge factor 8-32 (vertex count rounded to a power of two) and 2-D grids
+    with 4-neighbour edges, alternating."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for i in range(count):
+        lg = rng.uniform(10, 18)
+        if i % 2 == 0:
+            scale = int(round(lg))
+            parts.append(ctx.rmat(scale, int(rng.integers(8, 33)) << scale, seed + i))
+        else:
+            side = int(2 ** (lg / 2))
+            parts.append(ctx.grid(side, max(1, int(2 ** lg) // side), seed + i))
+    return parts
+
+
+def batch_eval(ctx, g, roots, hbm_peak, n_small):
+    """(a) 64-root multi-source BFS and 128-seed PPR on R-MAT 22 ef 16;
+    (b) BFS from vertex 0 and CC of `n_small` small graphs as one union."""
+    from graptor_b200 import gg
+    out = {}
+    n, m = g.n, g.m
+    r64 = [int(r) for r in roots[:64]]
+    gg.msbfs(g, r64, host=False)
+    ms = []
+    edges = 0
+    for _ in range(3):
+        st = gg.RunStats()
+        gg.msbfs(g, r64, host=False, stats=st)
+        ms.append(st.total_ms)
+        edges = st.edges_reached
+    t = float(np.median(ms))
+    seq = 0.0
+    for r in r64:
+        st = gg.RunStats()
+        g.bfs_level(r, host=False, stats=st)
+        seq += st.total_ms
+    out["msbfs64"] = {"ms": round(t, 3), "gteps": round(edges / 2.0 / (t / 1e3) / 1e9, 2),
+                      "sequential_64_bfs_ms": round(seq, 3), "speedup_vs_sequential": round(seq / t, 2)}
+    seeds = [int(r) for r in roots[:64]] + [int(r) for r in roots[:64][::-1]]
+    seeds = seeds[:128]
+    gg.ppr(g, seeds, iters=2, host=False)
+    ms = []
+    for _ in range(3):
+        st = gg.RunStats()
+        gg.ppr(g, seeds, alpha=0.15, iters=20, host=False, stats=st)
+        ms.append(st.total_ms / 20)
+    t = float(np.median(ms))
+    ppr_bytes = m * (256.0 + 4.0) + 8.0 * (n + 1) + n * 256.0 * 2
+    out["ppr128"] = {"ms_per_iter": round(t, 3), "gedges_per_s_per_iter": round(m / (t / 1e3) / 1e9, 3),
+                     "seed_edges_per_s": round(128 * m / (t / 1e3) / 1e9, 1),
+                     "frac_of_hbm": round(ppr_bytes / (t / 1e3) / 1e9 / hbm_peak, 4),
+                     "bytes_per_iter": ppr_bytes, "storage": "bf16 rows of 128 seeds, fp32 sums"}
+    # (b) many small graphs
+    t0 = time.time()
+    parts = small_graph_batch(ctx, n_small)
+    U, base = gg.graph_union(ctx, parts)
+    for p in parts:
+        p.close()
+    build_s = time.time() - t0
+    gg.bfs_level_multi(U, base[:-1], host=False)
+    U.cc(host=False)
+    bm, cm = [], []
+    for _ in range(3):
+        st = gg.RunStats()
+        gg.bfs_level_multi(U, base[:-1], host=False, stats=st)
+        bm.append(st.total_ms)
+        bst = st
+        st = gg.RunStats()
+        U.cc(host=False, stats=st)
+        cm.append(st.total_ms)
+        cst = st
+    tb, tc = float(np.median(bm)), float(np.median(cm))
+    out["small_graphs"] = {"graphs": n_small, "n": U.n, "m": U.m, "build_s": round(build_s, 1),
+                           "bfs_ms": round(tb, 3), "bfs_gteps": round(bst.edges_reached / 2.0 / (tb / 1e3) / 1e9, 2),
+                           "bfs_iterations": bst.iterations, "bfs_launches": 1,
+                           "cc_ms": round(tc, 3), "cc_iterations": cst.iterations,
+                           "cc_device_driven": bool(gg.tuning_get("persistent") & 4),
+                           "graphs_per_s": round(n_small / ((tb + tc) / 1e3), 1)}
+    U.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
 def run_ours(args, ws, rank, local):
@@ -355,6 +511,20 @@ def run_ours(args, ws, rank, local):
         prs["f32"]["frac_of_hbm"] = round(pr_bytes_f32 / (base / 1e3) / 1e9 / hbm_peak, 4)
         out["pr"] = prs
 
+    # ---- learned selector vs threshold vs oracle-best (held-out RMAT-24 and a road-like grid) ----
+    if not args.quick and not args.no_selector and rank == 0:
+        grid = ctx.grid(2896, 2896, seed=77, del_bp=100)  # 2^23 vertices, 1% edges deleted
+        out["selector"] = selector_eval(ctx, [("rmat24", g, [int(r) for r in roots[:4]]), ("grid2896", grid, [0])])
+        grid.close()
+
+    # ---- batching: multi-source BFS, 128-seed PPR (R-MAT 22), many small graphs ----
+    if not args.quick and not args.no_batch and rank == 0:
+        g22 = ctx.rmat(22, EDGE_FACTOR << 22, GRAPH_SEED)
+        off22, _ = g22.download()
+        out["batch"] = batch_eval(ctx, g22, pick_roots(np.diff(off22).astype(np.int64)), hbm_peak, args.batch_graphs)
+        out["batch"]["graph"] = "rmat22 ef16 seed 1 (msbfs64, ppr128)"
+        g22.close()
+
     # ---- e2e: public C-ABI call, graph uploaded from host memory, levels back to pinned host ----
     e2e = None
     if not args.quick:
@@ -438,6 +608,9 @@ def main():
     ap.add_argument("--cpu-roots", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="BFS only (no CC/PR/e2e)")
+    ap.add_argument("--no-selector", action="store_true", help="skip the learned-selector evaluation")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-traversal measurements")
+    ap.add_argument("--batch-graphs", type=int, default=2000, help="small graphs in the union workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     ws, rank, local = dist_setup(args)

@@ -22,7 +22,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
               "--expt-relaxed-constexpr", "-I" + INCLUDE, "-I" + CSRC]
 
-SOURCES = ["gg_core.cu", "gg_emap.cu", "gg_pr.cu", "gg_vmap.cu", "gg_select.cu", "gg_noalloc.cu", "gg_persist.cu"]
+SOURCES = ["gg_core.cu", "gg_emap.cu", "gg_pr.cu", "gg_vmap.cu", "gg_select.cu", "gg_noalloc.cu", "gg_persist.cu", "gg_batch.cu", "gg_tune.cu"]
 
 
 def nvcc() -> str:

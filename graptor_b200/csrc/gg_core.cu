@@ -737,6 +737,7 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
         return GG_OK;
     }
     if (v > (int64_t)1 << 31) return GG_ERR_ARG;
+    const Tuning saved = t;  // an invalid combination leaves every knob as it was
     if (k == "bin_small_max") t.bin_small_max = (uint32_t)v;
     else if (k == "bin_medium_max") t.bin_medium_max = (uint32_t)v;
     else if (k == "pull_k" && v >= 1 && v <= 1024) t.pull_k = (int)v;
@@ -749,7 +750,10 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "persistent" && v <= 7) t.persistent = (int)v;
     else if (k == "barrier_timeout_ns" && v >= 1) t.barrier_timeout_ns = (unsigned long long)v;
     else return GG_ERR_ARG;
-    if (t.bin_small_max > t.bin_medium_max) return GG_ERR_ARG;
+    if (t.bin_small_max > t.bin_medium_max) {
+        t = saved;
+        return GG_ERR_ARG;
+    }
     return GG_OK;
 }
 
@@ -804,6 +808,34 @@ gg_status gg_graph_upload(gg_ctx *ctx, uint32_t n, uint64_t m, const uint64_t *o
     *out = g;
     return GG_OK;
 }
+
+}  // extern "C"
+
+namespace gg {
+// Takes ownership of a CSR already in device memory (off: n+1, adj: m).
+gg_status graph_adopt_device_csr(gg_ctx *ctx, uint32_t n, uint64_t m, uint64_t *off, uint32_t *adj, int symmetric,
+                                 gg_graph **out) {
+    *out = nullptr;
+    gg_graph *g = new (std::nothrow) gg_graph;
+    if (!g) {
+        cudaFree(off);
+        cudaFree(adj);
+        return GG_ERR_OOM;
+    }
+    g->ctx = ctx;
+    g->n = n;
+    g->m = m;
+    g->symmetric = symmetric ? 1 : 0;
+    g->off = off;
+    g->adj = adj;
+    gg_status s = graph_finish(g);
+    if (s != GG_OK) { graph_free(g); return s; }
+    *out = g;
+    return GG_OK;
+}
+}  // namespace gg
+
+extern "C" {
 
 gg_status gg_graph_read_bin(gg_ctx *ctx, const char *path, int symmetric, gg_graph **out) {
     if (!ctx || !path || !out) return GG_ERR_ARG;

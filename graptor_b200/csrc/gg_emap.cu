@@ -35,6 +35,7 @@
 #include <cstring>
 #include <type_traits>
 
+#include "gg_batch.h"
 #include "gg_internal.cuh"
 
 namespace gg {
@@ -559,6 +560,14 @@ __global__ void k_copy_prev(const uint32_t *b0, const uint32_t *b1, const uint32
     }
 }
 
+__global__ void k_scatter_zero_i32(int32_t *a, int32_t *b, const uint32_t *idx, uint32_t k) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) {
+        a[idx[i]] = 0;
+        b[idx[i]] = 0;
+    }
+}
+
 __global__ void k_iota_u32(uint32_t *a, uint32_t n) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t stride = gridDim.x * blockDim.x;
@@ -1065,6 +1074,65 @@ gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop
     }
     if (host_level) GG_CHECK(gg_prop_download(level, host_level));
     return gg_ctx_sync(g->ctx);
+}
+
+gg_status gg_bfs_level_multi(gg_graph *g, const uint32_t *roots, uint32_t k, const gg_run_opts *o, gg_prop *level,
+                             int32_t *host_level, gg_run_stats *st) {
+    if (!g || (k && !roots)) return GG_ERR_ARG;
+    if (level && (level->g != g || level->t != GG_I32)) return set_error(g->ctx, GG_ERR_ARG, "level must be an I32 property of g");
+    gg_ctx *ctx = g->ctx;
+    // distinct, in-range roots
+    std::vector<uint32_t> r(roots, roots + k);
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+    if (!r.empty() && r.back() >= g->n) return set_error(ctx, GG_ERR_ARG, "gg_bfs_level_multi: root out of range");
+    gg_run_opts opt;
+    default_opts(o, &opt, GG_THRESH_DEFAULT, 0);
+    if (!level) GG_CHECK(tmp_prop(g, 0, GG_I32, &level));
+    gg_prop *prev;
+    GG_CHECK(tmp_prop(g, 1, GG_I32, &prev));
+    if (st) memset(st, 0, sizeof(*st));
+    uint64_t k0 = ctx->launches;
+    // roots staged in the graph scratch space past the traversal's merge
+    // scratch (n + grid + 1 words, grid <= 16 CTAs per SM), so that the
+    // traversal never regrows the buffer under them
+    const size_t roots_at = ((size_t)g->n + (size_t)ctx->sm_count * 16 + 64) * 8;
+    void *scr;
+    GG_CHECK(graph_scratch(g, roots_at + r.size() * 4 + 256, &scr));
+    uint32_t *d_roots = (uint32_t *)((char *)scr + roots_at);
+    if (!r.empty())
+        GG_CUDA(ctx, cudaMemcpyAsync(d_roots, r.data(), r.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
+    RunTimer tm(ctx);
+    int32_t inf = (int32_t)g->n + 1;
+    GG_CHECK(gg_prop_fill(level, &inf));
+    GG_CHECK(gg_prop_fill(prev, &inf));
+    if (!r.empty()) {
+        k_scatter_zero_i32<<<((unsigned)r.size() + 255) / 256, 256, 0, ctx->stream>>>(
+            (int32_t *)level->d, (int32_t *)prev->d, d_roots, (uint32_t)r.size());
+        GG_LAUNCHED(ctx);
+    }
+    gg_emap_desc desc;
+    memset(&desc, 0, sizeof(desc));
+    desc.relax = GG_RELAX_MIN_PLUS1_I32;
+    desc.a = level;
+    desc.dst_filter = GG_FILTER_GT_CONST;
+    desc.src_level_sync = 1;
+    desc.record = GG_RECORD_NE_PREV;
+    desc.prev = prev;
+    desc.threshold = opt.threshold;
+    desc.threshold_k = opt.threshold_k;
+    desc.variant = opt.variant;
+    // one device-driven launch for all roots
+    int iters = 0;
+    GG_CHECK(persistent_traverse(g, desc, 1, false, 0, opt, st, &iters, -1, -1, d_roots, (uint32_t)r.size()));
+    double ms = tm.stop();
+    if (st) {
+        st->iterations = iters;
+        st->total_ms = ms;
+        st->kernels = ctx->launches - k0;
+    }
+    if (host_level) GG_CHECK(gg_prop_download(level, host_level));
+    return gg_ctx_sync(ctx);
 }
 
 gg_status gg_bfs_parent(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop *parent,

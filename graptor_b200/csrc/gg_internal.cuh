@@ -171,7 +171,10 @@ uint32_t bin_of_degree(uint64_t deg);
 gg_status build_heavy_rows(gg_graph *g);
 gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, bool start_all, uint32_t root,
                               const gg_run_opts &opt, gg_run_stats *stats, int *iters_out,
-                              int force_iter = -1, int force_variant = -1);
+                              int force_iter = -1, int force_variant = -1,
+                              const uint32_t *d_roots = nullptr, uint32_t nroots = 0);
+gg_status graph_adopt_device_csr(gg_ctx *ctx, uint32_t n, uint64_t m, uint64_t *off, uint32_t *adj, int symmetric,
+                                 gg_graph **out);
 gg_status graph_gini(gg_graph *g, float *out);
 void selector_features(float *x, double nactv, double nacte, double unreached, int iter, double n, double m,
                        float gini);

@@ -673,6 +673,10 @@ __device__ int choose_variant(const PArgs &P, int iter, unsigned long long nactv
                 int best = 0;
                 for (int v = 1; v < GG_SEL_VARIANTS; ++v)
                     if (o[v] < o[best]) best = v;
+                // the threshold's choice stands unless the network predicts
+                // a clear gain over it
+                const int tv = (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+                if (!(o[best] < o[tv] - mlp::kSelMargin)) best = tv;
                 if (threadIdx.x == 0) *s_choice = best;
             }
             __syncthreads();
@@ -798,6 +802,21 @@ __global__ void k_traverse_init(PFront F, uint32_t root, const uint64_t *off, ui
     }
 }
 
+// Initial frontier from a list of distinct roots (multi-root traversals).
+__global__ void k_traverse_init_list(PFront F, const uint32_t *roots, uint32_t k, const uint64_t *off, uint32_t smax,
+                                     uint32_t mmax) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < k; i += gridDim.x * blockDim.x) {
+        const uint32_t r = roots[i];
+        const uint64_t deg = off[r + 1] - off[r];
+        const int b = deg <= smax ? 0 : (deg <= mmax ? 1 : 2);
+        const unsigned long long slot = atomicAdd(&F.cnt[FC_BIN0 + b], 1ull);
+        F.bins[b][slot] = r;
+        atomicAdd(&F.cnt[FC_NACTV], 1ull);
+        atomicAdd(&F.cnt[FC_NACTE], (unsigned long long)deg);
+        atomicOr(&F.bitmap[r >> 5], 1u << (r & 31));
+    }
+}
+
 // Host side -----------------------------------------------------------------
 template <int R>
 static const void *traverse_kernel() { return (const void *)k_traverse<R>; }
@@ -806,7 +825,7 @@ const void *selector_weights(gg_graph *g);
 
 gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, bool start_all, uint32_t root,
                               const gg_run_opts &opt, gg_run_stats *stats, int *iters_out, int force_iter,
-                              int force_variant) {
+                              int force_variant, const uint32_t *d_roots, uint32_t nroots) {
     gg_ctx *ctx = g->ctx;
     cudaStream_t s = ctx->stream;
     const Tuning &t = tuning();
@@ -882,7 +901,13 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
         uint64_t cnt[2] = {g->n, g->m};
         GG_CUDA(ctx, cudaMemcpyAsync(P.fr[0].cnt, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
     } else {
-        k_traverse_init<<<1, 1, 0, s>>>(P.fr[0], root, g->off, P.smax, P.mmax, 1);
+        if (d_roots) {
+            if (nroots)
+                k_traverse_init_list<<<(nroots + 255) / 256, 256, 0, s>>>(P.fr[0], d_roots, nroots, g->off, P.smax,
+                                                                          P.mmax);
+        } else {
+            k_traverse_init<<<1, 1, 0, s>>>(P.fr[0], root, g->off, P.smax, P.mmax, 1);
+        }
         GG_LAUNCHED(ctx);
         int one = 1;
         GG_CUDA(ctx, cudaMemcpyAsync(&st->has_list[0], &one, sizeof(int), cudaMemcpyHostToDevice, s));

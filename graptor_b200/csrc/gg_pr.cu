@@ -35,6 +35,9 @@
 #include <cmath>
 #include <cstring>
 
+#include <cstdio>
+#include <cstdlib>
+
 #include "gg_internal.cuh"
 
 namespace gg {
@@ -43,6 +46,14 @@ namespace gg {
 // Storage formats
 // ---------------------------------------------------------------------------
 template <int DT> struct Store;
+// Rank / accumulator type of the vertex passes: double for the FP64 variant
+// (PR_vary's FP64 run_prec instantiation), float otherwise.
+template <int DT> using XT = typename std::conditional<DT == GG_F64, double, float>::type;
+template <> struct Store<GG_F64> {
+    using T = double;
+    __device__ static double dec(T v) { return v; }
+    __device__ static T enc(double f) { return f; }
+};
 template <> struct Store<GG_F32> {
     using T = float;
     __device__ static float dec(T v) { return v; }
@@ -293,8 +304,8 @@ k_pr_heavy_finalize(HeavyRows H, const typename std::conditional<ACC64, double, 
 
 template <int DT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
-k_pr_update(const float *__restrict__ y, float *__restrict__ x, typename Store<DT>::T *contrib,
-            const uint64_t *__restrict__ off, uint32_t n, float damp, int renorm_f32, PrState *st) {
+k_pr_update(const XT<DT> *__restrict__ y, XT<DT> *__restrict__ x, typename Store<DT>::T *contrib,
+            const uint64_t *__restrict__ off, uint32_t n, float damp, double damp64, int renorm_f32, PrState *st) {
     using S = Store<DT>;
     if (st->done) return;
     const double s1 = st->s1;
@@ -306,6 +317,18 @@ k_pr_update(const float *__restrict__ y, float *__restrict__ x, typename Store<D
     double dl = 0;
     float cm = 0.0f;
     const uint32_t stride = gridDim.x * BLOCK;
+    if constexpr (DT == GG_F64) {
+        // all double: y += w, renormalise by 1/s, contrib = d * x / deg
+        for (uint32_t v = blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
+            const double yv = (y[v] + w) * wf64;
+            dl += fabs(x[v] - yv);
+            x[v] = yv;
+            const uint64_t deg = off[v + 1] - off[v];
+            contrib[v] = damp64 * yv / (double)deg;
+        }
+        (void)wf32;
+        (void)enc_scale;
+    } else
     for (uint32_t v = blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
         float yv = (float)((double)y[v] + w);
         yv = renorm_f32 ? yv * wf32 : (float)((double)yv * wf64);
@@ -346,12 +369,26 @@ __global__ void k_pr_finish(PrState *st, int dt) {
 
 // Initial x = 1/n, contrib = d*x/deg (PRv.C:155-182); first pass finds the max.
 template <int DT, int BLOCK>
-__global__ void k_pr_init(float *x, typename Store<DT>::T *contrib, const uint64_t *off, uint32_t n,
-                          float damp, PrState *st, int pass) {
+__global__ void k_pr_init(XT<DT> *x, typename Store<DT>::T *contrib, const uint64_t *off, uint32_t n,
+                          float damp, double damp64, PrState *st, int pass) {
     using S = Store<DT>;
     const float x0 = 1.0f / (float)n;
     float cm = 0.0f;
     const uint32_t stride = gridDim.x * BLOCK;
+    if constexpr (DT == GG_F64) {
+        if (pass == 1)
+            for (uint32_t v = blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
+                const double xd = 1.0 / (double)n;
+                x[v] = xd;
+                contrib[v] = damp64 * xd / (double)(off[v + 1] - off[v]);
+            }
+        if (pass == 1 && blockIdx.x == 0 && threadIdx.x == 0) {
+            st->scale = 1.0f;
+            st->scale_inv = 1.0f;
+            st->cmax = 0.0f;
+        }
+        return;
+    }
     const float scale = pass == 1 ? scale_for(DT, st->cmax) : 1.0f;
     for (uint32_t v = blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
         const uint64_t deg = off[v + 1] - off[v];
@@ -413,26 +450,40 @@ static gg_status gather_launch(gg_graph *g, const typename Store<DT>::T *contrib
     return GG_OK;
 }
 
+// Damping of the FP64 variant: the shortest decimal that rounds to the float
+// parameter (0.85f -> 0.85), as the double-precision reference uses it.
+static double damping_f64(float d) {
+    char buf[32];
+    for (int prec = 1; prec <= 9; ++prec) {
+        std::snprintf(buf, sizeof(buf), "%.*g", prec, (double)d);
+        const double v = std::strtod(buf, nullptr);
+        if ((float)v == d) return v;
+    }
+    return (double)d;
+}
+
 template <int DT>
-static gg_status pr_run(gg_graph *g, const gg_pr_params *p, float *x, float *y, void *contrib,
+static gg_status pr_run(gg_graph *g, const gg_pr_params *p, XT<DT> *x, XT<DT> *y, void *contrib,
                         PrState *st, void *partial) {
     gg_ctx *ctx = g->ctx;
     cudaStream_t s = ctx->stream;
     using T = typename Store<DT>::T;
     const uint32_t n = g->n;
-    const unsigned gw = pr_grid(ctx, (uint64_t)((n + 31) / 32) * 32);
     const unsigned gv = pr_grid(ctx, n);
-    k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, n, p->damping, st, 0);
+    const double d64 = damping_f64(p->damping);
+    k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, n, p->damping, d64, st, 0);
     GG_LAUNCHED(ctx);
-    k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, n, p->damping, st, 1);
+    k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, n, p->damping, d64, st, 1);
     GG_LAUNCHED(ctx);
-    (void)gw;
+    float *yf = DT == GG_F64 ? nullptr : (float *)y;
+    double *yd = DT == GG_F64 ? (double *)y : nullptr;
     for (int it = 0; it < p->maxiter; ++it) {
-        if (p->accum_f64)
-            GG_CHECK((gather_launch<DT, true, false>(g, (const T *)contrib, y, nullptr, st, 1.0f, partial)));
+        if (p->accum_f64 || DT == GG_F64)
+            GG_CHECK((gather_launch<DT, true, false>(g, (const T *)contrib, yf, yd, st, 1.0f, partial)));
         else
-            GG_CHECK((gather_launch<DT, false, false>(g, (const T *)contrib, y, nullptr, st, 1.0f, partial)));
-        k_pr_update<DT, kBlock><<<gv, kBlock, 0, s>>>(y, x, (T *)contrib, g->off, n, p->damping, p->renorm_f32, st);
+            GG_CHECK((gather_launch<DT, false, false>(g, (const T *)contrib, yf, yd, st, 1.0f, partial)));
+        k_pr_update<DT, kBlock><<<gv, kBlock, 0, s>>>(y, x, (T *)contrib, g->off, n, p->damping, d64,
+                                                      p->renorm_f32, st);
         GG_LAUNCHED(ctx);
         k_pr_finish<<<1, 1, 0, s>>>(st, DT);
         GG_LAUNCHED(ctx);
@@ -482,19 +533,22 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
     if (!g || !p) return GG_ERR_ARG;
     gg_ctx *ctx = g->ctx;
     if (p->maxiter < 0 || p->maxiter > GG_MAX_ITERS) return set_error(ctx, GG_ERR_ARG, "maxiter out of range");
-    if (x && (x->g != g || x->t != GG_F32)) return set_error(ctx, GG_ERR_ARG, "x must be an F32 property of g");
     const int dt = p->contrib_dtype;
     if (dt != GG_F32 && dt != GG_BF16 && dt != GG_F16 && dt != GG_FP8E4M3 && dt != GG_CFP_6_10 &&
-        dt != GG_BF16_TRUNC)
+        dt != GG_BF16_TRUNC && dt != GG_F64)
         return set_error(ctx, GG_ERR_UNSUPPORTED, "contribution dtype");
+    const gg_dtype xt = dt == GG_F64 ? GG_F64 : GG_F32;
+    if (x && (x->g != g || x->t != xt))
+        return set_error(ctx, GG_ERR_ARG, "x must be an F32 property of g (F64 for the FP64 variant)");
     if (g->n == 0) return GG_OK;
     gg_prop *xp = x, *tmpx = nullptr;
     if (!xp) {
-        GG_CHECK(gg_prop_create(g, GG_F32, &tmpx));
+        GG_CHECK(gg_prop_create(g, xt, &tmpx));
         xp = tmpx;
     }
-    // scratch: y (f32), contrib (up to 4 B), state
-    const size_t nb = (((size_t)g->n + 1) * 4 + 255) / 256 * 256;
+    // scratch: y (f32 / f64), contrib (up to 8 B), state
+    const size_t esz = dt == GG_F64 ? 8 : 4;
+    const size_t nb = (((size_t)g->n + 1) * esz + 255) / 256 * 256;
     const size_t sb = (sizeof(PrState) + 255) / 256 * 256;
     void *base = nullptr;
     gg_status s = graph_scratch(g, 2 * nb + sb + (g->heavy.nchunks + 1) * 8, &base);
@@ -515,6 +569,7 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
     cudaError_t e = cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
         switch (dt) {
+        case GG_F64: s = pr_run<GG_F64>(g, p, (double *)xp->d, (double *)base, contrib, st, partial); break;
         case GG_F32: s = pr_run<GG_F32>(g, p, (float *)xp->d, y, contrib, st, partial); break;
         case GG_BF16: s = pr_run<GG_BF16>(g, p, (float *)xp->d, y, contrib, st, partial); break;
         case GG_F16: s = pr_run<GG_F16>(g, p, (float *)xp->d, y, contrib, st, partial); break;
@@ -548,7 +603,15 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
         }
         stats->scanned_edges = (uint64_t)fin.iters * g->m;
     }
-    if (s == GG_OK && host_x) s = gg_prop_download(xp, host_x);
+    if (s == GG_OK && host_x) {
+        if (xt == GG_F64) {  // the float copy of the double ranks
+            std::vector<double> hx(g->n);
+            s = gg_prop_download(xp, hx.data());
+            for (uint32_t v = 0; s == GG_OK && v < g->n; ++v) host_x[v] = (float)hx[v];
+        } else {
+            s = gg_prop_download(xp, host_x);
+        }
+    }
     if (tmpx) gg_prop_destroy(tmpx);
     return s;
 }

@@ -386,7 +386,7 @@ void selector_features(float *x, double nactv, double nacte, double unreached, i
                        float gini) {
     x[0] = (float)(std::log2(1.0 + nactv) / 32);
     x[1] = (float)(std::log2(1.0 + nacte) / 40);
-    x[2] = (float)(std::log2(1.0 + unreached) / 32);
+    x[2] = (float)(std::log2(1.0 + std::max(0.0, unreached)) / 32);
     x[3] = (float)(std::min(iter, 255) / 64.0);
     x[4] = (float)(std::log2(1.0 + (n > 0 ? m / n : 0)) / 8);
     x[5] = gini;
@@ -429,7 +429,10 @@ int learned_select(gg_graph *g, uint64_t nactv, uint64_t nacte, int iter, bool c
         o[v] = a;
         if (o[v] < o[best]) best = v;
     }
-    return best;  // variant ids are the output order
+    // variant ids are the output order; the threshold's choice stands unless
+    // the network predicts a clear gain over it
+    const int tv = (nactv + nacte) <= (g->m / 20) ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+    return o[best] < o[tv] - mlp::kSelMargin ? best : tv;
 }
 
 }  // namespace gg
@@ -480,9 +483,11 @@ extern "C" gg_status gg_selector_collect(gg_graph *g, int analytic, uint32_t roo
             for (int rep = 0; rep < 2; ++rep) {  // min of two runs: less timing noise
                 s = run(&rs);
                 if (s != GG_OK) { g->force_iter = -1; return s; }
-                best = std::min(best, rs.iter_ms[it]);
+                // CC's push steps race (a label can travel several hops in one
+                // step), so a run may converge before iteration `it`: no sample
+                if (rs.iterations > it && rs.iter_ms[it] > 0) best = std::min(best, rs.iter_ms[it]);
             }
-            y[v] = (float)std::log2(std::max(best * 1e3, 1e-3));
+            y[v] = best < 1e30 ? (float)std::log2(best * 1e3) : std::nanf("");
         }
         ++*nrec;
     }

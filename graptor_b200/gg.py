@@ -343,6 +343,14 @@ class Graph:
                  damping=0.85, x: "Prop" = None, host: bool = True, stats: RunStats = None):
         p = PrParams(maxiter=maxiter, tol=tol, damping=damping, contrib_dtype=contrib,
                      accum_f64=int(accum_f64), renorm_f32=int(renorm_f32))
+        if contrib == F64 and host and x is None:
+            # the FP64 variant: return the double ranks
+            xp = self.prop(F64)
+            self.ctx.check(lib().gg_pagerank(self.h, C.byref(p), xp.h, None,
+                                             C.byref(stats) if stats is not None else None), "gg_pagerank")
+            out = xp.download()
+            xp.close()
+            return out
         out = np.empty(self.n, dtype=np.float32) if host else None
         self.ctx.check(lib().gg_pagerank(self.h, C.byref(p), x.h if x else None,
                                          _p(out) if host else None,
@@ -581,3 +589,99 @@ def selector_collect(g: "Graph", analytic: int, root: int = 0, max_samples: int 
 
 def attach_selector(g: "Graph", sel: "Selector | None"):
     g.ctx.check(_sel_lib().gg_graph_set_selector(g.h, sel.h if sel else None), "gg_graph_set_selector")
+
+
+# ---------------------------------------------------------------------------
+# Batched traversals (include/gg_batch.h)
+# ---------------------------------------------------------------------------
+MSBFS_MAX_ROOTS, PPR_MAX_SEEDS = 64, 128
+
+
+def _batch_lib():
+    L = lib()
+    if not getattr(L, "_batch_bound", False):
+        vp, u32 = C.c_void_p, C.c_uint32
+        L.gg_msbfs.argtypes = [vp, vp, C.c_int, vp, C.POINTER(RunStats)]
+        L.gg_ppr.argtypes = [vp, vp, C.c_int, C.c_float, C.c_int, vp, C.POINTER(RunStats)]
+        L.gg_graph_union.argtypes = [vp, vp, C.c_int, C.POINTER(vp), vp]
+        L.gg_bfs_level_multi.argtypes = [vp, vp, u32, C.POINTER(RunOpts), vp, vp, C.POINTER(RunStats)]
+        for n in ["gg_msbfs", "gg_ppr", "gg_graph_union", "gg_bfs_level_multi"]:
+            getattr(L, n).restype = C.c_int
+        L._batch_bound = True
+    return L
+
+
+def msbfs(g: Graph, roots, host: bool = True, stats: RunStats = None):
+    """BFS levels from up to 64 roots in one launch: [n][k] int32 (or None)."""
+    r = np.ascontiguousarray(roots, dtype=np.uint32)
+    out = np.empty((g.n, len(r)), dtype=np.int32) if host else None
+    g.ctx.check(_batch_lib().gg_msbfs(g.h, _p(r), len(r), _p(out) if host else None,
+                                      C.byref(stats) if stats is not None else None), "gg_msbfs")
+    return out
+
+
+def ppr(g: Graph, seeds, alpha: float = 0.15, iters: int = 20, host: bool = True, stats: RunStats = None):
+    """Personalized PageRank for up to 128 seeds (bfloat16 storage): [n][k] float32."""
+    s = np.ascontiguousarray(seeds, dtype=np.uint32)
+    out = np.empty((g.n, len(s)), dtype=np.float32) if host else None
+    g.ctx.check(_batch_lib().gg_ppr(g.h, _p(s), len(s), alpha, iters, _p(out) if host else None,
+                                    C.byref(stats) if stats is not None else None), "gg_ppr")
+    return out
+
+
+def graph_union(ctx: Context, parts):
+    """Disjoint union of graphs: (Graph, vertex_base[k+1])."""
+    hs = (C.c_void_p * len(parts))(*[p.h.value if isinstance(p.h, C.c_void_p) else p.h for p in parts])
+    base = np.empty(len(parts) + 1, dtype=np.uint32)
+    h = C.c_void_p()
+    ctx.check(_batch_lib().gg_graph_union(ctx.h, hs, len(parts), C.byref(h), _p(base)), "gg_graph_union")
+    return Graph(ctx, h), base
+
+
+def bfs_level_multi(g: Graph, roots, host: bool = True, opts: RunOpts = None, stats: RunStats = None):
+    """BFS levels with every root at level 0, one device-driven launch."""
+    r = np.ascontiguousarray(roots, dtype=np.uint32)
+    out = np.empty(g.n, dtype=np.int32) if host else None
+    g.ctx.check(_batch_lib().gg_bfs_level_multi(g.h, _p(r), len(r), C.byref(opts) if opts else None, None,
+                                                _p(out) if host else None,
+                                                C.byref(stats) if stats is not None else None),
+                "gg_bfs_level_multi")
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Autotuner (include/gg_tune.h)
+# ---------------------------------------------------------------------------
+TUNE_BFS, TUNE_CC, TUNE_PR = 1, 2, 4
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("initial_ms", C.c_double), ("best_ms", C.c_double), ("evaluations", C.c_int),
+                ("best", C.c_char * 512)]
+
+
+def _tune_lib():
+    L = lib()
+    if not getattr(L, "_tune_bound", False):
+        L.gg_graph_retune.argtypes = [C.c_void_p]
+        L.gg_autotune.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                  C.POINTER(TuneResult)]
+        L.gg_graph_retune.restype = C.c_int
+        L.gg_autotune.restype = C.c_int
+        L._tune_bound = True
+    return L
+
+
+def graph_retune(g: Graph):
+    g.ctx.check(_tune_lib().gg_graph_retune(g.h), "gg_graph_retune")
+
+
+def autotune(g: Graph, analytics: int = TUNE_BFS | TUNE_CC, roots=(), passes: int = 2, reps: int = 2) -> dict:
+    """Coordinate-descent tuning on g; the chosen knobs are set and returned."""
+    r = np.ascontiguousarray(roots, dtype=np.uint32)
+    res = TuneResult()
+    g.ctx.check(_tune_lib().gg_autotune(g.h, analytics, _p(r) if len(r) else None, len(r), passes, reps,
+                                        C.byref(res)), "gg_autotune")
+    best = dict(kv.split("=") for kv in res.best.decode().split(",") if kv)
+    return dict(initial_ms=res.initial_ms, best_ms=res.best_ms, evaluations=res.evaluations,
+                knobs={k: int(v) for k, v in best.items()})

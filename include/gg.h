@@ -323,7 +323,9 @@ typedef struct gg_pr_params {
     int maxiter;        /* PRv -pr:maxiter (default 100) */
     double tol;         /* stop when L1 residual <= tol (PRv: 1e-7) */
     float damping;      /* 0.85 */
-    int contrib_dtype;  /* gg_dtype of the stored contribution: F32, BF16, F16, FP8E4M3, CFP_6_10, BF16_TRUNC */
+    int contrib_dtype;  /* gg_dtype of the stored contribution: F32, BF16, F16, FP8E4M3, CFP_6_10, BF16_TRUNC,
+                           or F64 (PR_vary's FP64 variant: ranks, sums and contributions all double, x an
+                           F64 property, damping taken as the shortest decimal of the float) */
     int accum_f64;      /* accumulate gathers in double (PRv) rather than float */
     int renorm_f32;     /* PRv renormalises by float(1)/float(s); PR_vary by double */
 } gg_pr_params;

@@ -7,8 +7,9 @@
  * every iteration of a device-driven traversal, predicts the time of each
  * traversal variant from frontier statistics already on the device and runs
  * the fastest; the threshold stays the fallback (no selector attached, or
- * GG_THRESH_DEFAULT/FRAC).  Every variant computes the same result, so the
- * choice changes time only.
+ * GG_THRESH_DEFAULT/FRAC), and its choice stands unless the network
+ * predicts the other variant at least 13% faster.  Every variant computes
+ * the same result, so the choice changes time only.
  *
  * Network: 10 -> 32 -> 32 -> 4, ReLU, output = predicted log2 of the
  * variant's iteration time in microseconds (push_sparse, push_merge,
@@ -53,7 +54,9 @@ GG_API gg_status gg_selector_train(gg_selector *s, const float *X, const float *
  * device-driven, once per (sampled iteration, variant), every iteration
  * using the threshold's choice except the sampled one, and records per
  * sampled iteration its features X[k][10] and the measured log2 us of each
- * variant Y[k][4].  At most `max_samples` iterations are sampled (spread
+ * variant Y[k][4] (NaN where the forced run ended before that iteration,
+ * which CC's racing push steps can cause).  At most `max_samples`
+ * iterations are sampled (spread
  * evenly); *nrec receives the record count (<= cap). */
 GG_API gg_status gg_selector_collect(gg_graph *g, int analytic, uint32_t root, int max_samples,
                                      float *X, float *Y, int cap, int *nrec);

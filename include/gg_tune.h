@@ -1,7 +1,7 @@
 /*
  * gg_tune.h -- tuning knobs of libgg.so (degree-bin thresholds, chunk sizes,
- * per-lane scan depths, kernel variants).  Set by the project's autotuner
- * (graptor_b200/autotune.py) or by hand; values are process-wide.
+ * per-lane scan depths, grid sizes, kernel variants) and the autotuner that
+ * picks them.  Values are process-wide.
  *
  * No reference counterpart: Graptor fixes its equivalents at compile time
  * (EMAP_BLOCK_SIZE, include/graptor/dsl/edgemap.h:29-31; the edge-chunk
@@ -9,14 +9,14 @@
  *
  * Names: bin_small_max, bin_medium_max (sparse-push degree bins),
  * pull_k, push_k (edges a lane scans alone before its warp helps),
- * heavy_deg, heavy_chunk (CSC rows chunked for gathers; applies to graphs
- * created afterwards), large_chunk (push: edges per chunk of a hub row),
- * pr_stream (1: warp-streamed segmented PageRank gather, 0: per-row),
- * persistent (bit mask: 1 BFS levels, 2 BFS parents, 4 CC run as one
- * device-driven cooperative launch; otherwise one launch per iteration from
- * the host), barrier_timeout_ns
- * (how long a CTA of a persistent run waits at a grid barrier before it
- * reports GG_ERR_TIMEOUT).
+ * heavy_deg, heavy_chunk (CSC rows chunked for gathers; apply to graphs
+ * created afterwards or after gg_graph_retune), large_chunk (push: edges
+ * per chunk of a hub row), blocks_per_sm (CTAs per SM of the grid-stride
+ * kernels), pr_stream (1: warp-streamed segmented PageRank gather, 0:
+ * per-row), persistent (bit mask: 1 BFS levels, 2 BFS parents, 4 CC run as
+ * one device-driven cooperative launch; otherwise one launch per iteration
+ * from the host), barrier_timeout_ns (how long a CTA of a persistent run
+ * waits at a grid barrier before it reports GG_ERR_TIMEOUT).
  */
 #ifndef GG_TUNE_H
 #define GG_TUNE_H
@@ -26,6 +26,27 @@ extern "C" {
 #endif
 GG_API gg_status gg_tuning_set(const char *name, int64_t value);
 GG_API gg_status gg_tuning_get(const char *name, int64_t *value);
+
+/* Rebuild the graph's tuning-dependent tables (chunked heavy rows, per-word
+ * cost prefixes) with the current heavy_deg / heavy_chunk. */
+GG_API gg_status gg_graph_retune(gg_graph *g);
+
+/* Autotuner.  Coordinate descent over the knobs above on graph g: each knob
+ * in turn takes each of its candidate values while the others stay at their
+ * best so far; a candidate is kept when the objective (the sum of the
+ * analytics' device times, each the minimum of `reps` runs) drops by more
+ * than 1%.  `passes` sweeps over all knobs.  Every candidate's BFS levels
+ * and CC labels are compared with the first run's and must be identical
+ * (GG_ERR_STATE otherwise).  On return the best values are set. */
+enum { GG_TUNE_BFS = 1, GG_TUNE_CC = 2, GG_TUNE_PR = 4 };
+typedef struct gg_tune_result {
+    double initial_ms;   /* objective with the values on entry */
+    double best_ms;      /* objective with the chosen values */
+    int evaluations;     /* objective evaluations */
+    char best[512];      /* "name=value,..." of every knob tuned */
+} gg_tune_result;
+GG_API gg_status gg_autotune(gg_graph *g, int analytics, const uint32_t *roots, int nroots, int passes, int reps,
+                             gg_tune_result *out);
 #ifdef __cplusplus
 }
 #endif

@@ -81,7 +81,21 @@ def test_tuning_knobs_roundtrip():
     small = gg.tuning_get("bin_small_max")
     with pytest.raises(gg.GGError):  # small bin above the medium bin
         gg.tuning_set("bin_small_max", gg.tuning_get("bin_medium_max") + 1)
-    gg.tuning_set("bin_small_max", small)
+    assert gg.tuning_get("bin_small_max") == small  # a rejected set changes nothing
+
+
+def test_autotune_apply_orders_the_bin_pair():
+    from graptor_b200 import autotune, gg
+    old = {k: gg.tuning_get(k) for k in ("bin_small_max", "bin_medium_max", "pull_k")}
+    try:
+        # both directions: the new small bin above the old medium one, and back
+        autotune.apply({"bin_small_max": 4096, "bin_medium_max": 8192, "pull_k": 4})
+        assert (gg.tuning_get("bin_small_max"), gg.tuning_get("bin_medium_max")) == (4096, 8192)
+        autotune.apply({"bin_medium_max": 64, "bin_small_max": 16})
+        assert (gg.tuning_get("bin_small_max"), gg.tuning_get("bin_medium_max")) == (16, 64)
+        assert gg.tuning_get("pull_k") == 4
+    finally:
+        autotune.apply(old)
 
 
 def test_tuning_accepts_long_timeouts():

@@ -302,3 +302,19 @@ def test_repeat_runs_deterministic(ctx):
     for _ in range(3):
         assert np.array_equal(g.bfs_level(0), a)
         assert np.array_equal(g.cc(), c)
+
+
+@pytest.mark.parametrize("kind", ["rmat", "er_dangling"])
+def test_pagerank_f64_variant_matches_f64_oracle(ctx, kind):
+    # the FP64 variant (ranks, sums, contributions in double) is the
+    # double-precision reference the reduced formats are measured against
+    g = O.rmat(14, 16 << 14, 3) if kind == "rmat" else O.er(1 << 14, 24.0, 5, dangling_bp=100)
+    G = upload(ctx, g)
+    st = gg.RunStats()
+    x = G.pagerank(maxiter=100, tol=1e-7, contrib=gg.F64, stats=st)
+    ref, it, deltas = O.pagerank(g, maxiter=100, tol=1e-7, f64=True)
+    assert x.dtype == np.float64
+    assert st.iterations == it
+    assert np.abs(x - ref).sum() < 1e-12
+    assert np.allclose([st.delta[i] for i in range(it)], deltas, rtol=1e-9, atol=1e-15)
+    G.close()

@@ -1,0 +1,72 @@
+"""What the trained selector gains over the density threshold, on measured
+per-variant iteration timings it was not trained on.
+
+The records (graptor_b200/data/selector_records.npz) hold, per sampled
+iteration of BFS / CC on the training graph families, the features and the
+measured time of all four traversal variants; every fifth record is held out
+of training.  The shipped network (graptor_b200/data/selector.npz, trained on
+the GPU by gg_selector_train) is evaluated here with the float64 oracle on
+bfloat16-rounded weights, applying the same rule as the device: the
+threshold's choice (push_sparse iff |F| + outdeg(F) <= m/20, else pull_dense)
+stands unless the network predicts another variant 2^0.2 times faster."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as M
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DATA = os.path.join(ROOT, "graptor_b200", "data")
+MARGIN = 0.2
+
+
+def heldout():
+    from graptor_b200.selector_train import clean, split
+    d = np.load(os.path.join(DATA, "selector_records.npz"))
+    X, Y, Mk = clean(d["X"], d["Y"])
+    _, te = split(len(X))
+    ok = Mk[te].all(1)
+    return X[te][ok], Y[te][ok]
+
+
+def choices(params, X):
+    out, _ = M.forward(M.bf16_round(params), X)
+    thr = np.where(X[:, 8] <= 0.05, 0, 2)  # feature 8 = (|F| + outdeg F) / m
+    best = out.argmin(1)
+    r = np.arange(len(X))
+    return np.where(out[r, best] < out[r, thr] - MARGIN, best, thr), thr
+
+
+def test_records_are_usable():
+    X, Y = heldout()
+    assert len(X) > 100
+    assert np.isfinite(X).all() and np.isfinite(Y).all()
+
+
+def test_trained_selector_beats_threshold_on_heldout_records():
+    z = np.load(os.path.join(DATA, "selector.npz"))
+    X, Y = heldout()
+    learned, thr = choices(z["params"].astype(np.float64), X)
+    t = 2.0 ** Y.astype(np.float64)  # microseconds
+    r = np.arange(len(X))
+    t_learned, t_thr, t_best = t[r, learned].sum(), t[r, thr].sum(), t.min(1).sum()
+    # the gain, stated: total held-out iteration time of each policy
+    print(f"held-out records {len(X)}: threshold {t_thr:.0f} us, learned {t_learned:.0f} us, "
+          f"oracle-best {t_best:.0f} us")
+    assert t_learned < t_thr
+    assert t_learned <= 1.25 * t_best
+
+
+def test_untrained_network_does_not_beat_threshold_by_luck():
+    # a control: random networks under the same margin rule are no better
+    X, Y = heldout()
+    t = 2.0 ** Y.astype(np.float64)
+    r = np.arange(len(X))
+    z = np.load(os.path.join(DATA, "selector.npz"))
+    trained, thr = choices(z["params"].astype(np.float64), X)
+    gains = []
+    for seed in range(5):
+        rnd, _ = choices(M.init_params(seed), X)
+        gains.append(t[r, thr].sum() / t[r, rnd].sum())
+    assert t[r, thr].sum() / t[r, trained].sum() > max(gains)
