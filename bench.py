@@ -309,6 +309,50 @@ def selector_eval(ctx, graphs):
 
 
 # ---------------------------------------------------------------------------
+# PageRank precision (R-MAT 25 ef16; directed ER 2^25 avg degree 32, 1% sinks)
+# ---------------------------------------------------------------------------
+def precision_eval(ctx, hbm_peak):
+    """Each storage format run until the L1 residual <= 1e-7 or 100 iterations,
+    timed per iteration, its ranks compared with the FP64 variant's (double
+    ranks, sums and contributions; checked against the CPU FP64 oracle by the
+    parity tests)."""
+    from graptor_b200 import gg
+    out = {}
+    fmts = [("f32", gg.F32, True), ("bf16", gg.BF16, False), ("f16", gg.F16, False),
+            ("fp8e4m3", gg.FP8E4M3, False), ("cfp_6_10", gg.CFP_6_10, False)]
+    for name, make in (("rmat25", lambda: ctx.rmat(25, 16 << 25, GRAPH_SEED)),
+                       ("er25_directed_1pct_sinks",
+                        lambda: ctx.er(1 << 25, 32.0, GRAPH_SEED, dangling_bp=100, symmetric=False))):
+        g = make()
+        n, m = g.n, g.m
+        x64 = g.pagerank(maxiter=100, tol=1e-7, contrib=gg.F64)
+        st = gg.RunStats()
+        g.pagerank(maxiter=100, tol=1e-7, contrib=gg.F64, host=False, stats=st)
+        res = {"n": n, "m": m, "f64": {"iterations": st.iterations,
+                                       "ms_per_iter": round(st.total_ms / max(st.iterations, 1), 4)}}
+        for fname, fmt, acc64 in fmts:
+            x = g.pagerank(maxiter=100, tol=1e-7, contrib=fmt, accum_f64=acc64, renorm_f32=(fname == "f32"))
+            ts, its = [], 0
+            for _ in range(2):
+                st = gg.RunStats()
+                g.pagerank(maxiter=100, tol=1e-7, contrib=fmt, accum_f64=acc64, renorm_f32=(fname == "f32"),
+                           host=False, stats=st)
+                ts.append(st.total_ms / max(st.iterations, 1))
+                its = st.iterations
+            err = np.abs(x.astype(np.float64) - x64)
+            nz = x64 > 0
+            res[fname] = {"iterations": its, "ms_per_iter": round(float(np.median(ts)), 4),
+                          "l1_vs_f64": float(err.sum()),
+                          "max_rel_vs_f64": float((err[nz] / x64[nz]).max())}
+        base = res["f32"]["ms_per_iter"]
+        for fname, _, _ in fmts:
+            res[fname]["speedup_vs_f32_per_iter"] = round(base / res[fname]["ms_per_iter"], 3)
+        out[name] = res
+        g.close()
+    return out
+
+
+# ---------------------------------------------------------------------------
 # batched traversals
 # ---------------------------------------------------------------------------
 def small_graph_batch(ctx, count, seed=2000):
@@ -499,9 +543,12 @@ def run_ours(args, ws, rank, local):
             ts = []
             for _ in range(3):
                 st = gg.RunStats()
-                g.pagerank(maxiter=20, tol=0, contrib=fmt, accum_f64=acc64, renorm_f32=(name == "f32"),
+                # tol < 0: exactly 20 iterations (a low-precision run can reach
+                # an exact fixed point, delta = 0, before that)
+                g.pagerank(maxiter=20, tol=-1.0, contrib=fmt, accum_f64=acc64, renorm_f32=(name == "f32"),
                            x=x, host=False, stats=st)
-                ts.append(st.total_ms / 20)
+                assert st.iterations == 20
+                ts.append(st.total_ms / st.iterations)
             t_it = float(np.median(ts))
             prs[name] = {"ms_per_iter": round(t_it, 4), "gedges_per_s_per_iter": round(m / (t_it / 1e3) / 1e9, 3)}
         base = prs["f32"]["ms_per_iter"]
@@ -516,6 +563,10 @@ def run_ours(args, ws, rank, local):
         grid = ctx.grid(2896, 2896, seed=77, del_bp=100)  # 2^23 vertices, 1% edges deleted
         out["selector"] = selector_eval(ctx, [("rmat24", g, [int(r) for r in roots[:4]]), ("grid2896", grid, [0])])
         grid.close()
+
+    # ---- PageRank precision workloads ----
+    if not args.quick and not args.no_precision and rank == 0:
+        out["pr_precision"] = precision_eval(ctx, hbm_peak)
 
     # ---- batching: multi-source BFS, 128-seed PPR (R-MAT 22), many small graphs ----
     if not args.quick and not args.no_batch and rank == 0:
@@ -610,6 +661,7 @@ def main():
     ap.add_argument("--quick", action="store_true", help="BFS only (no CC/PR/e2e)")
     ap.add_argument("--no-selector", action="store_true", help="skip the learned-selector evaluation")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-traversal measurements")
+    ap.add_argument("--no-precision", action="store_true", help="skip the PageRank precision workloads")
     ap.add_argument("--batch-graphs", type=int, default=2000, help="small graphs in the union workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup

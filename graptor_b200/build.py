@@ -40,7 +40,7 @@ def _needs(target: str, deps) -> bool:
 
 
 def _headers():
-    hs = [os.path.join(INCLUDE, "gg.h")]
+    hs = [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE) if f.endswith(".h")]
     hs += [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
     return hs
 

@@ -31,6 +31,7 @@ namespace gg {
 
 constexpr unsigned FULLB = 0xffffffffu;
 constexpr int kBB = 256;
+constexpr unsigned long long kMsPushDiv = 4;  // push while |F| + outdeg(F) <= m / 4
 
 // ---------------------------------------------------------------------------
 // Multi-source BFS
@@ -57,9 +58,127 @@ struct MsArgs {
     unsigned long long timeout_ns;
     int max_iters;
     int K;
+    HeavyRows H;     // CSC rows longer than H.T edges, cut into H.CH-edge chunks
+    int symmetric;   // the chunks also cut the CSR rows (push)
 };
 
 template <typename T> __device__ __forceinline__ T ldcgb(const T *p) { return __ldcg(p); }
+
+__device__ __forceinline__ unsigned long long warp_or64(unsigned long long x) {
+    const unsigned lo = __reduce_or_sync(FULLB, (unsigned)x);
+    const unsigned hi = __reduce_or_sync(FULLB, (unsigned)(x >> 32));
+    return ((unsigned long long)hi << 32) | lo;
+}
+
+// Push: out-edges of frontier vertices OR their frontier bits (minus the
+// target's visited bits) into the target's next word.  Light rows: a warp
+// per 32 vertices (lanes alone up to K edges, then the warp per long row);
+// heavy rows of a symmetric graph: a warp per chunk.
+__device__ void ms_push(const MsArgs &A, uint64_t gw, uint64_t nw, uint32_t lane) {
+    const uint32_t T = A.symmetric ? A.H.T : 0xFFFFFFFFu;
+    for (uint64_t w = gw; w * 32 < A.n; w += nw) {
+        const uint32_t v = (uint32_t)(w * 32 + lane);
+        const unsigned long long f = v < A.n ? ldcgb(A.front + v) : 0ull;
+        uint64_t beg = 0, end = 0;
+        if (f) {
+            beg = A.off[v];
+            end = A.off[v + 1];
+            if (end - beg > T) end = beg;  // chunked below
+        }
+        const uint32_t k1 = (uint32_t)min(end - beg, (uint64_t)A.K);
+        for (uint32_t k = 0; k < k1; ++k) {
+            const uint32_t u = __ldg(A.adj + beg + k);
+            const unsigned long long nv = f & ~ldcgb(A.visited + u);
+            if (nv) atomicOr(A.next + u, nv);
+        }
+        unsigned pend = __ballot_sync(FULLB, f && beg + k1 < end);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint64_t ej = __shfl_sync(FULLB, beg + k1, j), endj = __shfl_sync(FULLB, end, j);
+            const unsigned long long fj = __shfl_sync(FULLB, f, j);
+            for (uint64_t e = ej + lane; e < endj; e += 32) {
+                const uint32_t u = __ldg(A.adj + e);
+                const unsigned long long nv = fj & ~ldcgb(A.visited + u);
+                if (nv) atomicOr(A.next + u, nv);
+            }
+        }
+    }
+    if (!A.symmetric) return;
+    for (uint64_t c = gw; c < A.H.nchunks; c += nw) {
+        const uint32_t h = A.H.crow[c];
+        const uint32_t v = A.H.v[h];
+        const unsigned long long f = ldcgb(A.front + v);
+        if (!f) continue;
+        const uint64_t e0 = A.off[v] + (c - A.H.first[h]) * A.H.CH;
+        const uint64_t e1 = min(e0 + A.H.CH, A.off[v + 1]);
+        for (uint64_t e = e0 + lane; e < e1; e += 32) {
+            const uint32_t u = __ldg(A.adj + e);
+            const unsigned long long nv = f & ~ldcgb(A.visited + u);
+            if (nv) atomicOr(A.next + u, nv);
+        }
+    }
+}
+
+// Pull: a vertex ORs its in-neighbours' frontier words until every root it
+// has not been reached from is present.  Light rows: each warp a contiguous
+// range of 32-vertex words of equal light-edge work; heavy rows: a warp per
+// chunk, atomicOr of the chunk's new bits.
+__device__ void ms_pull(const MsArgs &A, uint64_t gw, uint64_t nw, uint32_t lane) {
+    const uint32_t nwords = (A.n + 31) / 32;
+    uint32_t wlo, whi;
+    dev::balanced_range(A.H.light_prefix, nwords, gw, nw, wlo, whi);
+    for (uint32_t w = wlo; w < whi; ++w) {
+        const uint32_t v = w * 32 + lane;
+        const bool valid = v < A.n;
+        const unsigned long long vis = valid ? ldcgb(A.visited + v) : A.all;
+        uint64_t e = 0, end = 0;
+        if (valid && vis != A.all) {
+            e = A.in_off[v];
+            end = A.in_off[v + 1];
+            if (end - e > A.H.T) end = e;  // heavy: chunked below
+        }
+        bool act = e < end;
+        unsigned long long acc = 0;
+        const uint64_t lim = min(end, e + (uint64_t)A.K);
+        for (; act && e < lim; ++e) {
+            acc |= ldcgb(A.front + __ldg(A.in_adj + e));
+            if ((acc | vis) == A.all) act = false;
+        }
+        unsigned pend = __ballot_sync(FULLB, act && e < end);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint64_t ej = __shfl_sync(FULLB, e, j), endj = __shfl_sync(FULLB, end, j);
+            const unsigned long long visj = __shfl_sync(FULLB, vis, j);
+            unsigned long long accj = __shfl_sync(FULLB, acc, j);
+            for (uint64_t base = ej; base < endj; base += 32) {
+                const uint64_t ed = base + lane;
+                accj |= warp_or64(ed < endj ? ldcgb(A.front + __ldg(A.in_adj + ed)) : 0ull);
+                if ((accj | visj) == A.all) break;
+            }
+            if ((int)lane == j) acc = accj;
+        }
+        const unsigned long long nx = acc & ~vis;
+        if (valid && nx) A.next[v] = nx;
+    }
+    for (uint64_t c = gw; c < A.H.nchunks; c += nw) {
+        const uint32_t h = A.H.crow[c];
+        const uint32_t v = A.H.v[h];
+        const unsigned long long vis = ldcgb(A.visited + v);
+        if (vis == A.all) continue;
+        const uint64_t e0 = A.in_off[v] + (c - A.H.first[h]) * A.H.CH;
+        const uint64_t e1 = min(e0 + A.H.CH, A.in_off[v + 1]);
+        unsigned long long acc = 0;
+        for (uint64_t base = e0; base < e1; base += 32) {
+            const uint64_t ed = base + lane;
+            acc |= warp_or64(ed < e1 ? ldcgb(A.front + __ldg(A.in_adj + ed)) : 0ull);
+            if ((acc | vis) == A.all) break;
+        }
+        const unsigned long long nx = acc & ~vis;
+        if (lane == 0 && nx) atomicOr(A.next + v, nx);
+    }
+}
 
 __global__ void __launch_bounds__(kBB) k_msbfs(MsArgs A) {
     MsState *st = A.st;
@@ -72,76 +191,13 @@ __global__ void __launch_bounds__(kBB) k_msbfs(MsArgs A) {
     for (; iter < A.max_iters; ++iter) {
         const unsigned long long nf = ldcgb(&st->nfront), ef = ldcgb(&st->efront);
         if (nf == 0) break;
-        const bool push = (nf + ef) <= A.m / 20;
+        // a pull scans most in-edges (it stops early only once every root
+        // has reached the vertex), a push only the frontier's out-edges
+        const bool push = (nf + ef) <= A.m / kMsPushDiv;
         if (blockIdx.x == 0 && threadIdx.x == 0 && iter < GG_MAX_ITERS)
             st->variant[iter] = push ? GG_VAR_PUSH_DENSE : GG_VAR_PULL_DENSE;
-        if (push) {
-            // a warp per 32 vertices; lanes with frontier bits push their rows
-            for (uint64_t w = gw; w * 32 < A.n; w += nw) {
-                const uint32_t v = (uint32_t)(w * 32 + lane);
-                const unsigned long long f = v < A.n ? ldcgb(A.front + v) : 0ull;
-                uint64_t beg = 0, end = 0;
-                if (f) {
-                    beg = A.off[v];
-                    end = A.off[v + 1];
-                }
-                const uint32_t k1 = (uint32_t)min(end - beg, (uint64_t)A.K);
-                for (uint32_t k = 0; k < k1; ++k) {
-                    const uint32_t u = __ldg(A.adj + beg + k);
-                    const unsigned long long nv = f & ~ldcgb(A.visited + u);
-                    if (nv) atomicOr(A.next + u, nv);
-                }
-                unsigned pend = __ballot_sync(FULLB, f && beg + k1 < end);
-                while (pend) {
-                    const int j = __ffs(pend) - 1;
-                    pend &= pend - 1;
-                    const uint64_t ej = __shfl_sync(FULLB, beg + k1, j), endj = __shfl_sync(FULLB, end, j);
-                    const unsigned long long fj = __shfl_sync(FULLB, f, j);
-                    for (uint64_t e = ej + lane; e < endj; e += 32) {
-                        const uint32_t u = __ldg(A.adj + e);
-                        const unsigned long long nv = fj & ~ldcgb(A.visited + u);
-                        if (nv) atomicOr(A.next + u, nv);
-                    }
-                }
-            }
-        } else {
-            for (uint64_t w = gw; w * 32 < A.n; w += nw) {
-                const uint32_t v = (uint32_t)(w * 32 + lane);
-                const bool valid = v < A.n;
-                const unsigned long long vis = valid ? ldcgb(A.visited + v) : A.all;
-                bool act = valid && vis != A.all;
-                uint64_t e = 0, end = 0;
-                if (act) {
-                    e = A.in_off[v];
-                    end = A.in_off[v + 1];
-                }
-                unsigned long long acc = 0;
-                const uint64_t lim = min(end, e + (uint64_t)A.K);
-                for (; act && e < lim; ++e) {
-                    acc |= ldcgb(A.front + __ldg(A.in_adj + e));
-                    if ((acc | vis) == A.all) act = false;
-                }
-                unsigned pend = __ballot_sync(FULLB, act && e < end);
-                while (pend) {
-                    const int j = __ffs(pend) - 1;
-                    pend &= pend - 1;
-                    const uint64_t ej = __shfl_sync(FULLB, e, j), endj = __shfl_sync(FULLB, end, j);
-                    const unsigned long long visj = __shfl_sync(FULLB, vis, j);
-                    unsigned long long accj = __shfl_sync(FULLB, acc, j);
-                    for (uint64_t base = ej; base < endj; base += 32) {
-                        const uint64_t ed = base + lane;
-                        unsigned long long f = ed < endj ? ldcgb(A.front + __ldg(A.in_adj + ed)) : 0ull;
-                        const unsigned lo = __reduce_or_sync(FULLB, (unsigned)f);
-                        const unsigned hi = __reduce_or_sync(FULLB, (unsigned)(f >> 32));
-                        accj |= ((unsigned long long)hi << 32) | lo;
-                        if ((accj | visj) == A.all) break;
-                    }
-                    if ((int)lane == j) acc = accj;
-                }
-                const unsigned long long nx = acc & ~vis;
-                if (valid && nx) A.next[v] = nx;
-            }
-        }
+        if (push) ms_push(A, gw, nw, lane);
+        else ms_pull(A, gw, nw, lane);
         if (!grid::sync(&st->bar, A.timeout_ns)) return;
         // update: visited, levels, next frontier, counts
         unsigned long long cnt = 0, edg = 0, red = 0;
@@ -391,6 +447,8 @@ gg_status gg_msbfs(gg_graph *g, const uint32_t *roots, int k, int32_t *host_leve
     A.timeout_ns = tuning().barrier_timeout_ns;
     A.max_iters = (int)std::min<uint64_t>(n + 2, 1u << 30);
     A.K = tuning().pull_k;
+    A.H = g->heavy;
+    A.symmetric = g->symmetric;
     GG_CUDA(ctx, cudaMemcpyAsync(droots, roots, k * 4, cudaMemcpyHostToDevice, s));
     GG_CUDA(ctx, cudaMemsetAsync(st, 0, sizeof(MsState), s));
     cudaEventRecord(ctx->ev0, s);

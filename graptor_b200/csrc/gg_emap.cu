@@ -321,6 +321,35 @@ __global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
 // ---------------------------------------------------------------------------
 // Degree-binned sparse push
 // ---------------------------------------------------------------------------
+// Edges [beg, end) of one source pushed by W cooperating threads (a warp,
+// W = 32, or a CTA, W = BLOCK; `t` = this thread's index among them), four
+// edges per thread in flight: the loads of the four targets' values and the
+// four atomics overlap instead of forming four dependent round trips.
+template <int R, int W>
+__device__ __forceinline__ void push_edges(const EmapArgs &A, const Op<R> &op, typename Op<R>::V sv, uint64_t beg,
+                                           uint64_t end, uint32_t t, unsigned long long &nv, unsigned long long &ne) {
+    constexpr int U = 4;
+    for (uint64_t base = beg; base < end; base += (uint64_t)W * U) {
+        uint32_t d[U];
+        bool rec[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t e = base + (uint64_t)u * W + t;
+            d[u] = e < end ? __ldg(A.adj + e) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t e = base + (uint64_t)u * W + t;
+            rec[u] = e < end && op.offer(d[u], sv, A.record, A.out_bits);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (base + (uint64_t)u * W >= end) break;  // uniform across the W threads
+            emit_out(A, rec[u], d[u], nv, ne);
+        }
+    }
+}
+
 template <int R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uint32_t nb_large,
                                                        uint32_t nb_med) {
@@ -343,16 +372,7 @@ __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uin
             const uint64_t beg = rb + (c - A.large_first[lo]) * A.large_ch;
             const uint64_t end = min(beg + A.large_ch, re);
             if (threadIdx.x == 0) sc += end - beg;
-            for (uint64_t base = beg; base < end; base += BLOCK) {
-                const uint64_t e = base + threadIdx.x;
-                bool rec = false;
-                uint32_t d = 0;
-                if (e < end) {
-                    d = __ldg(A.adj + e);
-                    rec = op.offer(d, sv, A.record, A.out_bits);
-                }
-                emit_out(A, rec, d, nv, ne);
-            }
+            push_edges<R, BLOCK>(A, op, sv, beg, end, threadIdx.x, nv, ne);
         }
     } else if (blockIdx.x < nb_large + nb_med) {
         // medium bin: a warp per source vertex
@@ -364,16 +384,7 @@ __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uin
             const V sv = op.src_val(s);
             const uint64_t beg = A.off[s], end = A.off[s + 1];
             if (lane == 0) sc += end - beg;
-            for (uint64_t base = beg; base < end; base += 32) {
-                const uint64_t e = base + lane;
-                bool rec = false;
-                uint32_t d = 0;
-                if (e < end) {
-                    d = __ldg(A.adj + e);
-                    rec = op.offer(d, sv, A.record, A.out_bits);
-                }
-                emit_out(A, rec, d, nv, ne);
-            }
+            push_edges<R, 32>(A, op, sv, beg, end, lane, nv, ne);
         }
     } else {
         // small bin: a thread per source vertex, warp-uniform edge loop

@@ -145,9 +145,16 @@ struct gg_graph {
     std::vector<uint32_t *> pool_bins, pool_bitmaps;
     std::vector<uint64_t *> pool_cnt;
     void *pstate = nullptr;       // device state block of persistent traversals
+    uint32_t *wq = nullptr;       // work queue of fused (asynchronous) pushes
+    size_t wq_cap = 0;
     float gini = -1.0f;           // degree Gini coefficient (selector feature), <0: unknown
     gg_selector *selector = nullptr;  // learned variant selector (GG_THRESH_LEARNED)
     int force_iter = -1, force_variant = -1;  // timing collection: one forced choice
+    struct ForceRecord {          // what the last device-driven run saw at force_iter
+        bool seen = false;
+        double iter_ms = 0, rest_ms = 0;  // that iteration; from its start to the run's end
+        double nactv = 0, nacte = 0, reached = 0;
+    } force_rec;
 };
 
 struct gg_prop {
@@ -196,6 +203,17 @@ struct Tuning {
     // during the launch through L2, which costs the big dense phases more
     // than the per-iteration host round trips it saves on R-MAT BFS)
     int persistent = 4;
+    // sparse push steps run fused (asynchronous multi-hop, as CCv with
+    // api::fusion) in device-driven runs: bit 2 CC.  Off by default: on
+    // B200 the shared work queue (three contended counters per vertex, and
+    // vertices revisited as ever smaller labels arrive) lost to both the
+    // level-synchronous steps and hooking on every graph measured.
+    int fusion = 0;
+    uint32_t fusion_queue = 0;  // queue entries (0: 2n + 65536)
+    // device-driven CC of a symmetric graph: after the first step, CCv's
+    // road-network test (fewer than n/10 zero labels) and, where it holds,
+    // min-id hooking for the rest of the run
+    int cc_hook = 1;
     unsigned long long barrier_timeout_ns = 5000000000ull;  // grid-barrier wait limit
 };
 Tuning &tuning();

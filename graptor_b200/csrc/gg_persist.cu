@@ -57,6 +57,16 @@ struct PState {
     unsigned long long scanned[GG_MAX_ITERS];
     unsigned long long t_ns[GG_MAX_ITERS + 1];
     unsigned long long reached_v, reached_e;
+    // timing collection: the forced iteration's input counts, its start and
+    // end, and the end of the run (any iteration index)
+    unsigned long long f_nactv, f_nacte, f_reached, f_t0, f_t1, t_end;
+    int f_seen;
+    unsigned long long zeros;  // CC: vertices labelled 0 after the first step
+    // fused push work queue counters (reset between iterations), one
+    // 128-byte line each so that claims, appends and completions do not
+    // contend for one L2 line
+    struct alignas(128) Line { unsigned long long v; };
+    Line wq_head, wq_tail, wq_done;
 };
 
 struct PArgs {
@@ -81,6 +91,10 @@ struct PArgs {
     const __nv_bfloat16 *sel_w;        // learned selector weights (bfloat16), or null
     float gini;
     int force_iter, force_variant;     // timing collection: one forced (iteration, variant)
+    int fusion;                        // sparse pushes run fused (asynchronous) through wq
+    int hook;                          // CC: road-network test after step 0, then hooking
+    uint32_t *wq;                      // fused push work queue, wq_cap entries, all kWqEmpty between phases
+    unsigned long long wq_cap;
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -212,6 +226,35 @@ __device__ __forceinline__ void p_flush(const PFront &O, unsigned long long nv, 
     }
 }
 
+// Edges [beg, end) of one source pushed by W cooperating threads (a warp or
+// the CTA; `t` = this thread's index among them), four edges per thread in
+// flight so that the target loads and atomics of the four overlap.
+template <int R, int W>
+__device__ __forceinline__ void p_push_edges(const PArgs &P, const POp<R> &op, const PFront &O,
+                                             typename POp<R>::V sv, uint64_t beg, uint64_t end, uint32_t t,
+                                             unsigned long long &nv, unsigned long long &ne) {
+    constexpr int U = 4;
+    for (uint64_t base = beg; base < end; base += (uint64_t)W * U) {
+        uint32_t d[U];
+        bool rec[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t e = base + (uint64_t)u * W + t;
+            d[u] = e < end ? __ldg(P.adj + e) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t e = base + (uint64_t)u * W + t;
+            rec[u] = e < end && op.offer(d[u], sv, P.record);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (base + (uint64_t)u * W >= end) break;  // uniform across the W threads
+            p_emit(P, O, rec[u], d[u], nv, ne);
+        }
+    }
+}
+
 // ---- sparse push F -> O ------------------------------------------------------
 // One shared buffer serves all phases (they never overlap in time).
 constexpr int kSmemWords = 3 * (kPB / 32) * 256;  // 24 KiB
@@ -249,16 +292,7 @@ __device__ void phase_push(const PArgs &P, const POp<R> &op, const PFront &F, co
             const uint64_t beg = P.off[s] + (c - s_first[lo]) * P.large_ch;
             const uint64_t end = min(beg + P.large_ch, P.off[s + 1]);
             if (threadIdx.x == 0) sc += end - beg;
-            for (uint64_t base = beg; base < end; base += kPB) {
-                const uint64_t e = base + threadIdx.x;
-                bool rec = false;
-                uint32_t d = 0;
-                if (e < end) {
-                    d = __ldg(P.adj + e);
-                    rec = op.offer(d, sv, P.record);
-                }
-                p_emit(P, O, rec, d, nv, ne);
-            }
+            p_push_edges<R, kPB>(P, op, O, sv, beg, end, threadIdx.x, nv, ne);
         }
     } else if (c2) {
         for (uint32_t i = blockIdx.x; i < c2; i += gridDim.x) {  // a CTA per row
@@ -266,16 +300,7 @@ __device__ void phase_push(const PArgs &P, const POp<R> &op, const PFront &F, co
             const V sv = op.src_val(s);
             const uint64_t beg = P.off[s], end = P.off[s + 1];
             if (threadIdx.x == 0) sc += end - beg;
-            for (uint64_t base = beg; base < end; base += kPB) {
-                const uint64_t e = base + threadIdx.x;
-                bool rec = false;
-                uint32_t d = 0;
-                if (e < end) {
-                    d = __ldg(P.adj + e);
-                    rec = op.offer(d, sv, P.record);
-                }
-                p_emit(P, O, rec, d, nv, ne);
-            }
+            p_push_edges<R, kPB>(P, op, O, sv, beg, end, threadIdx.x, nv, ne);
         }
     }
     // medium bin: a warp per row
@@ -286,16 +311,7 @@ __device__ void phase_push(const PArgs &P, const POp<R> &op, const PFront &F, co
         const V sv = op.src_val(s);
         const uint64_t beg = P.off[s], end = P.off[s + 1];
         if (lane == 0) sc += end - beg;
-        for (uint64_t base = beg; base < end; base += 32) {
-            const uint64_t e = base + lane;
-            bool rec = false;
-            uint32_t d = 0;
-            if (e < end) {
-                d = __ldg(P.adj + e);
-                rec = op.offer(d, sv, P.record);
-            }
-            p_emit(P, O, rec, d, nv, ne);
-        }
+        p_push_edges<R, 32>(P, op, O, sv, beg, end, lane, nv, ne);
     }
     // small bin: a thread per row, warp-uniform edge loop
     for (uint64_t base = gw * 32; base < c0; base += nw * 32) {
@@ -324,6 +340,238 @@ __device__ void phase_push(const PArgs &P, const POp<R> &op, const PFront &F, co
         }
     }
     p_flush(O, nv, ne, sc);
+}
+
+// ---- fused (asynchronous) sparse push ------------------------------------------
+// CCv's sparse steps with api::fusion (bench/CCv.C:564-566, executed by
+// dsl/emap/fusion.h:163-377): a destination whose label dropped is processed
+// at once instead of waiting for the next iteration, so labels cross many hops
+// in one step.  Here the pending vertices form one queue in device memory
+// shared by all warps: a warp claims the next slot (wq_head), waits until the
+// slot is written, processes that vertex's out-edges and appends every
+// destination it lowered (wq_tail).  wq_done counts finished entries; the
+// phase ends when wq_done == wq_tail (every appended entry finished, so none
+// is being processed and no more can appear).  Entries that find the queue
+// full are spilled into O (the next iteration's frontier) and counted done.
+// Every wait is bounded: a warp gives up after timeout_ns without progress,
+// sets DEV_ERR_TIMEOUT and the traversal returns.
+constexpr uint32_t kWqEmpty = 0xFFFFFFFFu;
+
+__device__ __forceinline__ unsigned long long ld_volatile(const unsigned long long *p) {
+    return *(const volatile unsigned long long *)p;
+}
+
+// spill d into O once (bitmap test-and-set), warp-aggregated list append
+__device__ __forceinline__ void p_spill(const PArgs &P, const PFront &O, bool sp, uint32_t d, unsigned long long &nv,
+                                        unsigned long long &ne) {
+    bool rec = false;
+    if (sp) {
+        const uint32_t bit = 1u << (d & 31);
+        rec = (atomicOr(O.bitmap + (d >> 5), bit) & bit) == 0;
+    }
+    uint64_t deg = 0;
+    if (rec) {
+        deg = P.off[d + 1] - P.off[d];
+        nv++;
+        ne += deg;
+    }
+    const uint32_t bin = deg <= P.smax ? 0u : (deg <= P.mmax ? 1u : 2u);
+    const uint32_t lane = threadIdx.x & 31u;
+#pragma unroll
+    for (uint32_t b = 0; b < NBINS; ++b) {
+        const unsigned mk = __ballot_sync(FULLP, rec && bin == b);
+        if (mk == 0) continue;
+        const int leader = __ffs(mk) - 1;
+        unsigned long long base = 0;
+        if ((int)lane == leader) base = atomicAdd(O.cnt + FC_BIN0 + b, (unsigned long long)__popc(mk));
+        base = __shfl_sync(FULLP, base, leader);
+        if (rec && bin == b) O.bins[b][base + __popc(mk & ((1u << lane) - 1u))] = d;
+    }
+}
+
+// append the lanes' vertices (mask `want`) to the queue; overflow spills
+__device__ __forceinline__ void wq_append(const PArgs &P, const PFront &O, bool want, uint32_t d,
+                                          unsigned long long &nv, unsigned long long &ne) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned mk = __ballot_sync(FULLP, want);
+    if (mk == 0) return;
+    unsigned long long pos = 0;
+    if (lane == 0) pos = atomicAdd(&P.st->wq_tail.v, (unsigned long long)__popc(mk));
+    pos = __shfl_sync(FULLP, pos, 0);
+    const unsigned long long slot = pos + __popc(mk & ((1u << lane) - 1u));
+    const bool spill = want && slot >= P.wq_cap;
+    if (want && !spill) *(volatile uint32_t *)(P.wq + slot) = d;
+    p_spill(P, O, spill, d, nv, ne);
+    const unsigned ns = __popc(__ballot_sync(FULLP, spill));
+    if (ns && lane == 0) {
+        __threadfence();
+        atomicAdd(&P.st->wq_done.v, (unsigned long long)ns);
+    }
+}
+
+// seed the queue with F's list (all warps), then a grid barrier follows
+__device__ void phase_fused_seed(const PArgs &P, const PFront &F, const PFront &O) {
+    const unsigned long long b0 = ldcg(F.cnt + FC_BIN0), b1 = ldcg(F.cnt + FC_BIN1), b2 = ldcg(F.cnt + FC_BIN2);
+    const unsigned long long tot = b0 + b1 + b2;
+    const uint64_t tid = (uint64_t)blockIdx.x * kPB + threadIdx.x, nth = (uint64_t)gridDim.x * kPB;
+    unsigned long long nv = 0, ne = 0;
+    for (uint64_t base = tid - (threadIdx.x & 31u); base < tot; base += nth) {
+        const uint64_t i = base + (threadIdx.x & 31u);
+        uint32_t v = 0;
+        if (i < tot) v = i < b0 ? ldcg(F.bins[0] + i) : (i < b0 + b1 ? ldcg(F.bins[1] + i - b0) : ldcg(F.bins[2] + i - b0 - b1));
+        wq_append(P, O, i < tot, v, nv, ne);
+    }
+    p_flush(O, nv, ne, 0);
+}
+
+template <int R>
+__device__ void phase_fused_run(const PArgs &P, const POp<R> &op, const PFront &O) {
+    using V = typename POp<R>::V;
+    PState *st = P.st;
+    const uint32_t lane = threadIdx.x & 31u;
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    for (;;) {
+        unsigned long long idx = 0;
+        uint32_t v = 0;
+        int state = 0;  // 1: got an entry, 2: finished, 3: error
+        if (lane == 0) {
+            idx = atomicAdd(&st->wq_head.v, 1ull);
+            unsigned long long t0 = globaltimer(), seen = ~0ull;
+            unsigned nap = 32, polls = 0;  // backoff: idle warps poll less often
+            for (;;) {
+                // poll the claimed slot itself (a different address per warp);
+                // the shared counters only every 8th time
+                if (idx < P.wq_cap) {
+                    v = *(volatile uint32_t *)(P.wq + idx);
+                    if (v != kWqEmpty) { state = 1; break; }
+                }
+                if ((++polls & 7u) == 0 || idx >= P.wq_cap) {
+                    const unsigned long long dn = ld_volatile(&st->wq_done.v);
+                    __threadfence();
+                    if (dn == ld_volatile(&st->wq_tail.v)) { state = 2; break; }
+                    if (dn != seen) {  // progress elsewhere: restart the clock
+                        seen = dn;
+                        t0 = globaltimer();
+                    }
+                }
+                if (*(volatile unsigned int *)&st->err) { state = 3; break; }
+                if (globaltimer() - t0 > P.timeout_ns) {
+                    atomicOr(&st->err, DEV_ERR_TIMEOUT);
+                    state = 3;
+                    break;
+                }
+                __nanosleep(nap);
+                if (nap < 1024) nap <<= 1;
+            }
+            if (state == 1) *(volatile uint32_t *)(P.wq + idx) = kWqEmpty;  // clean for the next phase
+        }
+        state = __shfl_sync(FULLP, state, 0);
+        if (state != 1) break;
+        v = __shfl_sync(FULLP, v, 0);
+        V lv = 0;
+        if (lane == 0) {
+            lv = ldcg((const V *)P.a + v);
+            if (P.record == GG_RECORD_NE_PREV) ((V *)P.prev)[v] = lv;  // prev == value once processed
+        }
+        lv = __shfl_sync(FULLP, lv, 0);
+        const uint64_t beg = P.off[v], end = P.off[v + 1];
+        if (lane == 0) sc += end - beg;
+        for (uint64_t base = beg; base < end; base += 32) {
+            const uint64_t e = base + lane;
+            bool want = false;
+            uint32_t d = 0;
+            if (e < end) {
+                d = __ldg(P.adj + e);
+                const V cur = ldcg((const V *)P.a + d);
+                if (op.dst_ok(cur) && lv < cur) want = lv < atomicMin((V *)P.a + d, lv);
+            }
+            if (__any_sync(FULLP, want)) {
+                __threadfence();  // the lowered values before the queue entries
+                wq_append(P, O, want, d, nv, ne);
+            }
+        }
+        if (lane == 0) {
+            __threadfence();  // appended entries before this one counts as done
+            atomicAdd(&st->wq_done.v, 1ull);
+        }
+    }
+    p_flush(O, nv, ne, sc);
+}
+
+// ---- CC by min-id hooking -------------------------------------------------------
+// label[] is a forest: every label is the id of a vertex of the same
+// component and never above the vertex's own id, so following labels ends at
+// a vertex labelled with itself (a root).  Hooking an edge's two roots, the
+// larger under the smaller (compare-and-swap on the larger root), and
+// repeating until they agree merges the trees; the root of a component is
+// then its minimum id, the CCv label.  Finds halve paths with plain stores
+// (a label only ever moves to an ancestor, so racing stores stay valid).
+__device__ __forceinline__ uint32_t uf_find(uint32_t *lab, uint32_t x) {
+    for (int guard = 0; guard < (1 << 26); ++guard) {  // a chain of n links at most
+        const uint32_t p = ldcg(lab + x);
+        if (p == x) return x;
+        const uint32_t gp = ldcg(lab + p);
+        if (gp != p) lab[x] = gp;
+        x = gp;
+    }
+    return x;
+}
+
+__device__ __forceinline__ void uf_hook(uint32_t *lab, uint32_t u, uint32_t v) {
+    uint32_t ru = uf_find(lab, u), rv = uf_find(lab, v);
+    for (int guard = 0; ru != rv && guard < (1 << 26); ++guard) {
+        const uint32_t lo = ru < rv ? ru : rv, hi = ru ^ rv ^ lo;
+        const uint32_t old = atomicCAS(lab + hi, hi, lo);
+        if (old == hi) break;
+        ru = uf_find(lab, old);
+        rv = uf_find(lab, lo);
+    }
+}
+
+__device__ void phase_hook(const PArgs &P) {
+    uint32_t *lab = (uint32_t *)P.a;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t gw = ((uint64_t)blockIdx.x * kPB + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * kPB) >> 5;
+    // a warp per 32 vertices; each vertex's edges to smaller ids (each
+    // undirected edge once): rows of up to 32 edges by their lane, longer
+    // rows by the whole warp in turn
+    for (uint64_t w = gw; w * 32 < P.n; w += nw) {
+        const uint32_t u = (uint32_t)(w * 32 + lane);
+        uint64_t beg = 0, end = 0;
+        if (u < P.n) {
+            beg = P.off[u];
+            end = P.off[u + 1];
+        }
+        const bool longrow = end - beg > 32;
+        if (!longrow)
+            for (uint64_t e = beg; e < end; ++e) {
+                const uint32_t v = __ldg(P.adj + e);
+                if (v >= u) break;  // rows are sorted: the rest are larger
+                uf_hook(lab, u, v);
+            }
+        unsigned pend = __ballot_sync(FULLP, longrow);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint32_t uj = __shfl_sync(FULLP, u, j);
+            const uint64_t bj = __shfl_sync(FULLP, beg, j), ej = __shfl_sync(FULLP, end, j);
+            for (uint64_t e = bj + lane; e < ej; e += 32) {
+                const uint32_t v = __ldg(P.adj + e);
+                if (v < uj) uf_hook(lab, uj, v);
+            }
+        }
+    }
+}
+
+__device__ void phase_hook_finish(const PArgs &P) {
+    uint32_t *lab = (uint32_t *)P.a;
+    const uint64_t tid = (uint64_t)blockIdx.x * kPB + threadIdx.x, nth = (uint64_t)gridDim.x * kPB;
+    for (uint64_t v = tid; v < P.n; v += nth) {
+        const uint32_t r = uf_find(lab, (uint32_t)v);
+        lab[v] = r;
+        if (P.prev) ((uint32_t *)P.prev)[v] = r;
+    }
 }
 
 // ---- dense pull F -> O over a candidate list -------------------------------
@@ -706,7 +954,10 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
     const uint64_t nthreads = (uint64_t)gridDim.x * kPB;
     int cur = 0;
     int iter = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->t_ns[0] = globaltimer();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->t_ns[0] = globaltimer();
+        if (P.force_iter == 0) st->f_t0 = st->t_ns[0];
+    }
     for (; iter < P.max_iters; ++iter) {
         const PFront F = P.fr[cur], O = P.fr[cur ^ 1];
         const unsigned long long nactv = ldcg(F.cnt + FC_NACTV), nacte = ldcg(F.cnt + FC_NACTE);
@@ -715,6 +966,12 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
         if (P.level_k) op.fk = iter + 1;
         const int var = choose_variant(P, iter, nactv, nacte, f_all != 0, st, &s_choice);
         const bool pushes = var != GG_VAR_PULL_DENSE;
+        if (blockIdx.x == 0 && threadIdx.x == 0 && iter == P.force_iter) {
+            st->f_nactv = nactv;
+            st->f_nacte = nacte;
+            st->f_reached = ldcg(&st->reached_v);
+            st->f_seen = 1;
+        }
         if (blockIdx.x == 0 && threadIdx.x == 0 && iter < GG_MAX_ITERS) {
             st->variant[iter] = var;
             st->nactv[iter] = nactv;
@@ -727,7 +984,11 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
                 if (!grid_barrier(st, P.timeout_ns)) return;
             }
             __syncthreads();
-            if (var == GG_VAR_PUSH_SPARSE) {
+            if (var == GG_VAR_PUSH_SPARSE && P.fusion) {
+                phase_fused_seed(P, F, O);
+                if (!grid_barrier(st, P.timeout_ns)) return;
+                phase_fused_run<R>(P, op, O);
+            } else if (var == GG_VAR_PUSH_SPARSE) {
                 phase_push<R>(P, op, F, O, smem);
             } else {
                 phase_merge_count(P, F);
@@ -769,6 +1030,9 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
             // every CTA's next choice reads the same values
             st->reached_v += nactv;
             st->reached_e += nacte;
+            st->wq_head.v = 0;
+            st->wq_tail.v = 0;
+            st->wq_done.v = 0;
             for (int i = 0; i < FC_WORDS; ++i) F.cnt[i] = 0;
             st->has_list[cur ^ 1] = pushes ? 1 : 0;
             st->all[cur] = 0;
@@ -782,11 +1046,46 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
                 st->scanned[iter] = ldcg(O.cnt + FC_SCANNED);
                 st->t_ns[iter + 1] = globaltimer();
             }
+            if (iter == P.force_iter || iter + 1 == P.force_iter) {
+                const unsigned long long now = globaltimer();
+                if (iter == P.force_iter) st->f_t1 = now; else st->f_t0 = now;
+            }
         }
         if (!grid_barrier(st, P.timeout_ns)) return;
         cur ^= 1;
+        if (P.hook && iter == 0) {
+            // CCv's road-network test (PUSH_ZERO): few zero labels after the
+            // first step.  Then the rest of the run is min-id hooking.
+            unsigned long long z = 0;
+            for (uint64_t v = tid; v < P.n; v += nthreads) z += ldcg((const uint32_t *)P.a + v) == 0;
+            z = dev::block_sum<unsigned long long, kPB>(z);
+            if (threadIdx.x == 0 && z) atomicAdd(&st->zeros, z);
+            if (!grid_barrier(st, P.timeout_ns)) return;
+            // (the count includes vertex 0 and its neighbours, CCv's initial_zeros)
+            if (ldcg(&st->zeros) * 10 < (unsigned long long)P.n) {
+                phase_hook(P);
+                if (!grid_barrier(st, P.timeout_ns)) return;
+                phase_hook_finish(P);
+                if (blockIdx.x == 0 && threadIdx.x == 0) {
+                    ++iter;
+                    if (iter < GG_MAX_ITERS) {
+                        st->variant[iter] = GG_VAR_HOOK;
+                        st->nactv[iter] = P.n;
+                        st->nacte[iter] = P.m;
+                        st->scanned[iter] = P.m;
+                        st->t_ns[iter + 1] = globaltimer();
+                    }
+                    st->iterations = iter + 1;
+                    st->t_end = globaltimer();
+                }
+                return;
+            }
+        }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->iterations = iter;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->iterations = iter;
+        st->t_end = globaltimer();
+    }
 }
 
 __global__ void k_traverse_init(PFront F, uint32_t root, const uint64_t *off, uint32_t smax, uint32_t mmax,
@@ -887,6 +1186,24 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
     P.force_iter = force_iter >= 0 ? force_iter : g->force_iter;
     P.force_variant = force_iter >= 0 ? force_variant : g->force_variant;
     P.sel_w = (const __nv_bfloat16 *)selector_weights(g);
+    // CC of a symmetric graph: road-network test after step 0, then hooking
+    P.hook = t.cc_hook && d.relax == GG_RELAX_MIN_U32 && d.dst_filter == GG_FILTER_NE_ZERO && g->symmetric &&
+             start_all && force_iter < 0 && g->force_iter < 0 && g->n > 0;
+    // fused sparse pushes (CC): the queue holds up to 2n + 64Ki entries, more spill
+    P.fusion = (t.fusion & 4) && d.relax == GG_RELAX_MIN_U32 && d.dst_filter == GG_FILTER_NE_ZERO;
+    if (P.fusion) {
+        const size_t cap = t.fusion_queue ? (size_t)t.fusion_queue : 2 * (size_t)g->n + 65536;
+        if (g->wq_cap != cap) {
+            cudaFree(g->wq);
+            g->wq = nullptr;
+            g->wq_cap = 0;
+            GG_CUDA(ctx, cudaMalloc(&g->wq, cap * 4));
+            g->wq_cap = cap;
+        }
+        GG_CUDA(ctx, cudaMemsetAsync(g->wq, 0xFF, g->wq_cap * 4, s));
+        P.wq = g->wq;
+        P.wq_cap = g->wq_cap;
+    }
     P.gini = g->gini < 0 ? 0.0f : g->gini;
     if (opt.threshold == GG_THRESH_LEARNED && P.sel_w && g->gini < 0) {
         float gi;
@@ -930,6 +1247,14 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
     if (hs.err & DEV_ERR_TIMEOUT) return set_error(ctx, GG_ERR_TIMEOUT, "traversal grid barrier timed out");
     if (hs.err) return set_error(ctx, GG_ERR_STATE, "traversal device error");
     *iters_out = hs.iterations;
+    g->force_rec.seen = P.force_iter >= 0 && P.force_iter < INT_MAX && hs.f_seen && hs.f_t1 >= hs.f_t0;
+    if (g->force_rec.seen) {
+        g->force_rec.iter_ms = (double)(hs.f_t1 - hs.f_t0) * 1e-6;
+        g->force_rec.rest_ms = (double)(hs.t_end - hs.f_t0) * 1e-6;
+        g->force_rec.nactv = (double)hs.f_nactv;
+        g->force_rec.nacte = (double)hs.f_nacte;
+        g->force_rec.reached = (double)hs.f_reached;
+    }
     if (stats) {
         stats->vertices_reached = hs.reached_v;
         stats->edges_reached = hs.reached_e;

@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <cub/cub.cuh>
@@ -453,29 +454,21 @@ extern "C" gg_status gg_selector_collect(gg_graph *g, int analytic, uint32_t roo
     auto run = [&](gg_run_stats *st) -> gg_status {
         return analytic == 0 ? gg_bfs_level(g, root, &o, nullptr, nullptr, st) : gg_cc(g, &o, nullptr, nullptr, st);
     };
-    // reference run with the threshold's choices (device-driven)
-    std::vector<gg_run_stats> st(1);
-    g->force_iter = GG_MAX_ITERS + 1;  // device-driven, nothing forced
+    // reference run with the threshold's choices (device-driven, nothing forced)
+    gg_run_stats rs;
+    g->force_iter = INT_MAX;
     g->force_variant = 0;
-    gg_status s = run(&st[0]);
+    gg_status s = run(&rs);
     if (s != GG_OK) { g->force_iter = -1; return s; }
-    const int T = std::min(st[0].iterations, GG_MAX_ITERS);
+    const int T = rs.iterations;
     // CC's first step starts from the all-true frontier and is always a pull
     const int first = (analytic == 1 && T > 1) ? 1 : 0;
     const int k = std::min(max_samples, T - first);
-    double reached = 0;
-    std::vector<double> reached_before(T + 1, 0.0);
-    for (int i = 0; i < T; ++i) {
-        reached_before[i] = reached;
-        reached += (double)st[0].nactv[i];
-    }
-    gg_run_stats rs;
     for (int si = 0; si < k && *nrec < cap; ++si) {
         const int it = first + (k == 1 ? 0 : (int)((long long)si * (T - 1 - first) / (k - 1)));
         float *x = X + (size_t)*nrec * GG_SEL_FEATURES;
-        selector_features(x, (double)st[0].nactv[it], (double)st[0].nacte[it], (double)g->n - reached_before[it], it,
-                          g->n, (double)g->m, gini);
         float *y = Y + (size_t)*nrec * GG_SEL_VARIANTS;
+        bool have_x = false;
         for (int v = 0; v < GG_SEL_VARIANTS; ++v) {
             g->force_iter = it;
             g->force_variant = v;
@@ -485,11 +478,22 @@ extern "C" gg_status gg_selector_collect(gg_graph *g, int analytic, uint32_t roo
                 if (s != GG_OK) { g->force_iter = -1; return s; }
                 // CC's push steps race (a label can travel several hops in one
                 // step), so a run may converge before iteration `it`: no sample
-                if (rs.iterations > it && rs.iter_ms[it] > 0) best = std::min(best, rs.iter_ms[it]);
+                const auto &fr = g->force_rec;
+                if (!fr.seen) continue;
+                if (!have_x) {
+                    selector_features(x, fr.nactv, fr.nacte, (double)g->n - fr.reached, it, g->n, (double)g->m,
+                                      gini);
+                    have_x = true;
+                }
+                // BFS: every variant leaves the same next frontier, so the
+                // iteration's own time decides; CC: a fused push finishes the
+                // run, so the time until the run ends does
+                const double t = analytic == 0 ? fr.iter_ms : fr.rest_ms;
+                if (t > 0) best = std::min(best, t);
             }
             y[v] = best < 1e30 ? (float)std::log2(best * 1e3) : std::nanf("");
         }
-        ++*nrec;
+        if (have_x) ++*nrec;
     }
     g->force_iter = -1;
     g->force_variant = -1;

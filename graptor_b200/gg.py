@@ -24,7 +24,7 @@ RELAX_MIN_PLUS1_I32, RELAX_MIN_U32, RELAX_SETIF_U32, RELAX_ADD_GATHER = range(4)
 FILTER_NONE, FILTER_GT_CONST, FILTER_NE_ZERO, FILTER_MSB_SET = range(4)
 RECORD_NONE, RECORD_REDUCTION, RECORD_NE_PREV = range(3)
 THRESH_DEFAULT, THRESH_FRAC, THRESH_ALWAYS_SPARSE, THRESH_ALWAYS_DENSE, THRESH_LEARNED = range(5)
-VAR_AUTO, VAR_PUSH_SPARSE, VAR_PUSH_MERGE, VAR_PULL_DENSE, VAR_PUSH_DENSE = -1, 0, 1, 2, 3
+VAR_AUTO, VAR_PUSH_SPARSE, VAR_PUSH_MERGE, VAR_PULL_DENSE, VAR_PUSH_DENSE, VAR_HOOK = -1, 0, 1, 2, 3, 4
 VARIANT_NAMES = {0: "push_sparse", 1: "push_merge", 2: "pull_dense", 3: "push_dense"}
 GEN_RMAT, GEN_ER, GEN_GRID = range(3)
 (VM_END, VM_LOAD, VM_STORE, VM_CONST, VM_VID, VM_DEGREE, VM_ADD, VM_SUB, VM_MUL, VM_DIV, VM_ABS,

@@ -196,7 +196,9 @@ typedef enum gg_variant {
     GG_VAR_PUSH_SPARSE = 0, /* degree-binned thread/warp/CTA push over the frontier list */
     GG_VAR_PUSH_MERGE = 1,  /* edge-balanced (merge-path) push over the frontier list   */
     GG_VAR_PULL_DENSE = 2,  /* bitmap-frontier pull over the CSC with early exit         */
-    GG_VAR_PUSH_DENSE = 3   /* push from a bitmap frontier, dense bitmap output          */
+    GG_VAR_PUSH_DENSE = 3,  /* push from a bitmap frontier, dense bitmap output          */
+    GG_VAR_HOOK = 4         /* CC only, reported in run stats: the rest of the run
+                               finished by min-id hooking (road-like graphs, see gg_cc) */
 } gg_variant;
 
 typedef struct gg_emap_desc {
@@ -315,7 +317,12 @@ GG_API gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, 
 /* BFS parents (BFSv): parent[root] = root, unreached = ~0u; any valid BFS tree. */
 GG_API gg_status gg_bfs_parent(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop *parent,
                                uint32_t *host_parent, gg_run_stats *st);
-/* Connected components (CCv): label = minimum vertex id of the component. */
+/* Connected components (CCv): label = minimum vertex id of the component.
+ * Device-driven runs of a symmetric graph take CCv's road-network test after
+ * the first step (PUSH_ZERO, bench/CCv.C:365-388: fewer than n/10 vertices
+ * labelled 0) and, where it holds, finish the run by hooking every edge's
+ * endpoints' roots, the larger under the smaller (labels unchanged: the
+ * minimum id of each component); otherwise label propagation continues. */
 GG_API gg_status gg_cc(gg_graph *g, const gg_run_opts *o, gg_prop *label, uint32_t *host_label,
                        gg_run_stats *st);
 

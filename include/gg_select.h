@@ -53,10 +53,12 @@ GG_API gg_status gg_selector_train(gg_selector *s, const float *X, const float *
 /* Timing collection.  Runs the analytic (0 = BFS levels from root, 1 = CC)
  * device-driven, once per (sampled iteration, variant), every iteration
  * using the threshold's choice except the sampled one, and records per
- * sampled iteration its features X[k][10] and the measured log2 us of each
- * variant Y[k][4] (NaN where the forced run ended before that iteration,
- * which CC's racing push steps can cause).  At most `max_samples`
- * iterations are sampled (spread
+ * sampled iteration its features X[k][10] and, per variant, the log2 us of
+ * the sampled iteration (BFS: every variant leaves the same next frontier)
+ * or of the rest of the run from that iteration on (CC: a fused push step
+ * finishes the run) in Y[k][4] (NaN where the forced run ended before that
+ * iteration, which CC's racing push steps can cause).  Any iteration of the
+ * run can be sampled.  At most `max_samples` iterations are sampled (spread
  * evenly); *nrec receives the record count (<= cap). */
 GG_API gg_status gg_selector_collect(gg_graph *g, int analytic, uint32_t root, int max_samples,
                                      float *X, float *Y, int cap, int *nrec);

@@ -15,8 +15,16 @@
  * kernels), pr_stream (1: warp-streamed segmented PageRank gather, 0:
  * per-row), persistent (bit mask: 1 BFS levels, 2 BFS parents, 4 CC run as
  * one device-driven cooperative launch; otherwise one launch per iteration
- * from the host), barrier_timeout_ns (how long a CTA of a persistent run
- * waits at a grid barrier before it reports GG_ERR_TIMEOUT).
+ * from the host), cc_hook (1: a device-driven CC run of a symmetric graph
+ * that passes CCv's road-network test after its first step finishes by
+ * min-id hooking; 0: label propagation throughout), fusion (4: the sparse
+ * push steps of a device-driven CC run fused, as CCv with api::fusion: a
+ * lowered label is propagated at once through a device work queue; 0, the
+ * default: level by level), fusion_queue (entries of
+ * that queue, 0 = 2n + 65536; entries beyond it spill into the next
+ * frontier), barrier_timeout_ns (how long a CTA of a persistent run waits
+ * at a grid barrier, or a warp on the work queue without progress, before
+ * it reports GG_ERR_TIMEOUT).
  */
 #ifndef GG_TUNE_H
 #define GG_TUNE_H

@@ -80,3 +80,70 @@ def test_grid_barrier_timeout_is_reported_and_recoverable(ctx, persistent_knob):
         gg.tuning_set("barrier_timeout_ns", old)
     assert np.array_equal(g.bfs_level(0), O.bfs_level(og, 0))
     assert np.array_equal(g.cc(), O.cc(og))
+
+
+@pytest.fixture
+def fusion_knobs():
+    old = {k: gg.tuning_get(k) for k in ("persistent", "fusion", "fusion_queue", "cc_hook")}
+    yield
+    for k, v in old.items():
+        gg.tuning_set(k, v)
+
+
+@pytest.mark.parametrize("gen", ["rmat", "grid", "union"])
+@pytest.mark.parametrize("queue", [0, 32])  # 32 entries: most appends spill into the next frontier
+def test_fused_cc_exact(ctx, fusion_knobs, gen, queue):
+    if gen == "rmat":
+        og = O.rmat(14, 16 << 14, seed=62)
+    elif gen == "grid":
+        og = O.grid(90, 110, seed=5, del_bp=300)
+    else:
+        from oracle import batch_oracle as B
+        og, _ = B.union([O.grid(20 + i, 30, seed=i, del_bp=500) for i in range(6)] +
+                        [O.rmat(9, 4000, seed=i) for i in range(6)])
+    g = ctx.upload(og.off, og.adj)
+    ref = O.cc(og)
+    gg.tuning_set("persistent", 4)
+    gg.tuning_set("cc_hook", 0)  # label propagation throughout
+    gg.tuning_set("fusion_queue", queue)
+    st = {}
+    for f in (0, 4):
+        gg.tuning_set("fusion", f)
+        s = gg.RunStats()
+        assert np.array_equal(g.cc(stats=s), ref), (gen, queue, f)
+        st[f] = s
+    if gen == "grid" and queue == 0:
+        # labels cross the grid inside one fused step instead of one hop per level
+        assert st[4].iterations < st[0].iterations, (st[4].iterations, st[0].iterations)
+    g.close()
+
+
+@pytest.mark.parametrize("gen", ["rmat", "grid", "union", "edgeless"])
+def test_cc_hooking_exact(ctx, fusion_knobs, gen):
+    from oracle import batch_oracle as B
+    if gen == "rmat":
+        og = O.rmat(14, 16 << 14, seed=63)
+    elif gen == "grid":
+        og = O.grid(120, 130, seed=6, del_bp=400)
+    elif gen == "union":
+        og, _ = B.union([O.grid(20 + i, 30, seed=i, del_bp=500) for i in range(8)] +
+                        [O.rmat(10, 12 << 10, seed=i) for i in range(8)] + [O.from_edges(9, [])])
+    else:
+        og = O.from_edges(50, [(1, 2), (3, 4)])
+    g = ctx.upload(og.off, og.adj)
+    ref = O.cc(og)
+    gg.tuning_set("persistent", 4)
+    st = {}
+    for h in (0, 1):
+        gg.tuning_set("cc_hook", h)
+        s = gg.RunStats()
+        assert np.array_equal(g.cc(stats=s), ref), (gen, h)
+        st[h] = s
+    used = [st[1].variant[i] for i in range(min(st[1].iterations, gg.MAX_ITERS))]
+    zeros_after_first = None
+    if gen == "rmat":
+        assert gg.VAR_HOOK not in used  # vertex 0 reaches most of an R-MAT graph in one step
+    else:
+        # road-like: the run ends with the hooking step
+        assert used[-1] == gg.VAR_HOOK and st[1].iterations == 2, used
+    g.close()
