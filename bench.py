@@ -347,6 +347,23 @@ def precision_eval(ctx, hbm_peak):
         base = res["f32"]["ms_per_iter"]
         for fname, _, _ in fmts:
             res[fname]["speedup_vs_f32_per_iter"] = round(base / res[fname]["ms_per_iter"], 3)
+        # staged precision (the switch taken on the device): time to the 1e-7 residual
+        t_f32 = res["f32"]["ms_per_iter"] * res["f32"]["iterations"]
+        for sname, stages in (("staged_f16_f32", [(gg.F16, False, 1e-3), (gg.F32, True, 0.0)]),
+                              ("staged_bf16_f32", [(gg.BF16, False, 1e-3), (gg.F32, True, 0.0)]),
+                              ("pr_vary_4620", [(gg.CFP_6_10, False, 1e-3), (gg.F32, True, 0.0)])):
+            x = g.pagerank(maxiter=100, tol=1e-7, renorm_f32=False, stages=stages)
+            ts = []
+            for _ in range(2):
+                st = gg.RunStats()
+                g.pagerank(maxiter=100, tol=1e-7, renorm_f32=False, stages=stages, host=False, stats=st)
+                ts.append(st.total_ms)
+            err = np.abs(x.astype(np.float64) - x64)
+            nz = x64 > 0
+            res[sname] = {"iterations": st.iterations, "total_ms": round(float(np.median(ts)), 3),
+                          "speedup_vs_f32_to_1e-7": round(t_f32 / float(np.median(ts)), 3),
+                          "l1_vs_f64": float(err.sum()), "max_rel_vs_f64": float((err[nz] / x64[nz]).max())}
+        res["f32"]["total_ms"] = round(t_f32, 3)
         out[name] = res
         g.close()
     return out
@@ -404,7 +421,9 @@ def batch_eval(ctx, g, roots, hbm_peak, n_small):
         gg.ppr(g, seeds, alpha=0.15, iters=20, host=False, stats=st)
         ms.append(st.total_ms / 20)
     t = float(np.median(ms))
-    ppr_bytes = m * (256.0 + 4.0) + 8.0 * (n + 1) + n * 256.0 * 2
+    # per iteration: ids + one 256-byte bf16 row per edge, offsets, the new
+    # contribution rows (the ranks are written by the last iteration only)
+    ppr_bytes = m * (256.0 + 4.0) + 8.0 * (n + 1) + n * 256.0
     out["ppr128"] = {"ms_per_iter": round(t, 3), "gedges_per_s_per_iter": round(m / (t / 1e3) / 1e9, 3),
                      "seed_edges_per_s": round(128 * m / (t / 1e3) / 1e9, 1),
                      "frac_of_hbm": round(ppr_bytes / (t / 1e3) / 1e9 / hbm_peak, 4),

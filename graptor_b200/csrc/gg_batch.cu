@@ -276,7 +276,7 @@ struct PprArgs {
     uint32_t n;
     const uint2 *cin;   // [n] rows of 128 bf16 (uint2 = 4 bf16 per lane)
     uint2 *cout;        // next contributions
-    uint2 *xout;        // ranks (bf16)
+    uint2 *xout;        // ranks (bf16), written by the last iteration only (else null)
     const uint32_t *seeds;  // [128]
     float alpha;
     HeavyRows H;
@@ -310,7 +310,7 @@ __device__ __forceinline__ void ppr_finish(const PprArgs &A, uint32_t d, float4 
     if (A.seeds[s0 + 3] == d) x.w += A.alpha;
     const uint64_t deg = A.off[d + 1] - A.off[d];
     const float inv = deg ? 1.0f / (float)deg : 0.0f;
-    A.xout[(uint64_t)d * 32 + lane] = f4_to_bf4(x);
+    if (A.xout) A.xout[(uint64_t)d * 32 + lane] = f4_to_bf4(x);
     A.cout[(uint64_t)d * 32 + lane] = f4_to_bf4(make_float4(x.x * inv, x.y * inv, x.z * inv, x.w * inv));
 }
 
@@ -529,7 +529,7 @@ gg_status gg_ppr(gg_graph *g, const uint32_t *seeds, int k, float alpha, int ite
     for (int it = 0; it < iters && e == cudaSuccess; ++it) {
         A.cin = (it & 1) ? c1 : c0;
         A.cout = (it & 1) ? c0 : c1;
-        A.xout = x;
+        A.xout = it + 1 == iters ? x : nullptr;  // only the ranks of the last iteration are kept
         k_ppr_light<<<gl, kBB, 0, cs>>>(A);
         if (A.H.nchunks) {
             k_ppr_heavy<<<gh, kBB, 0, cs>>>(A);

@@ -218,6 +218,35 @@ __global__ void k_csr_to_tkeys(const uint64_t *off, const uint32_t *adj, uint32_
     }
 }
 
+// Edge list -> sort keys (src << lg | dst), and the reverse edge when
+// symmetrising; ids out of range raise *bad and become self-loops (dropped).
+__global__ void k_edges_to_keys(const uint32_t *src, const uint32_t *dst, uint64_t ne, uint32_t n, int lg,
+                                int sym, uint64_t *keys, uint32_t *bad) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < ne; i += stride) {
+        uint32_t s = src[i], d = dst[i];
+        if (s >= n || d >= n) {
+            atomicOr(bad, 1u);
+            s = d = 0;
+        }
+        keys[i] = ((uint64_t)s << lg) | d;
+        if (sym) keys[ne + i] = ((uint64_t)d << lg) | s;
+    }
+}
+
+// CSR -> sort keys (src << lg | dst), plus the reverse edges when symmetrising
+__global__ void k_csr_to_keys(const uint64_t *off, const uint32_t *adj, uint32_t n, int lg, int sym, uint64_t m,
+                              uint64_t *keys) {
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t v = warp; v < n; v += nw)
+        for (uint64_t e = off[v] + lane; e < off[v + 1]; e += 32) {
+            const uint32_t d = adj[e];
+            keys[e] = ((uint64_t)v << lg) | d;
+            if (sym) keys[m + e] = ((uint64_t)d << lg) | v;
+        }
+}
+
 __global__ void k_max_degree(const uint64_t *off, uint32_t n, unsigned long long *best) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t stride = gridDim.x * blockDim.x;
@@ -877,6 +906,128 @@ gg_status gg_graph_read_bin(gg_ctx *ctx, const char *path, int symmetric, gg_gra
     gg_status s = gg_graph_upload(ctx, n, m, off.data(), adj.data(), symmetric, out);
     if (s == GG_ERR_ARG) return set_error(ctx, GG_ERR_IO, "corrupt graph file: " + ctx->err);
     return s;
+}
+
+// Ingest with cleaning on the device: sort + dedup drop duplicate edges
+// (tools/RmDupEdges.C) and self-loops (tools/RmSelfEdges.C); SYMMETRISE adds
+// every edge's reverse first (tools/CvtToUndir.C).
+static gg_status graph_from_keys(gg_ctx *ctx, uint32_t n, uint64_t *keys, uint64_t nk, int sym, gg_graph **out) {
+    const int lg = ceil_log2(n);
+    uint64_t *off = nullptr;
+    uint32_t *adj = nullptr;
+    uint64_t m = 0;
+    gg_status s = build_from_keys(ctx, n, keys, nk, lg, &off, &adj, &m);
+    cudaFree(keys);
+    if (s != GG_OK) return s;
+    return graph_adopt_device_csr(ctx, n, m, off, adj, sym, out);
+}
+
+gg_status gg_graph_from_edges(gg_ctx *ctx, uint32_t n, uint64_t nedges, const uint32_t *src, const uint32_t *dst,
+                              int flags, gg_graph **out) {
+    if (!ctx || !out || (nedges && (!src || !dst)) || n == 0xFFFFFFFFu || (flags & ~3)) return GG_ERR_ARG;
+    *out = nullptr;
+    const bool dev = flags & GG_INGEST_DEVICE, sym = flags & GG_INGEST_SYMMETRISE;
+    if (!dev)
+        for (uint64_t i = 0; i < nedges; ++i)
+            if (src[i] >= n || dst[i] >= n) return set_error(ctx, GG_ERR_ARG, "gg_graph_from_edges: vertex id out of range");
+    GG_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const uint64_t nk = sym ? 2 * nedges : nedges;
+    uint64_t *keys = nullptr;
+    uint32_t *tmp = nullptr, *bad = nullptr;
+    auto fail = [&](cudaError_t e) {
+        cudaFree(keys); cudaFree(tmp); cudaFree(bad);
+        return cuda_error(ctx, e, "gg_graph_from_edges");
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&keys, (nk ? nk : 1) * 8)) != cudaSuccess) return fail(e);
+    if ((e = cudaMalloc(&bad, 4)) != cudaSuccess || (e = cudaMemsetAsync(bad, 0, 4, st)) != cudaSuccess) return fail(e);
+    const uint32_t *ds = src, *dd = dst;
+    if (!dev && nedges) {
+        if ((e = cudaMalloc(&tmp, nedges * 8)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(tmp, src, nedges * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(tmp + nedges, dst, nedges * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+            return fail(e);
+        ds = tmp;
+        dd = tmp + nedges;
+    }
+    if (nedges) {
+        k_edges_to_keys<<<grid_for(ctx, nedges), 256, 0, st>>>(ds, dd, nedges, n, ceil_log2(n), sym, keys, bad);
+        ctx->launches++;
+    }
+    uint32_t hbad = 0;
+    if ((e = cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return fail(e);
+    cudaFree(tmp);
+    cudaFree(bad);
+    if (hbad) {
+        cudaFree(keys);
+        return set_error(ctx, GG_ERR_ARG, "gg_graph_from_edges: vertex id out of range");
+    }
+    return graph_from_keys(ctx, n, keys, nk, sym, out);
+}
+
+gg_status gg_graph_read_bin_clean(gg_ctx *ctx, const char *path, int flags, gg_graph **out) {
+    if (!ctx || !path || !out || (flags & ~GG_INGEST_SYMMETRISE)) return GG_ERR_ARG;
+    *out = nullptr;
+    FILE *f = fopen(path, "rb");
+    if (!f) return set_error(ctx, GG_ERR_IO, std::string("cannot open ") + path);
+    uint64_t hdr[8];
+    if (fread(hdr, sizeof(hdr), 1, f) != 1) { fclose(f); return set_error(ctx, GG_ERR_IO, "short header"); }
+    if ((hdr[0] != 2 && hdr[0] != 3) || hdr[4] != 4 || hdr[5] != 8 || hdr[2] >= 0xFFFFFFFFull) {
+        fclose(f);
+        return set_error(ctx, GG_ERR_IO, "not a Graptor v2/v3 file with 4-byte VID / 8-byte EID");
+    }
+    const uint32_t n = (uint32_t)hdr[2];
+    const uint64_t m = hdr[3];
+    std::vector<uint64_t> off;
+    std::vector<uint32_t> adj;
+    try {
+        off.resize((size_t)n + 1);
+        adj.resize(m);
+    } catch (...) {
+        fclose(f);
+        return set_error(ctx, GG_ERR_OOM, "host allocation");
+    }
+    bool ok = n == 0 || fread(off.data(), 8, n, f) == n;
+    if (ok && hdr[0] == 3) {
+        uint64_t last = 0;
+        ok = fread(&last, 8, 1, f) == 1 && last == m;
+    }
+    ok = ok && (m == 0 || fread(adj.data(), 4, m, f) == m);
+    fclose(f);
+    if (!ok) return set_error(ctx, GG_ERR_IO, "truncated graph file");
+    off[n] = m;
+    if (off[0] != 0) return set_error(ctx, GG_ERR_IO, "corrupt graph file: first offset");
+    for (uint32_t v = 0; v < n; ++v)
+        if (off[v] > off[v + 1]) return set_error(ctx, GG_ERR_IO, "corrupt graph file: offsets not monotone");
+    for (uint64_t e = 0; e < m; ++e)
+        if (adj[e] >= n) return set_error(ctx, GG_ERR_IO, "corrupt graph file: vertex id out of range");
+    GG_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const bool sym = flags & GG_INGEST_SYMMETRISE;
+    const uint64_t nk = sym ? 2 * m : m;
+    uint64_t *doff = nullptr, *keys = nullptr;
+    uint32_t *dadj = nullptr;
+    auto fail = [&](cudaError_t e) {
+        cudaFree(doff); cudaFree(dadj); cudaFree(keys);
+        return cuda_error(ctx, e, "gg_graph_read_bin_clean");
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&doff, ((size_t)n + 1) * 8)) != cudaSuccess || (e = cudaMalloc(&dadj, (m ? m : 1) * 4)) != cudaSuccess ||
+        (e = cudaMalloc(&keys, (nk ? nk : 1) * 8)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(doff, off.data(), ((size_t)n + 1) * 8, cudaMemcpyHostToDevice, st)) != cudaSuccess ||
+        (m && (e = cudaMemcpyAsync(dadj, adj.data(), m * 4, cudaMemcpyHostToDevice, st)) != cudaSuccess))
+        return fail(e);
+    if (m) {
+        k_csr_to_keys<<<grid_for(ctx, (uint64_t)n * 32), 256, 0, st>>>(doff, dadj, n, ceil_log2(n), sym, m, keys);
+        ctx->launches++;
+    }
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail(e);
+    cudaFree(doff);
+    cudaFree(dadj);
+    return graph_from_keys(ctx, n, keys, nk, sym, out);
 }
 
 gg_status gg_graph_write_bin(gg_graph *g, const char *path) {

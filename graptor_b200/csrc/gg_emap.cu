@@ -41,6 +41,8 @@
 namespace gg {
 
 constexpr unsigned FULL = 0xffffffffu;
+constexpr uint32_t kLargeLocal = 1024;  // push: large bins up to this size chunked in shared memory
+constexpr int kAppCap = 128;            // push: staged list appends per warp and bin
 
 struct EmapArgs {
     const uint64_t *off;      // CSR (push, out-degree)
@@ -61,6 +63,7 @@ struct EmapArgs {
     int K;
     const uint64_t *large_first;  // [c2 + 1] chunk prefix of the large bin (push)
     uint32_t large_ch;            // edges per large-bin chunk
+    int merge_med;                // push: medium bin chunked with the large one (small frontiers)
     // pull candidate lists (drivers only): the destinations that can still
     // pass the (monotone) dst filter.  cand == nullptr: scan all vertices.
     const uint32_t *cand;
@@ -325,9 +328,39 @@ __global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
 // W = 32, or a CTA, W = BLOCK; `t` = this thread's index among them), four
 // edges per thread in flight: the loads of the four targets' values and the
 // four atomics overlap instead of forming four dependent round trips.
-template <int R, int W>
+// Output list appends of one warp staged in shared memory per degree bin:
+// one global atomic per ~CAP records instead of one per warp round (the bin
+// counters are the hottest addresses of a push that activates many vertices).
+template <int CAP>
+struct BinAppender {
+    dev::WarpAppender<CAP> ap[NBINS];
+    unsigned long long nv = 0, ne = 0;
+    __device__ __forceinline__ void init(const EmapArgs &A, uint32_t *warp_buf) {
+        uint32_t *dst[NBINS] = {A.out_b0, A.out_b1, A.out_b2};
+#pragma unroll
+        for (int b = 0; b < NBINS; ++b) ap[b] = {warp_buf + b * CAP, 0u, dst[b], A.out_cnt + FC_BIN0 + b};
+    }
+    // all 32 lanes together
+    __device__ __forceinline__ void emit(const EmapArgs &A, bool rec, uint32_t d) {
+        uint64_t deg = 0;
+        if (rec) {
+            deg = A.off[d + 1] - A.off[d];
+            nv++;
+            ne += deg;
+        }
+        const uint32_t bin = deg <= A.smax ? 0u : (deg <= A.mmax ? 1u : 2u);
+#pragma unroll
+        for (int b = 0; b < NBINS; ++b) ap[b].push(rec && bin == (uint32_t)b, d);
+    }
+    __device__ __forceinline__ void flush() {
+#pragma unroll
+        for (int b = 0; b < NBINS; ++b) ap[b].flush();
+    }
+};
+
+template <int R, int W, typename Emit>
 __device__ __forceinline__ void push_edges(const EmapArgs &A, const Op<R> &op, typename Op<R>::V sv, uint64_t beg,
-                                           uint64_t end, uint32_t t, unsigned long long &nv, unsigned long long &ne) {
+                                           uint64_t end, uint32_t t, Emit &&emit) {
     constexpr int U = 4;
     for (uint64_t base = beg; base < end; base += (uint64_t)W * U) {
         uint32_t d[U];
@@ -345,7 +378,7 @@ __device__ __forceinline__ void push_edges(const EmapArgs &A, const Op<R> &op, t
 #pragma unroll
         for (int u = 0; u < U; ++u) {
             if (base + (uint64_t)u * W >= end) break;  // uniform across the W threads
-            emit_out(A, rec[u], d[u], nv, ne);
+            emit(rec[u], d[u]);
         }
     }
 }
@@ -355,24 +388,49 @@ __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uin
                                                        uint32_t nb_med) {
     using V = typename Op<R>::V;
     const uint32_t lane = threadIdx.x & 31u;
-    unsigned long long nv = 0, ne = 0, sc = 0;
+    unsigned long long sc = 0;
+    __shared__ uint64_t s_first[kLargeLocal + 1];
+    __shared__ uint32_t s_app[BLOCK / 32][NBINS * kAppCap];
+    BinAppender<kAppCap> app;
+    app.init(A, s_app[threadIdx.x >> 5]);
+    auto emit = [&](bool rec, uint32_t d) { app.emit(A, rec, d); };
     if (blockIdx.x < nb_large) {
         // large bin: rows cut into chunks of large_ch edges, a CTA per chunk,
-        // so one hub row is spread over many SMs
-        const uint64_t nch = A.large_first[A.c2];
+        // so one hub row is spread over many SMs.  The chunk prefix is built
+        // by each CTA in shared memory when the bin is small (no extra
+        // launches), else read from large_first (built on the device before).
+        // With merge_med the medium bin joins it (rows c2.. of the table):
+        // a frontier of a few vertices then still spreads over many CTAs.
+        const uint32_t cm = A.c2 + (A.merge_med ? A.c1 : 0u);
+        auto row = [&](uint32_t i) { return i < A.c2 ? A.in_b2[i] : A.in_b1[i - A.c2]; };
+        const uint64_t *first = A.large_first;
+        if (!first) {
+            for (uint32_t i = threadIdx.x; i < cm; i += BLOCK) {
+                const uint32_t v = row(i);
+                s_first[i + 1] = (A.off[v + 1] - A.off[v] + A.large_ch - 1) / A.large_ch;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                s_first[0] = 0;
+                for (uint32_t i = 1; i <= cm; ++i) s_first[i] += s_first[i - 1];
+            }
+            __syncthreads();
+            first = s_first;
+        }
+        const uint64_t nch = first[cm];
         for (uint64_t c = blockIdx.x; c < nch; c += nb_large) {
-            uint32_t lo = 0, hi = A.c2;  // last h with large_first[h] <= c
+            uint32_t lo = 0, hi = cm;  // last h with first[h] <= c
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (A.large_first[mid] <= c) lo = mid; else hi = mid;
+                if (first[mid] <= c) lo = mid; else hi = mid;
             }
-            const uint32_t s = A.in_b2[lo];
+            const uint32_t s = row(lo);
             const V sv = op.src_val(s);
             const uint64_t rb = A.off[s], re = A.off[s + 1];
-            const uint64_t beg = rb + (c - A.large_first[lo]) * A.large_ch;
+            const uint64_t beg = rb + (c - first[lo]) * A.large_ch;
             const uint64_t end = min(beg + A.large_ch, re);
             if (threadIdx.x == 0) sc += end - beg;
-            push_edges<R, BLOCK>(A, op, sv, beg, end, threadIdx.x, nv, ne);
+            push_edges<R, BLOCK>(A, op, sv, beg, end, threadIdx.x, emit);
         }
     } else if (blockIdx.x < nb_large + nb_med) {
         // medium bin: a warp per source vertex
@@ -384,7 +442,7 @@ __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uin
             const V sv = op.src_val(s);
             const uint64_t beg = A.off[s], end = A.off[s + 1];
             if (lane == 0) sc += end - beg;
-            push_edges<R, 32>(A, op, sv, beg, end, lane, nv, ne);
+            push_edges<R, 32>(A, op, sv, beg, end, lane, emit);
         }
     } else {
         // small bin: a thread per source vertex, warp-uniform edge loop
@@ -413,11 +471,12 @@ __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uin
                     d = __ldg(A.adj + beg + k);
                     rec = op.offer(d, sv, A.record, A.out_bits);
                 }
-                emit_out(A, rec, d, nv, ne);
+                app.emit(A, rec, d);
             }
         }
     }
-    flush_counts<BLOCK>(A, nv, ne, sc);
+    app.flush();
+    flush_counts<BLOCK>(A, app.nv, app.ne, sc);
 }
 
 // chunks of each large-bin vertex's row (first[c2] = 0 before the scan)
@@ -749,9 +808,13 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
         A.c2 = (uint32_t)in->h_cnt[FC_BIN2];
         const uint32_t cap = ctx->sm_count * t.blocks_per_sm;
         uint32_t nb_large = 0;
-        if (A.c2) {
+        A.large_ch = t.large_chunk;
+        A.large_first = nullptr;  // small large bin: chunk table built inside the kernel
+        // a few medium rows: chunk them like large rows, one CTA per chunk,
+        // instead of one warp walking each row alone
+        A.merge_med = A.c1 && A.c1 + A.c2 <= kLargeLocal && A.c1 < ctx->sm_count;
+        if (A.c2 > kLargeLocal) {
             // chunk table of the large bin: counts, then an exclusive scan
-            A.large_ch = t.large_chunk;
             size_t cub_bytes = 0;
             GG_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, cub_bytes, (uint64_t *)nullptr,
                                                        (uint64_t *)nullptr, (int64_t)A.c2 + 1, st));
@@ -765,11 +828,13 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
                                                        (int64_t)A.c2 + 1, st));
             ctx->launches++;
             A.large_first = first;
+        }
+        if (A.c2 || A.merge_med) {
             // upper bound on the chunk count from the host-known edge total
-            const uint64_t est = in->h_cnt[FC_NACTE] / A.large_ch + A.c2;
+            const uint64_t est = in->h_cnt[FC_NACTE] / A.large_ch + A.c2 + (A.merge_med ? A.c1 : 0);
             nb_large = (uint32_t)std::min<uint64_t>(est, cap);
         }
-        uint32_t nb_med = std::min<uint32_t>((A.c1 + kBlock / 32 - 1) / (kBlock / 32), cap);
+        uint32_t nb_med = A.merge_med ? 0 : std::min<uint32_t>((A.c1 + kBlock / 32 - 1) / (kBlock / 32), cap);
         uint32_t nb_small = std::min<uint32_t>((A.c0 + kBlock - 1) / kBlock, cap);
         uint32_t grid = nb_large + nb_med + nb_small;
         tstart();
@@ -815,7 +880,10 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     if (ctx->time_kernels) cudaEventRecord(ctx->evk1, st);
     if (have_out) {
         const bool list_written = variant != GG_VAR_PULL_DENSE;
-        if (d->record == GG_RECORD_NE_PREV && variant != GG_VAR_PULL_DENSE) {
+        // level-synchronous BFS: a push's unique first writer records d and no
+        // later step compares prev of a visited vertex, so no copy is needed
+        const bool sync_levels = d->src_level_sync && d->relax == GG_RELAX_MIN_PLUS1_I32;
+        if (d->record == GG_RECORD_NE_PREV && variant != GG_VAR_PULL_DENSE && !sync_levels) {
             if (!d->prev) return set_error(ctx, GG_ERR_ARG, "NE_PREV record needs prev");
             k_copy_prev<<<persistent_grid(ctx, words), kBlock, 0, st>>>(
                 out->bins[0], out->bins[1], out->bins[2], out->d_cnt, op.a, op.prev);
@@ -892,7 +960,7 @@ gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_f
     }
     gg_status s;
     ctx->time_kernels = stats != nullptr;
-    cudaEventRecord(ctx->evk0, ctx->stream);  // defined start even if nothing launches
+    if (stats) cudaEventRecord(ctx->evk0, ctx->stream);  // defined start even if nothing launches
     switch (d->relax) {
     case GG_RELAX_MIN_PLUS1_I32: s = launch_variant<GG_RELAX_MIN_PLUS1_I32>(g, d, in, out, variant); break;
     case GG_RELAX_MIN_U32: s = launch_variant<GG_RELAX_MIN_U32>(g, d, in, out, variant); break;

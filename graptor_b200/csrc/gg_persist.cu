@@ -888,8 +888,18 @@ __device__ void phase_merge_push(const PArgs &P, const POp<R> &op, const PFront 
 
 // Threshold / fixed / learned choice; identical in every CTA (same inputs,
 // same arithmetic).  Returns a gg_variant.
+// Last network evaluation of this CTA: consecutive iterations of a
+// high-diameter traversal have nearly the same features, and the choice is
+// reused while every feature stays within kSelReuse of the evaluated ones
+// (every CTA sees the same sequence, so all CTAs still agree).
+struct SelCache {
+    float x[GG_SEL_FEATURES];
+    int choice;
+    int valid;
+};
+
 __device__ int choose_variant(const PArgs &P, int iter, unsigned long long nactv, unsigned long long nacte,
-                              bool f_all, const PState *st, int *s_choice) {
+                              bool f_all, const PState *st, int *s_choice, SelCache *cache) {
     if (f_all) return GG_VAR_PULL_DENSE;
     if (iter == P.force_iter) return P.force_variant;
     if (P.variant >= 0) return P.variant;
@@ -916,15 +926,29 @@ __device__ int choose_variant(const PArgs &P, int iter, unsigned long long nactv
                 x[7] = (float)(m > 0 ? fe / m : 0);
                 x[8] = (float)fmin(4.0, m > 0 ? (fv + fe) / m : 0.0);
                 x[9] = (float)(log2(n > 1 ? n : 1.0) / 32);
-                float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
-                mlp::warp_forward(P.sel_w, x, o, z1, a1, z2, a2);
-                int best = 0;
-                for (int v = 1; v < GG_SEL_VARIANTS; ++v)
-                    if (o[v] < o[best]) best = v;
-                // the threshold's choice stands unless the network predicts
-                // a clear gain over it
-                const int tv = (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
-                if (!(o[best] < o[tv] - mlp::kSelMargin)) best = tv;
+                bool reuse = cache->valid != 0;
+                for (int i = 0; i < GG_SEL_FEATURES && reuse; ++i)
+                    reuse = fabsf(x[i] - cache->x[i]) <= (i == 3 ? 8.0f / 64 : 1.0f / 64);
+                int best;
+                if (reuse) {
+                    best = cache->choice;
+                } else {
+                    float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
+                    mlp::warp_forward(P.sel_w, x, o, z1, a1, z2, a2);
+                    best = 0;
+                    for (int v = 1; v < GG_SEL_VARIANTS; ++v)
+                        if (o[v] < o[best]) best = v;
+                    // the threshold's choice stands unless the network
+                    // predicts a clear gain over it
+                    const int tv = (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+                    if (!(o[best] < o[tv] - mlp::kSelMargin)) best = tv;
+                    __syncwarp();
+                    if (threadIdx.x == 0) {
+                        for (int i = 0; i < GG_SEL_FEATURES; ++i) cache->x[i] = x[i];
+                        cache->choice = best;
+                        cache->valid = 1;
+                    }
+                }
                 if (threadIdx.x == 0) *s_choice = best;
             }
             __syncthreads();
@@ -942,6 +966,9 @@ template <int R>
 __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
     __shared__ __align__(16) uint32_t smem[kSmemWords];
     __shared__ int s_choice;
+    __shared__ SelCache s_sel;
+    if (threadIdx.x == 0) s_sel.valid = 0;
+    __syncthreads();
     static_assert(kSmemWords * 4 >= (kLargeScan + 1) * 8, "chunk table fits the shared buffer");
     PState *st = P.st;
     POp<R> op;
@@ -964,7 +991,7 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
         const int f_all = ldcg(&st->all[cur]);
         if (nactv == 0 && !f_all) break;
         if (P.level_k) op.fk = iter + 1;
-        const int var = choose_variant(P, iter, nactv, nacte, f_all != 0, st, &s_choice);
+        const int var = choose_variant(P, iter, nactv, nacte, f_all != 0, st, &s_choice, &s_sel);
         const bool pushes = var != GG_VAR_PULL_DENSE;
         if (blockIdx.x == 0 && threadIdx.x == 0 && iter == P.force_iter) {
             st->f_nactv = nactv;

@@ -59,15 +59,18 @@ template <> struct Store<GG_F32> {
     __device__ static float dec(T v) { return v; }
     __device__ static T enc(float f) { return f; }
 };
+// bfloat16 / float16 stored as raw 16-bit words: plain integer loads and
+// stores (the class types' assignment made the bfloat16 update kernel several
+// times slower than the float16 one).
 template <> struct Store<GG_BF16> {
-    using T = __nv_bfloat16;
-    __device__ static float dec(T v) { return __bfloat162float(v); }
-    __device__ static T enc(float f) { return __float2bfloat16_rn(f); }
+    using T = uint16_t;
+    __device__ static float dec(T v) { return __uint_as_float((uint32_t)v << 16); }
+    __device__ static T enc(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
 };
 template <> struct Store<GG_F16> {
-    using T = __half;
-    __device__ static float dec(T v) { return __half2float(v); }
-    __device__ static T enc(float f) { return __float2half_rn(f); }
+    using T = uint16_t;
+    __device__ static float dec(T v) { return __half2float(__ushort_as_half(v)); }
+    __device__ static T enc(float f) { return __half_as_ushort(__float2half_rn(f)); }
 };
 template <> struct Store<GG_FP8E4M3> {
     using T = __nv_fp8_storage_t;
@@ -102,7 +105,18 @@ struct PrState {
     int maxiter;
     double tol;
     double deltas[GG_MAX_ITERS];
+    // staged runs (PR_vary's run_prec_X then run_prec_Y): the active stage,
+    // each stage's dtype and residual bound, and a re-encode request raised
+    // when the stage changes
+    int stage, nstages, reencode;
+    int stage_dt[4];
+    double stage_tol[4];
 };
+
+// true when a kernel of stage `stage` (-1: unstaged) has nothing to do
+__device__ __forceinline__ bool pr_idle(const PrState *st, int stage) {
+    return st && (st->done || (stage >= 0 && st->stage != stage));
+}
 
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -123,12 +137,12 @@ __global__ void __launch_bounds__(BLOCK)
 k_pr_gather(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj,
             const typename Store<DT>::T *__restrict__ contrib, uint32_t n, float *y_f32,
             double *y_f64, PrState *st, float scale_inv_arg, int K, uint32_t T, int stream,
-            const uint64_t *__restrict__ word_prefix) {
+            const uint64_t *__restrict__ word_prefix, int stage) {
     using S = Store<DT>;
     using Acc = typename std::conditional<ACC64, double, float>::type;
     constexpr int U = 4;  // 32-edge chunks in flight per warp iteration
     __shared__ Acc sm[BLOCK / 32][33];
-    if (st && st->done) return;
+    if (pr_idle(st, stage)) return;
     const float sinv = st ? st->scale_inv : scale_inv_arg;
     const uint32_t lane = threadIdx.x & 31u;
     Acc *row = sm[threadIdx.x >> 5];
@@ -241,10 +255,11 @@ template <int DT, bool ACC64>
 __global__ void __launch_bounds__(256)
 k_pr_heavy_chunks(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj,
                   const typename Store<DT>::T *__restrict__ contrib, HeavyRows H,
-                  typename std::conditional<ACC64, double, float>::type *partial, const PrState *st) {
+                  typename std::conditional<ACC64, double, float>::type *partial, const PrState *st,
+                  int stage) {
     using S = Store<DT>;
     using Acc = typename std::conditional<ACC64, double, float>::type;
-    if (st && st->done) return;
+    if (pr_idle(st, stage)) return;
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < H.nchunks; c += nw) {
@@ -276,9 +291,9 @@ k_pr_heavy_chunks(const uint64_t *__restrict__ in_off, const uint32_t *__restric
 template <int DT, bool ACC64, bool ADD_OLD, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_pr_heavy_finalize(HeavyRows H, const typename std::conditional<ACC64, double, float>::type *partial,
-                    float *y_f32, double *y_f64, PrState *st, float scale_inv_arg) {
+                    float *y_f32, double *y_f64, PrState *st, float scale_inv_arg, int stage) {
     using Acc = typename std::conditional<ACC64, double, float>::type;
-    if (st && st->done) return;
+    if (pr_idle(st, stage)) return;
     const float sinv = st ? st->scale_inv : scale_inv_arg;
     double ysum = 0;
     for (uint32_t h = blockIdx.x * BLOCK + threadIdx.x; h < H.nheavy; h += gridDim.x * BLOCK) {
@@ -305,9 +320,10 @@ k_pr_heavy_finalize(HeavyRows H, const typename std::conditional<ACC64, double, 
 template <int DT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_pr_update(const XT<DT> *__restrict__ y, XT<DT> *__restrict__ x, typename Store<DT>::T *contrib,
-            const uint64_t *__restrict__ off, uint32_t n, float damp, double damp64, int renorm_f32, PrState *st) {
+            const uint64_t *__restrict__ off, uint32_t n, float damp, double damp64, int renorm_f32, PrState *st,
+            int stage) {
     using S = Store<DT>;
-    if (st->done) return;
+    if (pr_idle(st, stage)) return;
     const double s1 = st->s1;
     const double w = (1.0 - s1) / (double)n;
     const double s2 = s1 + (double)n * w;
@@ -355,16 +371,61 @@ k_pr_update(const XT<DT> *__restrict__ y, XT<DT> *__restrict__ x, typename Store
 }
 
 __global__ void k_pr_finish(PrState *st, int dt) {
+    st->reencode = 0;
     if (st->done) return;
     const int it = st->iters;
     if (it < GG_MAX_ITERS) st->deltas[it] = st->delta;
     st->iters = it + 1;
-    if (st->iters >= st->maxiter || !(st->delta > st->tol)) st->done = 1;
-    st->scale_inv = 1.0f / st->scale;  // decode of what the update just wrote
-    st->scale = scale_for(dt, st->cmax);  // next encode
+    if (st->nstages > 1) dt = st->stage_dt[st->stage];
+    if (st->stage + 1 < st->nstages && !(st->delta > st->stage_tol[st->stage])) {
+        // next stage: its re-encode kernels rewrite the contributions from x
+        st->stage++;
+        st->reencode = 1;
+        if (st->iters >= st->maxiter) st->done = 1;
+    } else {
+        if (st->iters >= st->maxiter || !(st->delta > st->tol)) st->done = 1;
+        st->scale_inv = 1.0f / st->scale;     // decode of what the update just wrote
+        st->scale = scale_for(dt, st->cmax);  // next encode
+    }
     st->s1 = 0;
     st->delta = 0;
     st->cmax = 0.0f;
+}
+
+// Scale of the contributions about to be encoded, from the max found by the
+// pass-0 kernel (one thread, between the two passes: every CTA of pass 1
+// then reads the same value).  stage >= 0: only when that stage re-encodes.
+__global__ void k_pr_setscale(PrState *st, int dt, int stage) {
+    if (stage >= 0 && (st->done || !st->reencode || st->stage != stage)) return;
+    const float sc = scale_for(dt, st->cmax);
+    st->scale = sc;
+    st->scale_inv = 1.0f / sc;
+    st->cmax = 0.0f;
+}
+
+// A new stage's contributions from the current ranks: pass 0 finds the
+// max, pass 1 encodes with st->scale.
+template <int DT, int BLOCK>
+__global__ void k_pr_reencode(const float *x, typename Store<DT>::T *contrib, const uint64_t *off, uint32_t n,
+                              float damp, PrState *st, int stage, int pass) {
+    using S = Store<DT>;
+    if (st->done || !st->reencode || st->stage != stage) return;
+    float cm = 0.0f;
+    const float scale = st->scale;
+    const uint32_t stride = gridDim.x * BLOCK;
+    for (uint32_t v = blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
+        const uint64_t deg = off[v + 1] - off[v];
+        const float c = damp * x[v] / (float)deg;
+        if (pass == 0) {
+            if (deg && c > cm) cm = c;
+        } else {
+            contrib[v] = S::enc(scaled_format(DT) ? c * scale : c);
+        }
+    }
+    if (pass == 0) {
+        for (int o = 16; o > 0; o >>= 1) cm = fmaxf(cm, __shfl_xor_sync(FULL, cm, o));
+        if ((threadIdx.x & 31) == 0) atomicMax((int *)&st->cmax, __float_as_int(cm));
+    }
 }
 
 // Initial x = 1/n, contrib = d*x/deg (PRv.C:155-182); first pass finds the max.
@@ -389,7 +450,7 @@ __global__ void k_pr_init(XT<DT> *x, typename Store<DT>::T *contrib, const uint6
         }
         return;
     }
-    const float scale = pass == 1 ? scale_for(DT, st->cmax) : 1.0f;
+    const float scale = pass == 1 ? st->scale : 1.0f;  // set by k_pr_setscale between the passes
     for (uint32_t v = blockIdx.x * BLOCK + threadIdx.x; v < n; v += stride) {
         const uint64_t deg = off[v + 1] - off[v];
         const float c = damp * x0 / (float)deg;
@@ -403,10 +464,6 @@ __global__ void k_pr_init(XT<DT> *x, typename Store<DT>::T *contrib, const uint6
     if (pass == 0) {
         for (int o = 16; o > 0; o >>= 1) cm = fmaxf(cm, __shfl_xor_sync(FULL, cm, o));
         if ((threadIdx.x & 31) == 0) atomicMax((int *)&st->cmax, __float_as_int(cm));
-    } else if (blockIdx.x == 0 && threadIdx.x == 0) {
-        st->scale = scale;
-        st->scale_inv = 1.0f / scale;
-        st->cmax = 0.0f;
     }
 }
 
@@ -422,7 +479,7 @@ static unsigned pr_grid(gg_ctx *ctx, uint64_t work) {
 // gather of one iteration / one API call: light rows, heavy chunks, heavy totals
 template <int DT, bool ACC64, bool ADD_OLD>
 static gg_status gather_launch(gg_graph *g, const typename Store<DT>::T *contrib, float *yf,
-                               double *yd, PrState *st, float sinv, void *partial) {
+                               double *yd, PrState *st, float sinv, void *partial, int stage = -1) {
     gg_ctx *ctx = g->ctx;
     cudaStream_t s = ctx->stream;
     using Acc = typename std::conditional<ACC64, double, float>::type;
@@ -433,18 +490,18 @@ static gg_status gather_launch(gg_graph *g, const typename Store<DT>::T *contrib
     if (blocks > cap) blocks = cap;
     k_pr_gather<DT, ACC64, ADD_OLD, 256><<<(unsigned)(blocks ? blocks : 1), 256, 0, s>>>(
         g->in_off, g->in_adj, contrib, g->n, yf, yd, st, sinv, tuning().pull_k, H.T, tuning().pr_stream,
-        H.light_prefix);
+        H.light_prefix, stage);
     GG_LAUNCHED(ctx);
     if (H.nchunks) {
         uint64_t cb = (H.nchunks * 32 + 255) / 256;
         if (cb > cap) cb = cap;
         k_pr_heavy_chunks<DT, ACC64><<<(unsigned)cb, 256, 0, s>>>(g->in_off, g->in_adj, contrib, H,
-                                                                  (Acc *)partial, st);
+                                                                  (Acc *)partial, st, stage);
         GG_LAUNCHED(ctx);
         uint64_t fb = (H.nheavy + 255) / 256;
         if (fb > cap) fb = cap;
         k_pr_heavy_finalize<DT, ACC64, ADD_OLD, 256><<<(unsigned)fb, 256, 0, s>>>(H, (const Acc *)partial, yf, yd,
-                                                                                 st, sinv);
+                                                                                 st, sinv, stage);
         GG_LAUNCHED(ctx);
     }
     return GG_OK;
@@ -473,6 +530,8 @@ static gg_status pr_run(gg_graph *g, const gg_pr_params *p, XT<DT> *x, XT<DT> *y
     const double d64 = damping_f64(p->damping);
     k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, n, p->damping, d64, st, 0);
     GG_LAUNCHED(ctx);
+    k_pr_setscale<<<1, 1, 0, s>>>(st, DT, -1);
+    GG_LAUNCHED(ctx);
     k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, n, p->damping, d64, st, 1);
     GG_LAUNCHED(ctx);
     float *yf = DT == GG_F64 ? nullptr : (float *)y;
@@ -483,10 +542,83 @@ static gg_status pr_run(gg_graph *g, const gg_pr_params *p, XT<DT> *x, XT<DT> *y
         else
             GG_CHECK((gather_launch<DT, false, false>(g, (const T *)contrib, yf, yd, st, 1.0f, partial)));
         k_pr_update<DT, kBlock><<<gv, kBlock, 0, s>>>(y, x, (T *)contrib, g->off, n, p->damping, d64,
-                                                      p->renorm_f32, st);
+                                                      p->renorm_f32, st, -1);
         GG_LAUNCHED(ctx);
         k_pr_finish<<<1, 1, 0, s>>>(st, DT);
         GG_LAUNCHED(ctx);
+    }
+    return GG_OK;
+}
+
+// Staged runs (PR_vary.C:652-757, e.g. VARIANT 4620 = run_prec_46 with
+// customfp<6,10> contributions until the residual is below 1e-3, then
+// run_prec_20 with FP32 contributions and double sums until 1e-7): every
+// iteration launches each stage's kernels and those of inactive stages return
+// at once, so the switch is taken on the device without a host round trip.
+enum { OP_GATHER, OP_UPDATE, OP_REENC0, OP_SETSCALE, OP_REENC1, OP_INIT0, OP_INIT1 };
+
+template <int DT>
+static gg_status stage_op(gg_graph *g, int op, int stage, bool acc64, const gg_pr_params *p, float *x, float *y,
+                          void *contrib, PrState *st, void *partial) {
+    using T = typename Store<DT>::T;
+    gg_ctx *ctx = g->ctx;
+    cudaStream_t s = ctx->stream;
+    const unsigned gv = pr_grid(ctx, g->n);
+    switch (op) {
+    case OP_GATHER:
+        if (acc64) return gather_launch<DT, true, false>(g, (const T *)contrib, y, nullptr, st, 1.0f, partial, stage);
+        return gather_launch<DT, false, false>(g, (const T *)contrib, y, nullptr, st, 1.0f, partial, stage);
+    case OP_UPDATE:
+        k_pr_update<DT, kBlock><<<gv, kBlock, 0, s>>>(y, x, (T *)contrib, g->off, g->n, p->damping, 0.0,
+                                                      p->renorm_f32, st, stage);
+        break;
+    case OP_REENC0:
+    case OP_REENC1:
+        k_pr_reencode<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, g->n, p->damping, st, stage,
+                                                        op == OP_REENC1);
+        break;
+    case OP_SETSCALE: k_pr_setscale<<<1, 1, 0, s>>>(st, DT, stage); break;
+    default:
+        k_pr_init<DT, kBlock><<<gv, kBlock, 0, s>>>(x, (T *)contrib, g->off, g->n, p->damping, 0.0, st,
+                                                    op == OP_INIT1);
+        break;
+    }
+    GG_LAUNCHED(ctx);
+    return GG_OK;
+}
+
+static gg_status stage_dispatch(int dt, gg_graph *g, int op, int stage, bool acc64, const gg_pr_params *p,
+                                float *x, float *y, void *contrib, PrState *st, void *partial) {
+    switch (dt) {
+    case GG_F32: return stage_op<GG_F32>(g, op, stage, acc64, p, x, y, contrib, st, partial);
+    case GG_BF16: return stage_op<GG_BF16>(g, op, stage, acc64, p, x, y, contrib, st, partial);
+    case GG_F16: return stage_op<GG_F16>(g, op, stage, acc64, p, x, y, contrib, st, partial);
+    case GG_FP8E4M3: return stage_op<GG_FP8E4M3>(g, op, stage, acc64, p, x, y, contrib, st, partial);
+    case GG_CFP_6_10: return stage_op<GG_CFP_6_10>(g, op, stage, acc64, p, x, y, contrib, st, partial);
+    default: return stage_op<GG_BF16_TRUNC>(g, op, stage, acc64, p, x, y, contrib, st, partial);
+    }
+}
+
+static gg_status pr_run_staged(gg_graph *g, const gg_pr_params *p, float *x, float *y, void *contrib,
+                               PrState *st, void *partial) {
+    const int ns = p->nstages;
+    const int *dt = p->stage_dtype;
+    const int *acc = p->stage_accum_f64;
+    GG_CHECK(stage_dispatch(dt[0], g, OP_INIT0, -1, false, p, x, y, contrib, st, partial));
+    GG_CHECK(stage_dispatch(dt[0], g, OP_SETSCALE, -1, false, p, x, y, contrib, st, partial));
+    GG_CHECK(stage_dispatch(dt[0], g, OP_INIT1, -1, false, p, x, y, contrib, st, partial));
+    for (int it = 0; it < p->maxiter; ++it) {
+        for (int k = 0; k < ns; ++k)
+            GG_CHECK(stage_dispatch(dt[k], g, OP_GATHER, k, acc[k] != 0, p, x, y, contrib, st, partial));
+        for (int k = 0; k < ns; ++k)
+            GG_CHECK(stage_dispatch(dt[k], g, OP_UPDATE, k, false, p, x, y, contrib, st, partial));
+        k_pr_finish<<<1, 1, 0, g->ctx->stream>>>(st, dt[0]);
+        GG_LAUNCHED(g->ctx);
+        for (int k = 1; k < ns; ++k) {
+            GG_CHECK(stage_dispatch(dt[k], g, OP_REENC0, k, false, p, x, y, contrib, st, partial));
+            GG_CHECK(stage_dispatch(dt[k], g, OP_SETSCALE, k, false, p, x, y, contrib, st, partial));
+            GG_CHECK(stage_dispatch(dt[k], g, OP_REENC1, k, false, p, x, y, contrib, st, partial));
+        }
     }
     return GG_OK;
 }
@@ -533,10 +665,16 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
     if (!g || !p) return GG_ERR_ARG;
     gg_ctx *ctx = g->ctx;
     if (p->maxiter < 0 || p->maxiter > GG_MAX_ITERS) return set_error(ctx, GG_ERR_ARG, "maxiter out of range");
-    const int dt = p->contrib_dtype;
-    if (dt != GG_F32 && dt != GG_BF16 && dt != GG_F16 && dt != GG_FP8E4M3 && dt != GG_CFP_6_10 &&
-        dt != GG_BF16_TRUNC && dt != GG_F64)
-        return set_error(ctx, GG_ERR_UNSUPPORTED, "contribution dtype");
+    const bool staged = p->nstages > 1;
+    const int dt = staged ? p->stage_dtype[0] : p->contrib_dtype;
+    auto known = [](int t) {
+        return t == GG_F32 || t == GG_BF16 || t == GG_F16 || t == GG_FP8E4M3 || t == GG_CFP_6_10 || t == GG_BF16_TRUNC;
+    };
+    if (p->nstages < 0 || p->nstages > 4) return set_error(ctx, GG_ERR_ARG, "nstages must be 0..4");
+    if (staged)
+        for (int k = 0; k < p->nstages; ++k)
+            if (!known(p->stage_dtype[k])) return set_error(ctx, GG_ERR_UNSUPPORTED, "stage contribution dtype");
+    if (!staged && !known(dt) && dt != GG_F64) return set_error(ctx, GG_ERR_UNSUPPORTED, "contribution dtype");
     const gg_dtype xt = dt == GG_F64 ? GG_F64 : GG_F32;
     if (x && (x->g != g || x->t != xt))
         return set_error(ctx, GG_ERR_ARG, "x must be an F32 property of g (F64 for the FP64 variant)");
@@ -564,11 +702,18 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
     init.scale = 1.0f;
     init.scale_inv = 1.0f;
     init.done = p->maxiter == 0;
+    init.nstages = staged ? p->nstages : 1;
+    for (int k = 0; k < 4; ++k) {
+        init.stage_dt[k] = staged && k < p->nstages ? p->stage_dtype[k] : dt;
+        init.stage_tol[k] = staged && k + 1 < p->nstages ? p->stage_tol[k] : p->tol;
+    }
     uint64_t k0 = ctx->launches;
     cudaEventRecord(ctx->ev0, ctx->stream);
     cudaError_t e = cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) {
-        switch (dt) {
+        if (staged) {
+            s = pr_run_staged(g, p, (float *)xp->d, y, contrib, st, partial);
+        } else switch (dt) {
         case GG_F64: s = pr_run<GG_F64>(g, p, (double *)xp->d, (double *)base, contrib, st, partial); break;
         case GG_F32: s = pr_run<GG_F32>(g, p, (float *)xp->d, y, contrib, st, partial); break;
         case GG_BF16: s = pr_run<GG_BF16>(g, p, (float *)xp->d, y, contrib, st, partial); break;

@@ -79,7 +79,9 @@ class RunOpts(C.Structure):
 
 class PrParams(C.Structure):
     _fields_ = [("maxiter", C.c_int), ("tol", C.c_double), ("damping", C.c_float),
-                ("contrib_dtype", C.c_int), ("accum_f64", C.c_int), ("renorm_f32", C.c_int)]
+                ("contrib_dtype", C.c_int), ("accum_f64", C.c_int), ("renorm_f32", C.c_int),
+                ("nstages", C.c_int), ("stage_dtype", C.c_int * 4), ("stage_accum_f64", C.c_int * 4),
+                ("stage_tol", C.c_double * 4)]
 
 
 EXPORTS = [
@@ -257,6 +259,32 @@ class Context:
     def grid(self, rows: int, cols: int, seed: int, del_bp=0):
         return self.generate(GEN_GRID, seed, rows=rows, cols=cols, bp=del_bp)
 
+    def from_edges(self, n: int, src, dst, symmetrise: bool = True, device: bool = False) -> "Graph":
+        """Edge list -> graph, duplicates and self-loops dropped on the device.
+        device=True: src / dst are device pointers (ints) to nedges uint32 each,
+        with nedges passed as len(src) unless src is an int (then pass (ptr, count))."""
+        L = _ingest_lib()
+        h = C.c_void_p()
+        flags = (INGEST_SYMMETRISE if symmetrise else 0) | (INGEST_DEVICE if device else 0)
+        if device:
+            (ps, ne), (pd, _) = src, dst
+            self.check(L.gg_graph_from_edges(self.h, n, ne, C.c_void_p(ps), C.c_void_p(pd), flags, C.byref(h)),
+                       "gg_graph_from_edges")
+        else:
+            s_ = np.ascontiguousarray(src, dtype=np.uint32)
+            d_ = np.ascontiguousarray(dst, dtype=np.uint32)
+            assert len(s_) == len(d_)
+            self.check(L.gg_graph_from_edges(self.h, n, len(s_), _p(s_) if len(s_) else None,
+                                             _p(d_) if len(d_) else None, flags, C.byref(h)), "gg_graph_from_edges")
+        return Graph(self, h)
+
+    def read_bin_clean(self, path: str, symmetrise: bool = True) -> "Graph":
+        h = C.c_void_p()
+        self.check(_ingest_lib().gg_graph_read_bin_clean(self.h, path.encode(),
+                                                         INGEST_SYMMETRISE if symmetrise else 0, C.byref(h)),
+                   "gg_graph_read_bin_clean")
+        return Graph(self, h)
+
 
 class Graph:
     def __init__(self, ctx: Context, h: C.c_void_p):
@@ -340,9 +368,16 @@ class Graph:
         return out
 
     def pagerank(self, maxiter=20, tol=1e-7, contrib=F32, accum_f64=True, renorm_f32=True,
-                 damping=0.85, x: "Prop" = None, host: bool = True, stats: RunStats = None):
+                 damping=0.85, x: "Prop" = None, host: bool = True, stats: RunStats = None, stages=None):
+        """stages: [(dtype, accum_f64, tol), ...] for a staged run (the last tol is ignored;
+        `tol` ends the last stage), e.g. PR_vary VARIANT 4620:
+        [(CFP_6_10, False, 1e-3), (F32, True, 0)]."""
         p = PrParams(maxiter=maxiter, tol=tol, damping=damping, contrib_dtype=contrib,
                      accum_f64=int(accum_f64), renorm_f32=int(renorm_f32))
+        if stages:
+            p.nstages = len(stages)
+            for k, (dt, acc, st_tol) in enumerate(stages):
+                p.stage_dtype[k], p.stage_accum_f64[k], p.stage_tol[k] = dt, int(acc), st_tol
         if contrib == F64 and host and x is None:
             # the FP64 variant: return the double ranks
             xp = self.prop(F64)
@@ -685,3 +720,21 @@ def autotune(g: Graph, analytics: int = TUNE_BFS | TUNE_CC, roots=(), passes: in
     best = dict(kv.split("=") for kv in res.best.decode().split(",") if kv)
     return dict(initial_ms=res.initial_ms, best_ms=res.best_ms, evaluations=res.evaluations,
                 knobs={k: int(v) for k, v in best.items()})
+
+
+# ---------------------------------------------------------------------------
+# Ingest with cleaning (gg_graph_from_edges / gg_graph_read_bin_clean)
+# ---------------------------------------------------------------------------
+INGEST_SYMMETRISE, INGEST_DEVICE = 1, 2
+
+
+def _ingest_lib():
+    L = lib()
+    if not getattr(L, "_ingest_bound", False):
+        L.gg_graph_from_edges.argtypes = [C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p, C.c_int,
+                                          C.POINTER(C.c_void_p)]
+        L.gg_graph_read_bin_clean.argtypes = [C.c_void_p, C.c_char_p, C.c_int, C.POINTER(C.c_void_p)]
+        L.gg_graph_from_edges.restype = C.c_int
+        L.gg_graph_read_bin_clean.restype = C.c_int
+        L._ingest_bound = True
+    return L

@@ -97,6 +97,19 @@ GG_API gg_status gg_graph_upload(gg_ctx *ctx, uint32_t n, uint64_t m, const uint
 /* Graptor version-2/3 binary file (GraphCSx::readFromBinaryFile,
  * graph/GraphCSx.h:2137-2262; writer GraphCSx.h:2009-2026). */
 GG_API gg_status gg_graph_read_bin(gg_ctx *ctx, const char *path, int symmetric, gg_graph **out);
+
+/* Ingest with cleaning on the device (the preprocessing the reference does
+ * with its tools before loading: tools/CvtToUndir.C, RmDupEdges.C,
+ * RmSelfEdges.C): duplicate edges and self-loops are dropped; with
+ * GG_INGEST_SYMMETRISE every edge's reverse is added first and the graph is
+ * symmetric.  gg_graph_from_edges takes an edge list (host arrays, or device
+ * pointers with GG_INGEST_DEVICE); gg_graph_read_bin_clean a Graptor v2/v3
+ * .bin file that may hold duplicates, self-loops or one direction only. */
+#define GG_INGEST_SYMMETRISE 1
+#define GG_INGEST_DEVICE 2
+GG_API gg_status gg_graph_from_edges(gg_ctx *ctx, uint32_t n, uint64_t nedges, const uint32_t *src,
+                                     const uint32_t *dst, int flags, gg_graph **out);
+GG_API gg_status gg_graph_read_bin_clean(gg_ctx *ctx, const char *path, int flags, gg_graph **out);
 GG_API gg_status gg_graph_write_bin(gg_graph *g, const char *path);
 
 /* Seeded synthetic graphs built on the device (the workloads' inputs). */
@@ -219,7 +232,9 @@ typedef struct gg_emap_desc {
     int fusion;             /* api::fusion present: multi-hop push allowed */
     int src_level_sync;     /* MIN_PLUS1 with GT_CONST filter k: every active source
                                holds a[s] == k-1 (level-synchronous BFS), so the
-                               relax offers k without loading a[s] */
+                               relax offers k without loading a[s]; a push then
+                               leaves prev of the vertices it records as it was
+                               (only unvisited vertices' prev is ever compared) */
 } gg_emap_desc;
 
 typedef struct gg_emap_stats {
@@ -335,6 +350,16 @@ typedef struct gg_pr_params {
                            F64 property, damping taken as the shortest decimal of the float) */
     int accum_f64;      /* accumulate gathers in double (PRv) rather than float */
     int renorm_f32;     /* PRv renormalises by float(1)/float(s); PR_vary by double */
+    /* Staged precision (PR_vary.C:652-757): nstages 2..4 runs stage k with
+     * stage_dtype[k] contributions (not F64) and stage_accum_f64[k] sums
+     * until the L1 residual <= stage_tol[k], the last stage until tol; the
+     * switch is taken on the device and the next stage's contributions are
+     * re-encoded from the ranks.  VARIANT 4620 = {CFP_6_10, float sums, 1e-3},
+     * {F32, double sums}.  nstages 0 or 1: contrib_dtype / accum_f64 only. */
+    int nstages;
+    int stage_dtype[4];
+    int stage_accum_f64[4];
+    double stage_tol[4];
 } gg_pr_params;
 /* PageRank power iteration (PRv / PR_vary run_prec); x receives the ranks. */
 GG_API gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x, float *host_x,

@@ -579,18 +579,20 @@ static float q_e4m3(float f) { return q_grid(f, 3, -6, 448.0f); }
  * each iteration so that max|contrib|*scale <= 448, and the gather
  * multiplies by 1/scale; ORC_F16 is scaled the same way (to 65504).
  * x_out gets the FP32 rank vector. */
-ORC_API int orc_pr_vary(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj,
-                        const uint32_t *outdeg, int fmt, int accum_f64, int maxiter,
-                        double tol, float *x_out, double *deltas) {
+/* One run_prec stage from the current x: iterations continue the shared
+ * count *iter while *iter < maxiter and the residual exceeds tol
+ * (PR_vary.C:247-447; a staged VARIANT such as 4620 calls run_prec once per
+ * stage with the previous stage's ranks, PR_vary.C:652-757). */
+ORC_API int orc_pr_vary_staged(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj,
+                               const uint32_t *outdeg, int nstages, const int *fmts, const int *accs,
+                               const double *tols, int maxiter, double tol, float *x_out, double *deltas);
+
+static int pr_vary_stage(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj, const uint32_t *outdeg,
+                         int fmt, int accum_f64, int *iter, int maxiter, double tol, float *x, double *y,
+                         float *cq, double *deltas) {
     const float damp = 0.85f;
-    float *x = x_out;
-    double *y = (double *)calloc(n ? n : 1, sizeof(double));
-    float *cq = (float *)malloc((size_t)(n ? n : 1) * sizeof(float));
-    if (!y || !cq) { free(y); free(cq); return -1; }
-    for (uint32_t v = 0; v < n; ++v) x[v] = (float)(1.0 / (double)n);
-    int iter = 0;
     double sdelta = 2;
-    while (iter < maxiter && sdelta > tol) {
+    while (*iter < maxiter && sdelta > tol) {
         /* contribution encode */
         float cmax = 0.0f;
         for (uint32_t v = 0; v < n; ++v) {
@@ -640,9 +642,34 @@ ORC_API int orc_pr_vary(uint32_t n, const uint64_t *in_off, const uint32_t *in_a
             sdelta += (double)fabsf(x[v] - yv);
             x[v] = yv;
         }
-        if (deltas) deltas[iter] = sdelta;
-        ++iter;
+        if (deltas) deltas[*iter] = sdelta;
+        ++*iter;
     }
+    return 0;
+}
+
+ORC_API int orc_pr_vary(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj,
+                        const uint32_t *outdeg, int fmt, int accum_f64, int maxiter,
+                        double tol, float *x_out, double *deltas) {
+    int f[1] = {fmt}, a[1] = {accum_f64};
+    double t[1] = {tol};
+    return orc_pr_vary_staged(n, in_off, in_adj, outdeg, 1, f, a, t, maxiter, tol, x_out, deltas);
+}
+
+/* Staged PR_vary run: stage k with format fmts[k] and accumulation accs[k]
+ * until the residual <= tols[k]; the last stage until tol. */
+ORC_API int orc_pr_vary_staged(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj,
+                               const uint32_t *outdeg, int nstages, const int *fmts, const int *accs,
+                               const double *tols, int maxiter, double tol, float *x_out, double *deltas) {
+    float *x = x_out;
+    double *y = (double *)calloc(n ? n : 1, sizeof(double));
+    float *cq = (float *)malloc((size_t)(n ? n : 1) * sizeof(float));
+    if (!y || !cq) { free(y); free(cq); return -1; }
+    for (uint32_t v = 0; v < n; ++v) x[v] = (float)(1.0 / (double)n);
+    int iter = 0;
+    for (int k = 0; k < nstages; ++k)
+        pr_vary_stage(n, in_off, in_adj, outdeg, fmts[k], accs[k], &iter, maxiter,
+                      k + 1 < nstages ? tols[k] : tol, x, y, cq, deltas);
     free(y);
     free(cq);
     return iter;

@@ -55,6 +55,8 @@ def lib() -> C.CDLL:
         L.orc_pr_f64.argtypes = L.orc_pr_f32.argtypes
         L.orc_pr_vary.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                   C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_pr_vary_staged.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p]
         L.orc_cfp_from_float.argtypes = [C.c_float, C.c_int, C.c_int, C.c_int]
         L.orc_cfp_from_float.restype = C.c_uint32
         L.orc_cfp_to_float.argtypes = [C.c_uint32, C.c_int, C.c_int, C.c_int]
@@ -193,6 +195,21 @@ def pagerank_vary(g: Graph, fmt: int, accum_f64: bool, maxiter: int = 100, tol: 
     deltas = np.zeros(max(maxiter, 1), dtype=np.float64)
     it = lib().orc_pr_vary(g.n, _p(csc.off), _p(csc.adj), _p(outdeg), fmt, int(accum_f64),
                            maxiter, tol, _p(x), _p(deltas))
+    return x, it, deltas[:it]
+
+
+def pagerank_vary_staged(g: Graph, stages, maxiter: int = 100, tol: float = 1e-7, csc: Graph | None = None):
+    """PR_vary staged run: stages = [(fmt, accum_f64, tol_k), ...]; the last
+    stage runs until `tol`.  Returns (x, iterations, deltas)."""
+    csc = csc if csc is not None else g.transpose()
+    outdeg = g.outdeg()
+    x = np.empty(g.n, dtype=np.float32)
+    deltas = np.zeros(max(maxiter, 1), dtype=np.float64)
+    f = np.array([s[0] for s in stages], dtype=np.int32)
+    a = np.array([int(s[1]) for s in stages], dtype=np.int32)
+    t = np.array([s[2] for s in stages], dtype=np.float64)
+    it = lib().orc_pr_vary_staged(g.n, _p(csc.off), _p(csc.adj), _p(outdeg), len(stages), _p(f), _p(a), _p(t),
+                                  maxiter, tol, _p(x), _p(deltas))
     return x, it, deltas[:it]
 
 

@@ -318,3 +318,29 @@ def test_pagerank_f64_variant_matches_f64_oracle(ctx, kind):
     assert np.abs(x - ref).sum() < 1e-12
     assert np.allclose([st.delta[i] for i in range(it)], deltas, rtol=1e-6, atol=1e-15)
     G.close()
+
+
+# library dtype -> oracle storage format
+ORC_FMT = {gg.F32: O.F32, gg.BF16: O.BF16, gg.F16: O.F16, gg.FP8E4M3: O.FP8, gg.CFP_6_10: O.CFP_6_10,
+           gg.BF16_TRUNC: O.BF16_TRUNC}
+
+
+@pytest.mark.parametrize("stages", [
+    [(gg.CFP_6_10, False, 1e-3), (gg.F32, True, 0.0)],                                 # PR_vary 4620
+    [(gg.BF16_TRUNC, False, 1e-2), (gg.F32, True, 0.0)],                               # PR_vary 9920
+    [(gg.BF16_TRUNC, False, 1e-2), (gg.CFP_6_10, False, 1e-3), (gg.F32, True, 0.0)],  # PR_vary 994620
+    [(gg.F16, False, 1e-3), (gg.F32, True, 0.0)],                                      # scaled, then FP32
+])
+def test_pagerank_staged_matches_restatement(ctx, stages):
+    """Staged precision (the switch taken on the device) against the restated
+    PR_vary staged loop: same switch point within one iteration, same ranks
+    to summation order."""
+    og = O.rmat(13, 16 << 13, seed=7)
+    g = upload(ctx, og)
+    st = gg.RunStats()
+    x = g.pagerank(maxiter=100, tol=1e-7, renorm_f32=False, stages=stages, stats=st)
+    xo, it, d = O.pagerank_vary_staged(og, [(ORC_FMT[f], a, t) for f, a, t in stages], maxiter=100, tol=1e-7)
+    assert abs(st.iterations - it) <= 1, (st.iterations, it)
+    assert np.abs(x.astype(np.float64) - xo).sum() <= 1e-5
+    x64, _, _ = O.pagerank(og, maxiter=100, tol=1e-10, f64=True)
+    assert np.abs(x.astype(np.float64) - x64).sum() <= 1e-5  # the FP32 stage restores full accuracy

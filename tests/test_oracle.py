@@ -154,3 +154,20 @@ def test_oracle_matches_reference_golden(path):
 
 def test_golden_present():
     assert len(golden_files()) >= 4
+
+
+def test_pr_vary_staged_single_stage_equals_plain():
+    g = O.rmat(10, 1 << 14, 4)
+    x1, it1, d1 = O.pagerank_vary(g, O.CFP_6_10, False, maxiter=30)
+    x2, it2, d2 = O.pagerank_vary_staged(g, [(O.CFP_6_10, False, 0.0)], maxiter=30)
+    assert it1 == it2 and np.array_equal(x1, x2) and np.array_equal(d1, d2)
+
+
+def test_pr_vary_4620_switches_and_converges():
+    # PR_vary VARIANT 4620: customfp<6,10> until 1e-3, then FP32 / double sums until 1e-7
+    g = O.rmat(11, 1 << 15, 6)
+    x, it, d = O.pagerank_vary_staged(g, [(O.CFP_6_10, False, 1e-3), (O.F32, True, 0.0)], maxiter=100)
+    k = int(np.argmax(d <= 1e-3))
+    assert 0 < k < it and d[-1] <= 1e-7
+    x64, _, _ = O.pagerank(g, maxiter=100, tol=1e-10, f64=True)
+    assert np.abs(x - x64).sum() < 1e-5

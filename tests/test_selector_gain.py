@@ -44,29 +44,33 @@ def test_records_are_usable():
     assert np.isfinite(X).all() and np.isfinite(Y).all()
 
 
+def regret(t, choice):
+    """Mean over records of the chosen variant's time over the best one's:
+    every sampled decision counts once, whatever its absolute duration (a CC
+    record's time runs to the end of the run and dwarfs a BFS iteration)."""
+    r = np.arange(len(t))
+    return float(np.mean(t[r, choice] / t.min(1)))
+
+
 def test_trained_selector_beats_threshold_on_heldout_records():
     z = np.load(os.path.join(DATA, "selector.npz"))
     X, Y = heldout()
     learned, thr = choices(z["params"].astype(np.float64), X)
     t = 2.0 ** Y.astype(np.float64)  # microseconds
     r = np.arange(len(X))
-    t_learned, t_thr, t_best = t[r, learned].sum(), t[r, thr].sum(), t.min(1).sum()
-    # the gain, stated: total held-out iteration time of each policy
-    print(f"held-out records {len(X)}: threshold {t_thr:.0f} us, learned {t_learned:.0f} us, "
-          f"oracle-best {t_best:.0f} us")
-    assert t_learned < t_thr
-    assert t_learned <= 1.25 * t_best
+    # the gain, stated: mean time over the oracle-best variant, and totals
+    print(f"held-out records {len(X)}: threshold {regret(t, thr):.3f} x best, learned {regret(t, learned):.3f} x best; "
+          f"totals threshold {t[r, thr].sum():.0f} us, learned {t[r, learned].sum():.0f} us, "
+          f"best {t.min(1).sum():.0f} us")
+    assert regret(t, learned) < regret(t, thr)
+    assert regret(t, learned) <= 1.10  # within 10% of the oracle-best choice
 
 
 def test_untrained_network_does_not_beat_threshold_by_luck():
     # a control: random networks under the same margin rule are no better
     X, Y = heldout()
     t = 2.0 ** Y.astype(np.float64)
-    r = np.arange(len(X))
     z = np.load(os.path.join(DATA, "selector.npz"))
     trained, thr = choices(z["params"].astype(np.float64), X)
-    gains = []
-    for seed in range(5):
-        rnd, _ = choices(M.init_params(seed), X)
-        gains.append(t[r, thr].sum() / t[r, rnd].sum())
-    assert t[r, thr].sum() / t[r, trained].sum() > max(gains)
+    rnd = [regret(t, choices(M.init_params(seed), X)[0]) for seed in range(5)]
+    assert regret(t, trained) < min(rnd)
