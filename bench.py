@@ -59,19 +59,54 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 5 ms from a thread (read-only queries), or
+    nvidia-smi at 200 ms when NVML is unavailable."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.rows = []
         self.proc = None
         self.thread = None
+        self.nvml = None
+        self.stop_flag = threading.Event()
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            p = torch.cuda.get_device_properties(gpu_index)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            try:
+                self.handle = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+            except Exception:
+                self.handle = pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+            self.nvml = pynvml
+        except Exception:
+            self.nvml = None
+
+    def _poll(self):
+        nv = self.nvml
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                self.rows.append((float(sm), int(rs)))
+            except Exception:
+                pass
+            self.stop_flag.wait(0.005)
 
     def start(self):
+        if self.nvml is not None:
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
@@ -88,6 +123,7 @@ class ClockSampler:
             self.rows.append([x.strip() for x in line.split(",")])
 
     def stop(self):
+        self.stop_flag.set()
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -97,18 +133,28 @@ class ClockSampler:
         if self.thread is not None:
             self.thread.join(timeout=5)
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
-            except (ValueError, IndexError):
-                continue
-            for i, nm in enumerate(names):
-                if len(r) > 5 + i and r[5 + i].lower() == "active":
-                    reasons.add(nm)
+        if self.nvml is not None:
+            mx = self.max_mhz
+            for clk, rs in self.rows:
+                sm.append(clk)
+                for nm, bit in self.REASONS.items():
+                    if rs & bit:
+                        reasons.add(nm)
+            src = "nvml 5 ms"
+        else:
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for r in self.rows:
+                try:
+                    sm.append(float(r[1]))
+                    mx = float(r[2])
+                except (ValueError, IndexError):
+                    continue
+                for i, nm in enumerate(names):
+                    if len(r) > 5 + i and r[5 + i].lower() == "active":
+                        reasons.add(nm)
+            src = "nvidia-smi 200 ms"
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": src}
 
 
 def dist_setup(args):

@@ -522,6 +522,7 @@ static void graph_free(gg_graph *g) {
     cudaFree(g->nonisolated_n);
     cudaFree(g->pstate);
     cudaFree(g->wq);
+    graph_bfs_free(g);
     cudaFree(g->heavy.light_prefix);
     cudaFree(g->heavy.pull_prefix);
     cudaFree(g->cand.list[0]);
@@ -781,6 +782,7 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "fusion" && (v == 0 || v == 4)) t.fusion = (int)v;
     else if (k == "fusion_queue" && (v == 0 || v >= 32)) t.fusion_queue = (uint32_t)v;
     else if (k == "cc_hook" && v <= 1) t.cc_hook = (int)v;
+    else if (k == "graph" && v <= 1) t.graph = (int)v;
     else if (k == "barrier_timeout_ns" && v >= 1) t.barrier_timeout_ns = (unsigned long long)v;
     else return GG_ERR_ARG;
     if (t.bin_small_max > t.bin_medium_max) {
@@ -807,6 +809,7 @@ gg_status gg_tuning_get(const char *name, int64_t *v) {
     else if (k == "fusion") *v = t.fusion;
     else if (k == "fusion_queue") *v = t.fusion_queue;
     else if (k == "cc_hook") *v = t.cc_hook;
+    else if (k == "graph") *v = t.graph;
     else if (k == "barrier_timeout_ns") *v = (int64_t)t.barrier_timeout_ns;
     else return GG_ERR_ARG;
     return GG_OK;

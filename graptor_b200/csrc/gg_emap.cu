@@ -31,6 +31,8 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cstddef>
+#include <cstdlib>
 #include <climits>
 #include <cstring>
 #include <type_traits>
@@ -64,6 +66,7 @@ struct EmapArgs {
     const uint64_t *large_first;  // [c2 + 1] chunk prefix of the large bin (push)
     uint32_t large_ch;            // edges per large-bin chunk
     int merge_med;                // push: medium bin chunked with the large one (small frontiers)
+    int large_as_med;             // push: large bin walked a warp per row with the medium one
     // pull candidate lists (drivers only): the destinations that can still
     // pass the (monotone) dst filter.  cand == nullptr: scan all vertices.
     const uint32_t *cand;
@@ -186,7 +189,7 @@ __device__ __forceinline__ void flush_counts(const EmapArgs &A, unsigned long lo
 // Loads are issued ahead of use: d's value and both offsets together, then
 // up to 4 neighbour ids, then their frontier bits and source values.
 template <int R, bool SRCF, bool CAND, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
+__device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
     using V = typename Op<R>::V;
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nitems = CAND ? *A.cand_n : (uint64_t)A.n;
@@ -321,6 +324,11 @@ __global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
     if (A.out_cnt) flush_counts<BLOCK>(A, nv, ne, sc);
 }
 
+template <int R, bool SRCF, bool CAND, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
+    pull_body<R, SRCF, CAND, BLOCK>(A, op);
+}
+
 // ---------------------------------------------------------------------------
 // Degree-binned sparse push
 // ---------------------------------------------------------------------------
@@ -384,8 +392,8 @@ __device__ __forceinline__ void push_edges(const EmapArgs &A, const Op<R> &op, t
 }
 
 template <int R, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uint32_t nb_large,
-                                                       uint32_t nb_med) {
+__device__ __forceinline__ void push_binned_body(const EmapArgs &A, const Op<R> &op, uint32_t nb_large,
+                                                 uint32_t nb_med) {
     using V = typename Op<R>::V;
     const uint32_t lane = threadIdx.x & 31u;
     unsigned long long sc = 0;
@@ -437,8 +445,9 @@ __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uin
         const uint32_t wpb = BLOCK / 32;
         const uint32_t nwm = nb_med * wpb;
         const uint32_t wid = (blockIdx.x - nb_large) * wpb + (threadIdx.x >> 5);
-        for (uint32_t i = wid; i < A.c1; i += nwm) {
-            const uint32_t s = A.in_b1[i];
+        const uint32_t cmed = A.c1 + (A.large_as_med ? A.c2 : 0u);
+        for (uint32_t i = wid; i < cmed; i += nwm) {
+            const uint32_t s = i < A.c1 ? A.in_b1[i] : A.in_b2[i - A.c1];
             const V sv = op.src_val(s);
             const uint64_t beg = A.off[s], end = A.off[s + 1];
             if (lane == 0) sc += end - beg;
@@ -477,6 +486,11 @@ __global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uin
     }
     app.flush();
     flush_counts<BLOCK>(A, app.nv, app.ne, sc);
+}
+
+template <int R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_push_binned(EmapArgs A, Op<R> op, uint32_t nb_large, uint32_t nb_med) {
+    push_binned_body<R, BLOCK>(A, op, nb_large, nb_med);
 }
 
 // chunks of each large-bin vertex's row (first[c2] = 0 before the scan)
@@ -1098,6 +1112,468 @@ static gg_status frontier_loop(gg_graph *g, gg_emap_desc &desc, gg_frontier *F, 
     return GG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Graph-driven BFS levels: the host loop's kernels, decided on the device
+// ---------------------------------------------------------------------------
+// The host-driven loop waits for every iteration's frontier counts before it
+// picks push or pull and launches the next kernels; on R-MAT scale 24 those
+// round trips are about a third of a BFS.  Here one CUDA graph holds a whole
+// run: a WHILE conditional node repeats
+//     decide -> IF(push){list, push} , IF(pull){pull} -> post
+// The one-warp decide kernel reads the frontier counts on the device, applies
+// the threshold (api.h:130-222) and writes the step's arguments to device
+// memory; the step kernels run the same bodies as the host-launched kernels
+// on fixed grids and read their arguments there; post recycles the consumed
+// frontier and sets the loop condition.  Every kernel keeps the normal L1
+// path (no grid-wide waits), and the host waits once, at the end.
+struct GFront {
+    uint32_t *bins[NBINS];
+    uint32_t *bitmap;
+    unsigned long long *cnt;
+};
+
+struct GCtl {
+    EmapArgs A;  // this step's traversal arguments
+    Op<GG_RELAX_MIN_PLUS1_I32> op;
+    int variant;  // GG_VAR_PUSH_SPARSE / GG_VAR_PULL_DENSE, -1: finished
+    int need_list, need_bitmap;
+    int cur, iter, max_iters, iterations;
+    int has_list[2], has_bitmap[2];
+    GFront f[2];
+    // per-run configuration
+    int32_t *level, *prev;
+    uint32_t root, n;
+    uint64_t m;
+    int threshold, threshold_k;
+    uint32_t smax, mmax, large_ch, sm_count;
+    int pull_k, push_k;
+    const uint64_t *off, *in_off, *word_prefix;
+    const uint32_t *adj, *in_adj;
+    const uint32_t *nonisolated;
+    const unsigned long long *nonisolated_n;
+    uint32_t *cand[2];
+    unsigned long long *cand_n;  // [2]
+    int cand_cur, cand_valid;
+    // records
+    unsigned long long reached_v, reached_e;
+    int variants[GG_MAX_ITERS];
+    unsigned long long nactv[GG_MAX_ITERS], nacte[GG_MAX_ITERS], scanned[GG_MAX_ITERS];
+    unsigned long long t_ns[GG_MAX_ITERS + 1];
+    cudaGraphConditionalHandle h_while, h_push, h_pull;
+};
+
+__device__ __forceinline__ unsigned long long g_now() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool d_threshold_sparse(int kind, int k, uint64_t nactv, uint64_t nacte, uint64_t m) {
+    switch (kind) {
+    case GG_THRESH_ALWAYS_SPARSE: return true;
+    case GG_THRESH_ALWAYS_DENSE: return false;
+    case GG_THRESH_FRAC: return (float)(nactv + nacte) <= (float)m / (float)(100.0 / (float)k);
+    default: return (nactv + nacte) <= (m / 20);
+    }
+}
+
+__global__ void k_g_init(GCtl *c) {
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
+    const int32_t inf = (int32_t)c->n + 1;
+    for (uint64_t v = tid; v < c->n; v += nth) {
+        const int32_t x = v == c->root ? 0 : inf;
+        c->level[v] = x;
+        c->prev[v] = x;
+    }
+    const uint64_t words = ((uint64_t)c->n + 31) / 32;
+    for (uint64_t w = tid; w < words; w += nth) {
+        c->f[0].bitmap[w] = w == (c->root >> 5) ? 1u << (c->root & 31) : 0u;
+        c->f[1].bitmap[w] = 0u;
+    }
+    if (tid == 0) {
+        for (int i = 0; i < FC_WORDS; ++i) {
+            c->f[0].cnt[i] = 0;
+            c->f[1].cnt[i] = 0;
+        }
+        const uint64_t deg = c->off[c->root + 1] - c->off[c->root];
+        const int b = deg <= c->smax ? 0 : (deg <= c->mmax ? 1 : 2);
+        c->f[0].bins[b][0] = c->root;
+        c->f[0].cnt[FC_BIN0 + b] = 1;
+        c->f[0].cnt[FC_NACTV] = 1;
+        c->f[0].cnt[FC_NACTE] = deg;
+        c->has_list[0] = 1;
+        c->has_list[1] = 0;
+        c->has_bitmap[0] = 1;
+        c->has_bitmap[1] = 0;
+        c->cur = 0;
+        c->iter = 0;
+        c->iterations = 0;
+        c->cand_valid = 0;
+        c->cand_cur = 0;
+        c->reached_v = 0;
+        c->reached_e = 0;
+        c->variant = -1;
+        c->t_ns[0] = g_now();
+    }
+}
+
+__global__ void k_g_decide(GCtl *c) {
+    if (threadIdx.x != 0) return;
+    const GFront F = c->f[c->cur], O = c->f[c->cur ^ 1];
+    const unsigned long long nactv = F.cnt[FC_NACTV], nacte = F.cnt[FC_NACTE];
+    const int iter = c->iter;
+    if (nactv == 0 || iter >= c->max_iters) {
+        c->variant = -1;
+        c->iterations = iter;
+        cudaGraphSetConditional(c->h_push, 0);
+        cudaGraphSetConditional(c->h_pull, 0);
+        return;
+    }
+    const bool push = d_threshold_sparse(c->threshold, c->threshold_k, nactv, nacte, c->m);
+    if (iter < GG_MAX_ITERS) {
+        c->variants[iter] = push ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+        c->nactv[iter] = nactv;
+        c->nacte[iter] = nacte;
+    }
+    c->reached_v += nactv;
+    c->reached_e += nacte;
+    EmapArgs A;
+    memset(&A, 0, sizeof(A));
+    A.off = c->off;
+    A.adj = c->adj;
+    A.in_off = c->in_off;
+    A.in_adj = c->in_adj;
+    A.n = c->n;
+    A.record = GG_RECORD_NE_PREV;
+    A.smax = c->smax;
+    A.mmax = c->mmax;
+    A.K = push ? c->push_k : c->pull_k;
+    A.word_prefix = c->word_prefix;
+    A.out_b0 = O.bins[0];
+    A.out_b1 = O.bins[1];
+    A.out_b2 = O.bins[2];
+    A.out_cnt = O.cnt;
+    A.in_bits = F.bitmap;
+    A.in_b0 = F.bins[0];
+    A.in_b1 = F.bins[1];
+    A.in_b2 = F.bins[2];
+    A.large_ch = c->large_ch;
+    if (!push) {
+        const int cc = c->cand_cur;
+        A.cand = c->cand_valid ? c->cand[cc] : c->nonisolated;
+        A.cand_n = c->cand_valid ? c->cand_n + cc : c->nonisolated_n;
+        A.cand_out = c->cand[cc ^ 1];
+        A.cand_out_n = c->cand_n + (cc ^ 1);
+        c->cand_n[cc ^ 1] = 0;
+        A.out_bits = O.bitmap;  // cleared by the post kernel of the step that consumed it
+    }
+    c->A = A;
+    Op<GG_RELAX_MIN_PLUS1_I32> op;
+    op.a = c->level;
+    op.prev = c->prev;
+    op.filter = GG_FILTER_GT_CONST;
+    op.fk = iter + 1;
+    op.level_sync = 1;
+    c->op = op;
+    c->variant = push ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+    c->need_list = push && !c->has_list[c->cur];
+    c->need_bitmap = !push && !c->has_bitmap[c->cur];
+    cudaGraphSetConditional(c->h_push, push ? 1u : 0u);
+    cudaGraphSetConditional(c->h_pull, push ? 0u : 1u);
+}
+
+// a frontier held as a bitmap only (after a pull) gets its binned list
+__global__ void __launch_bounds__(256) k_g_tolist(GCtl *c) {
+    if (!c->need_list) return;
+    const GFront F = c->f[c->cur];
+    __shared__ uint32_t sb[3][8][256];
+    const uint32_t wib = threadIdx.x >> 5;
+    dev::WarpAppender<256> ap0{sb[0][wib], 0, F.bins[0], F.cnt + FC_BIN0};
+    dev::WarpAppender<256> ap1{sb[1][wib], 0, F.bins[1], F.cnt + FC_BIN1};
+    dev::WarpAppender<256> ap2{sb[2][wib], 0, F.bins[2], F.cnt + FC_BIN2};
+    const uint32_t n = c->n, nwords = (n + 31) / 32;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    for (uint32_t w = warp; w < nwords; w += nw) {
+        const uint32_t word = F.bitmap[w];
+        if (word == 0) continue;  // warp-uniform
+        const uint32_t v = w * 32 + lane;
+        const bool act = v < n && ((word >> lane) & 1u);
+        const uint64_t deg = act ? c->off[v + 1] - c->off[v] : 0;
+        const uint32_t bin = deg <= c->smax ? 0 : (deg <= c->mmax ? 1 : 2);
+        ap0.push(act && bin == 0, v);
+        ap1.push(act && bin == 1, v);
+        ap2.push(act && bin == 2, v);
+    }
+    ap0.flush();
+    ap1.flush();
+    ap2.flush();
+}
+
+// the push step: the partition of the fixed grid over the three bins is
+// derived by every CTA from the same device counts
+__global__ void __launch_bounds__(kBlock) k_g_push(GCtl *c) {
+    if (c->variant != GG_VAR_PUSH_SPARSE) return;
+    EmapArgs A = c->A;
+    const GFront F = c->f[c->cur];
+    A.c0 = (uint32_t)F.cnt[FC_BIN0];
+    A.c1 = (uint32_t)F.cnt[FC_BIN1];
+    A.c2 = (uint32_t)F.cnt[FC_BIN2];
+    A.merge_med = A.c1 && A.c1 + A.c2 <= kLargeLocal && A.c1 < c->sm_count;
+    A.large_as_med = !A.merge_med && A.c2 > kLargeLocal;
+    const uint32_t cap = gridDim.x;
+    const uint64_t nacte = F.cnt[FC_NACTE];
+    uint32_t nl = 0;
+    if ((A.c2 && !A.large_as_med) || A.merge_med)
+        nl = (uint32_t)min((uint64_t)cap, nacte / A.large_ch + A.c2 + (A.merge_med ? A.c1 : 0u));
+    const uint32_t cmed = A.merge_med ? 0u : A.c1 + (A.large_as_med ? A.c2 : 0u);
+    uint32_t nm = (uint32_t)min((uint64_t)cap, ((uint64_t)cmed + kBlock / 32 - 1) / (kBlock / 32));
+    const uint32_t ns = (uint32_t)min((uint64_t)cap, ((uint64_t)A.c0 + kBlock - 1) / kBlock);
+    // demands above the grid: every path keeps a share in proportion, at
+    // least one CTA each, the small bin takes what the others leave
+    const uint64_t tot = (uint64_t)nl + nm + ns;
+    if (tot > cap) {
+        nl = nl ? max(1u, (uint32_t)((uint64_t)nl * cap / tot)) : 0u;
+        nm = nm ? max(1u, (uint32_t)((uint64_t)nm * cap / tot)) : 0u;
+        while (ns && nl + nm >= cap) {  // leave one CTA at least for the small bin
+            if (nl > 1) --nl; else if (nm > 1) --nm; else break;
+        }
+    }
+    push_binned_body<GG_RELAX_MIN_PLUS1_I32, kBlock>(A, c->op, nl, nm);
+}
+
+// a frontier held as a list only (after a push) gets its bitmap (clear since
+// the frontier's buffer was last consumed)
+__global__ void k_g_tobitmap(GCtl *c) {
+    if (!c->need_bitmap) return;
+    const GFront F = c->f[c->cur];
+    const unsigned long long c0 = F.cnt[FC_BIN0], c1 = F.cnt[FC_BIN1], c2 = F.cnt[FC_BIN2];
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = tid; i < c0 + c1 + c2; i += nth) {
+        const uint32_t v = i < c0 ? F.bins[0][i] : (i < c0 + c1 ? F.bins[1][i - c0] : F.bins[2][i - c0 - c1]);
+        atomicOr(F.bitmap + (v >> 5), 1u << (v & 31));
+    }
+}
+
+__global__ void __launch_bounds__(kBlock, 6) k_g_pull(GCtl *c) {
+    if (c->variant != GG_VAR_PULL_DENSE) return;
+    pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock>(c->A, c->op);
+}
+
+__global__ void k_g_post(GCtl *c) {
+    if (c->variant < 0) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(c->h_while, 0);
+        return;
+    }
+    const int cur = c->cur;
+    const GFront F = c->f[cur], O = c->f[cur ^ 1];
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t words = ((uint64_t)c->n + 31) / 32;
+    for (uint64_t w = tid; w < words; w += nth) F.bitmap[w] = 0u;  // F becomes the next output
+    if (tid == 0) {
+        const int iter = c->iter;
+        if (iter < GG_MAX_ITERS) c->scanned[iter] = O.cnt[FC_SCANNED];
+        for (int i = 0; i < FC_WORDS; ++i) F.cnt[i] = 0;
+        c->has_list[cur ^ 1] = c->variant == GG_VAR_PUSH_SPARSE;
+        c->has_list[cur] = 0;
+        c->has_bitmap[cur ^ 1] = c->variant == GG_VAR_PULL_DENSE;
+        c->has_bitmap[cur] = 0;
+        if (c->variant == GG_VAR_PULL_DENSE) {
+            c->cand_valid = 1;
+            c->cand_cur ^= 1;
+        }
+        c->cur = cur ^ 1;
+        c->iter = iter + 1;
+        if (iter + 1 <= GG_MAX_ITERS) c->t_ns[iter + 1] = g_now();
+        const bool more = O.cnt[FC_NACTV] != 0 && iter + 1 < c->max_iters;
+        if (!more) c->iterations = iter + 1;
+        cudaGraphSetConditional(c->h_while, more ? 1u : 0u);
+    }
+}
+
+struct GraphBfs {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    GCtl *ctl = nullptr;
+    unsigned push_grid = 0, pull_grid = 0, vgrid = 0;
+};
+
+static gg_status add_kernel(gg_ctx *ctx, cudaGraph_t g, cudaGraphNode_t *node, const cudaGraphNode_t *deps, size_t nd,
+                            const void *fn, unsigned grid, unsigned block, GCtl **arg) {
+    cudaKernelNodeParams kp;
+    memset(&kp, 0, sizeof(kp));
+    kp.func = (void *)fn;
+    kp.gridDim = dim3(grid);
+    kp.blockDim = dim3(block);
+    void *args[] = {arg};
+    kp.kernelParams = args;
+    GG_CUDA(ctx, cudaGraphAddKernelNode(node, g, deps, nd, &kp));
+    return GG_OK;
+}
+
+static gg_status add_cond(gg_ctx *ctx, cudaGraph_t g, cudaGraphNode_t *node, const cudaGraphNode_t *deps, size_t nd,
+                          cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaGraph_t *body) {
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    GG_CUDA(ctx, cudaGraphAddNode(node, g, deps, nd, &np));
+    *body = np.conditional.phGraph_out[0];
+    return GG_OK;
+}
+
+void graph_bfs_free(gg_graph *g) {
+    GraphBfs *gb = (GraphBfs *)g->gbfs;
+    if (!gb) return;
+    if (gb->exec) cudaGraphExecDestroy(gb->exec);
+    if (gb->graph) cudaGraphDestroy(gb->graph);
+    cudaFree(gb->ctl);
+    delete gb;
+    g->gbfs = nullptr;
+}
+
+static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
+    gg_ctx *ctx = g->ctx;
+    GG_CUDA(ctx, cudaMalloc(&gb->ctl, sizeof(GCtl)));
+    gb->push_grid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_g_push, kBlock));
+    gb->pull_grid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_g_pull, kBlock));
+    gb->vgrid = (unsigned)(ctx->sm_count * 8);
+    GG_CUDA(ctx, cudaGraphCreate(&gb->graph, 0));
+    cudaGraph_t G = gb->graph;
+    GCtl *ctl = gb->ctl;
+    GCtl **arg = &gb->ctl;
+    cudaGraphConditionalHandle hw, hp, hq;
+    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hw, G, 1, cudaGraphCondAssignDefault));
+    cudaGraphNode_t n_init, n_while;
+    GG_CHECK(add_kernel(ctx, G, &n_init, nullptr, 0, (const void *)k_g_init, gb->vgrid, 256, arg));
+    cudaGraph_t body;
+    GG_CHECK(add_cond(ctx, G, &n_while, &n_init, 1, hw, cudaGraphCondTypeWhile, &body));
+    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hp, body, 0, cudaGraphCondAssignDefault));
+    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hq, body, 0, cudaGraphCondAssignDefault));
+    cudaGraphNode_t n_dec, n_ifp, n_ifq, n_post;
+    GG_CHECK(add_kernel(ctx, body, &n_dec, nullptr, 0, (const void *)k_g_decide, 1, 32, arg));
+    cudaGraph_t bp, bq;
+    GG_CHECK(add_cond(ctx, body, &n_ifp, &n_dec, 1, hp, cudaGraphCondTypeIf, &bp));
+    GG_CHECK(add_cond(ctx, body, &n_ifq, &n_dec, 1, hq, cudaGraphCondTypeIf, &bq));
+    cudaGraphNode_t n_list, n_push, n_bits, n_pull;
+    GG_CHECK(add_kernel(ctx, bp, &n_list, nullptr, 0, (const void *)k_g_tolist, gb->vgrid, 256, arg));
+    GG_CHECK(add_kernel(ctx, bp, &n_push, &n_list, 1, (const void *)k_g_push, gb->push_grid, kBlock, arg));
+    GG_CHECK(add_kernel(ctx, bq, &n_bits, nullptr, 0, (const void *)k_g_tobitmap, gb->vgrid, 256, arg));
+    GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_bits, 1, (const void *)k_g_pull, gb->pull_grid, kBlock, arg));
+    cudaGraphNode_t deps[2] = {n_ifp, n_ifq};
+    GG_CHECK(add_kernel(ctx, body, &n_post, deps, 2, (const void *)k_g_post, gb->vgrid, 256, arg));
+    GG_CUDA(ctx, cudaGraphInstantiate(&gb->exec, G, 0));
+    // the handles live in the control block, set once
+    GCtl h;
+    h.h_while = hw;
+    h.h_push = hp;
+    h.h_pull = hq;
+    GG_CUDA(ctx, cudaMemcpyAsync(&ctl->h_while, &h.h_while, 3 * sizeof(cudaGraphConditionalHandle),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+    return GG_OK;
+}
+
+// BFS levels as one graph launch (host-driven kernels, device decisions)
+gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg_prop *level, gg_prop *prev,
+                          gg_run_stats *st, int *iters_out) {
+    gg_ctx *ctx = g->ctx;
+    if (!g->gbfs) {
+        GraphBfs *gb = new (std::nothrow) GraphBfs;
+        if (!gb) return GG_ERR_OOM;
+        g->gbfs = gb;
+        gg_status s = graph_bfs_build(g, gb);
+        if (s != GG_OK) {
+            graph_bfs_free(g);
+            return s;
+        }
+    }
+    GraphBfs *gb = (GraphBfs *)g->gbfs;
+    for (auto &f : g->tmp_front)
+        if (!f) GG_CHECK(gg_frontier_create(g, &f));
+    for (auto *f : g->tmp_front) {
+        GG_CHECK(frontier_alloc_bins(f));
+        GG_CHECK(frontier_alloc_bitmap(f));
+        f->host_valid = false;
+        f->has_list = f->has_bitmap = f->all = false;
+    }
+    CandLists &cl = g->cand;
+    if (!cl.list[0]) {
+        for (auto &l : cl.list) GG_CUDA(ctx, cudaMalloc(&l, ((size_t)g->n + 1) * 4));
+        GG_CUDA(ctx, cudaMalloc(&cl.cnt, 2 * sizeof(uint64_t)));
+    }
+    const Tuning &t = tuning();
+    // configuration part of the control block (everything before the records)
+    GCtl h;
+    memset(&h, 0, offsetof(GCtl, reached_v));
+    for (int i = 0; i < 2; ++i) {
+        gg_frontier *f = g->tmp_front[i];
+        for (int b = 0; b < NBINS; ++b) h.f[i].bins[b] = f->bins[b];
+        h.f[i].bitmap = f->bitmap;
+        h.f[i].cnt = (unsigned long long *)f->d_cnt;
+    }
+    h.level = (int32_t *)level->d;
+    h.prev = (int32_t *)prev->d;
+    h.root = root;
+    h.n = g->n;
+    h.m = g->m;
+    h.max_iters = (int)std::min<uint64_t>((uint64_t)g->n + 2, (uint64_t)INT_MAX / 2);
+    h.threshold = opt.threshold;
+    h.threshold_k = opt.threshold_k;
+    h.smax = t.bin_small_max;
+    h.mmax = t.bin_medium_max;
+    h.large_ch = t.large_chunk;
+    h.sm_count = (uint32_t)ctx->sm_count;
+    h.pull_k = t.pull_k;
+    h.push_k = t.push_k;
+    h.off = g->off;
+    h.in_off = g->in_off;
+    h.word_prefix = g->heavy.pull_prefix;
+    h.adj = g->adj;
+    h.in_adj = g->in_adj;
+    h.nonisolated = g->nonisolated;
+    h.nonisolated_n = (const unsigned long long *)g->nonisolated_n;
+    h.cand[0] = cl.list[0];
+    h.cand[1] = cl.list[1];
+    h.cand_n = (unsigned long long *)cl.cnt;
+    GG_CUDA(ctx, cudaMemcpyAsync(gb->ctl, &h, offsetof(GCtl, reached_v), cudaMemcpyHostToDevice, ctx->stream));
+    GG_CUDA(ctx, cudaGraphLaunch(gb->exec, ctx->stream));
+    // records back (one wait per run)
+    const size_t rec0 = offsetof(GCtl, reached_v), rec1 = offsetof(GCtl, h_while);
+    GCtl *hr = (GCtl *)std::malloc(sizeof(GCtl));
+    if (!hr) return GG_ERR_OOM;
+    cudaError_t e = cudaMemcpyAsync((char *)hr + offsetof(GCtl, iterations), (char *)gb->ctl + offsetof(GCtl, iterations),
+                                    sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync((char *)hr + rec0, (char *)gb->ctl + rec0, rec1 - rec0,
+                                              cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        std::free(hr);
+        return cuda_error(ctx, e, "graph BFS");
+    }
+    const int T = hr->iterations;
+    *iters_out = T;
+    // kernels the graph ran: init, then per iteration decide, two of the
+    // branch kernels and post (one more decide + post ends an empty run)
+    ctx->launches += 1 + 4 * (uint64_t)T + (T == 0 ? 2 : 0);
+    if (st) {
+        st->vertices_reached = hr->reached_v;
+        st->edges_reached = hr->reached_e;
+        for (int i = 0; i < std::min(T, GG_MAX_ITERS); ++i) {
+            st->variant[i] = hr->variants[i];
+            st->nactv[i] = hr->nactv[i];
+            st->nacte[i] = hr->nacte[i];
+            st->scanned[i] = hr->scanned[i];
+            st->scanned_edges += hr->scanned[i];
+            st->iter_ms[i] = i + 1 <= GG_MAX_ITERS ? (double)(hr->t_ns[i + 1] - hr->t_ns[i]) * 1e-6 : 0.0;
+        }
+    }
+    std::free(hr);
+    for (auto *f : g->tmp_front) f->host_valid = false;
+    g->cand.valid = false;
+    return GG_OK;
+}
+
 }  // namespace gg
 
 using namespace gg;
@@ -1121,6 +1597,22 @@ gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop
     GG_CHECK(tmp_prop(g, 1, GG_I32, &prev));
     if (st) memset(st, 0, sizeof(*st));
     uint64_t k0 = g->ctx->launches;
+    // one CUDA graph per run (device decisions) unless another driver is asked for
+    const bool graph_mode = !use_persistent(g, opt, 1) && (tuning().graph & 1) && opt.variant == GG_VAR_AUTO &&
+                            opt.threshold != GG_THRESH_LEARNED;
+    if (graph_mode) {
+        RunTimer tm(g->ctx);
+        int iters = 0;
+        GG_CHECK(graph_bfs_level(g, root, opt, level, prev, st, &iters));
+        const double ms = tm.stop();
+        if (st) {
+            st->iterations = iters;
+            st->total_ms = ms;
+            st->kernels = g->ctx->launches - k0;
+        }
+        if (host_level) GG_CHECK(gg_prop_download(level, host_level));
+        return gg_ctx_sync(g->ctx);
+    }
     RunTimer tm(g->ctx);
     // BFSLVLv.C:117-129: level = prev = n+1, level[start] = prev[start] = 0
     int32_t inf = (int32_t)g->n + 1, zero = 0;

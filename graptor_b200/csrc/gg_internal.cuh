@@ -145,6 +145,7 @@ struct gg_graph {
     std::vector<uint32_t *> pool_bins, pool_bitmaps;
     std::vector<uint64_t *> pool_cnt;
     void *pstate = nullptr;       // device state block of persistent traversals
+    void *gbfs = nullptr;         // graph-driven BFS: instantiated CUDA graph + control block
     uint32_t *wq = nullptr;       // work queue of fused (asynchronous) pushes
     size_t wq_cap = 0;
     float gini = -1.0f;           // degree Gini coefficient (selector feature), <0: unknown
@@ -183,6 +184,7 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
 gg_status graph_adopt_device_csr(gg_ctx *ctx, uint32_t n, uint64_t m, uint64_t *off, uint32_t *adj, int symmetric,
                                  gg_graph **out);
 gg_status graph_gini(gg_graph *g, float *out);
+void graph_bfs_free(gg_graph *g);
 void selector_features(float *x, double nactv, double nacte, double unreached, int iter, double n, double m,
                        float gini);
 
@@ -203,6 +205,10 @@ struct Tuning {
     // during the launch through L2, which costs the big dense phases more
     // than the per-iteration host round trips it saves on R-MAT BFS)
     int persistent = 4;
+    // analytics run as one CUDA graph whose conditional nodes take each
+    // iteration's push/pull decision on the device (host-driven kernels, no
+    // per-iteration host round trip): bit 0 BFS levels
+    int graph = 1;
     // sparse push steps run fused (asynchronous multi-hop, as CCv with
     // api::fusion) in device-driven runs: bit 2 CC.  Off by default: on
     // B200 the shared work queue (three contended counters per vertex, and

@@ -147,3 +147,40 @@ def test_cc_hooking_exact(ctx, fusion_knobs, gen):
         # road-like: the run ends with the hooking step
         assert used[-1] == gg.VAR_HOOK and st[1].iterations == 2, used
     g.close()
+
+
+@pytest.mark.parametrize("gen", ["rmat", "grid", "er_directed", "tiny"])
+def test_graph_driven_bfs_equals_host_loop(ctx, fusion_knobs, gen):
+    """BFS levels as one CUDA graph (device push/pull decisions) against the
+    host-driven loop: same levels, same iteration count and variant sequence."""
+    old = gg.tuning_get("graph")
+    if gen == "rmat":
+        og, sym = O.rmat(15, 16 << 15, seed=64), True
+    elif gen == "grid":
+        og, sym = O.grid(150, 90, seed=7, del_bp=200), True
+    elif gen == "er_directed":
+        og, sym = O.er(20000, 8.0, seed=3, dangling_bp=200, symmetric=False), False
+    else:
+        og, sym = O.from_edges(5, [(0, 1), (1, 2)]), True
+    g = ctx.upload(og.off, og.adj, symmetric=sym)
+    gg.tuning_set("persistent", 0)
+    roots = [0, int(np.argmax(og.outdeg())), og.n - 1]
+    try:
+        for r in roots:
+            res = {}
+            for mode in (0, 1):
+                gg.tuning_set("graph", mode)
+                st = gg.RunStats()
+                lv = g.bfs_level(r, opts=gg.default_opts(collect=True), stats=st)
+                res[mode] = (lv, st)
+            ref = O.bfs_level(og, r)
+            assert np.array_equal(res[0][0], ref) and np.array_equal(res[1][0], ref), (gen, r)
+            s0, s1 = res[0][1], res[1][1]
+            assert s0.iterations == s1.iterations
+            k = min(s0.iterations, gg.MAX_ITERS)
+            assert [s0.variant[i] for i in range(k)] == [s1.variant[i] for i in range(k)]
+            assert [s0.nactv[i] for i in range(k)] == [s1.nactv[i] for i in range(k)]
+            assert s0.edges_reached == s1.edges_reached
+    finally:
+        gg.tuning_set("graph", old)
+    g.close()
