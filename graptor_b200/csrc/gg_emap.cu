@@ -1136,7 +1136,7 @@ struct GCtl {
     EmapArgs A;  // this step's traversal arguments
     Op<GG_RELAX_MIN_PLUS1_I32> op;
     int variant;  // GG_VAR_PUSH_SPARSE / GG_VAR_PULL_DENSE, -1: finished
-    int need_list, need_bitmap;
+    int need_list, need_bitmap, use_first;
     int cur, iter, max_iters, iterations;
     int has_list[2], has_bitmap[2];
     GFront f[2];
@@ -1152,6 +1152,8 @@ struct GCtl {
     const uint32_t *nonisolated;
     const unsigned long long *nonisolated_n;
     uint32_t *cand[2];
+    uint64_t *chunk_first;  // large-bin chunk prefix (k_g_chunks), chunk_cap entries
+    uint64_t chunk_cap;
     unsigned long long *cand_n;  // [2]
     int cand_cur, cand_valid;
     // records
@@ -1159,7 +1161,7 @@ struct GCtl {
     int variants[GG_MAX_ITERS];
     unsigned long long nactv[GG_MAX_ITERS], nacte[GG_MAX_ITERS], scanned[GG_MAX_ITERS];
     unsigned long long t_ns[GG_MAX_ITERS + 1];
-    cudaGraphConditionalHandle h_while, h_push, h_pull;
+    cudaGraphConditionalHandle h_while, h_push, h_pull, h_list, h_bits, h_chunks;
 };
 
 __device__ __forceinline__ unsigned long long g_now() {
@@ -1176,6 +1178,8 @@ __device__ __forceinline__ bool d_threshold_sparse(int kind, int k, uint64_t nac
     default: return (nactv + nacte) <= (m / 20);
     }
 }
+
+__device__ void decide_step(GCtl *c);
 
 __global__ void k_g_init(GCtl *c) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
@@ -1214,11 +1218,13 @@ __global__ void k_g_init(GCtl *c) {
         c->reached_e = 0;
         c->variant = -1;
         c->t_ns[0] = g_now();
+        decide_step(c);  // the first step's decision
     }
 }
 
-__global__ void k_g_decide(GCtl *c) {
-    if (threadIdx.x != 0) return;
+// the decision of the step about to run (one thread): reads the frontier
+// counts, writes the step's arguments, sets the branch and loop conditions
+__device__ void decide_step(GCtl *c) {
     const GFront F = c->f[c->cur], O = c->f[c->cur ^ 1];
     const unsigned long long nactv = F.cnt[FC_NACTV], nacte = F.cnt[FC_NACTE];
     const int iter = c->iter;
@@ -1227,6 +1233,10 @@ __global__ void k_g_decide(GCtl *c) {
         c->iterations = iter;
         cudaGraphSetConditional(c->h_push, 0);
         cudaGraphSetConditional(c->h_pull, 0);
+        cudaGraphSetConditional(c->h_list, 0);
+        cudaGraphSetConditional(c->h_bits, 0);
+        cudaGraphSetConditional(c->h_chunks, 0);
+        cudaGraphSetConditional(c->h_while, 0);
         return;
     }
     const bool push = d_threshold_sparse(c->threshold, c->threshold_k, nactv, nacte, c->m);
@@ -1277,9 +1287,17 @@ __global__ void k_g_decide(GCtl *c) {
     c->op = op;
     c->variant = push ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
     c->need_list = push && !c->has_list[c->cur];
+    c->use_first = 0;
+    // a large bin too big for a CTA's shared table gets its chunk prefix from
+    // k_g_chunks (its size is known here unless the list is still to be built)
+    const bool chunks = push && (c->need_list || F.cnt[FC_BIN2] > kLargeLocal);
+    cudaGraphSetConditional(c->h_chunks, chunks ? 1u : 0u);
     c->need_bitmap = !push && !c->has_bitmap[c->cur];
     cudaGraphSetConditional(c->h_push, push ? 1u : 0u);
     cudaGraphSetConditional(c->h_pull, push ? 0u : 1u);
+    cudaGraphSetConditional(c->h_list, c->need_list ? 1u : 0u);
+    cudaGraphSetConditional(c->h_bits, c->need_bitmap ? 1u : 0u);
+    cudaGraphSetConditional(c->h_while, 1u);
 }
 
 // a frontier held as a bitmap only (after a pull) gets its binned list
@@ -1312,34 +1330,59 @@ __global__ void __launch_bounds__(256) k_g_tolist(GCtl *c) {
 
 // the push step: the partition of the fixed grid over the three bins is
 // derived by every CTA from the same device counts
-__global__ void __launch_bounds__(kBlock) k_g_push(GCtl *c) {
+// The step's arguments are copied once per CTA into shared memory: the
+// bodies then read them like kernel parameters (cheap broadcast loads), with
+// no register copy to spill and no global reloads after the kernel's stores.
+__device__ __noinline__ void g_push_setup(GCtl *c, uint32_t cap, EmapArgs *sA, Op<GG_RELAX_MIN_PLUS1_I32> *sOp,
+                                          uint32_t *s_nl, uint32_t *s_nm);
+
+__global__ void __launch_bounds__(kBlock, 6) k_g_push(GCtl *c) {
     if (c->variant != GG_VAR_PUSH_SPARSE) return;
-    EmapArgs A = c->A;
-    const GFront F = c->f[c->cur];
-    A.c0 = (uint32_t)F.cnt[FC_BIN0];
-    A.c1 = (uint32_t)F.cnt[FC_BIN1];
-    A.c2 = (uint32_t)F.cnt[FC_BIN2];
-    A.merge_med = A.c1 && A.c1 + A.c2 <= kLargeLocal && A.c1 < c->sm_count;
-    A.large_as_med = !A.merge_med && A.c2 > kLargeLocal;
-    const uint32_t cap = gridDim.x;
-    const uint64_t nacte = F.cnt[FC_NACTE];
-    uint32_t nl = 0;
-    if ((A.c2 && !A.large_as_med) || A.merge_med)
-        nl = (uint32_t)min((uint64_t)cap, nacte / A.large_ch + A.c2 + (A.merge_med ? A.c1 : 0u));
-    const uint32_t cmed = A.merge_med ? 0u : A.c1 + (A.large_as_med ? A.c2 : 0u);
-    uint32_t nm = (uint32_t)min((uint64_t)cap, ((uint64_t)cmed + kBlock / 32 - 1) / (kBlock / 32));
-    const uint32_t ns = (uint32_t)min((uint64_t)cap, ((uint64_t)A.c0 + kBlock - 1) / kBlock);
-    // demands above the grid: every path keeps a share in proportion, at
-    // least one CTA each, the small bin takes what the others leave
-    const uint64_t tot = (uint64_t)nl + nm + ns;
-    if (tot > cap) {
-        nl = nl ? max(1u, (uint32_t)((uint64_t)nl * cap / tot)) : 0u;
-        nm = nm ? max(1u, (uint32_t)((uint64_t)nm * cap / tot)) : 0u;
-        while (ns && nl + nm >= cap) {  // leave one CTA at least for the small bin
-            if (nl > 1) --nl; else if (nm > 1) --nm; else break;
+    __shared__ EmapArgs sA;
+    __shared__ Op<GG_RELAX_MIN_PLUS1_I32> sOp;
+    __shared__ uint32_t s_nl, s_nm;
+    if (threadIdx.x == 0) g_push_setup(c, gridDim.x, &sA, &sOp, &s_nl, &s_nm);
+    __syncthreads();
+    push_binned_body<GG_RELAX_MIN_PLUS1_I32, kBlock>(sA, sOp, s_nl, s_nm);
+}
+
+// one thread per CTA: the push arguments and the partition of the grid
+__device__ __noinline__ void g_push_setup(GCtl *c, uint32_t cap, EmapArgs *sA, Op<GG_RELAX_MIN_PLUS1_I32> *sOp,
+                                          uint32_t *s_nl, uint32_t *s_nm) {
+    {
+        EmapArgs A = c->A;
+        const GFront F = c->f[c->cur];
+        A.c0 = (uint32_t)F.cnt[FC_BIN0];
+        A.c1 = (uint32_t)F.cnt[FC_BIN1];
+        A.c2 = (uint32_t)F.cnt[FC_BIN2];
+        A.merge_med = A.c1 && A.c1 + A.c2 <= kLargeLocal && A.c1 < c->sm_count;
+        A.large_as_med = !A.merge_med && A.c2 > kLargeLocal;
+        if (A.c2 > kLargeLocal && c->use_first) {  // chunk prefix built by k_g_chunks
+            A.large_first = c->chunk_first;
+            A.large_as_med = 0;
         }
+        const uint64_t nacte = F.cnt[FC_NACTE];
+        uint32_t nl = 0;
+        if ((A.c2 && !A.large_as_med) || A.merge_med)
+            nl = (uint32_t)min((uint64_t)cap, nacte / A.large_ch + A.c2 + (A.merge_med ? A.c1 : 0u));
+        const uint32_t cmed = A.merge_med ? 0u : A.c1 + (A.large_as_med ? A.c2 : 0u);
+        uint32_t nm = (uint32_t)min((uint64_t)cap, ((uint64_t)cmed + kBlock / 32 - 1) / (kBlock / 32));
+        const uint32_t ns = (uint32_t)min((uint64_t)cap, ((uint64_t)A.c0 + kBlock - 1) / kBlock);
+        // demands above the grid: every path keeps a share in proportion, at
+        // least one CTA each, the small bin takes what the others leave
+        const uint64_t tot = (uint64_t)nl + nm + ns;
+        if (tot > cap) {
+            nl = nl ? max(1u, (uint32_t)((uint64_t)nl * cap / tot)) : 0u;
+            nm = nm ? max(1u, (uint32_t)((uint64_t)nm * cap / tot)) : 0u;
+            while (ns && nl + nm >= cap) {  // leave one CTA at least for the small bin
+                if (nl > 1) --nl; else if (nm > 1) --nm; else break;
+            }
+        }
+        *sA = A;
+        *sOp = c->op;
+        *s_nl = nl;
+        *s_nm = nm;
     }
-    push_binned_body<GG_RELAX_MIN_PLUS1_I32, kBlock>(A, c->op, nl, nm);
 }
 
 // a frontier held as a list only (after a push) gets its bitmap (clear since
@@ -1357,37 +1400,99 @@ __global__ void k_g_tobitmap(GCtl *c) {
 
 __global__ void __launch_bounds__(kBlock, 6) k_g_pull(GCtl *c) {
     if (c->variant != GG_VAR_PULL_DENSE) return;
-    pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock>(c->A, c->op);
+    __shared__ EmapArgs sA;
+    __shared__ Op<GG_RELAX_MIN_PLUS1_I32> sOp;
+    if (threadIdx.x == 0) {
+        sA = c->A;
+        sOp = c->op;
+    }
+    __syncthreads();
+    pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock>(sA, sOp);
 }
 
-__global__ void k_g_post(GCtl *c) {
+// the consumed frontier's bitmap is cleared for its next use as an output
+// (only when the step that made it, or the conversion for a pull, set one)
+__global__ void k_g_clear(GCtl *c) {
+    if (c->variant < 0 || (!c->has_bitmap[c->cur] && !c->need_bitmap)) return;
+    uint32_t *bm = c->f[c->cur].bitmap;
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t words = ((uint64_t)c->n + 31) / 32;
+    for (uint64_t w = tid; w < words; w += nth) bm[w] = 0u;
+}
+
+// bookkeeping of the step that ran, then the next step's decision (one thread)
+__global__ void k_g_next(GCtl *c) {
+    if (threadIdx.x != 0) return;
     if (c->variant < 0) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) cudaGraphSetConditional(c->h_while, 0);
+        cudaGraphSetConditional(c->h_while, 0);
         return;
     }
     const int cur = c->cur;
     const GFront F = c->f[cur], O = c->f[cur ^ 1];
-    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t words = ((uint64_t)c->n + 31) / 32;
-    for (uint64_t w = tid; w < words; w += nth) F.bitmap[w] = 0u;  // F becomes the next output
-    if (tid == 0) {
-        const int iter = c->iter;
-        if (iter < GG_MAX_ITERS) c->scanned[iter] = O.cnt[FC_SCANNED];
-        for (int i = 0; i < FC_WORDS; ++i) F.cnt[i] = 0;
-        c->has_list[cur ^ 1] = c->variant == GG_VAR_PUSH_SPARSE;
-        c->has_list[cur] = 0;
-        c->has_bitmap[cur ^ 1] = c->variant == GG_VAR_PULL_DENSE;
-        c->has_bitmap[cur] = 0;
-        if (c->variant == GG_VAR_PULL_DENSE) {
-            c->cand_valid = 1;
-            c->cand_cur ^= 1;
+    const int iter = c->iter;
+    if (iter < GG_MAX_ITERS) c->scanned[iter] = O.cnt[FC_SCANNED];
+    for (int i = 0; i < FC_WORDS; ++i) F.cnt[i] = 0;
+    c->has_list[cur ^ 1] = c->variant == GG_VAR_PUSH_SPARSE;
+    c->has_list[cur] = 0;
+    c->has_bitmap[cur ^ 1] = c->variant == GG_VAR_PULL_DENSE;
+    c->has_bitmap[cur] = 0;
+    if (c->variant == GG_VAR_PULL_DENSE) {
+        c->cand_valid = 1;
+        c->cand_cur ^= 1;
+    }
+    c->cur = cur ^ 1;
+    c->iter = iter + 1;
+    if (iter + 1 <= GG_MAX_ITERS) c->t_ns[iter + 1] = g_now();
+    decide_step(c);  // an empty frontier or the iteration bound ends the loop
+}
+
+// Chunk prefix of a large bin of more than kLargeLocal rows (one CTA of
+// 1024 threads, tiles of 1024 rows): first[i] = chunks of rows before i.
+__global__ void __launch_bounds__(1024) k_g_chunks(GCtl *c) {
+    __shared__ unsigned long long s_warp[32];
+    __shared__ unsigned long long s_base;
+    const GFront F = c->f[c->cur];
+    const uint64_t c2 = F.cnt[FC_BIN2];
+    if (c2 <= kLargeLocal || c2 + 1 > c->chunk_cap) return;  // use_first stays 0: warp rows
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    const uint64_t *off = c->off;
+    const uint32_t ch = c->large_ch;
+    if (threadIdx.x == 0) s_base = 0;
+    __syncthreads();
+    for (uint64_t base = 0; base < c2; base += 1024) {
+        const uint64_t i = base + threadIdx.x;
+        unsigned long long x = 0;
+        if (i < c2) {
+            const uint32_t v = F.bins[2][i];
+            x = (off[v + 1] - off[v] + ch - 1) / ch;
         }
-        c->cur = cur ^ 1;
-        c->iter = iter + 1;
-        if (iter + 1 <= GG_MAX_ITERS) c->t_ns[iter + 1] = g_now();
-        const bool more = O.cnt[FC_NACTV] != 0 && iter + 1 < c->max_iters;
-        if (!more) c->iterations = iter + 1;
-        cudaGraphSetConditional(c->h_while, more ? 1u : 0u);
+        unsigned long long inc = x;  // inclusive scan within the warp
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const unsigned long long t = __shfl_up_sync(0xffffffffu, inc, d);
+            if ((int)lane >= d) inc += t;
+        }
+        if (lane == 31) s_warp[wid] = inc;
+        __syncthreads();
+        if (wid == 0) {
+            unsigned long long w = s_warp[lane], wi = w;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const unsigned long long t = __shfl_up_sync(0xffffffffu, wi, d);
+                if ((int)lane >= d) wi += t;
+            }
+            s_warp[lane] = wi - w;  // exclusive prefix of the warp totals
+        }
+        __syncthreads();
+        const unsigned long long b = s_base;
+        if (i < c2) c->chunk_first[i] = b + s_warp[wid] + inc - x;
+        __syncthreads();
+        if (threadIdx.x == 1023) s_base = b + s_warp[wid] + inc;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        c->chunk_first[c2] = s_base;
+        c->use_first = 1;
     }
 }
 
@@ -1395,6 +1500,8 @@ struct GraphBfs {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     GCtl *ctl = nullptr;
+    uint64_t *chunk_first = nullptr;
+    uint64_t chunk_cap = 0;
     unsigned push_grid = 0, pull_grid = 0, vgrid = 0;
 };
 
@@ -1429,6 +1536,7 @@ void graph_bfs_free(gg_graph *g) {
     if (gb->exec) cudaGraphExecDestroy(gb->exec);
     if (gb->graph) cudaGraphDestroy(gb->graph);
     cudaFree(gb->ctl);
+    cudaFree(gb->chunk_first);
     delete gb;
     g->gbfs = nullptr;
 }
@@ -1443,34 +1551,44 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     cudaGraph_t G = gb->graph;
     GCtl *ctl = gb->ctl;
     GCtl **arg = &gb->ctl;
-    cudaGraphConditionalHandle hw, hp, hq;
+    // init (+ first decision) -> WHILE { IF push { IF list {tolist} -> push },
+    //                                  IF pull { IF bits {tobitmap} -> pull } -> clear -> next }
+    // The branch handles keep the value the decision set (no default
+    // assignment); the loop handle starts at 1 on every launch.
+    cudaGraphConditionalHandle hw, hp, hq, hl, hb, hc;
     GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hw, G, 1, cudaGraphCondAssignDefault));
     cudaGraphNode_t n_init, n_while;
     GG_CHECK(add_kernel(ctx, G, &n_init, nullptr, 0, (const void *)k_g_init, gb->vgrid, 256, arg));
     cudaGraph_t body;
     GG_CHECK(add_cond(ctx, G, &n_while, &n_init, 1, hw, cudaGraphCondTypeWhile, &body));
-    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hp, body, 0, cudaGraphCondAssignDefault));
-    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hq, body, 0, cudaGraphCondAssignDefault));
-    cudaGraphNode_t n_dec, n_ifp, n_ifq, n_post;
-    GG_CHECK(add_kernel(ctx, body, &n_dec, nullptr, 0, (const void *)k_g_decide, 1, 32, arg));
+    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hp, body, 0, 0));
+    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hq, body, 0, 0));
+    cudaGraphNode_t n_ifp, n_ifq, n_clear, n_next;
     cudaGraph_t bp, bq;
-    GG_CHECK(add_cond(ctx, body, &n_ifp, &n_dec, 1, hp, cudaGraphCondTypeIf, &bp));
-    GG_CHECK(add_cond(ctx, body, &n_ifq, &n_dec, 1, hq, cudaGraphCondTypeIf, &bq));
-    cudaGraphNode_t n_list, n_push, n_bits, n_pull;
-    GG_CHECK(add_kernel(ctx, bp, &n_list, nullptr, 0, (const void *)k_g_tolist, gb->vgrid, 256, arg));
-    GG_CHECK(add_kernel(ctx, bp, &n_push, &n_list, 1, (const void *)k_g_push, gb->push_grid, kBlock, arg));
-    GG_CHECK(add_kernel(ctx, bq, &n_bits, nullptr, 0, (const void *)k_g_tobitmap, gb->vgrid, 256, arg));
-    GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_bits, 1, (const void *)k_g_pull, gb->pull_grid, kBlock, arg));
+    GG_CHECK(add_cond(ctx, body, &n_ifp, nullptr, 0, hp, cudaGraphCondTypeIf, &bp));
+    GG_CHECK(add_cond(ctx, body, &n_ifq, nullptr, 0, hq, cudaGraphCondTypeIf, &bq));
+    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hl, bp, 0, 0));
+    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hc, bp, 0, 0));
+    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hb, bq, 0, 0));
+    cudaGraphNode_t n_ifl, n_ifb, n_list, n_push, n_bits, n_pull;
+    cudaGraph_t bl, bb;
+    GG_CHECK(add_cond(ctx, bp, &n_ifl, nullptr, 0, hl, cudaGraphCondTypeIf, &bl));
+    GG_CHECK(add_kernel(ctx, bl, &n_list, nullptr, 0, (const void *)k_g_tolist, gb->vgrid, 256, arg));
+    cudaGraphNode_t n_ifc, n_chunks;
+    cudaGraph_t bc;
+    GG_CHECK(add_cond(ctx, bp, &n_ifc, &n_ifl, 1, hc, cudaGraphCondTypeIf, &bc));
+    GG_CHECK(add_kernel(ctx, bc, &n_chunks, nullptr, 0, (const void *)k_g_chunks, 1, 1024, arg));
+    GG_CHECK(add_kernel(ctx, bp, &n_push, &n_ifc, 1, (const void *)k_g_push, gb->push_grid, kBlock, arg));
+    GG_CHECK(add_cond(ctx, bq, &n_ifb, nullptr, 0, hb, cudaGraphCondTypeIf, &bb));
+    GG_CHECK(add_kernel(ctx, bb, &n_bits, nullptr, 0, (const void *)k_g_tobitmap, gb->vgrid, 256, arg));
+    GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_ifb, 1, (const void *)k_g_pull, gb->pull_grid, kBlock, arg));
     cudaGraphNode_t deps[2] = {n_ifp, n_ifq};
-    GG_CHECK(add_kernel(ctx, body, &n_post, deps, 2, (const void *)k_g_post, gb->vgrid, 256, arg));
+    GG_CHECK(add_kernel(ctx, body, &n_clear, deps, 2, (const void *)k_g_clear, (unsigned)ctx->sm_count * 2, 256, arg));
+    GG_CHECK(add_kernel(ctx, body, &n_next, &n_clear, 1, (const void *)k_g_next, 1, 32, arg));
     GG_CUDA(ctx, cudaGraphInstantiate(&gb->exec, G, 0));
     // the handles live in the control block, set once
-    GCtl h;
-    h.h_while = hw;
-    h.h_push = hp;
-    h.h_pull = hq;
-    GG_CUDA(ctx, cudaMemcpyAsync(&ctl->h_while, &h.h_while, 3 * sizeof(cudaGraphConditionalHandle),
-                                 cudaMemcpyHostToDevice, ctx->stream));
+    cudaGraphConditionalHandle hs[6] = {hw, hp, hq, hl, hb, hc};
+    GG_CUDA(ctx, cudaMemcpyAsync(&ctl->h_while, hs, sizeof(hs), cudaMemcpyHostToDevice, ctx->stream));
     return GG_OK;
 }
 
@@ -1533,6 +1651,17 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     h.in_adj = g->in_adj;
     h.nonisolated = g->nonisolated;
     h.nonisolated_n = (const unsigned long long *)g->nonisolated_n;
+    // chunk prefix room: rows above bin_medium_max edges, at most m / (max + 1)
+    const uint64_t need = g->m / ((uint64_t)t.bin_medium_max + 1) + 2;
+    if (gb->chunk_cap < need) {
+        cudaFree(gb->chunk_first);
+        gb->chunk_first = nullptr;
+        gb->chunk_cap = 0;
+        GG_CUDA(ctx, cudaMalloc(&gb->chunk_first, need * 8));
+        gb->chunk_cap = need;
+    }
+    h.chunk_first = gb->chunk_first;
+    h.chunk_cap = gb->chunk_cap;
     h.cand[0] = cl.list[0];
     h.cand[1] = cl.list[1];
     h.cand_n = (unsigned long long *)cl.cnt;
@@ -1553,9 +1682,9 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     }
     const int T = hr->iterations;
     *iters_out = T;
-    // kernels the graph ran: init, then per iteration decide, two of the
-    // branch kernels and post (one more decide + post ends an empty run)
-    ctx->launches += 1 + 4 * (uint64_t)T + (T == 0 ? 2 : 0);
+    // kernels the graph ran: init, then per iteration the step kernel, clear
+    // and next (plus a list or bitmap conversion where the variant changes)
+    ctx->launches += 1 + 3 * (uint64_t)T;
     if (st) {
         st->vertices_reached = hr->reached_v;
         st->edges_reached = hr->reached_e;

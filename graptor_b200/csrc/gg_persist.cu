@@ -564,11 +564,23 @@ __device__ void phase_hook(const PArgs &P) {
     }
 }
 
+// The root of x without path halving: in the final pass every vertex's
+// entry is written once, by its own thread, with its root; a halving store
+// from another thread's walk could land after it and leave a non-root there.
+__device__ __forceinline__ uint32_t uf_root(const uint32_t *lab, uint32_t x) {
+    for (int guard = 0; guard < (1 << 26); ++guard) {  // a chain of n links at most
+        const uint32_t p = ldcg(lab + x);
+        if (p == x) return x;
+        x = p;
+    }
+    return x;
+}
+
 __device__ void phase_hook_finish(const PArgs &P) {
     uint32_t *lab = (uint32_t *)P.a;
     const uint64_t tid = (uint64_t)blockIdx.x * kPB + threadIdx.x, nth = (uint64_t)gridDim.x * kPB;
     for (uint64_t v = tid; v < P.n; v += nth) {
-        const uint32_t r = uf_find(lab, (uint32_t)v);
+        const uint32_t r = uf_root(lab, (uint32_t)v);
         lab[v] = r;
         if (P.prev) ((uint32_t *)P.prev)[v] = r;
     }

@@ -58,9 +58,12 @@ def main():
     ap.add_argument("--seeds", type=int, default=128)
     ap.add_argument("--persistent", type=int, default=None, help="tuning knob: device-driven analytics mask")
     ap.add_argument("--threshold", default="default", choices=["default", "learned"])
+    ap.add_argument("--graph-mode", type=int, default=None, help="tuning knob: graph-driven BFS levels (0/1)")
     a = ap.parse_args()
     if a.persistent is not None:
         gg.tuning_set("persistent", a.persistent)
+    if a.graph_mode is not None:
+        gg.tuning_set("graph", a.graph_mode)
     ctx = gg.Context(0)
     g = make_graph(ctx, a)
     out = {"case": a.case, "graph": a.graph, "n": g.n, "m": g.m, "persistent": gg.tuning_get("persistent")}
@@ -73,7 +76,7 @@ def main():
         rs = roots_of(g, a.roots)
         for r in rs[: a.warmup]:
             g.bfs_level(r, host=False)
-        tot, ker, last = [], [], None
+        tot, ker, last, worst = [], [], None, None
         for _ in range(a.reps):
             for r in rs:
                 st = gg.RunStats()
@@ -81,8 +84,12 @@ def main():
                 tot.append(st.total_ms)
                 ker.append(sum(st.iter_ms[i] for i in range(min(st.iterations, gg.MAX_ITERS))))
                 last = st
+                if worst is None or st.total_ms > worst[1]:
+                    worst = (r, st.total_ms, iter_table(st))
         out.update(ms_per_bfs=round(float(np.mean(tot)), 4), kernel_ms_per_bfs=round(float(np.mean(ker)), 4),
-                   iterations=iter_table(last))
+                   ms_per_bfs_median=round(float(np.median(tot)), 4),
+                   per_root_ms=[round(x, 3) for x in tot[: len(rs)]], iterations=iter_table(last),
+                   worst_root=worst[0], worst_ms=round(worst[1], 3), worst_iterations=worst[2])
     elif a.case == "cc":
         for _ in range(a.warmup):
             g.cc(host=False)

@@ -184,3 +184,18 @@ def test_graph_driven_bfs_equals_host_loop(ctx, fusion_knobs, gen):
     finally:
         gg.tuning_set("graph", old)
     g.close()
+
+
+def test_cc_hooking_repeated_long_chains(ctx, fusion_knobs):
+    """Hooking's final pass writes every label once; repeated runs on long
+    chains (deep trees) must always give the canonical labels."""
+    gg.tuning_set("persistent", 4)
+    gg.tuning_set("cc_hook", 1)
+    n = 200000
+    edges = [(i, i + 1) for i in range(n - 1) if i % 50000 != 49999]  # four long paths
+    og = O.from_edges(n, edges)
+    g = ctx.upload(og.off, og.adj)
+    ref = O.cc(og)
+    for _ in range(25):
+        assert np.array_equal(g.cc(), ref)
+    g.close()
