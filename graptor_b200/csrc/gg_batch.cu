@@ -292,10 +292,8 @@ __device__ __forceinline__ void bf4_acc(uint2 v, float4 &a) {
 
 __device__ __forceinline__ uint2 f4_to_bf4(float4 f) {
     uint2 r;
-    r.x = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f.x)) |
-          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f.y)) << 16);
-    r.y = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f.z)) |
-          ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(f.w)) << 16);
+    r.x = (uint32_t)dev::bf16_rne(f.x) | ((uint32_t)dev::bf16_rne(f.y) << 16);
+    r.y = (uint32_t)dev::bf16_rne(f.z) | ((uint32_t)dev::bf16_rne(f.w) << 16);
     return r;
 }
 

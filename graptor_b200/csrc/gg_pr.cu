@@ -65,7 +65,7 @@ template <> struct Store<GG_F32> {
 template <> struct Store<GG_BF16> {
     using T = uint16_t;
     __device__ static float dec(T v) { return __uint_as_float((uint32_t)v << 16); }
-    __device__ static T enc(float f) { return __bfloat16_as_ushort(__float2bfloat16_rn(f)); }
+    __device__ static T enc(float f) { return dev::bf16_rne(f); }
 };
 template <> struct Store<GG_F16> {
     using T = uint16_t;
