@@ -905,10 +905,18 @@ __device__ void phase_merge_push(const PArgs &P, const POp<R> &op, const PFront 
 // reused while every feature stays within kSelReuse of the evaluated ones
 // (every CTA sees the same sequence, so all CTAs still agree).
 struct SelCache {
-    float x[GG_SEL_FEATURES];
+    unsigned long long nactv, nacte, unreached;
+    int iter;
     int choice;
     int valid;
 };
+
+// within a factor 1 + 1/16 (log2 change below 0.09: under 1/256 of a
+// log-scaled feature)
+__device__ __forceinline__ bool sel_close(unsigned long long a, unsigned long long b) {
+    const unsigned long long d = a > b ? a - b : b - a, mx = a > b ? a : b;
+    return d * 16 <= mx;
+}
 
 __device__ int choose_variant(const PArgs &P, int iter, unsigned long long nactv, unsigned long long nacte,
                               bool f_all, const PState *st, int *s_choice, SelCache *cache) {
@@ -923,50 +931,48 @@ __device__ int choose_variant(const PArgs &P, int iter, unsigned long long nactv
                                                                                             : GG_VAR_PULL_DENSE;
     case GG_THRESH_LEARNED:
         if (P.sel_w) {
+            // reuse the last evaluation while the inputs stay close (every
+            // thread tests the shared cache: no barrier on the common path)
+            const double n = P.n, m = (double)P.m, fv = (double)nactv, fe = (double)nacte;
+            const unsigned long long reached = ldcg(&st->reached_v);
+            const unsigned long long unr = reached < P.n ? P.n - reached : 0ull;
+            const int it = min(iter, 255);
+            if (cache->valid && sel_close(nactv, cache->nactv) && sel_close(nacte, cache->nacte) &&
+                sel_close(unr, cache->unreached) && it - cache->iter < 8)
+                return cache->choice;
             // warp 0 evaluates the network, the CTA reads its choice
             if (threadIdx.x < 32) {
-                const double n = P.n, m = (double)P.m, fv = (double)nactv, fe = (double)nacte;
-                const double unr = n - (double)ldcg(&st->reached_v);
                 float x[GG_SEL_FEATURES];
                 x[0] = (float)(log2(1.0 + fv) / 32);
                 x[1] = (float)(log2(1.0 + fe) / 40);
-                x[2] = (float)(log2(1.0 + (unr > 0 ? unr : 0)) / 32);
-                x[3] = (float)(min(iter, 255) / 64.0);
+                x[2] = (float)(log2(1.0 + (double)unr) / 32);
+                x[3] = (float)(it / 64.0);
                 x[4] = (float)(log2(1.0 + (n > 0 ? m / n : 0)) / 8);
                 x[5] = P.gini;
                 x[6] = (float)(n > 0 ? fv / n : 0);
                 x[7] = (float)(m > 0 ? fe / m : 0);
                 x[8] = (float)fmin(4.0, m > 0 ? (fv + fe) / m : 0.0);
                 x[9] = (float)(log2(n > 1 ? n : 1.0) / 32);
-                bool reuse = cache->valid != 0;
-                for (int i = 0; i < GG_SEL_FEATURES && reuse; ++i)
-                    reuse = fabsf(x[i] - cache->x[i]) <= (i == 3 ? 8.0f / 64 : 1.0f / 64);
-                int best;
-                if (reuse) {
-                    best = cache->choice;
-                } else {
-                    float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
-                    mlp::warp_forward(P.sel_w, x, o, z1, a1, z2, a2);
-                    best = 0;
-                    for (int v = 1; v < GG_SEL_VARIANTS; ++v)
-                        if (o[v] < o[best]) best = v;
-                    // the threshold's choice stands unless the network
-                    // predicts a clear gain over it
-                    const int tv = (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
-                    if (!(o[best] < o[tv] - mlp::kSelMargin)) best = tv;
-                    __syncwarp();
-                    if (threadIdx.x == 0) {
-                        for (int i = 0; i < GG_SEL_FEATURES; ++i) cache->x[i] = x[i];
-                        cache->choice = best;
-                        cache->valid = 1;
-                    }
+                float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
+                mlp::warp_forward(P.sel_w, x, o, z1, a1, z2, a2);
+                int best = 0;
+                for (int v = 1; v < GG_SEL_VARIANTS; ++v)
+                    if (o[v] < o[best]) best = v;
+                // the threshold's choice stands unless the network predicts
+                // a clear gain over it
+                const int tv = (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+                if (!(o[best] < o[tv] - mlp::kSelMargin)) best = tv;
+                if (threadIdx.x == 0) {
+                    cache->nactv = nactv;
+                    cache->nacte = nacte;
+                    cache->unreached = unr;
+                    cache->iter = it;
+                    cache->choice = best;
+                    cache->valid = 1;
                 }
-                if (threadIdx.x == 0) *s_choice = best;
             }
             __syncthreads();
-            const int c = *s_choice;
-            __syncthreads();
-            return c;
+            return cache->choice;
         }
         // no network attached: the default threshold
     default:
