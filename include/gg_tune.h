@@ -15,7 +15,10 @@
  * kernels), pr_stream (1: warp-streamed segmented PageRank gather, 0:
  * per-row), persistent (bit mask: 1 BFS levels, 2 BFS parents, 4 CC run as
  * one device-driven cooperative launch; otherwise one launch per iteration
- * from the host), cc_hook (1: a device-driven CC run of a symmetric graph
+ * from the host), graph (1, the default: BFS levels run as one CUDA graph
+ * whose conditional nodes take each step's push/pull decision on the
+ * device; 0: one host round trip per iteration), cc_hook (1: a
+ * device-driven CC run of a symmetric graph
  * that passes CCv's road-network test after its first step finishes by
  * min-id hooking; 0: label propagation throughout), fusion (4: the sparse
  * push steps of a device-driven CC run fused, as CCv with api::fusion: a
