@@ -351,6 +351,24 @@ def selector_eval(ctx, graphs):
                 gg.attach_selector(g, None)
     finally:
         gg.tuning_set("persistent", old)
+    # the default BFS driver (one CUDA graph per run, device decisions): the
+    # network picks between its push and pull
+    if sel:
+        for name, g, roots in graphs:
+            gg.attach_selector(g, sel)
+            tot = {}
+            for mode, opts in (("threshold", gg.default_opts(gg.THRESH_DEFAULT, collect=True)),
+                               ("learned", gg.default_opts(gg.THRESH_LEARNED, collect=True))):
+                t = 0.0
+                for r in roots:
+                    g.bfs_level(r, host=False, opts=opts)
+                    st = gg.RunStats()
+                    g.bfs_level(r, host=False, opts=opts, stats=st)
+                    t += st.total_ms
+                tot[mode] = t / len(roots)
+            out[name]["bfs_graph_driver"] = {k: round(v, 4) for k, v in tot.items()}
+            out[name]["bfs_graph_driver"]["learned_vs_threshold"] = round(tot["threshold"] / tot["learned"], 3)
+            gg.attach_selector(g, None)
     return out
 
 

@@ -39,6 +39,7 @@
 
 #include "gg_batch.h"
 #include "gg_internal.cuh"
+#include "gg_mlp.cuh"
 
 namespace gg {
 
@@ -1145,6 +1146,11 @@ struct GCtl {
     uint32_t root, n;
     uint64_t m;
     int threshold, threshold_k;
+    const __nv_bfloat16 *sel_w;  // learned selector weights (bfloat16), or null: the threshold decides
+    float gini;
+    // last network evaluation: reused while the frontier counts stay within 1/16
+    unsigned long long sel_nactv, sel_nacte, sel_unr;
+    int sel_iter, sel_push, sel_valid;
     uint32_t smax, mmax, large_ch, sm_count;
     int pull_k, push_k;
     const uint64_t *off, *in_off, *word_prefix;
@@ -1214,21 +1220,29 @@ __global__ void k_g_init(GCtl *c) {
         c->iterations = 0;
         c->cand_valid = 0;
         c->cand_cur = 0;
+        c->sel_valid = 0;
         c->reached_v = 0;
         c->reached_e = 0;
         c->variant = -1;
         c->t_ns[0] = g_now();
-        decide_step(c);  // the first step's decision
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 32) {
+        __syncwarp();
+        decide_step(c);  // the first step's decision (warp 0 of CTA 0)
     }
 }
 
 // the decision of the step about to run (one thread): reads the frontier
 // counts, writes the step's arguments, sets the branch and loop conditions
+// Called by the 32 lanes of one warp (the network is evaluated by a warp);
+// lane 0 writes the decision.
 __device__ void decide_step(GCtl *c) {
+    const uint32_t lane = threadIdx.x & 31u;
     const GFront F = c->f[c->cur], O = c->f[c->cur ^ 1];
     const unsigned long long nactv = F.cnt[FC_NACTV], nacte = F.cnt[FC_NACTE];
     const int iter = c->iter;
     if (nactv == 0 || iter >= c->max_iters) {
+        if (lane != 0) return;
         c->variant = -1;
         c->iterations = iter;
         cudaGraphSetConditional(c->h_push, 0);
@@ -1239,7 +1253,47 @@ __device__ void decide_step(GCtl *c) {
         cudaGraphSetConditional(c->h_while, 0);
         return;
     }
-    const bool push = d_threshold_sparse(c->threshold, c->threshold_k, nactv, nacte, c->m);
+    bool push = d_threshold_sparse(c->threshold, c->threshold_k, nactv, nacte, c->m);
+    const unsigned long long unr_c = c->reached_v < c->n ? c->n - c->reached_v : 0ull;
+    const auto close = [](unsigned long long a, unsigned long long b) {
+        const unsigned long long d = a > b ? a - b : b - a, mx = a > b ? a : b;
+        return d * 16 <= mx;
+    };
+    if (c->sel_w && c->sel_valid && close(nactv, c->sel_nactv) && close(nacte, c->sel_nacte) &&
+        close(unr_c, c->sel_unr) && min(iter, 255) - c->sel_iter < 8) {
+        push = c->sel_push != 0;  // the last evaluation still applies
+    } else if (c->sel_w) {
+        // learned choice between the two variants this driver runs: the
+        // threshold's stands unless the network predicts a clear gain
+        const double n = c->n, m = (double)c->m, fv = (double)nactv, fe = (double)nacte;
+        const double unr = (double)unr_c;
+        float x[GG_SEL_FEATURES];
+        x[0] = (float)(log2(1.0 + fv) / 32);
+        x[1] = (float)(log2(1.0 + fe) / 40);
+        x[2] = (float)(log2(1.0 + unr) / 32);
+        x[3] = (float)(min(iter, 255) / 64.0);
+        x[4] = (float)(log2(1.0 + (n > 0 ? m / n : 0)) / 8);
+        x[5] = c->gini;
+        x[6] = (float)(n > 0 ? fv / n : 0);
+        x[7] = (float)(m > 0 ? fe / m : 0);
+        x[8] = (float)fmin(4.0, m > 0 ? (fv + fe) / m : 0.0);
+        x[9] = (float)(log2(n > 1 ? n : 1.0) / 32);
+        float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
+        mlp::warp_forward(c->sel_w, x, o, z1, a1, z2, a2);
+        const int tv = push ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+        const int best = o[GG_VAR_PUSH_SPARSE] < o[GG_VAR_PULL_DENSE] ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+        if (o[best] < o[tv] - mlp::kSelMargin) push = best == GG_VAR_PUSH_SPARSE;
+        __syncwarp();
+        if (lane == 0) {
+            c->sel_nactv = nactv;
+            c->sel_nacte = nacte;
+            c->sel_unr = unr_c;
+            c->sel_iter = min(iter, 255);
+            c->sel_push = push;
+            c->sel_valid = 1;
+        }
+    }
+    if (lane != 0) return;
     if (iter < GG_MAX_ITERS) {
         c->variants[iter] = push ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
         c->nactv[iter] = nactv;
@@ -1420,13 +1474,22 @@ __global__ void k_g_clear(GCtl *c) {
     for (uint64_t w = tid; w < words; w += nth) bm[w] = 0u;
 }
 
-// bookkeeping of the step that ran, then the next step's decision (one thread)
+__device__ void g_bookkeep(GCtl *c);
+
+// bookkeeping of the step that ran (thread 0), then the next step's decision (the warp)
 __global__ void k_g_next(GCtl *c) {
-    if (threadIdx.x != 0) return;
     if (c->variant < 0) {
-        cudaGraphSetConditional(c->h_while, 0);
+        if (threadIdx.x == 0) cudaGraphSetConditional(c->h_while, 0);
         return;
     }
+    if (threadIdx.x == 0) g_bookkeep(c);
+    __syncwarp();
+    decide_step(c);  // an empty frontier or the iteration bound ends the loop
+}
+
+// bookkeeping of the step that ran (one thread)
+__device__ void g_bookkeep(GCtl *c) {
+    {
     const int cur = c->cur;
     const GFront F = c->f[cur], O = c->f[cur ^ 1];
     const int iter = c->iter;
@@ -1443,7 +1506,7 @@ __global__ void k_g_next(GCtl *c) {
     c->cur = cur ^ 1;
     c->iter = iter + 1;
     if (iter + 1 <= GG_MAX_ITERS) c->t_ns[iter + 1] = g_now();
-    decide_step(c);  // an empty frontier or the iteration bound ends the loop
+    }
 }
 
 // Chunk prefix of a large bin of more than kLargeLocal rows (one CTA of
@@ -1495,6 +1558,8 @@ __global__ void __launch_bounds__(1024) k_g_chunks(GCtl *c) {
         c->use_first = 1;
     }
 }
+
+const void *selector_weights(gg_graph *g);
 
 struct GraphBfs {
     cudaGraph_t graph = nullptr;
@@ -1638,6 +1703,15 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     h.max_iters = (int)std::min<uint64_t>((uint64_t)g->n + 2, (uint64_t)INT_MAX / 2);
     h.threshold = opt.threshold;
     h.threshold_k = opt.threshold_k;
+    h.sel_w = nullptr;
+    if (opt.threshold == GG_THRESH_LEARNED && selector_weights(g)) {
+        if (g->gini < 0) {
+            float gi;
+            GG_CHECK(graph_gini(g, &gi));
+        }
+        h.sel_w = (const __nv_bfloat16 *)selector_weights(g);
+        h.gini = g->gini < 0 ? 0.0f : g->gini;
+    }
     h.smax = t.bin_small_max;
     h.mmax = t.bin_medium_max;
     h.large_ch = t.large_chunk;
@@ -1727,8 +1801,10 @@ gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop
     if (st) memset(st, 0, sizeof(*st));
     uint64_t k0 = g->ctx->launches;
     // one CUDA graph per run (device decisions) unless another driver is asked for
-    const bool graph_mode = !use_persistent(g, opt, 1) && (tuning().graph & 1) && opt.variant == GG_VAR_AUTO &&
-                            opt.threshold != GG_THRESH_LEARNED;
+    // (the learned selector runs inside the graph too, choosing between its
+    // push and pull; timing collection forces variants device-driven)
+    const bool graph_mode = (tuning().graph & 1) && !(tuning().persistent & 1) && g->force_iter < 0 &&
+                            opt.variant == GG_VAR_AUTO;
     if (graph_mode) {
         RunTimer tm(g->ctx);
         int iters = 0;
