@@ -1271,7 +1271,7 @@ __device__ void decide_step(GCtl *c) {
         x[0] = (float)(log2(1.0 + fv) / 32);
         x[1] = (float)(log2(1.0 + fe) / 40);
         x[2] = (float)(log2(1.0 + unr) / 32);
-        x[3] = (float)(min(iter, 255) / 64.0);
+        x[3] = (float)(log2(1.0 + min(iter, 255)) / 8);
         x[4] = (float)(log2(1.0 + (n > 0 ? m / n : 0)) / 8);
         x[5] = c->gini;
         x[6] = (float)(n > 0 ? fv / n : 0);

@@ -946,7 +946,7 @@ __device__ int choose_variant(const PArgs &P, int iter, unsigned long long nactv
                 x[0] = (float)(log2(1.0 + fv) / 32);
                 x[1] = (float)(log2(1.0 + fe) / 40);
                 x[2] = (float)(log2(1.0 + (double)unr) / 32);
-                x[3] = (float)(it / 64.0);
+                x[3] = (float)(log2(1.0 + it) / 8);
                 x[4] = (float)(log2(1.0 + (n > 0 ? m / n : 0)) / 8);
                 x[5] = P.gini;
                 x[6] = (float)(n > 0 ? fv / n : 0);

@@ -388,7 +388,7 @@ void selector_features(float *x, double nactv, double nacte, double unreached, i
     x[0] = (float)(std::log2(1.0 + nactv) / 32);
     x[1] = (float)(std::log2(1.0 + nacte) / 40);
     x[2] = (float)(std::log2(1.0 + std::max(0.0, unreached)) / 32);
-    x[3] = (float)(std::min(iter, 255) / 64.0);
+    x[3] = (float)(std::log2(1.0 + std::min(iter, 255)) / 8);
     x[4] = (float)(std::log2(1.0 + (n > 0 ? m / n : 0)) / 8);
     x[5] = gini;
     x[6] = (float)(n > 0 ? nactv / n : 0);
@@ -463,9 +463,22 @@ extern "C" gg_status gg_selector_collect(gg_graph *g, int analytic, uint32_t roo
     const int T = rs.iterations;
     // CC's first step starts from the all-true frontier and is always a pull
     const int first = (analytic == 1 && T > 1) ? 1 : 0;
-    const int k = std::min(max_samples, T - first);
-    for (int si = 0; si < k && *nrec < cap; ++si) {
-        const int it = first + (k == 1 ? 0 : (int)((long long)si * (T - 1 - first) / (k - 1)));
+    // sampled iterations: even positions spaced evenly over the run, odd ones
+    // geometrically (long runs spend many iterations on small frontiers
+    // early on, which even spacing would barely see); duplicates dropped
+    const int span = T - first;
+    const int k = std::min(max_samples, span);
+    std::vector<int> its;
+    for (int si = 0; si < k; ++si) {
+        int p = 0;
+        if (k > 1 && (si & 1)) p = (int)std::lround(std::pow((double)span, (double)si / (k - 1))) - 1;
+        else if (k > 1) p = (int)((long long)si * (span - 1) / (k - 1));
+        its.push_back(first + std::min(std::max(p, 0), span - 1));
+    }
+    std::sort(its.begin(), its.end());
+    its.erase(std::unique(its.begin(), its.end()), its.end());
+    for (size_t si = 0; si < its.size() && *nrec < cap; ++si) {
+        const int it = its[si];
         float *x = X + (size_t)*nrec * GG_SEL_FEATURES;
         float *y = Y + (size_t)*nrec * GG_SEL_VARIANTS;
         bool have_x = false;

@@ -19,10 +19,12 @@
  * W3[4][32], b3[4] (GG_SEL_NPARAMS floats).
  *
  * Features of an iteration (all computed on the device):
- *   0 log2(1+|F|)/32        1 log2(1+sum outdeg F)/40   2 log2(1+unreached)/32
- *   3 min(iter,255)/64      4 log2(1+m/n)/8             5 degree Gini of the graph
- *   6 |F|/n                 7 outdeg(F)/m               8 min((|F|+outdeg F)/m, 4)
+ *   0 log2(1+|F|)/32          1 log2(1+sum outdeg F)/40   2 log2(1+unreached)/32
+ *   3 log2(1+min(iter,255))/8 4 log2(1+m/n)/8             5 degree Gini of the graph
+ *   6 |F|/n                   7 outdeg(F)/m               8 min((|F|+outdeg F)/m, 4)
  *   9 log2(n)/32
+ * (the iteration enters by its logarithm: a linear count let the network
+ * fit bumps between the sampled iterations of long runs)
  */
 #ifndef GG_SELECT_H
 #define GG_SELECT_H
@@ -58,8 +60,9 @@ GG_API gg_status gg_selector_train(gg_selector *s, const float *X, const float *
  * or of the rest of the run from that iteration on (CC: a fused push step
  * finishes the run) in Y[k][4] (NaN where the forced run ended before that
  * iteration, which CC's racing push steps can cause).  Any iteration of the
- * run can be sampled.  At most `max_samples` iterations are sampled (spread
- * evenly); *nrec receives the record count (<= cap). */
+ * run can be sampled.  At most `max_samples` iterations are sampled,
+ * alternately spread evenly and geometrically over the run (duplicates
+ * dropped); *nrec receives the record count (<= cap). */
 GG_API gg_status gg_selector_collect(gg_graph *g, int analytic, uint32_t root, int max_samples,
                                      float *X, float *Y, int cap, int *nrec);
 
