@@ -603,23 +603,9 @@ __global__ void __launch_bounds__(256) k_bitmap_to_list(const uint32_t *bm, uint
     gg::dev::WarpAppender<256> ap0{sb[0][wib], 0, b0, cnt + FC_BIN0};
     gg::dev::WarpAppender<256> ap1{sb[1][wib], 0, b1, cnt + FC_BIN1};
     gg::dev::WarpAppender<256> ap2{sb[2][wib], 0, b2, cnt + FC_BIN2};
-    const uint32_t nwords = (n + 31) / 32;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
     const uint32_t lane = threadIdx.x & 31;
     unsigned long long nv = 0, ne = 0;
-    for (uint32_t w = warp; w < nwords; w += nw) {
-        const uint32_t word = bm ? bm[w] : 0xFFFFFFFFu;
-        if (word == 0) continue;  // warp-uniform
-        const uint32_t v = w * 32 + lane;
-        const bool act = v < n && ((word >> lane) & 1u);
-        const uint64_t deg = act ? off[v + 1] - off[v] : 0;
-        const uint32_t bin = deg <= smax ? 0 : (deg <= mmax ? 1 : 2);
-        if (act) { nv++; ne += deg; }
-        ap0.push(act && bin == 0, v);
-        ap1.push(act && bin == 1, v);
-        ap2.push(act && bin == 2, v);
-    }
+    gg::dev::bitmap_to_bins(bm, n, off, smax, mmax, ap0, ap1, ap2, nv, ne);
     ap0.flush();
     ap1.flush();
     ap2.flush();
@@ -783,6 +769,7 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "fusion_queue" && (v == 0 || v >= 32)) t.fusion_queue = (uint32_t)v;
     else if (k == "cc_hook" && v <= 1) t.cc_hook = (int)v;
     else if (k == "graph" && v <= 1) t.graph = (int)v;
+    else if (k == "graph_handoff" && v <= (1 << 20)) t.graph_handoff = (int)v;
     else if (k == "barrier_timeout_ns" && v >= 1) t.barrier_timeout_ns = (unsigned long long)v;
     else return GG_ERR_ARG;
     if (t.bin_small_max > t.bin_medium_max) {
@@ -810,6 +797,7 @@ gg_status gg_tuning_get(const char *name, int64_t *v) {
     else if (k == "fusion_queue") *v = t.fusion_queue;
     else if (k == "cc_hook") *v = t.cc_hook;
     else if (k == "graph") *v = t.graph;
+    else if (k == "graph_handoff") *v = t.graph_handoff;
     else if (k == "barrier_timeout_ns") *v = (int64_t)t.barrier_timeout_ns;
     else return GG_ERR_ARG;
     return GG_OK;

@@ -132,7 +132,9 @@ struct Op {
             old = atomicMin(a + d, sv);
             if (!(sv < old)) return false;
         }
-        if (record == GG_RECORD_NE_PREV) return old == prev[d];
+        // level-synchronous: d passed the filter, so it was unvisited and its
+        // prev equals the value this thread replaced (no prev load)
+        if (record == GG_RECORD_NE_PREV) return (R == GG_RELAX_MIN_PLUS1_I32 && level_sync) || old == prev[d];
         if (record == GG_RECORD_REDUCTION) {
             uint32_t bit = 1u << (d & 31);
             return (atomicOr(dedup + (d >> 5), bit) & bit) == 0;
@@ -455,7 +457,7 @@ __device__ __forceinline__ void push_binned_body(const EmapArgs &A, const Op<R> 
             push_edges<R, 32>(A, op, sv, beg, end, lane, emit);
         }
     } else {
-        // small bin: a thread per source vertex, warp-uniform edge loop
+        // small bin: a warp per 32 source vertices, their edges flattened
         const uint32_t wpb = BLOCK / 32;
         const uint32_t nws = (gridDim.x - nb_large - nb_med) * wpb;
         const uint32_t wid = (blockIdx.x - nb_large - nb_med) * wpb + (threadIdx.x >> 5);
@@ -473,16 +475,8 @@ __device__ __forceinline__ void push_binned_body(const EmapArgs &A, const Op<R> 
             }
             const uint32_t deg = (uint32_t)(end - beg);
             sc += deg;
-            const uint32_t maxd = __reduce_max_sync(FULL, deg);
-            for (uint32_t k = 0; k < maxd; ++k) {
-                bool rec = false;
-                uint32_t d = 0;
-                if (k < deg) {
-                    d = __ldg(A.adj + beg + k);
-                    rec = op.offer(d, sv, A.record, A.out_bits);
-                }
-                app.emit(A, rec, d);
-            }
+            dev::warp_flat_rows<4>(
+                A.adj, beg, deg, sv, [&](uint32_t d, V x) { return op.offer(d, x, A.record, A.out_bits); }, emit);
         }
     }
     app.flush();
@@ -1146,6 +1140,8 @@ struct GCtl {
     uint32_t root, n;
     uint64_t m;
     int threshold, threshold_k;
+    int handoff_iter;  // > 0: after this many iterations the run leaves the graph (handed_off = 1)
+    int handed_off;
     const __nv_bfloat16 *sel_w;  // learned selector weights (bfloat16), or null: the threshold decides
     float gini;
     // last network evaluation: reused while the frontier counts stay within 1/16
@@ -1221,6 +1217,7 @@ __global__ void k_g_init(GCtl *c) {
         c->cand_valid = 0;
         c->cand_cur = 0;
         c->sel_valid = 0;
+        c->handed_off = 0;
         c->reached_v = 0;
         c->reached_e = 0;
         c->variant = -1;
@@ -1241,8 +1238,11 @@ __device__ void decide_step(GCtl *c) {
     const GFront F = c->f[c->cur], O = c->f[c->cur ^ 1];
     const unsigned long long nactv = F.cnt[FC_NACTV], nacte = F.cnt[FC_NACTE];
     const int iter = c->iter;
-    if (nactv == 0 || iter >= c->max_iters) {
+    const bool handoff = c->handoff_iter > 0 && iter >= c->handoff_iter;
+    if (nactv == 0 || iter >= c->max_iters || handoff) {
         if (lane != 0) return;
+        // a long run of small steps continues in the device-driven traversal
+        c->handed_off = nactv != 0 && iter < c->max_iters;
         c->variant = -1;
         c->iterations = iter;
         cudaGraphSetConditional(c->h_push, 0);
@@ -1363,20 +1363,8 @@ __global__ void __launch_bounds__(256) k_g_tolist(GCtl *c) {
     dev::WarpAppender<256> ap0{sb[0][wib], 0, F.bins[0], F.cnt + FC_BIN0};
     dev::WarpAppender<256> ap1{sb[1][wib], 0, F.bins[1], F.cnt + FC_BIN1};
     dev::WarpAppender<256> ap2{sb[2][wib], 0, F.bins[2], F.cnt + FC_BIN2};
-    const uint32_t n = c->n, nwords = (n + 31) / 32;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31;
-    for (uint32_t w = warp; w < nwords; w += nw) {
-        const uint32_t word = F.bitmap[w];
-        if (word == 0) continue;  // warp-uniform
-        const uint32_t v = w * 32 + lane;
-        const bool act = v < n && ((word >> lane) & 1u);
-        const uint64_t deg = act ? c->off[v + 1] - c->off[v] : 0;
-        const uint32_t bin = deg <= c->smax ? 0 : (deg <= c->mmax ? 1 : 2);
-        ap0.push(act && bin == 0, v);
-        ap1.push(act && bin == 1, v);
-        ap2.push(act && bin == 2, v);
-    }
+    unsigned long long nv = 0, ne = 0;  // the counts are known already
+    dev::bitmap_to_bins(F.bitmap, c->n, c->off, c->smax, c->mmax, ap0, ap1, ap2, nv, ne);
     ap0.flush();
     ap1.flush();
     ap2.flush();
@@ -1703,6 +1691,7 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     h.max_iters = (int)std::min<uint64_t>((uint64_t)g->n + 2, (uint64_t)INT_MAX / 2);
     h.threshold = opt.threshold;
     h.threshold_k = opt.threshold_k;
+    h.handoff_iter = t.graph_handoff;
     h.sel_w = nullptr;
     if (opt.threshold == GG_THRESH_LEARNED && selector_weights(g)) {
         if (g->gini < 0) {
@@ -1741,14 +1730,12 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     h.cand_n = (unsigned long long *)cl.cnt;
     GG_CUDA(ctx, cudaMemcpyAsync(gb->ctl, &h, offsetof(GCtl, reached_v), cudaMemcpyHostToDevice, ctx->stream));
     GG_CUDA(ctx, cudaGraphLaunch(gb->exec, ctx->stream));
-    // records back (one wait per run)
-    const size_t rec0 = offsetof(GCtl, reached_v), rec1 = offsetof(GCtl, h_while);
+    // state and records back (one wait per run)
+    const size_t rec0 = offsetof(GCtl, variant), rec1 = offsetof(GCtl, h_while);
     GCtl *hr = (GCtl *)std::malloc(sizeof(GCtl));
     if (!hr) return GG_ERR_OOM;
-    cudaError_t e = cudaMemcpyAsync((char *)hr + offsetof(GCtl, iterations), (char *)gb->ctl + offsetof(GCtl, iterations),
-                                    sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync((char *)hr + rec0, (char *)gb->ctl + rec0, rec1 - rec0,
-                                              cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e = cudaMemcpyAsync((char *)hr + rec0, (char *)gb->ctl + rec0, rec1 - rec0, cudaMemcpyDeviceToHost,
+                                    ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
         std::free(hr);
@@ -1759,9 +1746,38 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     // kernels the graph ran: init, then per iteration the step kernel, clear
     // and next (plus a list or bitmap conversion where the variant changes)
     ctx->launches += 1 + 3 * (uint64_t)T;
-    if (st) {
+    if (hr->handed_off) {
+        // the rest of the run as one device-driven launch from the current
+        // frontier (a push leaves it as a list only: add its bitmap)
+        const int cur = hr->cur;
+        gg_frontier *f = g->tmp_front[cur];
+        gg_status s = GG_OK;
+        if (!hr->has_bitmap[cur]) {
+            f->has_list = true;
+            f->has_bitmap = f->all = f->host_valid = false;
+            s = frontier_ensure_bitmap(f);
+        }
+        gg_emap_desc desc;
+        memset(&desc, 0, sizeof(desc));
+        desc.relax = GG_RELAX_MIN_PLUS1_I32;
+        desc.a = level;
+        desc.dst_filter = GG_FILTER_GT_CONST;
+        desc.src_level_sync = 1;
+        desc.record = GG_RECORD_NE_PREV;
+        desc.prev = prev;
+        const PersistResume rs{T, cur, hr->has_list[cur], hr->reached_v, hr->reached_e};
+        int iters = 0;
+        if (s == GG_OK) s = persistent_traverse(g, desc, 1, false, root, opt, st, &iters, -1, -1, nullptr, 0, &rs);
+        if (s != GG_OK) {
+            std::free(hr);
+            return s;
+        }
+        *iters_out = iters;
+    } else if (st) {
         st->vertices_reached = hr->reached_v;
         st->edges_reached = hr->reached_e;
+    }
+    if (st) {
         for (int i = 0; i < std::min(T, GG_MAX_ITERS); ++i) {
             st->variant[i] = hr->variants[i];
             st->nactv[i] = hr->nactv[i];

@@ -177,10 +177,21 @@ gg_status frontier_ensure_list(gg_frontier *f);      // from bitmap / all
 gg_status frontier_reset_counts(gg_frontier *f);     // async zero of d_cnt
 uint32_t bin_of_degree(uint64_t deg);
 gg_status build_heavy_rows(gg_graph *g);
+// A BFS-levels run handed over to the device-driven traversal part way:
+// iter0 iterations done, the frontier in the graph's scratch frontier `cur`
+// (its bitmap always set, its binned list when has_list), the other scratch
+// frontier empty, reached_v / reached_e the counts so far.
+struct PersistResume {
+    int iter0;
+    int cur;
+    int has_list;
+    unsigned long long reached_v, reached_e;
+};
 gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, bool start_all, uint32_t root,
                               const gg_run_opts &opt, gg_run_stats *stats, int *iters_out,
                               int force_iter = -1, int force_variant = -1,
-                              const uint32_t *d_roots = nullptr, uint32_t nroots = 0);
+                              const uint32_t *d_roots = nullptr, uint32_t nroots = 0,
+                              const PersistResume *resume = nullptr);
 gg_status graph_adopt_device_csr(gg_ctx *ctx, uint32_t n, uint64_t m, uint64_t *off, uint32_t *adj, int symmetric,
                                  gg_graph **out);
 gg_status graph_gini(gg_graph *g, float *out);
@@ -209,6 +220,11 @@ struct Tuning {
     // iteration's push/pull decision on the device (host-driven kernels, no
     // per-iteration host round trip): bit 0 BFS levels
     int graph = 1;
+    // graph-driven BFS levels: a run still going after this many iterations
+    // (a high-diameter graph: many small frontiers, where the graph's
+    // per-step node launches cost more than a grid barrier) continues in the
+    // device-driven traversal; 0 = never
+    int graph_handoff = 32;
     // sparse push steps run fused (asynchronous multi-hop, as CCv with
     // api::fusion) in device-driven runs: bit 2 CC.  Off by default: on
     // B200 the shared work queue (three contended counters per vertex, and
@@ -314,6 +330,104 @@ struct WarpAppender {
         n = 0;
     }
 };
+
+// Frontier bitmap -> degree-binned vertex lists, one warp per group of 32
+// bitmap words.  Each lane loads one word (a coalesced 128-byte read), the
+// warp then walks the non-zero words four at a time: the degree loads of the
+// four words are issued before any append, so a warp keeps four offset
+// reads in flight instead of one.  bm == nullptr stands for all vertices.
+// nv / ne accumulate, per lane, the vertices and out-edges appended.  CG:
+// the bitmap was written earlier in the same kernel (read through L2).
+template <int CAP, bool CG = false>
+__device__ __forceinline__ void bitmap_to_bins(const uint32_t *bm, uint32_t n, const uint64_t *off, uint32_t smax,
+                                               uint32_t mmax, WarpAppender<CAP> &ap0, WarpAppender<CAP> &ap1,
+                                               WarpAppender<CAP> &ap2, unsigned long long &nv,
+                                               unsigned long long &ne) {
+    const uint32_t nwords = (n + 31) / 32;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+    for (uint64_t base = (uint64_t)warp * 32; base < nwords; base += (uint64_t)nw * 32) {
+        const uint64_t w = base + lane;
+        const uint32_t mine = w < nwords ? (bm ? (CG ? __ldcg(bm + w) : bm[w]) : 0xFFFFFFFFu) : 0u;
+        unsigned nz = __ballot_sync(0xffffffffu, mine != 0);
+        while (nz) {  // warp-uniform
+            uint32_t vv[4];
+            uint64_t dd[4];
+            bool aa[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int j = nz ? __ffs(nz) - 1 : -1;
+                if (j >= 0) nz &= nz - 1;
+                const uint32_t word = __shfl_sync(0xffffffffu, mine, j >= 0 ? j : 0);
+                vv[k] = (uint32_t)((base + (uint32_t)max(j, 0)) * 32 + lane);
+                aa[k] = j >= 0 && vv[k] < n && ((word >> lane) & 1u);
+                dd[k] = aa[k] ? off[vv[k] + 1] - off[vv[k]] : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const uint32_t bin = dd[k] <= smax ? 0 : (dd[k] <= mmax ? 1 : 2);
+                if (aa[k]) {
+                    nv++;
+                    ne += dd[k];
+                }
+                ap0.push(aa[k] && bin == 0, vv[k]);
+                ap1.push(aa[k] && bin == 1, vv[k]);
+                ap2.push(aa[k] && bin == 2, vv[k]);
+            }
+        }
+    }
+}
+
+// Push over the small rows held by a warp, one row per lane (beg, deg and
+// the offered value sv; deg = 0 for a lane without a row).  The 32 rows'
+// edges are walked as one flattened list: lane l takes edges l, l+32, ...,
+// U of them in flight, each mapped to its row by a binary search over the
+// lanes' exclusive degree prefix.  Work is balanced whatever the degree mix
+// (a lane-per-row walk waits for the warp's longest row, one dependent
+// round trip per edge).  offer(d, sv) -> recorded; emit(rec, d) is called
+// by all 32 lanes together.
+template <int U, typename V, typename Offer, typename Emit>
+__device__ __forceinline__ void warp_flat_rows(const uint32_t *adj, uint64_t beg, uint32_t deg, V sv,
+                                               Offer &&offer, Emit &&emit) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t incl = deg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t excl = incl - deg;
+    for (uint32_t e0 = 0; e0 < total; e0 += 32u * U) {  // warp-uniform
+        uint32_t d[U];
+        V x[U];
+        bool ok[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t idx = e0 + (uint32_t)u * 32u + lane;
+            uint32_t r = 0;  // the last lane whose prefix is <= idx
+#pragma unroll
+            for (uint32_t step = 16; step; step >>= 1) {
+                const uint32_t pr = __shfl_sync(0xffffffffu, excl, r + step);
+                if (pr <= idx) r += step;
+            }
+            const uint64_t b = __shfl_sync(0xffffffffu, beg, r);
+            const uint32_t ex = __shfl_sync(0xffffffffu, excl, r);
+            x[u] = __shfl_sync(0xffffffffu, sv, r);
+            ok[u] = idx < total;
+            d[u] = ok[u] ? __ldg(adj + b + (idx - ex)) : 0u;
+        }
+        bool rec[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) rec[u] = ok[u] && offer(d[u], x[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (e0 + (uint32_t)u * 32u >= total) break;  // warp-uniform
+            emit(rec[u], d[u]);
+        }
+    }
+}
 
 // Block-wide sum of a per-thread value; result valid in thread 0.
 template <typename T, int BLOCK>

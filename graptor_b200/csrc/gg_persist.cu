@@ -95,6 +95,7 @@ struct PArgs {
     int hook;                          // CC: road-network test after step 0, then hooking
     uint32_t *wq;                      // fused push work queue, wq_cap entries, all kWqEmpty between phases
     unsigned long long wq_cap;
+    int iter0;                         // iterations done before this launch (a resumed run)
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -181,6 +182,9 @@ template <int R> struct POp {
             old = atomicMin(a + d, sv);
             if (!(sv < old)) return false;
         }
+        // level-synchronous: d passed the filter, so it was unvisited and its
+        // prev equals the value this thread replaced (no prev load)
+        if (R == GG_RELAX_MIN_PLUS1_I32 && level_sync) return true;
         return record == GG_RECORD_NE_PREV ? old == ldcg(prev + d) : true;
     }
 };
@@ -313,7 +317,7 @@ __device__ void phase_push(const PArgs &P, const POp<R> &op, const PFront &F, co
         if (lane == 0) sc += end - beg;
         p_push_edges<R, 32>(P, op, O, sv, beg, end, lane, nv, ne);
     }
-    // small bin: a thread per row, warp-uniform edge loop
+    // small bin: a warp per 32 rows, their edges flattened
     for (uint64_t base = gw * 32; base < c0; base += nw * 32) {
         const uint64_t i = base + lane;
         const bool have = i < c0;
@@ -328,16 +332,9 @@ __device__ void phase_push(const PArgs &P, const POp<R> &op, const PFront &F, co
         }
         const uint32_t deg = (uint32_t)(end - beg);
         sc += deg;
-        const uint32_t maxd = __reduce_max_sync(FULLP, deg);
-        for (uint32_t k = 0; k < maxd; ++k) {
-            bool rec = false;
-            uint32_t d = 0;
-            if (k < deg) {
-                d = __ldg(P.adj + beg + k);
-                rec = op.offer(d, sv, P.record);
-            }
-            p_emit(P, O, rec, d, nv, ne);
-        }
+        dev::warp_flat_rows<4>(
+            P.adj, beg, deg, sv, [&](uint32_t d, V x) { return op.offer(d, x, P.record); },
+            [&](bool rec, uint32_t d) { p_emit(P, O, rec, d, nv, ne); });
     }
     p_flush(O, nv, ne, sc);
 }
@@ -708,24 +705,13 @@ __device__ void phase_pull(const PArgs &P, const POp<R> &op, const PFront &F, co
 
 // F's bitmap -> F's binned list (only before a push that follows a pull)
 __device__ void phase_bitmap_to_list(const PArgs &P, const PFront &F, uint32_t *smem) {
-    const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t wib = threadIdx.x >> 5;
     constexpr int per = (kPB / 32) * 256;
     dev::WarpAppender<256> ap0{smem + 0 * per + wib * 256, 0, F.bins[0], F.cnt + FC_BIN0};
     dev::WarpAppender<256> ap1{smem + 1 * per + wib * 256, 0, F.bins[1], F.cnt + FC_BIN1};
     dev::WarpAppender<256> ap2{smem + 2 * per + wib * 256, 0, F.bins[2], F.cnt + FC_BIN2};
-    const uint32_t nwords = (P.n + 31) / 32;
-    const uint64_t nw = ((uint64_t)gridDim.x * kPB) >> 5;
-    for (uint64_t w = ((uint64_t)blockIdx.x * kPB + threadIdx.x) >> 5; w < nwords; w += nw) {
-        const uint32_t word = ldcg(F.bitmap + w);
-        if (word == 0) continue;
-        const uint32_t v = (uint32_t)w * 32 + lane;
-        const bool act = v < P.n && ((word >> lane) & 1u);
-        const uint64_t deg = act ? P.off[v + 1] - P.off[v] : 0;
-        const uint32_t bin = deg <= P.smax ? 0 : (deg <= P.mmax ? 1 : 2);
-        ap0.push(act && bin == 0, v);
-        ap1.push(act && bin == 1, v);
-        ap2.push(act && bin == 2, v);
-    }
+    unsigned long long nv = 0, ne = 0;  // the counts are known already
+    dev::bitmap_to_bins<256, true>(F.bitmap, P.n, P.off, P.smax, P.mmax, ap0, ap1, ap2, nv, ne);
     ap0.flush();
     ap1.flush();
     ap2.flush();
@@ -998,10 +984,11 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
     const uint64_t tid = (uint64_t)blockIdx.x * kPB + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * kPB;
     int cur = 0;
-    int iter = 0;
+    int iter = P.iter0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        st->t_ns[0] = globaltimer();
-        if (P.force_iter == 0) st->f_t0 = st->t_ns[0];
+        const unsigned long long t0 = globaltimer();
+        if (iter <= GG_MAX_ITERS) st->t_ns[iter] = t0;
+        if (P.force_iter == iter) st->f_t0 = t0;
     }
     for (; iter < P.max_iters; ++iter) {
         const PFront F = P.fr[cur], O = P.fr[cur ^ 1];
@@ -1169,7 +1156,8 @@ const void *selector_weights(gg_graph *g);
 
 gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, bool start_all, uint32_t root,
                               const gg_run_opts &opt, gg_run_stats *stats, int *iters_out, int force_iter,
-                              int force_variant, const uint32_t *d_roots, uint32_t nroots) {
+                              int force_variant, const uint32_t *d_roots, uint32_t nroots,
+                              const PersistResume *resume) {
     gg_ctx *ctx = g->ctx;
     cudaStream_t s = ctx->stream;
     const Tuning &t = tuning();
@@ -1197,15 +1185,19 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
     P.n = g->n;
     P.m = g->m;
     for (int i = 0; i < 2; ++i) {
-        gg_frontier *f = g->tmp_front[i];
+        // a resumed run starts from the scratch frontier it was left in
+        gg_frontier *f = g->tmp_front[resume ? (i ^ resume->cur) : i];
         for (int b = 0; b < NBINS; ++b) P.fr[i].bins[b] = f->bins[b];
         P.fr[i].bitmap = f->bitmap;
         P.fr[i].cnt = (unsigned long long *)f->d_cnt;
-        GG_CUDA(ctx, cudaMemsetAsync(f->bitmap, 0, words * 4, s));
-        GG_CUDA(ctx, cudaMemsetAsync(f->d_cnt, 0, FC_WORDS * 8, s));
+        if (!resume) {
+            GG_CUDA(ctx, cudaMemsetAsync(f->bitmap, 0, words * 4, s));
+            GG_CUDA(ctx, cudaMemsetAsync(f->d_cnt, 0, FC_WORDS * 8, s));
+        }
         f->host_valid = false;
         f->has_list = f->has_bitmap = f->all = false;
     }
+    P.iter0 = resume ? resume->iter0 : 0;
     P.cand[0] = c.list[0];
     P.cand[1] = c.list[1];
     P.nonisolated = g->nonisolated;
@@ -1256,7 +1248,12 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
         P.gini = gi;
     }
     GG_CUDA(ctx, cudaMemsetAsync(st, 0, sizeof(PState), s));
-    if (start_all) {
+    if (resume) {
+        const int hl = resume->has_list ? 1 : 0;
+        const unsigned long long rc[2] = {resume->reached_v, resume->reached_e};
+        GG_CUDA(ctx, cudaMemcpyAsync(&st->has_list[0], &hl, sizeof(int), cudaMemcpyHostToDevice, s));
+        GG_CUDA(ctx, cudaMemcpyAsync(&st->reached_v, rc, sizeof(rc), cudaMemcpyHostToDevice, s));
+    } else if (start_all) {
         int one = 1;
         GG_CUDA(ctx, cudaMemcpyAsync(&st->all[0], &one, sizeof(int), cudaMemcpyHostToDevice, s));
         // counts of the all-true frontier: n vertices, m edges

@@ -234,7 +234,11 @@ typedef struct gg_emap_desc {
                                holds a[s] == k-1 (level-synchronous BFS), so the
                                relax offers k without loading a[s]; a push then
                                leaves prev of the vertices it records as it was
-                               (only unvisited vertices' prev is ever compared) */
+                               (only unvisited vertices' prev is ever compared),
+                               and every vertex passing the filter holds the same
+                               value in a and prev (BFSLVLv.C:117-129 sets both
+                               to n+1), so a push records the first writer of
+                               each such vertex without loading prev */
 } gg_emap_desc;
 
 typedef struct gg_emap_stats {

@@ -17,7 +17,10 @@
  * one device-driven cooperative launch; otherwise one launch per iteration
  * from the host), graph (1, the default: BFS levels run as one CUDA graph
  * whose conditional nodes take each step's push/pull decision on the
- * device; 0: one host round trip per iteration), cc_hook (1: a
+ * device; 0: one host round trip per iteration), graph_handoff (32, the
+ * default: a graph-driven BFS still running after that many iterations
+ * continues as one device-driven cooperative launch from its current
+ * frontier; 0: never), cc_hook (1: a
  * device-driven CC run of a symmetric graph
  * that passes CCv's road-network test after its first step finishes by
  * min-id hooking; 0: label propagation throughout), fusion (4: the sparse

@@ -186,6 +186,44 @@ def test_graph_driven_bfs_equals_host_loop(ctx, fusion_knobs, gen):
     g.close()
 
 
+@pytest.mark.parametrize("gen", ["rmat", "er_directed", "grid"])
+def test_graph_bfs_handoff_to_device_driven(ctx, fusion_knobs, gen):
+    """A graph-driven BFS handed over to the device-driven traversal after
+    k iterations (after a push: a list-only frontier; after a pull: a
+    bitmap-only one) gives the oracle's levels and the host loop's
+    iteration count, per-iteration frontier sizes and reached edges."""
+    old = {k: gg.tuning_get(k) for k in ("graph", "graph_handoff", "persistent")}
+    if gen == "rmat":
+        og, sym = O.rmat(15, 16 << 15, seed=65), True
+    elif gen == "er_directed":
+        og, sym = O.er(30000, 6.0, seed=4, dangling_bp=200, symmetric=False), False
+    else:
+        og, sym = O.grid(70, 40, seed=8, del_bp=300), True
+    g = ctx.upload(og.off, og.adj, symmetric=sym)
+    r = int(np.argmax(og.outdeg()))
+    ref = O.bfs_level(og, r)
+    try:
+        gg.tuning_set("persistent", 0)
+        gg.tuning_set("graph", 0)
+        s0 = gg.RunStats()
+        assert np.array_equal(g.bfs_level(r, opts=gg.default_opts(collect=True), stats=s0), ref)
+        k0 = min(s0.iterations, gg.MAX_ITERS)
+        gg.tuning_set("graph", 1)
+        for h in (1, 2, 3, 4, 7, 0):
+            gg.tuning_set("graph_handoff", h)
+            st = gg.RunStats()
+            lv = g.bfs_level(r, opts=gg.default_opts(collect=True), stats=st)
+            assert np.array_equal(lv, ref), (gen, h)
+            assert st.iterations == s0.iterations, (gen, h)
+            assert [st.nactv[i] for i in range(k0)] == [s0.nactv[i] for i in range(k0)], (gen, h)
+            assert [st.variant[i] for i in range(k0)] == [s0.variant[i] for i in range(k0)], (gen, h)
+            assert st.edges_reached == s0.edges_reached and st.vertices_reached == s0.vertices_reached
+    finally:
+        for k, v in old.items():
+            gg.tuning_set(k, v)
+    g.close()
+
+
 def test_cc_hooking_repeated_long_chains(ctx, fusion_knobs):
     """Hooking's final pass writes every label once; repeated runs on long
     chains (deep trees) must always give the canonical labels."""
