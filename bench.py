@@ -203,6 +203,12 @@ def pick_roots(deg: np.ndarray) -> np.ndarray:
     return rng.choice(nz, size=NROOTS, replace=False).astype(np.uint32)
 
 
+# DRAM bytes (read + write) per dense-pull launch, from one ncu capture of
+# k_pull (4 launches of R-MAT scale 23 BFS, 316 MB each on average) scaled
+# by the vertex count to scale 24: profiles/k_pull_rmat23_dram_traffic.md
+K_PULL_TRAFFIC_PER_LAUNCH = 632.5e6
+
+
 def bfs_bytes(n: int, st, it: int) -> float:
     """Algorithmic bytes of BFS iteration `it` (per-unit figures: 8-byte
     offsets, 4-byte ids and levels).  Sparse push: 4F + 16F + 4E + 4E + 4N.
@@ -723,7 +729,10 @@ def run_ours(args, ws, rank, local):
                        "graph_build_s": round(gen_s, 2)},
             "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": round(achieved, 1),
                          "peak": hbm_peak, "unit": "GB/s", "frac": round(achieved / hbm_peak, 4),
-                         "traffic": None, "peak_kind": peak_kind, "launches": nlaunch,
+                         "traffic": (K_PULL_TRAFFIC_PER_LAUNCH * n / (1 << 24)
+                                     if kernel_names[dom] == "k_pull" else None),
+                         "traffic_source": "ncu dram__bytes_read+write of k_pull, scale-23 capture scaled by n",
+                         "peak_kind": peak_kind, "launches": nlaunch,
                          "bytes_per_launch": round(kbytes[dom] / max(nlaunch, 1)),
                          "ms_per_launch": round(ktime[dom] / max(nlaunch, 1), 4)},
             "clocks": clocks, "gpu_launches": launches,
