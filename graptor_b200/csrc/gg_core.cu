@@ -770,6 +770,8 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "cc_hook" && v <= 1) t.cc_hook = (int)v;
     else if (k == "graph" && v <= 1) t.graph = (int)v;
     else if (k == "graph_handoff" && v <= (1 << 20)) t.graph_handoff = (int)v;
+    else if (k == "handoff_ctas" && v <= (1 << 16)) t.handoff_ctas = (int)v;
+    else if (k == "small_frontier" && v <= 1) t.small_frontier = (int)v;
     else if (k == "barrier_timeout_ns" && v >= 1) t.barrier_timeout_ns = (unsigned long long)v;
     else return GG_ERR_ARG;
     if (t.bin_small_max > t.bin_medium_max) {
@@ -798,6 +800,8 @@ gg_status gg_tuning_get(const char *name, int64_t *v) {
     else if (k == "cc_hook") *v = t.cc_hook;
     else if (k == "graph") *v = t.graph;
     else if (k == "graph_handoff") *v = t.graph_handoff;
+    else if (k == "handoff_ctas") *v = t.handoff_ctas;
+    else if (k == "small_frontier") *v = t.small_frontier;
     else if (k == "barrier_timeout_ns") *v = (int64_t)t.barrier_timeout_ns;
     else return GG_ERR_ARG;
     return GG_OK;

@@ -225,6 +225,14 @@ struct Tuning {
     // per-step node launches cost more than a grid barrier) continues in the
     // device-driven traversal; 0 = never
     int graph_handoff = 32;
+    // CTAs of the device-driven launch that continues a handed-over run
+    // (0 = all that fit; at most that many): its frontiers are small, and
+    // fewer CTAs make each grid barrier cheaper
+    int handoff_ctas = 148;
+    // device-driven BFS levels: small frontiers (at most 8192 vertices and
+    // 65536 edges) run in one thread-block cluster with the frontier in
+    // shared memory
+    int small_frontier = 1;
     // sparse push steps run fused (asynchronous multi-hop, as CCv with
     // api::fusion) in device-driven runs: bit 2 CC.  Off by default: on
     // B200 the shared work queue (three contended counters per vertex, and

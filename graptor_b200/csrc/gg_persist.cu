@@ -29,11 +29,17 @@
 #include "gg_internal.cuh"
 #include "gg_mlp.cuh"
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 namespace gg {
 
 constexpr unsigned FULLP = 0xffffffffu;
 constexpr int kPB = 256;           // threads per CTA
 constexpr uint32_t kLargeScan = 1024;  // large-bin rows chunked when at most this many
+// BFS levels: a listed frontier of at most this many vertices and edges
+// continues in the one-cluster kernel k_small_bfs
+constexpr unsigned long long kSmallEnterV = 8192, kSmallEnterE = 65536;
 
 struct PFront {
     uint32_t *bins[NBINS];
@@ -67,6 +73,10 @@ struct PState {
     // contend for one L2 line
     struct alignas(128) Line { unsigned long long v; };
     Line wq_head, wq_tail, wq_done;
+    // small-frontier hand-over (BFS levels): the traversal left the frontier
+    // at small_cur after small_iter iterations for k_small_bfs (exit_small),
+    // which either finishes the run (small_done) or hands back the same way
+    int exit_small, small_done, small_iter, small_cur;
 };
 
 struct PArgs {
@@ -96,6 +106,9 @@ struct PArgs {
     uint32_t *wq;                      // fused push work queue, wq_cap entries, all kWqEmpty between phases
     unsigned long long wq_cap;
     int iter0;                         // iterations done before this launch (a resumed run)
+    int cur0;                          // index in fr[] of the frontier it starts from
+    int small_ok;                      // BFS levels: small frontiers go to k_small_bfs
+    int small_from;                    // ... from this iteration on
 };
 
 __device__ __forceinline__ unsigned long long globaltimer() {
@@ -983,7 +996,7 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
     op.level_sync = P.level_sync;
     const uint64_t tid = (uint64_t)blockIdx.x * kPB + threadIdx.x;
     const uint64_t nthreads = (uint64_t)gridDim.x * kPB;
-    int cur = 0;
+    int cur = P.cur0;
     int iter = P.iter0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const unsigned long long t0 = globaltimer();
@@ -997,6 +1010,19 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
         if (nactv == 0 && !f_all) break;
         if (P.level_k) op.fk = iter + 1;
         const int var = choose_variant(P, iter, nactv, nacte, f_all != 0, st, &s_choice, &s_sel);
+        // a small listed frontier to push: the run continues in one CTA
+        // cluster (k_small_bfs); every CTA reads the same counts, so all
+        // leave together
+        if (P.small_ok && var == GG_VAR_PUSH_SPARSE && iter >= P.small_from && !f_all && nactv <= kSmallEnterV &&
+            nacte <= kSmallEnterE && ldcg(&st->has_list[cur])) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                st->exit_small = 1;
+                st->small_iter = iter;
+                st->small_cur = cur;
+                st->iterations = iter;
+            }
+            return;
+        }
         const bool pushes = var != GG_VAR_PULL_DENSE;
         if (blockIdx.x == 0 && threadIdx.x == 0 && iter == P.force_iter) {
             st->f_nactv = nactv;
@@ -1148,6 +1174,294 @@ __global__ void k_traverse_init_list(PFront F, const uint32_t *roots, uint32_t k
     }
 }
 
+// ---- small frontiers: one thread-block cluster, the frontier in shared memory --
+// A BFS-levels run whose frontier is small (a high-diameter graph: thousands
+// of levels of a few thousand vertices) pays, per level of the cooperative
+// kernel, two grid barriers and a dozen dependent global round trips.  Here
+// one cluster of kSmallCtas CTAs (1024 threads each, on kSmallCtas SMs) runs
+// those levels with the cluster barrier: each CTA keeps the frontier
+// vertices it discovered (vertex, first edge, degree) in its own shared
+// memory and expands them in the next level, each warp walking its 32 rows'
+// edges as one flattened list; the level's totals are read from the other
+// CTAs' shared memory (distributed shared memory) after the barrier, so
+// every CTA takes the same decisions.  A level costs the adjacency load, the
+// level test and atomicMin, and the new vertex's offsets.  The run leaves
+// the cluster when the frontier outgrows a CTA's queue, kSmallExitE edges or
+// the threshold's push choice (it is then written back as the binned list +
+// bitmap the cooperative kernel expects) or when it empties.
+constexpr int kSB = 1024;
+constexpr int kSmallCtas = 8;
+constexpr uint32_t kSmallCap = 4096;  // queue entries per CTA
+constexpr unsigned long long kSmallExitE = 262144;
+constexpr size_t kSmallSmem = (size_t)2 * kSmallCap * (8 + 4 + 4);
+
+struct SmallArgs {
+    const uint64_t *off;
+    const uint32_t *adj;
+    int32_t *level;
+    PFront fr[2];
+    PState *st;
+    int max_iters;
+    uint32_t smax, mmax;
+    uint64_t m;
+    int threshold, threshold_k;
+};
+
+// The threshold's push/pull choice (choose_variant's formulas; the learned
+// policy falls back to the default threshold here: it only ever overrides
+// it with a predicted gain, and a frontier this small is pushed).
+__device__ __forceinline__ bool small_pushes(const SmallArgs &S, unsigned long long v, unsigned long long e) {
+    switch (S.threshold) {
+    case GG_THRESH_ALWAYS_SPARSE: return true;
+    case GG_THRESH_ALWAYS_DENSE: return false;
+    case GG_THRESH_FRAC: return (float)(v + e) <= (float)S.m / (float)(100.0 / (float)S.threshold_k);
+    default: return (v + e) <= S.m / 20;
+    }
+}
+
+// Global frontier O: append v (out-degree dg) to its degree bin and bitmap.
+__device__ __forceinline__ void small_to_global(const SmallArgs &S, const PFront &O, uint32_t v, uint32_t dg) {
+    const uint32_t bin = dg <= S.smax ? 0u : (dg <= S.mmax ? 1u : 2u);
+    const unsigned long long pos = atomicAdd(O.cnt + FC_BIN0 + bin, 1ull);
+    O.bins[bin][pos] = v;
+    atomicOr(O.bitmap + (v >> 5), 1u << (v & 31));
+}
+
+// Appends the warp's recorded vertices to this CTA's queue (count *qn,
+// out-degree sum *qe); entries beyond kSmallCap go to the global frontier O.
+__device__ __forceinline__ void small_append(const SmallArgs &S, const PFront &O, bool rec, uint32_t d,
+                                             uint64_t b, uint32_t dg, uint32_t *qv, uint64_t *qb, uint32_t *qd,
+                                             unsigned *qn, unsigned long long *qe, int *over) {
+    if (!rec) dg = 0;
+    const unsigned mk = __ballot_sync(0xffffffffu, rec);
+    if (mk == 0) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int leader = __ffs(mk) - 1;
+    const unsigned long long esum = dev::warp_sum((unsigned long long)dg);
+    unsigned base = 0;
+    if ((int)lane == leader) {
+        base = atomicAdd(qn, (unsigned)__popc(mk));
+        atomicAdd(qe, esum);
+    }
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!rec) return;
+    const unsigned slot = base + __popc(mk & ((1u << lane) - 1u));
+    if (slot < kSmallCap) {
+        qv[slot] = d;
+        qb[slot] = b;
+        qd[slot] = dg;
+    } else {
+        small_to_global(S, O, d, dg);
+        *over = 1;
+    }
+}
+
+__global__ void __cluster_dims__(kSmallCtas, 1, 1) __launch_bounds__(kSB, 1) k_small_bfs(SmallArgs S) {
+    extern __shared__ __align__(16) unsigned char small_smem[];
+    // queue k (0 / 1): first edges, vertices, degrees
+    auto qb = [&](int k) { return (uint64_t *)small_smem + (size_t)k * kSmallCap; };
+    auto qv = [&](int k) { return (uint32_t *)(small_smem + 16 * (size_t)kSmallCap) + (size_t)k * kSmallCap; };
+    auto qd = [&](int k) { return (uint32_t *)(small_smem + 24 * (size_t)kSmallCap) + (size_t)k * kSmallCap; };
+    __shared__ unsigned s_n[2];
+    __shared__ unsigned long long s_e[2];
+    __shared__ int s_over[2];
+    __shared__ unsigned s_bin[NBINS], s_pos[NBINS];
+    __shared__ unsigned long long s_base[NBINS];
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    PState *st = S.st;
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5;
+    auto fr = [&](int k) { return k ? S.fr[1] : S.fr[0]; };  // no dynamic index into the parameters
+    int cur = st->small_cur;
+    int iter = st->small_iter;
+    if (tid == 0) {
+        s_n[0] = s_n[1] = 0;
+        s_e[0] = s_e[1] = 0;
+        s_over[0] = s_over[1] = 0;
+    }
+    __syncthreads();
+    // the frontier left by the cooperative kernel, dealt round-robin to the
+    // CTAs; its bitmap words and counters are cleared (it becomes an output)
+    {
+        const PFront F = fr(cur);
+        const unsigned long long c0 = F.cnt[FC_BIN0], c1 = F.cnt[FC_BIN1], c2 = F.cnt[FC_BIN2];
+        const unsigned total = (unsigned)(c0 + c1 + c2);  // <= kSmallEnterV <= kSmallCtas * kSmallCap
+        for (unsigned i = rank + kSmallCtas * tid; i < total; i += kSmallCtas * kSB) {
+            const uint32_t v = i < c0 ? F.bins[0][i] : (i < c0 + c1 ? F.bins[1][i - c0] : F.bins[2][i - c0 - c1]);
+            const uint64_t b = S.off[v];
+            const uint32_t dg = (uint32_t)(S.off[v + 1] - b);
+            const unsigned slot = atomicAdd(&s_n[0], 1u);
+            atomicAdd(&s_e[0], (unsigned long long)dg);
+            qv(0)[slot] = v;
+            qb(0)[slot] = b;
+            qd(0)[slot] = dg;
+            F.bitmap[v >> 5] = 0u;  // every set bit of this bitmap is a frontier vertex
+        }
+        cl.sync();
+        if (rank == 0 && tid < FC_WORDS) F.cnt[tid] = 0;
+    }
+    int q = 0;
+    bool first = true;
+    while (true) {
+        // this level's totals over the cluster (every CTA reads the same)
+        // lane r < kSmallCtas of every warp reads CTA r's counts; shuffles
+        // give each lane the totals and its exclusive prefix
+        unsigned nr = 0;
+        unsigned long long er = 0;
+        int ovr = 0;
+        if (lane < kSmallCtas) {
+            nr = *cl.map_shared_rank(&s_n[q], lane);
+            er = *cl.map_shared_rank(&s_e[q], lane);
+            ovr = *cl.map_shared_rank(&s_over[q], lane);
+        }
+        const unsigned long long tot_n = dev::warp_sum((unsigned long long)nr);
+        const unsigned long long tot_e = dev::warp_sum(er);
+        const int over = __any_sync(0xffffffffu, ovr != 0);
+        unsigned incl = min(nr, kSmallCap);  // prefix of the CTAs' queue lengths
+#pragma unroll
+        for (int o = 1; o < kSmallCtas; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o) incl += t;
+        }
+        const unsigned n_all = __shfl_sync(0xffffffffu, incl, kSmallCtas - 1);
+        const unsigned excl = incl - min(nr, kSmallCap);  // lane r: first row of CTA r
+        if (tot_n == 0 || iter >= S.max_iters) {
+            if (rank == 0 && tid == 0) {
+                st->iterations = iter;
+                st->small_done = 1;
+                st->exit_small = 0;
+                st->t_end = globaltimer();
+            }
+            cl.sync();  // no CTA leaves while another may still read its counts
+            return;
+        }
+        if (!first && (over || tot_e > kSmallExitE || !small_pushes(S, tot_n, tot_e))) {  // uniform
+            // back to the cooperative kernel: every CTA's queue (entries past
+            // its cap are there already) becomes fr[cur]'s list and bitmap
+            const PFront Fo = fr(cur);
+            const unsigned inq = min(s_n[q], kSmallCap);
+            if (tid < NBINS) s_bin[tid] = s_pos[tid] = 0;
+            __syncthreads();
+            for (unsigned i = tid; i < inq; i += kSB) {
+                const uint32_t dg = qd(q)[i];
+                atomicAdd(&s_bin[dg <= S.smax ? 0 : (dg <= S.mmax ? 1 : 2)], 1u);
+            }
+            __syncthreads();
+            if (tid < NBINS) s_base[tid] = atomicAdd(Fo.cnt + FC_BIN0 + tid, (unsigned long long)s_bin[tid]);
+            __syncthreads();
+            for (unsigned i = tid; i < inq; i += kSB) {
+                const uint32_t v = qv(q)[i], dg = qd(q)[i];
+                const uint32_t bin = dg <= S.smax ? 0 : (dg <= S.mmax ? 1 : 2);
+                Fo.bins[bin][s_base[bin] + atomicAdd(&s_pos[bin], 1u)] = v;
+                atomicOr(Fo.bitmap + (v >> 5), 1u << (v & 31));
+            }
+            if (rank == 0 && tid == 0) {
+                Fo.cnt[FC_NACTV] = tot_n;
+                Fo.cnt[FC_NACTE] = tot_e;
+                st->has_list[cur] = 1;
+                st->has_list[cur ^ 1] = 0;
+                st->all[0] = st->all[1] = 0;
+                st->cand_valid = 0;
+                st->small_iter = iter;
+                st->small_cur = cur;
+                st->small_done = 0;
+                st->exit_small = 0;
+                st->iterations = iter;
+            }
+            cl.sync();
+            return;
+        }
+        first = false;
+        const PFront O = fr(cur ^ 1);
+        if (rank == 0 && tid == 0) {
+            if (iter < GG_MAX_ITERS) {
+                st->variant[iter] = GG_VAR_PUSH_SPARSE;
+                st->nactv[iter] = tot_n;
+                st->nacte[iter] = tot_e;
+                st->scanned[iter] = tot_e;
+            }
+            st->reached_v += tot_n;
+            st->reached_e += tot_e;
+        }
+        // the other queue's counters: read by the other CTAs last level,
+        // before the barrier that ended it
+        if (tid == 0) {
+            s_n[q ^ 1] = 0;
+            s_e[q ^ 1] = 0;
+            s_over[q ^ 1] = 0;
+        }
+        __syncthreads();
+        const int32_t fk = iter + 1;
+        // the level's rows are the concatenation of all CTAs' queues, dealt
+        // to the cluster's warps in groups of 32 (a CTA's discoveries stay
+        // in its queue, so without this one CTA would expand a frontier that
+        // grew from one root); other CTAs' entries are read through
+        // distributed shared memory
+        // (group g of 32 rows goes to CTA g mod kSmallCtas: a level of a few
+        // thousand rows then spreads over every SM's load/store units)
+        for (unsigned base = (wid * kSmallCtas + rank) * 32; base < n_all; base += kSmallCtas * kSB) {
+            const unsigned i = base + lane;
+            const bool have = i < n_all;
+            unsigned r = 0;  // the CTA holding row i: last r whose first row <= i
+#pragma unroll
+            for (unsigned k = 1; k < kSmallCtas; ++k) r += __shfl_sync(0xffffffffu, excl, k) <= i;
+            const unsigned first_r = __shfl_sync(0xffffffffu, excl, r);
+            uint64_t b = 0;
+            uint32_t dg = 0;
+            if (have) {
+                const unsigned li = i - first_r;
+                b = cl.map_shared_rank(qb(q), r)[li];
+                dg = cl.map_shared_rank(qd(q), r)[li];
+            }
+            // the 32 rows' edges as one list, 4 per lane in flight; a target's
+            // offsets are loaded beside its atomicMin (needed only if it is
+            // new, but then without another round trip)
+            uint32_t incl_e = dg;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl_e, o);
+                if (lane >= (uint32_t)o) incl_e += t;
+            }
+            const uint32_t tot = __shfl_sync(0xffffffffu, incl_e, 31), ex = incl_e - dg;
+            for (uint32_t e0 = 0; e0 < tot; e0 += 128) {  // warp-uniform
+                uint32_t dd[4];
+                bool ok[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t idx = e0 + (uint32_t)u * 32u + lane;
+                    uint32_t rr = 0;
+#pragma unroll
+                    for (uint32_t step = 16; step; step >>= 1)
+                        if (__shfl_sync(0xffffffffu, ex, rr + step) <= idx) rr += step;
+                    const uint64_t rb = __shfl_sync(0xffffffffu, b, rr);
+                    const uint32_t rx = __shfl_sync(0xffffffffu, ex, rr);
+                    ok[u] = idx < tot;
+                    dd[u] = ok[u] ? __ldg(S.adj + rb + (idx - rx)) : 0u;
+                }
+                int32_t old[4];
+                uint64_t ob[4], oe[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    old[u] = ok[u] ? atomicMin(S.level + dd[u], fk) : fk;
+                    ob[u] = ok[u] ? __ldg(S.off + dd[u]) : 0;
+                    oe[u] = ok[u] ? __ldg(S.off + dd[u] + 1) : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (e0 + (uint32_t)u * 32u >= tot) break;  // warp-uniform
+                    small_append(S, O, old[u] > fk, dd[u], ob[u], (uint32_t)(oe[u] - ob[u]), qv(q ^ 1), qb(q ^ 1),
+                                 qd(q ^ 1), &s_n[q ^ 1], &s_e[q ^ 1], &s_over[q ^ 1]);
+                }
+            }
+        }
+        cl.sync();  // the level's appends and counts are complete in every CTA
+        ++iter;
+        cur ^= 1;
+        q ^= 1;
+        if (rank == 0 && tid == 0 && iter <= GG_MAX_ITERS) st->t_ns[iter] = globaltimer();
+    }
+}
+
 // Host side -----------------------------------------------------------------
 template <int R>
 static const void *traverse_kernel() { return (const void *)k_traverse<R>; }
@@ -1198,6 +1512,11 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
         f->has_list = f->has_bitmap = f->all = false;
     }
     P.iter0 = resume ? resume->iter0 : 0;
+    P.cur0 = 0;
+    // small frontiers after the iterations that mark a high-diameter run
+    // (a low-diameter one alternates between small and large frontiers,
+    // and each switch costs a host round trip)
+    P.small_from = std::max(P.iter0, t.graph_handoff > 0 ? t.graph_handoff : 32);
     P.cand[0] = c.list[0];
     P.cand[1] = c.list[1];
     P.nonisolated = g->nonisolated;
@@ -1241,6 +1560,9 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
         P.wq = g->wq;
         P.wq_cap = g->wq_cap;
     }
+    P.small_ok = t.small_frontier && d.relax == GG_RELAX_MIN_PLUS1_I32 && P.level_sync && level_k &&
+                 d.record == GG_RECORD_NE_PREV && P.force_iter < 0 && !start_all &&
+                 (opt.variant == GG_VAR_AUTO || opt.variant == GG_VAR_PUSH_SPARSE);
     P.gini = g->gini < 0 ? 0.0f : g->gini;
     if (opt.threshold == GG_THRESH_LEARNED && P.sel_w && g->gini < 0) {
         float gi;
@@ -1275,7 +1597,8 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
                     : d.relax == GG_RELAX_MIN_U32      ? traverse_kernel<GG_RELAX_MIN_U32>()
                                                         : traverse_kernel<GG_RELAX_SETIF_U32>();
     const int per_sm = resident_ctas(kfn, kPB);
-    const unsigned grid = (unsigned)(ctx->sm_count * per_sm);
+    unsigned grid = (unsigned)(ctx->sm_count * per_sm);
+    if (resume && t.handoff_ctas > 0) grid = std::min(grid, (unsigned)t.handoff_ctas);
     // merge-path scratch: one count per list entry (<= n) + one per CTA
     void *mp;
     GG_CHECK(graph_scratch(g, ((size_t)g->n + grid + 1) * 8, &mp));
@@ -1288,6 +1611,39 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
     GG_CUDA(ctx, cudaStreamSynchronize(s));
     if (hs.err & DEV_ERR_TIMEOUT) return set_error(ctx, GG_ERR_TIMEOUT, "traversal grid barrier timed out");
     if (hs.err) return set_error(ctx, GG_ERR_STATE, "traversal device error");
+    // small frontiers: the one-CTA kernel, then back to the cooperative one
+    // whenever the frontier outgrows it (records accumulate in the state block)
+    while (P.small_ok && hs.exit_small) {
+        // shared memory above 48 KiB is opt-in (set on the current device)
+        GG_CUDA(ctx, cudaFuncSetAttribute(k_small_bfs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem));
+        SmallArgs S;
+        S.off = g->off;
+        S.adj = g->adj;
+        S.level = (int32_t *)P.a;
+        S.fr[0] = P.fr[0];
+        S.fr[1] = P.fr[1];
+        S.st = st;
+        S.max_iters = P.max_iters;
+        S.smax = P.smax;
+        S.mmax = P.mmax;
+        S.m = P.m;
+        S.threshold = P.threshold;
+        S.threshold_k = P.threshold_k;
+        k_small_bfs<<<kSmallCtas, kSB, kSmallSmem, s>>>(S);
+        GG_LAUNCHED(ctx);
+        GG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PState), cudaMemcpyDeviceToHost, s));
+        GG_CUDA(ctx, cudaStreamSynchronize(s));
+        if (hs.small_done) break;
+        P.iter0 = hs.small_iter;
+        P.cur0 = hs.small_cur;
+        P.small_from = P.iter0 + 1;  // at least one cooperative step before the next hand-over
+        GG_CUDA(ctx, cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kPB), args, 0, s));
+        ctx->launches++;
+        GG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PState), cudaMemcpyDeviceToHost, s));
+        GG_CUDA(ctx, cudaStreamSynchronize(s));
+        if (hs.err & DEV_ERR_TIMEOUT) return set_error(ctx, GG_ERR_TIMEOUT, "traversal grid barrier timed out");
+        if (hs.err) return set_error(ctx, GG_ERR_STATE, "traversal device error");
+    }
     *iters_out = hs.iterations;
     g->force_rec.seen = P.force_iter >= 0 && P.force_iter < INT_MAX && hs.f_seen && hs.f_t1 >= hs.f_t0;
     if (g->force_rec.seen) {

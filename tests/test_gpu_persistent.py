@@ -224,6 +224,49 @@ def test_graph_bfs_handoff_to_device_driven(ctx, fusion_knobs, gen):
     g.close()
 
 
+@pytest.mark.parametrize("gen", ["rmat", "er_directed", "grid", "chain"])
+def test_small_frontier_kernel_equals_cooperative(ctx, fusion_knobs, gen):
+    """Device-driven BFS levels with the one-CTA small-frontier kernel on and
+    off: the oracle's levels, and the same iteration count, per-iteration
+    frontier sizes and reached counts.  R-MAT and ER frontiers outgrow the
+    kernel's shared-memory queue (hand-back to the cooperative kernel, also in
+    the middle of a level); the grid and the chain stay in it throughout."""
+    old = {k: gg.tuning_get(k) for k in ("small_frontier", "graph")}
+    if gen == "rmat":
+        og, sym = O.rmat(15, 16 << 15, seed=66), True
+    elif gen == "er_directed":
+        og, sym = O.er(40000, 12.0, seed=5, dangling_bp=200, symmetric=False), False
+    elif gen == "grid":
+        og, sym = O.grid(160, 120, seed=9, del_bp=300), True
+    else:
+        og, sym = O.from_edges(3000, [(i, i + 1) for i in range(2999)]), True
+    g = ctx.upload(og.off, og.adj, symmetric=sym)
+    deg = og.outdeg()
+    roots = [0, int(np.argmax(deg)), int(np.flatnonzero(deg)[-1])]
+    try:
+        gg.tuning_set("persistent", 1)
+        gg.tuning_set("graph", 0)
+        for r in roots:
+            ref = O.bfs_level(og, r)
+            res = {}
+            for sf in (0, 1):
+                gg.tuning_set("small_frontier", sf)
+                st = gg.RunStats()
+                lv = g.bfs_level(r, opts=gg.default_opts(collect=True), stats=st)
+                assert np.array_equal(lv, ref), (gen, r, sf)
+                res[sf] = st
+            s0, s1 = res[0], res[1]
+            assert s0.iterations == s1.iterations
+            k = min(s0.iterations, gg.MAX_ITERS)
+            assert [s0.nactv[i] for i in range(k)] == [s1.nactv[i] for i in range(k)], (gen, r)
+            assert [s0.nacte[i] for i in range(k)] == [s1.nacte[i] for i in range(k)], (gen, r)
+            assert s0.edges_reached == s1.edges_reached and s0.vertices_reached == s1.vertices_reached
+    finally:
+        for k, v in old.items():
+            gg.tuning_set(k, v)
+    g.close()
+
+
 def test_cc_hooking_repeated_long_chains(ctx, fusion_knobs):
     """Hooking's final pass writes every label once; repeated runs on long
     chains (deep trees) must always give the canonical labels."""
