@@ -522,7 +522,7 @@ def batch_eval(ctx, g, roots, hbm_peak, n_small):
     tb, tc = float(np.median(bm)), float(np.median(cm))
     out["small_graphs"] = {"graphs": n_small, "n": U.n, "m": U.m, "build_s": round(build_s, 1),
                            "bfs_ms": round(tb, 3), "bfs_gteps": round(bst.edges_reached / 2.0 / (tb / 1e3) / 1e9, 2),
-                           "bfs_iterations": bst.iterations, "bfs_launches": 1,
+                           "bfs_iterations": bst.iterations, "bfs_launches": int(bst.kernels),
                            "cc_ms": round(tc, 3), "cc_iterations": cst.iterations,
                            "cc_device_driven": bool(gg.tuning_get("persistent") & 4),
                            "graphs_per_s": round(n_small / ((tb + tc) / 1e3), 1)}
