@@ -1560,8 +1560,9 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
         P.wq = g->wq;
         P.wq_cap = g->wq_cap;
     }
+    // (not for multi-root runs: a batch of graphs stays one launch)
     P.small_ok = t.small_frontier && d.relax == GG_RELAX_MIN_PLUS1_I32 && P.level_sync && level_k &&
-                 d.record == GG_RECORD_NE_PREV && P.force_iter < 0 && !start_all &&
+                 d.record == GG_RECORD_NE_PREV && P.force_iter < 0 && !start_all && !d_roots &&
                  (opt.variant == GG_VAR_AUTO || opt.variant == GG_VAR_PUSH_SPARSE);
     P.gini = g->gini < 0 ? 0.0f : g->gini;
     if (opt.threshold == GG_THRESH_LEARNED && P.sel_w && g->gini < 0) {

@@ -20,9 +20,7 @@
  *  - gg_graph_union + gg_bfs_level_multi + gg_cc: many independent graphs
  *    are laid side by side as one graph (part i's vertex v becomes
  *    vertex_base[i] + v); BFS from one root per part is a multi-root BFS on
- *    the union (device-driven: one cooperative launch, plus a
- *    thread-block-cluster launch and a cooperative relaunch per phase of
- *    small frontiers after the 32nd level), CC of every part is CC of the
+ *    the union (one device-driven launch), CC of every part is CC of the
  *    union (label - vertex_base[i] = part-local label).
  */
 #ifndef GG_BATCH_H
@@ -52,9 +50,8 @@ GG_API gg_status gg_ppr(gg_graph *g, const uint32_t *seeds, int k, float alpha, 
  * each part and the total.  Symmetric iff every part is. */
 GG_API gg_status gg_graph_union(gg_ctx *ctx, gg_graph *const *parts, int k, gg_graph **out, uint32_t *vertex_base);
 
-/* BFS levels from several roots at once (all at level 0), run
- * device-driven (see above for the launches).  Duplicate roots are
- * ignored. */
+/* BFS levels from several roots at once (all at level 0), run as one
+ * device-driven launch.  Duplicate roots are ignored. */
 GG_API gg_status gg_bfs_level_multi(gg_graph *g, const uint32_t *roots, uint32_t k, const gg_run_opts *o,
                                     gg_prop *level, int32_t *host_level, gg_run_stats *st);
 
