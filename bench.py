@@ -621,8 +621,11 @@ def run_ours(args, ws, rank, local):
             cc_ms.append(st.total_ms)
             cst = st
         cc_best = float(np.median(cc_ms))
+        # one pass over the CSC and the labels, as the BFS line's one-pass fraction
+        cc_pass = 8.0 * (n + 1) + 4.0 * m + 8.0 * n
         out["cc"] = {"ms": round(cc_best, 3), "gedges_per_s": round(m / (cc_best / 1e3) / 1e9, 3),
-                     "iterations": cst.iterations}
+                     "iterations": cst.iterations,
+                     "one_pass_frac_of_hbm": round(cc_pass / (cc_best / 1e3) / 1e9 / hbm_peak, 4)}
 
         # ---- PageRank (PRv: FP32 storage, double gather accumulation, 20 iterations) ----
         x = g.prop(gg.F32)
