@@ -1612,7 +1612,7 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
     GG_CUDA(ctx, cudaStreamSynchronize(s));
     if (hs.err & DEV_ERR_TIMEOUT) return set_error(ctx, GG_ERR_TIMEOUT, "traversal grid barrier timed out");
     if (hs.err) return set_error(ctx, GG_ERR_STATE, "traversal device error");
-    // small frontiers: the one-CTA kernel, then back to the cooperative one
+    // small frontiers: the cluster kernel, then back to the cooperative one
     // whenever the frontier outgrows it (records accumulate in the state block)
     while (P.small_ok && hs.exit_small) {
         // shared memory above 48 KiB is opt-in (set on the current device)
