@@ -270,6 +270,16 @@ k_pr_heavy_chunks(const uint64_t *__restrict__ in_off, const uint32_t *__restric
         const uint64_t e1 = min(e0 + H.CH, re);
         Acc part = 0;
         uint64_t base = e0;
+        for (; base + 256 <= e1; base += 256) {  // two 128-edge blocks of loads in flight
+            uint32_t s8[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) s8[u] = __ldg(in_adj + base + 32 * u + lane);
+            Acc c8[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) c8[u] = (Acc)S::dec(contrib[s8[u]]);
+            part += c8[0] + c8[1] + c8[2] + c8[3];
+            part += c8[4] + c8[5] + c8[6] + c8[7];
+        }
         for (; base + 128 <= e1; base += 128) {
             uint32_t s0 = __ldg(in_adj + base + lane);
             uint32_t s1 = __ldg(in_adj + base + 32 + lane);
