@@ -14,6 +14,10 @@ constexpr int IN = GG_SEL_FEATURES, H = 32, OUT = GG_SEL_VARIANTS;
 // A learned choice replaces the threshold's only when its predicted time is
 // lower by more than this (log2 units: 2^-0.2 = 13% faster).
 constexpr float kSelMargin = 0.2f;
+// CC's records time the rest of the run, whose variants differ by a few per
+// cent at most on the training graphs: a CC step overrides the threshold
+// only on a predicted gain of more than 2^0.5 (41 %).
+constexpr float kSelMarginCC = 0.5f;
 constexpr int OW1 = 0, OB1 = OW1 + H * IN, OW2 = OB1 + H, OB2 = OW2 + H * H, OW3 = OB2 + H,
               OB3 = OW3 + OUT * H, NP = OB3 + OUT;
 static_assert(NP == GG_SEL_NPARAMS, "parameter layout");

@@ -77,6 +77,9 @@ struct PState {
     // at small_cur after small_iter iterations for k_small_bfs (exit_small),
     // which either finishes the run (small_done) or hands back the same way
     int exit_small, small_done, small_iter, small_cur;
+    // learned policy: the next step's choice, taken by one warp of CTA 0
+    // while the grid finishes the current step (slot = iteration & 1)
+    int next_choice[2];
 };
 
 struct PArgs {
@@ -917,8 +920,45 @@ __device__ __forceinline__ bool sel_close(unsigned long long a, unsigned long lo
     return d * 16 <= mx;
 }
 
+// The learned choice for a step with these frontier counts, unreached count
+// and iteration (one warp: every lane returns it; lane 0 updates the cache).
+__device__ int learned_choice(const PArgs &P, const __nv_bfloat16 *selw, unsigned long long nactv,
+                              unsigned long long nacte, unsigned long long unr, int it, SelCache *cache) {
+    const double n = P.n, m = (double)P.m, fv = (double)nactv, fe = (double)nacte;
+    float x[GG_SEL_FEATURES];
+    x[0] = (float)(log2(1.0 + fv) / 32);
+    x[1] = (float)(log2(1.0 + fe) / 40);
+    x[2] = (float)(log2(1.0 + (double)unr) / 32);
+    x[3] = (float)(log2(1.0 + it) / 8);
+    x[4] = (float)(log2(1.0 + (n > 0 ? m / n : 0)) / 8);
+    x[5] = P.gini;
+    x[6] = (float)(n > 0 ? fv / n : 0);
+    x[7] = (float)(m > 0 ? fe / m : 0);
+    x[8] = (float)fmin(4.0, m > 0 ? (fv + fe) / m : 0.0);
+    x[9] = (float)(log2(n > 1 ? n : 1.0) / 32);
+    float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
+    mlp::warp_forward(selw, x, o, z1, a1, z2, a2);
+    int best = 0;
+    for (int v = 1; v < GG_SEL_VARIANTS; ++v)
+        if (o[v] < o[best]) best = v;
+    // the threshold's choice stands unless the network predicts a clear gain over it
+    const int tv = (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+    const float margin = P.relax == GG_RELAX_MIN_U32 ? mlp::kSelMarginCC : mlp::kSelMargin;
+    if (!(o[best] < o[tv] - margin)) best = tv;
+    if ((threadIdx.x & 31) == 0) {
+        cache->nactv = nactv;
+        cache->nacte = nacte;
+        cache->unreached = unr;
+        cache->iter = it;
+        cache->choice = best;
+        cache->valid = 1;
+    }
+    return best;
+}
+
 __device__ int choose_variant(const PArgs &P, int iter, unsigned long long nactv, unsigned long long nacte,
-                              bool f_all, const PState *st, int *s_choice, SelCache *cache) {
+                              bool f_all, const PState *st, int *s_choice, SelCache *cache,
+                              const __nv_bfloat16 *selw) {
     if (f_all) return GG_VAR_PULL_DENSE;
     if (iter == P.force_iter) return P.force_variant;
     if (P.variant >= 0) return P.variant;
@@ -931,44 +971,18 @@ __device__ int choose_variant(const PArgs &P, int iter, unsigned long long nactv
     case GG_THRESH_LEARNED:
         if (P.sel_w) {
             // reuse the last evaluation while the inputs stay close (every
-            // thread tests the shared cache: no barrier on the common path)
-            const double n = P.n, m = (double)P.m, fv = (double)nactv, fe = (double)nacte;
-            const unsigned long long reached = ldcg(&st->reached_v);
-            const unsigned long long unr = reached < P.n ? P.n - reached : 0ull;
+            // thread tests the shared cache: no barrier on the common path;
+            // the frontier counts and the iteration decide a reuse, the
+            // unreached count, one more L2 load, only feeds an evaluation)
             const int it = min(iter, 255);
             if (cache->valid && sel_close(nactv, cache->nactv) && sel_close(nacte, cache->nacte) &&
-                sel_close(unr, cache->unreached) && it - cache->iter < 8)
+                it - cache->iter < 8)
                 return cache->choice;
             // warp 0 evaluates the network, the CTA reads its choice
             if (threadIdx.x < 32) {
-                float x[GG_SEL_FEATURES];
-                x[0] = (float)(log2(1.0 + fv) / 32);
-                x[1] = (float)(log2(1.0 + fe) / 40);
-                x[2] = (float)(log2(1.0 + (double)unr) / 32);
-                x[3] = (float)(log2(1.0 + it) / 8);
-                x[4] = (float)(log2(1.0 + (n > 0 ? m / n : 0)) / 8);
-                x[5] = P.gini;
-                x[6] = (float)(n > 0 ? fv / n : 0);
-                x[7] = (float)(m > 0 ? fe / m : 0);
-                x[8] = (float)fmin(4.0, m > 0 ? (fv + fe) / m : 0.0);
-                x[9] = (float)(log2(n > 1 ? n : 1.0) / 32);
-                float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
-                mlp::warp_forward(P.sel_w, x, o, z1, a1, z2, a2);
-                int best = 0;
-                for (int v = 1; v < GG_SEL_VARIANTS; ++v)
-                    if (o[v] < o[best]) best = v;
-                // the threshold's choice stands unless the network predicts
-                // a clear gain over it
-                const int tv = (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
-                if (!(o[best] < o[tv] - mlp::kSelMargin)) best = tv;
-                if (threadIdx.x == 0) {
-                    cache->nactv = nactv;
-                    cache->nacte = nacte;
-                    cache->unreached = unr;
-                    cache->iter = it;
-                    cache->choice = best;
-                    cache->valid = 1;
-                }
+                const unsigned long long reached = ldcg(&st->reached_v);
+                const unsigned long long unr = reached < P.n ? P.n - reached : 0ull;
+                learned_choice(P, selw, nactv, nacte, unr, it, cache);
             }
             __syncthreads();
             return cache->choice;
@@ -984,7 +998,12 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
     __shared__ __align__(16) uint32_t smem[kSmemWords];
     __shared__ int s_choice;
     __shared__ SelCache s_sel;
+    // the selector's weights in shared memory: an evaluation then waits on
+    // no global load (3 KiB, copied once per launch)
+    __shared__ __nv_bfloat16 s_selw[GG_SEL_NPARAMS];
     if (threadIdx.x == 0) s_sel.valid = 0;
+    if (P.sel_w && P.threshold == GG_THRESH_LEARNED)
+        for (int i = threadIdx.x; i < GG_SEL_NPARAMS; i += kPB) s_selw[i] = P.sel_w[i];
     __syncthreads();
     static_assert(kSmemWords * 4 >= (kLargeScan + 1) * 8, "chunk table fits the shared buffer");
     PState *st = P.st;
@@ -1009,7 +1028,15 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
         const int f_all = ldcg(&st->all[cur]);
         if (nactv == 0 && !f_all) break;
         if (P.level_k) op.fk = iter + 1;
-        const int var = choose_variant(P, iter, nactv, nacte, f_all != 0, st, &s_choice, &s_sel);
+        // learned policy: the choice was taken during the previous step's
+        // post-processing, except for a launch's first step
+        const bool pre = P.sel_w && P.threshold == GG_THRESH_LEARNED && P.variant < 0 && iter > P.iter0 &&
+                         !f_all && iter != P.force_iter;
+        const int var = pre ? ldcg(&st->next_choice[iter & 1])
+                            : choose_variant(P, iter, nactv, nacte, f_all != 0, st, &s_choice, &s_sel, s_selw);
+        // (the reached count this step starts from, for the next choice)
+        const unsigned long long reached_top =
+            (blockIdx.x == 0 && (threadIdx.x >> 5) == 1 && P.sel_w) ? ldcg(&st->reached_v) : 0ull;
         // a small listed frontier to push: the run continues in one CTA
         // cluster (k_small_bfs); every CTA reads the same counts, so all
         // leave together
@@ -1083,6 +1110,20 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
         }
         const uint32_t nwords = (P.n + 31) / 32;
         for (uint64_t w = tid; w < nwords; w += nthreads) F.bitmap[w] = 0u;
+        if (P.sel_w && P.threshold == GG_THRESH_LEARNED && P.variant < 0 && blockIdx.x == 0 &&
+            (threadIdx.x >> 5) == 1) {
+            // the next step's choice from the output frontier's final counts
+            const unsigned long long nv = ldcg(O.cnt + FC_NACTV), ne = ldcg(O.cnt + FC_NACTE);
+            const unsigned long long reached = reached_top + nactv;
+            const unsigned long long unr = reached < P.n ? P.n - reached : 0ull;
+            const int it = min(iter + 1, 255);
+            int c;
+            if (s_sel.valid && sel_close(nv, s_sel.nactv) && sel_close(ne, s_sel.nacte) && it - s_sel.iter < 8)
+                c = s_sel.choice;
+            else
+                c = learned_choice(P, s_selw, nv, ne, unr, it, &s_sel);
+            if ((threadIdx.x & 31) == 0) st->next_choice[(iter + 1) & 1] = c;
+        }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             // decision inputs change only here, between the two barriers, so
             // every CTA's next choice reads the same values

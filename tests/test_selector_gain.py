@@ -8,7 +8,8 @@ of training.  The shipped network (graptor_b200/data/selector.npz, trained on
 the GPU by gg_selector_train) is evaluated here with the float64 oracle on
 bfloat16-rounded weights, applying the same rule as the device: the
 threshold's choice (push_sparse iff |F| + outdeg(F) <= m/20, else pull_dense)
-stands unless the network predicts another variant 2^0.2 times faster."""
+stands unless the network predicts another variant 2^0.2 times faster (2^0.5
+for CC steps, whose records carry no unreached count: feature 2 is 0)."""
 import os
 
 import numpy as np
@@ -18,7 +19,7 @@ from oracle import mlp_oracle as M
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DATA = os.path.join(ROOT, "graptor_b200", "data")
-MARGIN = 0.2
+MARGIN, MARGIN_CC = 0.2, 0.5
 
 
 def heldout():
@@ -35,7 +36,8 @@ def choices(params, X):
     thr = np.where(X[:, 8] <= 0.05, 0, 2)  # feature 8 = (|F| + outdeg F) / m
     best = out.argmin(1)
     r = np.arange(len(X))
-    return np.where(out[r, best] < out[r, thr] - MARGIN, best, thr), thr
+    margin = np.where(X[:, 2] == 0, MARGIN_CC, MARGIN)
+    return np.where(out[r, best] < out[r, thr] - margin, best, thr), thr
 
 
 def test_records_are_usable():
