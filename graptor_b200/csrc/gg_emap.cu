@@ -1142,6 +1142,7 @@ struct GCtl {
     int threshold, threshold_k;
     int handoff_iter;  // > 0: after this many iterations the run leaves the graph (handed_off = 1)
     int handed_off;
+    int clr;  // written by the step kernel: 1 + the frontier whose bitmap `next` clears, or 0
     const __nv_bfloat16 *sel_w;  // learned selector weights (bfloat16), or null: the threshold decides
     float gini;
     // last network evaluation: reused while the frontier counts stay within 1/16
@@ -1218,6 +1219,7 @@ __global__ void k_g_init(GCtl *c) {
         c->cand_cur = 0;
         c->sel_valid = 0;
         c->handed_off = 0;
+        c->clr = 0;
         c->reached_v = 0;
         c->reached_e = 0;
         c->variant = -1;
@@ -1383,7 +1385,11 @@ __global__ void __launch_bounds__(kBlock, 6) k_g_push(GCtl *c) {
     __shared__ EmapArgs sA;
     __shared__ Op<GG_RELAX_MIN_PLUS1_I32> sOp;
     __shared__ uint32_t s_nl, s_nm;
-    if (threadIdx.x == 0) g_push_setup(c, gridDim.x, &sA, &sOp, &s_nl, &s_nm);
+    if (threadIdx.x == 0) {
+        g_push_setup(c, gridDim.x, &sA, &sOp, &s_nl, &s_nm);
+        // the pushed frontier's bitmap, if a pull made it, is cleared after
+        if (blockIdx.x == 0) c->clr = c->has_bitmap[c->cur] ? c->cur + 1 : 0;
+    }
     __syncthreads();
     push_binned_body<GG_RELAX_MIN_PLUS1_I32, kBlock>(sA, sOp, s_nl, s_nm);
 }
@@ -1447,25 +1453,28 @@ __global__ void __launch_bounds__(kBlock, 6) k_g_pull(GCtl *c) {
     if (threadIdx.x == 0) {
         sA = c->A;
         sOp = c->op;
+        if (blockIdx.x == 0) c->clr = c->cur + 1;  // a pulled frontier has a bitmap to clear after
     }
     __syncthreads();
     pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock>(sA, sOp);
 }
 
-// the consumed frontier's bitmap is cleared for its next use as an output
-// (only when the step that made it, or the conversion for a pull, set one)
-__global__ void k_g_clear(GCtl *c) {
-    if (c->variant < 0 || (!c->has_bitmap[c->cur] && !c->need_bitmap)) return;
-    uint32_t *bm = c->f[c->cur].bitmap;
-    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
-    const uint64_t words = ((uint64_t)c->n + 31) / 32;
-    for (uint64_t w = tid; w < words; w += nth) bm[w] = 0u;
-}
-
 __device__ void g_bookkeep(GCtl *c);
 
-// bookkeeping of the step that ran (thread 0), then the next step's decision (the warp)
-__global__ void k_g_next(GCtl *c) {
+// After a step: every CTA clears the consumed frontier's bitmap for its next
+// use as an output (when the step, or the conversion for a pull, set one:
+// the step kernel names it in `clr`, a field nothing here writes); warp 0 of
+// CTA 0 meanwhile does the step's bookkeeping (thread 0) and the next step's
+// decision, which touch no bitmap.
+__global__ void __launch_bounds__(256) k_g_next(GCtl *c) {
+    const int clr = c->clr;
+    if (clr) {
+        uint32_t *bm = c->f[clr - 1].bitmap;
+        const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
+        const uint64_t words = ((uint64_t)c->n + 31) / 32;
+        for (uint64_t w = tid; w < words; w += nth) bm[w] = 0u;
+    }
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
     if (c->variant < 0) {
         if (threadIdx.x == 0) cudaGraphSetConditional(c->h_while, 0);
         return;
@@ -1616,7 +1625,7 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     GG_CHECK(add_cond(ctx, G, &n_while, &n_init, 1, hw, cudaGraphCondTypeWhile, &body));
     GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hp, body, 0, 0));
     GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hq, body, 0, 0));
-    cudaGraphNode_t n_ifp, n_ifq, n_clear, n_next;
+    cudaGraphNode_t n_ifp, n_ifq, n_next;
     cudaGraph_t bp, bq;
     GG_CHECK(add_cond(ctx, body, &n_ifp, nullptr, 0, hp, cudaGraphCondTypeIf, &bp));
     GG_CHECK(add_cond(ctx, body, &n_ifq, nullptr, 0, hq, cudaGraphCondTypeIf, &bq));
@@ -1636,8 +1645,7 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     GG_CHECK(add_kernel(ctx, bb, &n_bits, nullptr, 0, (const void *)k_g_tobitmap, gb->vgrid, 256, arg));
     GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_ifb, 1, (const void *)k_g_pull, gb->pull_grid, kBlock, arg));
     cudaGraphNode_t deps[2] = {n_ifp, n_ifq};
-    GG_CHECK(add_kernel(ctx, body, &n_clear, deps, 2, (const void *)k_g_clear, (unsigned)ctx->sm_count * 2, 256, arg));
-    GG_CHECK(add_kernel(ctx, body, &n_next, &n_clear, 1, (const void *)k_g_next, 1, 32, arg));
+    GG_CHECK(add_kernel(ctx, body, &n_next, deps, 2, (const void *)k_g_next, (unsigned)ctx->sm_count * 2, 256, arg));
     GG_CUDA(ctx, cudaGraphInstantiate(&gb->exec, G, 0));
     // the handles live in the control block, set once
     cudaGraphConditionalHandle hs[6] = {hw, hp, hq, hl, hb, hc};
@@ -1743,9 +1751,9 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     }
     const int T = hr->iterations;
     *iters_out = T;
-    // kernels the graph ran: init, then per iteration the step kernel, clear
-    // and next (plus a list or bitmap conversion where the variant changes)
-    ctx->launches += 1 + 3 * (uint64_t)T;
+    // kernels the graph ran: init, then per iteration the step kernel and
+    // next (plus a list or bitmap conversion where the variant changes)
+    ctx->launches += 1 + 2 * (uint64_t)T;
     if (hr->handed_off) {
         // the rest of the run as one device-driven launch from the current
         // frontier (a push leaves it as a list only: add its bitmap)
