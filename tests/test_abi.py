@@ -84,6 +84,27 @@ def test_tuning_knobs_roundtrip():
     assert gg.tuning_get("bin_small_max") == small  # a rejected set changes nothing
 
 
+def test_traversal_mode_knobs():
+    """Defaults and ranges of the knobs that pick how a BFS run is driven:
+    graph-driven levels, the hand-over to the device-driven kernel (after
+    how many levels, on how many CTAs) and the small-frontier cluster."""
+    from graptor_b200 import gg
+    names = ("graph", "graph_handoff", "handoff_ctas", "small_frontier")
+    old = {k: gg.tuning_get(k) for k in names}
+    assert old == {"graph": 1, "graph_handoff": 32, "handoff_ctas": 148, "small_frontier": 1}
+    try:
+        for k, v in (("graph_handoff", 0), ("graph_handoff", 1000), ("handoff_ctas", 0), ("handoff_ctas", 37),
+                     ("small_frontier", 0)):
+            gg.tuning_set(k, v)
+            assert gg.tuning_get(k) == v
+        for k, v in (("graph", 2), ("small_frontier", 2), ("graph_handoff", -1), ("handoff_ctas", 1 << 20)):
+            with pytest.raises(gg.GGError):
+                gg.tuning_set(k, v)
+    finally:
+        for k, v in old.items():
+            gg.tuning_set(k, v)
+
+
 def test_autotune_apply_orders_the_bin_pair():
     from graptor_b200 import autotune, gg
     old = {k: gg.tuning_get(k) for k in ("bin_small_max", "bin_medium_max", "pull_k")}
