@@ -1613,8 +1613,8 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     cudaGraph_t G = gb->graph;
     GCtl *ctl = gb->ctl;
     GCtl **arg = &gb->ctl;
-    // init (+ first decision) -> WHILE { IF push { IF list {tolist} -> push },
-    //                                  IF pull { IF bits {tobitmap} -> pull } -> clear -> next }
+    // init (+ first decision) -> WHILE { IF push { IF list {tolist} -> IF chunks {chunks} -> push },
+    //                                  IF pull { IF bits {tobitmap} -> pull } -> next (clear + decision) }
     // The branch handles keep the value the decision set (no default
     // assignment); the loop handle starts at 1 on every launch.
     cudaGraphConditionalHandle hw, hp, hq, hl, hb, hc;
