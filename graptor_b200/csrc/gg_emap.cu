@@ -1247,8 +1247,7 @@ __device__ void decide_step(GCtl *c) {
         c->handed_off = nactv != 0 && iter < c->max_iters;
         c->variant = -1;
         c->iterations = iter;
-        cudaGraphSetConditional(c->h_push, 0);
-        cudaGraphSetConditional(c->h_pull, 0);
+        cudaGraphSetConditional(c->h_push, 2u);  // the step switch: no body
         cudaGraphSetConditional(c->h_list, 0);
         cudaGraphSetConditional(c->h_bits, 0);
         cudaGraphSetConditional(c->h_chunks, 0);
@@ -1349,8 +1348,7 @@ __device__ void decide_step(GCtl *c) {
     const bool chunks = push && (c->need_list || F.cnt[FC_BIN2] > kLargeLocal);
     cudaGraphSetConditional(c->h_chunks, chunks ? 1u : 0u);
     c->need_bitmap = !push && !c->has_bitmap[c->cur];
-    cudaGraphSetConditional(c->h_push, push ? 1u : 0u);
-    cudaGraphSetConditional(c->h_pull, push ? 0u : 1u);
+    cudaGraphSetConditional(c->h_push, push ? 0u : 1u);  // the step switch: push or pull body
     cudaGraphSetConditional(c->h_list, c->need_list ? 1u : 0u);
     cudaGraphSetConditional(c->h_bits, c->need_bitmap ? 1u : 0u);
     cudaGraphSetConditional(c->h_while, 1u);
@@ -1581,14 +1579,15 @@ static gg_status add_kernel(gg_ctx *ctx, cudaGraph_t g, cudaGraphNode_t *node, c
 }
 
 static gg_status add_cond(gg_ctx *ctx, cudaGraph_t g, cudaGraphNode_t *node, const cudaGraphNode_t *deps, size_t nd,
-                          cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaGraph_t *body) {
+                          cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type, cudaGraph_t *body,
+                          unsigned nbodies = 1) {
     cudaGraphNodeParams np = {};
     np.type = cudaGraphNodeTypeConditional;
     np.conditional.handle = h;
     np.conditional.type = type;
-    np.conditional.size = 1;
+    np.conditional.size = nbodies;
     GG_CUDA(ctx, cudaGraphAddNode(node, g, deps, nd, &np));
-    *body = np.conditional.phGraph_out[0];
+    for (unsigned i = 0; i < nbodies; ++i) body[i] = np.conditional.phGraph_out[i];
     return GG_OK;
 }
 
@@ -1613,8 +1612,8 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     cudaGraph_t G = gb->graph;
     GCtl *ctl = gb->ctl;
     GCtl **arg = &gb->ctl;
-    // init (+ first decision) -> WHILE { IF push { IF list {tolist} -> IF chunks {chunks} -> push },
-    //                                  IF pull { IF bits {tobitmap} -> pull } -> next (clear + decision) }
+    // init (+ first decision) -> WHILE { SWITCH { push: IF list {tolist} -> IF chunks {chunks} -> push,
+    //                                           pull: IF bits {tobitmap} -> pull } -> next (clear + decision) }
     // The branch handles keep the value the decision set (no default
     // assignment); the loop handle starts at 1 on every launch.
     cudaGraphConditionalHandle hw, hp, hq, hl, hb, hc;
@@ -1623,12 +1622,14 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     GG_CHECK(add_kernel(ctx, G, &n_init, nullptr, 0, (const void *)k_g_init, gb->vgrid, 256, arg));
     cudaGraph_t body;
     GG_CHECK(add_cond(ctx, G, &n_while, &n_init, 1, hw, cudaGraphCondTypeWhile, &body));
+    // one SWITCH picks the step: body 0 push, body 1 pull, 2 none (h_pull
+    // is the same handle)
     GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hp, body, 0, 0));
-    GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hq, body, 0, 0));
-    cudaGraphNode_t n_ifp, n_ifq, n_next;
-    cudaGraph_t bp, bq;
-    GG_CHECK(add_cond(ctx, body, &n_ifp, nullptr, 0, hp, cudaGraphCondTypeIf, &bp));
-    GG_CHECK(add_cond(ctx, body, &n_ifq, nullptr, 0, hq, cudaGraphCondTypeIf, &bq));
+    hq = hp;
+    cudaGraphNode_t n_sw, n_next;
+    cudaGraph_t bsw[2];
+    GG_CHECK(add_cond(ctx, body, &n_sw, nullptr, 0, hp, cudaGraphCondTypeSwitch, bsw, 2));
+    cudaGraph_t bp = bsw[0], bq = bsw[1];
     GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hl, bp, 0, 0));
     GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hc, bp, 0, 0));
     GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hb, bq, 0, 0));
@@ -1644,8 +1645,7 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     GG_CHECK(add_cond(ctx, bq, &n_ifb, nullptr, 0, hb, cudaGraphCondTypeIf, &bb));
     GG_CHECK(add_kernel(ctx, bb, &n_bits, nullptr, 0, (const void *)k_g_tobitmap, gb->vgrid, 256, arg));
     GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_ifb, 1, (const void *)k_g_pull, gb->pull_grid, kBlock, arg));
-    cudaGraphNode_t deps[2] = {n_ifp, n_ifq};
-    GG_CHECK(add_kernel(ctx, body, &n_next, deps, 2, (const void *)k_g_next, (unsigned)ctx->sm_count * 2, 256, arg));
+    GG_CHECK(add_kernel(ctx, body, &n_next, &n_sw, 1, (const void *)k_g_next, (unsigned)ctx->sm_count * 2, 256, arg));
     GG_CUDA(ctx, cudaGraphInstantiate(&gb->exec, G, 0));
     // the handles live in the control block, set once
     cudaGraphConditionalHandle hs[6] = {hw, hp, hq, hl, hb, hc};
