@@ -288,7 +288,11 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
         if (changed) {
             op.a[d] = best;
             if (A.record == GG_RECORD_NE_PREV) {
-                if (best != op.prev[d]) {
+                // level-synchronous: d was unvisited, so its prev equals the
+                // value replaced; prev is neither read nor written
+                if (R == GG_RELAX_MIN_PLUS1_I32 && op.level_sync) {
+                    rec = true;
+                } else if (best != op.prev[d]) {
                     op.prev[d] = best;
                     rec = true;
                 }
@@ -1187,11 +1191,8 @@ __device__ void decide_step(GCtl *c);
 __global__ void k_g_init(GCtl *c) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
     const int32_t inf = (int32_t)c->n + 1;
-    for (uint64_t v = tid; v < c->n; v += nth) {
-        const int32_t x = v == c->root ? 0 : inf;
-        c->level[v] = x;
-        c->prev[v] = x;
-    }
+    // (prev is not used by level-synchronous steps: only level is filled)
+    for (uint64_t v = tid; v < c->n; v += nth) c->level[v] = v == c->root ? 0 : inf;
     const uint64_t words = ((uint64_t)c->n + 31) / 32;
     for (uint64_t w = tid; w < words; w += nth) {
         c->f[0].bitmap[w] = w == (c->root >> 5) ? 1u << (c->root & 31) : 0u;
@@ -1843,12 +1844,12 @@ gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop
         return gg_ctx_sync(g->ctx);
     }
     RunTimer tm(g->ctx);
-    // BFSLVLv.C:117-129: level = prev = n+1, level[start] = prev[start] = 0
+    // BFSLVLv.C:117-129: level = prev = n+1, level[start] = prev[start] = 0;
+    // the level-synchronous steps below never read or write prev (an
+    // unvisited vertex's prev would equal its level), so only level is set
     int32_t inf = (int32_t)g->n + 1, zero = 0;
     GG_CHECK(gg_prop_fill(level, &inf));
-    GG_CHECK(gg_prop_fill(prev, &inf));
     GG_CHECK(gg_prop_set(level, root, &zero));
-    GG_CHECK(gg_prop_set(prev, root, &zero));
     gg_frontier *F, *O;
     GG_CHECK(get_tmp_frontiers(g, &F, &O));
     GG_CHECK(gg_frontier_set_single(F, root));
@@ -1904,8 +1905,7 @@ gg_status gg_bfs_level_multi(gg_graph *g, const uint32_t *roots, uint32_t k, con
         GG_CUDA(ctx, cudaMemcpyAsync(d_roots, r.data(), r.size() * 4, cudaMemcpyHostToDevice, ctx->stream));
     RunTimer tm(ctx);
     int32_t inf = (int32_t)g->n + 1;
-    GG_CHECK(gg_prop_fill(level, &inf));
-    GG_CHECK(gg_prop_fill(prev, &inf));
+    GG_CHECK(gg_prop_fill(level, &inf));  // (prev: unused by level-synchronous steps)
     if (!r.empty()) {
         k_scatter_zero_i32<<<((unsigned)r.size() + 255) / 256, 256, 0, ctx->stream>>>(
             (int32_t *)level->d, (int32_t *)prev->d, d_roots, (uint32_t)r.size());

@@ -691,7 +691,11 @@ __device__ void phase_pull(const PArgs &P, const POp<R> &op, const PFront &F, co
         if (changed) {
             op.a[d] = best;
             if (P.record == GG_RECORD_NE_PREV) {
-                if (best != ldcg(op.prev + d)) {
+                // level-synchronous: d was unvisited, so its prev equals the
+                // value replaced; prev is neither read nor written
+                if (R == GG_RELAX_MIN_PLUS1_I32 && op.level_sync) {
+                    rec = true;
+                } else if (best != ldcg(op.prev + d)) {
                     op.prev[d] = best;
                     rec = true;
                 }
@@ -1098,7 +1102,7 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
         }
         if (!grid_barrier(st, P.timeout_ns)) return;
         // post: maintain copies for a push, recycle the old frontier as next output
-        if (pushes && P.record == GG_RECORD_NE_PREV) {
+        if (pushes && P.record == GG_RECORD_NE_PREV && !(P.relax == GG_RELAX_MIN_PLUS1_I32 && P.level_sync)) {
             const unsigned long long b0 = ldcg(O.cnt + FC_BIN0), b1 = ldcg(O.cnt + FC_BIN1),
                                      b2 = ldcg(O.cnt + FC_BIN2);
             for (uint64_t i = tid; i < b0 + b1 + b2; i += nthreads) {

@@ -232,13 +232,12 @@ typedef struct gg_emap_desc {
     int fusion;             /* api::fusion present: multi-hop push allowed */
     int src_level_sync;     /* MIN_PLUS1 with GT_CONST filter k: every active source
                                holds a[s] == k-1 (level-synchronous BFS), so the
-                               relax offers k without loading a[s]; a push then
-                               leaves prev of the vertices it records as it was
-                               (only unvisited vertices' prev is ever compared),
-                               and every vertex passing the filter holds the same
+                               relax offers k without loading a[s]; every vertex
+                               passing the filter is unvisited and holds the same
                                value in a and prev (BFSLVLv.C:117-129 sets both
-                               to n+1), so a push records the first writer of
-                               each such vertex without loading prev */
+                               to n+1), so a step records the first writer of
+                               each such vertex and prev is neither read nor
+                               written */
 } gg_emap_desc;
 
 typedef struct gg_emap_stats {
