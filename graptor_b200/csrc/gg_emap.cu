@@ -322,7 +322,9 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
         if (rec) {
             // the output list is built from the bitmap only if a push needs it
             nv++;
-            ne += A.off[d + 1] - A.off[d];
+            // out-degree: for a symmetric graph the CSC is the CSR, and d's
+            // row bounds are already in registers
+            ne += A.off == A.in_off ? end - beg : A.off[d + 1] - A.off[d];
         }
         // still a candidate: passes the filter and has in-edges
         if (A.cand_out) keepers.push(valid && act && end > beg, d);

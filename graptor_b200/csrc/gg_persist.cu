@@ -715,7 +715,9 @@ __device__ void phase_pull(const PArgs &P, const POp<R> &op, const PFront &F, co
         }
         if (rec) {
             nv++;
-            ne += P.off[d + 1] - P.off[d];
+            // out-degree: for a symmetric graph the CSC is the CSR, and d's
+            // row bounds are already in registers
+            ne += P.off == P.in_off ? end - beg : P.off[d + 1] - P.off[d];
         }
         keepers.push(valid && act && end > beg, d);
     }
