@@ -231,7 +231,7 @@ def test_small_frontier_kernel_equals_cooperative(ctx, fusion_knobs, gen):
     frontier sizes and reached counts.  R-MAT and ER frontiers outgrow the
     kernel's shared-memory queue (hand-back to the cooperative kernel, also in
     the middle of a level); the grid and the chain stay in it throughout."""
-    old = {k: gg.tuning_get(k) for k in ("small_frontier", "graph")}
+    old = {k: gg.tuning_get(k) for k in ("small_frontier", "graph", "graph_handoff")}
     if gen == "rmat":
         og, sym = O.rmat(15, 16 << 15, seed=66), True
     elif gen == "er_directed":
@@ -246,6 +246,9 @@ def test_small_frontier_kernel_equals_cooperative(ctx, fusion_knobs, gen):
     try:
         gg.tuning_set("persistent", 1)
         gg.tuning_set("graph", 0)
+        # the cluster may take over from the second level on (by default only
+        # after 32), so that short R-MAT / ER runs go in and out of it
+        gg.tuning_set("graph_handoff", 1)
         for r in roots:
             ref = O.bfs_level(og, r)
             res = {}
@@ -261,6 +264,8 @@ def test_small_frontier_kernel_equals_cooperative(ctx, fusion_knobs, gen):
             assert [s0.nactv[i] for i in range(k)] == [s1.nactv[i] for i in range(k)], (gen, r)
             assert [s0.nacte[i] for i in range(k)] == [s1.nacte[i] for i in range(k)], (gen, r)
             assert s0.edges_reached == s1.edges_reached and s0.vertices_reached == s1.vertices_reached
+            if gen in ("grid", "chain"):  # small from the second level on: the cluster kernel ran
+                assert s1.kernels > s0.kernels, (gen, r, s0.kernels, s1.kernels)
     finally:
         for k, v in old.items():
             gg.tuning_set(k, v)
