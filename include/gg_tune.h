@@ -21,11 +21,12 @@
  * default: a graph-driven BFS still running after that many iterations
  * continues as one device-driven cooperative launch from its current
  * frontier; 0: never), handoff_ctas (CTAs of that launch, 148 by default,
- * 0 = all that fit), small_frontier (1, the default: a device-driven BFS
- * whose listed frontier is at most 8192 vertices and 65536 edges runs its
- * levels in one cluster of 8 CTAs with the frontier in shared memory until
- * the frontier outgrows a CTA's 4096-entry queue or 262144 edges; 0:
- * never), cc_hook (1: a
+ * 0 = all that fit), small_frontier (1, the default: from level
+ * graph_handoff on (32 when that knob is 0), a device-driven BFS whose
+ * listed frontier is at most 8192 vertices and 65536 edges runs its levels
+ * in one cluster of 8 CTAs with the frontier in shared memory until the
+ * frontier outgrows a CTA's 4096-entry queue or 262144 edges; 0: never),
+ * cc_hook (1: a
  * device-driven CC run of a symmetric graph
  * that passes CCv's road-network test after its first step finishes by
  * min-id hooking; 0: label propagation throughout), fusion (4: the sparse
