@@ -667,7 +667,9 @@ inline bool is_ref_at(const NP &n, NK var) { return n->k == NK::Ref && n->prop &
 inline bool is_const(const NP &n, double v) { return n->k == NK::Const && n->cval == v; }
 inline NP strip_cast(const NP &n) { return n->k == NK::Cast ? n->c[0] : n; }
 
-// relax(s,d,e) -> descriptor fields (SURVEY-documented lowering table)
+// relax(s,d,e) -> descriptor fields: a[d].min(a[s] + 1) -> MIN_PLUS1_I32,
+// a[d].min(a[s]) -> MIN_U32, a[d].setif(s) -> SETIF_U32,
+// y[d] += cast(contrib[s]) -> ADD_GATHER
 inline void lower_relax(const NP &r, gg_emap_desc &d) {
     if (r->k == NK::Min && is_ref_at(r->c[0], NK::VarDst)) {
         const NP &a = r->c[0], &x = r->c[1];
