@@ -1,0 +1,51 @@
+"""Host-side contracts checked without a GPU: the selector's training graph
+family covers the stated ranges, and the benchmark's reference arm prints
+one JSON line with the keys the measurement contract names."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_selector_training_family_ranges():
+    from graptor_b200.selector_train import graph_family
+    rng = np.random.default_rng(7)  # the seed collect() uses
+    fam = [graph_family(i, rng) for i in range(200)]
+    kinds = [k for k, _, _ in fam]
+    assert kinds.count("rmat") == 67 and kinds.count("er") == 67 and kinds.count("grid") == 66
+    for kind, kw, _ in fam:
+        if kind == "rmat":  # R-MAT scales 18-22, a in [0.45, 0.65], d = 0.05, b = c
+            assert 18 <= kw["scale"] <= 22 and kw["nedges"] == 16 << kw["scale"]
+            assert 0.45 <= kw["a"] <= 0.65 and kw["b"] == kw["c"]
+            assert abs(1.0 - kw["a"] - kw["b"] - kw["c"] - 0.05) < 1e-12
+        elif kind == "er":  # average degree 4-64
+            assert 4.0 <= kw["avgdeg"] <= 64.0 and 2 ** 18 <= kw["n"] <= 2 ** 21
+        else:  # 2-D grids of 2^20-2^22 vertices, 1 % of the edges deleted
+            n = kw["rows"] * kw["cols"]
+            assert 2 ** 20 <= n <= 2 ** 22 and kw["del_bp"] == 100
+
+
+def _reference_built():
+    from oracle import oracle as O
+    return O.ref_available("ref_bfslvl")
+
+
+@pytest.mark.skipif(not _reference_built(), reason="reference build (oracle/_ref) absent")
+def test_bench_reference_arm_json_line():
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--scale", "12",
+                          "--steps", "2", "--warmup", "3"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+              "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e", "impl"):
+        assert k in d, k
+    assert d["impl"] == "reference" and d["unit"] == "GTEPS" and d["value"] > 0
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+    assert d["cpu_baseline"]["kind"] == "reference" and d["cpu_baseline"]["cores"] >= 1
