@@ -205,7 +205,7 @@ def pick_roots(deg: np.ndarray) -> np.ndarray:
 
 # DRAM bytes (read + write) per dense-pull launch, from one ncu capture of
 # k_pull (4 launches of R-MAT scale 23 BFS, 316 MB each on average) scaled
-# by the vertex count to scale 24: profiles/k_pull_rmat23_dram_traffic.md
+# by the vertex count to scale 24
 K_PULL_TRAFFIC_PER_LAUNCH = 632.5e6
 
 
@@ -746,6 +746,115 @@ def run_ours(args, ws, rank, local):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# single workloads for profilers (--case): one JSON line with device times and
+# the per-iteration variant / frontier / kernel-time table of the last run
+#
+#   python bench.py --case bfs   --scale 24 --roots 4
+#   python bench.py --case pr    --scale 24 --format bf16 --iters 5
+#   python bench.py --case cc    --graph grid --side 2896
+#   python bench.py --case msbfs --scale 22
+#   python bench.py --case ppr   --scale 22 --iters 5
+# ---------------------------------------------------------------------------
+def case_formats():
+    from graptor_b200 import gg
+    return {"f32": gg.F32, "bf16": gg.BF16, "f16": gg.F16, "fp8": gg.FP8E4M3, "cfp": gg.CFP_6_10,
+            "bf16t": gg.BF16_TRUNC, "f64": gg.F64}
+
+
+def case_roots(g, k: int, seed: int = 12345):
+    off, _ = g.download()
+    nz = np.flatnonzero(np.diff(off))
+    return [int(r) for r in np.random.default_rng(seed).choice(nz, size=k, replace=False)]
+
+
+def iter_table(st):
+    from graptor_b200 import gg
+    t = min(st.iterations, gg.MAX_ITERS)
+    return [[i, st.variant[i], int(st.nactv[i]), int(st.nacte[i]), round(st.iter_ms[i], 4)] for i in range(t)]
+
+
+def run_case(a):
+    from graptor_b200 import gg
+    if a.persistent is not None:
+        gg.tuning_set("persistent", a.persistent)
+    if a.graph_mode is not None:
+        gg.tuning_set("graph", a.graph_mode)
+    ctx = gg.Context(0)
+    if a.graph == "grid":
+        g = ctx.grid(a.side, a.side, 77, del_bp=100)
+    elif a.graph == "er":
+        g = ctx.er(1 << a.scale, 32.0, 1, dangling_bp=100, symmetric=False)
+    else:
+        g = ctx.rmat(a.scale, 16 << a.scale, 1)
+    out = {"case": a.case, "graph": a.graph, "n": g.n, "m": g.m, "persistent": gg.tuning_get("persistent")}
+    opts = gg.default_opts(gg.THRESH_LEARNED if a.threshold == "learned" else gg.THRESH_DEFAULT, collect=True)
+    if a.threshold == "learned":
+        from graptor_b200.selector_train import load_selector
+        gg.attach_selector(g, load_selector(ctx))
+    if a.case == "bfs":
+        rs = case_roots(g, a.roots)
+        for r in rs[: a.warmup]:
+            g.bfs_level(r, host=False)
+        tot, ker, last, worst = [], [], None, None
+        for _ in range(a.reps):
+            for r in rs:
+                st = gg.RunStats()
+                g.bfs_level(r, host=False, opts=opts, stats=st)
+                tot.append(st.total_ms)
+                ker.append(sum(st.iter_ms[i] for i in range(min(st.iterations, gg.MAX_ITERS))))
+                last = st
+                if worst is None or st.total_ms > worst[1]:
+                    worst = (r, st.total_ms, iter_table(st))
+        out.update(ms_per_bfs=round(float(np.mean(tot)), 4), kernel_ms_per_bfs=round(float(np.mean(ker)), 4),
+                   ms_per_bfs_median=round(float(np.median(tot)), 4),
+                   per_root_ms=[round(x, 3) for x in tot[: len(rs)]], iterations=iter_table(last),
+                   worst_root=worst[0], worst_ms=round(worst[1], 3), worst_iterations=worst[2])
+    elif a.case == "cc":
+        for _ in range(a.warmup):
+            g.cc(host=False)
+        ts = []
+        for _ in range(a.reps):
+            st = gg.RunStats()
+            g.cc(host=False, opts=gg.default_opts(gg.THRESH_FRAC, 5, collect=True), stats=st)
+            ts.append(st.total_ms)
+        out.update(ms=round(float(np.median(ts)), 4), iterations=iter_table(st))
+    elif a.case == "pr":
+        fmt = case_formats()[a.format]
+        for _ in range(a.warmup):
+            g.pagerank(maxiter=2, tol=-1.0, contrib=fmt, host=False)
+        ts = []
+        for _ in range(a.reps):
+            st = gg.RunStats()
+            g.pagerank(maxiter=a.iters, tol=-1.0, contrib=fmt, accum_f64=fmt in (gg.F32, gg.F64), host=False,
+                       stats=st)
+            ts.append(st.total_ms / max(st.iterations, 1))
+        out.update(format=a.format, ms_per_iter=round(float(np.median(ts)), 4))
+    elif a.case == "msbfs":
+        rs = case_roots(g, 64)
+        for _ in range(a.warmup):
+            gg.msbfs(g, rs, host=False)
+        ts = []
+        for _ in range(a.reps):
+            st = gg.RunStats()
+            gg.msbfs(g, rs, host=False, stats=st)
+            ts.append(st.total_ms)
+        out.update(ms=round(float(np.median(ts)), 4), edges_reached=int(st.edges_reached),
+                   iterations=[[i, st.variant[i], round(st.iter_ms[i], 4)] for i in range(st.iterations)])
+    else:
+        rs = case_roots(g, min(a.seeds, gg.PPR_MAX_SEEDS))
+        for _ in range(a.warmup):
+            gg.ppr(g, rs, iters=1, host=False)
+        ts = []
+        for _ in range(a.reps):
+            st = gg.RunStats()
+            gg.ppr(g, rs, iters=a.iters, host=False, stats=st)
+            ts.append(st.total_ms / max(a.iters, 1))
+        out.update(seeds=len(rs), ms_per_iter=round(float(np.median(ts)), 4))
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -760,7 +869,22 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-traversal measurements")
     ap.add_argument("--no-precision", action="store_true", help="skip the PageRank precision workloads")
     ap.add_argument("--batch-graphs", type=int, default=2000, help="small graphs in the union workload")
+    # single workloads for profilers
+    ap.add_argument("--case", default=None, choices=["bfs", "pr", "cc", "msbfs", "ppr"],
+                    help="run one workload for a profiler instead of the benchmark")
+    ap.add_argument("--graph", default="rmat", choices=["rmat", "grid", "er"])
+    ap.add_argument("--side", type=int, default=2048)
+    ap.add_argument("--roots", type=int, default=4)
+    ap.add_argument("--format", default="f32", choices=["f32", "bf16", "f16", "fp8", "cfp", "bf16t", "f64"])
+    ap.add_argument("--iters", type=int, default=5)
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--seeds", type=int, default=128)
+    ap.add_argument("--persistent", type=int, default=None, help="tuning knob: device-driven analytics mask")
+    ap.add_argument("--threshold", default="default", choices=["default", "learned"])
+    ap.add_argument("--graph-mode", type=int, default=None, help="tuning knob: graph-driven BFS levels (0/1)")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args)
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     ws, rank, local = dist_setup(args)
     try:

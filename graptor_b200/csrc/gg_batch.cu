@@ -581,8 +581,10 @@ gg_status gg_graph_union(gg_ctx *ctx, gg_graph *const *parts, int k, gg_graph **
     if (!ctx || !parts || k < 1 || !out) return GG_ERR_ARG;
     uint64_t n = 0, m = 0;
     int sym = 1;
+    bool sorted = true;  // a part's rows keep their order, shifted by its vertex base
     for (int i = 0; i < k; ++i) {
         if (!parts[i] || parts[i]->ctx != ctx) return set_error(ctx, GG_ERR_ARG, "gg_graph_union: bad part");
+        sorted &= parts[i]->rows_sorted;
         if (vertex_base) vertex_base[i] = (uint32_t)n;
         n += parts[i]->n;
         m += parts[i]->m;
@@ -609,7 +611,7 @@ gg_status gg_graph_union(gg_ctx *ctx, gg_graph *const *parts, int k, gg_graph **
     ctx->launches++;
     e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { cudaFree(uoff); cudaFree(uadj); return cuda_error(ctx, e, "gg_graph_union"); }
-    return graph_adopt_device_csr(ctx, (uint32_t)n, m, uoff, uadj, sym, out);
+    return graph_adopt_device_csr(ctx, (uint32_t)n, m, uoff, uadj, sym, sorted, out);
 }
 
 }  // extern "C"

@@ -3,7 +3,9 @@
 // Graph storage replaces Graptor's GraphCSx + VEBO/Graptor SIMD layout
 // (include/graptor/graph/GraphCSx.h:293-2262, graph/CGraphVEBOGraptor.h:60-496)
 // with a plain device CSR (out-edges, used by push) and CSC (in-edges, used by
-// pull): uint64 offsets, uint32 vertex ids, rows sorted.  For symmetric graphs
+// pull): uint64 offsets, uint32 vertex ids; rows are sorted when the graph is
+// built on the device, and uploaded rows are checked (gg_graph::rows_sorted)
+// but kept in the caller's order.  For symmetric graphs
 // the CSC aliases the CSR.  Graph construction (generation, symmetrising,
 // self-loop removal, de-duplication, transposition) runs on the device with a
 // radix sort of packed (row, col) keys.
@@ -817,8 +819,12 @@ gg_status gg_graph_upload(gg_ctx *ctx, uint32_t n, uint64_t m, const uint64_t *o
     if (off[0] != 0 || off[n] != m) return set_error(ctx, GG_ERR_ARG, "gg_graph_upload: off[0] != 0 or off[n] != m");
     for (uint32_t v = 0; v < n; ++v)
         if (off[v] > off[v + 1]) return set_error(ctx, GG_ERR_ARG, "gg_graph_upload: offsets not monotone");
-    for (uint64_t e = 0; e < m; ++e)
-        if (adj[e] >= n) return set_error(ctx, GG_ERR_ARG, "gg_graph_upload: vertex id out of range");
+    bool sorted = true;  // min-id hooking stops a row at its first larger id when rows are sorted
+    for (uint32_t v = 0; v < n; ++v)
+        for (uint64_t e = off[v]; e < off[v + 1]; ++e) {
+            if (adj[e] >= n) return set_error(ctx, GG_ERR_ARG, "gg_graph_upload: vertex id out of range");
+            if (e > off[v] && adj[e] < adj[e - 1]) sorted = false;
+        }
     GG_CUDA(ctx, cudaSetDevice(ctx->device));
     gg_graph *g = new (std::nothrow) gg_graph;
     if (!g) return GG_ERR_OOM;
@@ -826,6 +832,7 @@ gg_status gg_graph_upload(gg_ctx *ctx, uint32_t n, uint64_t m, const uint64_t *o
     g->n = n;
     g->m = m;
     g->symmetric = symmetric ? 1 : 0;
+    g->rows_sorted = sorted;
     cudaError_t e;
     if ((e = cudaMalloc(&g->off, ((size_t)n + 1) * 8)) != cudaSuccess ||
         (e = cudaMalloc(&g->adj, (m ? m : 1) * 4)) != cudaSuccess ||
@@ -845,7 +852,7 @@ gg_status gg_graph_upload(gg_ctx *ctx, uint32_t n, uint64_t m, const uint64_t *o
 namespace gg {
 // Takes ownership of a CSR already in device memory (off: n+1, adj: m).
 gg_status graph_adopt_device_csr(gg_ctx *ctx, uint32_t n, uint64_t m, uint64_t *off, uint32_t *adj, int symmetric,
-                                 gg_graph **out) {
+                                 bool rows_sorted, gg_graph **out) {
     *out = nullptr;
     gg_graph *g = new (std::nothrow) gg_graph;
     if (!g) {
@@ -857,6 +864,7 @@ gg_status graph_adopt_device_csr(gg_ctx *ctx, uint32_t n, uint64_t m, uint64_t *
     g->n = n;
     g->m = m;
     g->symmetric = symmetric ? 1 : 0;
+    g->rows_sorted = rows_sorted;
     g->off = off;
     g->adj = adj;
     gg_status s = graph_finish(g);
@@ -914,7 +922,7 @@ static gg_status graph_from_keys(gg_ctx *ctx, uint32_t n, uint64_t *keys, uint64
     gg_status s = build_from_keys(ctx, n, keys, nk, lg, &off, &adj, &m);
     cudaFree(keys);
     if (s != GG_OK) return s;
-    return graph_adopt_device_csr(ctx, n, m, off, adj, sym, out);
+    return graph_adopt_device_csr(ctx, n, m, off, adj, sym, true, out);  // keys sorted: rows ascending
 }
 
 gg_status gg_graph_from_edges(gg_ctx *ctx, uint32_t n, uint64_t nedges, const uint32_t *src, const uint32_t *dst,
@@ -1096,6 +1104,7 @@ gg_status gg_graph_generate(gg_ctx *ctx, const gg_gen_params *p, gg_graph **out)
     g->ctx = ctx;
     g->n = n;
     g->symmetric = symmetric;
+    g->rows_sorted = true;  // built from sorted (row, col) keys
     gg_status s = build_from_keys(ctx, n, keys, nk, lg, &g->off, &g->adj, &g->m);
     cudaFree(keys);
     if (s != GG_OK) { graph_free(g); return s; }

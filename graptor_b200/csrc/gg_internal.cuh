@@ -125,6 +125,7 @@ struct gg_graph {
     uint32_t n = 0;
     uint64_t m = 0;
     int symmetric = 0;
+    bool rows_sorted = false;    // every CSR row ascending (device-built graphs; checked on upload)
     uint64_t *off = nullptr;     // CSR offsets [n+1]
     uint32_t *adj = nullptr;     // CSR targets [m]
     uint64_t *in_off = nullptr;  // CSC (== off when symmetric)
@@ -193,6 +194,7 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
                               const uint32_t *d_roots = nullptr, uint32_t nroots = 0,
                               const PersistResume *resume = nullptr);
 gg_status graph_adopt_device_csr(gg_ctx *ctx, uint32_t n, uint64_t m, uint64_t *off, uint32_t *adj, int symmetric,
+                                 bool rows_sorted,
                                  gg_graph **out);
 gg_status graph_gini(gg_graph *g, float *out);
 void graph_bfs_free(gg_graph *g);

@@ -22,21 +22,23 @@
 //     last call's contents; each call clears what must start at zero.  Calls
 //     whose work overlaps on the GPU (different streams or host threads)
 //     race on it and must be serialised by the caller.
-//   * The first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture begins.
+//   * Every call looks up the array's device address with
+//     cudaGetSymbolAddress, with the caller's device current.  The address
+//     belongs to the current context: after cudaDeviceReset, or under a second
+//     context that a driver-API caller created on the same device, the module
+//     is loaded again at another address, so no address is kept between calls.
+//     The first call on a device also loads the module there; make that first
+//     call before any stream capture begins.
 #include <cuda_runtime.h>
 
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "gg.h"
 
 namespace {
 
 constexpr uint32_t kMaxV = GG_NOALLOC_MAX_VERTICES;
-constexpr int kMaxDevices = 64;
 // [0, kMaxV)        frontier queue A
 // [kMaxV, 2 kMaxV)  frontier queue B
 // [2 kMaxV + 0]     length of the queue being written
@@ -44,9 +46,6 @@ constexpr int kMaxDevices = 64;
 constexpr size_t kWords = 2 * (size_t)kMaxV + 64;
 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kWords];
-
-std::mutex g_setup_mu;
-void *g_scratch_ptr[kMaxDevices] = {nullptr};
 
 void put_err(char *buf, size_t len, const char *msg) {
     if (buf && len) {
@@ -123,33 +122,32 @@ extern "C" gg_status gg_bfs_level_noalloc(const uint64_t *d_off, const uint32_t 
         return GG_ERR_ARG;
     }
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess) {
         cudaGetLastError();
         put_err(err, err_len, "gg_bfs_level_noalloc: no current CUDA device");
         return GG_ERR_NOT_FOUND;
     }
-    uint32_t *scratch;
+    // The host-side name of a __device__ array is not its device address:
+    // look the address up in the current context.
+    void *sp = nullptr;
     {
-        // once per device, with that device current: the host-side name of a
-        // __device__ array is not its device address
-        std::lock_guard<std::mutex> lk(g_setup_mu);
-        if (!g_scratch_ptr[dev]) {
-            void *p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess || !p) {
-                cudaGetLastError();
-                put_err(err, err_len, "gg_bfs_level_noalloc: cudaGetSymbolAddress failed");
-                return GG_ERR_CUDA;
-            }
-            g_scratch_ptr[dev] = p;
+        cudaError_t e = cudaGetSymbolAddress(&sp, g_noalloc_scratch);
+        if (e != cudaSuccess || !sp) {
+            cudaGetLastError();
+            put_err(err, err_len, "gg_bfs_level_noalloc: cudaGetSymbolAddress failed");
+            return GG_ERR_CUDA;
         }
-        scratch = (uint32_t *)g_scratch_ptr[dev];
     }
+    uint32_t *scratch = (uint32_t *)sp;
     cudaStream_t st = (cudaStream_t)cuda_stream;
     uint32_t *qa = scratch, *qb = scratch + kMaxV, *ctl = scratch + 2 * (size_t)kMaxV;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     k_na_init<<<sms * 4, 256, 0, st>>>(d_level, n, root, qa, ctl);
+    {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) { put_err(err, err_len, cudaGetErrorString(e)); return GG_ERR_CUDA; }
+    }
     uint32_t ncur = 1;
     int it = 0;
     uint32_t *cur = qa, *next = qb;
@@ -159,6 +157,7 @@ extern "C" gg_status gg_bfs_level_noalloc(const uint64_t *d_off, const uint32_t 
         uint32_t warps = ncur, blocks = (warps + 7) / 8;
         if (blocks > (uint32_t)sms * 8) blocks = (uint32_t)sms * 8;
         k_na_push<<<blocks, 256, 0, st>>>(d_off, d_adj, n, d_level, cur, ncur, next, ctl, it);
+        if ((e = cudaGetLastError()) != cudaSuccess) { put_err(err, err_len, cudaGetErrorString(e)); return GG_ERR_CUDA; }
         uint32_t hctl[2] = {0, 0};
         e = cudaMemcpyAsync(hctl, ctl, sizeof(hctl), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -106,6 +106,7 @@ struct PArgs {
     int force_iter, force_variant;     // timing collection: one forced (iteration, variant)
     int fusion;                        // sparse pushes run fused (asynchronous) through wq
     int hook;                          // CC: road-network test after step 0, then hooking
+    int rows_sorted;                   // CSR rows ascending: hooking stops a row at its first larger id
     uint32_t *wq;                      // fused push work queue, wq_cap entries, all kWqEmpty between phases
     unsigned long long wq_cap;
     int iter0;                         // iterations done before this launch (a resumed run)
@@ -560,7 +561,10 @@ __device__ void phase_hook(const PArgs &P) {
         if (!longrow)
             for (uint64_t e = beg; e < end; ++e) {
                 const uint32_t v = __ldg(P.adj + e);
-                if (v >= u) break;  // rows are sorted: the rest are larger
+                if (v >= u) {
+                    if (P.rows_sorted) break;  // the rest of the row is larger
+                    continue;
+                }
                 uf_hook(lab, u, v);
             }
         unsigned pend = __ballot_sync(FULLP, longrow);
@@ -1592,6 +1596,7 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
     // CC of a symmetric graph: road-network test after step 0, then hooking
     P.hook = t.cc_hook && d.relax == GG_RELAX_MIN_U32 && d.dst_filter == GG_FILTER_NE_ZERO && g->symmetric &&
              start_all && force_iter < 0 && g->force_iter < 0 && g->n > 0;
+    P.rows_sorted = g->rows_sorted ? 1 : 0;
     // fused sparse pushes (CC): the queue holds up to 2n + 64Ki entries, more spill
     P.fusion = (t.fusion & 4) && d.relax == GG_RELAX_MIN_U32 && d.dst_filter == GG_FILTER_NE_ZERO;
     if (P.fusion) {

@@ -387,9 +387,12 @@ GG_API gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x, flo
 /*     Every call on a device shares it and each call clears what must */
 /*     start at zero; calls that overlap on the GPU (other streams or  */
 /*     host threads) race on it, so the caller must serialise them.    */
-/*   - The first call on a device looks up the array's device address  */
-/*     (cudaGetSymbolAddress, once per device); make that first call   */
-/*     before any stream capture begins.                               */
+/*   - Every call looks up the array's device address in the current   */
+/*     context (cudaGetSymbolAddress), so the address stays right after*/
+/*     cudaDeviceReset or under a second context on the same device.  */
+/*     The first call on a device also loads the module there; make    */
+/*     that first call before any stream capture begins.               */
+/*   - An adjacency entry >= n is skipped and reported: GG_ERR_ARG.    */
 /*   - The call synchronises cuda_stream once per BFS level.           */
 /* ------------------------------------------------------------------ */
 #define GG_NOALLOC_MAX_VERTICES (1u << 20)

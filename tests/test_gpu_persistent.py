@@ -118,19 +118,38 @@ def test_fused_cc_exact(ctx, fusion_knobs, gen, queue):
     g.close()
 
 
-@pytest.mark.parametrize("gen", ["rmat", "grid", "union", "edgeless"])
+def _shuffled_rows(og, seed):
+    """The same graph with every adjacency row in a random order (a valid
+    symmetric CSR that a caller may upload)."""
+    rng = np.random.default_rng(seed)
+    adj = og.adj.copy()
+    for v in range(og.n):
+        b, e = int(og.off[v]), int(og.off[v + 1])
+        if e - b > 1:
+            adj[b:e] = rng.permutation(adj[b:e])
+    return adj
+
+
+@pytest.mark.parametrize("gen", ["rmat", "grid", "grid_shuffled", "union", "edgeless"])
 def test_cc_hooking_exact(ctx, fusion_knobs, gen):
     from oracle import batch_oracle as B
+    adj = None
     if gen == "rmat":
         og = O.rmat(14, 16 << 14, seed=63)
     elif gen == "grid":
         og = O.grid(120, 130, seed=6, del_bp=400)
+    elif gen == "grid_shuffled":
+        # unsorted rows: hooking must not stop a row at its first larger id
+        og = O.grid(120, 130, seed=8, del_bp=400)
+        adj = _shuffled_rows(og, 9)
+        assert not all(np.all(np.diff(adj[og.off[v]:og.off[v + 1]].astype(np.int64)) > 0)
+                       for v in range(og.n))
     elif gen == "union":
         og, _ = B.union([O.grid(20 + i, 30, seed=i, del_bp=500) for i in range(8)] +
                         [O.rmat(10, 12 << 10, seed=i) for i in range(8)] + [O.from_edges(9, [])])
     else:
         og = O.from_edges(50, [(1, 2), (3, 4)])
-    g = ctx.upload(og.off, og.adj)
+    g = ctx.upload(og.off, og.adj if adj is None else adj)
     ref = O.cc(og)
     gg.tuning_set("persistent", 4)
     st = {}
