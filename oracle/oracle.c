@@ -535,6 +535,21 @@ ORC_API float orc_cfp_to_float(uint32_t c, int S, int E, int M) {
     return f;
 }
 
+/* Array form on raw float bit patterns (no float->double round trip, so
+ * signalling NaNs keep their bits): codes[i] = encode(in[i]) and
+ * dec_bits[i] = bits of decode(codes[i]). */
+ORC_API void orc_cfp_convert_bits(const uint32_t *in, uint64_t k, int S, int E, int M,
+                                  uint32_t *codes, uint32_t *dec_bits) {
+    for (uint64_t i = 0; i < k; ++i) {
+        float f;
+        memcpy(&f, in + i, 4);
+        uint32_t c = orc_cfp_from_float(f, S, E, M);
+        float d = orc_cfp_to_float(c, S, E, M);
+        codes[i] = c;
+        memcpy(dec_bits + i, &d, 4);
+    }
+}
+
 /* Storage formats of the PageRank contribution vector in the
  * reduced-precision runs.  The cfp ones restate the reference
  * (PR_vary.C:511-570); the others are the GPU library's own formats:

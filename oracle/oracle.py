@@ -61,6 +61,8 @@ def lib() -> C.CDLL:
         L.orc_cfp_from_float.restype = C.c_uint32
         L.orc_cfp_to_float.argtypes = [C.c_uint32, C.c_int, C.c_int, C.c_int]
         L.orc_cfp_to_float.restype = C.c_float
+        L.orc_cfp_convert_bits.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int,
+                                           C.c_void_p, C.c_void_p]
         L.orc_free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
@@ -221,6 +223,16 @@ def cfp_to_float(c: int, S: int, E: int, M: int) -> float:
     return float(lib().orc_cfp_to_float(c, S, E, M))
 
 
+def cfp_convert_bits(bits: np.ndarray, S: int, E: int, M: int):
+    """Encode the float bit patterns `bits` (uint32) into customfp<S,E,M>
+    and decode them again: returns (codes, decoded float bit patterns)."""
+    b = np.ascontiguousarray(bits, dtype=np.uint32)
+    codes = np.empty_like(b)
+    dec = np.empty_like(b)
+    lib().orc_cfp_convert_bits(_p(b), len(b), S, E, M, _p(codes), _p(dec))
+    return codes, dec
+
+
 # ---------------------------------------------------------------------------
 # The reference's own programs, built from its sources by oracle/Makefile.
 # ---------------------------------------------------------------------------
@@ -244,14 +256,14 @@ def ref_available(name: str = "ref_bfslvl") -> bool:
     return ref_prog(name) is not None
 
 
-def _run(args, threads: int | None = None, timeout: int = 1800) -> str:
+def _run(args, threads: int | None = None, timeout: int = 1800, stderr: bool = False):
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
     r = subprocess.run(args, capture_output=True, text=True, env=env, timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError(f"{args[0]} failed rc={r.returncode}: {r.stderr[-2000:]}")
-    return r.stdout
+    return (r.stdout, r.stderr) if stderr else r.stdout
 
 
 class PaddedGraph(RuntimeError):
@@ -303,15 +315,20 @@ def ref_cc(bin_path: str, out_path: str, threads: int | None = None, rounds: int
 
 
 def ref_pr(bin_path: str, out_path: str, maxiter: int = 20, threads: int | None = None,
-           prog_name: str = "PRv", symmetric: bool = True, rounds: int = 1):
-    """Reference PRv / PR_vary: returns (x float64 array, [round seconds])."""
+           prog_name: str = "PRv", symmetric: bool = True, rounds: int = 1, iterations: bool = False):
+    """Reference PRv / PR_vary: returns (x float64 array, [round seconds]), and
+    with iterations=True also the iteration count of the last round (read from
+    the per-iteration report that -itimes enables)."""
     prog = ref_prog(prog_name)
     args = [prog] + (["-s"] if symmetric else []) + [
         "-b", "-rounds", str(rounds), "-c", "256", "-pr:maxiter", str(maxiter),
-        "-pr:outfile", out_path, bin_path]
-    txt = _run(args, threads)
+        "-pr:outfile", out_path] + (["-itimes"] if iterations else []) + [bin_path]
+    txt, err = _run(args, threads, stderr=True)
     x = np.loadtxt(out_path, dtype=np.float64)
     n = int(np.fromfile(bin_path, dtype=np.uint64, count=3)[2])
     if len(x) != n:
         raise PaddedGraph(f"reference padded {n} vertices to {len(x)}")
-    return x, _running_times(txt)
+    if not iterations:
+        return x, _running_times(txt)
+    its = [int(l.split("iterations:")[1].split()[0]) for l in err.splitlines() if "iterations:" in l]
+    return x, _running_times(txt), (its[-1] if its else None)

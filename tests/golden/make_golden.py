@@ -6,6 +6,14 @@ programs on it, compiled from the reference sources by oracle/Makefile:
   bfsv_parents - BFSv.C per root (any valid BFS tree; checked, not compared)
   cc           - CCv.C -cc:outfile (canonical min-original-id labels)
   pr           - PRv.C -pr:outfile after pr_iters iterations
+  pr_vary_<V>  - PR_vary.C -pr:outfile for VARIANT V (to the 1e-7 residual or
+                 100 iterations), with pr_vary_<V>_iters its iteration count:
+                 4620 (customfp<6,10> with float sums to 1e-3, then FP32 with
+                 double sums), 99 (bfloat16-by-truncation contributions, float
+                 sums) and 11 (FP64 throughout)
+customfp_sweep.npz holds float bit patterns and, per pattern, the codes and
+decoded floats of the reference's customfp<6,10> and scustomfp<true,8,7>
+conversions (harness oracle/harness/ref_cfp.C).
 The config-1 workload (R-MAT scale 16, 2^20 edges) is stored without its CSR
 (7 MB): the fixture keeps the CSR's SHA-256 and the generator parameters.
 
@@ -14,6 +22,7 @@ Run (needs the reference tree and `make -C oracle ref`):
 """
 import hashlib
 import os
+import subprocess
 import sys
 import tempfile
 
@@ -39,6 +48,9 @@ def roots_for(g, k, seed):
     return sorted(set(r), key=r.index)
 
 
+PR_VARY = {"4620": "PR_vary", "99": "PR_vary_99", "11": "PR_vary_11"}
+
+
 def run_reference(g, roots, pr_iters, tmp):
     p = os.path.join(tmp, "g.bin")
     O.write_bin(g, p)
@@ -46,19 +58,24 @@ def run_reference(g, roots, pr_iters, tmp):
     pa = O.ref_bfs(p, roots, out_prefix=os.path.join(tmp, "pa"), parents=True)
     cc, _ = O.ref_cc(p, os.path.join(tmp, "cc.txt"))
     pr, _ = O.ref_pr(p, os.path.join(tmp, "pr.txt"), maxiter=pr_iters)
+    vary = {}
+    for v, prog in PR_VARY.items():
+        x, _, it = O.ref_pr(p, os.path.join(tmp, "prv.txt"), maxiter=100, prog_name=prog, iterations=True)
+        vary[f"pr_vary_{v}"] = x.astype(np.float64)
+        vary[f"pr_vary_{v}_iters"] = np.int64(it)
     levels = np.stack([a for _, _, _, a in lv]).astype(np.int32)
     parents = np.stack([a for _, _, _, a in pa]).view(np.uint32)
-    return levels, parents, cc.astype(np.uint32), pr
+    return levels, parents, cc.astype(np.uint32), pr, vary
 
 
 def save(name, g, roots, pr_iters, tmp, store_csr=True, params=None):
-    levels, parents, cc, pr = run_reference(g, roots, pr_iters, tmp)
+    levels, parents, cc, pr, vary = run_reference(g, roots, pr_iters, tmp)
     # sanity: the restatement must agree before a fixture is written
     for r, l in zip(roots, levels):
         assert np.array_equal(O.bfs_level(g, r), l), name
     d = dict(n=np.int64(g.n), m=np.int64(g.m), bfs_roots=np.array(roots, dtype=np.uint32),
              bfs_levels=levels, bfsv_parents=parents, cc=cc, pr=pr.astype(np.float64),
-             pr_iters=np.int64(pr_iters), sha256=np.array(csr_sha256(g.off, g.adj)))
+             pr_iters=np.int64(pr_iters), sha256=np.array(csr_sha256(g.off, g.adj)), **vary)
     if store_csr:
         d.update(off=g.off, adj=g.adj)
     if params:
@@ -67,10 +84,31 @@ def save(name, g, roots, pr_iters, tmp, store_csr=True, params=None):
     print(name, g.n, g.m, "roots", roots)
 
 
+def save_customfp_sweep(tmp):
+    """Float bit patterns (special values, every exponent with a few
+    mantissas, random patterns) and the reference's conversions of each."""
+    rng = np.random.default_rng(2024)
+    special = [0x00000000, 0x80000000, 0x3F800000, 0xBF800000, 0x40000000, 0x3FFFFFFF, 0x7F7FFFFF,
+               0x7F800000, 0xFF800000, 0x7FC00000, 0x7F800001, 0x00000001, 0x007FFFFF, 0x00800000,
+               0x1F800000, 0x20000000, 0x207FFFFF, 0x3F7FFFFF]
+    exps = [(e << 23) | int(mt) for e in range(256) for mt in rng.integers(0, 1 << 23, size=8)]
+    signs = [x | 0x80000000 for x in exps[::3]]
+    rand = [int(x) for x in rng.integers(0, 1 << 32, size=4096, dtype=np.uint64)]
+    bits = np.array(special + exps + signs + rand, dtype=np.uint32)
+    i, o = os.path.join(tmp, "cfp.in"), os.path.join(tmp, "cfp.out")
+    bits.tofile(i)
+    subprocess.run([O.ref_prog("ref_cfp"), i, o], check=True)
+    ref = np.fromfile(o, dtype=np.uint32).reshape(-1, 4)
+    np.savez_compressed(os.path.join(HERE, "customfp_sweep.npz"), bits=bits, cfp_6_10_code=ref[:, 0],
+                        cfp_6_10_dec=ref[:, 1], bf16t_code=ref[:, 2], bf16t_dec=ref[:, 3])
+    print("customfp_sweep", len(bits))
+
+
 def main():
     if not O.ref_available("ref_bfslvl"):
         raise SystemExit("reference build missing: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
+        save_customfp_sweep(tmp)
         g = O.rmat(10, 8 << 10, seed=11)
         save("rmat10_ef8", g, roots_for(g, 3, 1), 20, tmp)
         g = O.rmat(12, 16 << 12, seed=12)

@@ -36,7 +36,7 @@ def upload(ctx, g, symmetric=True):
 
 def golden_names():
     return [os.path.basename(p)[:-4] for p in sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
-            if "config1" not in p]
+            if "config1" not in p and "customfp" not in p]
 
 
 def test_generator_matches_oracle(ctx):
@@ -67,6 +67,57 @@ def test_golden_bfs_cc_pr(ctx, name):
     assert np.array_equal(g.cc(), z["cc"])
     x = g.pagerank(maxiter=int(z["pr_iters"]), contrib=gg.F32, accum_f64=True, renorm_f32=True)
     assert np.abs(x.astype(np.float64) - z["pr"]).sum() <= PR_L1_VS_REF_F32
+
+
+# PR_vary VARIANT -> (pagerank keyword arguments, L1 bar against the reference's output)
+PR_VARY_RUNS = {
+    "4620": (dict(renorm_f32=False, stages=[(gg.CFP_6_10, False, 1e-3), (gg.F32, True, 0.0)]), 1e-6),
+    "99": (dict(renorm_f32=False, contrib=gg.BF16_TRUNC, accum_f64=False), 2e-6),
+    "11": (dict(contrib=gg.F64), 1e-11),
+}
+
+
+@pytest.mark.parametrize("variant", ["4620", "99", "11"])
+@pytest.mark.parametrize("name", golden_names())
+def test_golden_pr_vary(ctx, name, variant):
+    """PR_vary's storage formats and staged run against the reference's own
+    PR_vary builds (PR_vary.C:652-757): VARIANT 4620 (customfp<6,10>, then
+    FP32), 99 (bfloat16 by truncation) and 11 (FP64), each to the 1e-7
+    residual or 100 iterations."""
+    z = golden(name)
+    g = ctx.upload(z["off"], z["adj"], True)
+    kw, bar = PR_VARY_RUNS[variant]
+    st = gg.RunStats()
+    x = g.pagerank(maxiter=100, tol=1e-7, stats=st, **kw)
+    ref, its = z[f"pr_vary_{variant}"], int(z[f"pr_vary_{variant}_iters"])
+    assert abs(st.iterations - its) <= 1, (st.iterations, its)
+    assert np.abs(x.astype(np.float64) - ref).sum() <= bar
+
+
+def test_customfp_conversions_match_reference(ctx):
+    """The device's customfp<6,10> and scustomfp<true,8,7> stores and loads
+    (vertex-map property conversions) against the reference's conversion
+    class on the finite values of the committed sweep."""
+    z = golden("customfp_sweep")
+    bits = z["bits"]
+    f = bits.view(np.float32)
+    keep = np.isfinite(f)
+    bits, f = bits[keep], f[keep]
+    n = len(f)
+    g = ctx.upload(np.zeros(n + 1, dtype=np.uint64), np.zeros(0, dtype=np.uint32), True)
+    for dt, code_key, dec_key in ((gg.CFP_6_10, "cfp_6_10_code", "cfp_6_10_dec"),
+                                  (gg.BF16_TRUNC, "bf16t_code", "bf16t_dec")):
+        src, enc, dec = g.prop(gg.F32), g.prop(dt), g.prop(gg.F32)
+        src.upload(f)
+        d = gg.VmapDesc()
+        prog = [(gg.VM_LOAD, 0), (gg.VM_STORE, 1), (gg.VM_LOAD, 1), (gg.VM_STORE, 2)]
+        d.ncode = len(prog)
+        for i, (c, a) in enumerate(prog):
+            d.code[i], d.arg[i] = c, a
+        d.props[0], d.props[1], d.props[2] = src.h, enc.h, dec.h
+        g.vertexmap(d)
+        assert np.array_equal(enc.download().astype(np.uint32), z[code_key][keep]), dt
+        assert np.array_equal(dec.download().view(np.uint32), z[dec_key][keep]), dt
 
 
 def test_config1_rmat16(ctx):

@@ -125,7 +125,19 @@ def test_pr_sums_to_one():
 
 
 def golden_files():
-    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+    """The graph fixtures (customfp_sweep.npz holds conversions only)."""
+    return sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz")) if not p.endswith("customfp_sweep.npz"))
+
+
+def golden_graph(z):
+    if "off" in z:
+        return O.Graph(int(z["n"]), z["off"], z["adj"])
+    g = O.rmat(int(z["scale"]), int(z["nedges"]), int(z["seed"]))  # large workload: generator + CSR hash
+    h = hashlib.sha256()
+    h.update(g.off.tobytes())
+    h.update(g.adj.tobytes())
+    assert h.hexdigest() == str(z["sha256"])
+    return g
 
 
 @pytest.mark.parametrize("path", golden_files(), ids=lambda p: os.path.basename(p))
@@ -133,14 +145,7 @@ def test_oracle_matches_reference_golden(path):
     """Pins the restatement: the fixtures hold outputs of the reference's own
     build (BFSLVLv, BFSv, CCv, PRv) on seeded graphs."""
     z = np.load(path)
-    if "off" in z:
-        g = O.Graph(int(z["n"]), z["off"], z["adj"])
-    else:  # large workload stored by generator parameters + CSR hash
-        g = O.rmat(int(z["scale"]), int(z["nedges"]), int(z["seed"]))
-        h = hashlib.sha256()
-        h.update(g.off.tobytes())
-        h.update(g.adj.tobytes())
-        assert h.hexdigest() == str(z["sha256"])
+    g = golden_graph(z)
     for r, lv in zip(z["bfs_roots"], z["bfs_levels"]):
         assert np.array_equal(O.bfs_level(g, int(r)), lv)
     if "bfsv_parents" in z:
@@ -171,3 +176,47 @@ def test_pr_vary_4620_switches_and_converges():
     assert 0 < k < it and d[-1] <= 1e-7
     x64, _, _ = O.pagerank(g, maxiter=100, tol=1e-10, f64=True)
     assert np.abs(x - x64).sum() < 1e-5
+
+
+def test_cfp_restatement_matches_reference_conversions():
+    """customfp<6,10> and scustomfp<true,8,7> (customfp.h:97-166), bit for bit
+    against the reference's own conversion class on a sweep of float bit
+    patterns: every exponent, special values, random patterns."""
+    z = np.load(os.path.join(GOLDEN, "customfp_sweep.npz"))
+    codes, dec = O.cfp_convert_bits(z["bits"], 0, 6, 10)
+    assert np.array_equal(codes, z["cfp_6_10_code"])
+    assert np.array_equal(dec, z["cfp_6_10_dec"])
+    codes, dec = O.cfp_convert_bits(z["bits"], 1, 8, 7)
+    assert np.array_equal(codes, z["bf16t_code"])
+    assert np.array_equal(dec, z["bf16t_dec"])
+
+
+# PR_vary VARIANT -> restatement stages, L1 bar against the reference output.
+# 99 keeps float sums in the restatement's sequential order and matches the
+# reference's output exactly on these graphs; 4620's first stage accumulates
+# in float in a different order than the reference's vector lanes.
+PR_VARY_CASES = {
+    "4620": ([(O.CFP_6_10, False, 1e-3), (O.F32, True, 0.0)], 1e-6),
+    "99": ([(O.BF16_TRUNC, False, 0.0)], 1e-6),
+}
+
+
+@pytest.mark.parametrize("variant", ["4620", "99", "11"])
+@pytest.mark.parametrize("path", golden_files(), ids=lambda p: os.path.basename(p))
+def test_pr_vary_restatement_matches_reference(path, variant):
+    """Pins the PR_vary restatement (PR_vary.C:247-447 run_prec, staged runs
+    652-757) against the reference's PR_vary builds: VARIANT 4620 (the
+    default), 99 (bfloat16 by truncation) and 11 (FP64 throughout)."""
+    z = np.load(path)
+    g = golden_graph(z)
+    ref, its = z[f"pr_vary_{variant}"], int(z[f"pr_vary_{variant}_iters"])
+    if variant == "11":
+        x, it, d = O.pagerank(g, maxiter=100, tol=1e-7, f64=True)
+        bar = 1e-11  # double sums in another order: 1e-12 over 2^16 vertices
+    else:
+        stages, bar = PR_VARY_CASES[variant]
+        x, it, d = O.pagerank_vary_staged(g, stages, maxiter=100, tol=1e-7)
+    # the residual of the last step may fall on either side of 1e-7 with sums
+    # taken in another order: one step more or fewer, and then only there
+    assert it == its or (abs(it - its) == 1 and abs(d[min(it, its) - 1] - 1e-7) < 1e-8), (it, its)
+    assert np.abs(np.asarray(x, dtype=np.float64) - ref).sum() <= bar
