@@ -1172,6 +1172,22 @@ gg_status gg_prop_create(gg_graph *g, gg_dtype t, gg_prop **out) {
     return GG_OK;
 }
 
+gg_status gg_prop_create_managed(gg_graph *g, gg_dtype t, gg_prop **out) {
+    if (!g || !out) return GG_ERR_ARG;
+    size_t esz = dtype_size(t);
+    if (!esz) return set_error(g->ctx, GG_ERR_ARG, "bad dtype");
+    gg_prop *p = new (std::nothrow) gg_prop;
+    if (!p) return GG_ERR_OOM;
+    p->g = g;
+    p->t = t;
+    p->esz = esz;
+    // host code writes the initial values in place; kernels then migrate the pages
+    cudaError_t e = cudaMallocManaged(&p->d, ((size_t)g->n + 1) * esz, cudaMemAttachGlobal);
+    if (e != cudaSuccess) { delete p; return cuda_error(g->ctx, e, "gg_prop_create_managed"); }
+    *out = p;
+    return GG_OK;
+}
+
 gg_status gg_prop_fill(gg_prop *p, const void *value) {
     if (!p || !value) return GG_ERR_ARG;
     uint64_t v = 0;

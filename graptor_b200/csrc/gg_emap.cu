@@ -914,6 +914,80 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
 
 gg_status pr_edgemap_gather(gg_graph *g, const gg_emap_desc *d, gg_frontier *in);
 
+// CCv's validation edgemap (CCv.C:612-617): relax(s, d) = a[d] != a[s] with a
+// reduction record, i.e. d is recorded when an active in-neighbour holds
+// another value; nothing is written.  A warp per 32-vertex word walks the
+// word's in-rows one after the other, the lanes striding each row.
+__global__ void __launch_bounds__(kBlock) k_check_ne(EmapArgs A, const uint32_t *__restrict__ a,
+                                                     const uint32_t *__restrict__ src_bits) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwords = (A.n + 31u) >> 5;
+    const uint32_t nw = (gridDim.x * kBlock) >> 5;
+    unsigned long long nv = 0, ne = 0;
+    for (uint32_t w = (blockIdx.x * kBlock + threadIdx.x) >> 5; w < nwords; w += nw) {
+        bool rec = false;
+        for (uint32_t j = 0; j < 32; ++j) {
+            const uint32_t d = (w << 5) + j;
+            if (d >= A.n) break;
+            const uint32_t ad = a[d];
+            const uint64_t beg = A.in_off[d], end = A.in_off[d + 1];
+            bool found = false;
+            for (uint64_t base = beg; base < end && !found; base += 32) {
+                bool hit = false;
+                if (base + lane < end) {
+                    const uint32_t s = A.in_adj[base + lane];
+                    hit = (!src_bits || dev::bit_test(src_bits, s)) && a[s] != ad;
+                }
+                found = __any_sync(FULL, hit);
+            }
+            if (lane == j) rec = found;
+        }
+        const uint32_t d = (w << 5) + lane;
+        rec = rec && d < A.n;
+        const unsigned bits = __ballot_sync(FULL, rec);
+        if (lane == 0) A.out_bits[w] = bits;
+        emit_out(A, rec, d, nv, ne);
+    }
+    flush_counts<kBlock>(A, nv, ne, 0);
+}
+
+static gg_status check_ne(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_frontier *out) {
+    gg_ctx *ctx = g->ctx;
+    if (d->a->t != GG_U32) return set_error(ctx, GG_ERR_ARG, "NE_CHECK relaxes a uint32 property");
+    if (d->dst_filter != GG_FILTER_NONE) return set_error(ctx, GG_ERR_UNSUPPORTED, "NE_CHECK takes no dst filter");
+    if (!out) return GG_OK;  // nothing is written, so nothing to do without a record
+    EmapArgs A;
+    memset(&A, 0, sizeof(A));
+    A.off = g->off;
+    A.in_off = g->in_off;
+    A.in_adj = g->in_adj;
+    A.n = g->n;
+    const Tuning &t = tuning();
+    A.smax = t.bin_small_max;
+    A.mmax = t.bin_medium_max;
+    const uint32_t *src_bits = nullptr;
+    if (in && !in->all) {
+        GG_CHECK(frontier_ensure_bitmap(in));
+        src_bits = in->bitmap;
+    }
+    GG_CHECK(frontier_alloc_bins(out));
+    GG_CHECK(frontier_alloc_bitmap(out));
+    GG_CHECK(frontier_reset_counts(out));
+    A.out_bits = out->bitmap;
+    A.out_b0 = out->bins[0];
+    A.out_b1 = out->bins[1];
+    A.out_b2 = out->bins[2];
+    A.out_cnt = (unsigned long long *)out->d_cnt;
+    const uint64_t words = ((uint64_t)g->n + 31) / 32;
+    k_check_ne<<<persistent_grid(ctx, words), kBlock, 0, ctx->stream>>>(A, (const uint32_t *)d->a->d, src_bits);
+    GG_LAUNCHED(ctx);
+    out->all = false;
+    out->has_list = true;
+    out->has_bitmap = true;
+    out->host_valid = false;
+    return GG_OK;
+}
+
 gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_frontier *out,
                        gg_emap_stats *stats) {
     gg_ctx *ctx = g->ctx;
@@ -930,6 +1004,15 @@ gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_f
             stats->nactv_in = g->n;
             stats->nacte_in = g->m;
             stats->scanned = g->m;
+        }
+        return GG_OK;
+    }
+    if (d->relax == GG_RELAX_NE_CHECK) {
+        if (d->record != GG_RECORD_REDUCTION && out) return set_error(ctx, GG_ERR_UNSUPPORTED, "NE_CHECK records by reduction");
+        GG_CHECK(check_ne(g, d, in, out));
+        if (stats) {
+            memset(stats, 0, sizeof(*stats));
+            stats->variant = GG_VAR_PULL_DENSE;
         }
         return GG_OK;
     }

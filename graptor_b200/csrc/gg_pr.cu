@@ -662,6 +662,9 @@ gg_status pr_edgemap_gather(gg_graph *g, const gg_emap_desc *d, gg_frontier *in)
     case GG_FP8E4M3: return gather_api<GG_FP8E4M3>(g, d);
     case GG_CFP_6_10: return gather_api<GG_CFP_6_10>(g, d);
     case GG_BF16_TRUNC: return gather_api<GG_BF16_TRUNC>(g, d);
+    case GG_F64:  // PR_vary VARIANT 11: double contributions, double sums
+        if (!d->accum_f64) return set_error(ctx, GG_ERR_UNSUPPORTED, "double contributions take double sums");
+        return gather_api<GG_F64>(g, d);
     default: return set_error(ctx, GG_ERR_UNSUPPORTED, "contribution dtype");
     }
 }

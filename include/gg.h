@@ -148,6 +148,11 @@ GG_API gg_status gg_prop_download(gg_prop *p, void *host);
 GG_API gg_status gg_prop_upload(gg_prop *p, const void *host);
 GG_API gg_status gg_prop_device_ptr(gg_prop *p, void **dptr);
 GG_API gg_status gg_prop_destroy(gg_prop *p);                             /* vertexprop::del */
+/* A property whose storage is CUDA managed memory: gg_prop_device_ptr returns
+ * an address that host code may also read and write (between library calls,
+ * after gg_ctx_sync).  Replaces mmap_ptr<T>::allocate(numa_allocation_partitioned)
+ * (mm.h:741-745), whose arrays the reference's analytics index from host code. */
+GG_API gg_status gg_prop_create_managed(gg_graph *g, gg_dtype t, gg_prop **out);
 
 /* ------------------------------------------------------------------ */
 /* Frontiers (frontier/frontier.h:58-716).  A frontier holds a        */
@@ -175,7 +180,9 @@ typedef enum gg_relax_kind {
     GG_RELAX_MIN_PLUS1_I32 = 0, /* a[d].min(a[s] + _1) on int32      (BFSLVLv.C:209-215) */
     GG_RELAX_MIN_U32 = 1,       /* a[d].min(a[s]) on uint32          (CCv.C:575-581)     */
     GG_RELAX_SETIF_U32 = 2,     /* a[d].setif(s): a[d] = s once      (BFSv.C:144-146)    */
-    GG_RELAX_ADD_GATHER = 3     /* y[d] += cast(contrib[s])          (PRv.C:202-212)     */
+    GG_RELAX_ADD_GATHER = 3,    /* y[d] += cast(contrib[s])          (PRv.C:202-212)     */
+    GG_RELAX_NE_CHECK = 4       /* a[d] != a[s] on uint32: records d, writes nothing
+                                   (CCv.C:612-617, the validation edgemap)            */
 } gg_relax_kind;
 
 /* dst filters (api::filter(weak, dst, lambda), api.h:687-706). */

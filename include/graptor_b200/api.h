@@ -86,6 +86,26 @@ inline std::map<const void *, gg_prop *> &registry() {
     return r;
 }
 
+// Host code reads and writes managed arrays (mmap_ptr) in place; before it
+// does, the device work queued since the last wait must have finished.
+inline uint64_t &synced_epoch() {
+    static uint64_t e = 0;
+    return e;
+}
+inline void host_sync() {
+    if (synced_epoch() != device_epoch() && ctx_slot()) {
+        check(gg_ctx_sync(ctx_slot()), "gg_ctx_sync");
+        synced_epoch() = device_epoch();
+    }
+}
+
+// The graph that frontiers made from host vertex lists (frontier::sparse)
+// belong to: the last graph built, as the analytics use one graph at a time.
+inline gg_graph *&default_graph() {
+    static gg_graph *g = nullptr;
+    return g;
+}
+
 }  // namespace graptor_b200
 
 // ---------------------------------------------------------------------------
@@ -107,10 +127,51 @@ private:
     VID n_ = 0;
 };
 
+// Host view of the CSR (GraphCSx accessors the analytics call through
+// GA.getCSR(), graph/GraphCSx.h:293-420): index and edges in host memory,
+// the degree array in managed memory registered as a vertex property, so
+// that it serves both host reads and expr::array_ro(getDegree()) operands
+// (PRv.C:46,150; the reference's expr::aid_graph_degree).
+class GraphCSxView {
+public:
+    VID numVertices() const { return n_; }
+    EID numEdges() const { return m_; }
+    const EID *getIndex() const { return off_.data(); }
+    const VID *getEdges() const { return adj_.data(); }
+    const VID *getDegree() const { graptor_b200::host_sync(); return deg_; }
+    VID getDegree(VID v) const { graptor_b200::host_sync(); return deg_[v]; }
+    bool isSymmetric() const { return sym_; }
+
+private:
+    friend class GraphGPU;
+    VID n_ = 0;
+    EID m_ = 0;
+    bool sym_ = false;
+    std::vector<EID> off_;
+    std::vector<VID> adj_;
+    gg_prop *degp_ = nullptr;
+    VID *deg_ = nullptr;
+};
+
 class GraphGPU {
 public:
     GraphGPU() = default;
     explicit GraphGPU(gg_graph *g) : g_(g) { init(); }
+    // From a host CSR with GraphCSx's accessors (the driver's
+    // createGraph(G, npart, maxVL), bench/driver.C:12-19,110-116); the
+    // partition count and vector length do not apply to the device layout.
+    template <typename CSx, typename = decltype(std::declval<const CSx &>().getIndex())>
+    explicit GraphGPU(const CSx &G, int npart = 0, int maxVL = 0) {
+        (void)npart;
+        (void)maxVL;
+        gg_graph *g = nullptr;
+        graptor_b200::check(gg_graph_upload(graptor_b200::context(), (uint32_t)G.numVertices(),
+                                            (uint64_t)G.numEdges(), (const uint64_t *)G.getIndex(),
+                                            (const uint32_t *)G.getEdges(), G.isSymmetric() ? 1 : 0, &g),
+                            "gg_graph_upload");
+        g_ = g;
+        init();
+    }
     static GraphGPU read_bin(const std::string &path, bool symmetric) {
         gg_graph *g = nullptr;
         graptor_b200::check(gg_graph_read_bin(graptor_b200::context(), path.c_str(), symmetric, &g),
@@ -127,22 +188,52 @@ public:
     EID numEdges() const { return m_; }
     bool isSymmetric() const { return sym_ != 0; }
     const partitioner &get_partitioner() const { return part_; }
-    VID getOutDegree(VID v) const {
-        if (!deg_) {
-            std::vector<EID> off((size_t)n_ + 1);
-            graptor_b200::check(gg_graph_download(g_, off.data(), nullptr), "gg_graph_download");
-            deg_ = std::make_shared<std::vector<VID>>(n_);
-            for (VID i = 0; i < n_; ++i) (*deg_)[i] = (VID)(off[i + 1] - off[i]);
+    VID getOutDegree(VID v) const { return getCSR().getDegree(v); }
+    // The CSR in host memory, fetched once on first use.
+    const GraphCSxView &getCSR() const {
+        if (!csr_) {
+            auto c = std::make_shared<GraphCSxView>();
+            c->n_ = n_;
+            c->m_ = m_;
+            c->sym_ = sym_ != 0;
+            c->off_.resize((size_t)n_ + 1);
+            c->adj_.resize(m_ ? m_ : 1);
+            graptor_b200::check(gg_graph_download(g_, c->off_.data(), c->adj_.data()), "gg_graph_download");
+            graptor_b200::check(gg_prop_create_managed(g_, GG_U32, &c->degp_), "gg_prop_create_managed");
+            void *d = nullptr;
+            gg_prop_device_ptr(c->degp_, &d);
+            c->deg_ = (VID *)d;
+            for (VID i = 0; i < n_; ++i) c->deg_[i] = (VID)(c->off_[i + 1] - c->off_[i]);
+            graptor_b200::registry()[d] = c->degp_;
+            csr_ = c;
         }
-        return (*deg_)[v];
+        return *csr_;
     }
+    const GraphCSxView &getCSC() const { return getCSR(); }
     // no vertex renumbering on the device: ids are the file's ids
     VID remapID(VID v) const { return v; }
     VID originalID(VID v) const { return v; }
     gg_graph *handle() const { return g_; }
+    // the layout has no partition fragments to report (GraphVEBOGraptor::fragmentation)
+    void fragmentation() const {}
     void del() {
-        if (g_) gg_graph_destroy(g_);
+        if (csr_ && csr_->degp_) {
+            graptor_b200::registry().erase((const void *)csr_->deg_);
+            gg_prop_destroy(csr_->degp_);
+            csr_->degp_ = nullptr;
+        }
+        csr_.reset();
+        if (g_) {
+            if (graptor_b200::default_graph() == g_) graptor_b200::default_graph() = nullptr;
+            gg_graph_destroy(g_);
+        }
         g_ = nullptr;
+    }
+
+protected:
+    void adopt(gg_graph *g) {
+        g_ = g;
+        init();
     }
 
 private:
@@ -151,14 +242,18 @@ private:
         graptor_b200::check(gg_graph_info(g_, &n_, &m, &sym_), "gg_graph_info");
         m_ = m;
         part_ = partitioner(g_, n_);
+        graptor_b200::default_graph() = g_;
     }
     gg_graph *g_ = nullptr;
     VID n_ = 0;
     EID m_ = 0;
     int sym_ = 0;
     partitioner part_;
-    mutable std::shared_ptr<std::vector<VID>> deg_;
+    mutable std::shared_ptr<GraphCSxView> csr_;
 };
+
+// A W-byte truth value (Graptor's logical<W>, all bits set = true).
+template <unsigned short W> struct logical { unsigned char b[W]; };
 
 // ---------------------------------------------------------------------------
 // Frontier (value handle with manual del(), frontier/frontier.h:58-716)
@@ -195,15 +290,35 @@ public:
         f.nacte_ = m;
         return f;
     }
+    // frontier::sparse(n, k, list): k active vertices from a host array
+    // (frontier.h:236-245); the list is copied, the caller keeps its array
+    static frontier sparse(VID n, VID k, const VID *list) {
+        frontier f;
+        f.kind_ = K_LIST;
+        f.n_ = n;
+        f.list_ = std::make_shared<std::vector<VID>>(list, list + k);
+        return f;
+    }
     static frontier empty() { return frontier(); }
     void del() {
         if (f_) gg_frontier_destroy(f_);
         f_ = nullptr;
         kind_ = K_EMPTY;
     }
-    bool isEmpty() const { return nActiveVertices() == 0; }
-    VID nActiveVertices() const { refresh(); return (VID)nactv_; }
-    EID nActiveEdges() const { refresh(); return nacte_; }
+    bool isEmpty() const {
+        if (kind_ == K_LIST) return list_->empty();
+        return nActiveVertices() == 0;
+    }
+    VID nActiveVertices() const {
+        if (kind_ == K_LIST) return (VID)list_->size();
+        refresh();
+        return (VID)nactv_;
+    }
+    EID nActiveEdges() const {
+        if (kind_ == K_LIST) const_cast<frontier *>(this)->bind(graptor_b200::default_graph());
+        refresh();
+        return nacte_;
+    }
     float density(EID m) const { return m ? float(double(nActiveVertices() + nActiveEdges()) / double(m)) : 0.f; }
     frontier_type getType() const {
         return kind_ == K_ALL ? frontier_type::ft_true : kind_ == K_DEV ? frontier_type::ft_sparse
@@ -212,23 +327,58 @@ public:
     bool is_set(VID v) const {
         if (kind_ == K_ALL) return true;
         if (kind_ == K_SINGLE) return v == v_;
-        if (kind_ != K_DEV) return false;
-        uint64_t k = 0;
-        graptor_b200::check(gg_frontier_download(f_, nullptr, 0, &k), "gg_frontier_download");
-        std::vector<uint32_t> l(k ? k : 1);
-        graptor_b200::check(gg_frontier_download(f_, l.data(), k, &k), "gg_frontier_download");
-        for (uint64_t i = 0; i < k; ++i)
+        const VID *l = getSparse();
+        for (VID i = 0, k = nActiveVertices(); i < k; ++i)
             if (l[i] == v) return true;
         return false;
+    }
+    // The active vertices as a host list (frontier::getSparse, frontier.h:681),
+    // valid until the frontier changes; toSparse() is implied.
+    const VID *getSparse() const {
+        if (kind_ == K_LIST) return list_->data();
+        if (kind_ == K_SINGLE) return &v_;
+        auto h = std::make_shared<std::vector<VID>>();
+        if (kind_ == K_ALL) {
+            h->resize(n_);
+            for (VID v = 0; v < n_; ++v) (*h)[v] = v;
+        } else if (kind_ == K_DEV) {
+            uint64_t k = 0;
+            graptor_b200::check(gg_frontier_download(f_, nullptr, 0, &k), "gg_frontier_download");
+            h->resize(k ? k : 1);
+            graptor_b200::check(gg_frontier_download(f_, h->data(), k, &k), "gg_frontier_download");
+            h->resize(k);
+        }
+        host_ = h;
+        return host_->data();
+    }
+    void toSparse(const partitioner &) const {}
+    // Dense host copy, one W-byte logical per vertex (-1 active, 0 not)
+    // (frontier::getDenseL<W>, frontier.h:664).
+    template <unsigned short W> logical<W> *getDenseL() const {
+        const VID nv = n_ ? n_ : (f_ ? frontier_vertices() : 0);
+        auto d = std::make_shared<std::vector<int64_t>>((nv * W + 7) / 8 + 1, 0);
+        char *b = (char *)d->data();
+        auto set = [&](VID v) { std::memset(b + (size_t)v * W, 0xFF, W); };
+        if (kind_ == K_ALL) {
+            for (VID v = 0; v < nv; ++v) set(v);
+        } else {
+            const VID *l = getSparse();
+            for (VID i = 0, k = nActiveVertices(); i < k; ++i) set(l[i]);
+        }
+        dense_ = d;
+        return (logical<W> *)d->data();
     }
 
     // --- library side ---
     // Device frontier for graph g (materialises a pending single/all frontier).
     gg_frontier *bind(gg_graph *g) {
         if (kind_ == K_DEV) return f_;
+        if (!g) throw graptor_b200::error(GG_ERR_STATE, "frontier used before a graph exists");
         if (!f_) graptor_b200::check(gg_frontier_create(g, &f_), "gg_frontier_create");
         if (kind_ == K_SINGLE) graptor_b200::check(gg_frontier_set_single(f_, v_), "gg_frontier_set_single");
         else if (kind_ == K_ALL) graptor_b200::check(gg_frontier_set_all(f_), "gg_frontier_set_all");
+        else if (kind_ == K_LIST)
+            graptor_b200::check(gg_frontier_set_list(f_, list_->data(), list_->size()), "gg_frontier_set_list");
         else graptor_b200::check(gg_frontier_clear(f_), "gg_frontier_clear");
         kind_ = K_DEV;
         stale_ = true;
@@ -244,7 +394,12 @@ public:
     bool all() const { return kind_ == K_ALL; }
 
 private:
-    enum Kind { K_EMPTY, K_SINGLE, K_ALL, K_DEV };
+    enum Kind { K_EMPTY, K_SINGLE, K_ALL, K_DEV, K_LIST };
+    VID frontier_vertices() const {
+        uint32_t n = 0;
+        graptor_b200::check(gg_graph_info(graptor_b200::default_graph(), &n, nullptr, nullptr), "gg_graph_info");
+        return n;
+    }
     void refresh() const {
         if (kind_ == K_DEV && stale_) {
             uint64_t v = 0, e = 0;
@@ -260,6 +415,9 @@ private:
     mutable uint64_t nactv_ = 0;
     mutable EID nacte_ = 0;
     mutable bool stale_ = false;
+    std::shared_ptr<std::vector<VID>> list_;                 // K_LIST: pending host list
+    mutable std::shared_ptr<std::vector<VID>> host_;         // getSparse() copy
+    mutable std::shared_ptr<std::vector<int64_t>> dense_;    // getDenseL() copy
 };
 
 // ---------------------------------------------------------------------------
@@ -349,8 +507,21 @@ inline E::E(T v) : n_(cst((double)v, literal_dtype<T>()).node()) {}
 
 template <typename T> inline E _c(T v) { return cst((double)v, literal_dtype<T>()); }
 
-#define GG_BINOP(op, kind)                                                             \
-    inline E operator op(const E &a, const E &b) { return E(mk(NK::kind, {a.node(), b.node()})); }
+// Result type of an arithmetic node, as C++ promotes: double if either side
+// is double, else float if either side is float, else the integer type.
+inline gg_dtype promote(gg_dtype a, gg_dtype b) {
+    if (a == GG_F64 || b == GG_F64) return GG_F64;
+    if (a == GG_F32 || b == GG_F32) return GG_F32;
+    return a;
+}
+inline E binop(NK k, const E &a, const E &b) {
+    auto n = mk(k, {a.node(), b.node()});
+    n->dt = (k == NK::Add || k == NK::Sub || k == NK::Mul || k == NK::Div) ? promote(a.node()->dt, b.node()->dt)
+                                                                            : GG_I32;
+    return E(n);
+}
+#define GG_BINOP(op, kind) \
+    inline E operator op(const E &a, const E &b) { return binop(NK::kind, a, b); }
 GG_BINOP(+, Add)
 GG_BINOP(-, Sub)
 GG_BINOP(*, Mul)
@@ -372,18 +543,33 @@ static const E _true = cst(1, GG_I32);
 static const E _false = cst(0, GG_I32);
 
 inline E zero_val(const E &) { return cst(0, GG_I32); }
-template <typename T> inline E constant_val(const E &, T v) { return cst((double)v, literal_dtype<T>()); }
+// constant_val(x, v): v in the type of x (a float operand rounds v to float)
+template <typename T> inline E constant_val(const E &x, T v) {
+    const gg_dtype dt = x.node()->k == NK::Ref || x.node()->k == NK::Cast || x.node()->k == NK::Const
+                            ? x.node()->dt : literal_dtype<T>();
+    return cst(dt == GG_F32 ? (double)(float)v : (double)v, dt);
+}
+// The array id the reference gives the graph's degree array (PRv.C:46).
+constexpr short aid_graph_degree = 127;
 template <typename T> inline E cast(const E &a) {
     auto n = mk(NK::Cast, {a.node()});
     n->dt = literal_dtype<T>();
     return E(n);
 }
-inline E make_unop_abs(const E &a) { return E(mk(NK::Abs, {a.node()})); }
+inline E make_unop_abs(const E &a) {
+    auto n = mk(NK::Abs, {a.node()});
+    n->dt = a.node()->dt;
+    return E(n);
+}
 inline E iif(const E &c, const E &a, const E &b) { return E(mk(NK::Iif, {c.node(), a.node(), b.node()})); }
 inline E msbset(const E &a) { return E(mk(NK::MsbSet, {a.node()})); }
 inline E make_noop() { return E(mk(NK::Noop)); }
 
-inline E var(NK k) { return E(mk(k)); }
+inline E var(NK k) {
+    auto n = mk(k);
+    n->dt = GG_U32;  // vertex ids
+    return E(n);
+}
 
 // Reference to element idx of a device array (or of a host scalar).
 inline E ref(gg_prop *p, double *host, gg_dtype dt, const E &idx) {
@@ -394,36 +580,61 @@ inline E ref(gg_prop *p, double *host, gg_dtype dt, const E &idx) {
     return E(n);
 }
 
-// expr::array_ro<T,VID,AID,Enc>(ptr): a view over a device array registered
-// by mmap_ptr / vertexprop, or over a host scalar (reduction target).
-template <typename T, typename U = VID, short AID = 0, typename Enc = void>
+}  // namespace expr
+
+// Storage encodings (encoding.h / customfp.h types): the 16-bit formats are
+// two-byte words here, used as storage types and template tags.
+template <unsigned short E_, unsigned short M_> struct customfp { uint16_t bits; };
+template <bool S_, unsigned short E_, unsigned short M_, bool Z_, int B_> struct scustomfp { uint16_t bits; };
+template <typename T> struct array_encoding { using stored_type = T; };
+template <typename T, bool = false> struct array_encoding_wide { using stored_type = T; };
+
+namespace graptor_b200 {
+template <> struct dtype_of<customfp<6, 10>> { static constexpr gg_dtype value = GG_CFP_6_10; };
+template <> struct dtype_of<scustomfp<true, 8, 7, false, 0>> { static constexpr gg_dtype value = GG_BF16_TRUNC; };
+template <typename T, typename = void> struct has_dtype : std::false_type {};
+template <typename T> struct has_dtype<T, std::void_t<decltype(dtype_of<T>::value)>> : std::true_type {};
+template <typename T, typename Enc> struct stored_of { using type = typename Enc::stored_type; };
+template <typename T> struct stored_of<T, void> { using type = T; };
+}  // namespace graptor_b200
+
+namespace expr {
+// expr::array_ro<T,VID,AID,Enc>(ptr) (dsl/ast/memref.h:57-110): a view of
+// values of type T over an array stored as Enc::stored_type -- a device
+// array registered by mmap_ptr / vertexprop, or a host scalar (reduction
+// target).  Indexed with an expression it builds a tree; indexed with a
+// VID from host code it reads or writes the (managed) array in place.
+template <typename T, typename U = VID, short AID = 0, typename Enc = array_encoding<T>>
 class array_ro {
 public:
-    explicit array_ro(T *p) {
+    using storage_type = typename graptor_b200::stored_of<T, Enc>::type;
+    array_ro(storage_type *p) : ptr_(p) {
         auto &r = graptor_b200::registry();
         auto it = r.find((const void *)p);
         if (it != r.end()) prop_ = it->second;
         else host_ = reinterpret_cast<double *>(p);
-        static_assert(!std::is_same<T, void>::value, "element type");
-        if (!prop_ && !std::is_same<T, double>::value)
+        if (!prop_ && !std::is_same<storage_type, double>::value)
             throw graptor_b200::error(GG_ERR_UNSUPPORTED, "array_ro over host memory must be a double scalar");
     }
     E operator[](const E &i) const { return ref(prop_, host_, graptor_b200::dtype_of<T>::value, i); }
+    // host writes need no flush: the next kernel, queued after them, sees them
+    storage_type &operator[](VID v) {
+        graptor_b200::host_sync();
+        return ptr_[v];
+    }
+    const storage_type &operator[](VID v) const {
+        graptor_b200::host_sync();
+        return ptr_[v];
+    }
+    storage_type *ptr() const { return ptr_; }
 
 private:
+    storage_type *ptr_ = nullptr;
     gg_prop *prop_ = nullptr;
     double *host_ = nullptr;
 };
 
 }  // namespace expr
-
-// ---------------------------------------------------------------------------
-// Storage encodings (encoding.h / customfp.h types used as template tags)
-// ---------------------------------------------------------------------------
-template <unsigned short E_, unsigned short M_> struct customfp {};
-template <bool S_, unsigned short E_, unsigned short M_, bool Z_, int B_> struct scustomfp {};
-template <typename T> struct array_encoding { using stored_type = T; };
-template <typename T, bool = false> struct array_encoding_wide { using stored_type = T; };
 
 namespace graptor_b200 {
 template <typename T, typename Enc> struct storage_dtype { static constexpr gg_dtype value = dtype_of<T>::value; };
@@ -464,7 +675,12 @@ private:
 };
 }  // namespace graptor_b200
 
-// mmap_ptr<T>: device array of one element per vertex (mm.h), host access by proxy.
+// mmap_ptr<T> (mm.h:680-945): an array of one element per vertex that the
+// analytics index from host code as well as hand to the edgemap.  Element
+// types the device knows live in managed memory (gg_prop_create_managed) and
+// are registered as vertex properties; other types (size_t counters of the
+// host-side helpers) are plain host arrays.  Host indexing first waits for
+// the device work queued so far.
 struct numa_allocation_partitioned {
     explicit numa_allocation_partitioned(const partitioner &p) : part(p) {}
     partitioner part;
@@ -473,20 +689,39 @@ struct numa_allocation_partitioned {
 template <typename T>
 class mmap_ptr {
 public:
+    using type = T;
     void allocate(const numa_allocation_partitioned &a) {
-        graptor_b200::check(gg_prop_create(a.part.graph(), graptor_b200::dtype_of<T>::value, &p_),
-                            "gg_prop_create");
-        void *d = nullptr;
-        gg_prop_device_ptr(p_, &d);
-        graptor_b200::registry()[d] = p_;
-        d_ = (T *)d;
+        if constexpr (graptor_b200::has_dtype<T>::value) {
+            graptor_b200::check(gg_prop_create_managed(a.part.graph(), graptor_b200::dtype_of<T>::value, &p_),
+                                "gg_prop_create_managed");
+            void *d = nullptr;
+            gg_prop_device_ptr(p_, &d);
+            graptor_b200::registry()[d] = p_;
+            d_ = (T *)d;
+        } else {
+            d_ = (T *)std::calloc((size_t)a.part.get_num_vertices() + 1, sizeof(T));
+            if (!d_) throw graptor_b200::error(GG_ERR_OOM, "mmap_ptr host allocation");
+        }
     }
     T *get() const { return d_; }
-    graptor_b200::elem_proxy<T> operator[](VID v) const { return graptor_b200::elem_proxy<T>(p_, v); }
+    operator T *() { return d_; }
+    operator const T *() const { return d_; }
+    explicit operator bool() const { return d_ != nullptr; }
+    // host writes need no flush: the next kernel, queued after them, sees them
+    T &operator[](size_t v) {
+        graptor_b200::host_sync();
+        return d_[v];
+    }
+    const T &operator[](size_t v) const {
+        graptor_b200::host_sync();
+        return d_[v];
+    }
     void del() {
         if (p_) {
             graptor_b200::registry().erase(d_);
             gg_prop_destroy(p_);
+        } else {
+            std::free(d_);
         }
         p_ = nullptr;
         d_ = nullptr;
@@ -685,6 +920,12 @@ inline void lower_relax(const NP &r, gg_emap_desc &d) {
             return;
         }
     }
+    if (r->k == NK::Ne && is_ref_at(r->c[0], NK::VarDst) && is_ref_at(r->c[1], NK::VarSrc) &&
+        r->c[0]->prop == r->c[1]->prop && r->c[0]->dt == GG_U32) {
+        d.relax = GG_RELAX_NE_CHECK;  // a[d] != a[s]: record d, write nothing (CCv.C:612-617)
+        d.a = r->c[0]->prop;
+        return;
+    }
     if (r->k == NK::SetIf && is_ref_at(r->c[0], NK::VarDst) && r->c[1]->k == NK::VarSrc && r->c[0]->dt == GG_U32) {
         d.relax = GG_RELAX_SETIF_U32;  // a[d].setif(s)
         d.a = r->c[0]->prop;
@@ -788,10 +1029,9 @@ struct VmBuilder {
                                                   {NK::Div, GG_VM_DIV}, {NK::Eq, GG_VM_EQ}, {NK::Ne, GG_VM_NE},
                                                   {NK::Lt, GG_VM_LT}, {NK::Gt, GG_VM_GT}};
             if (!value(n->c[0]) || !value(n->c[1]) || !emit(ops.at(n->k))) return false;
-            // float arithmetic on float operands rounds like the reference
-            if (n->c[0]->dt == GG_F32 || n->c[1]->dt == GG_F32) {
-                if (n->k == NK::Add || n->k == NK::Sub || n->k == NK::Mul || n->k == NK::Div) return emit(GG_VM_TOF32);
-            }
+            // float arithmetic (float operands, no double one) rounds like the reference
+            if (n->dt == GG_F32 && (n->k == NK::Add || n->k == NK::Sub || n->k == NK::Mul || n->k == NK::Div))
+                return emit(GG_VM_TOF32);
             return true;
         }
         case NK::Cast: {
@@ -848,6 +1088,17 @@ public:
 
     template <typename Fn> lazy_executor &vertex_map(Fn fn) {
         stmts_.push_back(fn(expr::var(expr::NK::VarV)).node());
+        return *this;
+    }
+    // vertex_map(F, fn): the statement on the vertices of frontier F only
+    // (dsl/vertexmap.h:2190-2230), as its own pass
+    template <typename Fn> lazy_executor &vertex_map(frontier &F, Fn fn) {
+        flush();
+        if (F.isEmpty()) return *this;
+        graptor_b200::VmBuilder b;
+        expr::NP st = fn(expr::var(expr::NK::VarV)).node();
+        if (!b.statement(st)) graptor_b200::unsupported("vertex statement (too long)", st);
+        graptor_b200::run_vmap(part_.graph(), b, F.all() ? nullptr : F.bind(part_.graph()), nullptr);
         return *this;
     }
     template <typename Fn> lazy_executor &vertex_scan(Fn fn) { return vertex_map(fn); }

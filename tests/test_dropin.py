@@ -1,7 +1,11 @@
-"""The reference's own analytics sources (bench/BFSLVLv.C, bench/BFSv.C),
-unmodified, compiled against this library's Graptor-compatible headers
-(graptor_b200/dropin/Makefile) and run on the GPU: their levels must equal
-the oracle's and their parents must form a valid BFS tree."""
+"""The reference's own analytics sources (bench/BFSLVLv.C, BFSv.C, CCv.C,
+PRv.C, PR_vary.C), unmodified, compiled against this library's
+Graptor-compatible headers with the reference's own bench/driver.C as their
+main() (graptor_b200/dropin/Makefile) and run on the GPU: BFS levels equal the
+oracle's, BFS parents form a valid BFS tree, CC labels equal the reference
+build's bit for bit, PageRank ranks are within the stated L1 of the reference
+build's, and every program's own validate() passes."""
+import glob
 import os
 import subprocess
 
@@ -51,3 +55,79 @@ def test_reference_bfsv_source_on_gpu(tmp_path):
     for r in roots:
         lv = O.bfs_level(g, r)
         assert O.check_parents(g, r, out[r].view(np.uint32), lv) == 0
+
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def _golden_graphs():
+    return [os.path.basename(p)[:-4] for p in sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+            if "config1" not in p and "customfp" not in p]
+
+
+def _graph_file(tmp_path, name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    g = O.Graph(int(z["n"]), z["off"], z["adj"])
+    p = str(tmp_path / "g.bin")
+    O.write_bin(g, p)
+    return z, g, p
+
+
+def _driver(prog, args):
+    """Runs a drop-in program through the reference's driver main()."""
+    r = subprocess.run([_prog(prog)] + args, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, (prog, r.stdout[-1000:], r.stderr[-2000:])
+    assert "Running :" in r.stdout, r.stdout[-1000:]
+    return r
+
+
+@pytest.mark.parametrize("name", _golden_graphs())
+def test_reference_ccv_source_on_gpu(tmp_path, name):
+    """CCv.C with its driver: canonical labels (-cc:outfile, CCv.C:591-601)
+    equal the reference build's; its validate() neighbour check passes."""
+    z, g, p = _graph_file(tmp_path, name)
+    out = str(tmp_path / "cc.txt")
+    r = _driver("CCv", ["-s", "-b", "-rounds", "2", "-cc:outfile", out, p])
+    assert "Neighbour check: PASS" in r.stderr, r.stderr[-2000:]
+    lab = np.loadtxt(out, dtype=np.uint64).astype(np.uint32)
+    assert np.array_equal(lab, z["cc"])
+
+
+@pytest.mark.parametrize("name", _golden_graphs())
+def test_reference_prv_source_on_gpu(tmp_path, name):
+    """PRv.C with its driver, 20 iterations: ranks within 1e-6 L1 of the
+    reference build's PRv."""
+    z, g, p = _graph_file(tmp_path, name)
+    out = str(tmp_path / "pr.txt")
+    _driver("PRv", ["-s", "-b", "-rounds", "1", "-pr:maxiter", str(int(z["pr_iters"])), "-pr:outfile", out, p])
+    x = np.loadtxt(out, dtype=np.float64)
+    assert np.abs(x - z["pr"]).sum() <= 1e-6
+
+
+# drop-in program -> (fixture key, L1 bar against the reference build's output)
+PR_VARY_PROGS = {"PR_vary": ("4620", 1e-6), "PR_vary_99": ("99", 2e-6), "PR_vary_11": ("11", 1e-11)}
+
+
+@pytest.mark.parametrize("prog", sorted(PR_VARY_PROGS))
+@pytest.mark.parametrize("name", _golden_graphs())
+def test_reference_pr_vary_source_on_gpu(tmp_path, name, prog):
+    """PR_vary.C with its driver, built for VARIANT 4620 (the default), 99 and
+    11: ranks to the 1e-7 residual against the reference build of the same
+    variant, iteration counts within one."""
+    z, g, p = _graph_file(tmp_path, name)
+    key, bar = PR_VARY_PROGS[prog]
+    out = str(tmp_path / "prv.txt")
+    r = _driver(prog, ["-s", "-b", "-rounds", "1", "-itimes", "-pr:outfile", out, p])
+    its = [int(l.split("iterations:")[1].split()[0]) for l in r.stderr.splitlines() if "iterations:" in l]
+    assert its and abs(its[-1] - int(z[f"pr_vary_{key}_iters"])) <= 1, (its, int(z[f"pr_vary_{key}_iters"]))
+    x = np.loadtxt(out, dtype=np.float64)
+    assert np.abs(x - z[f"pr_vary_{key}"]).sum() <= bar
+
+
+@pytest.mark.parametrize("prog", ["BFSLVLv", "BFSv"])
+def test_reference_bfs_sources_with_their_driver(tmp_path, prog):
+    """BFSLVLv.C / BFSv.C with the reference's driver main() (no harness):
+    runs from -start and its own validate() passes."""
+    z, g, p = _graph_file(tmp_path, "rmat12_ef16")
+    r = _driver(prog, ["-s", "-b", "-rounds", "2", "-start", str(int(z["bfs_roots"][0])), p])
+    assert "FAIL" not in (r.stdout + r.stderr), (r.stdout[-1000:], r.stderr[-1000:])
