@@ -221,6 +221,22 @@ def bfs_bytes(n: int, st, it: int) -> float:
     return 20.0 * F + 8.0 * E + 4.0 * N
 
 
+def cc_bytes(n: int, m: int, st, it: int) -> float:
+    """Algorithmic bytes of CC iteration `it`: a dense pull reads offsets,
+    labels, the scanned in-edges and their sources' labels (8(n+1) + 4n + 8S
+    + 4N + 2n/8); a sparse push 4F + 16F + 4E + 4E + 4N; the hooking step
+    (road-like graphs) one pass over the CSR and the labels (8(n+1) + 4m + 8n)."""
+    from graptor_b200 import gg
+    F, E, S = st.nactv[it], st.nacte[it], st.scanned[it]
+    N = st.nactv[it + 1] if it + 1 < st.iterations else 0
+    v = st.variant[it]
+    if v == gg.VAR_PULL_DENSE:
+        return 8.0 * (n + 1) + 4.0 * n + 8.0 * S + 4.0 * N + 2.0 * n / 8
+    if v == gg.VAR_HOOK:
+        return 8.0 * (n + 1) + 4.0 * m + 8.0 * n
+    return 20.0 * F + 8.0 * E + 4.0 * N
+
+
 # ---------------------------------------------------------------------------
 # reference CPU arm / baseline
 # ---------------------------------------------------------------------------
@@ -289,6 +305,57 @@ def run_reference_arm(args, ws, rank):
     }
     print(json.dumps(line))
     return 0
+
+
+def reference_leg(g, roots, args, lvl):
+    """The reference build (oracle/_ref, compiled from the reference sources)
+    on this host's cores, on the benchmarked graph written out as a Graptor
+    .bin file: its BFSLVLv from the bench's roots is the CPU baseline (one
+    process, one graph load, each run timed like the reference driver's
+    "Running" bracket), and its outputs check the GPU's at this size -- BFS
+    levels by a pair of 64-bit checksums per root (bit-exact or not), CCv
+    labels in full (-cc:outfile), PRv ranks after 20 iterations in full
+    (-pr:outfile, L1)."""
+    from graptor_b200 import gg
+    from oracle import oracle as O
+    if not O.ref_available("ref_bfslvl"):
+        return None, None
+    cores, model = cpu_info()
+    sample_roots = [int(r) for r in roots[: args.cpu_roots]]
+    par = {"graph": f"rmat{args.scale} ef{EDGE_FACTOR}", "reference": "oracle/_ref build of the reference sources"}
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "rmat.bin")
+        g.write_bin(path)
+        tc = time.time()
+        res = O.ref_bfs(path, sample_roots, threads=cores, checksums=True)
+        wall = time.time() - tc
+        tt, ee, exact = 0.0, 0.0, 0
+        for r, t, _, h in res:
+            st = gg.RunStats()
+            lv = g.bfs_level(int(r), level=lvl, stats=st)
+            tt += t
+            ee += st.edges_reached / 2.0
+            exact += int(O.level_checksums(lv) == h)
+        cpu = {"value": round(ee / tt / 1e9, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
+               "sample": f"{len(res)} BFSLVLv runs (the first {len(res)} of the 64 roots) of the reference "
+                         f"build, OpenMP, {model}; load+VEBO+runs wall {wall:.0f} s"}
+        par["bfs_roots_checked"] = len(res)
+        par["bfs_roots_bitexact"] = exact
+        if not args.no_parity_cc_pr:
+            tc = time.time()
+            lab_ref, cc_t = O.ref_cc(path, os.path.join(tmp, "cc.txt"), threads=cores)
+            lab = g.cc()
+            par["cc_bitexact"] = bool(np.array_equal(lab, lab_ref))
+            par["cc_reference_ms"] = round(min(cc_t) * 1e3, 2) if cc_t else None
+            x_ref, pr_t = O.ref_pr(path, os.path.join(tmp, "pr.txt"), maxiter=20, threads=cores)
+            x = g.pagerank(maxiter=20, tol=1e-7, contrib=gg.F32, accum_f64=True, renorm_f32=True)
+            par["pr_iters"] = 20
+            par["pr_l1_vs_ref"] = float(np.abs(x.astype(np.float64) - x_ref).sum())
+            par["pr_max_rel_vs_ref"] = float((np.abs(x.astype(np.float64) - x_ref) /
+                                              np.maximum(x_ref, 1e-30)).max())
+            par["pr_reference_ms_per_iter"] = round(min(pr_t) * 1e3 / 20, 2) if pr_t else None
+            par["cc_pr_wall_s"] = round(time.time() - tc, 1)
+    return cpu, par
 
 
 # ---------------------------------------------------------------------------
@@ -383,7 +450,27 @@ def selector_eval(ctx, graphs):
 # ---------------------------------------------------------------------------
 # PageRank precision (R-MAT 25 ef16; directed ER 2^25 avg degree 32, 1% sinks)
 # ---------------------------------------------------------------------------
-def precision_eval(ctx, hbm_peak):
+def reference_f64_check(g, x64):
+    """PR_vary VARIANT 11 of the reference build (FP64 ranks, contributions
+    and sums, to the 1e-7 residual) on graph g against the FP64 variant's
+    ranks x64: L1, max relative difference, iteration counts."""
+    from oracle import oracle as O
+    if not O.ref_available("PR_vary_11"):
+        return {"reference": "unavailable (reference build missing)"}
+    cores, _ = cpu_info()
+    t0 = time.time()
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "g.bin")
+        g.write_bin(path)
+        xr, ts, its = O.ref_pr(path, os.path.join(tmp, "x.txt"), maxiter=100, threads=cores,
+                               prog_name="PR_vary_11", iterations=True)
+    d = np.abs(x64 - xr)
+    return {"l1_vs_reference_f64": float(d.sum()), "max_rel_vs_reference_f64": float((d / np.maximum(xr, 1e-300)).max()),
+            "reference_iterations": its, "reference_wall_s": round(time.time() - t0, 1),
+            "reference_ms_per_iter": round(min(ts) * 1e3 / max(its or 1, 1), 1) if ts else None}
+
+
+def precision_eval(ctx, hbm_peak, with_ref=True):
     """Each storage format run until the L1 residual <= 1e-7 or 100 iterations,
     timed per iteration, its ranks compared with the FP64 variant's (double
     ranks, sums and contributions; checked against the CPU FP64 oracle by the
@@ -402,6 +489,11 @@ def precision_eval(ctx, hbm_peak):
         g.pagerank(maxiter=100, tol=1e-7, contrib=gg.F64, host=False, stats=st)
         res = {"n": n, "m": m, "f64": {"iterations": st.iterations,
                                        "ms_per_iter": round(st.total_ms / max(st.iterations, 1), 4)}}
+        # the reference's own FP64 run (PR_vary VARIANT 11) checks the FP64
+        # variant on the symmetric graph (the reference build computes a
+        # different iteration on directed graphs, so ER is not compared)
+        if with_ref and name == "rmat25":
+            res["f64"].update(reference_f64_check(g, x64))
         for fname, fmt, acc64 in fmts:
             x = g.pagerank(maxiter=100, tol=1e-7, contrib=fmt, accum_f64=acc64, renorm_f32=(fname == "f32"))
             ts, its = [], 0
@@ -596,6 +688,16 @@ def run_ours(args, ws, rank, local):
                     gg.VAR_PUSH_MERGE: "k_push_merge", gg.VAR_PUSH_DENSE: "k_push_dense"}
     bfs_iter_total_ms = sum(ktime.values())
     bfs_pass_bytes = 8.0 * (n + 1) + 4.0 * m + 8.0 * n
+    # whole-run roofline: the algorithmic bytes of every iteration of every
+    # timed step over the whole timed region (launch gaps and decisions included)
+    bfs_all_bytes = sum(kbytes.values())
+    kernel_roofline = {}
+    for v, t in ktime.items():
+        nl = sum(1 for st in stats for it in range(st.iterations) if st.variant[it] == v)
+        a = kbytes[v] / (t / 1e3) / 1e9
+        kernel_roofline[kernel_names[v]] = {"launches": nl, "ms_per_launch": round(t / max(nl, 1), 4),
+                                            "bytes_per_launch": round(kbytes[v] / max(nl, 1)),
+                                            "achieved_gbs": round(a, 1), "frac": round(a / hbm_peak, 4)}
 
     out = {}
     if rank == 0:
@@ -605,6 +707,9 @@ def run_ours(args, ws, rank, local):
             "ms_per_root_mean": round(float(np.mean([st.total_ms for st in stats])), 4),
             "iterations_mean": round(float(np.mean([st.iterations for st in stats])), 2),
             "kernel_share": {kernel_names[v]: round(t / bfs_iter_total_ms, 3) for v, t in ktime.items()},
+            "kernel_roofline": kernel_roofline,
+            "whole_run_bytes_per_step": round(bfs_all_bytes / args.steps),
+            "whole_run_frac_of_hbm": round(bfs_all_bytes / (t_ms / 1e3) / 1e9 / hbm_peak, 4),
             "one_pass_frac_of_hbm": round(bfs_pass_bytes / (np.mean([st.total_ms for st in stats]) / 1e3)
                                           / 1e9 / hbm_peak, 4),
         }
@@ -621,10 +726,18 @@ def run_ours(args, ws, rank, local):
             cc_ms.append(st.total_ms)
             cst = st
         cc_best = float(np.median(cc_ms))
+        # per-iteration records (variant, counts) of one more run
+        cst = gg.RunStats()
+        g.cc(label=lab, host=False, opts=gg.default_opts(gg.THRESH_FRAC, 5, collect=True), stats=cst)
         # one pass over the CSC and the labels, as the BFS line's one-pass fraction
         cc_pass = 8.0 * (n + 1) + 4.0 * m + 8.0 * n
+        cc_all = sum(cc_bytes(n, m, cst, it) for it in range(min(cst.iterations, gg.MAX_ITERS)))
         out["cc"] = {"ms": round(cc_best, 3), "gedges_per_s": round(m / (cc_best / 1e3) / 1e9, 3),
                      "iterations": cst.iterations,
+                     "variants": [gg.VARIANT_NAMES.get(cst.variant[i], "hook")
+                                  for i in range(min(cst.iterations, gg.MAX_ITERS))],
+                     "whole_run_bytes": round(cc_all),
+                     "whole_run_frac_of_hbm": round(cc_all / (cc_best / 1e3) / 1e9 / hbm_peak, 4),
                      "one_pass_frac_of_hbm": round(cc_pass / (cc_best / 1e3) / 1e9 / hbm_peak, 4)}
 
         # ---- PageRank (PRv: FP32 storage, double gather accumulation, 20 iterations) ----
@@ -660,7 +773,7 @@ def run_ours(args, ws, rank, local):
 
     # ---- PageRank precision workloads ----
     if not args.quick and not args.no_precision and rank == 0:
-        out["pr_precision"] = precision_eval(ctx, hbm_peak)
+        out["pr_precision"] = precision_eval(ctx, hbm_peak, with_ref=not args.no_cpu_baseline)
 
     # ---- batching: multi-source BFS, 128-seed PPR (R-MAT 22), many small graphs ----
     if not args.quick and not args.no_batch and rank == 0:
@@ -693,29 +806,11 @@ def run_ours(args, ws, rank, local):
                "d2h_bytes_per_step": 4 * n, "graph_upload_s": round(upload_s, 3)}
         del gh
 
-    # ---- CPU baseline: the reference build on this host, bounded sample ----
-    cpu = None
+    # ---- CPU baseline and parity: the reference build on this host, same graph ----
+    cpu, parity = None, None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            from oracle import oracle as O
-            if O.ref_available("ref_bfslvl"):
-                cores, model = cpu_info()
-                sample_roots = [int(r) for r in roots[: args.cpu_roots]]
-                with tempfile.TemporaryDirectory() as tmp:
-                    path = os.path.join(tmp, "rmat.bin")
-                    g.write_bin(path)
-                    tc = time.time()
-                    res = reference_bfs(path, sample_roots, cores)
-                    wall = time.time() - tc
-                tt, ee = 0.0, 0.0
-                for r, t, _, _ in res:
-                    st = gg.RunStats()
-                    g.bfs_level(int(r), level=lvl, host=False, stats=st)
-                    tt += t
-                    ee += st.edges_reached / 2.0
-                cpu = {"value": round(ee / tt / 1e9, 4), "unit": "GTEPS", "cores": cores, "kind": "reference",
-                       "sample": f"{len(res)} BFSLVLv runs (roots 0..{len(res)-1} of the 64) of the reference "
-                                 f"build, OpenMP, {model}; load+VEBO+runs wall {wall:.0f} s"}
+            cpu, parity = reference_leg(g, roots, args, lvl)
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "GTEPS", "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"failed: {e}"[:300]}
@@ -739,7 +834,7 @@ def run_ours(args, ws, rank, local):
                          "bytes_per_launch": round(kbytes[dom] / max(nlaunch, 1)),
                          "ms_per_launch": round(ktime[dom] / max(nlaunch, 1), 4)},
             "clocks": clocks, "gpu_launches": launches,
-            "e2e": e2e, "cpu_baseline": cpu,
+            "e2e": e2e, "cpu_baseline": cpu, "parity": parity,
         }
         line.update(out)
         print(json.dumps(line))
@@ -862,8 +957,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--scale", type=int, default=SCALE)
-    ap.add_argument("--cpu-roots", type=int, default=4)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-roots", type=int, default=NROOTS,
+                    help="roots of the reference's BFS runs (CPU baseline and level parity)")
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the reference leg (baseline and parity)")
+    ap.add_argument("--no-parity-cc-pr", action="store_true", help="reference leg: BFS only")
     ap.add_argument("--quick", action="store_true", help="BFS only (no CC/PR/e2e)")
     ap.add_argument("--no-selector", action="store_true", help="skip the learned-selector evaluation")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-traversal measurements")

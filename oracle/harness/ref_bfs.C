@@ -19,8 +19,14 @@
 // file's n; the padded count is printed so callers can reject padded graphs
 // where a comparison depends on it.
 //
-// Usage: ref_bfs <graph.bin> <out_prefix|-> <root> [root ...]
-//   prints one line per root:  "root <r> time_s <t> reached <k>"
+// With out_prefix "+" nothing is written; each root's line instead ends
+// with two 64-bit checksums of the per-vertex result, sum over v of
+// (uint32)value[v] * w_k(v) modulo 2^64 with w_k(v) = splitmix64 finaliser of
+// (v + k * 0x9E3779B97F4A7C15), k = 1, 2, so that a caller can compare the
+// result of a large graph without reading it.
+//
+// Usage: ref_bfs <graph.bin> <out_prefix|-|+> <root> [root ...]
+//   prints one line per root:  "root <r> time_s <t> reached <k> [check <h1> <h2>]"
 #include "graptor/graptor.h"
 #include "graptor/api.h"
 #include <chrono>
@@ -38,6 +44,12 @@
 #undef private
 
 using HarnessGraph = GraphVEBOGraptor<GRAPTOR_MODE_MACRO(1,0,1)>;
+
+static uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
 
 int main(int argc, char **argv) {
     if (argc < 4) {
@@ -70,7 +82,9 @@ int main(int argc, char **argv) {
         auto t1 = std::chrono::steady_clock::now();
         double sec = std::chrono::duration<double>(t1 - t0).count();
         VID reached = 0;
-        std::vector<int32_t> dump(out == "-" ? 0 : n);
+        const bool check = out == "+";
+        uint64_t h1 = 0, h2 = 0;
+        std::vector<int32_t> dump(out == "-" || check ? 0 : n);
         for (VID v = 0; v < n; ++v) {
             VID rv = PG.remapID(v);
 #ifdef REF_BFSV
@@ -83,8 +97,16 @@ int main(int argc, char **argv) {
             reached += ((VID)val <= n);
 #endif
             if (!dump.empty()) dump[v] = val;
+            if (check) {
+                h1 += (uint64_t)(uint32_t)val * mix64((uint64_t)v + 0x9E3779B97F4A7C15ull);
+                h2 += (uint64_t)(uint32_t)val * mix64((uint64_t)v + 2 * 0x9E3779B97F4A7C15ull);
+            }
         }
-        std::printf("root %s time_s %.9f reached %u\n", root.c_str(), sec, (unsigned)reached);
+        if (check)
+            std::printf("root %s time_s %.9f reached %u check %016llx %016llx\n", root.c_str(), sec,
+                        (unsigned)reached, (unsigned long long)h1, (unsigned long long)h2);
+        else
+            std::printf("root %s time_s %.9f reached %u\n", root.c_str(), sec, (unsigned)reached);
         std::fflush(stdout);
         if (!dump.empty()) {
             std::string path = out + "." + root + ".i32";

@@ -272,14 +272,16 @@ class PaddedGraph(RuntimeError):
 
 
 def ref_bfs(bin_path: str, roots, out_prefix: str | None = None, parents: bool = False,
-            threads: int | None = None):
+            threads: int | None = None, checksums: bool = False):
     """Run the reference BFSLVLv (or BFSv) from each root.
 
-    Returns a list of (root, seconds, reached, per-vertex int32 array or None)."""
+    Returns a list of (root, seconds, reached, per-vertex int32 array or None);
+    with checksums=True the last field is the pair of result checksums
+    (level_checksums() of the reference's levels) and nothing is written."""
     prog = ref_prog("ref_bfsv" if parents else "ref_bfslvl")
     if prog is None:
         raise RuntimeError("reference BFS harness not built")
-    outp = out_prefix or "-"
+    outp = "+" if checksums else (out_prefix or "-")
     txt = _run([prog, bin_path, outp] + [str(r) for r in roots], threads)
     res = []
     for line in txt.splitlines():
@@ -292,10 +294,31 @@ def ref_bfs(bin_path: str, roots, out_prefix: str | None = None, parents: bool =
         f = line.split()
         r, t, k = int(f[1]), float(f[3]), int(f[5])
         arr = None
-        if out_prefix:
+        if checksums:
+            arr = (int(f[7], 16), int(f[8], 16))
+        elif out_prefix:
             arr = np.fromfile(f"{out_prefix}.{r}.i32", dtype=np.int32)
         res.append((r, t, k, arr))
     return res
+
+
+def _mix64(z: np.ndarray) -> np.ndarray:
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return z ^ (z >> np.uint64(31))
+
+
+def level_checksums(values: np.ndarray):
+    """The pair of checksums the reference BFS harness prints for a
+    per-vertex int32 result: sum_v (uint32)values[v] * w_k(v) mod 2^64."""
+    v = np.ascontiguousarray(values).view(np.uint32).astype(np.uint64)
+    idx = np.arange(len(v), dtype=np.uint64)
+    out = []
+    with np.errstate(over="ignore"):
+        for k in (1, 2):
+            w = _mix64(idx + np.uint64((k * 0x9E3779B97F4A7C15) & 0xFFFFFFFFFFFFFFFF))
+            out.append(int(np.sum(v * w, dtype=np.uint64)))
+    return tuple(out)
 
 
 def _running_times(txt: str):
@@ -307,7 +330,7 @@ def ref_cc(bin_path: str, out_path: str, threads: int | None = None, rounds: int
     prog = ref_prog("CCv")
     txt = _run([prog, "-s", "-b", "-rounds", str(rounds), "-c", "256",
                 "-cc:outfile", out_path, bin_path], threads)
-    lab = np.loadtxt(out_path, dtype=np.uint64).astype(np.uint32)
+    lab = np.fromfile(out_path, dtype=np.uint64, sep=" ").astype(np.uint32)
     n = int(np.fromfile(bin_path, dtype=np.uint64, count=3)[2])
     if len(lab) != n:
         raise PaddedGraph(f"reference padded {n} vertices to {len(lab)}")
@@ -324,7 +347,7 @@ def ref_pr(bin_path: str, out_path: str, maxiter: int = 20, threads: int | None 
         "-b", "-rounds", str(rounds), "-c", "256", "-pr:maxiter", str(maxiter),
         "-pr:outfile", out_path] + (["-itimes"] if iterations else []) + [bin_path]
     txt, err = _run(args, threads, stderr=True)
-    x = np.loadtxt(out_path, dtype=np.float64)
+    x = np.fromfile(out_path, dtype=np.float64, sep=" ")
     n = int(np.fromfile(bin_path, dtype=np.uint64, count=3)[2])
     if len(x) != n:
         raise PaddedGraph(f"reference padded {n} vertices to {len(x)}")
