@@ -75,6 +75,7 @@ struct EmapArgs {
     uint32_t *cand_out;                 // vertices still passing after this step
     unsigned long long *cand_out_n;
     const uint64_t *word_prefix;        // full-scan pull: per-word cost prefix
+    const uint2 *first_in;              // pull: first two in-neighbours per vertex, or null
 };
 
 template <int R>
@@ -212,15 +213,39 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
         const uint32_t d = CAND ? (valid ? A.cand[item] : 0u) : (uint32_t)item;
         V best = Op<R>::none();
         uint64_t e = 0, end = 0;
+        uint2 f2 = make_uint2(0u, 0u);
         if (valid) {
             best = op.load(d);
             e = A.in_off[d];
             end = A.in_off[d + 1];
+            if (A.first_in) f2 = A.first_in[d];
         }
         bool act = valid && op.dst_ok(best);
         bool changed = false;
         const uint64_t beg = e;
         const uint64_t lim = min(end, e + (uint64_t)A.K);
+        if (A.first_in && act && e < lim) {
+            // the row's first two in-neighbours, loaded beside its offsets:
+            // the same edges in the same order as the loop below takes them
+            const int cnt = (int)min((uint64_t)2, lim - e);
+            const uint32_t sv[2] = {f2.x, f2.y};
+            int used = cnt;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                if (j < cnt && act && (!SRCF || dev::bit_test(A.in_bits, sv[j]))) {
+                    const V x = op.src_val(sv[j]);
+                    if (op.better(x, best)) {
+                        best = x;
+                        changed = true;
+                        if (!op.dst_ok(best)) {
+                            act = false;
+                            used = j + 1;
+                        }
+                    }
+                }
+            }
+            e += used;
+        }
         while (act && e < lim) {
             const int cnt = (int)min((uint64_t)4, lim - e);
             uint32_t sv[4];
@@ -721,6 +746,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     A.mmax = t.bin_medium_max;
     A.K = variant == GG_VAR_PULL_DENSE ? t.pull_k : t.push_k;
     A.word_prefix = g->heavy.pull_prefix;
+    A.first_in = t.pull_first ? g->first_in : nullptr;
     const bool have_out = out != nullptr && d->record != GG_RECORD_NONE;
     if (have_out) {
         GG_CHECK(frontier_alloc_bins(out));
@@ -1241,6 +1267,7 @@ struct GCtl {
     int pull_k, push_k;
     const uint64_t *off, *in_off, *word_prefix;
     const uint32_t *adj, *in_adj;
+    const uint2 *first_in;
     const uint32_t *nonisolated;
     const unsigned long long *nonisolated_n;
     uint32_t *cand[2];
@@ -1400,6 +1427,7 @@ __device__ void decide_step(GCtl *c) {
     A.mmax = c->mmax;
     A.K = push ? c->push_k : c->pull_k;
     A.word_prefix = c->word_prefix;
+    A.first_in = push ? nullptr : c->first_in;
     A.out_b0 = O.bins[0];
     A.out_b1 = O.bins[1];
     A.out_b2 = O.bins[2];
@@ -1806,6 +1834,7 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     h.word_prefix = g->heavy.pull_prefix;
     h.adj = g->adj;
     h.in_adj = g->in_adj;
+    h.first_in = t.pull_first ? g->first_in : nullptr;
     h.nonisolated = g->nonisolated;
     h.nonisolated_n = (const unsigned long long *)g->nonisolated_n;
     // chunk prefix room: rows above bin_medium_max edges, at most m / (max + 1)

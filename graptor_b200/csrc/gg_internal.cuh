@@ -137,6 +137,9 @@ struct gg_graph {
     gg_frontier *tmp_front[2] = {nullptr, nullptr};
     uint64_t *aux_cnt = nullptr;  // counters of steps that record no frontier
     HeavyRows heavy;              // chunked long rows of the CSC (pull / gather)
+    // first two in-neighbours of every vertex (CSC row order; 0xFFFFFFFF past
+    // the row's end): most dense-pull rows find their parent there
+    uint2 *first_in = nullptr;
     gg_prop *tmp_prop[4] = {nullptr, nullptr, nullptr, nullptr};  // cached run temporaries
     uint32_t *nonisolated = nullptr;    // vertices with in-edges, ascending
     uint64_t *nonisolated_n = nullptr;  // its length (device)
@@ -246,6 +249,9 @@ struct Tuning {
     // road-network test (fewer than n/10 zero labels) and, where it holds,
     // min-id hooking for the rest of the run
     int cc_hook = 1;
+    // dense pull: each row's first two in-neighbours read from a per-vertex
+    // pair array (coalesced with the row's offsets) before the row itself
+    int pull_first = 1;
     unsigned long long barrier_timeout_ns = 5000000000ull;  // grid-barrier wait limit
 };
 Tuning &tuning();
