@@ -783,27 +783,36 @@ def run_ours(args, ws, rank, local):
         out["batch"]["graph"] = "rmat22 ef16 seed 1 (msbfs64, ppr128)"
         g22.close()
 
-    # ---- e2e: public C-ABI call, graph uploaded from host memory, levels back to pinned host ----
+    # ---- e2e: public C-ABI call, graph uploaded from host memory, every step's
+    # levels delivered to page-locked host memory (gg_bfs_level_host_async: the
+    # copy of step k runs behind the BFS of step k+1; the last one is waited
+    # for inside the timed region) ----
     e2e = None
     if not args.quick:
-        pin = torch.empty(n, dtype=torch.int32, pin_memory=True).numpy()
+        pins = [torch.empty(n, dtype=torch.int32, pin_memory=True).numpy() for _ in range(2)]
         t_up = time.time()
         gh = ctx.upload(off, adj, symmetric=True)
         upload_s = time.time() - t_up
-        lv2 = gh.prop(gg.I32)
         for k in range(min(args.warmup, 3)):
-            gh.bfs_level(seq[k], level=lv2, out=pin)
+            gh.bfs_level_host_async(seq[k], out=pins[k % 2])
+        gh.bfs_level_host_wait()
         barrier(ws)
         t1 = time.perf_counter()
         e2e_edges = 0.0
         for k in range(args.steps):
             st = gg.RunStats()
-            gh.bfs_level(seq[args.warmup + k], level=lv2, out=pin, stats=st)
+            gh.bfs_level_host_async(seq[args.warmup + k], out=pins[k % 2], stats=st)
             e2e_edges += st.edges_reached / 2.0
+        gh.bfs_level_host_wait()
         e2e_s = max_over_ranks(time.perf_counter() - t1, ws)
         e2e_val = sum_over_ranks(e2e_edges, ws) / e2e_s / 1e9
+        # the last step's levels, checked against the device-resident run of the same root
+        last_ok = bool(np.array_equal(pins[(args.steps - 1) % 2], g.bfs_level(seq[args.warmup + args.steps - 1])))
         e2e = {"value": round(e2e_val, 4), "unit": "GTEPS", "h2d_bytes_per_step": 4,
-               "d2h_bytes_per_step": 4 * n, "graph_upload_s": round(upload_s, 3)}
+               "d2h_bytes_per_step": 4 * n, "graph_upload_s": round(upload_s, 3),
+               "api": "gg_bfs_level_host_async (levels to page-locked host memory, copy behind the next BFS)",
+               "last_step_levels_match": last_ok}
+        gh.close()
         del gh
 
     # ---- CPU baseline and parity: the reference build on this host, same graph ----

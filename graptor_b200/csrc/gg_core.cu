@@ -536,6 +536,14 @@ static void graph_free(gg_graph *g) {
     cudaFree(g->nonisolated);
     cudaFree(g->nonisolated_n);
     cudaFree(g->first_in);
+    for (int i = 0; i < 2; ++i) {
+        if (g->copy_done[i]) {
+            cudaEventSynchronize(g->copy_done[i]);
+            cudaEventDestroy(g->copy_done[i]);
+        }
+        if (g->async_level[i]) gg_prop_destroy(g->async_level[i]);
+    }
+    if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
     cudaFree(g->pstate);
     cudaFree(g->wq);
     graph_bfs_free(g);

@@ -1991,6 +1991,46 @@ gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop
     return gg_ctx_sync(g->ctx);
 }
 
+// BFS levels of one root into host memory, the copy overlapping the caller's
+// next call: the run writes one of two level buffers in turn, its copy to
+// host_level runs on the graph's copy stream, and the call returns once its
+// BFS is done and the previous call's copy has landed.
+gg_status gg_bfs_level_host_async(gg_graph *g, uint32_t root, const gg_run_opts *o, int32_t *host_level,
+                                  gg_run_stats *st) {
+    if (!g || !host_level || root >= g->n) return GG_ERR_ARG;
+    gg_ctx *ctx = g->ctx;
+    if (!g->copy_stream) {
+        GG_CUDA(ctx, cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            GG_CUDA(ctx, cudaEventCreateWithFlags(&g->copy_done[i], cudaEventDisableTiming));
+            GG_CHECK(gg_prop_create(g, GG_I32, &g->async_level[i]));
+        }
+    }
+    const int slot = g->async_next;
+    // the buffer's last copy (two calls ago) finished before the previous call returned
+    GG_CHECK(gg_bfs_level(g, root, o, g->async_level[slot], nullptr, st));
+    GG_CUDA(ctx, cudaMemcpyAsync(host_level, g->async_level[slot]->d, (size_t)g->n * 4, cudaMemcpyDeviceToHost,
+                                 g->copy_stream));
+    GG_CUDA(ctx, cudaEventRecord(g->copy_done[slot], g->copy_stream));
+    g->copy_pending[slot] = true;
+    g->async_next = slot ^ 1;
+    if (g->copy_pending[slot ^ 1]) {
+        GG_CUDA(ctx, cudaEventSynchronize(g->copy_done[slot ^ 1]));
+        g->copy_pending[slot ^ 1] = false;
+    }
+    return GG_OK;
+}
+
+gg_status gg_bfs_level_host_wait(gg_graph *g) {
+    if (!g) return GG_ERR_ARG;
+    for (int i = 0; i < 2; ++i)
+        if (g->copy_pending[i]) {
+            GG_CUDA(g->ctx, cudaEventSynchronize(g->copy_done[i]));
+            g->copy_pending[i] = false;
+        }
+    return GG_OK;
+}
+
 gg_status gg_bfs_level_multi(gg_graph *g, const uint32_t *roots, uint32_t k, const gg_run_opts *o, gg_prop *level,
                              int32_t *host_level, gg_run_stats *st) {
     if (!g || (k && !roots)) return GG_ERR_ARG;

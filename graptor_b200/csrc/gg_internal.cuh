@@ -140,6 +140,13 @@ struct gg_graph {
     // first two in-neighbours of every vertex (CSC row order; 0xFFFFFFFF past
     // the row's end): most dense-pull rows find their parent there
     uint2 *first_in = nullptr;
+    // gg_bfs_level_host_async: two level buffers used in turn, the stream
+    // their host copies run on, and an event per buffer marking its copy done
+    gg_prop *async_level[2] = {nullptr, nullptr};
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_done[2] = {nullptr, nullptr};
+    bool copy_pending[2] = {false, false};
+    int async_next = 0;
     gg_prop *tmp_prop[4] = {nullptr, nullptr, nullptr, nullptr};  // cached run temporaries
     uint32_t *nonisolated = nullptr;    // vertices with in-edges, ascending
     uint64_t *nonisolated_n = nullptr;  // its length (device)

@@ -93,7 +93,8 @@ EXPORTS = [
     "gg_prop_upload", "gg_prop_device_ptr", "gg_prop_destroy", "gg_prop_create_managed", "gg_frontier_create",
     "gg_frontier_clear", "gg_frontier_set_single", "gg_frontier_set_all", "gg_frontier_set_list",
     "gg_frontier_counts", "gg_frontier_download", "gg_frontier_destroy", "gg_edgemap",
-    "gg_vertexmap", "gg_bfs_level", "gg_bfs_parent", "gg_cc", "gg_pagerank",
+    "gg_vertexmap", "gg_bfs_level", "gg_bfs_level_host_async", "gg_bfs_level_host_wait",
+    "gg_bfs_parent", "gg_cc", "gg_pagerank",
     "gg_tuning_set", "gg_tuning_get",
 ]
 
@@ -348,6 +349,19 @@ class Graph:
                                           C.byref(stats) if stats is not None else None),
                        "gg_bfs_level")
         return out
+
+    def bfs_level_host_async(self, root: int, out: np.ndarray, opts: RunOpts = None, stats: RunStats = None):
+        """BFS levels into `out` (int32, n entries, ideally page-locked), the
+        copy finishing behind the next call: `out` of call i is complete once
+        call i+1 or bfs_level_host_wait() has returned."""
+        assert out.dtype == np.int32 and out.size >= self.n and out.flags.c_contiguous
+        self.ctx.check(lib().gg_bfs_level_host_async(self.h, root, C.byref(opts) if opts else None, _p(out),
+                                                     C.byref(stats) if stats is not None else None),
+                       "gg_bfs_level_host_async")
+        return out
+
+    def bfs_level_host_wait(self):
+        self.ctx.check(lib().gg_bfs_level_host_wait(self.h), "gg_bfs_level_host_wait")
 
     def bfs_parent(self, root: int, parent: "Prop" = None, host: bool = True,
                    opts: RunOpts = None, stats: RunStats = None):

@@ -339,6 +339,22 @@ typedef struct gg_run_opts {
 /* BFS levels (BFSLVLv): level[root] = 0, unreached = n+1. */
 GG_API gg_status gg_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop *level,
                               int32_t *host_level, gg_run_stats *st);
+
+/* BFS levels of one root delivered to host memory with the copy running
+ * behind the caller's next call (the reference's BFSLVLv leaves its level
+ * array in host memory, BFSLVLv.C:110-254; a GPU run pays a device-to-host
+ * copy for it).  The call runs the BFS into one of two library-owned level
+ * buffers, starts the copy of the levels into host_level (n entries) on the
+ * graph's copy stream, and returns when the BFS is done and the copy started
+ * by the PREVIOUS call on this graph has landed in its host_level.
+ * gg_bfs_level_host_wait(g) waits for the last copy.  The caller may read
+ * the host_level of call i once call i+1 (or the wait) has returned, and must
+ * not reuse it before then.  host_level should be page-locked memory
+ * (cudaHostAlloc / cudaHostRegister): a pageable destination makes each copy
+ * synchronous.  Calls on one graph come from one host thread. */
+GG_API gg_status gg_bfs_level_host_async(gg_graph *g, uint32_t root, const gg_run_opts *o,
+                                         int32_t *host_level, gg_run_stats *st);
+GG_API gg_status gg_bfs_level_host_wait(gg_graph *g);
 /* BFS parents (BFSv): parent[root] = root, unreached = ~0u; any valid BFS tree. */
 GG_API gg_status gg_bfs_parent(gg_graph *g, uint32_t root, const gg_run_opts *o, gg_prop *parent,
                                uint32_t *host_parent, gg_run_stats *st);
