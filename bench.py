@@ -361,16 +361,46 @@ def reference_leg(g, roots, args, lvl):
 # ---------------------------------------------------------------------------
 # learned selector evaluation (held-out graphs)
 # ---------------------------------------------------------------------------
+def deviation_oracle(g, analytic, root, thr_variant, t_thr, max_iters=64):
+    """Oracle-best time of one run from forced timings on the threshold run's
+    own state (gg_selector_collect: the run follows the threshold except at
+    one iteration, which takes each of the four variants in turn).  BFS: every
+    variant leaves the same next frontier, so the per-iteration gains over the
+    threshold's own choice add up, oracle = T_thr - sum_i (t_i(thr) - min_v
+    t_i(v)); CC: a step's choice changes what follows, so the best single
+    deviation counts, oracle = T_thr - max_i (rest_i(thr) - min_v rest_i(v)).
+    Returns (oracle ms, iterations covered) or (None, 0) for runs longer than
+    max_iters iterations."""
+    from graptor_b200 import gg
+    T = len(thr_variant)
+    if T > max_iters:
+        return None, 0
+    X, Y = gg.selector_collect(g, 0 if analytic == "bfs" else 1, root, max_samples=max_iters, cap=max_iters)
+    gains = []
+    for x, y in zip(X, Y):
+        it = int(round(2.0 ** (8.0 * float(x[3])) - 1.0))  # the iteration feature, log2(1 + it) / 8
+        if it >= T or not np.all(np.isfinite(y)):
+            continue
+        t = 2.0 ** y.astype(np.float64) / 1e3  # ms
+        gains.append(max(0.0, t[thr_variant[it]] - t.min()))
+    if not gains:
+        return t_thr, 0
+    g_all = sum(gains) if analytic == "bfs" else max(gains)
+    return t_thr - g_all, len(gains)
+
+
 def selector_eval(ctx, graphs):
     """Device-driven BFS / CC with the density threshold, the learned selector
-    and each fixed variant; oracle-best = per-iteration minimum over the fixed
-    variants (BFS: every variant walks the same levels)."""
+    and each fixed variant, medians of three runs; oracle-best from forced
+    one-iteration deviations of the threshold run (deviation_oracle)."""
     from graptor_b200 import gg
     from graptor_b200.selector_train import load_selector
     sel = load_selector(ctx)
     old = gg.tuning_get("persistent")
     gg.tuning_set("persistent", 7)
-    out = {"weights": "graptor_b200/data/selector.npz" if sel else None}
+    out = {"weights": "graptor_b200/data/selector.npz" if sel else None,
+           "oracle": "threshold run with one iteration forced to each variant in turn (same state); "
+                     "BFS sums the per-iteration gains, CC takes the best single deviation"}
     try:
         for name, g, roots in graphs:
             if sel:
@@ -385,41 +415,41 @@ def selector_eval(ctx, graphs):
                         g.cc(host=False, opts=opts, stats=st)
                     return st
                 rs = roots if analytic == "bfs" else [0]
-                modes = {"threshold": gg.default_opts(gg.THRESH_DEFAULT if analytic == "bfs" else gg.THRESH_FRAC,
-                                                      0 if analytic == "bfs" else 5, collect=True)}
+                thr_opts = gg.default_opts(gg.THRESH_DEFAULT if analytic == "bfs" else gg.THRESH_FRAC,
+                                           0 if analytic == "bfs" else 5)
+                modes = {"threshold": thr_opts}
                 if sel:
-                    modes["learned"] = gg.default_opts(gg.THRESH_LEARNED, collect=True)
+                    modes["learned"] = gg.default_opts(gg.THRESH_LEARNED)
                 for v, vn in gg.VARIANT_NAMES.items():
-                    modes["fixed_" + vn] = gg.default_opts(variant=v, collect=True)
+                    modes["fixed_" + vn] = gg.default_opts(variant=v)
                 tot = {k: 0.0 for k in modes}
-                oracle = 0.0
+                oracle, covered = 0.0, 0
                 for r in rs:
                     per = {}
                     for k, o in modes.items():
                         run(o, r)  # warm
-                        # the median of three runs (CC lasts well under a millisecond)
-                        sts = sorted((run(o, r) for _ in range(3)), key=lambda s: s.total_ms)
-                        st = sts[1]
-                        tot[k] += st.total_ms
-                        per[k] = st
-                    fixed = [per["fixed_" + vn] for vn in gg.VARIANT_NAMES.values()]
-                    its = {f.iterations for f in fixed}
-                    if len(its) == 1 and fixed[0].iterations <= gg.MAX_ITERS:
-                        T = fixed[0].iterations
-                        it_min = sum(min(f.iter_ms[i] for f in fixed) for i in range(T))
-                        it_thr = sum(per["threshold"].iter_ms[i] for i in range(T))
-                        # whole-run overheads (launch, setup) as in the threshold run
-                        oracle += it_min + (per["threshold"].total_ms - it_thr)
+                        per[k] = float(np.median([run(o, r).total_ms for _ in range(3)]))
+                        tot[k] += per[k]
+                    rec = run(gg.default_opts(gg.THRESH_DEFAULT if analytic == "bfs" else gg.THRESH_FRAC,
+                                              0 if analytic == "bfs" else 5, collect=True), r)
+                    thr_var = [rec.variant[i] for i in range(min(rec.iterations, gg.MAX_ITERS))]
+                    o_ms, cov = deviation_oracle(g, analytic, r, thr_var, per["threshold"])
+                    if o_ms is None or oracle is None:
+                        oracle = None
                     else:
-                        oracle = float("nan")
+                        oracle += o_ms
+                        covered += cov
                 best_fixed = min(v for k, v in tot.items() if k.startswith("fixed_"))
                 d = {k: round(v / len(rs), 4) for k, v in tot.items()}
-                d["oracle_best_ms"] = round(oracle / len(rs), 4) if oracle == oracle else None
+                d["oracle_best_ms"] = round(oracle / len(rs), 4) if oracle is not None else None
+                d["oracle_iterations_covered"] = covered
                 d["best_fixed_ms"] = round(best_fixed / len(rs), 4)
                 if sel:
                     d["learned_vs_threshold"] = round(tot["threshold"] / tot["learned"], 3)
-                    if oracle == oracle:
+                    if oracle is not None:
                         d["learned_over_oracle"] = round(tot["learned"] / oracle, 3)
+                if oracle is not None:
+                    d["threshold_over_oracle"] = round(tot["threshold"] / oracle, 3)
                 res[analytic] = d
             out[name] = res
             if sel:

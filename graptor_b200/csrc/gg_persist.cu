@@ -935,6 +935,22 @@ __device__ __forceinline__ bool sel_close(unsigned long long a, unsigned long lo
 __device__ int learned_choice(const PArgs &P, const __nv_bfloat16 *selw, unsigned long long nactv,
                               unsigned long long nacte, unsigned long long unr, int it, SelCache *cache) {
     const double n = P.n, m = (double)P.m, fv = (double)nactv, fe = (double)nacte;
+    const int tv = (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+    // CC: a frontier far from the threshold's boundary (more than 8x on
+    // either side) keeps the threshold's choice without an evaluation -- a CC
+    // step's records differ by a few per cent between variants there, less
+    // than an evaluation in the step's critical path costs
+    if (P.relax == GG_RELAX_MIN_U32 && ((nactv + nacte) * 8 < P.m / 20 || (nactv + nacte) > (P.m / 20) * 8)) {
+        if ((threadIdx.x & 31) == 0) {
+            cache->nactv = nactv;
+            cache->nacte = nacte;
+            cache->unreached = unr;
+            cache->iter = it;
+            cache->choice = tv;
+            cache->valid = 1;
+        }
+        return tv;
+    }
     float x[GG_SEL_FEATURES];
     x[0] = (float)(log2(1.0 + fv) / 32);
     x[1] = (float)(log2(1.0 + fe) / 40);
@@ -952,7 +968,6 @@ __device__ int learned_choice(const PArgs &P, const __nv_bfloat16 *selw, unsigne
     for (int v = 1; v < GG_SEL_VARIANTS; ++v)
         if (o[v] < o[best]) best = v;
     // the threshold's choice stands unless the network predicts a clear gain over it
-    const int tv = (nactv + nacte) <= P.m / 20 ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
     const float margin = P.relax == GG_RELAX_MIN_U32 ? mlp::kSelMarginCC : mlp::kSelMargin;
     if (!(o[best] < o[tv] - margin)) best = tv;
     if ((threadIdx.x & 31) == 0) {

@@ -7,10 +7,13 @@ deleted.  For every graph, gg_selector_collect runs BFS (from a seeded
 non-isolated root) and CC device-driven, forcing each of the four traversal
 variants at sampled iterations, and records the iteration's features and the
 measured log2 time of every variant.  The network is then trained by the
-library's GPU kernels (gg_selector_train) on four fifths of the records
-(every fifth is held out and only scored) and the parameters are written to
-graptor_b200/data/selector.npz, which load_selector() attaches to graphs.
-The collected records are kept in graptor_b200/data/selector_records.npz.
+library's GPU kernels (gg_selector_train) on the records of four fifths of
+the graphs (every fifth graph is held out: its records are only scored, so
+the held-out figures are on graphs the network never saw) and the
+parameters are written to graptor_b200/data/selector.npz, which
+load_selector() attaches to graphs.  The collected records are kept in
+graptor_b200/data/selector_records.npz with the index of the graph each
+record comes from.
 
     python -m graptor_b200.selector_train [--graphs 200] [--out path]
     python -m graptor_b200.selector_train --dataset-in graptor_b200/data/selector_records.npz
@@ -56,7 +59,7 @@ def make_graph(ctx: gg.Context, kind: str, kw: dict) -> gg.Graph:
 
 def collect(ctx: gg.Context, n_graphs: int, seed: int = 7, samples: int = 6, log=print):
     rng = np.random.default_rng(seed)
-    Xs, Ys, meta = [], [], []
+    Xs, Ys, Gs, meta = [], [], [], []
     t0 = time.time()
     for i in range(n_graphs):
         kind, kw, label = graph_family(i, rng)
@@ -69,11 +72,12 @@ def collect(ctx: gg.Context, n_graphs: int, seed: int = 7, samples: int = 6, log
             X, Y = gg.selector_collect(g, analytic, root=root, max_samples=samples)
             Xs.append(X)
             Ys.append(Y)
+            Gs.append(np.full(len(X), i, dtype=np.int64))
             meta += [(label, analytic)] * len(X)
         g.close()
         if log and (i + 1) % 20 == 0:
             log(f"collected {i + 1}/{n_graphs} graphs, {sum(len(x) for x in Xs)} records, {time.time() - t0:.0f} s")
-    return np.concatenate(Xs), np.concatenate(Ys), meta
+    return np.concatenate(Xs), np.concatenate(Ys), np.concatenate(Gs), meta
 
 
 def clean(X, Y):
@@ -86,10 +90,14 @@ def clean(X, Y):
     return X, np.nan_to_num(Y, nan=0.0), M
 
 
-def split(n: int):
-    """(training, held-out) record indices: every fifth record is held out."""
-    idx = np.arange(n)
-    return idx[idx % 5 != 0], idx[idx % 5 == 0]
+def split(graph: np.ndarray):
+    """(training, held-out) record indices: the records of every fifth
+    training graph are held out, so that no held-out record shares a graph
+    (or a run) with a training record."""
+    graph = np.asarray(graph)
+    idx = np.arange(len(graph))
+    hold = graph % 5 == 0
+    return idx[~hold], idx[hold]
 
 
 def train(ctx: gg.Context, X, Y, epochs: int = 3000, lr: float = 3e-3, seed: int = 0):
@@ -138,22 +146,23 @@ def main():
     t0 = time.time()
     if args.dataset_in:
         d = np.load(args.dataset_in)
-        X, Y = d["X"], d["Y"]
+        X, Y, G = d["X"], d["Y"], d["graph"]
     else:
-        X, Y, _ = collect(ctx, args.graphs, samples=args.samples)
+        X, Y, G, _ = collect(ctx, args.graphs, samples=args.samples)
     t1 = time.time()
-    # every fifth record is held out (never trained on) to report generalisation
-    tr, te = split(len(X))
+    # every fifth graph is held out (never trained on) to report generalisation
+    tr, te = split(G)
     sel, loss = train(ctx, X[tr], Y[tr], epochs=args.epochs, lr=args.lr)
     hold = quality(sel, X[te], Y[te])
     t2 = time.time()
     agree, regret = quality(sel, X[tr], Y[tr])
-    info = dict(records=int(len(X)), graphs=args.graphs, train_mse=loss, argmin_agreement=agree,
+    info = dict(records=int(len(X)), graphs=int(len(np.unique(G))), heldout_graphs=int(len(np.unique(G[te]))),
+                train_mse=loss, argmin_agreement=agree,
                 regret_vs_best=regret, heldout_argmin_agreement=hold[0], heldout_regret_vs_best=hold[1],
                 collect_s=round(t1 - t0, 1), train_s=round(t2 - t1, 1), epochs=args.epochs, lr=args.lr)
     save_selector(sel, args.out, info)
     if args.dataset_out:
-        np.savez(args.dataset_out, X=X, Y=Y)
+        np.savez(args.dataset_out, X=X, Y=Y, graph=G)
     print(json.dumps(info))
 
 

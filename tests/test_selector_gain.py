@@ -3,8 +3,9 @@ per-variant iteration timings it was not trained on.
 
 The records (graptor_b200/data/selector_records.npz) hold, per sampled
 iteration of BFS / CC on the training graph families, the features and the
-measured time of all four traversal variants; every fifth record is held out
-of training.  The shipped network (graptor_b200/data/selector.npz, trained on
+measured time of all four traversal variants, and the graph each comes from;
+the records of every fifth graph are held out of training, so the held-out
+records come from graphs the network never saw.  The shipped network (graptor_b200/data/selector.npz, trained on
 the GPU by gg_selector_train) is evaluated here with the float64 oracle on
 bfloat16-rounded weights, applying the same rule as the device: the
 threshold's choice (push_sparse iff |F| + outdeg(F) <= m/20, else pull_dense)
@@ -26,7 +27,7 @@ def heldout():
     from graptor_b200.selector_train import clean, split
     d = np.load(os.path.join(DATA, "selector_records.npz"))
     X, Y, Mk = clean(d["X"], d["Y"])
-    _, te = split(len(X))
+    _, te = split(d["graph"])
     ok = Mk[te].all(1)
     return X[te][ok], Y[te][ok]
 
@@ -76,3 +77,11 @@ def test_untrained_network_does_not_beat_threshold_by_luck():
     trained, thr = choices(z["params"].astype(np.float64), X)
     rnd = [regret(t, choices(M.init_params(seed), X)[0]) for seed in range(5)]
     assert regret(t, trained) < min(rnd)
+
+
+def test_heldout_records_come_from_unseen_graphs():
+    from graptor_b200.selector_train import split
+    d = np.load(os.path.join(DATA, "selector_records.npz"))
+    tr, te = split(d["graph"])
+    assert len(te) > 100 and len(tr) > 4 * len(te) // 2
+    assert not set(d["graph"][tr]) & set(d["graph"][te])
