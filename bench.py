@@ -40,6 +40,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "BFS/CC GTEPS, PR GEdges/s/iter @RMAT-24, %HBM peak; BF16/learned vs plain"
+# Output checks that need the oracle / the reference build, queued by the
+# measurement sections as (check(O, result_dict), result_dict) and run by the
+# reference leg (the only part of the GPU arm that executes oracle/)
+REF_CHECKS = []
 SCALE, EDGE_FACTOR, GRAPH_SEED, ROOT_SEED, NROOTS = 24, 16, 1, 12345, 64
 WORKLOAD = ("BFSLVLv levels from 64 seeded non-isolated roots, R-MAT scale 24 edge factor 16 "
             "(a,b,c=.57,.19,.19, seed 1), symmetrised, deduplicated, no self-loops")
@@ -318,6 +322,12 @@ def reference_leg(g, roots, args, lvl):
     (-pr:outfile, L1)."""
     from graptor_b200 import gg
     from oracle import oracle as O
+    for check, res in REF_CHECKS:
+        try:
+            check(O, res)
+        except Exception as e:  # recorded, never fatal
+            res["check_failed"] = f"{e}"[:300]
+    REF_CHECKS.clear()
     if not O.ref_available("ref_bfslvl"):
         return None, None
     cores, model = cpu_info()
@@ -480,24 +490,26 @@ def selector_eval(ctx, graphs):
 # ---------------------------------------------------------------------------
 # PageRank precision (R-MAT 25 ef16; directed ER 2^25 avg degree 32, 1% sinks)
 # ---------------------------------------------------------------------------
-def reference_f64_check(g, x64):
+def reference_f64_check(O, path, x64, tmpd, res):
     """PR_vary VARIANT 11 of the reference build (FP64 ranks, contributions
-    and sums, to the 1e-7 residual) on graph g against the FP64 variant's
-    ranks x64: L1, max relative difference, iteration counts."""
-    from oracle import oracle as O
-    if not O.ref_available("PR_vary_11"):
-        return {"reference": "unavailable (reference build missing)"}
-    cores, _ = cpu_info()
-    t0 = time.time()
-    with tempfile.TemporaryDirectory() as tmp:
-        path = os.path.join(tmp, "g.bin")
-        g.write_bin(path)
-        xr, ts, its = O.ref_pr(path, os.path.join(tmp, "x.txt"), maxiter=100, threads=cores,
+    and sums, to the 1e-7 residual) on the graph file `path` against the
+    FP64 variant's ranks x64: L1, max relative difference, iterations."""
+    import shutil
+    try:
+        if not O.ref_available("PR_vary_11"):
+            res["reference"] = "unavailable (reference build missing)"
+            return
+        cores, _ = cpu_info()
+        t0 = time.time()
+        xr, ts, its = O.ref_pr(path, os.path.join(tmpd, "x.txt"), maxiter=100, threads=cores,
                                prog_name="PR_vary_11", iterations=True)
-    d = np.abs(x64 - xr)
-    return {"l1_vs_reference_f64": float(d.sum()), "max_rel_vs_reference_f64": float((d / np.maximum(xr, 1e-300)).max()),
-            "reference_iterations": its, "reference_wall_s": round(time.time() - t0, 1),
-            "reference_ms_per_iter": round(min(ts) * 1e3 / max(its or 1, 1), 1) if ts else None}
+        d = np.abs(x64 - xr)
+        res.update({"l1_vs_reference_f64": float(d.sum()),
+                    "max_rel_vs_reference_f64": float((d / np.maximum(xr, 1e-300)).max()),
+                    "reference_iterations": its, "reference_wall_s": round(time.time() - t0, 1),
+                    "reference_ms_per_iter": round(min(ts) * 1e3 / max(its or 1, 1), 1) if ts else None})
+    finally:
+        shutil.rmtree(tmpd, ignore_errors=True)
 
 
 def precision_eval(ctx, hbm_peak, with_ref=True):
@@ -523,7 +535,11 @@ def precision_eval(ctx, hbm_peak, with_ref=True):
         # variant on the symmetric graph (the reference build computes a
         # different iteration on directed graphs, so ER is not compared)
         if with_ref and name == "rmat25":
-            res["f64"].update(reference_f64_check(g, x64))
+            tmpd = tempfile.mkdtemp(prefix="gg_pr25_")
+            path = os.path.join(tmpd, "g.bin")
+            g.write_bin(path)
+            REF_CHECKS.append((lambda O, r, path=path, x64=x64, tmpd=tmpd: reference_f64_check(O, path, x64, tmpd, r),
+                               res["f64"]))
         for fname, fmt, acc64 in fmts:
             x = g.pagerank(maxiter=100, tol=1e-7, contrib=fmt, accum_f64=acc64, renorm_f32=(fname == "f32"))
             ts, its = [], 0
@@ -622,32 +638,76 @@ def batch_eval(ctx, g, roots, hbm_peak, n_small):
                      "seed_edges_per_s": round(128 * m / (t / 1e3) / 1e9, 1),
                      "frac_of_hbm": round(ppr_bytes / (t / 1e3) / 1e9 / hbm_peak, 4),
                      "bytes_per_iter": ppr_bytes, "storage": "bf16 rows of 128 seeds, fp32 sums"}
-    # (b) many small graphs
+    # (b) many small graphs: one union; BFS from every part's vertex 0 plus CC,
+    # submitted as one CUDA graph launch (gg_batch_bfs_cc), with the knobs the
+    # autotuner picks on a 200-graph union of the same family
+    from graptor_b200 import autotune as AT
     t0 = time.time()
     parts = small_graph_batch(ctx, n_small)
     U, base = gg.graph_union(ctx, parts)
     for p in parts:
         p.close()
     build_s = time.time() - t0
-    gg.bfs_level_multi(U, base[:-1], host=False)
-    U.cc(host=False)
-    bm, cm = [], []
-    for _ in range(3):
-        st = gg.RunStats()
-        gg.bfs_level_multi(U, base[:-1], host=False, stats=st)
-        bm.append(st.total_ms)
-        bst = st
-        st = gg.RunStats()
-        U.cc(host=False, stats=st)
-        cm.append(st.total_ms)
-        cst = st
-    tb, tc = float(np.median(bm)), float(np.median(cm))
+
+    def batch_runs(reps=3):
+        gg.batch_bfs_cc(U, base[:-1], host=False)
+        runs = []
+        for _ in range(reps):
+            bs, cs = gg.RunStats(), gg.RunStats()
+            w0 = time.perf_counter()
+            _, _, glaunch, kernels = gg.batch_bfs_cc(U, base[:-1], host=False, bfs_stats=bs, cc_stats=cs)
+            runs.append((bs.total_ms, (time.perf_counter() - w0) * 1e3, bs, cs, glaunch, kernels))
+        runs.sort(key=lambda r: r[0])
+        return runs[len(runs) // 2]
+
+    t_def = batch_runs()
+    knob_names = ["bin_small_max", "bin_medium_max", "pull_k", "push_k", "large_chunk", "blocks_per_sm",
+                  "heavy_deg", "heavy_chunk", "persistent", "cc_hook"]
+    defaults = {k: gg.tuning_get(k) for k in knob_names}
+    tparts = small_graph_batch(ctx, 200, seed=7000)
+    TU, tbase = gg.graph_union(ctx, tparts)
+    for p in tparts:
+        p.close()
+    ta = time.time()
+    tuned = AT.tune_graph(TU, gg.TUNE_BFS | gg.TUNE_CC, nroots=4, passes=1, reps=2)
+    tune_s = time.time() - ta
+    TU.close()
+    gg.graph_retune(U)  # heavy-row tables with the tuned cut
+    t_tun = batch_runs()
+    use_tuned = t_tun[0] <= t_def[0]
+    if not use_tuned:
+        AT.apply(defaults)
+        gg.graph_retune(U)
+    tb, wall, bst, cst, glaunch, kernels = t_tun if use_tuned else t_def
+    # parity on every part: the checker (the reference leg) runs the oracle's
+    # multi-root BFS and CC over the union and compares
+    lv, lb, _, _ = gg.batch_bfs_cc(U, base[:-1])
+    uoff, uadj = U.download()
+    roots0 = base[:-1].copy()
+    union_n = U.n
+
+    def check_union(O, res):
+        p0 = time.time()
+        OU = O.Graph(union_n, uoff, uadj)
+        res["bfs_levels_bitexact"] = bool(np.array_equal(lv, O.bfs_level_multi(OU, roots0)))
+        res["cc_labels_bitexact"] = bool(np.array_equal(lb, O.cc(OU)))
+        res["wall_s"] = round(time.time() - p0, 1)
+
+    sg_parity = {"parts": n_small, "checked_against": "oracle multi-root BFS and CC over the union"}
+    REF_CHECKS.append((check_union, sg_parity))
     out["small_graphs"] = {"graphs": n_small, "n": U.n, "m": U.m, "build_s": round(build_s, 1),
-                           "bfs_ms": round(tb, 3), "bfs_gteps": round(bst.edges_reached / 2.0 / (tb / 1e3) / 1e9, 2),
-                           "bfs_iterations": bst.iterations, "bfs_launches": int(bst.kernels),
-                           "cc_ms": round(tc, 3), "cc_iterations": cst.iterations,
-                           "cc_device_driven": bool(gg.tuning_get("persistent") & 4),
-                           "graphs_per_s": round(n_small / ((tb + tc) / 1e3), 1)}
+                           "bfs_cc_ms": round(tb, 3), "bfs_cc_wall_ms": round(wall, 3),
+                           "bfs_iterations": bst.iterations, "cc_iterations": cst.iterations,
+                           "graph_launches": glaunch, "kernels_in_launch": int(kernels),
+                           "bfs_gteps": round(bst.edges_reached / 2.0 / (tb / 1e3) / 1e9, 2),
+                           "graphs_per_s": round(n_small / (tb / 1e3), 1),
+                           "default_knobs_ms": round(t_def[0], 3), "tuned_knobs_ms": round(t_tun[0], 3),
+                           "knobs": tuned["knobs"] if use_tuned else "defaults (the tuned ones were slower)",
+                           "tuned_on": "a 200-graph union of the same family (BFS from 4 part roots + CC)",
+                           "tune_s": round(tune_s, 1),
+                           "parity": sg_parity}
+    AT.apply(defaults)
+    gg.graph_retune(U)
     U.close()
     return out
 

@@ -536,6 +536,7 @@ static void graph_free(gg_graph *g) {
     cudaFree(g->nonisolated);
     cudaFree(g->nonisolated_n);
     cudaFree(g->first_in);
+    cudaFree(g->pstate2);
     for (int i = 0; i < 2; ++i) {
         if (g->copy_done[i]) {
             cudaEventSynchronize(g->copy_done[i]);

@@ -1916,6 +1916,39 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     return GG_OK;
 }
 
+// Starts of the batch traversals, enqueued on the context's stream (kernel
+// launches only, so a graph capture can record them).
+// BFS levels from many roots: level = n+1, 0 at each root.
+gg_status enqueue_bfs_start(gg_graph *g, gg_prop *level, gg_prop *prev, const uint32_t *d_roots, uint32_t k) {
+    gg_ctx *ctx = g->ctx;
+    int32_t inf = (int32_t)g->n + 1;
+    GG_CHECK(gg_prop_fill(level, &inf));  // (prev: unused by level-synchronous steps)
+    if (k) {
+        k_scatter_zero_i32<<<(k + 255) / 256, 256, 0, ctx->stream>>>((int32_t *)level->d, (int32_t *)prev->d,
+                                                                     d_roots, k);
+        GG_LAUNCHED(ctx);
+    }
+    return GG_OK;
+}
+
+// CC: IDs[v] = v, prevIDs = IDs (CCv.C:246-248), PRESET_ZERO on a symmetric graph.
+gg_status enqueue_cc_start(gg_graph *g, gg_prop *label, gg_prop *prev) {
+    gg_ctx *ctx = g->ctx;
+    if (!g->n) return GG_OK;
+    k_iota_u32<<<persistent_grid(ctx, (g->n + 31) / 32), kBlock, 0, ctx->stream>>>((uint32_t *)label->d, g->n);
+    GG_LAUNCHED(ctx);
+    k_iota_u32<<<persistent_grid(ctx, (g->n + 31) / 32), kBlock, 0, ctx->stream>>>((uint32_t *)prev->d, g->n);
+    GG_LAUNCHED(ctx);
+    if (g->symmetric) {
+        k_preset_zero<<<ctx->sm_count, kBlock, 0, ctx->stream>>>(g->off, g->adj, 0, (uint32_t *)label->d,
+                                                                 (uint32_t *)prev->d);
+        GG_LAUNCHED(ctx);
+    }
+    return GG_OK;
+}
+
+gg_status run_tmp_prop(gg_graph *g, int slot, gg_dtype t, gg_prop **out) { return tmp_prop(g, slot, t, out); }
+
 }  // namespace gg
 
 using namespace gg;
@@ -2030,6 +2063,7 @@ gg_status gg_bfs_level_host_wait(gg_graph *g) {
         }
     return GG_OK;
 }
+
 
 gg_status gg_bfs_level_multi(gg_graph *g, const uint32_t *roots, uint32_t k, const gg_run_opts *o, gg_prop *level,
                              int32_t *host_level, gg_run_stats *st) {

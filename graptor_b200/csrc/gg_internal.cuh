@@ -156,6 +156,7 @@ struct gg_graph {
     std::vector<uint32_t *> pool_bins, pool_bitmaps;
     std::vector<uint64_t *> pool_cnt;
     void *pstate = nullptr;       // device state block of persistent traversals
+    void *pstate2 = nullptr;      // a second one (the CC run of a BFS + CC batch)
     void *gbfs = nullptr;         // graph-driven BFS: instantiated CUDA graph + control block
     uint32_t *wq = nullptr;       // work queue of fused (asynchronous) pushes
     size_t wq_cap = 0;
@@ -203,6 +204,9 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
                               int force_iter = -1, int force_variant = -1,
                               const uint32_t *d_roots = nullptr, uint32_t nroots = 0,
                               const PersistResume *resume = nullptr);
+gg_status enqueue_bfs_start(gg_graph *g, gg_prop *level, gg_prop *prev, const uint32_t *d_roots, uint32_t k);
+gg_status enqueue_cc_start(gg_graph *g, gg_prop *label, gg_prop *prev);
+gg_status run_tmp_prop(gg_graph *g, int slot, gg_dtype t, gg_prop **out);
 gg_status graph_adopt_device_csr(gg_ctx *ctx, uint32_t n, uint64_t m, uint64_t *off, uint32_t *adj, int symmetric,
                                  bool rows_sorted,
                                  gg_graph **out);

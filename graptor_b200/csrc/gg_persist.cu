@@ -20,6 +20,7 @@
 // DEV_ERR_TIMEOUT in the state block and every CTA returns at its next
 // barrier check, so the host sees GG_ERR_TIMEOUT and the context stays
 // usable.  Co-residency of all CTAs is guaranteed by the cooperative launch.
+#include <algorithm>
 #include <climits>
 #include <cuda_bf16.h>
 
@@ -27,6 +28,7 @@
 #include <type_traits>
 
 #include "gg_internal.cuh"
+#include "gg_batch.h"
 #include "gg_mlp.cuh"
 
 #include <cooperative_groups.h>
@@ -1534,10 +1536,25 @@ static const void *traverse_kernel() { return (const void *)k_traverse<R>; }
 
 const void *selector_weights(gg_graph *g);
 
-gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, bool start_all, uint32_t root,
-                              const gg_run_opts &opt, gg_run_stats *stats, int *iters_out, int force_iter,
-                              int force_variant, const uint32_t *d_roots, uint32_t nroots,
-                              const PersistResume *resume) {
+// The run's state starts from a device-side write (no host memory is read
+// when the stream runs, so the enqueue below can be captured in a graph).
+__global__ void k_state_init(PState *st, PFront f0, int all, int has_list, unsigned long long n,
+                             unsigned long long m) {
+    if (all) {
+        st->all[0] = 1;
+        f0.cnt[FC_NACTV] = n;
+        f0.cnt[FC_NACTE] = m;
+    }
+    if (has_list) st->has_list[0] = 1;
+}
+
+// Enqueues a device-driven run on the context's stream: buffers, the initial
+// frontier and state, and the cooperative launch; nothing waits on the host.
+// With a resumed run the state is copied from host values (not capture-safe).
+gg_status persistent_enqueue(gg_graph *g, const gg_emap_desc &d, int level_k, bool start_all, uint32_t root,
+                             const gg_run_opts &opt, int force_iter, int force_variant, const uint32_t *d_roots,
+                             uint32_t nroots, const PersistResume *resume, void *state, PArgs &P,
+                             const void **kfn_out, unsigned *grid_out, void *merge_scratch = nullptr) {
     gg_ctx *ctx = g->ctx;
     cudaStream_t s = ctx->stream;
     const Tuning &t = tuning();
@@ -1553,10 +1570,8 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
         for (auto &l : c.list) GG_CUDA(ctx, cudaMalloc(&l, ((size_t)g->n + 1) * 4));
         GG_CUDA(ctx, cudaMalloc(&c.cnt, 2 * sizeof(uint64_t)));
     }
-    if (!g->pstate) GG_CUDA(ctx, cudaMalloc(&g->pstate, sizeof(PState)));
-    PState *st = (PState *)g->pstate;
+    PState *st = (PState *)state;
     const size_t words = ((size_t)g->n + 31) / 32 + 1;
-    PArgs P;
     std::memset(&P, 0, sizeof(P));
     P.off = g->off;
     P.adj = g->adj;
@@ -1644,11 +1659,9 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
         GG_CUDA(ctx, cudaMemcpyAsync(&st->has_list[0], &hl, sizeof(int), cudaMemcpyHostToDevice, s));
         GG_CUDA(ctx, cudaMemcpyAsync(&st->reached_v, rc, sizeof(rc), cudaMemcpyHostToDevice, s));
     } else if (start_all) {
-        int one = 1;
-        GG_CUDA(ctx, cudaMemcpyAsync(&st->all[0], &one, sizeof(int), cudaMemcpyHostToDevice, s));
-        // counts of the all-true frontier: n vertices, m edges
-        uint64_t cnt[2] = {g->n, g->m};
-        GG_CUDA(ctx, cudaMemcpyAsync(P.fr[0].cnt, cnt, sizeof(cnt), cudaMemcpyHostToDevice, s));
+        // the all-true frontier: n vertices, m edges
+        k_state_init<<<1, 1, 0, s>>>(st, P.fr[0], 1, 0, g->n, g->m);
+        GG_LAUNCHED(ctx);
     } else {
         if (d_roots) {
             if (nroots)
@@ -1658,8 +1671,8 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
             k_traverse_init<<<1, 1, 0, s>>>(P.fr[0], root, g->off, P.smax, P.mmax, 1);
         }
         GG_LAUNCHED(ctx);
-        int one = 1;
-        GG_CUDA(ctx, cudaMemcpyAsync(&st->has_list[0], &one, sizeof(int), cudaMemcpyHostToDevice, s));
+        k_state_init<<<1, 1, 0, s>>>(st, P.fr[0], 0, 1, 0, 0);
+        GG_LAUNCHED(ctx);
     }
     const void *kfn = d.relax == GG_RELAX_MIN_PLUS1_I32 ? traverse_kernel<GG_RELAX_MIN_PLUS1_I32>()
                     : d.relax == GG_RELAX_MIN_U32      ? traverse_kernel<GG_RELAX_MIN_U32>()
@@ -1668,12 +1681,68 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
     unsigned grid = (unsigned)(ctx->sm_count * per_sm);
     if (resume && t.handoff_ctas > 0) grid = std::min(grid, (unsigned)t.handoff_ctas);
     // merge-path scratch: one count per list entry (<= n) + one per CTA
-    void *mp;
-    GG_CHECK(graph_scratch(g, ((size_t)g->n + grid + 1) * 8, &mp));
+    void *mp = merge_scratch;
+    if (!mp) GG_CHECK(graph_scratch(g, ((size_t)g->n + grid + 1) * 8, &mp));
     P.merge = (unsigned long long *)mp;
     void *args[] = {&P};
     GG_CUDA(ctx, cudaLaunchCooperativeKernel(kfn, dim3(grid), dim3(kPB), args, 0, s));
     ctx->launches++;
+    if (kfn_out) *kfn_out = kfn;
+    if (grid_out) *grid_out = grid;
+    return GG_OK;
+}
+
+// The records of a finished run from its state block (read to the host).
+static void persistent_collect(gg_graph *g, const PArgs &P, const PState &hs, gg_run_stats *stats, int *iters_out) {
+    *iters_out = hs.iterations;
+    g->force_rec.seen = P.force_iter >= 0 && P.force_iter < INT_MAX && hs.f_seen && hs.f_t1 >= hs.f_t0;
+    if (g->force_rec.seen) {
+        g->force_rec.iter_ms = (double)(hs.f_t1 - hs.f_t0) * 1e-6;
+        g->force_rec.rest_ms = (double)(hs.t_end - hs.f_t0) * 1e-6;
+        g->force_rec.nactv = (double)hs.f_nactv;
+        g->force_rec.nacte = (double)hs.f_nacte;
+        g->force_rec.reached = (double)hs.f_reached;
+    }
+    if (stats) {
+        stats->vertices_reached = hs.reached_v;
+        stats->edges_reached = hs.reached_e;
+        const int k = std::min(hs.iterations, GG_MAX_ITERS);
+        for (int i = 0; i < k; ++i) {
+            stats->variant[i] = hs.variant[i];
+            stats->nactv[i] = hs.nactv[i];
+            stats->nacte[i] = hs.nacte[i];
+            stats->scanned[i] = hs.scanned[i];
+            stats->iter_ms[i] = (double)(hs.t_ns[i + 1] - hs.t_ns[i]) * 1e-6;
+            stats->scanned_edges += hs.scanned[i];
+        }
+    }
+}
+
+gg_status persistent_state_read(gg_graph *g, void *state, const PArgs &P, gg_run_stats *stats, int *iters_out) {
+    gg_ctx *ctx = g->ctx;
+    PState hs;
+    GG_CUDA(ctx, cudaMemcpyAsync(&hs, state, sizeof(PState), cudaMemcpyDeviceToHost, ctx->stream));
+    GG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (hs.err & DEV_ERR_TIMEOUT) return set_error(ctx, GG_ERR_TIMEOUT, "traversal grid barrier timed out");
+    if (hs.err) return set_error(ctx, GG_ERR_STATE, "traversal device error");
+    persistent_collect(g, P, hs, stats, iters_out);
+    return GG_OK;
+}
+
+gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, bool start_all, uint32_t root,
+                              const gg_run_opts &opt, gg_run_stats *stats, int *iters_out, int force_iter,
+                              int force_variant, const uint32_t *d_roots, uint32_t nroots,
+                              const PersistResume *resume) {
+    gg_ctx *ctx = g->ctx;
+    cudaStream_t s = ctx->stream;
+    if (!g->pstate) GG_CUDA(ctx, cudaMalloc(&g->pstate, sizeof(PState)));
+    PState *st = (PState *)g->pstate;
+    PArgs P;
+    const void *kfn = nullptr;
+    unsigned grid = 0;
+    GG_CHECK(persistent_enqueue(g, d, level_k, start_all, root, opt, force_iter, force_variant, d_roots, nroots,
+                                resume, st, P, &kfn, &grid));
+    void *args[] = {&P};
     PState hs;
     GG_CUDA(ctx, cudaMemcpyAsync(&hs, st, sizeof(PState), cudaMemcpyDeviceToHost, s));
     GG_CUDA(ctx, cudaStreamSynchronize(s));
@@ -1712,30 +1781,170 @@ gg_status persistent_traverse(gg_graph *g, const gg_emap_desc &d, int level_k, b
         if (hs.err & DEV_ERR_TIMEOUT) return set_error(ctx, GG_ERR_TIMEOUT, "traversal grid barrier timed out");
         if (hs.err) return set_error(ctx, GG_ERR_STATE, "traversal device error");
     }
-    *iters_out = hs.iterations;
-    g->force_rec.seen = P.force_iter >= 0 && P.force_iter < INT_MAX && hs.f_seen && hs.f_t1 >= hs.f_t0;
-    if (g->force_rec.seen) {
-        g->force_rec.iter_ms = (double)(hs.f_t1 - hs.f_t0) * 1e-6;
-        g->force_rec.rest_ms = (double)(hs.t_end - hs.f_t0) * 1e-6;
-        g->force_rec.nactv = (double)hs.f_nactv;
-        g->force_rec.nacte = (double)hs.f_nacte;
-        g->force_rec.reached = (double)hs.f_reached;
-    }
-    if (stats) {
-        stats->vertices_reached = hs.reached_v;
-        stats->edges_reached = hs.reached_e;
-        const int k = std::min(hs.iterations, GG_MAX_ITERS);
-        for (int i = 0; i < k; ++i) {
-            stats->variant[i] = hs.variant[i];
-            stats->nactv[i] = hs.nactv[i];
-            stats->nacte[i] = hs.nacte[i];
-            stats->scanned[i] = hs.scanned[i];
-            stats->iter_ms[i] = (double)(hs.t_ns[i + 1] - hs.t_ns[i]) * 1e-6;
-            stats->scanned_edges += hs.scanned[i];
-        }
-    }
+    persistent_collect(g, P, hs, stats, iters_out);
     // the final frontier is empty; no host state to keep
     return GG_OK;
 }
 
+// Device time between construction and stop_record() (CUDA events on the
+// context's stream, recorded outside any capture).
+struct RunTimerP {
+    gg_ctx *ctx;
+    explicit RunTimerP(gg_ctx *c) : ctx(c) { cudaEventRecord(ctx->ev0, ctx->stream); }
+    void stop_record() { cudaEventRecord(ctx->ev1, ctx->stream); }
+    double elapsed() {
+        cudaEventSynchronize(ctx->ev1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        return ms;
+    }
+};
+
+// BFS levels from many roots and CC labels of one graph (the disjoint union
+// of many small graphs: every part's BFS from its first vertex and its
+// components), submitted as ONE CUDA graph launch: the BFS start, the
+// multi-root device-driven BFS, the CC start (PRESET_ZERO) and the
+// device-driven CC, captured on the context's stream.  The graph is captured
+// per call (every buffer it names is fixed for the call) and released after
+// it; the host waits once.  A capture the runtime refuses leaves the same
+// launches on the stream, one after the other.
+gg_status batch_bfs_cc(gg_graph *g, const uint32_t *roots, uint32_t k, gg_prop *level, gg_prop *label,
+                       gg_run_stats *bfs_st, gg_run_stats *cc_st, int *graph_launches, uint64_t *kernel_nodes) {
+    gg_ctx *ctx = g->ctx;
+    cudaStream_t s = ctx->stream;
+    std::vector<uint32_t> r(roots, roots + k);
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+    if (!r.empty() && r.back() >= g->n) return set_error(ctx, GG_ERR_ARG, "gg_batch_bfs_cc: root out of range");
+    if (!level) GG_CHECK(run_tmp_prop(g, 0, GG_I32, &level));
+    if (!label) GG_CHECK(run_tmp_prop(g, 2, GG_U32, &label));
+    gg_prop *prev1, *prev2;
+    GG_CHECK(run_tmp_prop(g, 1, GG_I32, &prev1));
+    GG_CHECK(run_tmp_prop(g, 3, GG_U32, &prev2));
+    // every buffer the captured launches name exists before the capture
+    for (auto &f : g->tmp_front)
+        if (!f) GG_CHECK(gg_frontier_create(g, &f));
+    for (auto *f : g->tmp_front) {
+        GG_CHECK(frontier_alloc_bins(f));
+        GG_CHECK(frontier_alloc_bitmap(f));
+    }
+    CandLists &c = g->cand;
+    if (!c.list[0]) {
+        for (auto &l : c.list) GG_CUDA(ctx, cudaMalloc(&l, ((size_t)g->n + 1) * 4));
+        GG_CUDA(ctx, cudaMalloc(&c.cnt, 2 * sizeof(uint64_t)));
+    }
+    if (!g->pstate) GG_CUDA(ctx, cudaMalloc(&g->pstate, sizeof(PState)));
+    if (!g->pstate2) GG_CUDA(ctx, cudaMalloc(&g->pstate2, sizeof(PState)));
+    void *merge;
+    GG_CHECK(graph_scratch(g, ((size_t)g->n + (size_t)ctx->sm_count * 32 + 1) * 8, &merge));
+    uint32_t *d_roots = nullptr;
+    GG_CUDA(ctx, cudaMalloc(&d_roots, (r.size() + 1) * 4));
+    if (!r.empty()) GG_CUDA(ctx, cudaMemcpyAsync(d_roots, r.data(), r.size() * 4, cudaMemcpyHostToDevice, s));
+    GG_CUDA(ctx, cudaStreamSynchronize(s));
+    gg_run_opts opt_b, opt_c;
+    std::memset(&opt_b, 0, sizeof(opt_b));
+    opt_b.threshold = GG_THRESH_DEFAULT;
+    opt_b.variant = GG_VAR_AUTO;
+    opt_c = opt_b;
+    opt_c.threshold = GG_THRESH_FRAC;  // CCv.C:309 emap_step(F, 5)
+    opt_c.threshold_k = 5;
+    gg_emap_desc db, dc;
+    std::memset(&db, 0, sizeof(db));
+    db.relax = GG_RELAX_MIN_PLUS1_I32;
+    db.a = level;
+    db.dst_filter = GG_FILTER_GT_CONST;
+    db.src_level_sync = 1;
+    db.record = GG_RECORD_NE_PREV;
+    db.prev = prev1;
+    db.threshold = opt_b.threshold;
+    db.variant = GG_VAR_AUTO;
+    std::memset(&dc, 0, sizeof(dc));
+    dc.relax = GG_RELAX_MIN_U32;
+    dc.a = label;
+    dc.dst_filter = GG_FILTER_NE_ZERO;
+    dc.record = GG_RECORD_NE_PREV;
+    dc.prev = prev2;
+    dc.threshold = opt_c.threshold;
+    dc.threshold_k = opt_c.threshold_k;
+    dc.variant = GG_VAR_AUTO;
+    PArgs P1, P2;
+    auto enqueue_all = [&]() -> gg_status {
+        GG_CHECK(enqueue_bfs_start(g, level, prev1, d_roots, (uint32_t)r.size()));
+        GG_CHECK(persistent_enqueue(g, db, 1, false, 0, opt_b, -1, -1, d_roots, (uint32_t)r.size(), nullptr,
+                                    g->pstate, P1, nullptr, nullptr, merge));
+        GG_CHECK(enqueue_cc_start(g, label, prev2));
+        GG_CHECK(persistent_enqueue(g, dc, 0, true, 0, opt_c, -1, -1, nullptr, 0, nullptr, g->pstate2, P2, nullptr,
+                                    nullptr, merge));
+        return GG_OK;
+    };
+    RunTimerP tm(ctx);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const uint64_t l0 = ctx->launches;
+    gg_status st = GG_OK;
+    bool captured = false;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        st = enqueue_all();
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (st == GG_OK && e == cudaSuccess && graph &&
+            cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess && cudaGraphLaunch(exec, s) == cudaSuccess)
+            captured = true;
+        cudaGetLastError();  // a refused capture leaves no sticky error
+    }
+    if (kernel_nodes) *kernel_nodes = ctx->launches - l0;
+    if (!captured) {
+        // the same launches, one after the other
+        ctx->launches = l0;
+        st = enqueue_all();
+    } else {
+        ctx->launches = l0 + 1;
+    }
+    if (graph_launches) *graph_launches = captured ? 1 : 0;
+    tm.stop_record();
+    int it1 = 0, it2 = 0;
+    if (st == GG_OK) st = persistent_state_read(g, g->pstate, P1, bfs_st, &it1);
+    if (st == GG_OK) st = persistent_state_read(g, g->pstate2, P2, cc_st, &it2);
+    const double ms = tm.elapsed();
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaFree(d_roots);
+    GG_CHECK(st);
+    if (bfs_st) {
+        bfs_st->iterations = it1;
+        bfs_st->total_ms = ms;
+        bfs_st->kernels = captured ? 1 : ctx->launches - l0;
+    }
+    if (cc_st) {
+        cc_st->iterations = it2;
+        cc_st->total_ms = ms;
+        cc_st->kernels = 0;
+    }
+    return GG_OK;
+}
+
 }  // namespace gg
+
+extern "C" gg_status gg_batch_bfs_cc(gg_graph *g, const uint32_t *roots, uint32_t k, gg_prop *level,
+                                     gg_prop *label, int32_t *host_level, uint32_t *host_label,
+                                     gg_run_stats *bfs_stats, gg_run_stats *cc_stats, int *graph_launches,
+                                     uint64_t *kernel_launches) {
+    using namespace gg;
+    if (!g || (k && !roots)) return GG_ERR_ARG;
+    if (level && (level->g != g || level->t != GG_I32)) return set_error(g->ctx, GG_ERR_ARG, "level must be an I32 property of g");
+    if (label && (label->g != g || label->t != GG_U32)) return set_error(g->ctx, GG_ERR_ARG, "label must be a U32 property of g");
+    if (bfs_stats) std::memset(bfs_stats, 0, sizeof(*bfs_stats));
+    if (cc_stats) std::memset(cc_stats, 0, sizeof(*cc_stats));
+    if (g->n == 0) return GG_OK;
+    GG_CHECK(batch_bfs_cc(g, roots, k, level, label, bfs_stats, cc_stats, graph_launches, kernel_launches));
+    if (host_level) {
+        gg_prop *lv = level;
+        if (!lv) GG_CHECK(run_tmp_prop(g, 0, GG_I32, &lv));
+        GG_CHECK(gg_prop_download(lv, host_level));
+    }
+    if (host_label) {
+        gg_prop *lb = label;
+        if (!lb) GG_CHECK(run_tmp_prop(g, 2, GG_U32, &lb));
+        GG_CHECK(gg_prop_download(lb, host_label));
+    }
+    return GG_OK;
+}

@@ -654,7 +654,9 @@ def _batch_lib():
         L.gg_ppr.argtypes = [vp, vp, C.c_int, C.c_float, C.c_int, vp, C.POINTER(RunStats)]
         L.gg_graph_union.argtypes = [vp, vp, C.c_int, C.POINTER(vp), vp]
         L.gg_bfs_level_multi.argtypes = [vp, vp, u32, C.POINTER(RunOpts), vp, vp, C.POINTER(RunStats)]
-        for n in ["gg_msbfs", "gg_ppr", "gg_graph_union", "gg_bfs_level_multi"]:
+        L.gg_batch_bfs_cc.argtypes = [vp, vp, u32, vp, vp, vp, vp, C.POINTER(RunStats), C.POINTER(RunStats),
+                                      C.POINTER(C.c_int), C.POINTER(C.c_uint64)]
+        for n in ["gg_msbfs", "gg_ppr", "gg_graph_union", "gg_bfs_level_multi", "gg_batch_bfs_cc"]:
             getattr(L, n).restype = C.c_int
         L._batch_bound = True
     return L
@@ -696,6 +698,21 @@ def bfs_level_multi(g: Graph, roots, host: bool = True, opts: RunOpts = None, st
                                                 C.byref(stats) if stats is not None else None),
                 "gg_bfs_level_multi")
     return out
+
+
+def batch_bfs_cc(g: Graph, roots, host: bool = True, bfs_stats: RunStats = None, cc_stats: RunStats = None):
+    """BFS levels from every root at once and CC labels, one CUDA graph launch:
+    (levels, labels, graph_launches, kernel_launches); arrays None if not host."""
+    r = np.ascontiguousarray(roots, dtype=np.uint32)
+    lv = np.empty(g.n, dtype=np.int32) if host else None
+    lb = np.empty(g.n, dtype=np.uint32) if host else None
+    gl, kl = C.c_int(), C.c_uint64()
+    g.ctx.check(_batch_lib().gg_batch_bfs_cc(g.h, _p(r), len(r), None, None, _p(lv) if host else None,
+                                             _p(lb) if host else None,
+                                             C.byref(bfs_stats) if bfs_stats is not None else None,
+                                             C.byref(cc_stats) if cc_stats is not None else None,
+                                             C.byref(gl), C.byref(kl)), "gg_batch_bfs_cc")
+    return lv, lb, gl.value, kl.value
 
 
 # ---------------------------------------------------------------------------

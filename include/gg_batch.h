@@ -55,6 +55,22 @@ GG_API gg_status gg_graph_union(gg_ctx *ctx, gg_graph *const *parts, int k, gg_g
 GG_API gg_status gg_bfs_level_multi(gg_graph *g, const uint32_t *roots, uint32_t k, const gg_run_opts *o,
                                     gg_prop *level, int32_t *host_level, gg_run_stats *st);
 
+/* BFS levels from several roots and CC labels of one graph -- a disjoint
+ * union of many small graphs (gg_graph_union), each part's BFS from its own
+ * root and its components -- submitted as ONE CUDA graph launch (the BFS
+ * start, the device-driven multi-root BFS, the CC start and the
+ * device-driven CC; the host waits once).  The reference runs BFSLVLv.C and
+ * CCv.C once per graph (bench/BFSLVLv.C:110-254, bench/CCv.C:221-471); this
+ * batch has no counterpart there.  level (I32) / label (U32) may be NULL
+ * (library temporaries).  bfs_stats / cc_stats receive each run's records
+ * and the batch's device time in total_ms; *graph_launches is 1 when the
+ * work went out as one graph launch (0 if the runtime refused the capture
+ * and the launches went out one by one) and *kernel_launches the kernels
+ * the batch holds.  Duplicate roots are ignored. */
+GG_API gg_status gg_batch_bfs_cc(gg_graph *g, const uint32_t *roots, uint32_t k, gg_prop *level, gg_prop *label,
+                                 int32_t *host_level, uint32_t *host_label, gg_run_stats *bfs_stats,
+                                 gg_run_stats *cc_stats, int *graph_launches, uint64_t *kernel_launches);
+
 #ifdef __cplusplus
 }
 #endif

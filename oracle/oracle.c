@@ -325,6 +325,38 @@ ORC_API int orc_bfs_level(uint32_t n, const uint64_t *off, const uint32_t *adj,
     return depth;
 }
 
+/* BFS levels with several start vertices at level 0 (a multi-root run of
+ * BFSLVLv's level relaxation, BFSLVLv.C:165-216, as on a disjoint union of
+ * graphs with one root per part): unreached = n + 1.  Returns the depth. */
+ORC_API int orc_bfs_level_multi(uint32_t n, const uint64_t *off, const uint32_t *adj,
+                                const uint32_t *roots, uint64_t k, int32_t *level) {
+    for (uint32_t v = 0; v < n; ++v) level[v] = (int32_t)(n + 1);
+    uint32_t *q = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    if (!q) return -1;
+    uint64_t head = 0, tail = 0;
+    for (uint64_t i = 0; i < k; ++i) {
+        if (roots[i] >= n) { free(q); return -1; }
+        if (level[roots[i]] != 0) {
+            level[roots[i]] = 0;
+            q[tail++] = roots[i];
+        }
+    }
+    int depth = 0;
+    while (head < tail) {
+        uint32_t u = q[head++];
+        if (level[u] + 1 > depth) depth = level[u] + 1;
+        for (uint64_t e = off[u]; e < off[u + 1]; ++e) {
+            uint32_t v = adj[e];
+            if (level[v] == (int32_t)(n + 1)) {
+                level[v] = level[u] + 1;
+                q[tail++] = v;
+            }
+        }
+    }
+    free(q);
+    return depth;
+}
+
 /* Sum of out-degrees of reached vertices (= directed edges incident to
  * the reached component of a symmetric graph): the GTEPS numerator. */
 ORC_API uint64_t orc_reached_edges(uint32_t n, const uint64_t *off, const int32_t *level) {

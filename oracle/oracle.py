@@ -44,6 +44,7 @@ def lib() -> C.CDLL:
         L.orc_write_bin.argtypes = [C.c_char_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p]
         L.orc_read_bin.argtypes = [C.c_char_p, u32p, u64p, C.POINTER(u64p), C.POINTER(u32p)]
         L.orc_bfs_level.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        L.orc_bfs_level_multi.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]
         L.orc_reached_edges.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p]
         L.orc_reached_edges.restype = C.c_uint64
         L.orc_check_parents.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_uint32,
@@ -157,6 +158,15 @@ def read_bin(path: str) -> Graph:
 def bfs_level(g: Graph, root: int) -> np.ndarray:
     lv = np.empty(g.n, dtype=np.int32)
     lib().orc_bfs_level(g.n, _p(g.off), _p(g.adj), root, _p(lv))
+    return lv
+
+
+def bfs_level_multi(g: Graph, roots) -> np.ndarray:
+    """BFS levels with every root at level 0 (unreached n + 1)."""
+    r = np.ascontiguousarray(roots, dtype=np.uint32)
+    lv = np.empty(g.n, dtype=np.int32)
+    if lib().orc_bfs_level_multi(g.n, _p(g.off), _p(g.adj), _p(r), len(r), _p(lv)) < 0:
+        raise ValueError("root out of range")
     return lv
 
 

@@ -65,3 +65,19 @@ def test_union_layout():
     for i, p in enumerate(parts):
         lab = O.cc(u)[base[i]:base[i + 1]] - base[i]
         assert np.array_equal(lab, O.cc(p))
+
+
+def test_multi_root_bfs_over_union_is_per_part_bfs():
+    """The oracle's multi-root BFS (the checker of the one-launch union
+    batch) equals each part's own BFS from its first vertex."""
+    parts = [O.rmat(8, 2000, seed=i) for i in range(4)] + [O.grid(9, 13, seed=2, del_bp=500),
+                                                           O.from_edges(5, [(1, 2)])]
+    u, base = B.union(parts)
+    lv = O.bfs_level_multi(u, base[:-1])
+    for i, p in enumerate(parts):
+        a, b = int(base[i]), int(base[i + 1])
+        got = lv[a:b].copy()
+        got[got == u.n + 1] = p.n + 1
+        assert np.array_equal(got, O.bfs_level(p, 0)), i
+    # duplicate roots count once
+    assert np.array_equal(O.bfs_level_multi(u, [0, 0, 3]), O.bfs_level_multi(u, [3, 0]))

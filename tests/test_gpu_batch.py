@@ -160,6 +160,29 @@ def test_union_bfs_and_cc_per_part(ctx):
     U.close()
 
 
+def test_batch_bfs_cc_one_graph_launch(ctx):
+    """BFS from every part's vertex 0 and CC of the union, submitted as one
+    CUDA graph launch: per-part levels and labels equal the oracle's, twice
+    in a row."""
+    parts = small_graph_family(41, 5)
+    Gs = [upload(ctx, p) for p in parts]
+    U, base = gg.graph_union(ctx, Gs)
+    for _ in range(2):
+        bs, cs = gg.RunStats(), gg.RunStats()
+        lv, lb, glaunch, kernels = gg.batch_bfs_cc(U, base[:-1], bfs_stats=bs, cc_stats=cs)
+        assert glaunch == 1 and kernels > 2
+        assert bs.iterations >= 1 and cs.iterations >= 1
+        for i, p in enumerate(parts):
+            a, b = int(base[i]), int(base[i + 1])
+            got = lv[a:b].copy()
+            got[got == U.n + 1] = p.n + 1
+            assert np.array_equal(got, O.bfs_level(p, 0)), i
+            assert np.array_equal(lb[a:b] - a, O.cc(p)), i
+    for G in Gs:
+        G.close()
+    U.close()
+
+
 def test_bfs_level_multi_single_root_matches_bfs_level(ctx):
     g = O.rmat(11, 1 << 15, 8)
     G = upload(ctx, g)
