@@ -940,12 +940,24 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
 
 gg_status pr_edgemap_gather(gg_graph *g, const gg_emap_desc *d, gg_frontier *in);
 
-// CCv's validation edgemap (CCv.C:612-617): relax(s, d) = a[d] != a[s] with a
-// reduction record, i.e. d is recorded when an active in-neighbour holds
-// another value; nothing is written.  A warp per 32-vertex word walks the
-// word's in-rows one after the other, the lanes striding each row.
-__global__ void __launch_bounds__(kBlock) k_check_ne(EmapArgs A, const uint32_t *__restrict__ a,
-                                                     const uint32_t *__restrict__ src_bits) {
+// The analytics' validation edgemaps: relax(s, d) returns a condition and
+// the record is a reduction, so d is recorded when an active in-neighbour
+// satisfies it; nothing is written.  CCv.C:612-617: a[d] != a[s] (labels);
+// BFSLVLv.C:288-305: a[s] > a[d] + 1 || a[s] < a[d] - 1 (symmetric graph)
+// or a[s] < a[d] - 1 (directed) on the levels.
+template <int K>
+__device__ __forceinline__ bool check_hit(uint32_t as, uint32_t ad) {
+    if constexpr (K == GG_RELAX_NE_CHECK) return as != ad;
+    else if constexpr (K == GG_RELAX_GAP_CHECK)
+        return (int64_t)(int32_t)as > (int64_t)(int32_t)ad + 1 || (int64_t)(int32_t)as < (int64_t)(int32_t)ad - 1;
+    else return (int64_t)(int32_t)as < (int64_t)(int32_t)ad - 1;
+}
+
+// A warp per 32-vertex word walks the word's in-rows one after the other,
+// the lanes striding each row.
+template <int K>
+__global__ void __launch_bounds__(kBlock) k_check(EmapArgs A, const uint32_t *__restrict__ a,
+                                                  const uint32_t *__restrict__ src_bits) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t nwords = (A.n + 31u) >> 5;
     const uint32_t nw = (gridDim.x * kBlock) >> 5;
@@ -962,7 +974,7 @@ __global__ void __launch_bounds__(kBlock) k_check_ne(EmapArgs A, const uint32_t 
                 bool hit = false;
                 if (base + lane < end) {
                     const uint32_t s = A.in_adj[base + lane];
-                    hit = (!src_bits || dev::bit_test(src_bits, s)) && a[s] != ad;
+                    hit = (!src_bits || dev::bit_test(src_bits, s)) && check_hit<K>(a[s], ad);
                 }
                 found = __any_sync(FULL, hit);
             }
@@ -977,10 +989,11 @@ __global__ void __launch_bounds__(kBlock) k_check_ne(EmapArgs A, const uint32_t 
     flush_counts<kBlock>(A, nv, ne, 0);
 }
 
-static gg_status check_ne(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_frontier *out) {
+static gg_status check_relax(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_frontier *out) {
     gg_ctx *ctx = g->ctx;
-    if (d->a->t != GG_U32) return set_error(ctx, GG_ERR_ARG, "NE_CHECK relaxes a uint32 property");
-    if (d->dst_filter != GG_FILTER_NONE) return set_error(ctx, GG_ERR_UNSUPPORTED, "NE_CHECK takes no dst filter");
+    if (d->a->t != (d->relax == GG_RELAX_NE_CHECK ? GG_U32 : GG_I32))
+        return set_error(ctx, GG_ERR_ARG, "check relax: NE on a uint32 property, GAP / AHEAD on an int32 one");
+    if (d->dst_filter != GG_FILTER_NONE) return set_error(ctx, GG_ERR_UNSUPPORTED, "check relaxes take no dst filter");
     if (!out) return GG_OK;  // nothing is written, so nothing to do without a record
     EmapArgs A;
     memset(&A, 0, sizeof(A));
@@ -1005,7 +1018,11 @@ static gg_status check_ne(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, g
     A.out_b2 = out->bins[2];
     A.out_cnt = (unsigned long long *)out->d_cnt;
     const uint64_t words = ((uint64_t)g->n + 31) / 32;
-    k_check_ne<<<persistent_grid(ctx, words), kBlock, 0, ctx->stream>>>(A, (const uint32_t *)d->a->d, src_bits);
+    const unsigned grid = persistent_grid(ctx, words);
+    const uint32_t *av = (const uint32_t *)d->a->d;
+    if (d->relax == GG_RELAX_NE_CHECK) k_check<GG_RELAX_NE_CHECK><<<grid, kBlock, 0, ctx->stream>>>(A, av, src_bits);
+    else if (d->relax == GG_RELAX_GAP_CHECK) k_check<GG_RELAX_GAP_CHECK><<<grid, kBlock, 0, ctx->stream>>>(A, av, src_bits);
+    else k_check<GG_RELAX_AHEAD_CHECK><<<grid, kBlock, 0, ctx->stream>>>(A, av, src_bits);
     GG_LAUNCHED(ctx);
     out->all = false;
     out->has_list = true;
@@ -1033,9 +1050,10 @@ gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_f
         }
         return GG_OK;
     }
-    if (d->relax == GG_RELAX_NE_CHECK) {
-        if (d->record != GG_RECORD_REDUCTION && out) return set_error(ctx, GG_ERR_UNSUPPORTED, "NE_CHECK records by reduction");
-        GG_CHECK(check_ne(g, d, in, out));
+    if (d->relax >= GG_RELAX_NE_CHECK && d->relax <= GG_RELAX_AHEAD_CHECK) {
+        if (d->record != GG_RECORD_REDUCTION && out)
+            return set_error(ctx, GG_ERR_UNSUPPORTED, "check relaxes record by reduction");
+        GG_CHECK(check_relax(g, d, in, out));
         if (stats) {
             memset(stats, 0, sizeof(*stats));
             stats->variant = GG_VAR_PULL_DENSE;

@@ -181,8 +181,12 @@ typedef enum gg_relax_kind {
     GG_RELAX_MIN_U32 = 1,       /* a[d].min(a[s]) on uint32          (CCv.C:575-581)     */
     GG_RELAX_SETIF_U32 = 2,     /* a[d].setif(s): a[d] = s once      (BFSv.C:144-146)    */
     GG_RELAX_ADD_GATHER = 3,    /* y[d] += cast(contrib[s])          (PRv.C:202-212)     */
-    GG_RELAX_NE_CHECK = 4       /* a[d] != a[s] on uint32: records d, writes nothing
-                                   (CCv.C:612-617, the validation edgemap)            */
+    /* checks: record d when the condition holds for an active in-neighbour
+     * s; nothing is written (the analytics' validation edgemaps) */
+    GG_RELAX_NE_CHECK = 4,      /* a[d] != a[s] on uint32            (CCv.C:612-617)     */
+    GG_RELAX_GAP_CHECK = 5,     /* a[s] > a[d] + 1 || a[s] < a[d] - 1 on int32
+                                                                      (BFSLVLv.C:288-294) */
+    GG_RELAX_AHEAD_CHECK = 6    /* a[s] < a[d] - 1 on int32          (BFSLVLv.C:299-305) */
 } gg_relax_kind;
 
 /* dst filters (api::filter(weak, dst, lambda), api.h:687-706). */

@@ -926,6 +926,38 @@ inline void lower_relax(const NP &r, gg_emap_desc &d) {
         d.a = r->c[0]->prop;
         return;
     }
+    // a[s] > a[d] + 1 || a[s] < a[d] - 1 and a[s] < a[d] - 1 on int32 levels (BFSLVLv.C:288-305)
+    auto ahead = [](const NP &x, gg_prop *&p) {  // a[s] < a[d] - 1
+        if (x->k == NK::Lt && is_ref_at(x->c[0], NK::VarSrc) && x->c[1]->k == NK::Sub &&
+            is_ref_at(x->c[1]->c[0], NK::VarDst) && is_const(x->c[1]->c[1], 1) && x->c[0]->prop == x->c[1]->c[0]->prop &&
+            x->c[0]->dt == GG_I32) {
+            p = x->c[0]->prop;
+            return true;
+        }
+        return false;
+    };
+    auto behind = [](const NP &x, gg_prop *&p) {  // a[s] > a[d] + 1
+        if (x->k == NK::Gt && is_ref_at(x->c[0], NK::VarSrc) && x->c[1]->k == NK::Add &&
+            is_ref_at(x->c[1]->c[0], NK::VarDst) && is_const(x->c[1]->c[1], 1) && x->c[0]->prop == x->c[1]->c[0]->prop &&
+            x->c[0]->dt == GG_I32) {
+            p = x->c[0]->prop;
+            return true;
+        }
+        return false;
+    };
+    {
+        gg_prop *p1 = nullptr, *p2 = nullptr;
+        if (r->k == NK::LOr && behind(r->c[0], p1) && ahead(r->c[1], p2) && p1 == p2) {
+            d.relax = GG_RELAX_GAP_CHECK;
+            d.a = p1;
+            return;
+        }
+        if (ahead(r, p1)) {
+            d.relax = GG_RELAX_AHEAD_CHECK;
+            d.a = p1;
+            return;
+        }
+    }
     if (r->k == NK::SetIf && is_ref_at(r->c[0], NK::VarDst) && r->c[1]->k == NK::VarSrc && r->c[0]->dt == GG_U32) {
         d.relax = GG_RELAX_SETIF_U32;  // a[d].setif(s)
         d.a = r->c[0]->prop;
