@@ -161,7 +161,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm), "source": src}
 
 
-def dist_setup(args):
+def dist_setup(args, backend: str = "nccl"):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE); the
+    replicas share nothing on the data path, the process group only carries
+    the barrier and the max / sum of the timing scalars."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -169,9 +172,12 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return ws, rank, local
 
 
@@ -181,24 +187,29 @@ def barrier(ws):
         dist.barrier()
 
 
-def max_over_ranks(x: float, ws: int) -> float:
+def _reduce(x: float, ws: int, op: str) -> float:
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    return _reduce(x, ws, "max")
 
 
 def sum_over_ranks(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    return _reduce(x, ws, "sum")
+
+
+def replica_roots(roots, ws: int, rank: int, count: int):
+    """Rank `rank`'s sequence of `count` roots: the 64 roots dealt round-robin
+    over the ranks (step k of rank r takes root (k * ws + r) mod 64)."""
+    return [int(roots[(k * ws + rank) % len(roots)]) for k in range(count)]
 
 
 def pick_roots(deg: np.ndarray) -> np.ndarray:
@@ -731,7 +742,7 @@ def run_ours(args, ws, rank, local):
 
     lvl = g.prop(gg.I32)
     opts = gg.default_opts(collect=True)
-    seq = [int(roots[(k * ws + rank) % NROOTS]) for k in range(args.warmup + args.steps)]
+    seq = replica_roots(roots, ws, rank, args.warmup + args.steps)
 
     # ---- warm-up ----
     for k in range(args.warmup):
