@@ -981,6 +981,9 @@ def iter_table(st):
 
 def run_case(a):
     from graptor_b200 import gg
+    for kv in a.knob:
+        name, val = kv.split("=")
+        gg.tuning_set(name, int(val))
     if a.persistent is not None:
         gg.tuning_set("persistent", a.persistent)
     if a.graph_mode is not None:
@@ -992,7 +995,8 @@ def run_case(a):
         g = ctx.er(1 << a.scale, 32.0, 1, dangling_bp=100, symmetric=False)
     else:
         g = ctx.rmat(a.scale, 16 << a.scale, 1)
-    out = {"case": a.case, "graph": a.graph, "n": g.n, "m": g.m, "persistent": gg.tuning_get("persistent")}
+    out = {"case": a.case, "graph": a.graph, "n": g.n, "m": g.m, "persistent": gg.tuning_get("persistent"),
+           "knobs": a.knob}
     opts = gg.default_opts(gg.THRESH_LEARNED if a.threshold == "learned" else gg.THRESH_DEFAULT, collect=True)
     if a.threshold == "learned":
         from graptor_b200.selector_train import load_selector
@@ -1089,6 +1093,7 @@ def main():
     ap.add_argument("--persistent", type=int, default=None, help="tuning knob: device-driven analytics mask")
     ap.add_argument("--threshold", default="default", choices=["default", "learned"])
     ap.add_argument("--graph-mode", type=int, default=None, help="tuning knob: graph-driven BFS levels (0/1)")
+    ap.add_argument("--knob", action="append", default=[], help="name=value of a tuning knob (repeatable)")
     args = ap.parse_args()
     if args.case:
         return run_case(args)

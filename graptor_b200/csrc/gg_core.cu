@@ -474,10 +474,12 @@ gg_status build_heavy_rows(gg_graph *g) {
 }
 
 __global__ void k_first_in(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj, uint32_t n,
-                           uint2 *first_in) {
+                           uint4 *first_in) {
     for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < n; d += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t b = in_off[d], e = in_off[d + 1];
-        first_in[d] = make_uint2(b < e ? in_adj[b] : 0xFFFFFFFFu, b + 1 < e ? in_adj[b + 1] : 0xFFFFFFFFu);
+        const uint64_t deg = e - b;
+        first_in[d] = make_uint4(b < e ? in_adj[b] : 0xFFFFFFFFu, b + 1 < e ? in_adj[b + 1] : 0xFFFFFFFFu,
+                                 deg > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)deg, 0u);
     }
 }
 
@@ -514,7 +516,7 @@ static gg_status graph_finish(gg_graph *g) {
     cudaFree(d_best);
     g->maxdeg = (uint32_t)(h_best >> 32);
     g->maxdeg_v = g->n ? (uint32_t)(0xFFFFFFFFull - (h_best & 0xFFFFFFFFull)) : 0;
-    GG_CUDA(ctx, cudaMalloc(&g->first_in, ((size_t)g->n + 1) * sizeof(uint2)));
+    GG_CUDA(ctx, cudaMalloc(&g->first_in, ((size_t)g->n + 1) * sizeof(uint4)));
     if (g->n) {
         k_first_in<<<grid_for(ctx, g->n), 256, 0, st>>>(g->in_off, g->in_adj, g->n, g->first_in);
         GG_LAUNCHED(ctx);
@@ -783,7 +785,7 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     if (k == "bin_small_max") t.bin_small_max = (uint32_t)v;
     else if (k == "bin_medium_max") t.bin_medium_max = (uint32_t)v;
     else if (k == "pull_k" && v >= 1 && v <= 1024) t.pull_k = (int)v;
-    else if (k == "pull_first" && v <= 1) t.pull_first = (int)v;
+    else if (k == "pull_first" && v <= 2) t.pull_first = (int)v;
     else if (k == "push_k" && v >= 1 && v <= 1024) t.push_k = (int)v;
     else if (k == "heavy_deg" && v >= 32) t.heavy_deg = (uint32_t)v;
     else if (k == "heavy_chunk" && v >= 32) t.heavy_chunk = (uint32_t)v;

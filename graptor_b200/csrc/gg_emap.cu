@@ -75,7 +75,8 @@ struct EmapArgs {
     uint32_t *cand_out;                 // vertices still passing after this step
     unsigned long long *cand_out_n;
     const uint64_t *word_prefix;        // full-scan pull: per-word cost prefix
-    const uint2 *first_in;              // pull: first two in-neighbours per vertex, or null
+    const uint4 *first_in;              // pull: first two in-neighbours + in-degree per vertex, or null
+    int lazy_off;                       // pull: offsets only for rows the first two edges do not settle
 };
 
 template <int R>
@@ -213,17 +214,22 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
         const uint32_t d = CAND ? (valid ? A.cand[item] : 0u) : (uint32_t)item;
         V best = Op<R>::none();
         uint64_t e = 0, end = 0;
-        uint2 f2 = make_uint2(0u, 0u);
+        uint4 f2 = make_uint4(0u, 0u, 0u, 0u);
+        const bool lazy = A.first_in && A.lazy_off;
         if (valid) {
             best = op.load(d);
-            e = A.in_off[d];
-            end = A.in_off[d + 1];
             if (A.first_in) f2 = A.first_in[d];
+            if (!lazy) {
+                e = A.in_off[d];
+                end = A.in_off[d + 1];
+            } else {
+                end = f2.z;  // row bounds relative to its start until the offsets are needed
+            }
         }
         bool act = valid && op.dst_ok(best);
         bool changed = false;
-        const uint64_t beg = e;
-        const uint64_t lim = min(end, e + (uint64_t)A.K);
+        uint64_t beg = e;
+        uint64_t lim = min(end, e + (uint64_t)A.K);
         if (A.first_in && act && e < lim) {
             // the row's first two in-neighbours, loaded beside its offsets:
             // the same edges in the same order as the loop below takes them
@@ -245,6 +251,16 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
                 }
             }
             e += used;
+        }
+        if (lazy && valid) {
+            // the row's offsets, for rows still open after their first two edges
+            if (act && e < end) {
+                const uint64_t b0 = A.in_off[d];
+                e += b0;
+                end += b0;
+                beg = b0;
+                lim = min(end, b0 + (uint64_t)A.K);
+            }
         }
         while (act && e < lim) {
             const int cnt = (int)min((uint64_t)4, lim - e);
@@ -747,6 +763,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     A.K = variant == GG_VAR_PULL_DENSE ? t.pull_k : t.push_k;
     A.word_prefix = g->heavy.pull_prefix;
     A.first_in = t.pull_first ? g->first_in : nullptr;
+    A.lazy_off = t.pull_first == 2;
     const bool have_out = out != nullptr && d->record != GG_RECORD_NONE;
     if (have_out) {
         GG_CHECK(frontier_alloc_bins(out));
@@ -1285,7 +1302,8 @@ struct GCtl {
     int pull_k, push_k;
     const uint64_t *off, *in_off, *word_prefix;
     const uint32_t *adj, *in_adj;
-    const uint2 *first_in;
+    const uint4 *first_in;
+    int lazy_off;
     const uint32_t *nonisolated;
     const unsigned long long *nonisolated_n;
     uint32_t *cand[2];
@@ -1446,6 +1464,7 @@ __device__ void decide_step(GCtl *c) {
     A.K = push ? c->push_k : c->pull_k;
     A.word_prefix = c->word_prefix;
     A.first_in = push ? nullptr : c->first_in;
+    A.lazy_off = c->lazy_off;
     A.out_b0 = O.bins[0];
     A.out_b1 = O.bins[1];
     A.out_b2 = O.bins[2];
@@ -1853,6 +1872,7 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     h.adj = g->adj;
     h.in_adj = g->in_adj;
     h.first_in = t.pull_first ? g->first_in : nullptr;
+    h.lazy_off = t.pull_first == 2;
     h.nonisolated = g->nonisolated;
     h.nonisolated_n = (const unsigned long long *)g->nonisolated_n;
     // chunk prefix room: rows above bin_medium_max edges, at most m / (max + 1)

@@ -137,9 +137,9 @@ struct gg_graph {
     gg_frontier *tmp_front[2] = {nullptr, nullptr};
     uint64_t *aux_cnt = nullptr;  // counters of steps that record no frontier
     HeavyRows heavy;              // chunked long rows of the CSC (pull / gather)
-    // first two in-neighbours of every vertex (CSC row order; 0xFFFFFFFF past
-    // the row's end): most dense-pull rows find their parent there
-    uint2 *first_in = nullptr;
+    // per vertex {first two in-neighbours (CSC row order; 0xFFFFFFFF past the
+    // row's end), in-degree, 0}: most dense-pull rows find their parent there
+    uint4 *first_in = nullptr;
     // gg_bfs_level_host_async: two level buffers used in turn, the stream
     // their host copies run on, and an event per buffer marking its copy done
     gg_prop *async_level[2] = {nullptr, nullptr};
@@ -261,7 +261,9 @@ struct Tuning {
     // min-id hooking for the rest of the run
     int cc_hook = 1;
     // dense pull: each row's first two in-neighbours read from a per-vertex
-    // pair array (coalesced with the row's offsets) before the row itself
+    // record (coalesced with the row's offsets) before the row itself;
+    // 2: the record's degree stands in for the offsets, which are loaded only
+    // for rows the first two edges do not settle; 0: rows only
     int pull_first = 1;
     unsigned long long barrier_timeout_ns = 5000000000ull;  // grid-barrier wait limit
 };

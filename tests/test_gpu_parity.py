@@ -395,3 +395,38 @@ def test_pagerank_staged_matches_restatement(ctx, stages):
     assert np.abs(x.astype(np.float64) - xo).sum() <= 1e-5
     x64, _, _ = O.pagerank(og, maxiter=100, tol=1e-10, f64=True)
     assert np.abs(x.astype(np.float64) - x64).sum() <= 1e-5  # the FP32 stage restores full accuracy
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("gen", ["rmat", "grid", "er_directed"])
+def test_pull_first_record_modes_exact(ctx, mode, gen):
+    """The dense pull's per-vertex record of first in-neighbours (knob
+    pull_first: 0 rows only, 1 record then rows, 2 record with the offsets
+    loaded only for rows it does not settle): BFS levels, parents and CC
+    labels identical to the oracle's in every mode, host- and graph-driven."""
+    if gen == "rmat":
+        og, sym = O.rmat(14, 16 << 14, seed=81), True
+    elif gen == "grid":
+        og, sym = O.grid(70, 90, seed=8, del_bp=300), True
+    else:
+        og, sym = O.er(6000, 10.0, seed=9, dangling_bp=100, symmetric=False), False
+    g = ctx.upload(og.off, og.adj, sym)
+    old = {k: gg.tuning_get(k) for k in ("pull_first", "graph")}
+    try:
+        gg.tuning_set("pull_first", mode)
+        deg = og.outdeg()
+        roots = [int(np.argmax(deg)), int(np.flatnonzero(deg)[len(np.flatnonzero(deg)) // 2])]
+        for graph_mode in (0, 1):
+            gg.tuning_set("graph", graph_mode)
+            for r in roots:
+                lv = O.bfs_level(og, r)
+                assert np.array_equal(g.bfs_level(r), lv), (mode, graph_mode, r)
+                for v in (gg.VAR_PULL_DENSE,):
+                    assert np.array_equal(g.bfs_level(r, opts=gg.default_opts(variant=v)), lv)
+                assert O.check_parents(og, r, g.bfs_parent(r), lv) == 0
+        if sym:
+            assert np.array_equal(g.cc(), O.cc(og))
+    finally:
+        for k, v in old.items():
+            gg.tuning_set(k, v)
+        g.close()
