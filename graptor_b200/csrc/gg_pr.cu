@@ -38,6 +38,7 @@
 #include <cstdio>
 #include <cstdlib>
 
+#include <algorithm>
 #include "gg_internal.cuh"
 
 namespace gg {
@@ -111,7 +112,29 @@ struct PrState {
     int stage, nstages, reencode;
     int stage_dt[4];
     double stage_tol[4];
+    // BF16 stochastic rounding; tail averaging from iteration avg_from on
+    int sr;
+    int avg_from, avg_n;
 };
+
+// MurmurHash3's fmix32 finaliser: 16 random bits per (vertex, iteration)
+__device__ __forceinline__ uint32_t sr_bits(uint32_t v, uint32_t it) {
+    uint32_t h = v * 0x9E3779B1u + it * 0x85EBCA77u + 0x165667B1u;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h & 0xFFFFu;
+}
+// bfloat16 of a non-negative float rounded up with probability (f - down) /
+// (up - down): the low 16 bits of the pattern plus 16 random bits carry into
+// bit 16 exactly that often (inf stays inf)
+__device__ __forceinline__ uint16_t bf16_stochastic(float f, uint32_t v, uint32_t it) {
+    const uint32_t u = __float_as_uint(f);
+    if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)(u >> 16);
+    return (uint16_t)((u + sr_bits(v, it)) >> 16);
+}
 
 // true when a kernel of stage `stage` (-1: unstaged) has nothing to do
 __device__ __forceinline__ bool pr_idle(const PrState *st, int stage) {
@@ -331,9 +354,12 @@ template <int DT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK)
 k_pr_update(const XT<DT> *__restrict__ y, XT<DT> *__restrict__ x, typename Store<DT>::T *contrib,
             const uint64_t *__restrict__ off, uint32_t n, float damp, double damp64, int renorm_f32, PrState *st,
-            int stage) {
+            int stage, float *acc = nullptr) {
     using S = Store<DT>;
     if (pr_idle(st, stage)) return;
+    const int it = st->iters;
+    const bool sr = DT == GG_BF16 && st->sr;
+    const bool accum = acc && it >= st->avg_from;
     const double s1 = st->s1;
     const double w = (1.0 - s1) / (double)n;
     const double s2 = s1 + (double)n * w;
@@ -363,7 +389,12 @@ k_pr_update(const XT<DT> *__restrict__ y, XT<DT> *__restrict__ x, typename Store
         x[v] = yv;
         const uint64_t deg = off[v + 1] - off[v];
         const float c = damp * yv / (float)deg;
-        contrib[v] = S::enc(scaled_format(DT) ? c * enc_scale : c);
+        if constexpr (DT == GG_BF16) {
+            contrib[v] = sr ? bf16_stochastic(c, v, (uint32_t)it) : S::enc(c);
+            if (accum) acc[v] += yv;
+        } else {
+            contrib[v] = S::enc(scaled_format(DT) ? c * enc_scale : c);
+        }
         if (deg && c > cm) cm = c;
     }
     dl = dev::block_sum<double, BLOCK>(dl);
@@ -384,6 +415,7 @@ __global__ void k_pr_finish(PrState *st, int dt) {
     st->reencode = 0;
     if (st->done) return;
     const int it = st->iters;
+    if (st->avg_from >= 0 && it >= st->avg_from) st->avg_n++;
     if (it < GG_MAX_ITERS) st->deltas[it] = st->delta;
     st->iters = it + 1;
     if (st->nstages > 1) dt = st->stage_dt[st->stage];
@@ -400,6 +432,14 @@ __global__ void k_pr_finish(PrState *st, int dt) {
     st->s1 = 0;
     st->delta = 0;
     st->cmax = 0.0f;
+}
+
+// Tail averaging: the ranks become the mean of the accumulated iterations.
+__global__ void k_pr_average(float *x, const float *acc, uint32_t n, const PrState *st) {
+    const int k = st->avg_n;
+    if (k <= 0) return;
+    const float inv = 1.0f / (float)k;
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) x[v] = acc[v] * inv;
 }
 
 // Scale of the contributions about to be encoded, from the max found by the
@@ -531,7 +571,7 @@ static double damping_f64(float d) {
 
 template <int DT>
 static gg_status pr_run(gg_graph *g, const gg_pr_params *p, XT<DT> *x, XT<DT> *y, void *contrib,
-                        PrState *st, void *partial) {
+                        PrState *st, void *partial, float *acc = nullptr) {
     gg_ctx *ctx = g->ctx;
     cudaStream_t s = ctx->stream;
     using T = typename Store<DT>::T;
@@ -552,10 +592,16 @@ static gg_status pr_run(gg_graph *g, const gg_pr_params *p, XT<DT> *x, XT<DT> *y
         else
             GG_CHECK((gather_launch<DT, false, false>(g, (const T *)contrib, yf, yd, st, 1.0f, partial)));
         k_pr_update<DT, kBlock><<<gv, kBlock, 0, s>>>(y, x, (T *)contrib, g->off, n, p->damping, d64,
-                                                      p->renorm_f32, st, -1);
+                                                      p->renorm_f32, st, -1, acc);
         GG_LAUNCHED(ctx);
         k_pr_finish<<<1, 1, 0, s>>>(st, DT);
         GG_LAUNCHED(ctx);
+    }
+    if constexpr (DT == GG_BF16) {
+        if (acc) {
+            k_pr_average<<<gv, kBlock, 0, s>>>(x, acc, n, st);
+            GG_LAUNCHED(ctx);
+        }
     }
     return GG_OK;
 }
@@ -688,6 +734,9 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
         for (int k = 0; k < p->nstages; ++k)
             if (!known(p->stage_dtype[k])) return set_error(ctx, GG_ERR_UNSUPPORTED, "stage contribution dtype");
     if (!staged && !known(dt) && dt != GG_F64) return set_error(ctx, GG_ERR_UNSUPPORTED, "contribution dtype");
+    if ((p->stochastic || p->average_last) && (staged || dt != GG_BF16))
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "stochastic rounding / tail averaging apply to BF16 runs only");
+    if (p->average_last < 0) return set_error(ctx, GG_ERR_ARG, "average_last must be >= 0");
     const gg_dtype xt = dt == GG_F64 ? GG_F64 : GG_F32;
     if (x && (x->g != g || x->t != xt))
         return set_error(ctx, GG_ERR_ARG, "x must be an F32 property of g (F64 for the FP64 variant)");
@@ -702,12 +751,14 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
     const size_t nb = (((size_t)g->n + 1) * esz + 255) / 256 * 256;
     const size_t sb = (sizeof(PrState) + 255) / 256 * 256;
     void *base = nullptr;
-    gg_status s = graph_scratch(g, 2 * nb + sb + (g->heavy.nchunks + 1) * 8, &base);
+    const size_t ab = p->average_last > 0 ? (((size_t)g->n + 1) * 4 + 255) / 256 * 256 : 0;
+    gg_status s = graph_scratch(g, 2 * nb + sb + ab + (g->heavy.nchunks + 1) * 8, &base);
     if (s != GG_OK) { if (tmpx) gg_prop_destroy(tmpx); return s; }
     float *y = (float *)base;
     void *contrib = (char *)base + nb;
     PrState *st = (PrState *)((char *)base + 2 * nb);
-    void *partial = (char *)base + 2 * nb + sb;
+    float *acc = ab ? (float *)((char *)base + 2 * nb + sb) : nullptr;
+    void *partial = (char *)base + 2 * nb + sb + ab;
     PrState init;
     memset(&init, 0, sizeof(init));
     init.maxiter = p->maxiter;
@@ -720,16 +771,19 @@ extern "C" gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x,
         init.stage_dt[k] = staged && k < p->nstages ? p->stage_dtype[k] : dt;
         init.stage_tol[k] = staged && k + 1 < p->nstages ? p->stage_tol[k] : p->tol;
     }
+    init.sr = p->stochastic ? 1 : 0;
+    init.avg_from = p->average_last > 0 ? std::max(0, p->maxiter - p->average_last) : -1;
     uint64_t k0 = ctx->launches;
     cudaEventRecord(ctx->ev0, ctx->stream);
     cudaError_t e = cudaMemcpyAsync(st, &init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess && acc) e = cudaMemsetAsync(acc, 0, (size_t)g->n * 4, ctx->stream);
     if (e == cudaSuccess) {
         if (staged) {
             s = pr_run_staged(g, p, (float *)xp->d, y, contrib, st, partial);
         } else switch (dt) {
         case GG_F64: s = pr_run<GG_F64>(g, p, (double *)xp->d, (double *)base, contrib, st, partial); break;
         case GG_F32: s = pr_run<GG_F32>(g, p, (float *)xp->d, y, contrib, st, partial); break;
-        case GG_BF16: s = pr_run<GG_BF16>(g, p, (float *)xp->d, y, contrib, st, partial); break;
+        case GG_BF16: s = pr_run<GG_BF16>(g, p, (float *)xp->d, y, contrib, st, partial, acc); break;
         case GG_F16: s = pr_run<GG_F16>(g, p, (float *)xp->d, y, contrib, st, partial); break;
         case GG_FP8E4M3: s = pr_run<GG_FP8E4M3>(g, p, (float *)xp->d, y, contrib, st, partial); break;
         case GG_CFP_6_10: s = pr_run<GG_CFP_6_10>(g, p, (float *)xp->d, y, contrib, st, partial); break;

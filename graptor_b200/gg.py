@@ -81,7 +81,7 @@ class PrParams(C.Structure):
     _fields_ = [("maxiter", C.c_int), ("tol", C.c_double), ("damping", C.c_float),
                 ("contrib_dtype", C.c_int), ("accum_f64", C.c_int), ("renorm_f32", C.c_int),
                 ("nstages", C.c_int), ("stage_dtype", C.c_int * 4), ("stage_accum_f64", C.c_int * 4),
-                ("stage_tol", C.c_double * 4)]
+                ("stage_tol", C.c_double * 4), ("stochastic", C.c_int), ("average_last", C.c_int)]
 
 
 EXPORTS = [
@@ -382,12 +382,15 @@ class Graph:
         return out
 
     def pagerank(self, maxiter=20, tol=1e-7, contrib=F32, accum_f64=True, renorm_f32=True,
-                 damping=0.85, x: "Prop" = None, host: bool = True, stats: RunStats = None, stages=None):
+                 damping=0.85, x: "Prop" = None, host: bool = True, stats: RunStats = None, stages=None,
+                 stochastic: bool = False, average_last: int = 0):
         """stages: [(dtype, accum_f64, tol), ...] for a staged run (the last tol is ignored;
         `tol` ends the last stage), e.g. PR_vary VARIANT 4620:
-        [(CFP_6_10, False, 1e-3), (F32, True, 0)]."""
+        [(CFP_6_10, False, 1e-3), (F32, True, 0)].  BF16 runs: stochastic rounding of the
+        stored contributions, and the mean of the last `average_last` iterations' ranks."""
         p = PrParams(maxiter=maxiter, tol=tol, damping=damping, contrib_dtype=contrib,
-                     accum_f64=int(accum_f64), renorm_f32=int(renorm_f32))
+                     accum_f64=int(accum_f64), renorm_f32=int(renorm_f32), stochastic=int(stochastic),
+                     average_last=int(average_last))
         if stages:
             p.nstages = len(stages)
             for k, (dt, acc, st_tol) in enumerate(stages):

@@ -390,6 +390,16 @@ typedef struct gg_pr_params {
     int stage_dtype[4];
     int stage_accum_f64[4];
     double stage_tol[4];
+    /* BF16 contributions only (no reference counterpart): stochastic = 1
+     * rounds each stored contribution up or down at random, with probability
+     * by its distance to the two neighbouring bfloat16 values (16 random bits
+     * per vertex and iteration from a counter hash, MurmurHash3's fmix32, so
+     * runs repeat exactly); average_last = K > 0 returns the mean of the
+     * ranks of iterations maxiter-K .. maxiter-1 (of those run).  Rounding
+     * to nearest leaves a bias that the iteration amplifies; unbiased
+     * rounding leaves noise that the average removes. */
+    int stochastic;
+    int average_last;
 } gg_pr_params;
 /* PageRank power iteration (PRv / PR_vary run_prec); x receives the ranks. */
 GG_API gg_status gg_pagerank(gg_graph *g, const gg_pr_params *p, gg_prop *x, float *host_x,

@@ -695,6 +695,84 @@ static int pr_vary_stage(uint32_t n, const uint64_t *in_off, const uint32_t *in_
     return 0;
 }
 
+/* BF16 PageRank with stochastic rounding and tail averaging (the GPU
+ * library's own extension, no reference counterpart): the GPU's update
+ * formula (y + (1 - s)/n, renormalised by the double 1/s), float sums,
+ * contributions rounded to bfloat16 up or down at random with 16 bits from
+ * MurmurHash3's fmix32 of (vertex, iteration) -- the same bits the device
+ * uses -- and, with average_last = K, the ranks returned as the mean of
+ * iterations maxiter-K .. maxiter-1.  The initial contributions are rounded
+ * to nearest. */
+static uint32_t sr_bits(uint32_t v, uint32_t it) {
+    uint32_t h = v * 0x9E3779B1u + it * 0x85EBCA77u + 0x165667B1u;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= 0xC2B2AE35u;
+    h ^= h >> 16;
+    return h & 0xFFFFu;
+}
+
+static float bf16_sr(float f, uint32_t v, uint32_t it) {
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7F800000u) != 0x7F800000u) u += sr_bits(v, it);
+    u &= 0xFFFF0000u;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+ORC_API int orc_pr_bf16_sr(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj, const uint32_t *outdeg,
+                           int stochastic, int maxiter, double tol, int average_last, float *x,
+                           double *deltas) {
+    const float damp = 0.85f;
+    float *c = (float *)malloc((size_t)(n ? n : 1) * sizeof(float));
+    float *y = (float *)malloc((size_t)(n ? n : 1) * sizeof(float));
+    float *acc = (float *)calloc(n ? n : 1, sizeof(float));
+    if (!c || !y || !acc) { free(c); free(y); free(acc); return -1; }
+    const float x0 = 1.0f / (float)n;
+    for (uint32_t v = 0; v < n; ++v) {
+        x[v] = x0;
+        c[v] = q_bf16_rne(damp * x0 / (float)outdeg[v]);
+    }
+    const int avg_from = average_last > 0 ? (maxiter - average_last > 0 ? maxiter - average_last : 0) : -1;
+    int it = 0, navg = 0;
+    double sdelta = 2;
+    while (it < maxiter && sdelta > tol) {
+        #pragma omp parallel for schedule(dynamic, 4096)
+        for (int64_t d = 0; d < (int64_t)n; ++d) {
+            float a = 0;
+            for (uint64_t e = in_off[d]; e < in_off[d + 1]; ++e) a += c[in_adj[e]];
+            y[d] = a;
+        }
+        double s1 = 0;
+        for (uint32_t v = 0; v < n; ++v) s1 += (double)y[v];
+        const double w = (1.0 - s1) / (double)n;
+        const double wf64 = 1.0 / (s1 + (double)n * w);
+        sdelta = 0;
+        for (uint32_t v = 0; v < n; ++v) {
+            float yv = (float)((double)y[v] + w);
+            yv = (float)((double)yv * wf64);
+            sdelta += (double)fabsf(x[v] - yv);
+            x[v] = yv;
+            const float cv = damp * yv / (float)outdeg[v];
+            c[v] = stochastic ? bf16_sr(cv, v, (uint32_t)it) : q_bf16_rne(cv);
+            if (avg_from >= 0 && it >= avg_from) acc[v] += yv;
+        }
+        if (avg_from >= 0 && it >= avg_from) ++navg;
+        if (deltas) deltas[it] = sdelta;
+        ++it;
+    }
+    if (navg > 0) {
+        const float inv = 1.0f / (float)navg;
+        for (uint32_t v = 0; v < n; ++v) x[v] = acc[v] * inv;
+    }
+    free(c);
+    free(y);
+    free(acc);
+    return it;
+}
+
 ORC_API int orc_pr_vary(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj,
                         const uint32_t *outdeg, int fmt, int accum_f64, int maxiter,
                         double tol, float *x_out, double *deltas) {

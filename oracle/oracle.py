@@ -62,6 +62,8 @@ def lib() -> C.CDLL:
         L.orc_cfp_from_float.restype = C.c_uint32
         L.orc_cfp_to_float.argtypes = [C.c_uint32, C.c_int, C.c_int, C.c_int]
         L.orc_cfp_to_float.restype = C.c_float
+        L.orc_pr_bf16_sr.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                     C.c_double, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_cfp_convert_bits.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int,
                                            C.c_void_p, C.c_void_p]
         L.orc_free.argtypes = [C.c_void_p]
@@ -207,6 +209,20 @@ def pagerank_vary(g: Graph, fmt: int, accum_f64: bool, maxiter: int = 100, tol: 
     deltas = np.zeros(max(maxiter, 1), dtype=np.float64)
     it = lib().orc_pr_vary(g.n, _p(csc.off), _p(csc.adj), _p(outdeg), fmt, int(accum_f64),
                            maxiter, tol, _p(x), _p(deltas))
+    return x, it, deltas[:it]
+
+
+def pagerank_bf16_sr(g: Graph, stochastic: bool = True, maxiter: int = 100, tol: float = 1e-7,
+                     average_last: int = 0, csc: Graph | None = None):
+    """BF16 PageRank with stochastic rounding of the contributions and the
+    mean of the last `average_last` iterations' ranks (the GPU library's
+    extension).  Returns (x, iterations, deltas)."""
+    csc = csc if csc is not None else g.transpose()
+    outdeg = g.outdeg()
+    x = np.empty(g.n, dtype=np.float32)
+    deltas = np.zeros(max(maxiter, 1), dtype=np.float64)
+    it = lib().orc_pr_bf16_sr(g.n, _p(csc.off), _p(csc.adj), _p(outdeg), int(stochastic), maxiter, tol,
+                              average_last, _p(x), _p(deltas))
     return x, it, deltas[:it]
 
 

@@ -430,3 +430,32 @@ def test_pull_first_record_modes_exact(ctx, mode, gen):
         for k, v in old.items():
             gg.tuning_set(k, v)
         g.close()
+
+
+@pytest.mark.parametrize("stochastic,avg", [(False, 0), (True, 0), (True, 50)])
+def test_bf16_stochastic_rounding_matches_restatement(ctx, stochastic, avg):
+    """BF16 PageRank with rounding to nearest, stochastic rounding (the same
+    hash-derived random bits as the restatement) and tail averaging: ranks
+    within summation-order distance of the restatement; stochastic rounding
+    averaged over the last 50 iterations within the 1e-4 L1 bar of the FP64
+    oracle."""
+    og = O.rmat(14, 16 << 14, seed=5)
+    g = upload(ctx, og)
+    st = gg.RunStats()
+    x = g.pagerank(maxiter=100, tol=1e-7, contrib=gg.BF16, accum_f64=False, renorm_f32=False,
+                   stochastic=stochastic, average_last=avg, stats=st)
+    xo, it, _ = O.pagerank_bf16_sr(og, stochastic=stochastic, maxiter=100, tol=1e-7, average_last=avg)
+    assert st.iterations == it
+    assert np.abs(x.astype(np.float64) - xo).sum() <= 2e-5
+    if stochastic and avg:
+        x64, _, _ = O.pagerank(og, maxiter=200, tol=1e-12, f64=True)
+        assert np.abs(x.astype(np.float64) - x64).sum() <= 1e-4
+
+
+def test_bf16_stochastic_options_rejected_elsewhere(ctx):
+    og = O.rmat(10, 8 << 10, seed=2)
+    g = upload(ctx, og)
+    with pytest.raises(gg.GGError):
+        g.pagerank(maxiter=5, contrib=gg.F32, stochastic=True)
+    with pytest.raises(gg.GGError):
+        g.pagerank(maxiter=5, contrib=gg.BF16, average_last=-1)
