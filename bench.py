@@ -784,13 +784,18 @@ def run_ours(args, ws, rank, local):
     value = total_half_edges / (t_ms_max / 1e3) / 1e9
     per_root = [st.edges_reached / 2.0 / (st.total_ms / 1e3) / 1e9 for st in stats]
 
-    # roofline of the dominant traversal kernel (by summed kernel time)
+    # roofline of the dominant traversal kernel (by summed kernel time): each
+    # step's traversal kernel span (first CTA start to last CTA end, stamped
+    # by the kernel) and, beside it, the whole step (launch gaps, list/bitmap
+    # conversions and the next step's decision included)
     ktime = {}
     kbytes = {}
+    stime = {}
     for st in stats:
         for it in range(st.iterations):
             v = st.variant[it]
-            ktime[v] = ktime.get(v, 0.0) + st.iter_ms[it]
+            ktime[v] = ktime.get(v, 0.0) + st.kernel_ms[it]
+            stime[v] = stime.get(v, 0.0) + st.iter_ms[it]
             kbytes[v] = kbytes.get(v, 0.0) + bfs_bytes(n, st, it)
     dom = max(ktime, key=ktime.get)
     nlaunch = sum(1 for st in stats for it in range(st.iterations) if st.variant[it] == dom)
@@ -807,6 +812,7 @@ def run_ours(args, ws, rank, local):
         nl = sum(1 for st in stats for it in range(st.iterations) if st.variant[it] == v)
         a = kbytes[v] / (t / 1e3) / 1e9
         kernel_roofline[kernel_names[v]] = {"launches": nl, "ms_per_launch": round(t / max(nl, 1), 4),
+                                            "step_ms_per_launch": round(stime[v] / max(nl, 1), 4),
                                             "bytes_per_launch": round(kbytes[v] / max(nl, 1)),
                                             "achieved_gbs": round(a, 1), "frac": round(a / hbm_peak, 4)}
 
@@ -818,6 +824,8 @@ def run_ours(args, ws, rank, local):
             "ms_per_root_mean": round(float(np.mean([st.total_ms for st in stats])), 4),
             "iterations_mean": round(float(np.mean([st.iterations for st in stats])), 2),
             "kernel_share": {kernel_names[v]: round(t / bfs_iter_total_ms, 3) for v, t in ktime.items()},
+            "kernel_ms_per_root": round(bfs_iter_total_ms / args.steps, 4),
+            "step_ms_per_root": round(sum(stime.values()) / args.steps, 4),
             "kernel_roofline": kernel_roofline,
             "whole_run_bytes_per_step": round(bfs_all_bytes / args.steps),
             "whole_run_frac_of_hbm": round(bfs_all_bytes / (t_ms / 1e3) / 1e9 / hbm_peak, 4),
@@ -952,7 +960,9 @@ def run_ours(args, ws, rank, local):
                          "traffic_source": "ncu dram__bytes_read+write of k_pull, scale-23 capture scaled by n",
                          "peak_kind": peak_kind, "launches": nlaunch,
                          "bytes_per_launch": round(kbytes[dom] / max(nlaunch, 1)),
-                         "ms_per_launch": round(ktime[dom] / max(nlaunch, 1), 4)},
+                         "ms_per_launch": round(ktime[dom] / max(nlaunch, 1), 4),
+                         "duration": "kernel span per launch (first CTA start to last CTA end, stamped by the "
+                                     "kernel inside the graph-driven run)"},
             "clocks": clocks, "gpu_launches": launches,
             "e2e": e2e, "cpu_baseline": cpu, "parity": parity,
         }
@@ -986,7 +996,8 @@ def case_roots(g, k: int, seed: int = 12345):
 def iter_table(st):
     from graptor_b200 import gg
     t = min(st.iterations, gg.MAX_ITERS)
-    return [[i, st.variant[i], int(st.nactv[i]), int(st.nacte[i]), round(st.iter_ms[i], 4)] for i in range(t)]
+    return [[i, st.variant[i], int(st.nactv[i]), int(st.nacte[i]), round(st.iter_ms[i], 4), round(st.kernel_ms[i], 4)]
+            for i in range(t)]
 
 
 def run_case(a):
@@ -1021,7 +1032,7 @@ def run_case(a):
                 st = gg.RunStats()
                 g.bfs_level(r, host=False, opts=opts, stats=st)
                 tot.append(st.total_ms)
-                ker.append(sum(st.iter_ms[i] for i in range(min(st.iterations, gg.MAX_ITERS))))
+                ker.append(sum(st.kernel_ms[i] for i in range(min(st.iterations, gg.MAX_ITERS))))
                 last = st
                 if worst is None or st.total_ms > worst[1]:
                     worst = (r, st.total_ms, iter_table(st))

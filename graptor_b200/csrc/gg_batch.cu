@@ -473,6 +473,7 @@ gg_status gg_msbfs(gg_graph *g, const uint32_t *roots, int k, int32_t *host_leve
         for (int i = 0; i < std::min(hs.iterations, GG_MAX_ITERS); ++i) {
             stats->variant[i] = hs.variant[i];
             stats->iter_ms[i] = (hs.t_ns[i + 1] - hs.t_ns[i]) * 1e-6;
+            stats->kernel_ms[i] = stats->iter_ms[i];
         }
     }
     if (host_levels) {

@@ -1190,6 +1190,7 @@ static void record_iter(gg_run_stats *st, int it, const gg_emap_stats &es) {
     st->nacte[it] = es.nacte_in;
     st->scanned[it] = es.scanned;
     st->iter_ms[it] = es.kernel_ms;
+    st->kernel_ms[it] = es.kernel_ms;
     st->scanned_edges += es.scanned;
 }
 
@@ -1316,6 +1317,8 @@ struct GCtl {
     int variants[GG_MAX_ITERS];
     unsigned long long nactv[GG_MAX_ITERS], nacte[GG_MAX_ITERS], scanned[GG_MAX_ITERS];
     unsigned long long t_ns[GG_MAX_ITERS + 1];
+    // span of each step's traversal kernel (first CTA start, last CTA end)
+    unsigned long long kt0[GG_MAX_ITERS], kt1[GG_MAX_ITERS];
     cudaGraphConditionalHandle h_while, h_push, h_pull, h_list, h_bits, h_chunks;
 };
 
@@ -1338,6 +1341,10 @@ __device__ void decide_step(GCtl *c);
 
 __global__ void k_g_init(GCtl *c) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = tid; i < GG_MAX_ITERS; i += nth) {
+        c->kt0[i] = ~0ull;
+        c->kt1[i] = 0ull;
+    }
     const int32_t inf = (int32_t)c->n + 1;
     // (prev is not used by level-synchronous steps: only level is filled)
     for (uint64_t v = tid; v < c->n; v += nth) c->level[v] = v == c->root ? 0 : inf;
@@ -1529,18 +1536,35 @@ __global__ void __launch_bounds__(256) k_g_tolist(GCtl *c) {
 __device__ __noinline__ void g_push_setup(GCtl *c, uint32_t cap, EmapArgs *sA, Op<GG_RELAX_MIN_PLUS1_I32> *sOp,
                                           uint32_t *s_nl, uint32_t *s_nm);
 
+// Span of a step's traversal kernel: the first CTA to start and the last to
+// finish (the last warp of each CTA records its end) stamp the step's record.
+__device__ __forceinline__ void kspan_start(GCtl *c, int it) {
+    if (it < GG_MAX_ITERS) atomicMin(&c->kt0[it], g_now());
+}
+__device__ __forceinline__ void kspan_end(GCtl *c, int it, unsigned *s_done) {
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0 && atomicAdd(s_done, 1u) == blockDim.x / 32 - 1 && it < GG_MAX_ITERS)
+        atomicMax(&c->kt1[it], g_now());
+}
+
 __global__ void __launch_bounds__(kBlock, 6) k_g_push(GCtl *c) {
     if (c->variant != GG_VAR_PUSH_SPARSE) return;
     __shared__ EmapArgs sA;
     __shared__ Op<GG_RELAX_MIN_PLUS1_I32> sOp;
     __shared__ uint32_t s_nl, s_nm;
+    __shared__ int s_it;
+    __shared__ unsigned s_done;
     if (threadIdx.x == 0) {
+        s_it = c->iter;
+        s_done = 0;
+        kspan_start(c, s_it);
         g_push_setup(c, gridDim.x, &sA, &sOp, &s_nl, &s_nm);
         // the pushed frontier's bitmap, if a pull made it, is cleared after
         if (blockIdx.x == 0) c->clr = c->has_bitmap[c->cur] ? c->cur + 1 : 0;
     }
     __syncthreads();
     push_binned_body<GG_RELAX_MIN_PLUS1_I32, kBlock>(sA, sOp, s_nl, s_nm);
+    kspan_end(c, s_it, &s_done);
 }
 
 // one thread per CTA: the push arguments and the partition of the grid
@@ -1599,13 +1623,19 @@ __global__ void __launch_bounds__(kBlock, 6) k_g_pull(GCtl *c) {
     if (c->variant != GG_VAR_PULL_DENSE) return;
     __shared__ EmapArgs sA;
     __shared__ Op<GG_RELAX_MIN_PLUS1_I32> sOp;
+    __shared__ int s_it;
+    __shared__ unsigned s_done;
     if (threadIdx.x == 0) {
+        s_it = c->iter;
+        s_done = 0;
+        kspan_start(c, s_it);
         sA = c->A;
         sOp = c->op;
         if (blockIdx.x == 0) c->clr = c->cur + 1;  // a pulled frontier has a bitmap to clear after
     }
     __syncthreads();
     pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock>(sA, sOp);
+    kspan_end(c, s_it, &s_done);
 }
 
 __device__ void g_bookkeep(GCtl *c);
@@ -1946,6 +1976,8 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
             st->scanned[i] = hr->scanned[i];
             st->scanned_edges += hr->scanned[i];
             st->iter_ms[i] = i + 1 <= GG_MAX_ITERS ? (double)(hr->t_ns[i + 1] - hr->t_ns[i]) * 1e-6 : 0.0;
+            st->kernel_ms[i] = hr->kt1[i] > hr->kt0[i] && hr->kt0[i] != ~0ull
+                                   ? (double)(hr->kt1[i] - hr->kt0[i]) * 1e-6 : st->iter_ms[i];
         }
     }
     std::free(hr);

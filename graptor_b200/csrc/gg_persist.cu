@@ -1713,6 +1713,7 @@ static void persistent_collect(gg_graph *g, const PArgs &P, const PState &hs, gg
             stats->nacte[i] = hs.nacte[i];
             stats->scanned[i] = hs.scanned[i];
             stats->iter_ms[i] = (double)(hs.t_ns[i + 1] - hs.t_ns[i]) * 1e-6;
+            stats->kernel_ms[i] = stats->iter_ms[i];
             stats->scanned_edges += hs.scanned[i];
         }
     }

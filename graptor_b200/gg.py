@@ -69,7 +69,7 @@ class RunStats(C.Structure):
                 ("edges_reached", C.c_uint64), ("variant", C.c_int * MAX_ITERS),
                 ("nactv", C.c_uint64 * MAX_ITERS), ("nacte", C.c_uint64 * MAX_ITERS),
                 ("scanned", C.c_uint64 * MAX_ITERS), ("delta", C.c_double * MAX_ITERS),
-                ("iter_ms", C.c_double * MAX_ITERS)]
+                ("iter_ms", C.c_double * MAX_ITERS), ("kernel_ms", C.c_double * MAX_ITERS)]
 
 
 class RunOpts(C.Structure):

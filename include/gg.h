@@ -330,7 +330,10 @@ typedef struct gg_run_stats {
     uint64_t nacte[GG_MAX_ITERS];
     uint64_t scanned[GG_MAX_ITERS];
     double delta[GG_MAX_ITERS];       /* PageRank L1 residual per iteration */
-    double iter_ms[GG_MAX_ITERS];     /* traversal-kernel device time (collect_stats) */
+    double iter_ms[GG_MAX_ITERS];     /* the iteration's device time (collect_stats; graph- and device-driven
+                                         runs: from its start to the next one's, launch gaps included) */
+    double kernel_ms[GG_MAX_ITERS];   /* its traversal kernel's own span (first CTA start to last CTA end;
+                                         = iter_ms where the step is not a separate kernel) */
 } gg_run_stats;
 
 typedef struct gg_run_opts {
