@@ -400,7 +400,9 @@ def deviation_oracle(g, analytic, root, thr_variant, t_thr, max_iters=64):
     gains = []
     for x, y in zip(X, Y):
         it = int(round(2.0 ** (8.0 * float(x[3])) - 1.0))  # the iteration feature, log2(1 + it) / 8
-        if it >= T or not np.all(np.isfinite(y)):
+        # (an iteration the threshold run took as CC's hooking step has no
+        # traversal variant to deviate from)
+        if it >= T or not np.all(np.isfinite(y)) or not 0 <= thr_variant[it] < len(y):
             continue
         t = 2.0 ** y.astype(np.float64) / 1e3  # ms
         gains.append(max(0.0, t[thr_variant[it]] - t.min()))
