@@ -687,16 +687,21 @@ def batch_eval(ctx, g, roots, hbm_peak, n_small):
     knob_names = ["bin_small_max", "bin_medium_max", "pull_k", "push_k", "large_chunk", "blocks_per_sm",
                   "heavy_deg", "heavy_chunk", "persistent", "cc_hook"]
     defaults = {k: gg.tuning_get(k) for k in knob_names}
-    tparts = small_graph_batch(ctx, 200, seed=7000)
-    TU, tbase = gg.graph_union(ctx, tparts)
-    for p in tparts:
-        p.close()
-    ta = time.time()
-    tuned = AT.tune_graph(TU, gg.TUNE_BFS | gg.TUNE_CC, nroots=4, passes=1, reps=2)
-    tune_s = time.time() - ta
-    TU.close()
-    gg.graph_retune(U)  # heavy-row tables with the tuned cut
-    t_tun = batch_runs()
+    try:
+        tparts = small_graph_batch(ctx, 200, seed=7000)
+        TU, tbase = gg.graph_union(ctx, tparts)
+        for p in tparts:
+            p.close()
+        ta = time.time()
+        tuned = AT.tune_graph(TU, gg.TUNE_BFS | gg.TUNE_CC, nroots=4, passes=1, reps=2)
+        tune_s = time.time() - ta
+        TU.close()
+        gg.graph_retune(U)  # heavy-row tables with the tuned cut
+        t_tun = batch_runs()
+    except Exception:
+        AT.apply(defaults)  # later measurements run with the default knobs
+        gg.graph_retune(U)
+        raise
     use_tuned = t_tun[0] <= t_def[0]
     if not use_tuned:
         AT.apply(defaults)
