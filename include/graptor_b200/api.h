@@ -561,7 +561,14 @@ inline E make_unop_abs(const E &a) {
     n->dt = a.node()->dt;
     return E(n);
 }
-inline E iif(const E &c, const E &a, const E &b) { return E(mk(NK::Iif, {c.node(), a.node(), b.node()})); }
+// iif(c, l, r) selects r where c holds and l elsewhere, as the reference's
+// blend (dsl/ast/ternop.h:65-125 -> blendm(m, l, r) = m ? r : l,
+// target/scalar_int.h:212-214); the node keeps (c, taken, not taken)
+inline E iif(const E &c, const E &l, const E &r) {
+    auto n = mk(NK::Iif, {c.node(), r.node(), l.node()});
+    n->dt = promote(l.node()->dt, r.node()->dt);
+    return E(n);
+}
 inline E msbset(const E &a) { return E(mk(NK::MsbSet, {a.node()})); }
 inline E make_noop() { return E(mk(NK::Noop)); }
 

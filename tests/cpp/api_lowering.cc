@@ -1,0 +1,90 @@
+// Lowering of the operator surface (include/graptor_b200/api.h) checked on
+// the host: the analytics' relax / filter / record expressions become the
+// descriptor kinds of gg.h, vertex statements the expected stack programs.
+// Built and run by tests/test_api_lowering.py; prints "ok" and returns 0.
+#include <cstdio>
+#include <cstdlib>
+
+#include "graptor_b200/api.h"
+
+using namespace expr;
+
+static int fails = 0;
+#define CHECK(c)                                                   \
+    do {                                                           \
+        if (!(c)) {                                                \
+            std::printf("FAIL %s:%d %s\n", __FILE__, __LINE__, #c); \
+            ++fails;                                               \
+        }                                                          \
+    } while (0)
+
+static gg_prop *P(int i) { return reinterpret_cast<gg_prop *>(0x1000 * i); }
+static E at(int p, gg_dtype dt, NK who) { return ref(P(p), nullptr, dt, var(who)); }
+
+static gg_emap_desc relax_of(const E &e) {
+    gg_emap_desc d;
+    std::memset(&d, 0, sizeof(d));
+    graptor_b200::lower_relax(e.node(), d);
+    return d;
+}
+
+int main() {
+    const NK S = NK::VarSrc, D = NK::VarDst, V = NK::VarV;
+    // BFSLVLv.C:209-215, CCv.C:575-581, BFSv.C:144-146, PRv.C:202-212
+    CHECK(relax_of(at(1, GG_I32, D).min(at(1, GG_I32, S) + _1)).relax == GG_RELAX_MIN_PLUS1_I32);
+    CHECK(relax_of(at(2, GG_U32, D).min(at(2, GG_U32, S))).relax == GG_RELAX_MIN_U32);
+    CHECK(relax_of(at(3, GG_U32, D).setif(var(S))).relax == GG_RELAX_SETIF_U32);
+    {
+        gg_emap_desc d = relax_of(at(4, GG_F64, D) += cast<double>(at(5, GG_F32, S)));
+        CHECK(d.relax == GG_RELAX_ADD_GATHER && d.a == P(4) && d.src == P(5) && d.accum_f64 == 1);
+        d = relax_of(at(4, GG_F32, D) += cast<float>(at(5, GG_F32, S)));
+        CHECK(d.relax == GG_RELAX_ADD_GATHER && d.accum_f64 == 0);
+    }
+    // validation edgemaps: CCv.C:612-617, BFSLVLv.C:288-305
+    CHECK(relax_of(at(2, GG_U32, D) != at(2, GG_U32, S)).relax == GG_RELAX_NE_CHECK);
+    CHECK(relax_of(at(1, GG_I32, S) > at(1, GG_I32, D) + _1 || at(1, GG_I32, S) < at(1, GG_I32, D) - _1).relax ==
+          GG_RELAX_GAP_CHECK);
+    CHECK(relax_of(at(1, GG_I32, S) < at(1, GG_I32, D) - _1).relax == GG_RELAX_AHEAD_CHECK);
+    // a relax outside the table names itself
+    bool threw = false;
+    try {
+        relax_of(at(1, GG_I32, D) += at(1, GG_I32, S) * at(1, GG_I32, S));
+    } catch (const graptor_b200::error &e) {
+        threw = e.status == GG_ERR_UNSUPPORTED;
+    }
+    CHECK(threw);
+    // dst filters and the record method
+    {
+        gg_emap_desc d;
+        std::memset(&d, 0, sizeof(d));
+        graptor_b200::lower_dst_filter((at(1, GG_I32, D) > _c(7)).node(), d);
+        CHECK(d.dst_filter == GG_FILTER_GT_CONST && d.dst_filter_k == 7);
+        graptor_b200::lower_dst_filter((at(2, GG_U32, D) != zero_val(var(D))).node(), d);
+        CHECK(d.dst_filter == GG_FILTER_NE_ZERO);
+        graptor_b200::lower_record_method((at(2, GG_U32, D) != at(6, GG_U32, D)).node(), d);
+        CHECK(d.record == GG_RECORD_NE_PREV && d.prev == P(6));
+    }
+    // iif(c, l, r) takes r where c holds (the reference's blend order): the
+    // program pushes c, then r, then l, then selects
+    {
+        graptor_b200::VmBuilder b;
+        E st = (at(7, GG_F64, V) = iif(at(8, GG_F64, V) > _c(0.5), _c(1.0), _c(2.0)));
+        CHECK(b.statement(st.node()));
+        // LOAD 8, CONST 0.5, GT, CONST 2.0, CONST 1.0, SELECT, STORE 7
+        CHECK(b.d.ncode == 7 && b.d.code[5] == GG_VM_SELECT && b.d.code[6] == GG_VM_STORE);
+        CHECK(b.d.consts[b.d.arg[3]] == 2.0 && b.d.consts[b.d.arg[4]] == 1.0);
+    }
+    // float arithmetic rounds to float; constant_val takes the operand's type
+    {
+        graptor_b200::VmBuilder b;
+        E y = at(9, GG_F32, V);
+        CHECK(b.statement((y = constant_val(y, 0.85) * y).node()));
+        int tof32 = 0;
+        for (int i = 0; i < b.d.ncode; ++i) tof32 += b.d.code[i] == GG_VM_TOF32;
+        CHECK(tof32 >= 2);  // the load of y and the float product
+        CHECK(b.d.consts[0] == (double)0.85f);
+    }
+    if (fails) return 1;
+    std::printf("ok\n");
+    return 0;
+}
