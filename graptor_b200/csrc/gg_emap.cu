@@ -84,6 +84,7 @@ struct Op {
     using V = typename std::conditional<R == GG_RELAX_MIN_PLUS1_I32, int32_t, uint32_t>::type;
     V *a;
     V *prev;
+    const V *b;      // OR_U32: the source property (a[d] |= b[s])
     int filter;
     int64_t fk;
     int level_sync;  // MIN_PLUS1: active sources hold fk-1, offer fk without a load
@@ -98,6 +99,7 @@ struct Op {
         case GG_FILTER_GT_CONST: return (int64_t)cur > fk;
         case GG_FILTER_NE_ZERO: return cur != 0;
         case GG_FILTER_MSB_SET: return ((uint32_t)cur >> 31) != 0;
+        case GG_FILTER_NE_CONST: return (uint32_t)cur != (uint32_t)fk;
         default: return true;
         }
     }
@@ -105,16 +107,25 @@ struct Op {
     __device__ __forceinline__ V src_val(uint32_t s) const {
         if constexpr (R == GG_RELAX_MIN_PLUS1_I32) return level_sync ? (V)fk : a[s] + 1;
         else if constexpr (R == GG_RELAX_MIN_U32) return a[s];
+        else if constexpr (R == GG_RELAX_OR_U32) return b[s];
         else return (V)s;
     }
     __device__ __forceinline__ bool better(V x, V best) const {
         if constexpr (R == GG_RELAX_SETIF_U32) return ((uint32_t)best >> 31) != 0;
+        else if constexpr (R == GG_RELAX_OR_U32) return (best | x) != best;
         else return x < best;
     }
-    // among the lanes with ok set (mask okm) pick the winner's value
-    __device__ __forceinline__ V warp_pick(bool ok, V x, unsigned okm) const {
+    // the value after a better offer x
+    __device__ __forceinline__ V combine(V best, V x) const {
+        if constexpr (R == GG_RELAX_OR_U32) return best | x;
+        else return x;
+    }
+    // the row's value after the lanes with ok set (mask okm) offered theirs
+    __device__ __forceinline__ V warp_merge(V best, bool ok, V x, unsigned okm) const {
         if constexpr (R == GG_RELAX_SETIF_U32) {
             return __shfl_sync(FULL, x, __ffs(okm) - 1);
+        } else if constexpr (R == GG_RELAX_OR_U32) {
+            return best | __reduce_or_sync(FULL, ok ? x : 0u);
         } else {
             V mine = ok ? x : none();
             return __reduce_min_sync(FULL, mine);
@@ -129,6 +140,10 @@ struct Op {
             if (((uint32_t)cur >> 31) == 0) return false;
             old = atomicCAS(a + d, cur, sv);
             if (old != cur) return false;
+        } else if constexpr (R == GG_RELAX_OR_U32) {
+            if ((cur | sv) == cur) return false;
+            old = atomicOr(a + d, sv);
+            if ((old | sv) == old) return false;
         } else {
             if (!(sv < cur)) return false;
             old = atomicMin(a + d, sv);
@@ -241,7 +256,7 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
                 if (j < cnt && act && (!SRCF || dev::bit_test(A.in_bits, sv[j]))) {
                     const V x = op.src_val(sv[j]);
                     if (op.better(x, best)) {
-                        best = x;
+                        best = op.combine(best, x);
                         changed = true;
                         if (!op.dst_ok(best)) {
                             act = false;
@@ -278,7 +293,7 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (j < cnt && act && inF[j] && op.better(xv[j], best)) {
-                    best = xv[j];
+                    best = op.combine(best, xv[j]);
                     changed = true;
                     if (!op.dst_ok(best)) {
                         act = false;
@@ -311,7 +326,7 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
                 if (lane == 0) sc += min((uint64_t)32, endj - base);
                 const unsigned okm = __ballot_sync(FULL, ok);
                 if (okm) {
-                    bj = op.warp_pick(ok, x, okm);
+                    bj = op.warp_merge(bj, ok, x, okm);
                     chj = true;
                     if (!op.dst_ok(bj)) {
                         actj = false;
@@ -333,6 +348,9 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
                 // value replaced; prev is neither read nor written
                 if (R == GG_RELAX_MIN_PLUS1_I32 && op.level_sync) {
                     rec = true;
+                } else if constexpr (R == GG_RELAX_OR_U32) {
+                    // prev may be the relax's source: the copy runs after the step
+                    rec = best != op.prev[d];
                 } else if (best != op.prev[d]) {
                     op.prev[d] = best;
                     rec = true;
@@ -746,6 +764,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     Op<R> op;
     op.a = (typename Op<R>::V *)d->a->d;
     op.prev = d->prev ? (typename Op<R>::V *)d->prev->d : nullptr;
+    op.b = (R == GG_RELAX_OR_U32 && d->src) ? (const typename Op<R>::V *)d->src->d : nullptr;
     op.filter = d->dst_filter;
     op.fk = d->dst_filter_k;
     op.level_sync = (d->src_level_sync && d->dst_filter == GG_FILTER_GT_CONST) ? 1 : 0;
@@ -941,7 +960,9 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
         // level-synchronous BFS: a push's unique first writer records d and no
         // later step compares prev of a visited vertex, so no copy is needed
         const bool sync_levels = d->src_level_sync && d->relax == GG_RELAX_MIN_PLUS1_I32;
-        if (d->record == GG_RECORD_NE_PREV && variant != GG_VAR_PULL_DENSE && !sync_levels) {
+        // (an OR pull leaves the copy to here: its prev may be its source)
+        if (d->record == GG_RECORD_NE_PREV && (variant != GG_VAR_PULL_DENSE || R == GG_RELAX_OR_U32) &&
+            !sync_levels) {
             if (!d->prev) return set_error(ctx, GG_ERR_ARG, "NE_PREV record needs prev");
             k_copy_prev<<<persistent_grid(ctx, words), kBlock, 0, st>>>(
                 out->bins[0], out->bins[1], out->bins[2], out->d_cnt, op.a, op.prev);
@@ -1078,11 +1099,14 @@ gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_f
         return GG_OK;
     }
     const gg_dtype want = d->relax == GG_RELAX_MIN_PLUS1_I32 ? GG_I32 : GG_U32;
-    if (d->relax < 0 || d->relax > GG_RELAX_SETIF_U32) return set_error(ctx, GG_ERR_ARG, "unknown relax kind");
+    if (d->relax < 0 || (d->relax > GG_RELAX_SETIF_U32 && d->relax != GG_RELAX_OR_U32))
+        return set_error(ctx, GG_ERR_ARG, "unknown relax kind");
+    if (d->relax == GG_RELAX_OR_U32 && (!d->src || d->src->g != g || d->src->t != GG_U32))
+        return set_error(ctx, GG_ERR_ARG, "OR_U32 needs a uint32 source property of g");
     if (d->a->t != want) return set_error(ctx, GG_ERR_ARG, "relaxed property has the wrong dtype");
     if (d->prev && (d->prev->t != want || d->prev->g != g)) return set_error(ctx, GG_ERR_ARG, "prev property mismatch");
     if (d->record == GG_RECORD_NE_PREV && !d->prev) return set_error(ctx, GG_ERR_ARG, "NE_PREV record needs prev");
-    if (d->dst_filter < GG_FILTER_NONE || d->dst_filter > GG_FILTER_MSB_SET) return set_error(ctx, GG_ERR_ARG, "unknown dst filter");
+    if (d->dst_filter < GG_FILTER_NONE || d->dst_filter > GG_FILTER_NE_CONST) return set_error(ctx, GG_ERR_ARG, "unknown dst filter");
     if (d->dst_filter != GG_FILTER_NONE && d->dst_filter_prop && d->dst_filter_prop != d->a)
         return set_error(ctx, GG_ERR_UNSUPPORTED, "dst filter on a property other than the relaxed one");
     if (d->threshold == GG_THRESH_FRAC && d->threshold_k <= 0) return set_error(ctx, GG_ERR_ARG, "frac threshold needs k > 0");
@@ -1123,6 +1147,7 @@ gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_f
     switch (d->relax) {
     case GG_RELAX_MIN_PLUS1_I32: s = launch_variant<GG_RELAX_MIN_PLUS1_I32>(g, d, in, out, variant); break;
     case GG_RELAX_MIN_U32: s = launch_variant<GG_RELAX_MIN_U32>(g, d, in, out, variant); break;
+    case GG_RELAX_OR_U32: s = launch_variant<GG_RELAX_OR_U32>(g, d, in, out, variant); break;
     default: s = launch_variant<GG_RELAX_SETIF_U32>(g, d, in, out, variant); break;
     }
     if (stats && s == GG_OK) cudaEventRecord(ctx->evk1, ctx->stream);

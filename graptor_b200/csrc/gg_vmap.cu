@@ -80,6 +80,7 @@ __global__ void __launch_bounds__(kBlock) k_vmap(VmArgs A) {
     const uint32_t nw = (gridDim.x * kBlock) >> 5;
     double red[GG_VM_MAX_REDUCE] = {0, 0, 0, 0};
     unsigned long long nv = 0, ne = 0;
+    auto u32 = [](double x) { return (uint32_t)(int64_t)x; };
     for (uint32_t w = (blockIdx.x * kBlock + threadIdx.x) >> 5; w < nwords; w += nw) {
         const uint32_t v = (w << 5) + lane;
         bool act = v < A.n;
@@ -87,6 +88,7 @@ __global__ void __launch_bounds__(kBlock) k_vmap(VmArgs A) {
         bool sel = false;
         if (act) {
             double st[kVmStack];
+            double tmp[GG_VM_MAX_TMP];
             int sp = 0;
             for (int pc = 0; pc < A.ncode; ++pc) {
                 const int a = A.arg[pc];
@@ -112,6 +114,15 @@ __global__ void __launch_bounds__(kBlock) k_vmap(VmArgs A) {
                 case GG_VM_SELECT: sp -= 2; st[sp - 1] = st[sp - 1] != 0.0 ? st[sp] : st[sp + 1]; break;
                 case GG_VM_FILTER: sel = st[--sp] != 0.0; break;
                 case GG_VM_DUP: st[sp] = st[sp - 1]; ++sp; break;
+                case GG_VM_AND: --sp; st[sp - 1] = (double)(u32(st[sp - 1]) & u32(st[sp])); break;
+                case GG_VM_OR: --sp; st[sp - 1] = (double)(u32(st[sp - 1]) | u32(st[sp])); break;
+                case GG_VM_XOR: --sp; st[sp - 1] = (double)(u32(st[sp - 1]) ^ u32(st[sp])); break;
+                case GG_VM_NOT: st[sp - 1] = (double)(~u32(st[sp - 1])); break;
+                case GG_VM_TOU32: st[sp - 1] = (double)u32(st[sp - 1]); break;
+                case GG_VM_TSET: tmp[a & (GG_VM_MAX_TMP - 1)] = st[--sp]; break;
+                case GG_VM_TGET: st[sp++] = tmp[a & (GG_VM_MAX_TMP - 1)]; break;
+                case GG_VM_LE: --sp; st[sp - 1] = st[sp - 1] <= st[sp] ? 1.0 : 0.0; break;
+                case GG_VM_GE: --sp; st[sp - 1] = st[sp - 1] >= st[sp] ? 1.0 : 0.0; break;
                 default: break;
                 }
             }
@@ -172,8 +183,11 @@ static bool vm_validate(const gg_vmap_desc *d, gg_graph *g, std::string &why) {
         case GG_VM_VID: case GG_VM_DEGREE: push = 1; break;
         case GG_VM_ADD: case GG_VM_SUB: case GG_VM_MUL: case GG_VM_DIV: case GG_VM_MIN:
         case GG_VM_MAX: case GG_VM_EQ: case GG_VM_NE: case GG_VM_LT: case GG_VM_GT:
+        case GG_VM_AND: case GG_VM_OR: case GG_VM_XOR: case GG_VM_LE: case GG_VM_GE:
             pop = 2; push = 1; break;
-        case GG_VM_ABS: case GG_VM_TOF32: pop = 1; push = 1; break;
+        case GG_VM_ABS: case GG_VM_TOF32: case GG_VM_NOT: case GG_VM_TOU32: pop = 1; push = 1; break;
+        case GG_VM_TSET: if (a >= GG_VM_MAX_TMP) { why = "bad temporary"; return false; } pop = 1; break;
+        case GG_VM_TGET: if (a >= GG_VM_MAX_TMP) { why = "bad temporary"; return false; } push = 1; break;
         case GG_VM_REDUCE_ADD: if (a >= d->nreduce) { why = "reduction index"; return false; } pop = 1; break;
         case GG_VM_SELECT: pop = 3; push = 1; break;
         case GG_VM_FILTER: pop = 1; break;

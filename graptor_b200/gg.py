@@ -20,8 +20,9 @@ LIB_PATH = os.path.join(PKG, "libgg.so")
 GG_OK, GG_ERR_ARG, GG_ERR_OOM, GG_ERR_CUDA, GG_ERR_TIMEOUT, GG_ERR_UNSUPPORTED, GG_ERR_IO, \
     GG_ERR_STATE, GG_ERR_NOT_FOUND = range(9)
 I32, U32, F32, F64, BF16, F16, FP8E4M3, CFP_6_10, BF16_TRUNC, U8 = range(10)
-RELAX_MIN_PLUS1_I32, RELAX_MIN_U32, RELAX_SETIF_U32, RELAX_ADD_GATHER = range(4)
-FILTER_NONE, FILTER_GT_CONST, FILTER_NE_ZERO, FILTER_MSB_SET = range(4)
+(RELAX_MIN_PLUS1_I32, RELAX_MIN_U32, RELAX_SETIF_U32, RELAX_ADD_GATHER, RELAX_NE_CHECK, RELAX_GAP_CHECK,
+ RELAX_AHEAD_CHECK, RELAX_OR_U32) = range(8)
+FILTER_NONE, FILTER_GT_CONST, FILTER_NE_ZERO, FILTER_MSB_SET, FILTER_NE_CONST = range(5)
 RECORD_NONE, RECORD_REDUCTION, RECORD_NE_PREV = range(3)
 THRESH_DEFAULT, THRESH_FRAC, THRESH_ALWAYS_SPARSE, THRESH_ALWAYS_DENSE, THRESH_LEARNED = range(5)
 VAR_AUTO, VAR_PUSH_SPARSE, VAR_PUSH_MERGE, VAR_PULL_DENSE, VAR_PUSH_DENSE, VAR_HOOK = -1, 0, 1, 2, 3, 4
@@ -29,7 +30,7 @@ VARIANT_NAMES = {0: "push_sparse", 1: "push_merge", 2: "pull_dense", 3: "push_de
 GEN_RMAT, GEN_ER, GEN_GRID = range(3)
 (VM_END, VM_LOAD, VM_STORE, VM_CONST, VM_VID, VM_DEGREE, VM_ADD, VM_SUB, VM_MUL, VM_DIV, VM_ABS,
  VM_MIN, VM_MAX, VM_EQ, VM_NE, VM_LT, VM_GT, VM_REDUCE_ADD, VM_TOF32, VM_SELECT, VM_FILTER,
- VM_DUP) = range(22)
+ VM_DUP, VM_AND, VM_OR, VM_XOR, VM_NOT, VM_TOU32, VM_TSET, VM_TGET, VM_LE, VM_GE) = range(31)
 MAX_ITERS = 256
 
 NP_DTYPE = {I32: np.int32, U32: np.uint32, F32: np.float32, F64: np.float64, BF16: np.uint16,

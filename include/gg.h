@@ -186,7 +186,9 @@ typedef enum gg_relax_kind {
     GG_RELAX_NE_CHECK = 4,      /* a[d] != a[s] on uint32            (CCv.C:612-617)     */
     GG_RELAX_GAP_CHECK = 5,     /* a[s] > a[d] + 1 || a[s] < a[d] - 1 on int32
                                                                       (BFSLVLv.C:288-294) */
-    GG_RELAX_AHEAD_CHECK = 6    /* a[s] < a[d] - 1 on int32          (BFSLVLv.C:299-305) */
+    GG_RELAX_AHEAD_CHECK = 6,   /* a[s] < a[d] - 1 on int32          (BFSLVLv.C:299-305) */
+    GG_RELAX_OR_U32 = 7         /* a[d] |= src[s] on uint32 (another property as source;
+                                   FMv.C:356-358, its neighbourhood bit masks)          */
 } gg_relax_kind;
 
 /* dst filters (api::filter(weak, dst, lambda), api.h:687-706). */
@@ -194,7 +196,8 @@ typedef enum gg_filter_kind {
     GG_FILTER_NONE = 0,
     GG_FILTER_GT_CONST = 1, /* a[d] > _c(k)       (BFSLVLv.C:190-194) */
     GG_FILTER_NE_ZERO = 2,  /* a[d] != zero_val   (CCv.C:566-570)     */
-    GG_FILTER_MSB_SET = 3   /* msbset(a[d])       (BFSv.C:139-142)    */
+    GG_FILTER_MSB_SET = 3,  /* msbset(a[d])       (BFSv.C:139-142)    */
+    GG_FILTER_NE_CONST = 4  /* a[d] != _c(k)      (FMv.C:353-354, k = _1s: all ones) */
 } gg_filter_kind;
 
 /* record (api::record, api.h:1450-1516). */
@@ -228,12 +231,12 @@ typedef enum gg_variant {
 typedef struct gg_emap_desc {
     int relax;              /* gg_relax_kind */
     gg_prop *a;             /* relaxed property a[d] (level / label / parent / y) */
-    gg_prop *src;           /* ADD_GATHER: contrib[s] (may be reduced precision) */
+    gg_prop *src;           /* ADD_GATHER: contrib[s] (may be reduced precision); OR_U32: src[s] */
     float src_scale;        /* ADD_GATHER: multiply gathered values by this (FP8 scale) */
     int accum_f64;          /* ADD_GATHER: accumulate in double (PRv) instead of float */
     int dst_filter;         /* gg_filter_kind */
     gg_prop *dst_filter_prop;
-    int64_t dst_filter_k;   /* GT_CONST constant */
+    int64_t dst_filter_k;   /* GT_CONST / NE_CONST constant */
     int src_strong;         /* api::strong src filter (0 = weak) */
     int record;             /* gg_record_kind */
     gg_prop *prev;          /* NE_PREV: previous copy of a */
@@ -277,6 +280,7 @@ GG_API gg_status gg_edgemap(gg_graph *g, const gg_emap_desc *d, gg_frontier *in,
 #define GG_VM_MAX_PROPS 8
 #define GG_VM_MAX_CONSTS 8
 #define GG_VM_MAX_REDUCE 4
+#define GG_VM_MAX_TMP 4
 
 /* Stack-machine opcodes.  Operands are double on the stack; property
  * loads/stores convert from/to the property's dtype. */
@@ -294,7 +298,13 @@ typedef enum gg_vm_op {
     GG_VM_TOF32 = 18,      /* round top of stack to float */
     GG_VM_SELECT = 19,     /* c ? x : y  (pops y, x, c) */
     GG_VM_FILTER = 20,     /* pop; if non-zero add v to the output frontier */
-    GG_VM_DUP = 21
+    GG_VM_DUP = 21,
+    /* uint32 bit operations on the operands taken modulo 2^32 (FMv.C:370-392) */
+    GG_VM_AND = 22, GG_VM_OR = 23, GG_VM_XOR = 24, GG_VM_NOT = 25,
+    GG_VM_TOU32 = 26,      /* top of stack modulo 2^32 (unsigned arithmetic) */
+    GG_VM_TSET = 27,       /* tmp[arg] = pop (expr::let bindings, GG_VM_MAX_TMP of them) */
+    GG_VM_TGET = 28,       /* push tmp[arg] */
+    GG_VM_LE = 29, GG_VM_GE = 30
 } gg_vm_op;
 
 typedef struct gg_vmap_desc {

@@ -118,13 +118,22 @@ public:
     partitioner() = default;
     partitioner(gg_graph *g, VID n) : g_(g), n_(n) {}
     VID get_num_vertices() const { return n_; }
-    VID get_num_elements() const { return n_; }
+    VID get_num_elements() const { return n_ * scale_; }
     int get_num_partitions() const { return 1; }
+    // scale(k): the partitioning of k consecutive elements per vertex
+    // (graph/partitioning.h); arrays allocated from it hold n*k elements
+    partitioner scale(VID k) const {
+        partitioner p(*this);
+        p.scale_ *= k;
+        return p;
+    }
+    VID get_scale() const { return scale_; }
     gg_graph *graph() const { return g_; }
 
 private:
     gg_graph *g_ = nullptr;
     VID n_ = 0;
+    VID scale_ = 1;
 };
 
 // Host view of the CSR (GraphCSx accessors the analytics call through
@@ -268,6 +277,10 @@ inline std::ostream &operator<<(std::ostream &os, frontier_type t) {
     int i = (int)t;
     return os << names[(i >= 0 && i <= 11) ? i : 11];
 }
+
+// How an operator computes its output frontier (frontier/type.h:148-153);
+// analytics name it in operator structs.
+enum frontier_mode { fm_all_true = 0, fm_reduction = 1, fm_calculate = 2, fm_N = 3 };
 
 class frontier {
 public:
@@ -427,7 +440,8 @@ namespace expr {
 
 enum class NK {
     VarSrc, VarDst, VarV, VarEdge, Const, Ref, Min, SetIf, Assign, AddAssign, MulAssign,
-    Add, Sub, Mul, Div, Eq, Ne, Lt, Gt, Le, Ge, LAnd, LOr, Cast, Abs, Iif, MsbSet, Noop
+    Add, Sub, Mul, Div, Eq, Ne, Lt, Gt, Le, Ge, LAnd, LOr, Cast, Abs, Iif, MsbSet, Noop,
+    OrAssign, BAnd, BOr, BXor, BNot, Let, Tmp, Seq
 };
 
 struct Node {
@@ -437,6 +451,7 @@ struct Node {
     gg_dtype dt = GG_F64;  // Const / Ref / Cast: value type
     gg_prop *prop = nullptr;  // Ref: device array
     double *host = nullptr;   // Ref: host scalar accumulator (array_ro over a host variable)
+    bool ones = false;        // Const _1s: all bits set in the type of the other operand
 };
 using NP = std::shared_ptr<Node>;
 
@@ -450,7 +465,8 @@ inline NP mk(NK k, std::vector<NP> c = {}) {
 inline std::string show(const NP &n) {
     static const char *nm[] = {"s", "d", "v", "e", "const", "ref", "min", "setif", "=", "+=", "*=",
                                "+", "-", "*", "/", "==", "!=", "<", ">", "<=", ">=", "&&", "||",
-                               "cast", "abs", "iif", "msbset", "noop"};
+                               "cast", "abs", "iif", "msbset", "noop", "|=", "&", "|", "^", "~", "let", "tmp",
+                               "seq"};
     std::ostringstream os;
     if (n->k == NK::Const) return (os << n->cval, os.str());
     os << nm[(int)n->k];
@@ -464,6 +480,7 @@ inline std::string show(const NP &n) {
 
 class E;
 template <typename T> E _c(T v);
+inline E make_noop();
 
 // An expression value.  Copying an E copies the handle, not the tree.
 class E {
@@ -480,6 +497,8 @@ public:
     E setif(const E &x) const { return E(mk(NK::SetIf, {n_, x.n_})); }
     E operator+=(const E &x) const { return E(mk(NK::AddAssign, {n_, x.n_})); }
     E operator*=(const E &x) const { return E(mk(NK::MulAssign, {n_, x.n_})); }
+    // a[d] |= x: bitwise-or relax, "changed" as value (FMv.C:356-358)
+    E operator|=(const E &x) const { return E(mk(NK::OrAssign, {n_, x.n_})); }
     // assignment builds a node (a[v] = x); E values are never re-seated
     E operator=(const E &x) const { return E(mk(NK::Assign, {n_, x.n_})); }
     // _0(vid): the zero index of a scalar accumulator (PRv.C:241)
@@ -488,6 +507,8 @@ public:
 private:
     NP n_;
 };
+
+inline E make_noop() { return E(mk(NK::Noop)); }
 
 inline E cst(double v, gg_dtype dt) {
     auto n = mk(NK::Const);
@@ -508,16 +529,29 @@ inline E::E(T v) : n_(cst((double)v, literal_dtype<T>()).node()) {}
 template <typename T> inline E _c(T v) { return cst((double)v, literal_dtype<T>()); }
 
 // Result type of an arithmetic node, as C++ promotes: double if either side
-// is double, else float if either side is float, else the integer type.
+// is double, else float if either side is float, else uint32 if either side
+// is uint32, else the integer type.
 inline gg_dtype promote(gg_dtype a, gg_dtype b) {
     if (a == GG_F64 || b == GG_F64) return GG_F64;
     if (a == GG_F32 || b == GG_F32) return GG_F32;
+    if (a == GG_U32 || b == GG_U32) return GG_U32;
     return a;
 }
+// _1s takes the type of the operand it meets (dsl/ast/value.h: all bits
+// set in the element type): 2^32-1 beside a uint32 operand, -1 elsewhere.
+inline NP fit_ones(const NP &c, gg_dtype dt) {
+    if (c->k != NK::Const || !c->ones) return c;
+    auto n = mk(NK::Const);
+    n->cval = dt == GG_U32 ? 4294967295.0 : -1.0;
+    n->dt = dt;
+    return n;
+}
 inline E binop(NK k, const E &a, const E &b) {
-    auto n = mk(k, {a.node(), b.node()});
-    n->dt = (k == NK::Add || k == NK::Sub || k == NK::Mul || k == NK::Div) ? promote(a.node()->dt, b.node()->dt)
-                                                                            : GG_I32;
+    const NP l = fit_ones(a.node(), b.node()->dt), r = fit_ones(b.node(), a.node()->dt);
+    auto n = mk(k, {l, r});
+    const bool arith = k == NK::Add || k == NK::Sub || k == NK::Mul || k == NK::Div;
+    const bool bits = k == NK::BAnd || k == NK::BOr || k == NK::BXor;
+    n->dt = arith || bits ? promote(l->dt, r->dt) : GG_I32;
     return E(n);
 }
 #define GG_BINOP(op, kind) \
@@ -534,15 +568,30 @@ GG_BINOP(<=, Le)
 GG_BINOP(>=, Ge)
 GG_BINOP(&&, LAnd)
 GG_BINOP(||, LOr)
+GG_BINOP(&, BAnd)
+GG_BINOP(|, BOr)
+GG_BINOP(^, BXor)
 #undef GG_BINOP
+inline E operator~(const E &a) {
+    auto n = mk(NK::BNot, {a.node()});
+    n->dt = a.node()->dt == GG_I32 ? GG_I32 : GG_U32;
+    return E(n);
+}
 
 static const E _0 = cst(0, GG_I32);
 static const E _1 = cst(1, GG_I32);
-static const E _1s = cst(-1, GG_I32);
+static const E _1s = [] {
+    E e = cst(-1, GG_I32);
+    e.node()->ones = true;
+    return e;
+}();
 static const E _true = cst(1, GG_I32);
 static const E _false = cst(0, GG_I32);
 
 inline E zero_val(const E &) { return cst(0, GG_I32); }
+inline E true_val(const E &) { return cst(1, GG_I32); }
+// constant_val2(x, v): v in its own type T (dsl/ast/value.h:93-98)
+template <typename T> inline E constant_val2(const E &, T v) { return cst((double)v, literal_dtype<T>()); }
 // constant_val(x, v): v in the type of x (a float operand rounds v to float)
 template <typename T> inline E constant_val(const E &x, T v) {
     const gg_dtype dt = x.node()->k == NK::Ref || x.node()->k == NK::Cast || x.node()->k == NK::Const
@@ -565,12 +614,29 @@ inline E make_unop_abs(const E &a) {
 // blend (dsl/ast/ternop.h:65-125 -> blendm(m, l, r) = m ? r : l,
 // target/scalar_int.h:212-214); the node keeps (c, taken, not taken)
 inline E iif(const E &c, const E &l, const E &r) {
-    auto n = mk(NK::Iif, {c.node(), r.node(), l.node()});
-    n->dt = promote(l.node()->dt, r.node()->dt);
+    const NP ln = fit_ones(l.node(), r.node()->dt), rn = fit_ones(r.node(), l.node()->dt);
+    auto n = mk(NK::Iif, {c.node(), rn, ln});
+    n->dt = promote(ln->dt, rn->dt);
+    return E(n);
+}
+// let<AID>(init, cont): cont receives a reference to a temporary holding
+// init (dsl/ast/binop.h:1540-1580); the temporary lives for one vertex
+template <auto AID, typename Fn> inline E let(const E &init, Fn cont) {
+    auto t = mk(NK::Tmp);
+    t->dt = init.node()->dt;
+    E body = cont(E(t));
+    auto n = mk(NK::Let, {init.node(), body.node(), t});
+    n->dt = body.node()->dt;
+    return E(n);
+}
+// make_seq(a, b, ...): the statements in order (dsl/ast/binop.h:370-395)
+inline E make_seq() { return make_noop(); }
+template <typename... R> inline E make_seq(const E &a, const R &... r) {
+    auto n = mk(NK::Seq, {a.node(), E(r).node()...});
+    n->dt = n->c.back()->dt;
     return E(n);
 }
 inline E msbset(const E &a) { return E(mk(NK::MsbSet, {a.node()})); }
-inline E make_noop() { return E(mk(NK::Noop)); }
 
 inline E var(NK k) {
     auto n = mk(k);
@@ -699,6 +765,9 @@ public:
     using type = T;
     void allocate(const numa_allocation_partitioned &a) {
         if constexpr (graptor_b200::has_dtype<T>::value) {
+            // device arrays hold one element per vertex
+            if (a.part.get_scale() != 1)
+                throw graptor_b200::error(GG_ERR_UNSUPPORTED, "mmap_ptr of more than one element per vertex");
             graptor_b200::check(gg_prop_create_managed(a.part.graph(), graptor_b200::dtype_of<T>::value, &p_),
                                 "gg_prop_create_managed");
             void *d = nullptr;
@@ -706,11 +775,15 @@ public:
             graptor_b200::registry()[d] = p_;
             d_ = (T *)d;
         } else {
-            d_ = (T *)std::calloc((size_t)a.part.get_num_vertices() + 1, sizeof(T));
+            d_ = (T *)std::calloc((size_t)a.part.get_num_elements() + 1, sizeof(T));
             if (!d_) throw graptor_b200::error(GG_ERR_OOM, "mmap_ptr host allocation");
         }
     }
-    T *get() const { return d_; }
+    // the array, for host reads and writes: waits for the device work queued so far
+    T *get() const {
+        graptor_b200::host_sync();
+        return d_;
+    }
     operator T *() { return d_; }
     operator const T *() const { return d_; }
     explicit operator bool() const { return d_ != nullptr; }
@@ -965,6 +1038,13 @@ inline void lower_relax(const NP &r, gg_emap_desc &d) {
             return;
         }
     }
+    if (r->k == NK::OrAssign && is_ref_at(r->c[0], NK::VarDst) && is_ref_at(r->c[1], NK::VarSrc) &&
+        r->c[0]->dt == GG_U32 && r->c[1]->dt == GG_U32) {
+        d.relax = GG_RELAX_OR_U32;  // a[d] |= b[s] (FMv.C:356-358)
+        d.a = r->c[0]->prop;
+        d.src = r->c[1]->prop;
+        return;
+    }
     if (r->k == NK::SetIf && is_ref_at(r->c[0], NK::VarDst) && r->c[1]->k == NK::VarSrc && r->c[0]->dt == GG_U32) {
         d.relax = GG_RELAX_SETIF_U32;  // a[d].setif(s)
         d.a = r->c[0]->prop;
@@ -993,6 +1073,12 @@ inline void lower_dst_filter(const NP &f, gg_emap_desc &d) {
     if (f->k == NK::Ne && is_ref_at(f->c[0], NK::VarDst) && is_const(f->c[1], 0)) {
         d.dst_filter = GG_FILTER_NE_ZERO;
         d.dst_filter_prop = f->c[0]->prop;
+        return;
+    }
+    if (f->k == NK::Ne && is_ref_at(f->c[0], NK::VarDst) && f->c[1]->k == NK::Const) {
+        d.dst_filter = GG_FILTER_NE_CONST;  // a[d] != k, e.g. k = _1s (FMv.C:353-354)
+        d.dst_filter_prop = f->c[0]->prop;
+        d.dst_filter_k = (int64_t)f->c[1]->cval;
         return;
     }
     if (f->k == NK::MsbSet && is_ref_at(f->c[0], NK::VarDst)) {
@@ -1050,8 +1136,17 @@ struct VmBuilder {
     int saved_code = 0, saved_const = 0;
     gg_vmap_desc saved;
     std::vector<double *> saved_red;
-    void mark() { saved = d; saved_code = d.ncode; saved_const = nconst; saved_red = red_targets; }
-    void undo() { d = saved; nconst = saved_const; red_targets = saved_red; }
+    std::map<const expr::Node *, int> tmps, saved_tmps;  // let temporaries -> slot
+    void mark() { saved = d; saved_code = d.ncode; saved_const = nconst; saved_red = red_targets; saved_tmps = tmps; }
+    void undo() { d = saved; nconst = saved_const; red_targets = saved_red; tmps = saved_tmps; }
+    // let: evaluate init into a fresh temporary slot
+    bool bind(const NP &let) {
+        if (tmps.size() >= GG_VM_MAX_TMP) unsupported("let (too many temporaries)", let);
+        const int slot = (int)tmps.size();
+        if (!value(let->c[0]) || !emit(GG_VM_TSET, slot)) return false;
+        tmps[let->c[2].get()] = slot;
+        return true;
+    }
 
     bool value(const NP &n) {
         switch (n->k) {
@@ -1063,16 +1158,27 @@ struct VmBuilder {
             return s >= 0 && emit(GG_VM_LOAD, s) && (n->dt == GG_F32 ? emit(GG_VM_TOF32) : true);
         }
         case NK::Add: case NK::Sub: case NK::Mul: case NK::Div: case NK::Eq: case NK::Ne:
-        case NK::Lt: case NK::Gt: {
+        case NK::Lt: case NK::Gt: case NK::Le: case NK::Ge: case NK::BAnd: case NK::BOr: case NK::BXor: {
             static const std::map<NK, int> ops = {{NK::Add, GG_VM_ADD}, {NK::Sub, GG_VM_SUB}, {NK::Mul, GG_VM_MUL},
                                                   {NK::Div, GG_VM_DIV}, {NK::Eq, GG_VM_EQ}, {NK::Ne, GG_VM_NE},
-                                                  {NK::Lt, GG_VM_LT}, {NK::Gt, GG_VM_GT}};
+                                                  {NK::Lt, GG_VM_LT}, {NK::Gt, GG_VM_GT}, {NK::Le, GG_VM_LE},
+                                                  {NK::Ge, GG_VM_GE}, {NK::BAnd, GG_VM_AND}, {NK::BOr, GG_VM_OR},
+                                                  {NK::BXor, GG_VM_XOR}};
             if (!value(n->c[0]) || !value(n->c[1]) || !emit(ops.at(n->k))) return false;
+            const bool arith = n->k == NK::Add || n->k == NK::Sub || n->k == NK::Mul || n->k == NK::Div;
             // float arithmetic (float operands, no double one) rounds like the reference
-            if (n->dt == GG_F32 && (n->k == NK::Add || n->k == NK::Sub || n->k == NK::Mul || n->k == NK::Div))
-                return emit(GG_VM_TOF32);
+            if (n->dt == GG_F32 && arith) return emit(GG_VM_TOF32);
+            // uint32 arithmetic wraps modulo 2^32
+            if (n->dt == GG_U32 && arith && n->k != NK::Div) return emit(GG_VM_TOU32);
             return true;
         }
+        case NK::BNot: return value(n->c[0]) && emit(GG_VM_NOT);
+        case NK::Tmp: {
+            auto it = tmps.find(n.get());
+            if (it == tmps.end()) unsupported("temporary outside its let", n);
+            return emit(GG_VM_TGET, it->second);
+        }
+        case NK::Let: return bind(n) && value(n->c[1]);
         case NK::Cast: {
             if (!value(n->c[0])) return false;
             return n->dt == GG_F32 ? emit(GG_VM_TOF32) : true;
@@ -1085,8 +1191,19 @@ struct VmBuilder {
     // one statement; returns false when the program is full
     bool statement(const NP &s) {
         mark();
+        const bool ok = stmt(s);
+        if (!ok) undo();
+        return ok;
+    }
+    bool stmt(const NP &s) {
         bool ok = true;
         if (s->k == NK::Noop) return true;
+        if (s->k == NK::Seq) {
+            for (const NP &c : s->c)
+                if (!stmt(c)) return false;
+            return true;
+        }
+        if (s->k == NK::Let) return bind(s) && stmt(s->c[1]);
         const NP &lhs = s->c.empty() ? s : s->c[0];
         if (lhs->k != NK::Ref) unsupported("vertex statement", s);
         if (lhs->host) {  // scalar accumulator: accum[_0(v)] += x
@@ -1104,7 +1221,6 @@ struct VmBuilder {
                 else unsupported("vertex statement", s);
             }
         }
-        if (!ok) undo();
         return ok;
     }
 };
@@ -1141,6 +1257,9 @@ public:
         return *this;
     }
     template <typename Fn> lazy_executor &vertex_scan(Fn fn) { return vertex_map(fn); }
+    // vertex_scan(F, fn) (dsl/vertexmap.h:2217-2227): fn on the vertices of F,
+    // its scalar reductions summed into their host variables
+    template <typename Fn> lazy_executor &vertex_scan(frontier &F, Fn fn) { return vertex_map(F, fn); }
     template <typename G, typename Fn>
     lazy_executor &vertex_filter(const G &GA, frontier &F, frontier &out, Fn fn) {
         flush();

@@ -206,6 +206,9 @@ template <typename Fn> void map_vertexL(const partitioner &part, Fn fn) {
     graptor_b200::host_sync();
     for (VID v = 0, n = part.get_num_vertices(); v < n; ++v) fn(v);
 }
+// map_vertex_serialL: the same loop, in vertex order (the reference runs it
+// serially for repeatable random draws, FMv.C:291-298)
+template <typename Fn> void map_vertex_serialL(const partitioner &part, Fn fn) { map_vertexL(part, fn); }
 template <typename I, typename Fn> void parallel_loop(I lo, I hi, Fn fn) {
     graptor_b200::host_sync();
     for (I i = lo; i < hi; ++i) fn(i);

@@ -799,3 +799,74 @@ ORC_API int orc_pr_vary_staged(uint32_t n, const uint64_t *in_off, const uint32_
     free(cq);
     return iter;
 }
+
+/* ---------------------------------------------------------------------------
+ * Flajolet-Martin neighbourhood sizes (reference: bench/FMv.C:262-452, K = 1
+ * bit string of 32 bits per vertex, DEFERRED_UPDATE / CONVERGENCE on).
+ *
+ * mask/prev start at init.  Each iteration over the frontier F (all vertices
+ * first): mask[d] |= prev[s] for every edge s->d with s in F (FMv.C:356-358);
+ * the output frontier is {d : mask[d] != prev[d]} (FMv.C:347-350).  Over the
+ * output, in vertex order: the estimate 2^(lowest zero bit of mask[v]) / 0.77351
+ * (2^32-1 for mask 0, 0 for all ones) replaces est[v] (a float), prev[v] =
+ * mask[v], and the iteration's sum accumulates estimate - old estimate
+ * (FMv.C:386-412); nhm[i] is the running sum as a float, nactv[i] = |F|.
+ * Returns the iteration count (the first empty output ends the loop), or -1
+ * on an allocation failure or when more than max_iters would be needed.
+ * ------------------------------------------------------------------------ */
+ORC_API int orc_fm(uint32_t n, const uint64_t *off, const uint32_t *adj, const uint32_t *init,
+                   uint32_t *mask, float *nhm, uint64_t *nactv, int max_iters) {
+    uint32_t *prev = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    float *est = (float *)calloc(n ? n : 1, sizeof(float));
+    uint32_t *F = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    uint32_t *out = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    if (!prev || !est || !F || !out) { free(prev); free(est); free(F); free(out); return -1; }
+    for (uint32_t v = 0; v < n; ++v) { mask[v] = prev[v] = init[v]; F[v] = v; }
+    uint64_t nf = n;
+    double accum = 0;
+    int it = 0;
+    while (nf) {
+        if (it >= max_iters) { it = -1; break; }
+        nactv[it] = nf;
+        for (uint64_t i = 0; i < nf; ++i) {
+            const uint32_t s = F[i];
+            for (uint64_t e = off[s]; e < off[s + 1]; ++e) mask[adj[e]] |= prev[s];
+        }
+        uint64_t no = 0;
+        for (uint32_t v = 0; v < n; ++v)
+            if (mask[v] != prev[v]) out[no++] = v;
+        double sum = 0;
+        for (uint64_t i = 0; i < no; ++i) {
+            const uint32_t v = out[i], z = ~mask[v];
+            const double low = mask[v] == 0 ? 4294967295.0 : (double)(z & (0u - z));
+            const double e_new = (1.0 / 0.77351) * low, e_old = (double)est[v];
+            prev[v] = mask[v];
+            est[v] = (float)e_new;
+            sum += e_new - e_old;
+        }
+        accum += sum;
+        nhm[it] = (float)accum;
+        uint32_t *t = F; F = out; out = t;
+        nf = no;
+        ++it;
+    }
+    free(prev); free(est); free(F); free(out);
+    return it;
+}
+
+/* The effective diameter FMv derives from the running sums (FMv.C:452-478):
+ * interpolated hop count at which the sum reaches 0.9 of its final value,
+ * in float arithmetic. */
+ORC_API float orc_fm_deffg(const float *nhm, int iters) {
+    if (iters <= 1) return 1.0f;
+    const float nmax = nhm[iters - 1];
+    float nh = nmax, nhm1 = nmax;
+    int i;
+    for (i = iters - 2; i >= 0; --i) {
+        nhm1 = nhm[i];
+        if (nhm1 < 0.9 * nmax) break;
+        nh = nhm1;
+    }
+    if (nh == nhm1) return 1.0f;
+    return (float)(i + (0.9 * nmax - nhm1) / (nh - nhm1));
+}

@@ -66,6 +66,10 @@ def lib() -> C.CDLL:
                                      C.c_double, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_cfp_convert_bits.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int,
                                            C.c_void_p, C.c_void_p]
+        L.orc_fm.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                             C.c_void_p, C.c_int]
+        L.orc_fm_deffg.argtypes = [C.c_void_p, C.c_int]
+        L.orc_fm_deffg.restype = C.c_float
         L.orc_free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
@@ -262,6 +266,47 @@ def cfp_convert_bits(bits: np.ndarray, S: int, E: int, M: int):
 # ---------------------------------------------------------------------------
 # The reference's own programs, built from its sources by oracle/Makefile.
 # ---------------------------------------------------------------------------
+
+def fm_draws(n: int) -> np.ndarray:
+    """FMv's initial bit masks for draws 0..n-1 (oracle/fm_draws.cc: the C++
+    standard library's mt19937_64 and uniform_int_distribution, as FMv.C
+    draws them)."""
+    p = os.path.join(os.path.dirname(LIB_PATH), "liboracle_fm.so")
+    if not os.path.exists(p):
+        raise RuntimeError(f"oracle library missing: {p} (run make -C oracle)")
+    L = C.CDLL(p)
+    L.orc_fm_draws.argtypes = [C.c_uint64, C.c_void_p]
+    out = np.empty(max(n, 1), dtype=np.uint32)
+    L.orc_fm_draws(n, _p(out))
+    return out[:n]
+
+
+def fm(g: Graph, init: np.ndarray, max_iters: int = 4096):
+    """Flajolet-Martin neighbourhood estimation as FMv runs it (oracle.c
+    orc_fm): returns (final masks, per-iteration running sums as float32,
+    per-iteration frontier sizes, effective diameter deffG)."""
+    init = np.ascontiguousarray(init, dtype=np.uint32)
+    mask = np.empty(max(g.n, 1), dtype=np.uint32)
+    nhm = np.zeros(max_iters, dtype=np.float32)
+    nactv = np.zeros(max_iters, dtype=np.uint64)
+    it = lib().orc_fm(g.n, _p(g.off), _p(g.adj), _p(init), _p(mask), _p(nhm), _p(nactv), max_iters)
+    if it < 0:
+        raise RuntimeError("orc_fm failed (allocation or iteration cap)")
+    return mask[:g.n], nhm[:it], nactv[:it], float(lib().orc_fm_deffg(_p(nhm), it))
+
+
+def ref_fm(bin_path: str, out_prefix: str, threads: int | None = None):
+    """The reference FMv run by oracle/harness/ref_fm.C: returns (final masks
+    in original order, layout id of each vertex, iterations, deffG, frontier
+    sizes per iteration, padded vertex count)."""
+    txt = _run([ref_prog("ref_fm"), bin_path, out_prefix], threads)
+    head = next(l for l in txt.splitlines() if l.startswith("n "))
+    w = head.split()
+    nact = next(l for l in txt.splitlines() if l.startswith("nactv")).split()[1:]
+    mask = np.fromfile(out_prefix + ".mask", dtype=np.uint32)
+    remap = np.fromfile(out_prefix + ".remap", dtype=np.uint32)
+    return mask, remap, int(w[5]), float(w[7]), np.array([int(x) for x in nact], dtype=np.uint64), int(w[3])
+
 
 def ref_variant() -> str:
     """Pick the reference build the host CPU can execute (AVX-512 or AVX2)."""

@@ -15,10 +15,10 @@ def pytest_configure(config):
 
 
 def _ensure_oracle():
-    lib = os.path.join(ROOT, "oracle", "liboracle.so")
-    src = os.path.join(ROOT, "oracle", "oracle.c")
-    if not os.path.exists(lib) or os.path.getmtime(lib) < os.path.getmtime(src):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
+    for lib, src in (("liboracle.so", "oracle.c"), ("liboracle_fm.so", "fm_draws.cc")):
+        lib, src = os.path.join(ROOT, "oracle", lib), os.path.join(ROOT, "oracle", src)
+        if not os.path.exists(lib) or os.path.getmtime(lib) < os.path.getmtime(src):
+            subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
 
 
 _ensure_oracle()

@@ -84,6 +84,69 @@ int main() {
         CHECK(tof32 >= 2);  // the load of y and the float product
         CHECK(b.d.consts[0] == (double)0.85f);
     }
+    // FMv.C:347-358: a[d] |= b[s] relax, dst filter a[d] != _1s
+    {
+        gg_emap_desc d = relax_of(at(1, GG_U32, D) |= at(2, GG_U32, S));
+        CHECK(d.relax == GG_RELAX_OR_U32 && d.a == P(1) && d.src == P(2));
+        std::memset(&d, 0, sizeof(d));
+        graptor_b200::lower_dst_filter((at(1, GG_U32, D) != _1s).node(), d);
+        CHECK(d.dst_filter == GG_FILTER_NE_CONST && (uint32_t)d.dst_filter_k == 0xFFFFFFFFu);
+    }
+    // FMv.C:386-412: the neighbourhood estimate as one vertex program, run
+    // here through the documented stack semantics of the opcodes
+    {
+        double accum = 0;
+        E m = at(1, GG_U32, V), pm = at(2, GG_U32, V), est = at(3, GG_F32, V);
+        E acc = ref(nullptr, &accum, GG_F64, zero_val(var(V)));
+        E st = let<4>(cast<double>(est), [&](E old_est) {
+            return let<3>(_c<double>(1.0 / 0.77351) * cast<double>(iif(m != _0, _1s, ~m ^ (~m & (~m - _1)))),
+                          [&](E new_est) {
+                              return make_seq(pm = m, est = cast<float>(new_est), acc += new_est - old_est);
+                          });
+        });
+        graptor_b200::VmBuilder b;
+        CHECK(b.statement(st.node()));
+        CHECK(b.d.nreduce == 1);
+        const uint32_t masks[] = {0u, 1u, 3u, 0x17u, 0x7FFFFFFFu, 0xFFFFFFFFu, 0x80000000u};
+        for (uint32_t mv : masks) {
+            double props[8] = {0};
+            const int sm = b.prop_slot(P(1)), sp = b.prop_slot(P(2)), se = b.prop_slot(P(3));
+            props[sm] = mv;
+            props[se] = 5.0;  // the previous estimate
+            double stk[16], tmp[GG_VM_MAX_TMP] = {0}, red = 0;
+            int sp_ = 0;
+            auto u = [](double x) { return (uint32_t)(int64_t)x; };
+            for (int i = 0; i < b.d.ncode; ++i) {
+                const int a = b.d.arg[i];
+                switch (b.d.code[i]) {
+                case GG_VM_CONST: stk[sp_++] = b.d.consts[a]; break;
+                case GG_VM_LOAD: stk[sp_++] = props[a]; break;
+                case GG_VM_STORE: props[a] = stk[--sp_]; break;
+                case GG_VM_ADD: --sp_; stk[sp_ - 1] += stk[sp_]; break;
+                case GG_VM_SUB: --sp_; stk[sp_ - 1] -= stk[sp_]; break;
+                case GG_VM_MUL: --sp_; stk[sp_ - 1] *= stk[sp_]; break;
+                case GG_VM_NE: --sp_; stk[sp_ - 1] = stk[sp_ - 1] != stk[sp_]; break;
+                case GG_VM_AND: --sp_; stk[sp_ - 1] = u(stk[sp_ - 1]) & u(stk[sp_]); break;
+                case GG_VM_XOR: --sp_; stk[sp_ - 1] = u(stk[sp_ - 1]) ^ u(stk[sp_]); break;
+                case GG_VM_NOT: stk[sp_ - 1] = (uint32_t)~u(stk[sp_ - 1]); break;
+                case GG_VM_TOU32: stk[sp_ - 1] = u(stk[sp_ - 1]); break;
+                case GG_VM_TOF32: stk[sp_ - 1] = (float)stk[sp_ - 1]; break;
+                case GG_VM_TSET: tmp[a] = stk[--sp_]; break;
+                case GG_VM_TGET: stk[sp_++] = tmp[a]; break;
+                case GG_VM_SELECT: sp_ -= 2; stk[sp_ - 1] = stk[sp_ - 1] != 0 ? stk[sp_] : stk[sp_ + 1]; break;
+                case GG_VM_REDUCE_ADD: red += stk[--sp_]; break;
+                default: CHECK(!"unexpected opcode"); i = b.d.ncode; break;
+                }
+            }
+            // rho(~m) = lowest zero bit of m; m == 0 counts as 2^32 - 1 (FMv.C:83-103)
+            double lowest = mv == 0 ? 4294967295.0 : (~mv == 0 ? 0.0 : (double)(~mv & (0u - ~mv)));
+            const double want = (1.0 / 0.77351) * lowest;
+            CHECK(sp_ == 0);
+            CHECK(props[sp] == (double)mv);
+            CHECK(props[se] == (double)(float)want);
+            CHECK(red == want - 5.0);
+        }
+    }
     if (fails) return 1;
     std::printf("ok\n");
     return 0;

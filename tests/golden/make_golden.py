@@ -11,6 +11,12 @@ programs on it, compiled from the reference sources by oracle/Makefile:
                  4620 (customfp<6,10> with float sums to 1e-3, then FP32 with
                  double sums), 99 (bfloat16-by-truncation contributions, float
                  sums) and 11 (FP64 throughout)
+  fm_*         - FMv.C run by oracle/harness/ref_fm.C: the final bit mask of
+                 each vertex (fm_mask), its layout id (fm_remap: the vertex
+                 starts with FMv's initial draw number fm_remap[v]), the
+                 iteration count, deffG and the frontier size per iteration
+                 (fm_nactv; the first counts the layout's padding vertices,
+                 fm_padded in all)
 customfp_sweep.npz holds float bit patterns and, per pattern, the codes and
 decoded floats of the reference's customfp<6,10> and scustomfp<true,8,7>
 conversions (harness oracle/harness/ref_cfp.C).
@@ -18,7 +24,8 @@ The config-1 workload (R-MAT scale 16, 2^20 edges) is stored without its CSR
 (7 MB): the fixture keeps the CSR's SHA-256 and the generator parameters.
 
 Run (needs the reference tree and `make -C oracle ref`):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py --fm-only  # add / refresh the fm_* keys only
 """
 import hashlib
 import os
@@ -68,8 +75,33 @@ def run_reference(g, roots, pr_iters, tmp):
     return levels, parents, cc.astype(np.uint32), pr, vary
 
 
+def fm_reference(g, tmp):
+    p = os.path.join(tmp, "g.bin")
+    O.write_bin(g, p)
+    mask, remap, iters, deffg, nactv, padded = O.ref_fm(p, os.path.join(tmp, "fm"))
+    # sanity: the restatement must agree before a fixture is written
+    m2, _, na2, _ = O.fm(g, O.fm_draws(padded)[remap])
+    assert np.array_equal(mask, m2) and np.array_equal(nactv[1:], na2[1:])
+    return dict(fm_mask=mask, fm_remap=remap, fm_iters=np.int64(iters), fm_deffg=np.float64(deffg),
+                fm_nactv=nactv, fm_padded=np.int64(padded))
+
+
+def add_fm(name, tmp):
+    path = os.path.join(HERE, name + ".npz")
+    d = dict(np.load(path))
+    if "off" in d:
+        g = O.Graph(int(d["n"]), d["off"], d["adj"])
+    else:
+        g = O.rmat(int(d["scale"]), int(d["nedges"]), seed=int(d["seed"]))
+        assert csr_sha256(g.off, g.adj) == str(d["sha256"]), name
+    d.update(fm_reference(g, tmp))
+    np.savez_compressed(path, **d)
+    print(name, "fm iters", int(d["fm_iters"]), "deffG", float(d["fm_deffg"]))
+
+
 def save(name, g, roots, pr_iters, tmp, store_csr=True, params=None):
     levels, parents, cc, pr, vary = run_reference(g, roots, pr_iters, tmp)
+    vary.update(fm_reference(g, tmp))
     # sanity: the restatement must agree before a fixture is written
     for r, l in zip(roots, levels):
         assert np.array_equal(O.bfs_level(g, r), l), name
@@ -108,6 +140,11 @@ def main():
     if not O.ref_available("ref_bfslvl"):
         raise SystemExit("reference build missing: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
+        if "--fm-only" in sys.argv:
+            for name in ["rmat10_ef8", "rmat12_ef16", "grid20x32_del5pct", "er2000_deg6", "edgecases32",
+                         "config1_rmat16"]:
+                add_fm(name, tmp)
+            return
         save_customfp_sweep(tmp)
         g = O.rmat(10, 8 << 10, seed=11)
         save("rmat10_ef8", g, roots_for(g, 3, 1), 20, tmp)

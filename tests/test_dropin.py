@@ -131,3 +131,36 @@ def test_reference_bfs_sources_with_their_driver(tmp_path, prog):
     z, g, p = _graph_file(tmp_path, "rmat12_ef16")
     r = _driver(prog, ["-s", "-b", "-rounds", "2", "-start", str(int(z["bfs_roots"][0])), p])
     assert "FAIL" not in (r.stdout + r.stderr), (r.stdout[-1000:], r.stderr[-1000:])
+
+
+def _fm_lines(txt):
+    head = next(l for l in txt.splitlines() if l.startswith("n ")).split()
+    nact = next(l for l in txt.splitlines() if l.startswith("nactv")).split()[1:]
+    return int(head[5]), float(head[7]), np.array([int(x) for x in nact], dtype=np.uint64)
+
+
+@pytest.mark.parametrize("name", _golden_graphs())
+def test_reference_fmv_source_on_gpu(tmp_path, name):
+    """FMv.C run on the GPU by the fm harness: with the same initial draws in
+    vertex order, the final bit masks equal the oracle's bit for bit (the
+    oracle is pinned to the reference build), as do the iteration count and
+    the frontier sizes; deffG agrees to float rounding of the running sums."""
+    z, g, p = _graph_file(tmp_path, name)
+    r = subprocess.run([_prog("fm"), p, str(tmp_path / "fm")], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    iters, deffg, nactv = _fm_lines(r.stdout)
+    mask = np.fromfile(str(tmp_path / "fm.mask"), dtype=np.uint32)
+    m2, nhm, na2, dg2 = O.fm(g, O.fm_draws(g.n))
+    assert np.array_equal(mask, m2)
+    assert iters == len(nhm) and np.array_equal(nactv, na2)
+    assert abs(deffg - dg2) <= 1e-4 * max(1.0, abs(dg2))
+
+
+def test_reference_fmv_with_its_driver(tmp_path):
+    """FMv.C with the reference's driver main(): two rounds, each deffG as the
+    oracle's."""
+    z, g, p = _graph_file(tmp_path, "grid20x32_del5pct")
+    r = _driver("FMv", ["-s", "-b", "-rounds", "2", p])
+    got = [float(l.split("deffG:")[1]) for l in r.stderr.splitlines() if l.startswith("deffG:")]
+    _, _, _, dg = O.fm(g, O.fm_draws(g.n))
+    assert len(got) == 2 and all(abs(x - dg) <= 1e-4 * max(1.0, abs(dg)) for x in got), (got, dg)
