@@ -1069,6 +1069,106 @@ static gg_status check_relax(gg_graph *g, const gg_emap_desc *d, gg_frontier *in
     return GG_OK;
 }
 
+// Maximal independent set step (MISv.C:235-255 with the dfsaop_MIS
+// relation of dsl/ast/dfsaop.h:49-230): a warp per 32-vertex word of the
+// destination set walks each destination's in-row, the lanes striding it.
+// Over its in-edges (s, d), s != d: d becomes out (2) when some s is in (3);
+// else a conditionally-in (1) d becomes undecided (0) when some s < d is
+// undecided or conditionally in.  The relation is order-independent per d;
+// states of sources that change during the step are read as the reference's
+// parallel step reads them, before or after the change (either way the
+// rounds converge to the same set: the greedy one in vertex-id order).
+// Recorded (EQ_ZERO): the destinations left undecided.
+__global__ void __launch_bounds__(kBlock) k_mis(EmapArgs A, uint8_t *__restrict__ st,
+                                                const uint32_t *__restrict__ dst_bits) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwords = (A.n + 31u) >> 5;
+    const uint32_t nw = (gridDim.x * kBlock) >> 5;
+    unsigned long long nv = 0, ne = 0, sc = 0;
+    for (uint32_t w = (blockIdx.x * kBlock + threadIdx.x) >> 5; w < nwords; w += nw) {
+        const uint32_t valid = (w + 1) * 32u <= A.n ? FULL : ((1u << (A.n & 31u)) - 1u);
+        uint32_t todo = (dst_bits ? dst_bits[w] : FULL) & valid;
+        bool rec = false;
+        while (todo) {
+            const uint32_t j = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const uint32_t d = (w << 5) + j;
+            const uint8_t old = st[d];
+            const uint64_t beg = A.in_off[d], end = A.in_off[d + 1];
+            bool in = false, low = false;
+            for (uint64_t e = beg + lane; e < end; e += 32) {
+                const uint32_t s = A.in_adj[e];
+                if (s == d) continue;
+                const uint8_t u = *(volatile const uint8_t *)(st + s);
+                in |= u == 3;
+                low |= s < d && u < 2;
+            }
+            in = __any_sync(FULL, in);
+            low = __any_sync(FULL, low);
+            const uint8_t nwv = in ? 2 : ((old == 1 && low) ? 0 : old);
+            if (lane == 0) {
+                if (nwv != old) st[d] = nwv;
+                sc += end - beg;
+            }
+            if (lane == j) rec = nwv == 0;
+        }
+        const uint32_t d = (w << 5) + lane;
+        rec = rec && A.record == GG_RECORD_EQ_ZERO;
+        if (A.out_bits) {
+            const unsigned bits = __ballot_sync(FULL, rec);
+            if (lane == 0) A.out_bits[w] = bits;
+            emit_out(A, rec, d, nv, ne);
+        }
+    }
+    if (A.out_cnt) flush_counts<kBlock>(A, nv, ne, sc);
+}
+
+static gg_status mis_relax(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_frontier *out) {
+    gg_ctx *ctx = g->ctx;
+    if (d->a->t != GG_U8) return set_error(ctx, GG_ERR_ARG, "MIS relax: uint8 states");
+    if (d->dst_filter != GG_FILTER_NONE && d->dst_filter != GG_FILTER_IN_FRONTIER)
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "MIS relax: dst filter NONE or IN_FRONTIER");
+    if (d->record != GG_RECORD_NONE && d->record != GG_RECORD_EQ_ZERO)
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "MIS relax: record NONE or EQ_ZERO");
+    if (d->dst_filter == GG_FILTER_NONE && in && !in->all)
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "MIS relax: the frontier filters destinations (IN_FRONTIER)");
+    EmapArgs A;
+    memset(&A, 0, sizeof(A));
+    A.off = g->off;
+    A.in_off = g->in_off;
+    A.in_adj = g->in_adj;
+    A.n = g->n;
+    A.record = out ? d->record : GG_RECORD_NONE;
+    const Tuning &t = tuning();
+    A.smax = t.bin_small_max;
+    A.mmax = t.bin_medium_max;
+    const uint32_t *dst_bits = nullptr;
+    if (d->dst_filter == GG_FILTER_IN_FRONTIER && in && !in->all) {
+        GG_CHECK(frontier_ensure_bitmap(in));
+        dst_bits = in->bitmap;
+    }
+    if (out) {
+        GG_CHECK(frontier_alloc_bins(out));
+        GG_CHECK(frontier_alloc_bitmap(out));
+        GG_CHECK(frontier_reset_counts(out));
+        A.out_bits = out->bitmap;
+        A.out_b0 = out->bins[0];
+        A.out_b1 = out->bins[1];
+        A.out_b2 = out->bins[2];
+        A.out_cnt = (unsigned long long *)out->d_cnt;
+    }
+    const uint64_t words = ((uint64_t)g->n + 31) / 32;
+    k_mis<<<persistent_grid(ctx, words), kBlock, 0, ctx->stream>>>(A, (uint8_t *)d->a->d, dst_bits);
+    GG_LAUNCHED(ctx);
+    if (out) {
+        out->all = false;
+        out->has_list = true;
+        out->has_bitmap = true;
+        out->host_valid = false;
+    }
+    return GG_OK;
+}
+
 gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_frontier *out,
                        gg_emap_stats *stats) {
     gg_ctx *ctx = g->ctx;
@@ -1085,6 +1185,14 @@ gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_f
             stats->nactv_in = g->n;
             stats->nacte_in = g->m;
             stats->scanned = g->m;
+        }
+        return GG_OK;
+    }
+    if (d->relax == GG_RELAX_MIS_U8) {
+        GG_CHECK(mis_relax(g, d, in, out));
+        if (stats) {
+            memset(stats, 0, sizeof(*stats));
+            stats->variant = GG_VAR_PULL_DENSE;
         }
         return GG_OK;
     }

@@ -21,9 +21,9 @@ GG_OK, GG_ERR_ARG, GG_ERR_OOM, GG_ERR_CUDA, GG_ERR_TIMEOUT, GG_ERR_UNSUPPORTED, 
     GG_ERR_STATE, GG_ERR_NOT_FOUND = range(9)
 I32, U32, F32, F64, BF16, F16, FP8E4M3, CFP_6_10, BF16_TRUNC, U8 = range(10)
 (RELAX_MIN_PLUS1_I32, RELAX_MIN_U32, RELAX_SETIF_U32, RELAX_ADD_GATHER, RELAX_NE_CHECK, RELAX_GAP_CHECK,
- RELAX_AHEAD_CHECK, RELAX_OR_U32) = range(8)
-FILTER_NONE, FILTER_GT_CONST, FILTER_NE_ZERO, FILTER_MSB_SET, FILTER_NE_CONST = range(5)
-RECORD_NONE, RECORD_REDUCTION, RECORD_NE_PREV = range(3)
+ RELAX_AHEAD_CHECK, RELAX_OR_U32, RELAX_MIS_U8) = range(9)
+FILTER_NONE, FILTER_GT_CONST, FILTER_NE_ZERO, FILTER_MSB_SET, FILTER_NE_CONST, FILTER_IN_FRONTIER = range(6)
+RECORD_NONE, RECORD_REDUCTION, RECORD_NE_PREV, RECORD_EQ_ZERO = range(4)
 THRESH_DEFAULT, THRESH_FRAC, THRESH_ALWAYS_SPARSE, THRESH_ALWAYS_DENSE, THRESH_LEARNED = range(5)
 VAR_AUTO, VAR_PUSH_SPARSE, VAR_PUSH_MERGE, VAR_PULL_DENSE, VAR_PUSH_DENSE, VAR_HOOK = -1, 0, 1, 2, 3, 4
 VARIANT_NAMES = {0: "push_sparse", 1: "push_merge", 2: "pull_dense", 3: "push_dense"}

@@ -187,8 +187,15 @@ typedef enum gg_relax_kind {
     GG_RELAX_GAP_CHECK = 5,     /* a[s] > a[d] + 1 || a[s] < a[d] - 1 on int32
                                                                       (BFSLVLv.C:288-294) */
     GG_RELAX_AHEAD_CHECK = 6,   /* a[s] < a[d] - 1 on int32          (BFSLVLv.C:299-305) */
-    GG_RELAX_OR_U32 = 7         /* a[d] |= src[s] on uint32 (another property as source;
+    GG_RELAX_OR_U32 = 7,        /* a[d] |= src[s] on uint32 (another property as source;
                                    FMv.C:356-358, its neighbourhood bit masks)          */
+    GG_RELAX_MIS_U8 = 8         /* maximal independent set states on uint8, 0 undecided,
+                                   1 conditionally in, 2 out, 3 in: over the in-edges
+                                   (s, d), s != d, d becomes out when some s is in, else
+                                   undecided when it is conditionally in and some s < d
+                                   is undecided or conditionally in (MISv.C:235-255,
+                                   dsl/ast/dfsaop.h:49-230).  Takes dst filter NONE or
+                                   IN_FRONTIER and record NONE or EQ_ZERO. */
 } gg_relax_kind;
 
 /* dst filters (api::filter(weak, dst, lambda), api.h:687-706). */
@@ -197,15 +204,18 @@ typedef enum gg_filter_kind {
     GG_FILTER_GT_CONST = 1, /* a[d] > _c(k)       (BFSLVLv.C:190-194) */
     GG_FILTER_NE_ZERO = 2,  /* a[d] != zero_val   (CCv.C:566-570)     */
     GG_FILTER_MSB_SET = 3,  /* msbset(a[d])       (BFSv.C:139-142)    */
-    GG_FILTER_NE_CONST = 4  /* a[d] != _c(k)      (FMv.C:353-354, k = _1s: all ones) */
+    GG_FILTER_NE_CONST = 4, /* a[d] != _c(k)      (FMv.C:353-354, k = _1s: all ones) */
+    GG_FILTER_IN_FRONTIER = 5 /* d in the input frontier, every source active
+                                 (api::filter(F, dst, strong), MISv.C:254)      */
 } gg_filter_kind;
 
 /* record (api::record, api.h:1450-1516). */
 typedef enum gg_record_kind {
     GG_RECORD_NONE = 0,      /* no output frontier (PRv) */
     GG_RECORD_REDUCTION = 1, /* vertices whose relax returned true */
-    GG_RECORD_NE_PREV = 2    /* method a[d] != prev[d]; prev[d] = a[d] afterwards
+    GG_RECORD_NE_PREV = 2,   /* method a[d] != prev[d]; prev[d] = a[d] afterwards
                                 (record(..., λd: a[d]!=prev[d]) + maintain_copies) */
+    GG_RECORD_EQ_ZERO = 3    /* method a[d] == 0 after the step (MISv.C:246-253) */
 } gg_record_kind;
 
 /* sparse/dense threshold (api.h:130-222) and the learned selector. */

@@ -76,6 +76,7 @@ inline uint64_t &device_epoch() {
 template <typename T> struct dtype_of;
 template <> struct dtype_of<int32_t> { static constexpr gg_dtype value = GG_I32; };
 template <> struct dtype_of<uint32_t> { static constexpr gg_dtype value = GG_U32; };
+template <> struct dtype_of<uint8_t> { static constexpr gg_dtype value = GG_U8; };
 template <> struct dtype_of<float> { static constexpr gg_dtype value = GG_F32; };
 template <> struct dtype_of<double> { static constexpr gg_dtype value = GG_F64; };
 
@@ -149,6 +150,7 @@ public:
     const VID *getEdges() const { return adj_.data(); }
     const VID *getDegree() const { graptor_b200::host_sync(); return deg_; }
     VID getDegree(VID v) const { graptor_b200::host_sync(); return deg_[v]; }
+    VID getNeighbor(VID v, VID i) const { return adj_[off_[v] + i]; }
     bool isSymmetric() const { return sym_; }
 
 private:
@@ -197,6 +199,10 @@ public:
     EID numEdges() const { return m_; }
     bool isSymmetric() const { return sym_ != 0; }
     const partitioner &get_partitioner() const { return part_; }
+    // the vector length the layout's pull traversal is built for: the device
+    // processes one destination per lane, so analytics see scalar code paths
+    static constexpr unsigned short getPullVLBound() { return 1; }
+    static constexpr unsigned short getPushVLBound() { return 1; }
     VID getOutDegree(VID v) const { return getCSR().getDegree(v); }
     // The CSR in host memory, fetched once on first use.
     const GraphCSxView &getCSR() const {
@@ -441,7 +447,7 @@ namespace expr {
 enum class NK {
     VarSrc, VarDst, VarV, VarEdge, Const, Ref, Min, SetIf, Assign, AddAssign, MulAssign,
     Add, Sub, Mul, Div, Eq, Ne, Lt, Gt, Le, Ge, LAnd, LOr, Cast, Abs, Iif, MsbSet, Noop,
-    OrAssign, BAnd, BOr, BXor, BNot, Let, Tmp, Seq
+    OrAssign, BAnd, BOr, BXor, BNot, Let, Tmp, Seq, SetMask, MisOp
 };
 
 struct Node {
@@ -466,7 +472,7 @@ inline std::string show(const NP &n) {
     static const char *nm[] = {"s", "d", "v", "e", "const", "ref", "min", "setif", "=", "+=", "*=",
                                "+", "-", "*", "/", "==", "!=", "<", ">", "<=", ">=", "&&", "||",
                                "cast", "abs", "iif", "msbset", "noop", "|=", "&", "|", "^", "~", "let", "tmp",
-                               "seq"};
+                               "seq", "setmask", "mis"};
     std::ostringstream os;
     if (n->k == NK::Const) return (os << n->cval, os.str());
     os << nm[(int)n->k];
@@ -485,6 +491,8 @@ inline E make_noop();
 // An expression value.  Copying an E copies the handle, not the tree.
 class E {
 public:
+    // one lane per expression value (the reference's vector length)
+    static constexpr unsigned short VL = 1;
     E() : n_(mk(NK::Noop)) {}
     explicit E(NP n) : n_(std::move(n)) {}
     template <typename T, typename = std::enable_if_t<std::is_arithmetic<T>::value>>
@@ -629,6 +637,28 @@ template <auto AID, typename Fn> inline E let(const E &init, Fn cont) {
     n->dt = body.node()->dt;
     return E(n);
 }
+// set_mask(c, x): x where c holds (dsl/ast/ctrl.h); remove_mask(x): x
+inline E set_mask(const E &c, const E &x) {
+    auto n = mk(NK::SetMask, {c.node(), x.node()});
+    n->dt = x.node()->dt;
+    return E(n);
+}
+inline E remove_mask(const E &x) { return x; }
+template <typename Tr> inline E make_unop_cvt_to_mask(const E &x) { return x; }
+// The maximal independent set relation (dsl/ast/dfsaop.h:49-230): state
+// a[d], update a[s], condition s < d.
+struct dfsaop_MIS {
+    enum mis_state_t { mis_undecided = 0, mis_conditionally_in = 1, mis_out = 2, mis_in = 3 };
+};
+inline E make_dfsaop_MIS(const E &state, const E &update, const E &cond) {
+    auto n = mk(NK::MisOp, {state.node(), update.node(), cond.node()});
+    n->dt = state.node()->dt;
+    return E(n);
+}
+// value<Tr, vk_zero>(): zero in Tr's element type (dsl/ast/value.h)
+struct vk_zero {};
+template <typename Tr, typename K> inline E value();
+
 // make_seq(a, b, ...): the statements in order (dsl/ast/binop.h:370-395)
 inline E make_seq() { return make_noop(); }
 template <typename... R> inline E make_seq(const E &a, const R &... r) {
@@ -655,12 +685,44 @@ inline E ref(gg_prop *p, double *host, gg_dtype dt, const E &idx) {
 
 }  // namespace expr
 
+// Vector type traits the analytics name in their lambdas (simd/ types):
+// one lane on the device.
+namespace simd {
+template <typename T, unsigned short VL_> struct ty {
+    using member_type = T;
+    static constexpr unsigned short VL = VL_;
+};
+namespace detail {
+template <typename T, unsigned short VL_> using mask_preferred_traits_type = ty<T, VL_>;
+}  // namespace detail
+}  // namespace simd
+
 // Storage encodings (encoding.h / customfp.h types): the 16-bit formats are
 // two-byte words here, used as storage types and template tags.
 template <unsigned short E_, unsigned short M_> struct customfp { uint16_t bits; };
 template <bool S_, unsigned short E_, unsigned short M_, bool Z_, int B_> struct scustomfp { uint16_t bits; };
 template <typename T> struct array_encoding { using stored_type = T; };
 template <typename T, bool = false> struct array_encoding_wide { using stored_type = T; };
+// bitfield<B> / array_encoding_bit<B> (encoding.h:453-520): B-bit states.  On
+// the device each state takes one byte; host reads give a bitfield value.
+template <unsigned short B> struct bitfield {
+    uint8_t v;
+    uint8_t get() const { return v; }
+    operator uint8_t() const { return v; }
+};
+template <typename T> class mmap_ptr;
+struct numa_allocation_partitioned;
+template <unsigned short B> struct array_encoding_bit {
+    static constexpr unsigned short bits = B;
+    using stored_type = uint8_t;
+    using storage_type = uint8_t;
+    static mmap_ptr<uint8_t> allocate(const numa_allocation_partitioned &a);
+    static bitfield<B> get(const uint8_t *base, VID v);
+};
+template <typename Enc> struct is_bit_encoding : std::false_type { static constexpr unsigned short bits = 0; };
+template <unsigned short B> struct is_bit_encoding<array_encoding_bit<B>> : std::true_type {
+    static constexpr unsigned short bits = B;
+};
 
 namespace graptor_b200 {
 template <> struct dtype_of<customfp<6, 10>> { static constexpr gg_dtype value = GG_CFP_6_10; };
@@ -691,15 +753,26 @@ public:
     }
     E operator[](const E &i) const { return ref(prop_, host_, graptor_b200::dtype_of<T>::value, i); }
     // host writes need no flush: the next kernel, queued after them, sees them
-    storage_type &operator[](VID v) {
+    // (states of a bit encoding are read on the host as bitfield values)
+    using host_ref = std::conditional_t<is_bit_encoding<Enc>::value, bitfield<is_bit_encoding<Enc>::bits>,
+                                        storage_type &>;
+    using host_cref = std::conditional_t<is_bit_encoding<Enc>::value, bitfield<is_bit_encoding<Enc>::bits>,
+                                         const storage_type &>;
+    host_ref operator[](VID v) {
         graptor_b200::host_sync();
-        return ptr_[v];
+        if constexpr (is_bit_encoding<Enc>::value) return host_ref{ptr_[v]};
+        else return ptr_[v];
     }
-    const storage_type &operator[](VID v) const {
+    host_cref operator[](VID v) const {
         graptor_b200::host_sync();
-        return ptr_[v];
+        if constexpr (is_bit_encoding<Enc>::value) return host_cref{ptr_[v]};
+        else return ptr_[v];
     }
     storage_type *ptr() const { return ptr_; }
+    // the same array viewed as its stored type (dsl/ast/memref.h:95-106)
+    array_ro<typename Enc::stored_type, U, AID, Enc> observe_stored() const {
+        return array_ro<typename Enc::stored_type, U, AID, Enc>(ptr_);
+    }
 
 private:
     storage_type *ptr_ = nullptr;
@@ -812,6 +885,23 @@ private:
     gg_prop *p_ = nullptr;
     T *d_ = nullptr;
 };
+
+template <unsigned short B> mmap_ptr<uint8_t> array_encoding_bit<B>::allocate(const numa_allocation_partitioned &a) {
+    mmap_ptr<uint8_t> p;
+    p.allocate(a);
+    return p;
+}
+template <unsigned short B> bitfield<B> array_encoding_bit<B>::get(const uint8_t *base, VID v) {
+    graptor_b200::host_sync();
+    return bitfield<B>{base[v]};
+}
+
+namespace expr {
+template <typename Tr, typename K> inline E value() {
+    static_assert(std::is_same<K, vk_zero>::value, "only the zero value kind");
+    return cst(0, graptor_b200::dtype_of<typename Tr::member_type>::value);
+}
+}  // namespace expr
 
 namespace api {
 
@@ -933,11 +1023,26 @@ template <typename Fn> arg_relax<Fn> relax(Fn fn) { return arg_relax<Fn>{fn}; }
 template <typename Fn> struct arg_fusion { Fn fn; };
 template <typename Fn> arg_fusion<Fn> fusion(Fn fn) { return arg_fusion<Fn>{fn}; }
 
-struct arg_filter_src { frontier *F; bool strong; };
+// A frontier filter: on sources (the input frontier), or on destinations
+// (api::filter(F, dst, strong), MISv.C:254: every source active).  The
+// reference takes the three arguments in any order.
+struct arg_filter_src { frontier *F; bool strong; bool dst; };
 template <typename Fn> struct arg_filter_dst { Fn fn; bool strong; };
-template <filter_strength S>
-arg_filter_src filter(filter_strength_argument<S>, filter_entity_argument<filter_entity::src>, frontier &F) {
-    return arg_filter_src{&F, S == filter_strength::strong};
+template <filter_strength S, filter_entity E_>
+arg_filter_src filter(filter_strength_argument<S>, filter_entity_argument<E_>, frontier &F) {
+    return arg_filter_src{&F, S == filter_strength::strong, E_ == filter_entity::dst};
+}
+template <filter_strength S, filter_entity E_>
+arg_filter_src filter(frontier &F, filter_strength_argument<S>, filter_entity_argument<E_>) {
+    return arg_filter_src{&F, S == filter_strength::strong, E_ == filter_entity::dst};
+}
+template <filter_strength S, filter_entity E_>
+arg_filter_src filter(frontier &F, filter_entity_argument<E_>, filter_strength_argument<S>) {
+    return arg_filter_src{&F, S == filter_strength::strong, E_ == filter_entity::dst};
+}
+template <filter_strength S, filter_entity E_>
+arg_filter_src filter(filter_entity_argument<E_>, filter_strength_argument<S>, frontier &F) {
+    return arg_filter_src{&F, S == filter_strength::strong, E_ == filter_entity::dst};
 }
 template <filter_strength S, typename Fn>
 arg_filter_dst<Fn> filter(filter_strength_argument<S>, filter_entity_argument<filter_entity::dst>, Fn fn) {
@@ -1038,6 +1143,18 @@ inline void lower_relax(const NP &r, gg_emap_desc &d) {
             return;
         }
     }
+    // set_mask(s != d, make_dfsaop_MIS(a[d], a[s], s < d)) on uint8 states (MISv.C:235-245)
+    if (r->k == NK::SetMask && r->c[0]->k == NK::Ne && r->c[0]->c[0]->k == NK::VarSrc &&
+        r->c[0]->c[1]->k == NK::VarDst && r->c[1]->k == NK::MisOp) {
+        const NP &op = r->c[1];
+        if (is_ref_at(op->c[0], NK::VarDst) && is_ref_at(op->c[1], NK::VarSrc) && op->c[0]->prop == op->c[1]->prop &&
+            op->c[0]->dt == GG_U8 && op->c[2]->k == NK::Lt && op->c[2]->c[0]->k == NK::VarSrc &&
+            op->c[2]->c[1]->k == NK::VarDst) {
+            d.relax = GG_RELAX_MIS_U8;
+            d.a = op->c[0]->prop;
+            return;
+        }
+    }
     if (r->k == NK::OrAssign && is_ref_at(r->c[0], NK::VarDst) && is_ref_at(r->c[1], NK::VarSrc) &&
         r->c[0]->dt == GG_U32 && r->c[1]->dt == GG_U32) {
         d.relax = GG_RELAX_OR_U32;  // a[d] |= b[s] (FMv.C:356-358)
@@ -1090,6 +1207,10 @@ inline void lower_dst_filter(const NP &f, gg_emap_desc &d) {
 }
 
 inline void lower_record_method(const NP &m, gg_emap_desc &d) {
+    if (m->k == NK::Eq && is_ref_at(m->c[0], NK::VarDst) && is_const(m->c[1], 0)) {
+        d.record = GG_RECORD_EQ_ZERO;  // a[d] == 0 (MISv.C:246-253)
+        return;
+    }
     if (m->k == NK::Ne && is_ref_at(m->c[0], NK::VarDst) && is_ref_at(m->c[1], NK::VarDst)) {
         d.record = GG_RECORD_NE_PREV;  // a[d] != prev[d]
         d.prev = m->c[1]->prop;
@@ -1335,7 +1456,8 @@ inline void emap_arg(emap_state &s, const arg_config &c) {
 }
 inline void emap_arg(emap_state &s, const arg_filter_src &f) {
     s.in = f.F;
-    s.d.src_strong = f.strong;
+    if (f.dst) s.d.dst_filter = GG_FILTER_IN_FRONTIER;
+    else s.d.src_strong = f.strong;
 }
 template <typename Fn> void emap_arg(emap_state &s, const arg_filter_dst<Fn> &f) {
     graptor_b200::lower_dst_filter(f.fn(expr::var(expr::NK::VarDst)).node(), s.d);

@@ -7,7 +7,7 @@
 // the same GraphVEBOGraptor<GRAPTOR_MODE_MACRO(1,0,1)> layout the reference
 // driver builds (bench/driver.C:70-75, 110-116), runs FMv::run() once with
 // -itimes, and reports
-//   * "n <file n> padded <layout n> iters <k> deffG <x>";
+//   * "n <file n> padded <layout n> iters <k> deffG <x> time_s <run() seconds>";
 //   * "nactv <|F| of iteration 0> <|F| of iteration 1> ..." (FMv.C:416-425);
 //   * <prefix>.mask: the final bit mask per vertex, in ORIGINAL order (uint32);
 //   * <prefix>.remap: the layout id of each original vertex (uint32): FMv
@@ -16,6 +16,7 @@
 // Usage: ref_fm <graph.bin> <out_prefix>
 #include "graptor/graptor.h"
 #include "graptor/api.h"
+#include <chrono>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -42,9 +43,11 @@ int main(int argc, char **argv) {
     char *cargv[] = {a0, a1, nullptr};
     commandLine P(2, cargv, "");
     FMv<HarnessGraph> problem(PG, P);
+    auto t0 = std::chrono::steady_clock::now();
     problem.run();
-    std::printf("n %u padded %u iters %d deffG %.9g\n", (unsigned)n, (unsigned)PG.numVertices(), problem.iter,
-                (double)problem.deffG);
+    const double sec = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::printf("n %u padded %u iters %d deffG %.9g time_s %.6f\n", (unsigned)n, (unsigned)PG.numVertices(),
+                problem.iter, (double)problem.deffG, sec);
     std::printf("nactv");
     for (int i = 0; i < problem.iter; ++i) std::printf(" %llu", (unsigned long long)problem.info_buf[i].nactv);
     std::printf("\n");

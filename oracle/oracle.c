@@ -870,3 +870,34 @@ ORC_API float orc_fm_deffg(const float *nhm, int iters) {
     if (nh == nhm1) return 1.0f;
     return (float)(i + (0.9 * nmax - nhm1) / (nh - nhm1));
 }
+
+/* ---------------------------------------------------------------------------
+ * Maximal independent set (reference: bench/MISv.C:165-300 with the
+ * dfsaop_MIS relation, dsl/ast/dfsaop.h:49-230).  MISv's rounds settle on the
+ * greedy set in priority order: a vertex is in (3) when no neighbour of
+ * lower priority is in, else out (2); self loops are ignored.  prio[v] is the
+ * vertex's rank (MISv compares vertex ids: the file's ids on the device, the
+ * layout's ids in the reference build).  Returns the number of vertices in,
+ * or -1 on an allocation failure.
+ * ------------------------------------------------------------------------ */
+ORC_API int64_t orc_mis(uint32_t n, const uint64_t *off, const uint32_t *adj, const uint32_t *prio,
+                        uint8_t *state) {
+    uint32_t *order = (uint32_t *)malloc((size_t)(n ? n : 1) * sizeof(uint32_t));
+    if (!order) return -1;
+    for (uint32_t v = 0; v < n; ++v) { order[v] = 0xFFFFFFFFu; state[v] = 0; }
+    for (uint32_t v = 0; v < n; ++v) {
+        if (prio[v] >= n || order[prio[v]] != 0xFFFFFFFFu) { free(order); return -1; }  /* not a permutation */
+        order[prio[v]] = v;
+    }
+    int64_t in = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const uint32_t v = order[i];
+        int blocked = 0;
+        for (uint64_t e = off[v]; e < off[v + 1] && !blocked; ++e)
+            blocked = adj[e] != v && state[adj[e]] == 3;
+        state[v] = blocked ? 2 : 3;
+        in += !blocked;
+    }
+    free(order);
+    return in;
+}

@@ -70,6 +70,8 @@ def lib() -> C.CDLL:
                              C.c_void_p, C.c_int]
         L.orc_fm_deffg.argtypes = [C.c_void_p, C.c_int]
         L.orc_fm_deffg.restype = C.c_float
+        L.orc_mis.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_mis.restype = C.c_int64
         L.orc_free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
@@ -306,6 +308,24 @@ def ref_fm(bin_path: str, out_prefix: str, threads: int | None = None):
     mask = np.fromfile(out_prefix + ".mask", dtype=np.uint32)
     remap = np.fromfile(out_prefix + ".remap", dtype=np.uint32)
     return mask, remap, int(w[5]), float(w[7]), np.array([int(x) for x in nact], dtype=np.uint64), int(w[3])
+
+
+def mis(g: Graph, prio: np.ndarray | None = None) -> np.ndarray:
+    """MISv's final states (2 out, 3 in): the greedy independent set in
+    priority order (vertex ids when prio is None; oracle.c orc_mis)."""
+    prio = np.arange(g.n, dtype=np.uint32) if prio is None else np.ascontiguousarray(prio, dtype=np.uint32)
+    st = np.empty(max(g.n, 1), dtype=np.uint8)
+    if lib().orc_mis(g.n, _p(g.off), _p(g.adj), _p(prio), _p(st)) < 0:
+        raise RuntimeError("orc_mis failed (allocation, or prio not a permutation)")
+    return st[:g.n]
+
+
+def ref_mis(bin_path: str, out_path: str, threads: int | None = None):
+    """The reference MISv run by oracle/harness/ref_mis.C: returns (states in
+    original order, layout id of each vertex, iterations)."""
+    txt = _run([ref_prog("ref_mis"), bin_path, out_path], threads)
+    w = next(l for l in txt.splitlines() if l.startswith("n ")).split()
+    return np.fromfile(out_path, dtype=np.uint8), np.fromfile(out_path + ".remap", dtype=np.uint32), int(w[5])
 
 
 def ref_variant() -> str:

@@ -147,6 +147,22 @@ int main() {
             CHECK(red == want - 5.0);
         }
     }
+    // MISv.C:235-256: the MIS relation, record a[d] == 0, frontier on destinations
+    {
+        E rel = set_mask(var(S) != var(D),
+                         make_dfsaop_MIS(at(7, GG_U8, D), at(7, GG_U8, S), make_unop_cvt_to_mask<int>(var(S) < var(D))));
+        gg_emap_desc d = relax_of(rel);
+        CHECK(d.relax == GG_RELAX_MIS_U8 && d.a == P(7));
+        graptor_b200::lower_record_method((at(7, GG_U8, D) == value<simd::ty<uint8_t, 1>, vk_zero>()).node(), d);
+        CHECK(d.record == GG_RECORD_EQ_ZERO);
+        frontier F;
+        api::emap_state st;
+        api::emap_arg(st, api::filter(F, api::dst, api::strong));
+        CHECK(st.in == &F && st.d.dst_filter == GG_FILTER_IN_FRONTIER);
+        api::emap_state st2;
+        api::emap_arg(st2, api::filter(F, api::strong, api::src));
+        CHECK(st2.in == &F && st2.d.dst_filter == GG_FILTER_NONE && st2.d.src_strong == 1);
+    }
     if (fails) return 1;
     std::printf("ok\n");
     return 0;

@@ -17,6 +17,9 @@ programs on it, compiled from the reference sources by oracle/Makefile:
                  iteration count, deffG and the frontier size per iteration
                  (fm_nactv; the first counts the layout's padding vertices,
                  fm_padded in all)
+  mis_state    - MISv.C run by oracle/harness/ref_mis.C: the final state of
+                 each vertex (2 out, 3 in), with mis_remap the layout id of
+                 each vertex (MISv's priorities)
 customfp_sweep.npz holds float bit patterns and, per pattern, the codes and
 decoded floats of the reference's customfp<6,10> and scustomfp<true,8,7>
 conversions (harness oracle/harness/ref_cfp.C).
@@ -26,6 +29,7 @@ The config-1 workload (R-MAT scale 16, 2^20 edges) is stored without its CSR
 Run (needs the reference tree and `make -C oracle ref`):
     python tests/golden/make_golden.py            # every fixture
     python tests/golden/make_golden.py --fm-only  # add / refresh the fm_* keys only
+    python tests/golden/make_golden.py --mis-only # add / refresh the mis_* keys only
 """
 import hashlib
 import os
@@ -86,7 +90,15 @@ def fm_reference(g, tmp):
                 fm_nactv=nactv, fm_padded=np.int64(padded))
 
 
-def add_fm(name, tmp):
+def mis_reference(g, tmp):
+    p = os.path.join(tmp, "g.bin")
+    O.write_bin(g, p)
+    st, remap, _ = O.ref_mis(p, os.path.join(tmp, "mis"))
+    assert np.array_equal(st, O.mis(g, remap))  # the restatement must agree
+    return dict(mis_state=st, mis_remap=remap)
+
+
+def add_keys(name, tmp, fn):
     path = os.path.join(HERE, name + ".npz")
     d = dict(np.load(path))
     if "off" in d:
@@ -94,14 +106,16 @@ def add_fm(name, tmp):
     else:
         g = O.rmat(int(d["scale"]), int(d["nedges"]), seed=int(d["seed"]))
         assert csr_sha256(g.off, g.adj) == str(d["sha256"]), name
-    d.update(fm_reference(g, tmp))
+    new = fn(g, tmp)
+    d.update(new)
     np.savez_compressed(path, **d)
-    print(name, "fm iters", int(d["fm_iters"]), "deffG", float(d["fm_deffg"]))
+    print(name, sorted(new))
 
 
 def save(name, g, roots, pr_iters, tmp, store_csr=True, params=None):
     levels, parents, cc, pr, vary = run_reference(g, roots, pr_iters, tmp)
     vary.update(fm_reference(g, tmp))
+    vary.update(mis_reference(g, tmp))
     # sanity: the restatement must agree before a fixture is written
     for r, l in zip(roots, levels):
         assert np.array_equal(O.bfs_level(g, r), l), name
@@ -140,11 +154,13 @@ def main():
     if not O.ref_available("ref_bfslvl"):
         raise SystemExit("reference build missing: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
-        if "--fm-only" in sys.argv:
-            for name in ["rmat10_ef8", "rmat12_ef16", "grid20x32_del5pct", "er2000_deg6", "edgecases32",
-                         "config1_rmat16"]:
-                add_fm(name, tmp)
-            return
+        only = {"--fm-only": fm_reference, "--mis-only": mis_reference}
+        for flag, fn in only.items():
+            if flag in sys.argv:
+                for name in ["rmat10_ef8", "rmat12_ef16", "grid20x32_del5pct", "er2000_deg6", "edgecases32",
+                             "config1_rmat16"]:
+                    add_keys(name, tmp, fn)
+                return
         save_customfp_sweep(tmp)
         g = O.rmat(10, 8 << 10, seed=11)
         save("rmat10_ef8", g, roots_for(g, 3, 1), 20, tmp)

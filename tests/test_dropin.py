@@ -164,3 +164,23 @@ def test_reference_fmv_with_its_driver(tmp_path):
     got = [float(l.split("deffG:")[1]) for l in r.stderr.splitlines() if l.startswith("deffG:")]
     _, _, _, dg = O.fm(g, O.fm_draws(g.n))
     assert len(got) == 2 and all(abs(x - dg) <= 1e-4 * max(1.0, abs(dg)) for x in got), (got, dg)
+
+
+@pytest.mark.parametrize("name", _golden_graphs())
+def test_reference_misv_source_on_gpu(tmp_path, name):
+    """MISv.C run on the GPU by the mis harness: its own validate() passes
+    and the states equal the oracle's greedy set in vertex-id order (the
+    oracle is pinned to the reference build with the reference's priorities)."""
+    z, g, p = _graph_file(tmp_path, name)
+    out = str(tmp_path / "mis.u8")
+    r = subprocess.run([_prog("mis"), p, out], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "result: PASS" in r.stderr, r.stderr[-2000:]
+    assert np.array_equal(np.fromfile(out, dtype=np.uint8), O.mis(g))
+
+
+def test_reference_misv_with_its_driver(tmp_path):
+    """MISv.C with the reference's driver main(): validate() passes in each round."""
+    z, g, p = _graph_file(tmp_path, "rmat12_ef16")
+    r = _driver("MISv", ["-s", "-b", "-rounds", "2", p])
+    assert r.stderr.count("result: PASS") == 2, r.stderr[-2000:]
