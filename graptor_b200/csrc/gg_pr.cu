@@ -693,14 +693,79 @@ static gg_status gather_api(gg_graph *g, const gg_emap_desc *d) {
     return gather_launch<DT, false, true>(g, (const T *)d->src->d, yf, yd, nullptr, sc, partial);
 }
 
+// ADD_GATHER with a source frontier (APRv.C:477-487, api::filter(F, strong,
+// src)): y[d] += sum over in-edges (s, d) with s in F of contrib[s].  A warp
+// per 32-vertex word walks the word's rows one after the other, the lanes
+// striding each row and testing the frontier bitmap; rows without an active
+// source keep y.  Float sums (APRv's FloatTy) or double sums (accum_f64).
+template <typename T, typename Acc>
+__global__ void __launch_bounds__(256)
+k_gather_src_bits(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj,
+                  const T *__restrict__ contrib, const uint32_t *__restrict__ bits, uint32_t n,
+                  float *__restrict__ y_f32, double *__restrict__ y_f64) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t nwords = (n + 31u) >> 5;
+    const uint32_t nw = (gridDim.x * 256u) >> 5;
+    for (uint32_t w = (blockIdx.x * 256u + threadIdx.x) >> 5; w < nwords; w += nw) {
+        Acc mine = 0;
+        bool any_mine = false;
+        for (uint32_t j = 0; j < 32; ++j) {
+            const uint32_t d = (w << 5) + j;
+            if (d >= n) break;
+            const uint64_t beg = in_off[d], end = in_off[d + 1];
+            Acc part = 0;
+            bool any = false;
+            for (uint64_t e = beg + lane; e < end; e += 32) {
+                const uint32_t s = __ldg(in_adj + e);
+                if (dev::bit_test(bits, s)) {
+                    part += (Acc)contrib[s];
+                    any = true;
+                }
+            }
+            part = dev::warp_sum(part);
+            any = __any_sync(FULL, any);
+            if (lane == j) {
+                mine = part;
+                any_mine = any;
+            }
+        }
+        const uint32_t d = (w << 5) + lane;
+        if (d < n && any_mine) {
+            if (y_f64) y_f64[d] += (double)mine;
+            else y_f32[d] = (float)((double)y_f32[d] + (double)mine);
+        }
+    }
+}
+
+static gg_status gather_src_filtered(gg_graph *g, const gg_emap_desc *d, gg_frontier *in) {
+    gg_ctx *ctx = g->ctx;
+    GG_CHECK(frontier_ensure_bitmap(in));
+    float *yf = d->a->t == GG_F32 ? (float *)d->a->d : nullptr;
+    double *yd = d->a->t == GG_F64 ? (double *)d->a->d : nullptr;
+    const unsigned grid = pr_grid(ctx, g->n);
+    if (d->src->t == GG_F32 && !d->accum_f64)
+        k_gather_src_bits<float, float><<<grid, 256, 0, ctx->stream>>>(g->in_off, g->in_adj, (const float *)d->src->d,
+                                                                     in->bitmap, g->n, yf, yd);
+    else if (d->src->t == GG_F32)
+        k_gather_src_bits<float, double><<<grid, 256, 0, ctx->stream>>>(g->in_off, g->in_adj, (const float *)d->src->d,
+                                                                      in->bitmap, g->n, yf, yd);
+    else if (d->src->t == GG_F64 && d->accum_f64)
+        k_gather_src_bits<double, double><<<grid, 256, 0, ctx->stream>>>(
+            g->in_off, g->in_adj, (const double *)d->src->d, in->bitmap, g->n, yf, yd);
+    else
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "a source-filtered ADD_GATHER takes F32 or F64 contributions");
+    GG_LAUNCHED(ctx);
+    return GG_OK;
+}
+
 gg_status pr_edgemap_gather(gg_graph *g, const gg_emap_desc *d, gg_frontier *in) {
     gg_ctx *ctx = g->ctx;
-    if (in && !in->all) return set_error(ctx, GG_ERR_UNSUPPORTED, "ADD_GATHER runs over all vertices (no src filter)");
     if (!d->src || d->src->g != g) return set_error(ctx, GG_ERR_ARG, "ADD_GATHER needs a contribution property of g");
     if (d->a->t != GG_F32 && d->a->t != GG_F64) return set_error(ctx, GG_ERR_ARG, "ADD_GATHER accumulator must be F32 or F64");
     if (d->dst_filter != GG_FILTER_NONE) return set_error(ctx, GG_ERR_UNSUPPORTED, "ADD_GATHER takes no dst filter");
     if (d->src_scale != 0.0f && d->src->t != GG_FP8E4M3)
         return set_error(ctx, GG_ERR_UNSUPPORTED, "src_scale applies to FP8 contributions only");
+    if (in && !in->all) return gather_src_filtered(g, d, in);
     switch (d->src->t) {
     case GG_F32: return gather_api<GG_F32>(g, d);
     case GG_BF16: return gather_api<GG_BF16>(g, d);

@@ -129,6 +129,8 @@ public:
         return p;
     }
     VID get_scale() const { return scale_; }
+    // the vertex range of partition k (one partition: [0, n))
+    VID start_of(int k) const { return k <= 0 ? 0 : n_; }
     gg_graph *graph() const { return g_; }
 
 private:
@@ -269,6 +271,12 @@ private:
 
 // A W-byte truth value (Graptor's logical<W>, all bits set = true).
 template <unsigned short W> struct logical { unsigned char b[W]; };
+// add_logical<T>::type: the logical of T's width (simd/ types)
+template <typename T> struct add_logical { using type = logical<sizeof(T)>; };
+namespace graptor_b200 {
+template <> struct dtype_of<logical<4>> { static constexpr gg_dtype value = GG_U32; };
+template <> struct dtype_of<logical<1>> { static constexpr gg_dtype value = GG_U8; };
+}  // namespace graptor_b200
 
 // ---------------------------------------------------------------------------
 // Frontier (value handle with manual del(), frontier/frontier.h:58-716)
@@ -319,10 +327,53 @@ public:
         return f;
     }
     static frontier empty() { return frontier(); }
+    // frontier::dense<W>(part) (frontier.h): one W-byte logical per vertex
+    // in device memory, all clear, for vertex programs to write (all bits set
+    // = active, APRv.C:365-367); calculateActiveCounts() makes it the
+    // frontier's active set.  The array lives until del().
+    template <unsigned short W> static frontier dense(const partitioner &part) {
+        static_assert(W == 1 || W == 4, "dense logical frontiers of 1 or 4 bytes");
+        frontier f;
+        f.kind_ = K_DENSE;
+        f.n_ = part.get_num_vertices();
+        gg_prop *p = nullptr;
+        graptor_b200::check(gg_prop_create_managed(part.graph(), W == 4 ? GG_U32 : GG_U8, &p),
+                            "gg_prop_create_managed");
+        const uint32_t zero = 0;
+        graptor_b200::check(gg_prop_fill(p, &zero), "gg_prop_fill");
+        void *d = nullptr;
+        gg_prop_device_ptr(p, &d);
+        graptor_b200::registry()[d] = p;
+        f.dense_store_ = std::shared_ptr<gg_prop>(p, [d](gg_prop *q) {
+            graptor_b200::registry().erase(d);
+            gg_prop_destroy(q);
+        });
+        return f;
+    }
+    // the dense array of a frontier made by dense<W>()
+    template <typename T> T *getDense() const {
+        if (!dense_store_) throw graptor_b200::error(GG_ERR_STATE, "getDense() of a frontier without a dense array");
+        void *d = nullptr;
+        gg_prop_device_ptr(dense_store_.get(), &d);
+        return (T *)d;
+    }
+    // the active set and its counts from the dense array (frontier.h:380-383)
+    template <typename GraphType> void calculateActiveCounts(const GraphType &G) {
+        if (!dense_store_) throw graptor_b200::error(GG_ERR_STATE, "calculateActiveCounts() without a dense array");
+        gg_vmap_desc d;
+        std::memset(&d, 0, sizeof(d));
+        const uint8_t code[] = {GG_VM_LOAD, GG_VM_CONST, GG_VM_NE, GG_VM_FILTER};
+        d.ncode = 4;
+        for (int i = 0; i < 4; ++i) d.code[i] = code[i];
+        d.props[0] = dense_store_.get();
+        double red[GG_VM_MAX_REDUCE] = {0, 0, 0, 0};
+        graptor_b200::check(gg_vertexmap(G.handle(), &d, nullptr, output(G.handle()), red), "gg_vertexmap");
+    }
     void del() {
         if (f_) gg_frontier_destroy(f_);
         f_ = nullptr;
         kind_ = K_EMPTY;
+        dense_store_.reset();
     }
     bool isEmpty() const {
         if (kind_ == K_LIST) return list_->empty();
@@ -338,7 +389,7 @@ public:
         refresh();
         return nacte_;
     }
-    float density(EID m) const { return m ? float(double(nActiveVertices() + nActiveEdges()) / double(m)) : 0.f; }
+    double density(EID m) const { return m ? (double(nActiveVertices()) + double(nActiveEdges())) / double(m) : 0.0; }
     frontier_type getType() const {
         return kind_ == K_ALL ? frontier_type::ft_true : kind_ == K_DEV ? frontier_type::ft_sparse
                                                                        : frontier_type::ft_unbacked;
@@ -413,7 +464,7 @@ public:
     bool all() const { return kind_ == K_ALL; }
 
 private:
-    enum Kind { K_EMPTY, K_SINGLE, K_ALL, K_DEV, K_LIST };
+    enum Kind { K_EMPTY, K_SINGLE, K_ALL, K_DEV, K_LIST, K_DENSE };
     VID frontier_vertices() const {
         uint32_t n = 0;
         graptor_b200::check(gg_graph_info(graptor_b200::default_graph(), &n, nullptr, nullptr), "gg_graph_info");
@@ -437,6 +488,7 @@ private:
     std::shared_ptr<std::vector<VID>> list_;                 // K_LIST: pending host list
     mutable std::shared_ptr<std::vector<VID>> host_;         // getSparse() copy
     mutable std::shared_ptr<std::vector<int64_t>> dense_;    // getDenseL() copy
+    std::shared_ptr<gg_prop> dense_store_;                   // dense<W>() array
 };
 
 // ---------------------------------------------------------------------------
@@ -447,7 +499,7 @@ namespace expr {
 enum class NK {
     VarSrc, VarDst, VarV, VarEdge, Const, Ref, Min, SetIf, Assign, AddAssign, MulAssign,
     Add, Sub, Mul, Div, Eq, Ne, Lt, Gt, Le, Ge, LAnd, LOr, Cast, Abs, Iif, MsbSet, Noop,
-    OrAssign, BAnd, BOr, BXor, BNot, Let, Tmp, Seq, SetMask, MisOp
+    OrAssign, BAnd, BOr, BXor, BNot, Let, Tmp, Seq, SetMask, MisOp, Pred, CvtVec
 };
 
 struct Node {
@@ -472,7 +524,7 @@ inline std::string show(const NP &n) {
     static const char *nm[] = {"s", "d", "v", "e", "const", "ref", "min", "setif", "=", "+=", "*=",
                                "+", "-", "*", "/", "==", "!=", "<", ">", "<=", ">=", "&&", "||",
                                "cast", "abs", "iif", "msbset", "noop", "|=", "&", "|", "^", "~", "let", "tmp",
-                               "seq", "setmask", "mis"};
+                               "seq", "setmask", "mis", "pred", "cvtvec"};
     std::ostringstream os;
     if (n->k == NK::Const) return (os << n->cval, os.str());
     os << nm[(int)n->k];
@@ -644,6 +696,13 @@ inline E set_mask(const E &c, const E &x) {
     return E(n);
 }
 inline E remove_mask(const E &x) { return x; }
+// add_predicate(x, c): x where c holds; an update with it leaves the other
+// vertices untouched (APRv.C:455-458)
+inline E add_predicate(const E &x, const E &c) {
+    auto n = mk(NK::Pred, {x.node(), c.node()});
+    n->dt = x.node()->dt;
+    return E(n);
+}
 template <typename Tr> inline E make_unop_cvt_to_mask(const E &x) { return x; }
 // The maximal independent set relation (dsl/ast/dfsaop.h:49-230): state
 // a[d], update a[s], condition s < d.
@@ -857,7 +916,10 @@ public:
         graptor_b200::host_sync();
         return d_;
     }
-    operator T *() { return d_; }
+    operator T *() {
+        graptor_b200::host_sync();
+        return d_;
+    }
     operator const T *() const { return d_; }
     explicit operator bool() const { return d_ != nullptr; }
     // host writes need no flush: the next kernel, queued after them, sees them
@@ -897,6 +959,13 @@ template <unsigned short B> bitfield<B> array_encoding_bit<B>::get(const uint8_t
 }
 
 namespace expr {
+// make_unop_cvt_to_vector<logical<W>>(c): c as a W-byte logical, all bits
+// set where c holds (APRv.C:411-415)
+template <typename T> inline E make_unop_cvt_to_vector(const E &c) {
+    auto n = mk(NK::CvtVec, {c.node()});
+    n->dt = graptor_b200::dtype_of<T>::value;
+    return E(n);
+}
 template <typename Tr, typename K> inline E value() {
     static_assert(std::is_same<K, vk_zero>::value, "only the zero value kind");
     return cst(0, graptor_b200::dtype_of<typename Tr::member_type>::value);
@@ -1300,6 +1369,15 @@ struct VmBuilder {
             return emit(GG_VM_TGET, it->second);
         }
         case NK::Let: return bind(n) && value(n->c[1]);
+        case NK::Pred: {  // c ? x : 0
+            int z = const_slot(0.0);
+            return z >= 0 && value(n->c[1]) && value(n->c[0]) && emit(GG_VM_CONST, z) && emit(GG_VM_SELECT);
+        }
+        case NK::CvtVec: {  // (c != 0) * all-ones
+            int z = const_slot(0.0), o = const_slot(n->dt == GG_U8 ? 255.0 : 4294967295.0);
+            return z >= 0 && o >= 0 && value(n->c[0]) && emit(GG_VM_CONST, z) && emit(GG_VM_NE) &&
+                   emit(GG_VM_CONST, o) && emit(GG_VM_MUL);
+        }
         case NK::Cast: {
             if (!value(n->c[0])) return false;
             return n->dt == GG_F32 ? emit(GG_VM_TOF32) : true;
@@ -1337,6 +1415,10 @@ struct VmBuilder {
             ok = p >= 0;
             if (ok) {
                 if (s->k == NK::Assign) ok = value(s->c[1]) && emit(GG_VM_STORE, p);
+                else if (s->k == NK::AddAssign && s->c[1]->k == NK::Pred)  // c ? a + x : a
+                    ok = value(s->c[1]->c[1]) && emit(GG_VM_LOAD, p) && value(s->c[1]->c[0]) && emit(GG_VM_ADD) &&
+                         (lhs->dt == GG_F32 ? emit(GG_VM_TOF32) : true) && emit(GG_VM_LOAD, p) &&
+                         emit(GG_VM_SELECT) && emit(GG_VM_STORE, p);
                 else if (s->k == NK::AddAssign) ok = emit(GG_VM_LOAD, p) && value(s->c[1]) && emit(GG_VM_ADD) && emit(GG_VM_STORE, p);
                 else if (s->k == NK::MulAssign) ok = emit(GG_VM_LOAD, p) && value(s->c[1]) && emit(GG_VM_MUL) && emit(GG_VM_STORE, p);
                 else unsupported("vertex statement", s);

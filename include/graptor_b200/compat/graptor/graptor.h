@@ -209,6 +209,22 @@ template <typename Fn> void map_vertexL(const partitioner &part, Fn fn) {
 // map_vertex_serialL: the same loop, in vertex order (the reference runs it
 // serially for repeatable random draws, FMv.C:291-298)
 template <typename Fn> void map_vertex_serialL(const partitioner &part, Fn fn) { map_vertexL(part, fn); }
+// map_partitionL(part, fn(k)): fn per partition (one partition on the device)
+template <typename Fn> void map_partitionL(const partitioner &part, Fn fn) {
+    graptor_b200::host_sync();
+    for (int k = 0, p = part.get_num_partitions(); k < p; ++k) fn((unsigned)k);
+}
+// vertexMap(part, F, functor): a host functor over the vertices of F
+// (legacy vertexMap with a C++ functor, APRv.C:500)
+template <typename F> void vertexMap(const partitioner &part, const frontier &Fr, F fn) {
+    graptor_b200::host_sync();
+    if (Fr.all()) {
+        for (VID v = 0, n = part.get_num_vertices(); v < n; ++v) fn(v);
+    } else {
+        const VID *l = Fr.getSparse();
+        for (VID i = 0, k = Fr.nActiveVertices(); i < k; ++i) fn(l[i]);
+    }
+}
 template <typename I, typename Fn> void parallel_loop(I lo, I hi, Fn fn) {
     graptor_b200::host_sync();
     for (I i = lo; i < hi; ++i) fn(i);

@@ -901,3 +901,94 @@ ORC_API int64_t orc_mis(uint32_t n, const uint64_t *off, const uint32_t *adj, co
     free(order);
     return in;
 }
+
+/* ---------------------------------------------------------------------------
+ * Accelerated (delta) PageRank (reference: bench/APRv.C:289-505; FloatTy
+ * float, DEFERRED_UPDATE, MEMO and UNCOND_EXEC on, UNCOND_EXEC_THRESHOLD 0.6).
+ *
+ * x = 0, delta = 1/n.  Iteration 0: contrib = delta / outdeg, z[d] = sum of
+ * contrib over all in-edges, delta = 0.85 z + 0.15/n, x += delta, delta -=
+ * 1/n.  Later iterations sum either over all in-edges with every vertex's
+ * contrib (frontier density (|F| + outdeg(F)) / m above 0.6) or over the
+ * in-edges from the frontier F only; then delta = 0.85 z and x += delta
+ * where the vertex is active.  Active: |delta| > 0.01 x; the active set is
+ * the next F.  The loop ends after maxiter iterations or once sum |delta|
+ * (a compensated double sum, as a float) is below 1e-7; x is then scaled by
+ * 1 / sum |x|.  All vertex arithmetic in float, z summed in float in CSC
+ * order.  l1[i] receives each iteration's sum |delta|.  Returns the iteration
+ * count, or -1 on an allocation failure.
+ * ------------------------------------------------------------------------ */
+static double apr_abs_sum(const float *a, uint32_t n) {
+    double d = 0.0, err = 0.0;
+    for (uint32_t i = 0; i < n; ++i) {
+        const double t = d, y = fabs((double)a[i]) + err;
+        d = t + y;
+        err = t - d;
+        err += y;
+    }
+    return d;
+}
+
+ORC_API int orc_apr(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj, const uint32_t *outdeg,
+                    int maxiter, float *x, double *l1) {
+    const size_t nb = (size_t)(n ? n : 1);
+    float *delta = (float *)malloc(nb * sizeof(float)), *z = (float *)malloc(nb * sizeof(float));
+    float *contrib = (float *)malloc(nb * sizeof(float)), *od = (float *)malloc(nb * sizeof(float));
+    uint8_t *F = (uint8_t *)malloc(nb), *act = (uint8_t *)malloc(nb);
+    if (!delta || !z || !contrib || !od || !F || !act) {
+        free(delta); free(z); free(contrib); free(od); free(F); free(act);
+        return -1;
+    }
+    const float dampen = 0.85f, eps = 1e-7f, eps2 = 1e-2f;
+    const float ninv = 1.0f / (float)n;
+    const uint64_t m = in_off[n];
+    for (uint32_t v = 0; v < n; ++v) {
+        x[v] = 0.0f;
+        delta[v] = ninv;
+        od[v] = (float)outdeg[v];
+        F[v] = 1;
+    }
+    double nactv = n, nacte = (double)m;
+    int iter = 0;
+    while (iter < maxiter) {
+        const float cst = (1.0f - dampen) * ninv;
+        const int all_src = iter == 0 || (nactv + nacte) / (double)m > 0.6;
+        for (uint32_t v = 0; v < n; ++v) {
+            z[v] = 0.0f;
+            if (all_src || F[v]) contrib[v] = delta[v] / od[v];
+        }
+        for (uint32_t d = 0; d < n; ++d) {
+            float acc = z[d];
+            for (uint64_t e = in_off[d]; e < in_off[d + 1]; ++e)
+                if (all_src || F[in_adj[e]]) acc += contrib[in_adj[e]];
+            z[d] = acc;
+        }
+        nactv = 0;
+        nacte = 0;
+        for (uint32_t v = 0; v < n; ++v) {
+            if (iter == 0) {
+                delta[v] = dampen * z[v] + cst;
+                x[v] += delta[v];
+                delta[v] = delta[v] - ninv;
+                act[v] = fabsf(delta[v]) > eps2 * x[v];
+            } else {
+                delta[v] = z[v] * dampen;
+                act[v] = fabsf(delta[v]) > eps2 * x[v];
+                if (act[v]) x[v] += delta[v];
+            }
+            if (act[v]) {
+                nactv += 1;
+                nacte += outdeg[v];
+            }
+        }
+        const float L1 = (float)apr_abs_sum(delta, n);
+        if (l1) l1[iter] = L1;
+        ++iter;
+        memcpy(F, act, nb);
+        if (L1 < eps) break;
+    }
+    const float s = 1.0f / (float)apr_abs_sum(x, n);
+    for (uint32_t v = 0; v < n; ++v) x[v] *= s;
+    free(delta); free(z); free(contrib); free(od); free(F); free(act);
+    return iter;
+}

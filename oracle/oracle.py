@@ -72,6 +72,7 @@ def lib() -> C.CDLL:
         L.orc_fm_deffg.restype = C.c_float
         L.orc_mis.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_mis.restype = C.c_int64
+        L.orc_apr.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
@@ -326,6 +327,33 @@ def ref_mis(bin_path: str, out_path: str, threads: int | None = None):
     txt = _run([ref_prog("ref_mis"), bin_path, out_path], threads)
     w = next(l for l in txt.splitlines() if l.startswith("n ")).split()
     return np.fromfile(out_path, dtype=np.uint8), np.fromfile(out_path + ".remap", dtype=np.uint32), int(w[5])
+
+
+def apr(g: Graph, maxiter: int = 100, csc: Graph | None = None):
+    """APRv's accelerated PageRank (oracle.c orc_apr): returns (x float32,
+    iterations, per-iteration sum |delta|)."""
+    csc = csc if csc is not None else g.transpose()
+    x = np.empty(max(g.n, 1), dtype=np.float32)
+    l1 = np.zeros(max(maxiter, 1), dtype=np.float64)
+    outdeg = g.outdeg()
+    it = lib().orc_apr(g.n, _p(csc.off), _p(csc.adj), _p(outdeg), maxiter, _p(x), _p(l1))
+    if it < 0:
+        raise RuntimeError("orc_apr failed")
+    return x[:g.n], it, l1[:it]
+
+
+def ref_apr(bin_path: str, out_path: str, maxiter: int = 100, threads: int | None = None):
+    """Reference APRv (its driver, -pr:outfile): returns (x float64 in
+    original order, iterations)."""
+    args = [ref_prog("APRv"), "-s", "-b", "-rounds", "1", "-c", "256", "-pr:maxiter", str(maxiter),
+            "-pr:outfile", out_path, "-itimes", bin_path]
+    _, err = _run(args, threads, stderr=True)
+    x = np.fromfile(out_path, dtype=np.float64, sep=" ")
+    n = int(np.fromfile(bin_path, dtype=np.uint64, count=3)[2])
+    if len(x) != n:
+        raise PaddedGraph(f"reference padded {n} vertices to {len(x)}")
+    its = sum(1 for l in err.splitlines() if l.startswith("Iteration "))
+    return x, its
 
 
 def ref_variant() -> str:

@@ -163,6 +163,20 @@ int main() {
         api::emap_arg(st2, api::filter(F, api::strong, api::src));
         CHECK(st2.in == &F && st2.d.dst_filter == GG_FILTER_NONE && st2.d.src_strong == 1);
     }
+    // APRv.C:409-416,455-458: active = cvt_to_vector(|delta| > eps2 * x); x += add_predicate(delta, active != 0)
+    {
+        graptor_b200::VmBuilder b;
+        E x = at(1, GG_F32, V), delta = at(2, GG_F32, V), active = at(3, GG_U32, V);
+        CHECK(b.statement((active = make_unop_cvt_to_vector<logical<4>>(make_unop_abs(delta) >
+                                                                       constant_val(x, 0.01f) * x)).node()));
+        CHECK(b.d.code[b.d.ncode - 1] == GG_VM_STORE && b.d.code[b.d.ncode - 2] == GG_VM_MUL);
+        CHECK(b.d.consts[b.d.arg[b.d.ncode - 3]] == 4294967295.0);
+        graptor_b200::VmBuilder c;
+        CHECK(c.statement((x += add_predicate(delta, active != _0)).node()));
+        // the untaken side reloads x: masked vertices keep their value exactly
+        CHECK(c.d.code[c.d.ncode - 1] == GG_VM_STORE && c.d.code[c.d.ncode - 2] == GG_VM_SELECT &&
+              c.d.code[c.d.ncode - 3] == GG_VM_LOAD && c.d.code[c.d.ncode - 4] == GG_VM_TOF32);
+    }
     if (fails) return 1;
     std::printf("ok\n");
     return 0;

@@ -20,6 +20,8 @@ programs on it, compiled from the reference sources by oracle/Makefile:
   mis_state    - MISv.C run by oracle/harness/ref_mis.C: the final state of
                  each vertex (2 out, 3 in), with mis_remap the layout id of
                  each vertex (MISv's priorities)
+  apr_x        - APRv.C -pr:outfile (to sum |delta| < 1e-7 or 100 iterations),
+                 with apr_iters its iteration count
 customfp_sweep.npz holds float bit patterns and, per pattern, the codes and
 decoded floats of the reference's customfp<6,10> and scustomfp<true,8,7>
 conversions (harness oracle/harness/ref_cfp.C).
@@ -30,6 +32,7 @@ Run (needs the reference tree and `make -C oracle ref`):
     python tests/golden/make_golden.py            # every fixture
     python tests/golden/make_golden.py --fm-only  # add / refresh the fm_* keys only
     python tests/golden/make_golden.py --mis-only # add / refresh the mis_* keys only
+    python tests/golden/make_golden.py --apr-only # add / refresh the apr_* keys only
 """
 import hashlib
 import os
@@ -98,6 +101,15 @@ def mis_reference(g, tmp):
     return dict(mis_state=st, mis_remap=remap)
 
 
+def apr_reference(g, tmp):
+    p = os.path.join(tmp, "g.bin")
+    O.write_bin(g, p)
+    x, its = O.ref_apr(p, os.path.join(tmp, "apr.txt"))
+    xo, ito, _ = O.apr(g)
+    assert ito == its and np.abs(xo - x).sum() < 1e-5  # the restatement must agree
+    return dict(apr_x=x, apr_iters=np.int64(its))
+
+
 def add_keys(name, tmp, fn):
     path = os.path.join(HERE, name + ".npz")
     d = dict(np.load(path))
@@ -116,6 +128,7 @@ def save(name, g, roots, pr_iters, tmp, store_csr=True, params=None):
     levels, parents, cc, pr, vary = run_reference(g, roots, pr_iters, tmp)
     vary.update(fm_reference(g, tmp))
     vary.update(mis_reference(g, tmp))
+    vary.update(apr_reference(g, tmp))
     # sanity: the restatement must agree before a fixture is written
     for r, l in zip(roots, levels):
         assert np.array_equal(O.bfs_level(g, r), l), name
@@ -154,7 +167,7 @@ def main():
     if not O.ref_available("ref_bfslvl"):
         raise SystemExit("reference build missing: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
-        only = {"--fm-only": fm_reference, "--mis-only": mis_reference}
+        only = {"--fm-only": fm_reference, "--mis-only": mis_reference, "--apr-only": apr_reference}
         for flag, fn in only.items():
             if flag in sys.argv:
                 for name in ["rmat10_ef8", "rmat12_ef16", "grid20x32_del5pct", "er2000_deg6", "edgecases32",

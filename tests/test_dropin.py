@@ -184,3 +184,16 @@ def test_reference_misv_with_its_driver(tmp_path):
     z, g, p = _graph_file(tmp_path, "rmat12_ef16")
     r = _driver("MISv", ["-s", "-b", "-rounds", "2", p])
     assert r.stderr.count("result: PASS") == 2, r.stderr[-2000:]
+
+
+@pytest.mark.parametrize("name", _golden_graphs())
+def test_reference_aprv_source_on_gpu(tmp_path, name):
+    """APRv.C with its driver: ranks within 2e-6 L1 of the reference build's
+    APRv, iteration counts within one."""
+    z, g, p = _graph_file(tmp_path, name)
+    out = str(tmp_path / "apr.txt")
+    r = _driver("APRv", ["-s", "-b", "-rounds", "1", "-itimes", "-pr:outfile", out, p])
+    its = sum(1 for l in r.stderr.splitlines() if l.startswith("Iteration "))
+    assert abs(its - int(z["apr_iters"])) <= 1, (its, int(z["apr_iters"]))
+    x = np.loadtxt(out, dtype=np.float64)
+    assert np.abs(x - z["apr_x"]).sum() <= 2e-6
