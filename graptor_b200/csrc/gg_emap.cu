@@ -77,6 +77,10 @@ struct EmapArgs {
     const uint64_t *word_prefix;        // full-scan pull: per-word cost prefix
     const uint4 *first_in;              // pull: first two in-neighbours + in-degree per vertex, or null
     int lazy_off;                       // pull: offsets only for rows the first two edges do not settle
+    // split pull, first pass: candidates still open after their first two
+    // in-edges are appended here for the second pass (graph-driven BFS)
+    uint32_t *rest_out;
+    unsigned long long *rest_out_n;
 };
 
 template <int R>
@@ -208,8 +212,15 @@ __device__ __forceinline__ void flush_counts(const EmapArgs &A, unsigned long lo
 // list of destinations (output bitmap pre-cleared, bits set with atomicOr).
 // Loads are issued ahead of use: d's value and both offsets together, then
 // up to 4 neighbour ids, then their frontier bits and source values.
-template <int R, bool SRCF, bool CAND, int BLOCK>
+//
+// Split pull (level-synchronous BFS, candidate lists, first_in records):
+// PASS 1 settles what each candidate's first two in-edges settle and appends
+// the candidates with more edges still to look at to rest_out; PASS 2 walks
+// that list from each row's third edge.  A warp of PASS 1 then waits for no
+// lane's long row, and a warp of PASS 2 has every lane on an open row.
+template <int R, bool SRCF, bool CAND, int BLOCK, int PASS = 0>
 __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
+    static_assert(PASS == 0 || (CAND && R == GG_RELAX_MIN_PLUS1_I32), "split pull: BFS levels, candidate lists");
     using V = typename Op<R>::V;
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t nitems = CAND ? *A.cand_n : (uint64_t)A.n;
@@ -223,6 +234,8 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
     unsigned long long nv = 0, ne = 0, sc = 0;
     __shared__ uint32_t s_cand[BLOCK / 32][256];
     dev::WarpAppender<256> keepers{s_cand[threadIdx.x >> 5], 0, A.cand_out, A.cand_out_n};
+    __shared__ uint32_t s_rest[PASS == 1 ? BLOCK / 32 : 1][PASS == 1 ? 256 : 1];
+    dev::WarpAppender<256> rest{s_rest[PASS == 1 ? threadIdx.x >> 5 : 0], 0, A.rest_out, A.rest_out_n};
     for (uint64_t w = CAND ? gw : wlo; CAND ? ((w << 5) < nitems) : (w < whi); w += wstep) {
         const uint64_t item = (w << 5) + lane;
         const bool valid = item < nitems;
@@ -230,10 +243,10 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
         V best = Op<R>::none();
         uint64_t e = 0, end = 0;
         uint4 f2 = make_uint4(0u, 0u, 0u, 0u);
-        const bool lazy = A.first_in && A.lazy_off;
+        const bool lazy = PASS != 2 && A.first_in && A.lazy_off;
         if (valid) {
             best = op.load(d);
-            if (A.first_in) f2 = A.first_in[d];
+            if (PASS != 2 && A.first_in) f2 = A.first_in[d];
             if (!lazy) {
                 e = A.in_off[d];
                 end = A.in_off[d + 1];
@@ -244,8 +257,9 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
         bool act = valid && op.dst_ok(best);
         bool changed = false;
         uint64_t beg = e;
+        if (PASS == 2) e += 2;  // the first pass took the first two edges
         uint64_t lim = min(end, e + (uint64_t)A.K);
-        if (A.first_in && act && e < lim) {
+        if (PASS != 2 && A.first_in && act && e < lim) {
             // the row's first two in-neighbours, loaded beside its offsets:
             // the same edges in the same order as the loop below takes them
             const int cnt = (int)min((uint64_t)2, lim - e);
@@ -266,6 +280,13 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
                 }
             }
             e += used;
+        }
+        // first pass: rows still open after two edges go to the second
+        bool deferred = false;
+        if (PASS == 1) {
+            deferred = act && e < end;
+            rest.push(deferred, d);
+            if (deferred) act = false;
         }
         if (lazy && valid) {
             // the row's offsets, for rows still open after their first two edges
@@ -303,7 +324,7 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
             }
             e += used;
         }
-        sc += e - beg;
+        sc += e - beg - (PASS == 2 ? 2 : 0);
         unsigned pend = __ballot_sync(FULL, act && e < end);
         while (pend) {
             const int j = __ffs(pend) - 1;
@@ -389,6 +410,7 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
         if (A.cand_out) keepers.push(valid && act && end > beg, d);
     }
     if (A.cand_out) keepers.flush();
+    if (PASS == 1) rest.flush();
     if (A.out_cnt) flush_counts<BLOCK>(A, nv, ne, sc);
 }
 
@@ -1438,6 +1460,9 @@ struct GCtl {
     const uint32_t *adj, *in_adj;
     const uint4 *first_in;
     int lazy_off;
+    int split;                        // pulls in two passes (pull_body PASS 1 / 2)
+    uint32_t *rest;                   // split pull: the second pass's rows
+    unsigned long long rest_n;
     const uint32_t *nonisolated;
     const unsigned long long *nonisolated_n;
     uint32_t *cand[2];
@@ -1622,6 +1647,11 @@ __device__ void decide_step(GCtl *c) {
         A.cand_out_n = c->cand_n + (cc ^ 1);
         c->cand_n[cc ^ 1] = 0;
         A.out_bits = O.bitmap;  // cleared by the post kernel of the step that consumed it
+        if (c->split) {
+            A.rest_out = c->rest;
+            A.rest_out_n = &c->rest_n;
+            c->rest_n = 0;
+        }
     }
     c->A = A;
     Op<GG_RELAX_MIN_PLUS1_I32> op;
@@ -1767,7 +1797,32 @@ __global__ void __launch_bounds__(kBlock, 6) k_g_pull(GCtl *c) {
         if (blockIdx.x == 0) c->clr = c->cur + 1;  // a pulled frontier has a bitmap to clear after
     }
     __syncthreads();
-    pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock>(sA, sOp);
+    if (sA.rest_out) pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock, 1>(sA, sOp);
+    else pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock>(sA, sOp);
+    kspan_end(c, s_it, &s_done);
+}
+
+// second pass of a split pull: the rows the first pass left open, from
+// their third in-edge
+__global__ void __launch_bounds__(kBlock, 6) k_g_pull2(GCtl *c) {
+    if (c->variant != GG_VAR_PULL_DENSE || !c->A.rest_out) return;
+    __shared__ EmapArgs sA;
+    __shared__ Op<GG_RELAX_MIN_PLUS1_I32> sOp;
+    __shared__ int s_it;
+    __shared__ unsigned s_done;
+    if (threadIdx.x == 0) {
+        s_it = c->iter;
+        s_done = 0;
+        kspan_start(c, s_it);
+        sA = c->A;
+        sA.cand = c->rest;
+        sA.cand_n = &c->rest_n;
+        sA.first_in = nullptr;
+        sA.rest_out = nullptr;
+        sOp = c->op;
+    }
+    __syncthreads();
+    pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock, 2>(sA, sOp);
     kspan_end(c, s_it, &s_done);
 }
 
@@ -1876,6 +1931,8 @@ struct GraphBfs {
     GCtl *ctl = nullptr;
     uint64_t *chunk_first = nullptr;
     uint64_t chunk_cap = 0;
+    uint32_t *rest = nullptr;  // split pull: second-pass rows (n entries)
+    uint64_t rest_cap = 0;
     unsigned push_grid = 0, pull_grid = 0, vgrid = 0;
 };
 
@@ -1912,6 +1969,7 @@ void graph_bfs_free(gg_graph *g) {
     if (gb->graph) cudaGraphDestroy(gb->graph);
     cudaFree(gb->ctl);
     cudaFree(gb->chunk_first);
+    cudaFree(gb->rest);
     delete gb;
     g->gbfs = nullptr;
 }
@@ -1959,6 +2017,8 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     GG_CHECK(add_cond(ctx, bq, &n_ifb, nullptr, 0, hb, cudaGraphCondTypeIf, &bb));
     GG_CHECK(add_kernel(ctx, bb, &n_bits, nullptr, 0, (const void *)k_g_tobitmap, gb->vgrid, 256, arg));
     GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_ifb, 1, (const void *)k_g_pull, gb->pull_grid, kBlock, arg));
+    cudaGraphNode_t n_pull2;
+    GG_CHECK(add_kernel(ctx, bq, &n_pull2, &n_pull, 1, (const void *)k_g_pull2, gb->pull_grid, kBlock, arg));
     GG_CHECK(add_kernel(ctx, body, &n_next, &n_sw, 1, (const void *)k_g_next, (unsigned)ctx->sm_count * 2, 256, arg));
     GG_CUDA(ctx, cudaGraphInstantiate(&gb->exec, G, 0));
     // the handles live in the control block, set once
@@ -2036,6 +2096,18 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     h.in_adj = g->in_adj;
     h.first_in = t.pull_first ? g->first_in : nullptr;
     h.lazy_off = t.pull_first == 2;
+    // the split pull's second pass starts at each row's third edge: it needs
+    // the first pass to have taken the first two from the first_in records
+    h.split = t.pull_split && h.first_in;
+    if (h.split && gb->rest_cap < (uint64_t)g->n) {
+        cudaFree(gb->rest);
+        gb->rest = nullptr;
+        gb->rest_cap = 0;
+        GG_CUDA(ctx, cudaMalloc(&gb->rest, ((uint64_t)g->n + 1) * 4));
+        gb->rest_cap = g->n;
+    }
+    h.rest = gb->rest;
+    h.rest_n = 0;
     h.nonisolated = g->nonisolated;
     h.nonisolated_n = (const unsigned long long *)g->nonisolated_n;
     // chunk prefix room: rows above bin_medium_max edges, at most m / (max + 1)

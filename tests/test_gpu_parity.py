@@ -432,6 +432,41 @@ def test_pull_first_record_modes_exact(ctx, mode, gen):
         g.close()
 
 
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("gen", ["rmat", "grid", "er_directed", "edgecases"])
+def test_split_pull_exact(ctx, mode, gen):
+    """Graph-driven BFS with the split pull (knob pull_split: the first pass
+    settles what each candidate's first two in-edges settle, the second walks
+    the rows left open from their third edge): levels identical to the
+    oracle's, with the threshold's variants and with every step a pull."""
+    if gen == "rmat":
+        og, sym = O.rmat(15, 16 << 15, seed=82), True
+    elif gen == "grid":
+        og, sym = O.grid(70, 90, seed=8, del_bp=300), True
+    elif gen == "er_directed":
+        og, sym = O.er(6000, 10.0, seed=9, dangling_bp=100, symmetric=False), False
+    else:
+        z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "edgecases32.npz"))
+        og, sym = O.Graph(int(z["n"]), z["off"], z["adj"]), True
+    g = ctx.upload(og.off, og.adj, sym)
+    old = {k: gg.tuning_get(k) for k in ("pull_first", "graph", "pull_split")}
+    try:
+        gg.tuning_set("pull_first", mode)
+        gg.tuning_set("graph", 1)
+        gg.tuning_set("pull_split", 1)
+        deg = og.outdeg()
+        nz = np.flatnonzero(deg)
+        roots = [int(np.argmax(deg)), int(nz[len(nz) // 2]), int(nz[-1])]
+        for r in roots:
+            lv = O.bfs_level(og, r)
+            assert np.array_equal(g.bfs_level(r), lv), (mode, r)
+            assert np.array_equal(g.bfs_level(r, opts=gg.default_opts(variant=gg.VAR_PULL_DENSE)), lv), (mode, r)
+    finally:
+        for k, v in old.items():
+            gg.tuning_set(k, v)
+        g.close()
+
+
 @pytest.mark.parametrize("stochastic,avg", [(False, 0), (True, 0), (True, 50)])
 def test_bf16_stochastic_rounding_matches_restatement(ctx, stochastic, avg):
     """BF16 PageRank with rounding to nearest, stochastic rounding (the same
