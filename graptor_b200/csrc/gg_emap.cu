@@ -1934,7 +1934,18 @@ struct GraphBfs {
     uint32_t *rest = nullptr;  // split pull: second-pass rows (n entries)
     uint64_t rest_cap = 0;
     unsigned push_grid = 0, pull_grid = 0, vgrid = 0;
+    // page-locked host copies of the control block: the configuration sent
+    // before a run, and the records a kernel writes back after it through the
+    // mapping (no copy-engine transfer: a run's records do not queue behind
+    // a caller's large device-to-host copy on another stream)
+    GCtl *h_up = nullptr;
+    GCtl *h_rec = nullptr, *d_rec = nullptr;
 };
+
+__global__ void k_copy_bytes(const unsigned char *__restrict__ src, unsigned char *__restrict__ dst, size_t nb) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
 
 static gg_status add_kernel(gg_ctx *ctx, cudaGraph_t g, cudaGraphNode_t *node, const cudaGraphNode_t *deps, size_t nd,
                             const void *fn, unsigned grid, unsigned block, GCtl **arg) {
@@ -1970,6 +1981,8 @@ void graph_bfs_free(gg_graph *g) {
     cudaFree(gb->ctl);
     cudaFree(gb->chunk_first);
     cudaFree(gb->rest);
+    cudaFreeHost(gb->h_up);
+    cudaFreeHost(gb->h_rec);
     delete gb;
     g->gbfs = nullptr;
 }
@@ -1977,6 +1990,9 @@ void graph_bfs_free(gg_graph *g) {
 static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     gg_ctx *ctx = g->ctx;
     GG_CUDA(ctx, cudaMalloc(&gb->ctl, sizeof(GCtl)));
+    GG_CUDA(ctx, cudaHostAlloc(&gb->h_up, sizeof(GCtl), cudaHostAllocDefault));
+    GG_CUDA(ctx, cudaHostAlloc(&gb->h_rec, sizeof(GCtl), cudaHostAllocMapped));
+    GG_CUDA(ctx, cudaHostGetDevicePointer((void **)&gb->d_rec, gb->h_rec, 0));
     gb->push_grid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_g_push, kBlock));
     gb->pull_grid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_g_pull, kBlock));
     gb->vgrid = (unsigned)(ctx->sm_count * 8);
@@ -2057,7 +2073,7 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     }
     const Tuning &t = tuning();
     // configuration part of the control block (everything before the records)
-    GCtl h;
+    GCtl &h = *gb->h_up;  // the previous run's upload finished before it returned
     memset(&h, 0, offsetof(GCtl, reached_v));
     for (int i = 0; i < 2; ++i) {
         gg_frontier *f = g->tmp_front[i];
@@ -2128,20 +2144,20 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     GG_CUDA(ctx, cudaGraphLaunch(gb->exec, ctx->stream));
     // state and records back (one wait per run)
     const size_t rec0 = offsetof(GCtl, variant), rec1 = offsetof(GCtl, h_while);
-    GCtl *hr = (GCtl *)std::malloc(sizeof(GCtl));
-    if (!hr) return GG_ERR_OOM;
-    cudaError_t e = cudaMemcpyAsync((char *)hr + rec0, (char *)gb->ctl + rec0, rec1 - rec0, cudaMemcpyDeviceToHost,
-                                    ctx->stream);
+    GCtl *hr = gb->h_rec;
+    k_copy_bytes<<<8, 256, 0, ctx->stream>>>((const unsigned char *)gb->ctl + rec0, (unsigned char *)gb->d_rec + rec0,
+                                            rec1 - rec0);
+    cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) {
-        std::free(hr);
-        return cuda_error(ctx, e, "graph BFS");
-    }
+    if (e != cudaSuccess) return cuda_error(ctx, e, "graph BFS");
     const int T = hr->iterations;
     *iters_out = T;
     // kernels the graph ran: init, then per iteration the step kernel and
-    // next (plus a list or bitmap conversion where the variant changes)
-    ctx->launches += 1 + 2 * (uint64_t)T;
+    // next, a pull's second-pass kernel (plus a list or bitmap conversion
+    // where the variant changes); then the records' copy
+    uint64_t npull = 0;
+    for (int i = 0; i < T && i < GG_MAX_ITERS; ++i) npull += hr->variants[i] == GG_VAR_PULL_DENSE;
+    ctx->launches += 2 + 2 * (uint64_t)T + npull;
     if (hr->handed_off) {
         // the rest of the run as one device-driven launch from the current
         // frontier (a push leaves it as a list only: add its bitmap)
@@ -2164,10 +2180,7 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
         const PersistResume rs{T, cur, hr->has_list[cur], hr->reached_v, hr->reached_e};
         int iters = 0;
         if (s == GG_OK) s = persistent_traverse(g, desc, 1, false, root, opt, st, &iters, -1, -1, nullptr, 0, &rs);
-        if (s != GG_OK) {
-            std::free(hr);
-            return s;
-        }
+        if (s != GG_OK) return s;
         *iters_out = iters;
     } else if (st) {
         st->vertices_reached = hr->reached_v;
@@ -2185,7 +2198,6 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
                                    ? (double)(hr->kt1[i] - hr->kt0[i]) * 1e-6 : st->iter_ms[i];
         }
     }
-    std::free(hr);
     for (auto *f : g->tmp_front) f->host_valid = false;
     g->cand.valid = false;
     return GG_OK;
