@@ -1213,7 +1213,17 @@ gg_status gg_prop_create_managed(gg_graph *g, gg_dtype t, gg_prop **out) {
     // host code writes the initial values in place; kernels then migrate the pages
     cudaError_t e = cudaMallocManaged(&p->d, ((size_t)g->n + 1) * esz, cudaMemAttachGlobal);
     if (e != cudaSuccess) { delete p; return cuda_error(g->ctx, e, "gg_prop_create_managed"); }
+    p->managed = true;
     *out = p;
+    return GG_OK;
+}
+
+gg_status gg_prop_prefetch(gg_prop *p, int to_device) {
+    if (!p) return GG_ERR_ARG;
+    if (!p->managed) return GG_OK;
+    gg_ctx *ctx = p->g->ctx;
+    const size_t bytes = ((size_t)p->g->n + 1) * p->esz;
+    GG_CUDA(ctx, cudaMemPrefetchAsync(p->d, bytes, to_device ? ctx->device : cudaCpuDeviceId, ctx->stream));
     return GG_OK;
 }
 

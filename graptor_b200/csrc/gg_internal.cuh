@@ -175,6 +175,7 @@ struct gg_prop {
     gg_dtype t = GG_I32;
     size_t esz = 4;
     void *d = nullptr;
+    bool managed = false;  // gg_prop_create_managed
 };
 
 namespace gg {

@@ -91,7 +91,8 @@ EXPORTS = [
     "gg_graph_read_bin", "gg_graph_write_bin", "gg_graph_generate", "gg_graph_info",
     "gg_graph_download", "gg_graph_device_ptrs", "gg_graph_max_degree_vertex", "gg_graph_destroy",
     "gg_prop_create", "gg_prop_fill", "gg_prop_set", "gg_prop_get", "gg_prop_download",
-    "gg_prop_upload", "gg_prop_device_ptr", "gg_prop_destroy", "gg_prop_create_managed", "gg_frontier_create",
+    "gg_prop_upload", "gg_prop_device_ptr", "gg_prop_destroy", "gg_prop_create_managed", "gg_prop_prefetch",
+    "gg_frontier_create",
     "gg_frontier_clear", "gg_frontier_set_single", "gg_frontier_set_all", "gg_frontier_set_list",
     "gg_frontier_counts", "gg_frontier_download", "gg_frontier_destroy", "gg_edgemap",
     "gg_vertexmap", "gg_bfs_level", "gg_bfs_level_host_async", "gg_bfs_level_host_wait",

@@ -153,6 +153,10 @@ GG_API gg_status gg_prop_destroy(gg_prop *p);                             /* ver
  * after gg_ctx_sync).  Replaces mmap_ptr<T>::allocate(numa_allocation_partitioned)
  * (mm.h:741-745), whose arrays the reference's analytics index from host code. */
 GG_API gg_status gg_prop_create_managed(gg_graph *g, gg_dtype t, gg_prop **out);
+/* Moves a managed property's pages to the device (to_device = 1) or to the
+ * host (0) ahead of use, in order on the context's stream (one bulk
+ * migration instead of page faults); a no-op for other properties. */
+GG_API gg_status gg_prop_prefetch(gg_prop *p, int to_device);
 
 /* ------------------------------------------------------------------ */
 /* Frontiers (frontier/frontier.h:58-716).  A frontier holds a        */

@@ -23,6 +23,7 @@
 #include <functional>
 #include <iostream>
 #include <map>
+#include <set>
 #include <memory>
 #include <mutex>
 #include <sstream>
@@ -98,6 +99,19 @@ inline void host_sync() {
         check(gg_ctx_sync(ctx_slot()), "gg_ctx_sync");
         synced_epoch() = device_epoch();
     }
+}
+
+// Managed arrays that host code has indexed since the last device step:
+// their pages are moved to the device in one prefetch before the next step
+// (kernels would otherwise fault them over page by page).
+inline std::set<gg_prop *> &host_touched() {
+    static std::set<gg_prop *> s;
+    return s;
+}
+inline void before_device() {
+    auto &t = host_touched();
+    for (gg_prop *p : t) check(gg_prop_prefetch(p, 1), "gg_prop_prefetch");
+    t.clear();
 }
 
 // The graph that frontiers made from host vertex lists (frontier::sparse)
@@ -367,6 +381,7 @@ public:
         for (int i = 0; i < 4; ++i) d.code[i] = code[i];
         d.props[0] = dense_store_.get();
         double red[GG_VM_MAX_REDUCE] = {0, 0, 0, 0};
+        graptor_b200::before_device();
         graptor_b200::check(gg_vertexmap(G.handle(), &d, nullptr, output(G.handle()), red), "gg_vertexmap");
     }
     void del() {
@@ -925,15 +940,18 @@ public:
     // host writes need no flush: the next kernel, queued after them, sees them
     T &operator[](size_t v) {
         graptor_b200::host_sync();
+        if (p_) graptor_b200::host_touched().insert(p_);
         return d_[v];
     }
     const T &operator[](size_t v) const {
         graptor_b200::host_sync();
+        if (p_) graptor_b200::host_touched().insert(p_);
         return d_[v];
     }
     void del() {
         if (p_) {
             graptor_b200::registry().erase(d_);
+            graptor_b200::host_touched().erase(p_);
             gg_prop_destroy(p_);
         } else {
             std::free(d_);
@@ -1429,6 +1447,7 @@ struct VmBuilder {
 };
 
 inline void run_vmap(gg_graph *g, VmBuilder &b, gg_frontier *filter, gg_frontier *out) {
+    before_device();
     double red[GG_VM_MAX_REDUCE] = {0, 0, 0, 0};
     check(gg_vertexmap(g, &b.d, filter, out, red), "gg_vertexmap");
     ++device_epoch();
@@ -1578,6 +1597,7 @@ lazy_executor edgemap(const GraphType &GA, Args &&... args) {
             graptor_b200::check(gg_frontier_clear(fout), "gg_frontier_clear");
             fout = nullptr;
         }
+        graptor_b200::before_device();
         graptor_b200::check(gg_edgemap(g, &s.d, fin, fout, nullptr), "gg_edgemap");
         ++graptor_b200::device_epoch();
     });
