@@ -1223,6 +1223,7 @@ gg_status gg_prop_prefetch(gg_prop *p, int to_device) {
     if (!p->managed) return GG_OK;
     gg_ctx *ctx = p->g->ctx;
     const size_t bytes = ((size_t)p->g->n + 1) * p->esz;
+    if (to_device == 2) GG_CUDA(ctx, cudaMemAdvise(p->d, bytes, cudaMemAdviseSetReadMostly, ctx->device));
     GG_CUDA(ctx, cudaMemPrefetchAsync(p->d, bytes, to_device ? ctx->device : cudaCpuDeviceId, ctx->stream));
     return GG_OK;
 }

@@ -1647,7 +1647,10 @@ __device__ void decide_step(GCtl *c) {
         A.cand_out_n = c->cand_n + (cc ^ 1);
         c->cand_n[cc ^ 1] = 0;
         A.out_bits = O.bitmap;  // cleared by the post kernel of the step that consumed it
-        if (c->split) {
+        // split when the frontier holds less than half the edges: then most
+        // candidates' first two in-edges leave them open, and a warp of the
+        // single pass waits for its lanes' long rows
+        if (c->split && 2 * nacte < c->m) {
             A.rest_out = c->rest;
             A.rest_out_n = &c->rest_n;
             c->rest_n = 0;
@@ -1942,8 +1945,10 @@ struct GraphBfs {
     GCtl *h_rec = nullptr, *d_rec = nullptr;
 };
 
-__global__ void k_copy_bytes(const unsigned char *__restrict__ src, unsigned char *__restrict__ dst, size_t nb) {
-    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nb; i += (size_t)gridDim.x * blockDim.x)
+// 16-byte words: whole-line writes over the host link (byte stores would
+// each be a transaction of their own)
+__global__ void k_copy_words16(const uint4 *__restrict__ src, uint4 *__restrict__ dst, size_t nw) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < nw; i += (size_t)gridDim.x * blockDim.x)
         dst[i] = src[i];
 }
 
@@ -1989,9 +1994,10 @@ void graph_bfs_free(gg_graph *g) {
 
 static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     gg_ctx *ctx = g->ctx;
-    GG_CUDA(ctx, cudaMalloc(&gb->ctl, sizeof(GCtl)));
+    // (16 bytes of slack: the records' copy moves whole 16-byte words)
+    GG_CUDA(ctx, cudaMalloc(&gb->ctl, sizeof(GCtl) + 16));
     GG_CUDA(ctx, cudaHostAlloc(&gb->h_up, sizeof(GCtl), cudaHostAllocDefault));
-    GG_CUDA(ctx, cudaHostAlloc(&gb->h_rec, sizeof(GCtl), cudaHostAllocMapped));
+    GG_CUDA(ctx, cudaHostAlloc(&gb->h_rec, sizeof(GCtl) + 16, cudaHostAllocMapped));
     GG_CUDA(ctx, cudaHostGetDevicePointer((void **)&gb->d_rec, gb->h_rec, 0));
     gb->push_grid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_g_push, kBlock));
     gb->pull_grid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_g_pull, kBlock));
@@ -2145,8 +2151,8 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     // state and records back (one wait per run)
     const size_t rec0 = offsetof(GCtl, variant), rec1 = offsetof(GCtl, h_while);
     GCtl *hr = gb->h_rec;
-    k_copy_bytes<<<8, 256, 0, ctx->stream>>>((const unsigned char *)gb->ctl + rec0, (unsigned char *)gb->d_rec + rec0,
-                                            rec1 - rec0);
+    const size_t w0 = rec0 / 16, w1 = (rec1 + 15) / 16;  // both bases are 16-byte aligned
+    k_copy_words16<<<8, 256, 0, ctx->stream>>>((const uint4 *)gb->ctl + w0, (uint4 *)gb->d_rec + w0, w1 - w0);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "graph BFS");

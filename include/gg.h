@@ -155,7 +155,9 @@ GG_API gg_status gg_prop_destroy(gg_prop *p);                             /* ver
 GG_API gg_status gg_prop_create_managed(gg_graph *g, gg_dtype t, gg_prop **out);
 /* Moves a managed property's pages to the device (to_device = 1) or to the
  * host (0) ahead of use, in order on the context's stream (one bulk
- * migration instead of page faults); a no-op for other properties. */
+ * migration instead of page faults); 2 marks a property that is no longer
+ * written read-mostly (host and device each keep a copy of the pages they
+ * read) and prefetches it to the device.  A no-op for other properties. */
 GG_API gg_status gg_prop_prefetch(gg_prop *p, int to_device);
 
 /* ------------------------------------------------------------------ */

@@ -101,16 +101,39 @@ inline void host_sync() {
     }
 }
 
-// Managed arrays that host code has indexed since the last device step:
-// their pages are moved to the device in one prefetch before the next step
-// (kernels would otherwise fault them over page by page).
-inline std::set<gg_prop *> &host_touched() {
-    static std::set<gg_prop *> s;
+// Where a managed array's pages are (mmap_ptr).  Host code that reaches
+// for an array the device holds first brings it over in one prefetch;
+// arrays the host has reached for since the last device step go back to
+// the device in one prefetch before the next step.  Page by page, either
+// side would fault them over (or read them across the host link).
+struct managed_state {
+    gg_prop *p = nullptr;
+    bool on_device = false;
+    bool touched = false;
+};
+inline std::set<managed_state *> &host_touched() {
+    static std::set<managed_state *> s;
     return s;
+}
+inline void host_access(managed_state *st) {
+    host_sync();
+    if (st->on_device) {
+        check(gg_prop_prefetch(st->p, 0), "gg_prop_prefetch");
+        check(gg_ctx_sync(ctx_slot()), "gg_ctx_sync");
+        st->on_device = false;
+    }
+    if (!st->touched) {
+        st->touched = true;
+        host_touched().insert(st);
+    }
 }
 inline void before_device() {
     auto &t = host_touched();
-    for (gg_prop *p : t) check(gg_prop_prefetch(p, 1), "gg_prop_prefetch");
+    for (managed_state *st : t) {
+        check(gg_prop_prefetch(st->p, 1), "gg_prop_prefetch");
+        st->on_device = true;
+        st->touched = false;
+    }
     t.clear();
 }
 
@@ -235,6 +258,8 @@ public:
             gg_prop_device_ptr(c->degp_, &d);
             c->deg_ = (VID *)d;
             for (VID i = 0; i < n_; ++i) c->deg_[i] = (VID)(c->off_[i + 1] - c->off_[i]);
+            // never written again: host and device each keep their copy
+            graptor_b200::check(gg_prop_prefetch(c->degp_, 2), "gg_prop_prefetch");
             graptor_b200::registry()[d] = c->degp_;
             csr_ = c;
         }
@@ -921,37 +946,39 @@ public:
             gg_prop_device_ptr(p_, &d);
             graptor_b200::registry()[d] = p_;
             d_ = (T *)d;
+            st_ = std::make_shared<graptor_b200::managed_state>();
+            st_->p = p_;
         } else {
             d_ = (T *)std::calloc((size_t)a.part.get_num_elements() + 1, sizeof(T));
             if (!d_) throw graptor_b200::error(GG_ERR_OOM, "mmap_ptr host allocation");
         }
     }
-    // the array, for host reads and writes: waits for the device work queued so far
+    // the array, for host reads and writes: waits for the device work queued
+    // so far and brings the pages to the host
     T *get() const {
-        graptor_b200::host_sync();
+        access();
         return d_;
     }
     operator T *() {
-        graptor_b200::host_sync();
+        access();
         return d_;
     }
     operator const T *() const { return d_; }
     explicit operator bool() const { return d_ != nullptr; }
     // host writes need no flush: the next kernel, queued after them, sees them
     T &operator[](size_t v) {
-        graptor_b200::host_sync();
-        if (p_) graptor_b200::host_touched().insert(p_);
+        access();
         return d_[v];
     }
     const T &operator[](size_t v) const {
-        graptor_b200::host_sync();
-        if (p_) graptor_b200::host_touched().insert(p_);
+        access();
         return d_[v];
     }
     void del() {
         if (p_) {
             graptor_b200::registry().erase(d_);
-            graptor_b200::host_touched().erase(p_);
+            graptor_b200::host_touched().erase(st_.get());
+            st_.reset();
             gg_prop_destroy(p_);
         } else {
             std::free(d_);
@@ -962,8 +989,13 @@ public:
     gg_prop *handle() const { return p_; }
 
 private:
+    void access() const {
+        if (st_ && (st_->on_device || !st_->touched)) graptor_b200::host_access(st_.get());
+        else graptor_b200::host_sync();
+    }
     gg_prop *p_ = nullptr;
     T *d_ = nullptr;
+    std::shared_ptr<graptor_b200::managed_state> st_;  // shared by copies
 };
 
 template <unsigned short B> mmap_ptr<uint8_t> array_encoding_bit<B>::allocate(const numa_allocation_partitioned &a) {
