@@ -758,7 +758,21 @@ def run_ours(args, ws, rank, local):
     n, m = g.n, g.m
 
     lvl = g.prop(gg.I32)
-    opts = gg.default_opts(collect=True)
+    # variant choice per step: the learned selector (trained on other graphs:
+    # R-MAT scales 18-22, ER, grids), the density threshold as its fallback;
+    # the levels do not depend on the choice
+    sel = None
+    if args.select == "learned":
+        from graptor_b200.selector_train import load_selector
+        sel = load_selector(ctx)
+    if sel is not None:
+        gg.attach_selector(g, sel)
+        opts = gg.default_opts(gg.THRESH_LEARNED, collect=True)
+        select_desc = ("learned selector (graptor_b200/data/selector.npz, trained on R-MAT scales 18-22, ER and "
+                       "grids, not on this graph), density threshold m/20 as its fallback")
+    else:
+        opts = gg.default_opts(collect=True)
+        select_desc = "density threshold m/20"
     seq = replica_roots(roots, ws, rank, args.warmup + args.steps)
 
     # ---- warm-up ----
@@ -789,6 +803,19 @@ def run_ours(args, ws, rank, local):
     half_edges = sum(st.edges_reached for st in stats) / 2.0
     total_half_edges = sum_over_ranks(half_edges, ws)
     value = total_half_edges / (t_ms_max / 1e3) / 1e9
+    # the same steps with the density threshold alone, timed the same way
+    value_threshold = None
+    if sel is not None:
+        topts = gg.default_opts(collect=True)
+        barrier(ws)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for k in range(args.steps):
+            g.bfs_level(seq[args.warmup + k], level=lvl, host=False, opts=topts)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        t_thr = max_over_ranks(ev0.elapsed_time(ev1), ws)
+        value_threshold = total_half_edges / (t_thr / 1e3) / 1e9
     per_root = [st.edges_reached / 2.0 / (st.total_ms / 1e3) / 1e9 for st in stats]
 
     # roofline of the dominant traversal kernel (by summed kernel time): each
@@ -826,6 +853,8 @@ def run_ours(args, ws, rank, local):
     out = {}
     if rank == 0:
         out["bfs"] = {
+            "variant_selection": select_desc,
+            "value_threshold_gteps": round(value_threshold, 3) if value_threshold is not None else None,
             "gteps_mean": round(float(np.mean(per_root)), 3),
             "gteps_hmean": round(float(len(per_root) / np.sum(1.0 / np.array(per_root))), 3),
             "ms_per_root_mean": round(float(np.mean([st.total_ms for st in stats])), 4),
@@ -938,15 +967,19 @@ def run_ours(args, ws, rank, local):
         t_up = time.time()
         gh = ctx.upload(off, adj, symmetric=True)
         upload_s = time.time() - t_up
+        eopts = None
+        if sel is not None:
+            gg.attach_selector(gh, sel)
+            eopts = gg.default_opts(gg.THRESH_LEARNED)
         for k in range(min(args.warmup, 3)):
-            gh.bfs_level_host_async(seq[k], out=pins[k % 2])
+            gh.bfs_level_host_async(seq[k], out=pins[k % 2], opts=eopts)
         gh.bfs_level_host_wait()
         barrier(ws)
         t1 = time.perf_counter()
         e2e_edges = 0.0
         for k in range(args.steps):
             st = gg.RunStats()
-            gh.bfs_level_host_async(seq[args.warmup + k], out=pins[k % 2], stats=st)
+            gh.bfs_level_host_async(seq[args.warmup + k], out=pins[k % 2], opts=eopts, stats=st)
             e2e_edges += st.edges_reached / 2.0
         gh.bfs_level_host_wait()
         e2e_s = max_over_ranks(time.perf_counter() - t1, ws)
@@ -977,6 +1010,7 @@ def run_ours(args, ws, rank, local):
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "scale": args.scale, "edge_factor": EDGE_FACTOR, "n": n, "m": m,
                        "roots": NROOTS, "parallelism": f"replicas{ws}" if ws > 1 else "single",
+                       "variant_selection": "learned" if sel is not None else "threshold",
                        "l2": "graph 2.3 GB > 126 MB L2, no flush between steps",
                        "graph_build_s": round(gen_s, 2)},
             "roofline": {"bound": "hbm", "kernel": kernel_names[dom], "achieved": round(achieved, 1),
@@ -1124,6 +1158,8 @@ def main():
     ap.add_argument("--no-parity-cc-pr", action="store_true", help="reference leg: BFS only")
     ap.add_argument("--quick", action="store_true", help="BFS only (no CC/PR/e2e)")
     ap.add_argument("--no-selector", action="store_true", help="skip the learned-selector evaluation")
+    ap.add_argument("--select", default="learned", choices=["learned", "threshold"],
+                    help="variant choice of the timed BFS steps (levels are the same either way)")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-traversal measurements")
     ap.add_argument("--no-precision", action="store_true", help="skip the PageRank precision workloads")
     ap.add_argument("--batch-graphs", type=int, default=2000, help="small graphs in the union workload")
