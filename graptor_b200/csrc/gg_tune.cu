@@ -30,6 +30,7 @@ std::vector<Knob> knob_space(int analytics) {
         {"heavy_chunk", {512, 1024, 2048, 4096}, true},
     };
     if (analytics & (GG_TUNE_BFS | GG_TUNE_CC)) k.push_back({"persistent", {0, 1, 4, 5}, false});
+    if (analytics & GG_TUNE_BFS) k.push_back({"pull_split", {0, 1}, false});
     if (analytics & GG_TUNE_PR) k.push_back({"pr_stream", {0, 1}, false});
     return k;
 }
