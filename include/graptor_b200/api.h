@@ -17,6 +17,7 @@
 #define GRAPTOR_B200_API_H
 
 #include <cmath>
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -69,10 +70,27 @@ inline void check(gg_status s, const char *what) {
 }
 
 // Device writes bump this epoch; host mirrors of properties refresh on change.
-inline uint64_t &device_epoch() {
-    static uint64_t e = 1;
+// (Atomic: the analytics' host loops run on several threads.)
+inline std::atomic<uint64_t> &device_epoch() {
+    static std::atomic<uint64_t> e{1};
     return e;
 }
+inline std::mutex &host_mutex() {
+    static std::mutex m;
+    return m;
+}
+// an atomic that copies by value (members of copyable host-side handles)
+template <typename T> struct catomic {
+    std::atomic<T> v;
+    catomic(T x = T()) : v(x) {}
+    catomic(const catomic &o) : v(o.v.load()) {}
+    catomic &operator=(const catomic &o) {
+        v.store(o.v.load());
+        return *this;
+    }
+    T load() const { return v.load(); }
+    void store(T x) { v.store(x); }
+};
 
 template <typename T> struct dtype_of;
 template <> struct dtype_of<int32_t> { static constexpr gg_dtype value = GG_I32; };
@@ -90,14 +108,15 @@ inline std::map<const void *, gg_prop *> &registry() {
 
 // Host code reads and writes managed arrays (mmap_ptr) in place; before it
 // does, the device work queued since the last wait must have finished.
-inline uint64_t &synced_epoch() {
-    static uint64_t e = 0;
+inline std::atomic<uint64_t> &synced_epoch() {
+    static std::atomic<uint64_t> e{0};
     return e;
 }
 inline void host_sync() {
-    if (synced_epoch() != device_epoch() && ctx_slot()) {
+    const uint64_t d = device_epoch().load();
+    if (synced_epoch().load() != d && ctx_slot()) {
         check(gg_ctx_sync(ctx_slot()), "gg_ctx_sync");
-        synced_epoch() = device_epoch();
+        synced_epoch().store(d);
     }
 }
 
@@ -108,14 +127,15 @@ inline void host_sync() {
 // side would fault them over (or read them across the host link).
 struct managed_state {
     gg_prop *p = nullptr;
-    bool on_device = false;
-    bool touched = false;
+    std::atomic<bool> on_device{false};
+    std::atomic<bool> touched{false};
 };
 inline std::set<managed_state *> &host_touched() {
     static std::set<managed_state *> s;
     return s;
 }
 inline void host_access(managed_state *st) {
+    std::lock_guard<std::mutex> lock(host_mutex());
     host_sync();
     if (st->on_device) {
         check(gg_prop_prefetch(st->p, 0), "gg_prop_prefetch");
@@ -154,10 +174,12 @@ class GraphGPU;
 class partitioner {
 public:
     partitioner() = default;
-    partitioner(gg_graph *g, VID n) : g_(g), n_(n) {}
+    // np: host-side partitions of the vertex range (the driver's -c); the
+    // device does not partition
+    partitioner(gg_graph *g, VID n, int np = 1) : g_(g), n_(n), np_(np > 0 ? np : 1) {}
     VID get_num_vertices() const { return n_; }
     VID get_num_elements() const { return n_ * scale_; }
-    int get_num_partitions() const { return 1; }
+    int get_num_partitions() const { return np_; }
     // scale(k): the partitioning of k consecutive elements per vertex
     // (graph/partitioning.h); arrays allocated from it hold n*k elements
     partitioner scale(VID k) const {
@@ -166,13 +188,15 @@ public:
         return p;
     }
     VID get_scale() const { return scale_; }
-    // the vertex range of partition k (one partition: [0, n))
-    VID start_of(int k) const { return k <= 0 ? 0 : n_; }
+    // the vertex range of partition k: [start_of(k), end_of(k))
+    VID start_of(int k) const { return k <= 0 ? 0 : (k >= np_ ? n_ : (VID)((uint64_t)k * n_ / np_)); }
+    VID end_of(int k) const { return start_of(k + 1); }
     gg_graph *graph() const { return g_; }
 
 private:
     gg_graph *g_ = nullptr;
     VID n_ = 0;
+    int np_ = 1;
     VID scale_ = 1;
 };
 
@@ -212,7 +236,6 @@ public:
     // partition count and vector length do not apply to the device layout.
     template <typename CSx, typename = decltype(std::declval<const CSx &>().getIndex())>
     explicit GraphGPU(const CSx &G, int npart = 0, int maxVL = 0) {
-        (void)npart;
         (void)maxVL;
         gg_graph *g = nullptr;
         graptor_b200::check(gg_graph_upload(graptor_b200::context(), (uint32_t)G.numVertices(),
@@ -221,6 +244,7 @@ public:
                             "gg_graph_upload");
         g_ = g;
         init();
+        if (npart > 0) part_ = partitioner(g_, n_, npart);
     }
     static GraphGPU read_bin(const std::string &path, bool symmetric) {
         gg_graph *g = nullptr;
@@ -1055,10 +1079,15 @@ public:
     // host read (vertexprop::operator[](VID)): served from a host mirror
     // refreshed when the device has written since the last read
     T operator[](VID v) const {
-        if (mirror_epoch_ != graptor_b200::device_epoch() || mirror_.size() != n_) {
-            mirror_.resize(n_);
-            graptor_b200::check(gg_prop_download(p_, mirror_.data()), "gg_prop_download");
-            mirror_epoch_ = graptor_b200::device_epoch();
+        if (mirror_epoch_.load() != graptor_b200::device_epoch().load() || mirror_n_.load() != n_) {
+            std::lock_guard<std::mutex> lock(graptor_b200::host_mutex());
+            const uint64_t e = graptor_b200::device_epoch().load();
+            if (mirror_epoch_.load() != e || mirror_n_.load() != n_) {
+                mirror_.resize(n_);
+                graptor_b200::check(gg_prop_download(p_, mirror_.data()), "gg_prop_download");
+                mirror_n_.store(n_);
+                mirror_epoch_.store(e);
+            }
         }
         return mirror_[v];
     }
@@ -1077,7 +1106,8 @@ private:
     gg_prop *p_ = nullptr;
     VID n_ = 0;
     mutable std::vector<T> mirror_;
-    mutable uint64_t mirror_epoch_ = 0;
+    mutable graptor_b200::catomic<uint64_t> mirror_epoch_{0};
+    mutable graptor_b200::catomic<VID> mirror_n_{0};
 };
 
 // ---------------------------------------------------------------------------

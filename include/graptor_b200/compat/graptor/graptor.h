@@ -201,33 +201,47 @@ template <graptor_mode_t Mode> struct GraphVEBOGraptor : GraphGPU {
 };
 
 // Host loops over the vertices (map_vertexL, legacy/parallel loops); the
-// functors are host code, as in the reference.
+// functors are host code, as in the reference, and run on the host's threads
+// where the program is built with OpenMP (the reference runs them in
+// parallel too).
 template <typename Fn> void map_vertexL(const partitioner &part, Fn fn) {
     graptor_b200::host_sync();
-    for (VID v = 0, n = part.get_num_vertices(); v < n; ++v) fn(v);
+    const int64_t n = part.get_num_vertices();
+#pragma omp parallel for schedule(static)
+    for (int64_t v = 0; v < n; ++v) fn((VID)v);
 }
 // map_vertex_serialL: the same loop, in vertex order (the reference runs it
 // serially for repeatable random draws, FMv.C:291-298)
-template <typename Fn> void map_vertex_serialL(const partitioner &part, Fn fn) { map_vertexL(part, fn); }
+template <typename Fn> void map_vertex_serialL(const partitioner &part, Fn fn) {
+    graptor_b200::host_sync();
+    for (VID v = 0, n = part.get_num_vertices(); v < n; ++v) fn(v);
+}
 // map_partitionL(part, fn(k)): fn per partition (one partition on the device)
 template <typename Fn> void map_partitionL(const partitioner &part, Fn fn) {
     graptor_b200::host_sync();
-    for (int k = 0, p = part.get_num_partitions(); k < p; ++k) fn((unsigned)k);
+    const int p = part.get_num_partitions();
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < p; ++k) fn((unsigned)k);
 }
 // vertexMap(part, F, functor): a host functor over the vertices of F
 // (legacy vertexMap with a C++ functor, APRv.C:500)
 template <typename F> void vertexMap(const partitioner &part, const frontier &Fr, F fn) {
     graptor_b200::host_sync();
     if (Fr.all()) {
-        for (VID v = 0, n = part.get_num_vertices(); v < n; ++v) fn(v);
+        const int64_t n = part.get_num_vertices();
+#pragma omp parallel for schedule(static)
+        for (int64_t v = 0; v < n; ++v) fn((VID)v);
     } else {
         const VID *l = Fr.getSparse();
-        for (VID i = 0, k = Fr.nActiveVertices(); i < k; ++i) fn(l[i]);
+        const int64_t k = Fr.nActiveVertices();
+#pragma omp parallel for schedule(static)
+        for (int64_t i = 0; i < k; ++i) fn(l[i]);
     }
 }
 template <typename I, typename Fn> void parallel_loop(I lo, I hi, Fn fn) {
     graptor_b200::host_sync();
-    for (I i = lo; i < hi; ++i) fn(i);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = (int64_t)lo; i < (int64_t)hi; ++i) fn((I)i);
 }
 
 // vertexFilter(GA, V, functor) (dsl/vmap_utils.h:62-72): the vertices of V
