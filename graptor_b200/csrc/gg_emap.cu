@@ -81,6 +81,9 @@ struct EmapArgs {
     // in-edges are appended here for the second pass (graph-driven BFS)
     uint32_t *rest_out;
     unsigned long long *rest_out_n;
+    // bitwise-or pulls: rows with more in-edges than this are left to the
+    // heavy-row chunk kernels (0: none)
+    uint32_t heavy_T;
 };
 
 template <int R>
@@ -255,6 +258,10 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
             }
         }
         bool act = valid && op.dst_ok(best);
+        if constexpr (R == GG_RELAX_OR_U32) {
+            // a bitwise-or row has no early exit: long rows go to k_or_heavy_chunks
+            if (A.heavy_T && act && (lazy ? (uint64_t)f2.z : end - e) > A.heavy_T) act = false;
+        }
         bool changed = false;
         uint64_t beg = e;
         if (PASS == 2) e += 2;  // the first pass took the first two edges
@@ -417,6 +424,57 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
 template <int R, bool SRCF, bool CAND, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
     pull_body<R, SRCF, CAND, BLOCK>(A, op);
+}
+
+// Bitwise-or pulls over the long rows (FMv's all-source steps): a warp per
+// chunk of a heavy row (the CSC's heavy-row chunk table) ORs its sources'
+// bits, four edges per lane in flight, and merges them into the row's value
+// with one atomicOr; then a thread per heavy row records it (NE_PREV: its
+// value differs from prev) into the output frontier.
+template <bool SRCF>
+__global__ void __launch_bounds__(256) k_or_heavy_chunks(EmapArgs A, Op<GG_RELAX_OR_U32> op, HeavyRows H) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < H.nchunks; c += nw) {
+        const uint32_t lo = H.crow[c];
+        const uint32_t d = H.v[lo];
+        const uint32_t cur = *(volatile const uint32_t *)(op.a + d);
+        if (!op.dst_ok(cur)) continue;  // the same row for the whole warp
+        const uint64_t rb = A.in_off[d], re = A.in_off[d + 1];
+        const uint64_t e0 = rb + (c - H.first[lo]) * H.CH;
+        const uint64_t e1 = min(e0 + H.CH, re);
+        uint32_t acc = 0;
+        for (uint64_t base = e0; base < e1; base += 128) {
+            uint32_t sv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint64_t e = base + j * 32 + lane;
+                sv[j] = e < e1 ? __ldg(A.in_adj + e) : 0xFFFFFFFFu;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (sv[j] != 0xFFFFFFFFu && (!SRCF || dev::bit_test(A.in_bits, sv[j]))) acc |= op.b[sv[j]];
+        }
+        acc = __reduce_or_sync(FULL, acc);
+        if (lane == 0 && (cur | acc) != cur) atomicOr(op.a + d, acc);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_or_heavy_finalize(EmapArgs A, Op<GG_RELAX_OR_U32> op, HeavyRows H) {
+    unsigned long long nv = 0, ne = 0;
+    const uint32_t nth = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < H.nheavy; i0 += nth) {
+        const uint32_t i = i0 + threadIdx.x;
+        bool rec = false;
+        uint32_t d = 0;
+        if (i < H.nheavy) {
+            d = H.v[i];
+            rec = A.record == GG_RECORD_NE_PREV && op.a[d] != op.prev[d];
+        }
+        if (rec && A.out_bits) atomicOr(A.out_bits + (d >> 5), 1u << (d & 31));
+        if (A.out_b0) emit_out(A, rec, d, nv, ne);
+    }
+    if (A.out_cnt) flush_counts<256>(A, nv, ne, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -860,6 +918,10 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
             }
             if (A.cand && A.out_bits) GG_CUDA(ctx, cudaMemsetAsync(A.out_bits, 0, words * 4, st));
         }
+        if constexpr (R == GG_RELAX_OR_U32) {
+            if (g->heavy.nchunks && (d->record == GG_RECORD_NE_PREV || d->record == GG_RECORD_NONE))
+                A.heavy_T = g->heavy.T;
+        }
         const uint64_t items = (A.cand && cl->host_n != UINT64_MAX) ? cl->host_n : (uint64_t)g->n;
         const void *kp = A.cand ? (all_in ? (const void *)k_pull<R, false, true, kBlock>
                                           : (const void *)k_pull<R, true, true, kBlock>)
@@ -875,6 +937,19 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
             else k_pull<R, true, false, kBlock><<<grid, kBlock, 0, st>>>(A, op);
         }
         GG_LAUNCHED(ctx);
+        if constexpr (R == GG_RELAX_OR_U32) {
+            if (A.heavy_T) {
+                const HeavyRows &H = g->heavy;
+                const unsigned cap = (unsigned)(ctx->sm_count * 8);
+                const unsigned cb = (unsigned)std::min<uint64_t>((H.nchunks * 32 + 255) / 256, cap);
+                if (all_in) k_or_heavy_chunks<false><<<cb, 256, 0, st>>>(A, op, H);
+                else k_or_heavy_chunks<true><<<cb, 256, 0, st>>>(A, op, H);
+                GG_LAUNCHED(ctx);
+                const unsigned fb = (unsigned)std::min<uint64_t>((H.nheavy + 255) / 256, cap);
+                k_or_heavy_finalize<<<fb ? fb : 1, 256, 0, st>>>(A, op, H);
+                GG_LAUNCHED(ctx);
+            }
+        }
         if (cl) {
             cl->cur ^= 1;
             cl->valid = true;

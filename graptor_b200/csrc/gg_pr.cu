@@ -694,68 +694,43 @@ static gg_status gather_api(gg_graph *g, const gg_emap_desc *d) {
 }
 
 // ADD_GATHER with a source frontier (APRv.C:477-487, api::filter(F, strong,
-// src)): y[d] += sum over in-edges (s, d) with s in F of contrib[s].  A warp
-// per 32-vertex word walks the word's rows one after the other, the lanes
-// striding each row and testing the frontier bitmap; rows without an active
-// source keep y.  Float sums (APRv's FloatTy) or double sums (accum_f64).
-template <typename T, typename Acc>
-__global__ void __launch_bounds__(256)
-k_gather_src_bits(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj,
-                  const T *__restrict__ contrib, const uint32_t *__restrict__ bits, uint32_t n,
-                  float *__restrict__ y_f32, double *__restrict__ y_f64) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t nwords = (n + 31u) >> 5;
-    const uint32_t nw = (gridDim.x * 256u) >> 5;
-    for (uint32_t w = (blockIdx.x * 256u + threadIdx.x) >> 5; w < nwords; w += nw) {
-        Acc mine = 0;
-        bool any_mine = false;
-        for (uint32_t j = 0; j < 32; ++j) {
-            const uint32_t d = (w << 5) + j;
-            if (d >= n) break;
-            const uint64_t beg = in_off[d], end = in_off[d + 1];
-            Acc part = 0;
-            bool any = false;
-            for (uint64_t e = beg + lane; e < end; e += 32) {
-                const uint32_t s = __ldg(in_adj + e);
-                if (dev::bit_test(bits, s)) {
-                    part += (Acc)contrib[s];
-                    any = true;
-                }
-            }
-            part = dev::warp_sum(part);
-            any = __any_sync(FULL, any);
-            if (lane == j) {
-                mine = part;
-                any_mine = any;
-            }
-        }
-        const uint32_t d = (w << 5) + lane;
-        if (d < n && any_mine) {
-            if (y_f64) y_f64[d] += (double)mine;
-            else y_f32[d] = (float)((double)y_f32[d] + (double)mine);
-        }
-    }
+// src)): y[d] += sum over in-edges (s, d) with s in F of contrib[s].  The
+// contributions of the vertices outside F are masked to zero in a scratch
+// copy (one pass over n values), which the regular gather then sums: its
+// light-row streaming and heavy-row chunks keep every warp busy whatever
+// the degree mix.
+template <typename T>
+__global__ void k_mask_contrib(const T *__restrict__ contrib, const uint32_t *__restrict__ bits, uint32_t n,
+                               T *__restrict__ out) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        out[v] = dev::bit_test(bits, v) ? contrib[v] : (T)0;
 }
 
 static gg_status gather_src_filtered(gg_graph *g, const gg_emap_desc *d, gg_frontier *in) {
     gg_ctx *ctx = g->ctx;
+    const bool f64 = d->src->t == GG_F64;
+    if (!(d->src->t == GG_F32 || (f64 && d->accum_f64)))
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "a source-filtered ADD_GATHER takes F32 or F64 contributions");
     GG_CHECK(frontier_ensure_bitmap(in));
     float *yf = d->a->t == GG_F32 ? (float *)d->a->d : nullptr;
     double *yd = d->a->t == GG_F64 ? (double *)d->a->d : nullptr;
+    // scratch: the masked contributions, then the heavy rows' partial sums
+    const size_t esz = f64 ? 8 : 4;
+    const size_t cb = (((size_t)g->n + 1) * esz + 255) / 256 * 256;
+    void *base = nullptr;
+    GG_CHECK(graph_scratch(g, cb + (g->heavy.nchunks + 1) * 8, &base));
+    void *partial = (char *)base + cb;
     const unsigned grid = pr_grid(ctx, g->n);
-    if (d->src->t == GG_F32 && !d->accum_f64)
-        k_gather_src_bits<float, float><<<grid, 256, 0, ctx->stream>>>(g->in_off, g->in_adj, (const float *)d->src->d,
-                                                                     in->bitmap, g->n, yf, yd);
-    else if (d->src->t == GG_F32)
-        k_gather_src_bits<float, double><<<grid, 256, 0, ctx->stream>>>(g->in_off, g->in_adj, (const float *)d->src->d,
-                                                                      in->bitmap, g->n, yf, yd);
-    else if (d->src->t == GG_F64 && d->accum_f64)
-        k_gather_src_bits<double, double><<<grid, 256, 0, ctx->stream>>>(
-            g->in_off, g->in_adj, (const double *)d->src->d, in->bitmap, g->n, yf, yd);
-    else
-        return set_error(ctx, GG_ERR_UNSUPPORTED, "a source-filtered ADD_GATHER takes F32 or F64 contributions");
+    if (f64) {
+        k_mask_contrib<double><<<grid, 256, 0, ctx->stream>>>((const double *)d->src->d, in->bitmap, g->n,
+                                                              (double *)base);
+        GG_LAUNCHED(ctx);
+        return gather_launch<GG_F64, true, true>(g, (const double *)base, yf, yd, nullptr, 1.0f, partial);
+    }
+    k_mask_contrib<float><<<grid, 256, 0, ctx->stream>>>((const float *)d->src->d, in->bitmap, g->n, (float *)base);
     GG_LAUNCHED(ctx);
-    return GG_OK;
+    if (d->accum_f64) return gather_launch<GG_F32, true, true>(g, (const float *)base, yf, yd, nullptr, 1.0f, partial);
+    return gather_launch<GG_F32, false, true>(g, (const float *)base, yf, yd, nullptr, 1.0f, partial);
 }
 
 gg_status pr_edgemap_gather(gg_graph *g, const gg_emap_desc *d, gg_frontier *in) {

@@ -399,9 +399,10 @@ public:
         frontier f;
         f.kind_ = K_DENSE;
         f.n_ = part.get_num_vertices();
+        // device memory: vertex programs write it, calculateActiveCounts()
+        // reads it; host code reads a frontier through getSparse / getDenseL
         gg_prop *p = nullptr;
-        graptor_b200::check(gg_prop_create_managed(part.graph(), W == 4 ? GG_U32 : GG_U8, &p),
-                            "gg_prop_create_managed");
+        graptor_b200::check(gg_prop_create(part.graph(), W == 4 ? GG_U32 : GG_U8, &p), "gg_prop_create");
         const uint32_t zero = 0;
         graptor_b200::check(gg_prop_fill(p, &zero), "gg_prop_fill");
         void *d = nullptr;
