@@ -1167,15 +1167,16 @@ static gg_status check_relax(gg_graph *g, const gg_emap_desc *d, gg_frontier *in
 }
 
 // Maximal independent set step (MISv.C:235-255 with the dfsaop_MIS
-// relation of dsl/ast/dfsaop.h:49-230): a warp per 32-vertex word of the
-// destination set walks each destination's in-row, the lanes striding it.
-// Over its in-edges (s, d), s != d: d becomes out (2) when some s is in (3);
-// else a conditionally-in (1) d becomes undecided (0) when some s < d is
-// undecided or conditionally in.  The relation is order-independent per d;
-// states of sources that change during the step are read as the reference's
-// parallel step reads them, before or after the change (either way the
-// rounds converge to the same set: the greedy one in vertex-id order).
-// Recorded (EQ_ZERO): the destinations left undecided.
+// relation of dsl/ast/dfsaop.h:49-230).  Over its in-edges (s, d), s != d:
+// d becomes out (2) when some s is in (3); else a conditionally-in (1) d
+// becomes undecided (0) when some s < d is undecided or conditionally in.
+// The relation is order-independent per d; states of sources that change
+// during the step are read as the reference's parallel step reads them,
+// before or after the change (either way the rounds converge to the same
+// set: the greedy one in vertex-id order).  A lane per destination of a
+// 32-vertex word walks its first 32 in-edges, four loads in flight, and stops
+// at an in source; the rest of longer rows is walked by the whole warp, one
+// row after the other.  Recorded (EQ_ZERO): the destinations left undecided.
 __global__ void __launch_bounds__(kBlock) k_mis(EmapArgs A, uint8_t *__restrict__ st,
                                                 const uint32_t *__restrict__ dst_bits) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -1183,34 +1184,64 @@ __global__ void __launch_bounds__(kBlock) k_mis(EmapArgs A, uint8_t *__restrict_
     const uint32_t nw = (gridDim.x * kBlock) >> 5;
     unsigned long long nv = 0, ne = 0, sc = 0;
     for (uint32_t w = (blockIdx.x * kBlock + threadIdx.x) >> 5; w < nwords; w += nw) {
-        const uint32_t valid = (w + 1) * 32u <= A.n ? FULL : ((1u << (A.n & 31u)) - 1u);
-        uint32_t todo = (dst_bits ? dst_bits[w] : FULL) & valid;
-        bool rec = false;
-        while (todo) {
-            const uint32_t j = __ffs(todo) - 1;
-            todo &= todo - 1;
-            const uint32_t d = (w << 5) + j;
-            const uint8_t old = st[d];
-            const uint64_t beg = A.in_off[d], end = A.in_off[d + 1];
-            bool in = false, low = false;
-            for (uint64_t e = beg + lane; e < end; e += 32) {
-                const uint32_t s = A.in_adj[e];
-                if (s == d) continue;
-                const uint8_t u = *(volatile const uint8_t *)(st + s);
-                in |= u == 3;
-                low |= s < d && u < 2;
-            }
-            in = __any_sync(FULL, in);
-            low = __any_sync(FULL, low);
-            const uint8_t nwv = in ? 2 : ((old == 1 && low) ? 0 : old);
-            if (lane == 0) {
-                if (nwv != old) st[d] = nwv;
-                sc += end - beg;
-            }
-            if (lane == j) rec = nwv == 0;
-        }
         const uint32_t d = (w << 5) + lane;
-        rec = rec && A.record == GG_RECORD_EQ_ZERO;
+        const bool act = d < A.n && (!dst_bits || ((dst_bits[w] >> lane) & 1u));
+        uint8_t old = 0;
+        uint64_t e = 0, end = 0;
+        if (act) {
+            old = st[d];
+            e = A.in_off[d];
+            end = A.in_off[d + 1];
+        }
+        const uint64_t beg = e;
+        bool in = false, low = false;
+        const uint64_t lim = min(end, e + 32);
+        while (e < lim && !in) {
+            uint32_t sv[4];
+            const int cnt = (int)min((uint64_t)4, lim - e);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) sv[j] = j < cnt ? __ldg(A.in_adj + e + j) : d;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (sv[j] == d) continue;  // self loop or unused slot
+                const uint8_t u = *(volatile const uint8_t *)(st + sv[j]);
+                in |= u == 3;
+                low |= sv[j] < d && u < 2;
+            }
+            e += cnt;
+        }
+        unsigned pend = __ballot_sync(FULL, act && !in && e < end);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint32_t dj = (w << 5) + j;
+            const uint64_t ej = __shfl_sync(FULL, e, j), endj = __shfl_sync(FULL, end, j);
+            bool inj = false, lowj = false;
+            for (uint64_t base = ej; base < endj && !inj; base += 32) {
+                bool hi = false, lo = false;
+                if (base + lane < endj) {
+                    const uint32_t s = __ldg(A.in_adj + base + lane);
+                    if (s != dj) {
+                        const uint8_t u = *(volatile const uint8_t *)(st + s);
+                        hi = u == 3;
+                        lo = s < dj && u < 2;
+                    }
+                }
+                inj = __any_sync(FULL, hi);
+                lowj = lowj || __any_sync(FULL, lo);
+            }
+            if ((int)lane == j) {
+                in = in || inj;
+                low = low || lowj;
+            }
+        }
+        bool rec = false;
+        if (act) {
+            const uint8_t nwv = in ? 2 : ((old == 1 && low) ? 0 : old);
+            if (nwv != old) st[d] = nwv;
+            rec = nwv == 0 && A.record == GG_RECORD_EQ_ZERO;
+            sc += end - beg;
+        }
         if (A.out_bits) {
             const unsigned bits = __ballot_sync(FULL, rec);
             if (lane == 0) A.out_bits[w] = bits;

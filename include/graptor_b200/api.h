@@ -157,6 +157,25 @@ inline void before_device() {
     t.clear();
 }
 
+// Dense frontier arrays (frontier::dense) released by one iteration are kept
+// for the next one's (an allocation and a free, which waits for the device,
+// per iteration otherwise); a graph's are freed with the graph.
+inline std::map<std::pair<gg_graph *, int>, std::vector<gg_prop *>> &dense_pool() {
+    static std::map<std::pair<gg_graph *, int>, std::vector<gg_prop *>> p;
+    return p;
+}
+inline void dense_pool_release(gg_graph *g) {
+    auto &pool = dense_pool();
+    for (auto it = pool.begin(); it != pool.end();) {
+        if (it->first.first == g) {
+            for (gg_prop *q : it->second) gg_prop_destroy(q);
+            it = pool.erase(it);
+        } else {
+            ++it;
+        }
+    }
+}
+
 // The graph that frontiers made from host vertex lists (frontier::sparse)
 // belong to: the last graph built, as the analytics use one graph at a time.
 inline gg_graph *&default_graph() {
@@ -297,6 +316,7 @@ public:
     // the layout has no partition fragments to report (GraphVEBOGraptor::fragmentation)
     void fragmentation() const {}
     void del() {
+        if (g_) graptor_b200::dense_pool_release(g_);
         if (csr_ && csr_->degp_) {
             graptor_b200::registry().erase((const void *)csr_->deg_);
             gg_prop_destroy(csr_->degp_);
@@ -401,16 +421,24 @@ public:
         f.n_ = part.get_num_vertices();
         // device memory: vertex programs write it, calculateActiveCounts()
         // reads it; host code reads a frontier through getSparse / getDenseL
+        const int dt = W == 4 ? GG_U32 : GG_U8;
+        auto key = std::make_pair(part.graph(), dt);
+        auto &free_list = graptor_b200::dense_pool()[key];
         gg_prop *p = nullptr;
-        graptor_b200::check(gg_prop_create(part.graph(), W == 4 ? GG_U32 : GG_U8, &p), "gg_prop_create");
+        if (!free_list.empty()) {
+            p = free_list.back();
+            free_list.pop_back();
+        } else {
+            graptor_b200::check(gg_prop_create(part.graph(), (gg_dtype)dt, &p), "gg_prop_create");
+        }
         const uint32_t zero = 0;
         graptor_b200::check(gg_prop_fill(p, &zero), "gg_prop_fill");
         void *d = nullptr;
         gg_prop_device_ptr(p, &d);
         graptor_b200::registry()[d] = p;
-        f.dense_store_ = std::shared_ptr<gg_prop>(p, [d](gg_prop *q) {
+        f.dense_store_ = std::shared_ptr<gg_prop>(p, [d, key](gg_prop *q) {
             graptor_b200::registry().erase(d);
-            gg_prop_destroy(q);
+            graptor_b200::dense_pool()[key].push_back(q);
         });
         return f;
     }
