@@ -1173,7 +1173,8 @@ static gg_status check_relax(gg_graph *g, const gg_emap_desc *d, gg_frontier *in
 // The relation is order-independent per d; states of sources that change
 // during the step are read as the reference's parallel step reads them,
 // before or after the change (either way the rounds converge to the same
-// set: the greedy one in vertex-id order).  A lane per destination of a
+// set: the greedy one in vertex-id order); the loads bypass L1 (ld.global.cg)
+// so that they see other SMs' changes as soon as L2 does.  A lane per destination of a
 // 32-vertex word walks its first 32 in-edges, four loads in flight, and stops
 // at an in source; the rest of longer rows is walked by the whole warp, one
 // row after the other.  Recorded (EQ_ZERO): the destinations left undecided.
@@ -1204,7 +1205,7 @@ __global__ void __launch_bounds__(kBlock) k_mis(EmapArgs A, uint8_t *__restrict_
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (sv[j] == d) continue;  // self loop or unused slot
-                const uint8_t u = *(volatile const uint8_t *)(st + sv[j]);
+                const uint8_t u = __ldcg(st + sv[j]);
                 in |= u == 3;
                 low |= sv[j] < d && u < 2;
             }
@@ -1222,7 +1223,7 @@ __global__ void __launch_bounds__(kBlock) k_mis(EmapArgs A, uint8_t *__restrict_
                 if (base + lane < endj) {
                     const uint32_t s = __ldg(A.in_adj + base + lane);
                     if (s != dj) {
-                        const uint8_t u = *(volatile const uint8_t *)(st + s);
+                        const uint8_t u = __ldcg(st + s);
                         hi = u == 3;
                         lo = s < dj && u < 2;
                     }
