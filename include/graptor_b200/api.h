@@ -264,6 +264,9 @@ public:
         g_ = g;
         init();
         if (npart > 0) part_ = partitioner(g_, n_, npart);
+        // the host CSR the device graph was built from (the same rows in the
+        // same order): getCSR() serves it without a download
+        make_csr_view((const EID *)G.getIndex(), (const VID *)G.getEdges());
     }
     static GraphGPU read_bin(const std::string &path, bool symmetric) {
         gg_graph *g = nullptr;
@@ -288,14 +291,25 @@ public:
     VID getOutDegree(VID v) const { return getCSR().getDegree(v); }
     // The CSR in host memory, fetched once on first use.
     const GraphCSxView &getCSR() const {
-        if (!csr_) {
+        if (!csr_) make_csr_view(nullptr, nullptr);
+        return *csr_;
+    }
+    // host CSR view: copied from off/adj, or downloaded from the device
+    void make_csr_view(const EID *off, const VID *adj) const {
+        {
             auto c = std::make_shared<GraphCSxView>();
             c->n_ = n_;
             c->m_ = m_;
             c->sym_ = sym_ != 0;
-            c->off_.resize((size_t)n_ + 1);
-            c->adj_.resize(m_ ? m_ : 1);
-            graptor_b200::check(gg_graph_download(g_, c->off_.data(), c->adj_.data()), "gg_graph_download");
+            if (off && adj) {
+                c->off_.assign(off, off + (size_t)n_ + 1);
+                c->adj_.assign(adj, adj + (size_t)m_);
+                if (c->adj_.empty()) c->adj_.resize(1);
+            } else {
+                c->off_.resize((size_t)n_ + 1);
+                c->adj_.resize(m_ ? m_ : 1);
+                graptor_b200::check(gg_graph_download(g_, c->off_.data(), c->adj_.data()), "gg_graph_download");
+            }
             graptor_b200::check(gg_prop_create_managed(g_, GG_U32, &c->degp_), "gg_prop_create_managed");
             void *d = nullptr;
             gg_prop_device_ptr(c->degp_, &d);
@@ -306,7 +320,6 @@ public:
             graptor_b200::registry()[d] = c->degp_;
             csr_ = c;
         }
-        return *csr_;
     }
     const GraphCSxView &getCSC() const { return getCSR(); }
     // no vertex renumbering on the device: ids are the file's ids
