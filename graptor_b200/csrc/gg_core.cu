@@ -786,6 +786,7 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "bin_medium_max") t.bin_medium_max = (uint32_t)v;
     else if (k == "pull_k" && v >= 1 && v <= 1024) t.pull_k = (int)v;
     else if (k == "pull_split" && (v == 0 || v == 1)) t.pull_split = (int)v;
+    else if (k == "graph_flat" && (v == 0 || v == 1)) t.graph_flat = (int)v;
     else if (k == "pull_first" && v <= 2) t.pull_first = (int)v;
     else if (k == "push_k" && v >= 1 && v <= 1024) t.push_k = (int)v;
     else if (k == "heavy_deg" && v >= 32) t.heavy_deg = (uint32_t)v;
@@ -818,6 +819,7 @@ gg_status gg_tuning_get(const char *name, int64_t *v) {
     else if (k == "bin_medium_max") *v = t.bin_medium_max;
     else if (k == "pull_k") *v = t.pull_k;
     else if (k == "pull_split") *v = t.pull_split;
+    else if (k == "graph_flat") *v = t.graph_flat;
     else if (k == "pull_first") *v = t.pull_first;
     else if (k == "push_k") *v = t.push_k;
     else if (k == "heavy_deg") *v = t.heavy_deg;

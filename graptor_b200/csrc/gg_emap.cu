@@ -1568,6 +1568,8 @@ struct GCtl {
     const uint4 *first_in;
     int lazy_off;
     int split;                        // pulls in two passes (pull_body PASS 1 / 2)
+    int flat;                         // the loop body is one chain of kernels (no step conditionals)
+    int need_chunks;                  // this push step needs k_g_chunks
     uint32_t *rest;                   // split pull: the second pass's rows
     unsigned long long rest_n;
     const uint32_t *nonisolated;
@@ -1668,10 +1670,12 @@ __device__ void decide_step(GCtl *c) {
         c->handed_off = nactv != 0 && iter < c->max_iters;
         c->variant = -1;
         c->iterations = iter;
-        cudaGraphSetConditional(c->h_push, 2u);  // the step switch: no body
-        cudaGraphSetConditional(c->h_list, 0);
-        cudaGraphSetConditional(c->h_bits, 0);
-        cudaGraphSetConditional(c->h_chunks, 0);
+        if (!c->flat) {
+            cudaGraphSetConditional(c->h_push, 2u);  // the step switch: no body
+            cudaGraphSetConditional(c->h_list, 0);
+            cudaGraphSetConditional(c->h_bits, 0);
+            cudaGraphSetConditional(c->h_chunks, 0);
+        }
         cudaGraphSetConditional(c->h_while, 0);
         return;
     }
@@ -1777,11 +1781,14 @@ __device__ void decide_step(GCtl *c) {
     // a large bin too big for a CTA's shared table gets its chunk prefix from
     // k_g_chunks (its size is known here unless the list is still to be built)
     const bool chunks = push && (c->need_list || F.cnt[FC_BIN2] > kLargeLocal);
-    cudaGraphSetConditional(c->h_chunks, chunks ? 1u : 0u);
+    c->need_chunks = chunks;
     c->need_bitmap = !push && !c->has_bitmap[c->cur];
-    cudaGraphSetConditional(c->h_push, push ? 0u : 1u);  // the step switch: push or pull body
-    cudaGraphSetConditional(c->h_list, c->need_list ? 1u : 0u);
-    cudaGraphSetConditional(c->h_bits, c->need_bitmap ? 1u : 0u);
+    if (!c->flat) {
+        cudaGraphSetConditional(c->h_chunks, chunks ? 1u : 0u);
+        cudaGraphSetConditional(c->h_push, push ? 0u : 1u);  // the step switch: push or pull body
+        cudaGraphSetConditional(c->h_list, c->need_list ? 1u : 0u);
+        cudaGraphSetConditional(c->h_bits, c->need_bitmap ? 1u : 0u);
+    }
     cudaGraphSetConditional(c->h_while, 1u);
 }
 
@@ -1988,6 +1995,7 @@ __device__ void g_bookkeep(GCtl *c) {
 __global__ void __launch_bounds__(1024) k_g_chunks(GCtl *c) {
     __shared__ unsigned long long s_warp[32];
     __shared__ unsigned long long s_base;
+    if (c->variant != GG_VAR_PUSH_SPARSE || !c->need_chunks) return;
     const GFront F = c->f[c->cur];
     const uint64_t c2 = F.cnt[FC_BIN2];
     if (c2 <= kLargeLocal || c2 + 1 > c->chunk_cap) return;  // use_first stays 0: warp rows
@@ -2044,6 +2052,7 @@ struct GraphBfs {
     uint32_t *rest = nullptr;  // split pull: second-pass rows (n entries)
     uint64_t rest_cap = 0;
     unsigned push_grid = 0, pull_grid = 0, vgrid = 0;
+    int flat = 0;  // built as one chain of kernels per step (knob graph_flat)
     // page-locked host copies of the control block: the configuration sent
     // before a run, and the records a kernel writes back after it through the
     // mapping (no copy-engine transfer: a run's records do not queue behind
@@ -2117,12 +2126,36 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     //                                           pull: IF bits {tobitmap} -> pull } -> next (clear + decision) }
     // The branch handles keep the value the decision set (no default
     // assignment); the loop handle starts at 1 on every launch.
-    cudaGraphConditionalHandle hw, hp, hq, hl, hb, hc;
+    cudaGraphConditionalHandle hw, hp = 0, hq = 0, hl = 0, hb = 0, hc = 0;
     GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hw, G, 1, cudaGraphCondAssignDefault));
     cudaGraphNode_t n_init, n_while;
     GG_CHECK(add_kernel(ctx, G, &n_init, nullptr, 0, (const void *)k_g_init, gb->vgrid, 256, arg));
     cudaGraph_t body;
     GG_CHECK(add_cond(ctx, G, &n_while, &n_init, 1, hw, cudaGraphCondTypeWhile, &body));
+    gb->flat = tuning().graph_flat;
+    if (gb->flat) {
+        // WHILE { tolist -> chunks -> push -> tobitmap -> pull -> pull2 -> next }: every
+        // kernel returns at once when the step does not need it.  A conditional
+        // node costs several times an idle kernel's launch inside the loop
+        // (measured on B200: SWITCH about 6.7 us, IF about 2.4 us, an idle
+        // kernel about 0.9 us per iteration).
+        const void *chain[] = {(const void *)k_g_tolist, (const void *)k_g_chunks, (const void *)k_g_push,
+                               (const void *)k_g_tobitmap, (const void *)k_g_pull, (const void *)k_g_pull2,
+                               (const void *)k_g_next};
+        const unsigned grids[] = {gb->vgrid, 1, gb->push_grid, gb->vgrid, gb->pull_grid, gb->pull_grid,
+                                  (unsigned)ctx->sm_count * 2};
+        const unsigned blocks[] = {256, 1024, kBlock, 256, kBlock, kBlock, 256};
+        cudaGraphNode_t prev = nullptr;
+        for (int i = 0; i < 7; ++i) {
+            cudaGraphNode_t nd;
+            GG_CHECK(add_kernel(ctx, body, &nd, prev ? &prev : nullptr, prev ? 1 : 0, chain[i], grids[i], blocks[i], arg));
+            prev = nd;
+        }
+        GG_CUDA(ctx, cudaGraphInstantiate(&gb->exec, G, 0));
+        cudaGraphConditionalHandle hs[6] = {hw, hp, hq, hl, hb, hc};
+        GG_CUDA(ctx, cudaMemcpyAsync(&ctl->h_while, hs, sizeof(hs), cudaMemcpyHostToDevice, ctx->stream));
+        return GG_OK;
+    }
     // one SWITCH picks the step: body 0 push, body 1 pull, 2 none (h_pull
     // is the same handle)
     GG_CUDA(ctx, cudaGraphConditionalHandleCreate(&hp, body, 0, 0));
@@ -2171,6 +2204,10 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
         }
     }
     GraphBfs *gb = (GraphBfs *)g->gbfs;
+    if (gb->flat != tuning().graph_flat) {  // built for the other loop shape
+        graph_bfs_free(g);
+        return graph_bfs_level(g, root, opt, level, prev, st, iters_out);
+    }
     for (auto &f : g->tmp_front)
         if (!f) GG_CHECK(gg_frontier_create(g, &f));
     for (auto *f : g->tmp_front) {
@@ -2228,6 +2265,7 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     // the split pull's second pass starts at each row's third edge: it needs
     // the first pass to have taken the first two from the first_in records
     h.split = t.pull_split && h.first_in;
+    h.flat = gb->flat;
     if (h.split && gb->rest_cap < (uint64_t)g->n) {
         cudaFree(gb->rest);
         gb->rest = nullptr;
@@ -2270,7 +2308,7 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     // where the variant changes); then the records' copy
     uint64_t npull = 0;
     for (int i = 0; i < T && i < GG_MAX_ITERS; ++i) npull += hr->variants[i] == GG_VAR_PULL_DENSE;
-    ctx->launches += 2 + 2 * (uint64_t)T + npull;
+    ctx->launches += gb->flat ? 2 + 7 * (uint64_t)T : 2 + 2 * (uint64_t)T + npull;
     if (hr->handed_off) {
         // the rest of the run as one device-driven launch from the current
         // frontier (a push leaves it as a list only: add its bitmap)

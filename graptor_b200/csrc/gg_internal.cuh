@@ -222,6 +222,7 @@ struct Tuning {
     uint32_t bin_medium_max = 2048; // deg <= this: warp per vertex, else CTA
     int pull_k = 8;                 // per-lane edges before warp cooperation (pull)
     int pull_split = 1;             // graph-driven BFS pulls in two passes (first two in-edges, then the rest)
+    int graph_flat = 1;             // graph-driven BFS: the loop body as one chain of kernels, no step conditionals
     int push_k = 8;
     int block = 256;
     int blocks_per_sm = 8;

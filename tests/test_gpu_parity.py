@@ -437,8 +437,9 @@ def test_pull_first_record_modes_exact(ctx, mode, gen):
 def test_split_pull_exact(ctx, mode, gen):
     """Graph-driven BFS with the split pull (knob pull_split: the first pass
     settles what each candidate's first two in-edges settle, the second walks
-    the rows left open from their third edge): levels identical to the
-    oracle's, with the threshold's variants and with every step a pull."""
+    the rows left open from their third edge), its loop built either way
+    (knob graph_flat): levels identical to the oracle's, with the threshold's
+    variants and with every step a pull."""
     if gen == "rmat":
         og, sym = O.rmat(15, 16 << 15, seed=82), True
     elif gen == "grid":
@@ -449,7 +450,7 @@ def test_split_pull_exact(ctx, mode, gen):
         z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "edgecases32.npz"))
         og, sym = O.Graph(int(z["n"]), z["off"], z["adj"]), True
     g = ctx.upload(og.off, og.adj, sym)
-    old = {k: gg.tuning_get(k) for k in ("pull_first", "graph", "pull_split")}
+    old = {k: gg.tuning_get(k) for k in ("pull_first", "graph", "pull_split", "graph_flat")}
     try:
         gg.tuning_set("pull_first", mode)
         gg.tuning_set("graph", 1)
@@ -457,10 +458,14 @@ def test_split_pull_exact(ctx, mode, gen):
         deg = og.outdeg()
         nz = np.flatnonzero(deg)
         roots = [int(np.argmax(deg)), int(nz[len(nz) // 2]), int(nz[-1])]
-        for r in roots:
-            lv = O.bfs_level(og, r)
-            assert np.array_equal(g.bfs_level(r), lv), (mode, r)
-            assert np.array_equal(g.bfs_level(r, opts=gg.default_opts(variant=gg.VAR_PULL_DENSE)), lv), (mode, r)
+        # the graph's loop as one chain of kernels (graph_flat 1) and with
+        # conditional nodes per step (0)
+        for flat in (1, 0):
+            gg.tuning_set("graph_flat", flat)
+            for r in roots:
+                lv = O.bfs_level(og, r)
+                assert np.array_equal(g.bfs_level(r), lv), (mode, flat, r)
+                assert np.array_equal(g.bfs_level(r, opts=gg.default_opts(variant=gg.VAR_PULL_DENSE)), lv), (mode, r)
     finally:
         for k, v in old.items():
             gg.tuning_set(k, v)
