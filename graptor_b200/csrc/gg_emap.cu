@@ -1194,6 +1194,9 @@ __global__ void __launch_bounds__(kBlock) k_mis(EmapArgs A, uint8_t *__restrict_
             e = A.in_off[d];
             end = A.in_off[d + 1];
         }
+        // rows longer than the heavy-row threshold: k_mis_heavy_chunks / _finalize
+        const bool heavy = act && A.heavy_T && end - e > A.heavy_T;
+        if (heavy) end = e;
         const uint64_t beg = e;
         bool in = false, low = false;
         const uint64_t lim = min(end, e + 32);
@@ -1237,7 +1240,7 @@ __global__ void __launch_bounds__(kBlock) k_mis(EmapArgs A, uint8_t *__restrict_
             }
         }
         bool rec = false;
-        if (act) {
+        if (act && !heavy) {
             const uint8_t nwv = in ? 2 : ((old == 1 && low) ? 0 : old);
             if (nwv != old) st[d] = nwv;
             rec = nwv == 0 && A.record == GG_RECORD_EQ_ZERO;
@@ -1250,6 +1253,67 @@ __global__ void __launch_bounds__(kBlock) k_mis(EmapArgs A, uint8_t *__restrict_
         }
     }
     if (A.out_cnt) flush_counts<kBlock>(A, nv, ne, sc);
+}
+
+// The MIS relation over the long rows: a warp per chunk of a heavy row ORs
+// "some source is in" (bit 0) and "some lower source is undecided or
+// conditionally in" (bit 1) into the row's flag word; then a thread per heavy
+// row applies the relation and records it.
+__global__ void __launch_bounds__(256) k_mis_heavy_chunks(EmapArgs A, const uint8_t *__restrict__ st,
+                                                          const uint32_t *__restrict__ dst_bits, HeavyRows H,
+                                                          uint32_t *__restrict__ flags) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t c = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < H.nchunks; c += nw) {
+        const uint32_t lo = H.crow[c];
+        const uint32_t d = H.v[lo];
+        if (dst_bits && !dev::bit_test(dst_bits, d)) continue;  // the same row for the whole warp
+        const uint64_t rb = A.in_off[d], re = A.in_off[d + 1];
+        const uint64_t e0 = rb + (c - H.first[lo]) * H.CH;
+        const uint64_t e1 = min(e0 + H.CH, re);
+        uint32_t f = 0;
+        for (uint64_t base = e0; base < e1; base += 128) {
+            uint32_t sv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint64_t e = base + j * 32 + lane;
+                sv[j] = e < e1 ? __ldg(A.in_adj + e) : d;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (sv[j] == d) continue;
+                const uint8_t u = __ldcg(st + sv[j]);
+                f |= (u == 3 ? 1u : 0u) | ((sv[j] < d && u < 2) ? 2u : 0u);
+            }
+        }
+        f = __reduce_or_sync(FULL, f);
+        if (lane == 0 && f) atomicOr(flags + lo, f);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_mis_heavy_finalize(EmapArgs A, uint8_t *__restrict__ st,
+                                                            const uint32_t *__restrict__ dst_bits, HeavyRows H,
+                                                            const uint32_t *__restrict__ flags) {
+    unsigned long long nv = 0, ne = 0;
+    const uint32_t nth = gridDim.x * blockDim.x;
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < H.nheavy; i0 += nth) {
+        const uint32_t i = i0 + threadIdx.x;
+        bool rec = false;
+        uint32_t d = 0;
+        if (i < H.nheavy) {
+            d = H.v[i];
+            if (!dst_bits || dev::bit_test(dst_bits, d)) {
+                const uint8_t old = st[d];
+                const uint32_t f = flags[i];
+                const uint8_t nwv = (f & 1u) ? 2 : ((old == 1 && (f & 2u)) ? 0 : old);
+                if (nwv != old) st[d] = nwv;
+                rec = nwv == 0 && A.record == GG_RECORD_EQ_ZERO;
+            }
+        }
+        if (rec && A.out_bits) atomicOr(A.out_bits + (d >> 5), 1u << (d & 31));
+        if (A.out_b0) emit_out(A, rec, d, nv, ne);
+    }
+    if (A.out_cnt) flush_counts<256>(A, nv, ne, 0);
 }
 
 static gg_status mis_relax(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_frontier *out) {
@@ -1286,9 +1350,27 @@ static gg_status mis_relax(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, 
         A.out_b2 = out->bins[2];
         A.out_cnt = (unsigned long long *)out->d_cnt;
     }
+    const HeavyRows &H = g->heavy;
+    uint32_t *flags = nullptr;
+    if (H.nchunks) {
+        void *scr = nullptr;
+        GG_CHECK(graph_scratch(g, ((size_t)H.nheavy + 1) * 4, &scr));
+        flags = (uint32_t *)scr;
+        GG_CUDA(ctx, cudaMemsetAsync(flags, 0, ((size_t)H.nheavy + 1) * 4, ctx->stream));
+        A.heavy_T = H.T;
+    }
     const uint64_t words = ((uint64_t)g->n + 31) / 32;
     k_mis<<<persistent_grid(ctx, words), kBlock, 0, ctx->stream>>>(A, (uint8_t *)d->a->d, dst_bits);
     GG_LAUNCHED(ctx);
+    if (flags) {
+        const unsigned cap = (unsigned)(ctx->sm_count * 8);
+        const unsigned cb = (unsigned)std::min<uint64_t>((H.nchunks * 32 + 255) / 256, cap);
+        k_mis_heavy_chunks<<<cb ? cb : 1, 256, 0, ctx->stream>>>(A, (const uint8_t *)d->a->d, dst_bits, H, flags);
+        GG_LAUNCHED(ctx);
+        const unsigned fb = (unsigned)std::min<uint64_t>((H.nheavy + 255) / 256, cap);
+        k_mis_heavy_finalize<<<fb ? fb : 1, 256, 0, ctx->stream>>>(A, (uint8_t *)d->a->d, dst_bits, H, flags);
+        GG_LAUNCHED(ctx);
+    }
     if (out) {
         out->all = false;
         out->has_list = true;
