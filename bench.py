@@ -1081,7 +1081,7 @@ def run_case(a):
     opts = gg.default_opts(gg.THRESH_LEARNED if a.threshold == "learned" else gg.THRESH_DEFAULT, collect=True)
     if a.threshold == "learned":
         from graptor_b200.selector_train import load_selector
-        gg.attach_selector(g, load_selector(ctx))
+        gg.attach_selector(g, load_selector(ctx))  # (the graph keeps its copy of the weights)
     if a.case == "bfs":
         rs = case_roots(g, a.roots)
         for r in rs[: a.warmup]:

@@ -526,6 +526,8 @@ static gg_status graph_finish(gg_graph *g) {
 
 static void graph_free(gg_graph *g) {
     if (!g) return;
+    delete[] g->sel_h;
+    cudaFree(g->sel_d);
     if (g->in_off && g->in_off != g->off) cudaFree(g->in_off);
     if (g->in_adj && g->in_adj != g->adj) cudaFree(g->in_adj);
     cudaFree(g->off);

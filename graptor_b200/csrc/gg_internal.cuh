@@ -161,7 +161,11 @@ struct gg_graph {
     uint32_t *wq = nullptr;       // work queue of fused (asynchronous) pushes
     size_t wq_cap = 0;
     float gini = -1.0f;           // degree Gini coefficient (selector feature), <0: unknown
-    gg_selector *selector = nullptr;  // learned variant selector (GG_THRESH_LEARNED)
+    // learned variant selector (GG_THRESH_LEARNED): the graph's own copy of
+    // the attached selector's weights (float on the host, bfloat16 on the device)
+    bool sel_on = false;
+    float *sel_h = nullptr;
+    void *sel_d = nullptr;
     int force_iter = -1, force_variant = -1;  // timing collection: one forced choice
     struct ForceRecord {          // what the last device-driven run saw at force_iter
         bool seen = false;

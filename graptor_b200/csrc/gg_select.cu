@@ -368,11 +368,24 @@ gg_status gg_selector_train(gg_selector *s, const float *X, const float *Y, cons
 gg_status gg_graph_set_selector(gg_graph *g, gg_selector *s) {
     if (!g) return GG_ERR_ARG;
     if (s && s->ctx != g->ctx) return set_error(g->ctx, GG_ERR_ARG, "selector of another context");
-    g->selector = s;
-    if (s) {
-        float gi;
-        GG_CHECK(graph_gini(g, &gi));
+    g->sel_on = false;
+    if (!s) return GG_OK;
+    // the graph copies the weights as they are now: the selector may be
+    // retrained or destroyed afterwards
+    gg_ctx *ctx = g->ctx;
+    if (!g->sel_h) {
+        g->sel_h = new (std::nothrow) float[NP];
+        if (!g->sel_h) return GG_ERR_OOM;
     }
+    if (!g->sel_d) GG_CUDA(ctx, cudaMalloc(&g->sel_d, NP * sizeof(__nv_bfloat16)));
+    GG_CUDA(ctx, cudaMemcpyAsync(g->sel_d, s->d_wbf, NP * sizeof(__nv_bfloat16), cudaMemcpyDeviceToDevice,
+                                 s->ctx->stream));
+    GG_CUDA(ctx, cudaMemcpyAsync(s->h_params, s->d_params, NP * 4, cudaMemcpyDeviceToHost, s->ctx->stream));
+    GG_CUDA(ctx, cudaStreamSynchronize(s->ctx->stream));
+    std::memcpy(g->sel_h, s->h_params, NP * 4);
+    g->sel_on = true;
+    float gi;
+    GG_CHECK(graph_gini(g, &gi));
     return GG_OK;
 }
 
@@ -380,7 +393,7 @@ gg_status gg_graph_set_selector(gg_graph *g, gg_selector *s) {
 
 namespace gg {
 
-const void *selector_weights(gg_graph *g) { return g->selector ? (const void *)g->selector->d_wbf : nullptr; }
+const void *selector_weights(gg_graph *g) { return g->sel_on ? (const void *)g->sel_d : nullptr; }
 
 // The ten selector features of an iteration (see gg_select.h).
 void selector_features(float *x, double nactv, double nacte, double unreached, int iter, double n, double m,
@@ -409,8 +422,8 @@ static float bf16r(float f) {  // round to bfloat16 like the device copy
 // host (bfloat16-rounded weights); the threshold when no selector is attached.
 int learned_select(gg_graph *g, uint64_t nactv, uint64_t nacte, int iter, bool can_early_exit) {
     (void)can_early_exit;
-    if (!g->selector) return (nactv + nacte) <= (g->m / 20) ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
-    const float *p = g->selector->h_params;
+    if (!g->sel_on) return (nactv + nacte) <= (g->m / 20) ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+    const float *p = g->sel_h;
     float x[IN], h1[H], h2[H], o[OUT];
     selector_features(x, (double)nactv, (double)nacte, 0.0, iter, g->n, (double)g->m, std::max(0.0f, g->gini));
     for (int j = 0; j < H; ++j) {

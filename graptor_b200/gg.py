@@ -642,6 +642,8 @@ def selector_collect(g: "Graph", analytic: int, root: int = 0, max_samples: int 
 
 
 def attach_selector(g: "Graph", sel: "Selector | None"):
+    """The graph copies the selector's weights as they are now (the selector
+    may be retrained or dropped afterwards)."""
     g.ctx.check(_sel_lib().gg_graph_set_selector(g.h, sel.h if sel else None), "gg_graph_set_selector")
 
 

@@ -66,7 +66,10 @@ GG_API gg_status gg_selector_train(gg_selector *s, const float *X, const float *
 GG_API gg_status gg_selector_collect(gg_graph *g, int analytic, uint32_t root, int max_samples,
                                      float *X, float *Y, int cap, int *nrec);
 
-/* Attach a selector to a graph: runs with GG_THRESH_LEARNED consult it. */
+/* Attach a selector to a graph (NULL detaches): runs with GG_THRESH_LEARNED
+ * consult its network.  The graph keeps its own copy of the weights as they
+ * are at this call, so the selector may be retrained or destroyed afterwards
+ * (attach again to use retrained weights). */
 GG_API gg_status gg_graph_set_selector(gg_graph *g, gg_selector *s);
 
 #ifdef __cplusplus

@@ -69,6 +69,35 @@ def test_learned_choice_never_changes_results(ctx):
     assert np.array_equal(g.bfs_level(0, opts=opts), ref_l)  # threshold fallback
 
 
+def test_graph_keeps_its_copy_of_the_weights(ctx):
+    """A graph attached to a selector that is then destroyed still runs its
+    learned choices (graph-driven, device-driven and host-driven) on its own
+    copy of the weights, with the same results."""
+    import gc
+    og = O.rmat(14, 16 << 14, seed=22)
+    g = ctx.upload(og.off, og.adj)
+    sel = gg.Selector(ctx)
+    sel.params = M.init_params(7) * 3
+    gg.attach_selector(g, sel)
+    sel.close()
+    del sel
+    gc.collect()
+    opts = gg.default_opts(gg.THRESH_LEARNED)
+    ref_l = O.bfs_level(og, 3)
+    old = {k: gg.tuning_get(k) for k in ("graph", "persistent")}
+    try:
+        for graph_mode, persistent in ((1, 4), (0, 5), (0, 4)):
+            gg.tuning_set("graph", graph_mode)
+            gg.tuning_set("persistent", persistent)
+            assert np.array_equal(g.bfs_level(3, opts=opts), ref_l), (graph_mode, persistent)
+        assert np.array_equal(g.cc(opts=opts), O.cc(og))
+    finally:
+        for k, v in old.items():
+            gg.tuning_set(k, v)
+        gg.attach_selector(g, None)
+        g.close()
+
+
 @pytest.mark.parametrize("variant", [gg.VAR_PUSH_SPARSE, gg.VAR_PUSH_MERGE, gg.VAR_PULL_DENSE, gg.VAR_PUSH_DENSE])
 def test_device_driven_every_variant(ctx, variant):
     og = O.grid(40, 50, seed=6, del_bp=200)
