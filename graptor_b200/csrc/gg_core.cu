@@ -479,8 +479,29 @@ __global__ void k_first_in(const uint64_t *__restrict__ in_off, const uint32_t *
         const uint64_t b = in_off[d], e = in_off[d + 1];
         const uint64_t deg = e - b;
         first_in[d] = make_uint4(b < e ? in_adj[b] : 0xFFFFFFFFu, b + 1 < e ? in_adj[b + 1] : 0xFFFFFFFFu,
-                                 deg > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)deg, 0u);
+                                 deg > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)deg,
+                                 b + 2 < e ? in_adj[b + 2] : 0xFFFFFFFFu);
     }
+}
+
+__global__ void k_first1(const uint64_t *__restrict__ in_off, const uint32_t *__restrict__ in_adj, uint32_t n,
+                         uint2 *first1) {
+    for (uint64_t d = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; d < n; d += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t b = in_off[d], e = in_off[d + 1];
+        const uint64_t deg = e - b;
+        first1[d] = make_uint2(b < e ? in_adj[b] : 0xFFFFFFFFu, deg > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)deg);
+    }
+}
+
+gg_status graph_ensure_first1(gg_graph *g) {
+    if (g->first1) return GG_OK;
+    gg_ctx *ctx = g->ctx;
+    GG_CUDA(ctx, cudaMalloc(&g->first1, ((size_t)g->n + 1) * sizeof(uint2)));
+    if (g->n) {
+        k_first1<<<grid_for(ctx, g->n), 256, 0, ctx->stream>>>(g->in_off, g->in_adj, g->n, g->first1);
+        GG_LAUNCHED(ctx);
+    }
+    return GG_OK;
 }
 
 static gg_status graph_finish(gg_graph *g) {
@@ -540,6 +561,7 @@ static void graph_free(gg_graph *g) {
     cudaFree(g->nonisolated);
     cudaFree(g->nonisolated_n);
     cudaFree(g->first_in);
+    cudaFree(g->first1);
     cudaFree(g->pstate2);
     for (int i = 0; i < 2; ++i) {
         if (g->copy_done[i]) {
@@ -789,7 +811,11 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "pull_k" && v >= 1 && v <= 1024) t.pull_k = (int)v;
     else if (k == "pull_split" && (v == 0 || v == 1)) t.pull_split = (int)v;
     else if (k == "graph_flat" && (v == 0 || v == 1)) t.graph_flat = (int)v;
-    else if (k == "pull_first" && v <= 2) t.pull_first = (int)v;
+    else if (k == "graph_pdl" && (v == 0 || v == 1)) t.graph_pdl = (int)v;
+    else if (k == "graph_unroll" && v >= 1 && v <= 4) t.graph_unroll = (int)v;
+    else if (k == "pull_first" && v <= 4) t.pull_first = (int)v;
+    else if (k == "pull_stage" && (v == 0 || v == 4 || v == 8 || v == 16 || v == 32)) t.pull_stage = (int)v;
+    else if (k == "pull_fresh" && v <= 1) t.pull_fresh = (int)v;
     else if (k == "push_k" && v >= 1 && v <= 1024) t.push_k = (int)v;
     else if (k == "heavy_deg" && v >= 32) t.heavy_deg = (uint32_t)v;
     else if (k == "heavy_chunk" && v >= 32) t.heavy_chunk = (uint32_t)v;
@@ -822,7 +848,11 @@ gg_status gg_tuning_get(const char *name, int64_t *v) {
     else if (k == "pull_k") *v = t.pull_k;
     else if (k == "pull_split") *v = t.pull_split;
     else if (k == "graph_flat") *v = t.graph_flat;
+    else if (k == "graph_pdl") *v = t.graph_pdl;
+    else if (k == "graph_unroll") *v = t.graph_unroll;
     else if (k == "pull_first") *v = t.pull_first;
+    else if (k == "pull_stage") *v = t.pull_stage;
+    else if (k == "pull_fresh") *v = t.pull_fresh;
     else if (k == "push_k") *v = t.push_k;
     else if (k == "heavy_deg") *v = t.heavy_deg;
     else if (k == "heavy_chunk") *v = t.heavy_chunk;

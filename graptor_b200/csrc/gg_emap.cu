@@ -75,8 +75,11 @@ struct EmapArgs {
     uint32_t *cand_out;                 // vertices still passing after this step
     unsigned long long *cand_out_n;
     const uint64_t *word_prefix;        // full-scan pull: per-word cost prefix
-    const uint4 *first_in;              // pull: first two in-neighbours + in-degree per vertex, or null
-    int lazy_off;                       // pull: offsets only for rows the first two edges do not settle
+    const uint4 *first_in;              // pull: {first two in-neighbours, in-degree, third} per vertex, or null
+    const uint2 *first1;                // pull: {first in-neighbour, in-degree} per vertex, or null
+    int rec_n;                          // pull: in-neighbours taken from the record (1 to 3)
+    int lazy_off;                       // pull: offsets only for rows the record's edges do not settle
+    int fresh;                          // pull: every candidate is unvisited (level not loaded)
     // split pull, first pass: candidates still open after their first two
     // in-edges are appended here for the second pass (graph-driven BFS)
     uint32_t *rest_out;
@@ -221,8 +224,30 @@ __device__ __forceinline__ void flush_counts(const EmapArgs &A, unsigned long lo
 // the candidates with more edges still to look at to rest_out; PASS 2 walks
 // that list from each row's third edge.  A warp of PASS 1 then waits for no
 // lane's long row, and a warp of PASS 2 has every lane on an open row.
-template <int R, bool SRCF, bool CAND, int BLOCK, int PASS = 0>
-__device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
+// frontier bit of source s: from the CTA's shared-memory copy of the
+// bitmap's first words when s falls there (STAGE), else through L1/L2
+template <bool STAGE>
+__device__ __forceinline__ bool probe_bit(const uint32_t *__restrict__ gbits, const uint32_t *sbits, uint32_t sn,
+                                          uint32_t s) {
+    if constexpr (STAGE) {
+        if (s < sn) return (sbits[s >> 5] >> (s & 31u)) & 1u;
+    }
+    return dev::bit_test(gbits, s);
+}
+
+// Shared-memory staging of the pull's list appends: 256 entries per warp for
+// the candidate list and, in a split pull's first pass, for the rest list.
+// Kernels that run several pull passes declare one and hand it to each.
+template <int BLOCK, bool REST>
+struct PullSmem {
+    uint32_t cand[BLOCK / 32][256];
+    uint32_t rest[REST ? BLOCK / 32 : 1][256];
+};
+
+template <int R, bool SRCF, bool CAND, int BLOCK, int PASS = 0, bool STAGE = false, bool REST>
+__device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op, PullSmem<BLOCK, REST> &sm,
+                                          const uint32_t *sbits = nullptr, uint32_t sn = 0) {
+    static_assert(PASS != 1 || REST, "a split pull's first pass stages its rest list");
     static_assert(PASS == 0 || (CAND && R == GG_RELAX_MIN_PLUS1_I32), "split pull: BFS levels, candidate lists");
     using V = typename Op<R>::V;
     const uint32_t lane = threadIdx.x & 31u;
@@ -235,10 +260,8 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
     if (!CAND) dev::balanced_range(A.word_prefix, (A.n + 31u) >> 5, gw, nw, wlo, whi);
     const uint64_t wstep = CAND ? nw : 1;
     unsigned long long nv = 0, ne = 0, sc = 0;
-    __shared__ uint32_t s_cand[BLOCK / 32][256];
-    dev::WarpAppender<256> keepers{s_cand[threadIdx.x >> 5], 0, A.cand_out, A.cand_out_n};
-    __shared__ uint32_t s_rest[PASS == 1 ? BLOCK / 32 : 1][PASS == 1 ? 256 : 1];
-    dev::WarpAppender<256> rest{s_rest[PASS == 1 ? threadIdx.x >> 5 : 0], 0, A.rest_out, A.rest_out_n};
+    dev::WarpAppender<256> keepers{sm.cand[threadIdx.x >> 5], 0, A.cand_out, A.cand_out_n};
+    dev::WarpAppender<256> rest{sm.rest[REST ? threadIdx.x >> 5 : 0], 0, A.rest_out, A.rest_out_n};
     for (uint64_t w = CAND ? gw : wlo; CAND ? ((w << 5) < nitems) : (w < whi); w += wstep) {
         const uint64_t item = (w << 5) + lane;
         const bool valid = item < nitems;
@@ -246,10 +269,18 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
         V best = Op<R>::none();
         uint64_t e = 0, end = 0;
         uint4 f2 = make_uint4(0u, 0u, 0u, 0u);
-        const bool lazy = PASS != 2 && A.first_in && A.lazy_off;
+        const bool has_rec = PASS != 2 && (A.first_in || A.first1);
+        const bool lazy = has_rec && A.lazy_off;
         if (valid) {
-            best = op.load(d);
-            if (PASS != 2 && A.first_in) f2 = A.first_in[d];
+            best = (CAND && A.fresh) ? Op<R>::none() : op.load(d);
+            if (has_rec) {
+                if (A.first1) {
+                    const uint2 r1 = A.first1[d];
+                    f2 = make_uint4(r1.x, 0xFFFFFFFFu, r1.y, 0xFFFFFFFFu);
+                } else {
+                    f2 = A.first_in[d];
+                }
+            }
             if (!lazy) {
                 e = A.in_off[d];
                 end = A.in_off[d + 1];
@@ -264,17 +295,19 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
         }
         bool changed = false;
         uint64_t beg = e;
-        if (PASS == 2) e += 2;  // the first pass took the first two edges
+        // the first pass took the record's edges (as many as K allowed)
+        const uint64_t skip = PASS == 2 ? (uint64_t)min(A.rec_n, A.K) : 0u;
+        e += skip;
         uint64_t lim = min(end, e + (uint64_t)A.K);
-        if (PASS != 2 && A.first_in && act && e < lim) {
-            // the row's first two in-neighbours, loaded beside its offsets:
-            // the same edges in the same order as the loop below takes them
-            const int cnt = (int)min((uint64_t)2, lim - e);
-            const uint32_t sv[2] = {f2.x, f2.y};
+        if (has_rec && act && e < lim) {
+            // the row's first in-neighbours, loaded beside its offsets: the
+            // same edges in the same order as the loop below takes them
+            const int cnt = (int)min((uint64_t)A.rec_n, lim - e);
+            const uint32_t sv[3] = {f2.x, f2.y, f2.w};
             int used = cnt;
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                if (j < cnt && act && (!SRCF || dev::bit_test(A.in_bits, sv[j]))) {
+            for (int j = 0; j < 3; ++j) {
+                if (j < cnt && act && (!SRCF || probe_bit<STAGE>(A.in_bits, sbits, sn, sv[j]))) {
                     const V x = op.src_val(sv[j]);
                     if (op.better(x, best)) {
                         best = op.combine(best, x);
@@ -314,7 +347,7 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
             for (int j = 0; j < 4; ++j) sv[j] = j < cnt ? __ldg(A.in_adj + e + j) : 0u;
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                inF[j] = j < cnt && (!SRCF || dev::bit_test(A.in_bits, sv[j]));
+                inF[j] = j < cnt && (!SRCF || probe_bit<STAGE>(A.in_bits, sbits, sn, sv[j]));
                 xv[j] = j < cnt ? op.src_val(sv[j]) : Op<R>::none();
             }
             int used = cnt;
@@ -331,7 +364,7 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
             }
             e += used;
         }
-        sc += e - beg - (PASS == 2 ? 2 : 0);
+        sc += e - beg - skip;
         unsigned pend = __ballot_sync(FULL, act && e < end);
         while (pend) {
             const int j = __ffs(pend) - 1;
@@ -346,7 +379,7 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
                 V x = Op<R>::none();
                 if (idx < endj) {
                     const uint32_t s = __ldg(A.in_adj + idx);
-                    if (!SRCF || dev::bit_test(A.in_bits, s)) {
+                    if (!SRCF || probe_bit<STAGE>(A.in_bits, sbits, sn, s)) {
                         x = op.src_val(s);
                         ok = op.better(x, bj);
                     }
@@ -423,7 +456,8 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op) {
 
 template <int R, bool SRCF, bool CAND, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 6) k_pull(EmapArgs A, Op<R> op) {
-    pull_body<R, SRCF, CAND, BLOCK>(A, op);
+    __shared__ PullSmem<BLOCK, false> sm;
+    pull_body<R, SRCF, CAND, BLOCK>(A, op, sm);
 }
 
 // Bitwise-or pulls over the long rows (FMv's all-source steps): a warp per
@@ -835,6 +869,28 @@ static bool threshold_sparse(int kind, int k, uint64_t nactv, uint64_t nacte, ui
 
 int learned_select(gg_graph *g, uint64_t nactv, uint64_t nacte, int iter, bool can_early_exit);
 
+// the dense pull's per-vertex records as knob pull_first selects them
+static gg_status pull_records(gg_graph *g, const Tuning &t, const uint4 **fi, const uint2 **f1, int *rec_n,
+                              int *lazy) {
+    *fi = nullptr;
+    *f1 = nullptr;
+    *rec_n = 0;
+    *lazy = 0;
+    switch (t.pull_first) {
+    case 1: *fi = g->first_in; *rec_n = 2; break;
+    case 2: *fi = g->first_in; *rec_n = 2; *lazy = 1; break;
+    case 3: *fi = g->first_in; *rec_n = 3; *lazy = 1; break;
+    case 4:
+        GG_CHECK(graph_ensure_first1(g));
+        *f1 = g->first1;
+        *rec_n = 1;
+        *lazy = 1;
+        break;
+    default: break;
+    }
+    return GG_OK;
+}
+
 template <int R>
 static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier *in,
                                 gg_frontier *out, int variant) {
@@ -861,8 +917,7 @@ static gg_status launch_variant(gg_graph *g, const gg_emap_desc *d, gg_frontier 
     A.mmax = t.bin_medium_max;
     A.K = variant == GG_VAR_PULL_DENSE ? t.pull_k : t.push_k;
     A.word_prefix = g->heavy.pull_prefix;
-    A.first_in = t.pull_first ? g->first_in : nullptr;
-    A.lazy_off = t.pull_first == 2;
+    GG_CHECK(pull_records(g, t, &A.first_in, &A.first1, &A.rec_n, &A.lazy_off));
     const bool have_out = out != nullptr && d->record != GG_RECORD_NONE;
     if (have_out) {
         GG_CHECK(frontier_alloc_bins(out));
@@ -1648,7 +1703,11 @@ struct GCtl {
     const uint64_t *off, *in_off, *word_prefix;
     const uint32_t *adj, *in_adj;
     const uint4 *first_in;
+    const uint2 *first1;
+    int rec_n;
     int lazy_off;
+    int fresh_ok;                     // a pull after a pull skips its candidates' level loads (knob pull_fresh)
+    uint32_t stage_words;             // bitmap words each pull CTA stages in shared memory (knob pull_stage)
     int split;                        // pulls in two passes (pull_body PASS 1 / 2)
     int flat;                         // the loop body is one chain of kernels (no step conditionals)
     int need_chunks;                  // this push step needs k_g_chunks
@@ -1663,13 +1722,18 @@ struct GCtl {
     int cand_cur, cand_valid;
     // records
     unsigned long long reached_v, reached_e;
-    int variants[GG_MAX_ITERS];
+    unsigned stage_timeouts;  // pull CTAs whose bitmap staging did not complete in time (probes went to L2)
+    cudaGraphConditionalHandle h_while, h_push, h_pull, h_list, h_bits, h_chunks;
+    // per-iteration records (after the head: `next` works on a shared-memory
+    // copy of everything before them)
+    alignas(16) int variants[GG_MAX_ITERS];
     unsigned long long nactv[GG_MAX_ITERS], nacte[GG_MAX_ITERS], scanned[GG_MAX_ITERS];
     unsigned long long t_ns[GG_MAX_ITERS + 1];
     // span of each step's traversal kernel (first CTA start, last CTA end)
     unsigned long long kt0[GG_MAX_ITERS], kt1[GG_MAX_ITERS];
-    cudaGraphConditionalHandle h_while, h_push, h_pull, h_list, h_bits, h_chunks;
 };
+constexpr size_t kCtlHead = offsetof(GCtl, variants);
+static_assert(kCtlHead % 16 == 0 && kCtlHead <= 4096, "control block head: whole 16-byte words, small");
 
 __device__ __forceinline__ unsigned long long g_now() {
     unsigned long long t;
@@ -1686,7 +1750,17 @@ __device__ __forceinline__ bool d_threshold_sparse(int kind, int k, uint64_t nac
     }
 }
 
-__device__ void decide_step(GCtl *c);
+__device__ void decide_step(GCtl *c, GCtl *h);
+
+// Programmatic dependent launch (knob graph_pdl): the loop body's kernels
+// are joined by programmatic edges, so each is launched while its
+// predecessor still runs; it lets its own successor launch at once and waits
+// here for its predecessor's completion (and memory) before it reads the
+// control block.  Without such an edge both instructions do nothing.
+__device__ __forceinline__ void chain_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
 
 __global__ void k_g_init(GCtl *c) {
     const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
@@ -1727,12 +1801,13 @@ __global__ void k_g_init(GCtl *c) {
         c->clr = 0;
         c->reached_v = 0;
         c->reached_e = 0;
+        c->stage_timeouts = 0;
         c->variant = -1;
         c->t_ns[0] = g_now();
     }
     if (blockIdx.x == 0 && threadIdx.x < 32) {
         __syncwarp();
-        decide_step(c);  // the first step's decision (warp 0 of CTA 0)
+        decide_step(c, c);  // the first step's decision (warp 0 of CTA 0)
     }
 }
 
@@ -1740,40 +1815,44 @@ __global__ void k_g_init(GCtl *c) {
 // counts, writes the step's arguments, sets the branch and loop conditions
 // Called by the 32 lanes of one warp (the network is evaluated by a warp);
 // lane 0 writes the decision.
-__device__ void decide_step(GCtl *c) {
+__device__ void decide_step(GCtl *c, GCtl *h) {
     const uint32_t lane = threadIdx.x & 31u;
-    const GFront F = c->f[c->cur], O = c->f[c->cur ^ 1];
+    const GFront F = h->f[h->cur], O = h->f[h->cur ^ 1];
     const unsigned long long nactv = F.cnt[FC_NACTV], nacte = F.cnt[FC_NACTE];
-    const int iter = c->iter;
-    const bool handoff = c->handoff_iter > 0 && iter >= c->handoff_iter;
-    if (nactv == 0 || iter >= c->max_iters || handoff) {
+    const int iter = h->iter;
+    const bool handoff = h->handoff_iter > 0 && iter >= h->handoff_iter;
+    if (nactv == 0 || iter >= h->max_iters || handoff) {
         if (lane != 0) return;
         // a long run of small steps continues in the device-driven traversal
-        c->handed_off = nactv != 0 && iter < c->max_iters;
-        c->variant = -1;
-        c->iterations = iter;
-        if (!c->flat) {
-            cudaGraphSetConditional(c->h_push, 2u);  // the step switch: no body
-            cudaGraphSetConditional(c->h_list, 0);
-            cudaGraphSetConditional(c->h_bits, 0);
-            cudaGraphSetConditional(c->h_chunks, 0);
+        h->handed_off = nactv != 0 && iter < h->max_iters;
+        h->variant = -1;
+        h->iterations = iter;
+        // kernels of the loop body still to run (an unrolled body) do nothing
+        h->need_list = 0;
+        h->need_bitmap = 0;
+        h->need_chunks = 0;
+        if (!h->flat) {
+            cudaGraphSetConditional(h->h_push, 2u);  // the step switch: no body
+            cudaGraphSetConditional(h->h_list, 0);
+            cudaGraphSetConditional(h->h_bits, 0);
+            cudaGraphSetConditional(h->h_chunks, 0);
         }
-        cudaGraphSetConditional(c->h_while, 0);
+        cudaGraphSetConditional(h->h_while, 0);
         return;
     }
-    bool push = d_threshold_sparse(c->threshold, c->threshold_k, nactv, nacte, c->m);
-    const unsigned long long unr_c = c->reached_v < c->n ? c->n - c->reached_v : 0ull;
+    bool push = d_threshold_sparse(h->threshold, h->threshold_k, nactv, nacte, h->m);
+    const unsigned long long unr_c = h->reached_v < h->n ? h->n - h->reached_v : 0ull;
     const auto close = [](unsigned long long a, unsigned long long b) {
         const unsigned long long d = a > b ? a - b : b - a, mx = a > b ? a : b;
         return d * 16 <= mx;
     };
-    if (c->sel_w && c->sel_valid && close(nactv, c->sel_nactv) && close(nacte, c->sel_nacte) &&
-        close(unr_c, c->sel_unr) && min(iter, 255) - c->sel_iter < 8) {
-        push = c->sel_push != 0;  // the last evaluation still applies
-    } else if (c->sel_w) {
+    if (h->sel_w && h->sel_valid && close(nactv, h->sel_nactv) && close(nacte, h->sel_nacte) &&
+        close(unr_c, h->sel_unr) && min(iter, 255) - h->sel_iter < 8) {
+        push = h->sel_push != 0;  // the last evaluation still applies
+    } else if (h->sel_w) {
         // learned choice between the two variants this driver runs: the
         // threshold's stands unless the network predicts a clear gain
-        const double n = c->n, m = (double)c->m, fv = (double)nactv, fe = (double)nacte;
+        const double n = h->n, m = (double)h->m, fv = (double)nactv, fe = (double)nacte;
         const double unr = (double)unr_c;
         float x[GG_SEL_FEATURES];
         x[0] = (float)(log2(1.0 + fv) / 32);
@@ -1781,24 +1860,24 @@ __device__ void decide_step(GCtl *c) {
         x[2] = (float)(log2(1.0 + unr) / 32);
         x[3] = (float)(log2(1.0 + min(iter, 255)) / 8);
         x[4] = (float)(log2(1.0 + (n > 0 ? m / n : 0)) / 8);
-        x[5] = c->gini;
+        x[5] = h->gini;
         x[6] = (float)(n > 0 ? fv / n : 0);
         x[7] = (float)(m > 0 ? fe / m : 0);
         x[8] = (float)fmin(4.0, m > 0 ? (fv + fe) / m : 0.0);
         x[9] = (float)(log2(n > 1 ? n : 1.0) / 32);
         float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
-        mlp::warp_forward(c->sel_w, x, o, z1, a1, z2, a2);
+        mlp::warp_forward(h->sel_w, x, o, z1, a1, z2, a2);
         const int tv = push ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
         const int best = o[GG_VAR_PUSH_SPARSE] < o[GG_VAR_PULL_DENSE] ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
         if (o[best] < o[tv] - mlp::kSelMargin) push = best == GG_VAR_PUSH_SPARSE;
         __syncwarp();
         if (lane == 0) {
-            c->sel_nactv = nactv;
-            c->sel_nacte = nacte;
-            c->sel_unr = unr_c;
-            c->sel_iter = min(iter, 255);
-            c->sel_push = push;
-            c->sel_valid = 1;
+            h->sel_nactv = nactv;
+            h->sel_nacte = nacte;
+            h->sel_unr = unr_c;
+            h->sel_iter = min(iter, 255);
+            h->sel_push = push;
+            h->sel_valid = 1;
         }
     }
     if (lane != 0) return;
@@ -1807,22 +1886,26 @@ __device__ void decide_step(GCtl *c) {
         c->nactv[iter] = nactv;
         c->nacte[iter] = nacte;
     }
-    c->reached_v += nactv;
-    c->reached_e += nacte;
+    h->reached_v += nactv;
+    h->reached_e += nacte;
     EmapArgs A;
     memset(&A, 0, sizeof(A));
-    A.off = c->off;
-    A.adj = c->adj;
-    A.in_off = c->in_off;
-    A.in_adj = c->in_adj;
-    A.n = c->n;
+    A.off = h->off;
+    A.adj = h->adj;
+    A.in_off = h->in_off;
+    A.in_adj = h->in_adj;
+    A.n = h->n;
     A.record = GG_RECORD_NE_PREV;
-    A.smax = c->smax;
-    A.mmax = c->mmax;
-    A.K = push ? c->push_k : c->pull_k;
-    A.word_prefix = c->word_prefix;
-    A.first_in = push ? nullptr : c->first_in;
-    A.lazy_off = c->lazy_off;
+    A.smax = h->smax;
+    A.mmax = h->mmax;
+    A.K = push ? h->push_k : h->pull_k;
+    A.word_prefix = h->word_prefix;
+    A.first_in = push ? nullptr : h->first_in;
+    A.first1 = push ? nullptr : h->first1;
+    A.rec_n = h->rec_n;
+    A.lazy_off = h->lazy_off;
+    // candidates left unsettled by the pull just run are all unvisited
+    A.fresh = !push && h->fresh_ok && h->cand_valid && h->variant == GG_VAR_PULL_DENSE;
     A.out_b0 = O.bins[0];
     A.out_b1 = O.bins[1];
     A.out_b2 = O.bins[2];
@@ -1831,51 +1914,52 @@ __device__ void decide_step(GCtl *c) {
     A.in_b0 = F.bins[0];
     A.in_b1 = F.bins[1];
     A.in_b2 = F.bins[2];
-    A.large_ch = c->large_ch;
+    A.large_ch = h->large_ch;
     if (!push) {
-        const int cc = c->cand_cur;
-        A.cand = c->cand_valid ? c->cand[cc] : c->nonisolated;
-        A.cand_n = c->cand_valid ? c->cand_n + cc : c->nonisolated_n;
-        A.cand_out = c->cand[cc ^ 1];
-        A.cand_out_n = c->cand_n + (cc ^ 1);
-        c->cand_n[cc ^ 1] = 0;
+        const int cc = h->cand_cur;
+        A.cand = h->cand_valid ? h->cand[cc] : h->nonisolated;
+        A.cand_n = h->cand_valid ? h->cand_n + cc : h->nonisolated_n;
+        A.cand_out = h->cand[cc ^ 1];
+        A.cand_out_n = h->cand_n + (cc ^ 1);
+        h->cand_n[cc ^ 1] = 0;
         A.out_bits = O.bitmap;  // cleared by the post kernel of the step that consumed it
         // split when the frontier holds less than half the edges: then most
         // candidates' first two in-edges leave them open, and a warp of the
         // single pass waits for its lanes' long rows
-        if (c->split && 2 * nacte < c->m) {
-            A.rest_out = c->rest;
+        if (h->split && 2 * nacte < h->m) {
+            A.rest_out = h->rest;
             A.rest_out_n = &c->rest_n;
-            c->rest_n = 0;
+            h->rest_n = 0;
         }
     }
-    c->A = A;
+    h->A = A;
     Op<GG_RELAX_MIN_PLUS1_I32> op;
-    op.a = c->level;
-    op.prev = c->prev;
+    op.a = h->level;
+    op.prev = h->prev;
     op.filter = GG_FILTER_GT_CONST;
     op.fk = iter + 1;
     op.level_sync = 1;
-    c->op = op;
-    c->variant = push ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
-    c->need_list = push && !c->has_list[c->cur];
-    c->use_first = 0;
+    h->op = op;
+    h->variant = push ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
+    h->need_list = push && !h->has_list[h->cur];
+    h->use_first = 0;
     // a large bin too big for a CTA's shared table gets its chunk prefix from
     // k_g_chunks (its size is known here unless the list is still to be built)
-    const bool chunks = push && (c->need_list || F.cnt[FC_BIN2] > kLargeLocal);
-    c->need_chunks = chunks;
-    c->need_bitmap = !push && !c->has_bitmap[c->cur];
-    if (!c->flat) {
-        cudaGraphSetConditional(c->h_chunks, chunks ? 1u : 0u);
-        cudaGraphSetConditional(c->h_push, push ? 0u : 1u);  // the step switch: push or pull body
-        cudaGraphSetConditional(c->h_list, c->need_list ? 1u : 0u);
-        cudaGraphSetConditional(c->h_bits, c->need_bitmap ? 1u : 0u);
+    const bool chunks = push && (h->need_list || F.cnt[FC_BIN2] > kLargeLocal);
+    h->need_chunks = chunks;
+    h->need_bitmap = !push && !h->has_bitmap[h->cur];
+    if (!h->flat) {
+        cudaGraphSetConditional(h->h_chunks, chunks ? 1u : 0u);
+        cudaGraphSetConditional(h->h_push, push ? 0u : 1u);  // the step switch: push or pull body
+        cudaGraphSetConditional(h->h_list, h->need_list ? 1u : 0u);
+        cudaGraphSetConditional(h->h_bits, h->need_bitmap ? 1u : 0u);
     }
-    cudaGraphSetConditional(c->h_while, 1u);
+    cudaGraphSetConditional(h->h_while, 1u);
 }
 
 // a frontier held as a bitmap only (after a pull) gets its binned list
 __global__ void __launch_bounds__(256) k_g_tolist(GCtl *c) {
+    chain_enter();
     if (!c->need_list) return;
     const GFront F = c->f[c->cur];
     __shared__ uint32_t sb[3][8][256];
@@ -1910,6 +1994,7 @@ __device__ __forceinline__ void kspan_end(GCtl *c, int it, unsigned *s_done) {
 }
 
 __global__ void __launch_bounds__(kBlock, 6) k_g_push(GCtl *c) {
+    chain_enter();
     if (c->variant != GG_VAR_PUSH_SPARSE) return;
     __shared__ EmapArgs sA;
     __shared__ Op<GG_RELAX_MIN_PLUS1_I32> sOp;
@@ -1971,6 +2056,7 @@ __device__ __noinline__ void g_push_setup(GCtl *c, uint32_t cap, EmapArgs *sA, O
 // a frontier held as a list only (after a push) gets its bitmap (clear since
 // the frontier's buffer was last consumed)
 __global__ void k_g_tobitmap(GCtl *c) {
+    chain_enter();
     if (!c->need_bitmap) return;
     const GFront F = c->f[c->cur];
     const unsigned long long c0 = F.cnt[FC_BIN0], c1 = F.cnt[FC_BIN1], c2 = F.cnt[FC_BIN2];
@@ -1981,8 +2067,68 @@ __global__ void k_g_tobitmap(GCtl *c) {
     }
 }
 
+// Frontier bitmap staging (knob pull_stage): thread 0 copies the bitmap's
+// first `words` words (rounded down to 16-byte units) into the CTA's dynamic
+// shared memory with one bulk copy (cp.async.bulk, completion counted on an
+// mbarrier); every thread waits on the barrier at most kStageSpin polls.
+// Returns the number of vertex ids the copy covers, the same for every
+// thread; 0 when nothing was staged or the wait ran out (then every probe
+// goes to L2 and the copy is waited for again before the CTA exits).
+constexpr uint32_t kStageSpin = 1u << 20;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool stage_poll(uint32_t bar, uint32_t limit) {
+    uint32_t ok = 0;
+    for (uint32_t i = 0; i < limit && !ok; ++i)
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(ok)
+                     : "r"(bar)
+                     : "memory");
+    return ok != 0;
+}
+
+__device__ uint32_t stage_bitmap(const uint32_t *src, uint64_t src_words, uint32_t words, uint32_t *dst,
+                                 unsigned long long *bar, bool *pending) {
+    words = (uint32_t)min((uint64_t)words, src_words) & ~3u;
+    *pending = false;
+    if (words == 0 || ((uintptr_t)src & 15u) != 0) return 0;
+    const uint32_t b = smem_u32(bar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(b) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(words * 4u) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_u32(dst)),
+                     "l"(src), "r"(words * 4u), "r"(b)
+                     : "memory");
+    }
+    __syncthreads();  // the barrier is initialised before any thread polls it
+    const bool ok = __syncthreads_and(stage_poll(b, kStageSpin)) != 0;
+    *pending = !ok;
+    return ok ? words * 32u : 0u;
+}
+
+// a CTA whose staging wait ran out waits (bounded) for the copy before it
+// exits, and counts the event
+__device__ __forceinline__ void stage_finish(GCtl *c, unsigned long long *bar, bool pending) {
+    if (!pending) return;
+    if (threadIdx.x == 0) {
+        atomicAdd(&c->stage_timeouts, 1u);
+        stage_poll(smem_u32(bar), kStageSpin);
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(kBlock, 6) k_g_pull(GCtl *c) {
+    chain_enter();
     if (c->variant != GG_VAR_PULL_DENSE) return;
+    extern __shared__ __align__(128) uint32_t s_stage[];
+    __shared__ __align__(8) unsigned long long s_bar;
     __shared__ EmapArgs sA;
     __shared__ Op<GG_RELAX_MIN_PLUS1_I32> sOp;
     __shared__ int s_it;
@@ -1996,15 +2142,29 @@ __global__ void __launch_bounds__(kBlock, 6) k_g_pull(GCtl *c) {
         if (blockIdx.x == 0) c->clr = c->cur + 1;  // a pulled frontier has a bitmap to clear after
     }
     __syncthreads();
-    if (sA.rest_out) pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock, 1>(sA, sOp);
-    else pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock>(sA, sOp);
+    __shared__ PullSmem<kBlock, true> sm;
+    if (c->stage_words) {
+        bool pending;
+        const uint32_t sn = stage_bitmap(sA.in_bits, ((uint64_t)sA.n + 31) / 32, c->stage_words, s_stage, &s_bar,
+                                         &pending);
+        if (sA.rest_out) pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock, 1, true>(sA, sOp, sm, s_stage, sn);
+        else pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock, 0, true>(sA, sOp, sm, s_stage, sn);
+        stage_finish(c, &s_bar, pending);
+    } else if (sA.rest_out) {
+        pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock, 1>(sA, sOp, sm);
+    } else {
+        pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock>(sA, sOp, sm);
+    }
     kspan_end(c, s_it, &s_done);
 }
 
 // second pass of a split pull: the rows the first pass left open, from
 // their third in-edge
 __global__ void __launch_bounds__(kBlock, 6) k_g_pull2(GCtl *c) {
+    chain_enter();
     if (c->variant != GG_VAR_PULL_DENSE || !c->A.rest_out) return;
+    extern __shared__ __align__(128) uint32_t s_stage[];
+    __shared__ __align__(8) unsigned long long s_bar;
     __shared__ EmapArgs sA;
     __shared__ Op<GG_RELAX_MIN_PLUS1_I32> sOp;
     __shared__ int s_it;
@@ -2017,15 +2177,26 @@ __global__ void __launch_bounds__(kBlock, 6) k_g_pull2(GCtl *c) {
         sA.cand = c->rest;
         sA.cand_n = &c->rest_n;
         sA.first_in = nullptr;
+        sA.first1 = nullptr;
         sA.rest_out = nullptr;
+        sA.fresh = c->fresh_ok;  // rows the first pass left open are unvisited
         sOp = c->op;
     }
     __syncthreads();
-    pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock, 2>(sA, sOp);
+    __shared__ PullSmem<kBlock, false> sm;
+    if (c->stage_words) {
+        bool pending;
+        const uint32_t sn = stage_bitmap(sA.in_bits, ((uint64_t)sA.n + 31) / 32, c->stage_words, s_stage, &s_bar,
+                                         &pending);
+        pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock, 2, true>(sA, sOp, sm, s_stage, sn);
+        stage_finish(c, &s_bar, pending);
+    } else {
+        pull_body<GG_RELAX_MIN_PLUS1_I32, true, true, kBlock, 2>(sA, sOp, sm);
+    }
     kspan_end(c, s_it, &s_done);
 }
 
-__device__ void g_bookkeep(GCtl *c);
+__device__ void g_bookkeep(GCtl *c, GCtl *h);
 
 // After a step: every CTA clears the consumed frontier's bitmap for its next
 // use as an output (when the step, or the conversion for a pull, set one:
@@ -2033,6 +2204,7 @@ __device__ void g_bookkeep(GCtl *c);
 // CTA 0 meanwhile does the step's bookkeeping (thread 0) and the next step's
 // decision, which touch no bitmap.
 __global__ void __launch_bounds__(256) k_g_next(GCtl *c) {
+    chain_enter();
     const int clr = c->clr;
     if (clr) {
         uint32_t *bm = c->f[clr - 1].bitmap;
@@ -2045,29 +2217,40 @@ __global__ void __launch_bounds__(256) k_g_next(GCtl *c) {
         if (threadIdx.x == 0) cudaGraphSetConditional(c->h_while, 0);
         return;
     }
-    if (threadIdx.x == 0) g_bookkeep(c);
+    // the control block's head (everything but the per-iteration records)
+    // is read into shared memory in one round of 16-byte loads, the
+    // bookkeeping and the decision work on that copy, and it is written
+    // back: one global round trip instead of one per dependent field
+    __shared__ __align__(16) unsigned char s_head[kCtlHead];
+    const uint32_t lane = threadIdx.x;
+    for (uint32_t i = lane; i < kCtlHead / 16; i += 32) ((uint4 *)s_head)[i] = ((const uint4 *)c)[i];
     __syncwarp();
-    decide_step(c);  // an empty frontier or the iteration bound ends the loop
+    GCtl *h = (GCtl *)s_head;
+    if (lane == 0) g_bookkeep(c, h);
+    __syncwarp();
+    decide_step(c, h);  // an empty frontier or the iteration bound ends the loop
+    __syncwarp();
+    for (uint32_t i = lane; i < kCtlHead / 16; i += 32) ((uint4 *)c)[i] = ((const uint4 *)s_head)[i];
 }
 
 // bookkeeping of the step that ran (one thread)
-__device__ void g_bookkeep(GCtl *c) {
+__device__ void g_bookkeep(GCtl *c, GCtl *h) {
     {
-    const int cur = c->cur;
-    const GFront F = c->f[cur], O = c->f[cur ^ 1];
-    const int iter = c->iter;
+    const int cur = h->cur;
+    const GFront F = h->f[cur], O = h->f[cur ^ 1];
+    const int iter = h->iter;
     if (iter < GG_MAX_ITERS) c->scanned[iter] = O.cnt[FC_SCANNED];
     for (int i = 0; i < FC_WORDS; ++i) F.cnt[i] = 0;
-    c->has_list[cur ^ 1] = c->variant == GG_VAR_PUSH_SPARSE;
-    c->has_list[cur] = 0;
-    c->has_bitmap[cur ^ 1] = c->variant == GG_VAR_PULL_DENSE;
-    c->has_bitmap[cur] = 0;
-    if (c->variant == GG_VAR_PULL_DENSE) {
-        c->cand_valid = 1;
-        c->cand_cur ^= 1;
+    h->has_list[cur ^ 1] = h->variant == GG_VAR_PUSH_SPARSE;
+    h->has_list[cur] = 0;
+    h->has_bitmap[cur ^ 1] = h->variant == GG_VAR_PULL_DENSE;
+    h->has_bitmap[cur] = 0;
+    if (h->variant == GG_VAR_PULL_DENSE) {
+        h->cand_valid = 1;
+        h->cand_cur ^= 1;
     }
-    c->cur = cur ^ 1;
-    c->iter = iter + 1;
+    h->cur = cur ^ 1;
+    h->iter = iter + 1;
     if (iter + 1 <= GG_MAX_ITERS) c->t_ns[iter + 1] = g_now();
     }
 }
@@ -2077,6 +2260,7 @@ __device__ void g_bookkeep(GCtl *c) {
 __global__ void __launch_bounds__(1024) k_g_chunks(GCtl *c) {
     __shared__ unsigned long long s_warp[32];
     __shared__ unsigned long long s_base;
+    chain_enter();
     if (c->variant != GG_VAR_PUSH_SPARSE || !c->need_chunks) return;
     const GFront F = c->f[c->cur];
     const uint64_t c2 = F.cnt[FC_BIN2];
@@ -2135,6 +2319,10 @@ struct GraphBfs {
     uint64_t rest_cap = 0;
     unsigned push_grid = 0, pull_grid = 0, vgrid = 0;
     int flat = 0;  // built as one chain of kernels per step (knob graph_flat)
+    int stage_kb = 0;  // pull kernels built with this much dynamic shared memory (knob pull_stage)
+    int pdl = 0;       // the flat loop body's kernels joined by programmatic edges (knob graph_pdl)
+    int pdl_refused = 0;  // the runtime refused programmatic edges here: built without them
+    int unroll = 1;       // copies of the flat chain per loop iteration (knob graph_unroll)
     // page-locked host copies of the control block: the configuration sent
     // before a run, and the records a kernel writes back after it through the
     // mapping (no copy-engine transfer: a run's records do not queue behind
@@ -2151,12 +2339,13 @@ __global__ void k_copy_words16(const uint4 *__restrict__ src, uint4 *__restrict_
 }
 
 static gg_status add_kernel(gg_ctx *ctx, cudaGraph_t g, cudaGraphNode_t *node, const cudaGraphNode_t *deps, size_t nd,
-                            const void *fn, unsigned grid, unsigned block, GCtl **arg) {
+                            const void *fn, unsigned grid, unsigned block, GCtl **arg, unsigned smem = 0) {
     cudaKernelNodeParams kp;
     memset(&kp, 0, sizeof(kp));
     kp.func = (void *)fn;
     kp.gridDim = dim3(grid);
     kp.blockDim = dim3(block);
+    kp.sharedMemBytes = smem;
     void *args[] = {arg};
     kp.kernelParams = args;
     GG_CUDA(ctx, cudaGraphAddKernelNode(node, g, deps, nd, &kp));
@@ -2190,7 +2379,7 @@ void graph_bfs_free(gg_graph *g) {
     g->gbfs = nullptr;
 }
 
-static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
+static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb, int pdl) {
     gg_ctx *ctx = g->ctx;
     // (16 bytes of slack: the records' copy moves whole 16-byte words)
     GG_CUDA(ctx, cudaMalloc(&gb->ctl, sizeof(GCtl) + 16));
@@ -2198,7 +2387,15 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     GG_CUDA(ctx, cudaHostAlloc(&gb->h_rec, sizeof(GCtl) + 16, cudaHostAllocMapped));
     GG_CUDA(ctx, cudaHostGetDevicePointer((void **)&gb->d_rec, gb->h_rec, 0));
     gb->push_grid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_g_push, kBlock));
-    gb->pull_grid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_g_pull, kBlock));
+    // pulls that stage the frontier bitmap's first words take that much
+    // dynamic shared memory per CTA (fewer CTAs may then fit on an SM)
+    gb->stage_kb = tuning().pull_stage;
+    const unsigned stage_bytes = (unsigned)gb->stage_kb * 1024u;
+    int pull_occ = 0;
+    for (const void *fn : {(const void *)k_g_pull, (const void *)k_g_pull2})
+        GG_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes));
+    GG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pull_occ, (const void *)k_g_pull, kBlock, stage_bytes));
+    gb->pull_grid = (unsigned)(ctx->sm_count * std::max(pull_occ, 1));
     gb->vgrid = (unsigned)(ctx->sm_count * 8);
     GG_CUDA(ctx, cudaGraphCreate(&gb->graph, 0));
     cudaGraph_t G = gb->graph;
@@ -2227,10 +2424,25 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
         const unsigned grids[] = {gb->vgrid, 1, gb->push_grid, gb->vgrid, gb->pull_grid, gb->pull_grid,
                                   (unsigned)ctx->sm_count * 2};
         const unsigned blocks[] = {256, 1024, kBlock, 256, kBlock, kBlock, 256};
+        const unsigned smem[] = {0, 0, 0, 0, stage_bytes, stage_bytes, 0};
+        // with graph_pdl each kernel is launched while its predecessor runs
+        // (programmatic edge from the predecessor's trigger port; the kernel
+        // waits for the predecessor's completion in chain_enter)
+        gb->pdl = pdl;
+        cudaGraphEdgeData ed;
+        memset(&ed, 0, sizeof(ed));
+        ed.from_port = cudaGraphKernelNodePortProgrammatic;
+        ed.type = cudaGraphDependencyTypeProgrammatic;
+        // graph_unroll copies of the chain per loop iteration: the loop's own
+        // cost is paid once per copies steps (a run that ends in an earlier
+        // copy leaves the later copies' kernels with nothing to do)
+        gb->unroll = tuning().graph_unroll;
         cudaGraphNode_t prev = nullptr;
-        for (int i = 0; i < 7; ++i) {
+        for (int i = 0; i < 7 * gb->unroll; ++i) {
             cudaGraphNode_t nd;
-            GG_CHECK(add_kernel(ctx, body, &nd, prev ? &prev : nullptr, prev ? 1 : 0, chain[i], grids[i], blocks[i], arg));
+            GG_CHECK(add_kernel(ctx, body, &nd, (prev && !gb->pdl) ? &prev : nullptr, (prev && !gb->pdl) ? 1 : 0,
+                                chain[i % 7], grids[i % 7], blocks[i % 7], arg, smem[i % 7]));
+            if (prev && gb->pdl) GG_CUDA(ctx, cudaGraphAddDependencies_v2(body, &prev, &nd, &ed, 1));
             prev = nd;
         }
         GG_CUDA(ctx, cudaGraphInstantiate(&gb->exec, G, 0));
@@ -2260,9 +2472,10 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb) {
     GG_CHECK(add_kernel(ctx, bp, &n_push, &n_ifc, 1, (const void *)k_g_push, gb->push_grid, kBlock, arg));
     GG_CHECK(add_cond(ctx, bq, &n_ifb, nullptr, 0, hb, cudaGraphCondTypeIf, &bb));
     GG_CHECK(add_kernel(ctx, bb, &n_bits, nullptr, 0, (const void *)k_g_tobitmap, gb->vgrid, 256, arg));
-    GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_ifb, 1, (const void *)k_g_pull, gb->pull_grid, kBlock, arg));
+    GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_ifb, 1, (const void *)k_g_pull, gb->pull_grid, kBlock, arg, stage_bytes));
     cudaGraphNode_t n_pull2;
-    GG_CHECK(add_kernel(ctx, bq, &n_pull2, &n_pull, 1, (const void *)k_g_pull2, gb->pull_grid, kBlock, arg));
+    GG_CHECK(add_kernel(ctx, bq, &n_pull2, &n_pull, 1, (const void *)k_g_pull2, gb->pull_grid, kBlock, arg,
+                        stage_bytes));
     GG_CHECK(add_kernel(ctx, body, &n_next, &n_sw, 1, (const void *)k_g_next, (unsigned)ctx->sm_count * 2, 256, arg));
     GG_CUDA(ctx, cudaGraphInstantiate(&gb->exec, G, 0));
     // the handles live in the control block, set once
@@ -2279,14 +2492,28 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
         GraphBfs *gb = new (std::nothrow) GraphBfs;
         if (!gb) return GG_ERR_OOM;
         g->gbfs = gb;
-        gg_status s = graph_bfs_build(g, gb);
+        const int pdl = tuning().graph_flat && tuning().graph_pdl;
+        gg_status s = graph_bfs_build(g, gb, pdl);
+        if (s != GG_OK && pdl) {
+            // programmatic edges refused (in a conditional body, say): the
+            // plain chain, and no retry while the knobs stay as they are
+            graph_bfs_free(g);
+            cudaGetLastError();
+            gb = new (std::nothrow) GraphBfs;
+            if (!gb) return GG_ERR_OOM;
+            g->gbfs = gb;
+            s = graph_bfs_build(g, gb, 0);
+            gb->pdl_refused = 1;
+        }
         if (s != GG_OK) {
             graph_bfs_free(g);
             return s;
         }
     }
     GraphBfs *gb = (GraphBfs *)g->gbfs;
-    if (gb->flat != tuning().graph_flat) {  // built for the other loop shape
+    if (gb->flat != tuning().graph_flat || gb->stage_kb != tuning().pull_stage ||
+        (gb->flat && !gb->pdl_refused && gb->pdl != tuning().graph_pdl) ||
+        (gb->flat && gb->unroll != tuning().graph_unroll)) {  // built for another shape
         graph_bfs_free(g);
         return graph_bfs_level(g, root, opt, level, prev, st, iters_out);
     }
@@ -2342,11 +2569,12 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     h.word_prefix = g->heavy.pull_prefix;
     h.adj = g->adj;
     h.in_adj = g->in_adj;
-    h.first_in = t.pull_first ? g->first_in : nullptr;
-    h.lazy_off = t.pull_first == 2;
-    // the split pull's second pass starts at each row's third edge: it needs
-    // the first pass to have taken the first two from the first_in records
-    h.split = t.pull_split && h.first_in;
+    GG_CHECK(pull_records(g, t, &h.first_in, &h.first1, &h.rec_n, &h.lazy_off));
+    h.fresh_ok = t.pull_fresh;
+    h.stage_words = (uint32_t)gb->stage_kb * 256u;
+    // the split pull's second pass starts past the record's edges: it needs
+    // the first pass to have taken them from the records
+    h.split = t.pull_split && (h.first_in || h.first1);
     h.flat = gb->flat;
     if (h.split && gb->rest_cap < (uint64_t)g->n) {
         cudaFree(gb->rest);
@@ -2376,13 +2604,15 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     GG_CUDA(ctx, cudaMemcpyAsync(gb->ctl, &h, offsetof(GCtl, reached_v), cudaMemcpyHostToDevice, ctx->stream));
     GG_CUDA(ctx, cudaGraphLaunch(gb->exec, ctx->stream));
     // state and records back (one wait per run)
-    const size_t rec0 = offsetof(GCtl, variant), rec1 = offsetof(GCtl, h_while);
+    const size_t rec0 = offsetof(GCtl, variant), rec1 = sizeof(GCtl);
     GCtl *hr = gb->h_rec;
     const size_t w0 = rec0 / 16, w1 = (rec1 + 15) / 16;  // both bases are 16-byte aligned
     k_copy_words16<<<8, 256, 0, ctx->stream>>>((const uint4 *)gb->ctl + w0, (uint4 *)gb->d_rec + w0, w1 - w0);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) return cuda_error(ctx, e, "graph BFS");
+    if (hr->stage_timeouts)
+        return set_error(ctx, GG_ERR_TIMEOUT, "graph BFS: frontier bitmap staging copy did not complete in time");
     const int T = hr->iterations;
     *iters_out = T;
     // kernels the graph ran: init, then per iteration the step kernel and
@@ -2390,7 +2620,9 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     // where the variant changes); then the records' copy
     uint64_t npull = 0;
     for (int i = 0; i < T && i < GG_MAX_ITERS; ++i) npull += hr->variants[i] == GG_VAR_PULL_DENSE;
-    ctx->launches += gb->flat ? 2 + 7 * (uint64_t)T : 2 + 2 * (uint64_t)T + npull;
+    // (an unrolled chain: every copy of a started loop iteration)
+    const uint64_t per_loop = 7 * (uint64_t)gb->unroll;
+    ctx->launches += gb->flat ? 2 + per_loop * (((uint64_t)T + gb->unroll) / gb->unroll) : 2 + 2 * (uint64_t)T + npull;
     if (hr->handed_off) {
         // the rest of the run as one device-driven launch from the current
         // frontier (a push leaves it as a list only: add its bitmap)

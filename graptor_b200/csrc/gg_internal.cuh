@@ -138,8 +138,12 @@ struct gg_graph {
     uint64_t *aux_cnt = nullptr;  // counters of steps that record no frontier
     HeavyRows heavy;              // chunked long rows of the CSC (pull / gather)
     // per vertex {first two in-neighbours (CSC row order; 0xFFFFFFFF past the
-    // row's end), in-degree, 0}: most dense-pull rows find their parent there
+    // row's end), in-degree, third in-neighbour}: most dense-pull rows find
+    // their parent there
     uint4 *first_in = nullptr;
+    // per vertex {first in-neighbour, in-degree} (8 bytes; pull_first 4),
+    // built on first use
+    uint2 *first1 = nullptr;
     // gg_bfs_level_host_async: two level buffers used in turn, the stream
     // their host copies run on, and an event per buffer marking its copy done
     gg_prop *async_level[2] = {nullptr, nullptr};
@@ -216,6 +220,8 @@ gg_status graph_adopt_device_csr(gg_ctx *ctx, uint32_t n, uint64_t m, uint64_t *
                                  bool rows_sorted,
                                  gg_graph **out);
 gg_status graph_gini(gg_graph *g, float *out);
+// builds g->first1 (the 8-byte pull records) if it is not there yet
+gg_status graph_ensure_first1(gg_graph *g);
 void graph_bfs_free(gg_graph *g);
 void selector_features(float *x, double nactv, double nacte, double unreached, int iter, double n, double m,
                        float gini);
@@ -227,6 +233,8 @@ struct Tuning {
     int pull_k = 8;                 // per-lane edges before warp cooperation (pull)
     int pull_split = 1;             // graph-driven BFS pulls in two passes (first two in-edges, then the rest)
     int graph_flat = 1;             // graph-driven BFS: the loop body as one chain of kernels, no step conditionals
+    int graph_pdl = 0;              // graph-driven BFS (flat): the chain's kernels joined by programmatic edges
+    int graph_unroll = 2;           // graph-driven BFS (flat): copies of the chain per loop iteration (1-4)
     int push_k = 8;
     int block = 256;
     int blocks_per_sm = 8;
@@ -267,11 +275,23 @@ struct Tuning {
     // road-network test (fewer than n/10 zero labels) and, where it holds,
     // min-id hooking for the rest of the run
     int cc_hook = 1;
-    // dense pull: each row's first two in-neighbours read from a per-vertex
-    // record (coalesced with the row's offsets) before the row itself;
-    // 2: the record's degree stands in for the offsets, which are loaded only
-    // for rows the first two edges do not settle; 0: rows only
-    int pull_first = 1;
+    // dense pull: each row's first in-neighbours read from a per-vertex
+    // record (coalesced with the row's offsets) before the row itself.
+    // 1: the 16-byte record's first two, offsets loaded with the record;
+    // 2: the same two, the record's degree standing in for the offsets, which
+    // are loaded only for rows the two edges do not settle; 3: as 2 with the
+    // record's three in-neighbours; 4: an 8-byte record {first in-neighbour,
+    // degree}, offsets as in 2; 0: rows only.  3, the default, measured
+    // fastest on R-MAT 24 BFS (dense pull 14 % under mode 1)
+    int pull_first = 3;
+    // graph-driven BFS pull: KiB of the frontier bitmap's first words (the
+    // lowest vertex ids) copied into each CTA's shared memory by a bulk copy
+    // (TMA) before the pull; probes of those ids read shared memory; 0: none
+    int pull_stage = 0;
+    // graph-driven BFS pull after a pull: its candidates are the previous
+    // pull's unsettled rows, so their levels are known (unvisited) and not
+    // loaded
+    int pull_fresh = 1;
     unsigned long long barrier_timeout_ns = 5000000000ull;  // grid-barrier wait limit
 };
 Tuning &tuning();

@@ -397,13 +397,15 @@ def test_pagerank_staged_matches_restatement(ctx, stages):
     assert np.abs(x.astype(np.float64) - x64).sum() <= 1e-5  # the FP32 stage restores full accuracy
 
 
-@pytest.mark.parametrize("mode", [0, 1, 2])
+@pytest.mark.parametrize("mode", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("gen", ["rmat", "grid", "er_directed"])
 def test_pull_first_record_modes_exact(ctx, mode, gen):
     """The dense pull's per-vertex record of first in-neighbours (knob
     pull_first: 0 rows only, 1 record then rows, 2 record with the offsets
-    loaded only for rows it does not settle): BFS levels, parents and CC
-    labels identical to the oracle's in every mode, host- and graph-driven."""
+    loaded only for rows it does not settle, 3 the same with three
+    in-neighbours, 4 an 8-byte record of one in-neighbour and the degree):
+    BFS levels, parents and CC labels identical to the oracle's in every
+    mode, host- and graph-driven."""
     if gen == "rmat":
         og, sym = O.rmat(14, 16 << 14, seed=81), True
     elif gen == "grid":
@@ -432,7 +434,7 @@ def test_pull_first_record_modes_exact(ctx, mode, gen):
         g.close()
 
 
-@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("mode", [1, 2, 3, 4])
 @pytest.mark.parametrize("gen", ["rmat", "grid", "er_directed", "edgecases"])
 def test_split_pull_exact(ctx, mode, gen):
     """Graph-driven BFS with the split pull (knob pull_split: the first pass
@@ -466,6 +468,52 @@ def test_split_pull_exact(ctx, mode, gen):
                 lv = O.bfs_level(og, r)
                 assert np.array_equal(g.bfs_level(r), lv), (mode, flat, r)
                 assert np.array_equal(g.bfs_level(r, opts=gg.default_opts(variant=gg.VAR_PULL_DENSE)), lv), (mode, r)
+    finally:
+        for k, v in old.items():
+            gg.tuning_set(k, v)
+        g.close()
+
+
+@pytest.mark.parametrize("stage", [0, 4, 16])
+@pytest.mark.parametrize("gen", ["rmat18", "rmat12", "er_directed", "edgecases"])
+def test_pull_stage_and_fresh_exact(ctx, stage, gen):
+    """Graph-driven BFS pulls that probe the frontier bitmap's first words
+    from a shared-memory copy made by a bulk copy (knob pull_stage: KiB per
+    CTA; the R-MAT 18 bitmap is 32 KiB, so 4 and 16 cover part of it, the
+    R-MAT 12 bitmap 512 bytes, which any stage covers whole; the edge-case
+    graph's bitmap is under 16 bytes, too small to stage) and that skip the
+    level loads of candidates a pull left open (knob pull_fresh): levels
+    identical to the oracle's with and without the split pull, with the
+    threshold's variants and with every step a pull, and every record mode."""
+    if gen == "rmat18":
+        og, sym = O.rmat(18, 16 << 18, seed=83), True
+    elif gen == "rmat12":
+        og, sym = O.rmat(12, 8 << 12, seed=84), True
+    elif gen == "er_directed":
+        og, sym = O.er(7000, 8.0, seed=10, dangling_bp=100, symmetric=False), False
+    else:
+        z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "edgecases32.npz"))
+        og, sym = O.Graph(int(z["n"]), z["off"], z["adj"]), True
+    g = ctx.upload(og.off, og.adj, sym)
+    knobs = ("pull_first", "graph", "pull_split", "pull_stage", "pull_fresh")
+    old = {k: gg.tuning_get(k) for k in knobs}
+    try:
+        gg.tuning_set("graph", 1)
+        gg.tuning_set("pull_stage", stage)
+        deg = og.outdeg()
+        nz = np.flatnonzero(deg)
+        roots = [int(np.argmax(deg)), int(nz[len(nz) // 3]), int(nz[-1])]
+        want = {r: O.bfs_level(og, r) for r in roots}
+        for mode in (1, 3, 4):
+            gg.tuning_set("pull_first", mode)
+            for split in (1, 0):
+                gg.tuning_set("pull_split", split)
+                for fresh in (1, 0):
+                    gg.tuning_set("pull_fresh", fresh)
+                    for r in roots:
+                        assert np.array_equal(g.bfs_level(r), want[r]), (mode, split, fresh, r)
+                        got = g.bfs_level(r, opts=gg.default_opts(variant=gg.VAR_PULL_DENSE))
+                        assert np.array_equal(got, want[r]), (mode, split, fresh, r, "pull")
     finally:
         for k, v in old.items():
             gg.tuning_set(k, v)

@@ -243,6 +243,59 @@ def test_graph_bfs_handoff_to_device_driven(ctx, fusion_knobs, gen):
     g.close()
 
 
+@pytest.mark.parametrize("unroll", [1, 2, 3])
+@pytest.mark.parametrize("pdl", [0, 1])
+@pytest.mark.parametrize("gen", ["rmat", "er_directed", "grid"])
+def test_graph_loop_shapes_exact(ctx, fusion_knobs, gen, pdl, unroll):
+    """The graph-driven BFS loop with its chain of kernels copied 1-3 times
+    per loop iteration (knob graph_unroll: a run ends in any copy, the later
+    copies then do nothing) and with the chain's kernels joined by
+    programmatic edges or plain ones (knob graph_pdl): the oracle's levels
+    and the host loop's iteration count, frontier sizes and variants, with
+    and without the hand-over to the device-driven traversal."""
+    knobs = ("graph", "graph_handoff", "persistent", "graph_unroll", "graph_pdl", "graph_flat")
+    old = {k: gg.tuning_get(k) for k in knobs}
+    if gen == "rmat":
+        og, sym = O.rmat(15, 16 << 15, seed=66), True
+    elif gen == "er_directed":
+        og, sym = O.er(30000, 6.0, seed=5, dangling_bp=200, symmetric=False), False
+    else:
+        og, sym = O.grid(70, 40, seed=9, del_bp=300), True
+    g = ctx.upload(og.off, og.adj, symmetric=sym)
+    deg = og.outdeg()
+    nz = np.flatnonzero(deg)
+    roots = [int(np.argmax(deg)), int(nz[len(nz) // 2])]
+    try:
+        gg.tuning_set("persistent", 0)
+        gg.tuning_set("graph", 0)
+        want = {}
+        for r in roots:
+            s0 = gg.RunStats()
+            lv = g.bfs_level(r, opts=gg.default_opts(collect=True), stats=s0)
+            assert np.array_equal(lv, O.bfs_level(og, r))
+            want[r] = (lv, s0)
+        gg.tuning_set("graph", 1)
+        gg.tuning_set("graph_flat", 1)
+        gg.tuning_set("graph_pdl", pdl)
+        gg.tuning_set("graph_unroll", unroll)
+        for h in (0, 3, 32):
+            gg.tuning_set("graph_handoff", h)
+            for r in roots:
+                ref, s0 = want[r]
+                k0 = min(s0.iterations, gg.MAX_ITERS)
+                for _ in range(2):
+                    st = gg.RunStats()
+                    lv = g.bfs_level(r, opts=gg.default_opts(collect=True), stats=st)
+                    assert np.array_equal(lv, ref), (gen, h, r)
+                    assert st.iterations == s0.iterations, (gen, h, r)
+                    assert [st.nactv[i] for i in range(k0)] == [s0.nactv[i] for i in range(k0)], (gen, h, r)
+                    assert [st.variant[i] for i in range(k0)] == [s0.variant[i] for i in range(k0)], (gen, h, r)
+    finally:
+        for k, v in old.items():
+            gg.tuning_set(k, v)
+    g.close()
+
+
 @pytest.mark.parametrize("gen", ["rmat", "er_directed", "grid", "chain"])
 def test_small_frontier_kernel_equals_cooperative(ctx, fusion_knobs, gen):
     """Device-driven BFS levels with the one-CTA small-frontier kernel on and
