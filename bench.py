@@ -219,9 +219,9 @@ def pick_roots(deg: np.ndarray) -> np.ndarray:
 
 
 # DRAM bytes (read + write) per dense-pull launch, from one ncu capture of
-# k_pull with the first-in-neighbour records (4 launches of R-MAT scale 23
-# BFS, 246.2 MB each on average) scaled by the vertex count to scale 24
-K_PULL_TRAFFIC_PER_LAUNCH = 492.4e6
+# k_pull with the three-neighbour records (4 launches of R-MAT scale 23 BFS,
+# 245.0 MB each on average) scaled by the vertex count to scale 24
+K_PULL_TRAFFIC_PER_LAUNCH = 490.0e6
 
 
 def bfs_bytes(n: int, st, it: int) -> float:

@@ -1695,6 +1695,7 @@ struct GCtl {
     int clr;  // written by the step kernel: 1 + the frontier whose bitmap `next` clears, or 0
     const __nv_bfloat16 *sel_w;  // learned selector weights (bfloat16), or null: the threshold decides
     float gini;
+    float sel_x4, sel_x9;  // the selector's per-graph features (average degree, size)
     // last network evaluation: reused while the frontier counts stay within 1/16
     unsigned long long sel_nactv, sel_nacte, sel_unr;
     int sel_iter, sel_push, sel_valid;
@@ -1750,7 +1751,7 @@ __device__ __forceinline__ bool d_threshold_sparse(int kind, int k, uint64_t nac
     }
 }
 
-__device__ void decide_step(GCtl *c, GCtl *h);
+__device__ void decide_step(GCtl *c, GCtl *h, const mlp::LaneWeights *lw = nullptr);
 
 // Programmatic dependent launch (knob graph_pdl): the loop body's kernels
 // are joined by programmatic edges, so each is launched while its
@@ -1815,7 +1816,7 @@ __global__ void k_g_init(GCtl *c) {
 // counts, writes the step's arguments, sets the branch and loop conditions
 // Called by the 32 lanes of one warp (the network is evaluated by a warp);
 // lane 0 writes the decision.
-__device__ void decide_step(GCtl *c, GCtl *h) {
+__device__ void decide_step(GCtl *c, GCtl *h, const mlp::LaneWeights *lw) {
     const uint32_t lane = threadIdx.x & 31u;
     const GFront F = h->f[h->cur], O = h->f[h->cur ^ 1];
     const unsigned long long nactv = F.cnt[FC_NACTV], nacte = F.cnt[FC_NACTE];
@@ -1851,22 +1852,28 @@ __device__ void decide_step(GCtl *c, GCtl *h) {
         push = h->sel_push != 0;  // the last evaluation still applies
     } else if (h->sel_w) {
         // learned choice between the two variants this driver runs: the
-        // threshold's stands unless the network predicts a clear gain
-        const double n = h->n, m = (double)h->m, fv = (double)nactv, fe = (double)nacte;
-        const double unr = (double)unr_c;
+        // threshold's stands unless the network predicts a clear gain.
+        // Features in single precision (the graph's constant ones come from
+        // the host): the network's inputs are floats either way.
+        const float n = (float)h->n, m = (float)h->m, fv = (float)nactv, fe = (float)nacte;
         float x[GG_SEL_FEATURES];
-        x[0] = (float)(log2(1.0 + fv) / 32);
-        x[1] = (float)(log2(1.0 + fe) / 40);
-        x[2] = (float)(log2(1.0 + unr) / 32);
-        x[3] = (float)(log2(1.0 + min(iter, 255)) / 8);
-        x[4] = (float)(log2(1.0 + (n > 0 ? m / n : 0)) / 8);
+        x[0] = log2f(1.0f + fv) / 32;
+        x[1] = log2f(1.0f + fe) / 40;
+        x[2] = log2f(1.0f + (float)unr_c) / 32;
+        x[3] = log2f(1.0f + (float)min(iter, 255)) / 8;
+        x[4] = h->sel_x4;
         x[5] = h->gini;
-        x[6] = (float)(n > 0 ? fv / n : 0);
-        x[7] = (float)(m > 0 ? fe / m : 0);
-        x[8] = (float)fmin(4.0, m > 0 ? (fv + fe) / m : 0.0);
-        x[9] = (float)(log2(n > 1 ? n : 1.0) / 32);
-        float o[GG_SEL_VARIANTS], z1, a1, z2, a2;
-        mlp::warp_forward(h->sel_w, x, o, z1, a1, z2, a2);
+        x[6] = n > 0 ? fv / n : 0.0f;
+        x[7] = m > 0 ? fe / m : 0.0f;
+        x[8] = fminf(4.0f, m > 0 ? (fv + fe) / m : 0.0f);
+        x[9] = h->sel_x9;
+        float o[GG_SEL_VARIANTS];
+        if (lw) {
+            mlp::warp_forward_regs(*lw, x, o);
+        } else {
+            float z1, a1, z2, a2;
+            mlp::warp_forward(h->sel_w, x, o, z1, a1, z2, a2);
+        }
         const int tv = push ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
         const int best = o[GG_VAR_PUSH_SPARSE] < o[GG_VAR_PULL_DENSE] ? GG_VAR_PUSH_SPARSE : GG_VAR_PULL_DENSE;
         if (o[best] < o[tv] - mlp::kSelMargin) push = best == GG_VAR_PUSH_SPARSE;
@@ -2223,12 +2230,17 @@ __global__ void __launch_bounds__(256) k_g_next(GCtl *c) {
     // back: one global round trip instead of one per dependent field
     __shared__ __align__(16) unsigned char s_head[kCtlHead];
     const uint32_t lane = threadIdx.x;
+    const __nv_bfloat16 *sel_w = c->sel_w;
     for (uint32_t i = lane; i < kCtlHead / 16; i += 32) ((uint4 *)s_head)[i] = ((const uint4 *)c)[i];
+    // the selector's weights, if any, are loaded now and arrive while the
+    // bookkeeping and the frontier counts are read
+    mlp::LaneWeights lw;
+    if (sel_w) mlp::load_lane(sel_w, lw);
     __syncwarp();
     GCtl *h = (GCtl *)s_head;
     if (lane == 0) g_bookkeep(c, h);
     __syncwarp();
-    decide_step(c, h);  // an empty frontier or the iteration bound ends the loop
+    decide_step(c, h, sel_w ? &lw : nullptr);  // an empty frontier or the iteration bound ends the loop
     __syncwarp();
     for (uint32_t i = lane; i < kCtlHead / 16; i += 32) ((uint4 *)c)[i] = ((const uint4 *)s_head)[i];
 }
@@ -2557,6 +2569,10 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
         }
         h.sel_w = (const __nv_bfloat16 *)selector_weights(g);
         h.gini = g->gini < 0 ? 0.0f : g->gini;
+        float xs[GG_SEL_FEATURES];
+        selector_features(xs, 0, 0, 0, 0, (double)g->n, (double)g->m, h.gini);
+        h.sel_x4 = xs[4];
+        h.sel_x9 = xs[9];
     }
     h.smax = t.bin_small_max;
     h.mmax = t.bin_medium_max;

@@ -54,5 +54,47 @@ __device__ __forceinline__ void warp_forward(const W *w, const float *x, float *
     }
 }
 
+// One lane's share of the network (hidden unit j = lane: its rows of the
+// two hidden layers, its column of the output layer, the output biases),
+// loaded into registers ahead of use so that the loads overlap other work.
+struct LaneWeights {
+    float w1[IN], b1, w2[H], b2, w3[OUT], b3[OUT];
+};
+
+template <typename W>
+__device__ __forceinline__ void load_lane(const W *w, LaneWeights &L) {
+    const int j = threadIdx.x & 31;
+#pragma unroll
+    for (int i = 0; i < IN; ++i) L.w1[i] = wv(w, OW1 + j * IN + i);
+    L.b1 = wv(w, OB1 + j);
+#pragma unroll
+    for (int k = 0; k < H; ++k) L.w2[k] = wv(w, OW2 + j * H + k);
+    L.b2 = wv(w, OB2 + j);
+#pragma unroll
+    for (int v = 0; v < OUT; ++v) {
+        L.w3[v] = wv(w, OW3 + v * H + j);
+        L.b3[v] = wv(w, OB3 + v);
+    }
+}
+
+// warp_forward on weights already in registers (same arithmetic, same order)
+__device__ __forceinline__ void warp_forward_regs(const LaneWeights &L, const float *x, float *out) {
+    float acc = L.b1;
+#pragma unroll
+    for (int i = 0; i < IN; ++i) acc = fmaf(L.w1[i], x[i], acc);
+    const float a1 = fmaxf(acc, 0.0f);
+    acc = L.b2;
+#pragma unroll
+    for (int k = 0; k < H; ++k) acc = fmaf(L.w2[k], __shfl_sync(0xffffffffu, a1, k), acc);
+    const float a2 = fmaxf(acc, 0.0f);
+#pragma unroll
+    for (int v = 0; v < OUT; ++v) {
+        float p = L.w3[v] * a2;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) p += __shfl_xor_sync(0xffffffffu, p, o);
+        out[v] = p + L.b3[v];
+    }
+}
+
 }  // namespace mlp
 }  // namespace gg
