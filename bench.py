@@ -376,6 +376,17 @@ def reference_leg(g, roots, args, lvl):
                                               np.maximum(x_ref, 1e-30)).max())
             par["pr_reference_ms_per_iter"] = round(min(pr_t) * 1e3 / 20, 2) if pr_t else None
             par["cc_pr_wall_s"] = round(time.time() - tc, 1)
+            if O.ref_available("KC_bucket"):
+                tc = time.time()
+                try:
+                    core_ref, kc_t = O.ref_kc(path, os.path.join(tmp, "kc.txt"), threads=cores)
+                    core, largest = g.kcore()
+                    par["kc_bitexact"] = bool(np.array_equal(core, core_ref))
+                    par["kc_largest"] = largest
+                    par["kc_reference_ms"] = round(kc_t * 1e3, 2) if kc_t else None
+                except Exception as e:  # recorded, never fatal
+                    par["kc_check_failed"] = f"{e}"[:300]
+                par["kc_wall_s"] = round(time.time() - tc, 1)
     return cpu, par
 
 
@@ -902,6 +913,21 @@ def run_ours(args, ws, rank, local):
                      "whole_run_frac_of_hbm": round(cc_all / (cc_best / 1e3) / 1e9 / hbm_peak, 4),
                      "one_pass_frac_of_hbm": round(cc_pass / (cc_best / 1e3) / 1e9 / hbm_peak, 4)}
 
+        # ---- k-core (KC_bucket: peel floors with count-down pushes) ----
+        core = g.prop(gg.U32)
+        g.kcore(coreness=core, host=False)
+        kc_ms = []
+        for _ in range(3):
+            st = gg.RunStats()
+            _, kc_largest = g.kcore(coreness=core, host=False, stats=st)
+            kc_ms.append(st.total_ms)
+        kc_best = float(np.median(kc_ms))
+        # one count-down per edge end (every edge is pushed from both ends)
+        out["kcore"] = {"ms": round(kc_best, 3), "gedges_per_s": round(m / (kc_best / 1e3) / 1e9, 3),
+                        "largest_core": kc_largest, "peel_steps": st.iterations,
+                        "floors": int(st.vertices_reached), "kernels": int(st.kernels)}
+        core.close()
+
         # ---- PageRank (PRv: FP32 storage, double gather accumulation, 20 iterations) ----
         x = g.prop(gg.F32)
         prs = {}
@@ -1045,6 +1071,7 @@ def run_ours(args, ws, rank, local):
 #   python bench.py --case bfs   --scale 24 --roots 4
 #   python bench.py --case pr    --scale 24 --format bf16 --iters 5
 #   python bench.py --case cc    --graph grid --side 2896
+#   python bench.py --case kc    --scale 24
 #   python bench.py --case msbfs --scale 22
 #   python bench.py --case ppr   --scale 22 --iters 5
 # ---------------------------------------------------------------------------
@@ -1116,6 +1143,17 @@ def run_case(a):
             g.cc(host=False, opts=gg.default_opts(gg.THRESH_FRAC, 5, collect=True), stats=st)
             ts.append(st.total_ms)
         out.update(ms=round(float(np.median(ts)), 4), iterations=iter_table(st))
+    elif a.case == "kc":
+        for _ in range(a.warmup):
+            g.kcore(host=False)
+        ts = []
+        for _ in range(a.reps):
+            st = gg.RunStats()
+            _, largest = g.kcore(host=False, opts=gg.default_opts(collect=a.reps == 1), stats=st)
+            ts.append(st.total_ms)
+        out.update(ms=round(float(np.median(ts)), 4), largest_core=largest, peel_steps=st.iterations,
+                   floors=int(st.vertices_reached), kernels=int(st.kernels),
+                   iterations=iter_table(st) if a.reps == 1 else None)
     elif a.case == "pr":
         fmt = case_formats()[a.format]
         for _ in range(a.warmup):
@@ -1171,7 +1209,7 @@ def main():
     ap.add_argument("--no-precision", action="store_true", help="skip the PageRank precision workloads")
     ap.add_argument("--batch-graphs", type=int, default=2000, help="small graphs in the union workload")
     # single workloads for profilers
-    ap.add_argument("--case", default=None, choices=["bfs", "pr", "cc", "msbfs", "ppr"],
+    ap.add_argument("--case", default=None, choices=["bfs", "pr", "cc", "kc", "msbfs", "ppr"],
                     help="run one workload for a profiler instead of the benchmark")
     ap.add_argument("--graph", default="rmat", choices=["rmat", "grid", "er"])
     ap.add_argument("--side", type=int, default=2048)

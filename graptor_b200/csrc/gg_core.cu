@@ -562,6 +562,9 @@ static void graph_free(gg_graph *g) {
     cudaFree(g->nonisolated_n);
     cudaFree(g->first_in);
     cudaFree(g->first1);
+    cudaFree(g->kc_alive[0]);
+    cudaFree(g->kc_alive[1]);
+    cudaFree(g->kc_cnt);
     cudaFree(g->pstate2);
     for (int i = 0; i < 2; ++i) {
         if (g->copy_done[i]) {

@@ -118,16 +118,19 @@ struct Op {
         if constexpr (R == GG_RELAX_MIN_PLUS1_I32) return level_sync ? (V)fk : a[s] + 1;
         else if constexpr (R == GG_RELAX_MIN_U32) return a[s];
         else if constexpr (R == GG_RELAX_OR_U32) return b[s];
+        else if constexpr (R == GG_RELAX_COUNT_DOWN_U32) return 1u;  // every active source takes one
         else return (V)s;
     }
     __device__ __forceinline__ bool better(V x, V best) const {
         if constexpr (R == GG_RELAX_SETIF_U32) return ((uint32_t)best >> 31) != 0;
         else if constexpr (R == GG_RELAX_OR_U32) return (best | x) != best;
+        else if constexpr (R == GG_RELAX_COUNT_DOWN_U32) return (int64_t)best > fk;
         else return x < best;
     }
     // the value after a better offer x
     __device__ __forceinline__ V combine(V best, V x) const {
         if constexpr (R == GG_RELAX_OR_U32) return best | x;
+        else if constexpr (R == GG_RELAX_COUNT_DOWN_U32) return best - 1u;
         else return x;
     }
     // the row's value after the lanes with ok set (mask okm) offered theirs
@@ -136,6 +139,10 @@ struct Op {
             return __shfl_sync(FULL, x, __ffs(okm) - 1);
         } else if constexpr (R == GG_RELAX_OR_U32) {
             return best | __reduce_or_sync(FULL, ok ? x : 0u);
+        } else if constexpr (R == GG_RELAX_COUNT_DOWN_U32) {
+            // one off per active source, not below the floor
+            const int64_t v = (int64_t)best - (int64_t)__popc(okm);
+            return v > fk ? (V)v : (V)fk;
         } else {
             V mine = ok ? x : none();
             return __reduce_min_sync(FULL, mine);
@@ -154,6 +161,20 @@ struct Op {
             if ((cur | sv) == cur) return false;
             old = atomicOr(a + d, sv);
             if ((old | sv) == old) return false;
+        } else if constexpr (R == GG_RELAX_COUNT_DOWN_U32) {
+            // count_down_value(k): the filter saw a[d] > k; a take that finds
+            // the count at the floor already (others took it meanwhile) is
+            // given back, so the count never stays below k, and exactly one
+            // take sees k + 1: the one that brings d to the floor.  Many
+            // concurrent takes can carry the count below zero for a moment:
+            // counts are below 2^31, so a count read as negative is below
+            // the floor too.
+            old = atomicSub(a + d, 1u);
+            if ((int32_t)old < 0 || (int64_t)old <= fk) {
+                atomicAdd(a + d, 1u);
+                return false;
+            }
+            if (record == GG_RECORD_AT_FLOOR) return (int64_t)old == fk + 1;
         } else {
             if (!(sv < cur)) return false;
             old = atomicMin(a + d, sv);
@@ -418,6 +439,8 @@ __device__ __forceinline__ void pull_body(const EmapArgs &A, const Op<R> &op, Pu
                 }
             } else if (A.record == GG_RECORD_REDUCTION) {
                 rec = true;
+            } else if (A.record == GG_RECORD_AT_FLOOR) {
+                rec = (int64_t)best == op.fk;  // COUNT_DOWN: counted down to the floor now
             }
         }
         if (A.out_bits) {
@@ -1473,8 +1496,17 @@ gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_f
         return GG_OK;
     }
     const gg_dtype want = d->relax == GG_RELAX_MIN_PLUS1_I32 ? GG_I32 : GG_U32;
-    if (d->relax < 0 || (d->relax > GG_RELAX_SETIF_U32 && d->relax != GG_RELAX_OR_U32))
+    if (d->relax < 0 ||
+        (d->relax > GG_RELAX_SETIF_U32 && d->relax != GG_RELAX_OR_U32 && d->relax != GG_RELAX_COUNT_DOWN_U32))
         return set_error(ctx, GG_ERR_ARG, "unknown relax kind");
+    if (d->relax == GG_RELAX_COUNT_DOWN_U32) {
+        if (d->dst_filter != GG_FILTER_GT_CONST || d->dst_filter_k < 0 || d->dst_filter_k > 0xFFFFFFFFll)
+            return set_error(ctx, GG_ERR_ARG, "COUNT_DOWN takes dst filter GT_CONST with the floor k");
+        if (d->record != GG_RECORD_NONE && d->record != GG_RECORD_REDUCTION && d->record != GG_RECORD_AT_FLOOR)
+            return set_error(ctx, GG_ERR_UNSUPPORTED, "COUNT_DOWN records NONE, REDUCTION or AT_FLOOR");
+    } else if (d->record == GG_RECORD_AT_FLOOR) {
+        return set_error(ctx, GG_ERR_UNSUPPORTED, "record AT_FLOOR belongs to COUNT_DOWN");
+    }
     if (d->relax == GG_RELAX_OR_U32 && (!d->src || d->src->g != g || d->src->t != GG_U32))
         return set_error(ctx, GG_ERR_ARG, "OR_U32 needs a uint32 source property of g");
     if (d->a->t != want) return set_error(ctx, GG_ERR_ARG, "relaxed property has the wrong dtype");
@@ -1522,6 +1554,7 @@ gg_status edgemap_impl(gg_graph *g, const gg_emap_desc *d, gg_frontier *in, gg_f
     case GG_RELAX_MIN_PLUS1_I32: s = launch_variant<GG_RELAX_MIN_PLUS1_I32>(g, d, in, out, variant); break;
     case GG_RELAX_MIN_U32: s = launch_variant<GG_RELAX_MIN_U32>(g, d, in, out, variant); break;
     case GG_RELAX_OR_U32: s = launch_variant<GG_RELAX_OR_U32>(g, d, in, out, variant); break;
+    case GG_RELAX_COUNT_DOWN_U32: s = launch_variant<GG_RELAX_COUNT_DOWN_U32>(g, d, in, out, variant); break;
     default: s = launch_variant<GG_RELAX_SETIF_U32>(g, d, in, out, variant); break;
     }
     if (stats && s == GG_OK) cudaEventRecord(ctx->evk1, ctx->stream);
@@ -2984,6 +3017,205 @@ gg_status gg_cc(gg_graph *g, const gg_run_opts *o, gg_prop *label, uint32_t *hos
         st->kernels = ctx->launches - k0;
     }
     if (host_label) GG_CHECK(gg_prop_download(label, host_label));
+    return gg_ctx_sync(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// k-core decomposition (KC_bucket, bench/KC_bucket.C:107-420)
+// ---------------------------------------------------------------------------
+// count[v] starts at v's degree (KC_bucket.C:125-133: coreness = degree).
+// For floors L = 0, 1, 2, ... the alive list (vertices not peeled yet, all
+// vertices before the first floor) is scanned once: vertices whose count is
+// L form the peel frontier F (degree-binned, with its counts), vertices above
+// L stay alive, and the smallest count among those is kept.  F's vertices
+// have coreness L; each peel step counts their alive neighbours down towards
+// L (edgemap: COUNT_DOWN with floor L, record AT_FLOOR) and the vertices that
+// reach L form the next step's F, until none does (the reference's bucket for
+// K and its fused re-insertions, KC_bucket.C:290-420).  A floor whose scan
+// finds no vertex jumps to the smallest count left.  Where the reference
+// keeps 127 buckets of vertex lists and moves vertices between them, this
+// keeps one alive list that every floor compacts.
+// count = degree; ngt1 counts the vertices of degree above one
+__global__ void __launch_bounds__(256) k_kc_init(const uint64_t *__restrict__ off, uint32_t n,
+                                                 uint32_t *__restrict__ count, unsigned long long *ngt1) {
+    unsigned long long k = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t deg = off[v + 1] - off[v];
+        count[v] = deg > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)deg;
+        k += deg > 1;
+    }
+    k = dev::block_sum<unsigned long long, 256>(k);
+    if (threadIdx.x == 0 && k) atomicAdd(ngt1, k);
+}
+
+// The reference's degree-one preprocessing (KC_bucket.C:131-160), taken
+// when fewer than n/2 vertices have a degree above one, raises every count
+// to at least 1 and leaves isolated vertices (in no bucket) at that 1: its
+// output reports coreness 1 for them then, as this does.
+__global__ void __launch_bounds__(256) k_kc_isolated(const uint64_t *__restrict__ off, uint32_t n,
+                                                     uint32_t *__restrict__ count) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        if (off[v + 1] == off[v]) count[v] = 1u;
+}
+
+// alive == nullptr: every vertex (the first floor)
+__global__ void __launch_bounds__(256) k_kc_scan(const uint32_t *__restrict__ alive, uint64_t nall,
+                                                 const unsigned long long *__restrict__ alive_n,
+                                                 const uint32_t *__restrict__ count, uint32_t L,
+                                                 const uint64_t *__restrict__ off, uint32_t smax, uint32_t mmax,
+                                                 uint32_t *b0, uint32_t *b1, uint32_t *b2,
+                                                 unsigned long long *fcnt, uint32_t *alive_out,
+                                                 unsigned long long *alive_out_n, unsigned long long *min_left) {
+    __shared__ uint32_t sb[4][8][256];
+    const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    dev::WarpAppender<256> ap0{sb[0][wib], 0, b0, fcnt + FC_BIN0};
+    dev::WarpAppender<256> ap1{sb[1][wib], 0, b1, fcnt + FC_BIN1};
+    dev::WarpAppender<256> ap2{sb[2][wib], 0, b2, fcnt + FC_BIN2};
+    dev::WarpAppender<256> keep{sb[3][wib], 0, alive_out, alive_out_n};
+    const uint64_t na = alive ? (uint64_t)*alive_n : nall;
+    unsigned long long nv = 0, ne = 0;
+    uint32_t mn = 0xFFFFFFFFu;
+    const uint64_t step = (uint64_t)gridDim.x * 256;
+    for (uint64_t base = ((uint64_t)blockIdx.x * 8 + wib) * 32; base < na; base += step) {
+        const uint64_t i = base + lane;
+        uint32_t v = 0;
+        bool at = false, above = false;
+        uint64_t deg = 0;
+        if (i < na) {
+            v = alive ? alive[i] : (uint32_t)i;
+            const uint32_t c = count[v];
+            at = c == L;
+            above = c > L;
+            if (at) deg = off[v + 1] - off[v];
+            if (above) mn = min(mn, c);
+        }
+        ap0.push(at && deg <= smax, v);
+        ap1.push(at && deg > smax && deg <= mmax, v);
+        ap2.push(at && deg > mmax, v);
+        keep.push(above, v);
+        if (at) {
+            nv++;
+            ne += deg;
+        }
+    }
+    ap0.flush();
+    ap1.flush();
+    ap2.flush();
+    keep.flush();
+    mn = __reduce_min_sync(FULL, mn);
+    if (lane == 0 && mn != 0xFFFFFFFFu) atomicMin(min_left, (unsigned long long)mn);
+    nv = dev::block_sum<unsigned long long, 256>(nv);
+    ne = dev::block_sum<unsigned long long, 256>(ne);
+    if (threadIdx.x == 0) {
+        if (nv) atomicAdd(fcnt + FC_NACTV, nv);
+        if (ne) atomicAdd(fcnt + FC_NACTE, ne);
+    }
+}
+
+gg_status gg_kcore(gg_graph *g, const gg_run_opts *o, gg_prop *coreness, uint32_t *host_coreness,
+                   uint32_t *largest_core, gg_run_stats *st) {
+    if (!g) return GG_ERR_ARG;
+    gg_ctx *ctx = g->ctx;
+    if (!g->symmetric) return set_error(ctx, GG_ERR_UNSUPPORTED, "gg_kcore: symmetric graphs only");
+    if (coreness && (coreness->g != g || coreness->t != GG_U32))
+        return set_error(ctx, GG_ERR_ARG, "coreness must be a U32 property of g");
+    // Sparse push by default: a count-down pull has no early exit, so one warp
+    // walks each high-degree row whole (measured at R-MAT 22: 34.5 ms with
+    // every step a push against 218 ms with the m/20 threshold, whose few
+    // pulls took most of it)
+    gg_run_opts opt;
+    default_opts(o, &opt, GG_THRESH_ALWAYS_SPARSE, 0);
+    if (opt.threshold == GG_THRESH_LEARNED) opt.threshold = GG_THRESH_ALWAYS_SPARSE;  // no network for this relax
+    if (!coreness) GG_CHECK(tmp_prop(g, 2, GG_U32, &coreness));
+    if (st) memset(st, 0, sizeof(*st));
+    if (!g->kc_cnt) {
+        for (auto &a : g->kc_alive) GG_CUDA(ctx, cudaMalloc(&a, ((size_t)g->n + 1) * 4));
+        GG_CUDA(ctx, cudaMalloc(&g->kc_cnt, 4 * sizeof(unsigned long long)));
+    }
+    const Tuning &t = tuning();
+    cudaStream_t sm = ctx->stream;
+    uint64_t k0 = ctx->launches;
+    RunTimer tm(ctx);
+    uint32_t *count = (uint32_t *)coreness->d;
+    GG_CUDA(ctx, cudaMemsetAsync(g->kc_cnt + 3, 0, 8, sm));
+    if (g->n) {
+        k_kc_init<<<persistent_grid(ctx, ((uint64_t)g->n + 31) / 32), 256, 0, sm>>>(g->off, g->n, count,
+                                                                                    g->kc_cnt + 3);
+        GG_LAUNCHED(ctx);
+    }
+    gg_frontier *F, *O;
+    GG_CHECK(get_tmp_frontiers(g, &F, &O));
+    gg_emap_desc desc;
+    memset(&desc, 0, sizeof(desc));
+    desc.relax = GG_RELAX_COUNT_DOWN_U32;  // coreness[d].count_down_value(cK)  (KC_bucket.C:371-380)
+    desc.a = coreness;
+    desc.dst_filter = GG_FILTER_GT_CONST;  // only counts above the floor move
+    desc.record = GG_RECORD_AT_FLOOR;      // old == cK + 1: d reached the floor  (KC_bucket.C:353-369)
+    desc.threshold = opt.threshold;
+    desc.threshold_k = opt.threshold_k;
+    desc.variant = opt.variant;
+    const unsigned sgrid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_kc_scan, 256));
+    // {alive A, alive B, min left, vertices of degree above one}, in a part of the pinned staging buffer
+    // that the frontier count reads (its first FC_WORDS words) leave alone
+    unsigned long long *hc = (unsigned long long *)ctx->h_pinned + 48;
+    uint64_t L = 0;
+    int cur = 0, steps = 0, floors = 0;
+    bool first = true;
+    uint32_t largest = 0;
+    while (g->n) {
+        // the scan at floor L: peel frontier F, the next alive list, the smallest count left
+        GG_CHECK(frontier_alloc_bins(F));
+        GG_CHECK(frontier_reset_counts(F));
+        GG_CUDA(ctx, cudaMemsetAsync(g->kc_cnt + (cur ^ 1), 0, 8, sm));
+        GG_CUDA(ctx, cudaMemsetAsync(g->kc_cnt + 2, 0xFF, 8, sm));
+        k_kc_scan<<<sgrid, 256, 0, sm>>>(first ? nullptr : g->kc_alive[cur], g->n, g->kc_cnt + cur, count,
+                                         (uint32_t)L, g->off, t.bin_small_max, t.bin_medium_max, F->bins[0],
+                                         F->bins[1], F->bins[2], (unsigned long long *)F->d_cnt,
+                                         g->kc_alive[cur ^ 1], g->kc_cnt + (cur ^ 1), g->kc_cnt + 2);
+        GG_LAUNCHED(ctx);
+        F->all = false;
+        F->has_list = true;
+        F->has_bitmap = false;
+        F->host_valid = false;
+        GG_CUDA(ctx, cudaMemcpyAsync(hc, g->kc_cnt, 4 * 8, cudaMemcpyDeviceToHost, sm));
+        GG_CHECK(frontier_fetch_counts(F));  // (synchronises: hc is current too)
+        cur ^= 1;
+        first = false;
+        ++floors;
+        const uint64_t left = hc[cur], min_left = hc[2];
+        if (F->h_cnt[FC_NACTV] == 0) {
+            if (left == 0) break;
+            L = min_left;  // no vertex at this floor: the next count that exists
+            continue;
+        }
+        largest = (uint32_t)L;
+        // peel steps at floor L: F's vertices have coreness L
+        desc.dst_filter_k = (int64_t)L;
+        while (F->h_cnt[FC_NACTV] != 0 && F->h_cnt[FC_NACTE] != 0) {
+            gg_emap_stats es;
+            GG_CHECK(edgemap_impl(g, &desc, F, O, opt.collect_stats ? &es : nullptr));
+            if (opt.collect_stats) record_iter(st, steps, es);
+            ++steps;
+            std::swap(F, O);
+            GG_CHECK(frontier_fetch_counts(F));
+        }
+        if (left == 0) break;
+        L = L + 1;
+    }
+    if (g->n && hc[3] < (unsigned long long)(g->n / 2)) {  // (hc[3]: vertices of degree above one)
+        k_kc_isolated<<<persistent_grid(ctx, ((uint64_t)g->n + 31) / 32), 256, 0, sm>>>(g->off, g->n, count);
+        GG_LAUNCHED(ctx);
+        largest = std::max(largest, 1u);
+    }
+    double ms = tm.stop();
+    if (st) {
+        st->iterations = steps;
+        st->total_ms = ms;
+        st->kernels = ctx->launches - k0;
+        st->vertices_reached = (uint64_t)floors;  // floors scanned
+    }
+    if (largest_core) *largest_core = largest;
+    if (host_coreness) GG_CHECK(gg_prop_download(coreness, host_coreness));
     return gg_ctx_sync(ctx);
 }
 

@@ -154,6 +154,10 @@ struct gg_graph {
     gg_prop *tmp_prop[4] = {nullptr, nullptr, nullptr, nullptr};  // cached run temporaries
     uint32_t *nonisolated = nullptr;    // vertices with in-edges, ascending
     uint64_t *nonisolated_n = nullptr;  // its length (device)
+    // gg_kcore: the two alive lists (vertices not yet peeled; n entries
+    // each) and their counters {count A, count B, smallest count left}
+    uint32_t *kc_alive[2] = {nullptr, nullptr};
+    unsigned long long *kc_cnt = nullptr;
     CandLists cand;               // pull candidate lists (driver runs)
     bool cand_active = false;     // a driver run uses them for its pull steps
     // released frontier buffers, reused in stream order

@@ -21,9 +21,9 @@ GG_OK, GG_ERR_ARG, GG_ERR_OOM, GG_ERR_CUDA, GG_ERR_TIMEOUT, GG_ERR_UNSUPPORTED, 
     GG_ERR_STATE, GG_ERR_NOT_FOUND = range(9)
 I32, U32, F32, F64, BF16, F16, FP8E4M3, CFP_6_10, BF16_TRUNC, U8 = range(10)
 (RELAX_MIN_PLUS1_I32, RELAX_MIN_U32, RELAX_SETIF_U32, RELAX_ADD_GATHER, RELAX_NE_CHECK, RELAX_GAP_CHECK,
- RELAX_AHEAD_CHECK, RELAX_OR_U32, RELAX_MIS_U8) = range(9)
+ RELAX_AHEAD_CHECK, RELAX_OR_U32, RELAX_MIS_U8, RELAX_COUNT_DOWN_U32) = range(10)
 FILTER_NONE, FILTER_GT_CONST, FILTER_NE_ZERO, FILTER_MSB_SET, FILTER_NE_CONST, FILTER_IN_FRONTIER = range(6)
-RECORD_NONE, RECORD_REDUCTION, RECORD_NE_PREV, RECORD_EQ_ZERO = range(4)
+RECORD_NONE, RECORD_REDUCTION, RECORD_NE_PREV, RECORD_EQ_ZERO, RECORD_AT_FLOOR = range(5)
 THRESH_DEFAULT, THRESH_FRAC, THRESH_ALWAYS_SPARSE, THRESH_ALWAYS_DENSE, THRESH_LEARNED = range(5)
 VAR_AUTO, VAR_PUSH_SPARSE, VAR_PUSH_MERGE, VAR_PULL_DENSE, VAR_PUSH_DENSE, VAR_HOOK = -1, 0, 1, 2, 3, 4
 VARIANT_NAMES = {0: "push_sparse", 1: "push_merge", 2: "pull_dense", 3: "push_dense"}
@@ -96,7 +96,7 @@ EXPORTS = [
     "gg_frontier_clear", "gg_frontier_set_single", "gg_frontier_set_all", "gg_frontier_set_list",
     "gg_frontier_counts", "gg_frontier_download", "gg_frontier_destroy", "gg_edgemap",
     "gg_vertexmap", "gg_bfs_level", "gg_bfs_level_host_async", "gg_bfs_level_host_wait",
-    "gg_bfs_parent", "gg_cc", "gg_pagerank",
+    "gg_bfs_parent", "gg_cc", "gg_kcore", "gg_pagerank",
     "gg_tuning_set", "gg_tuning_get",
 ]
 
@@ -161,6 +161,7 @@ def lib() -> C.CDLL:
     L.gg_bfs_level.argtypes = [vp, u32, C.POINTER(RunOpts), vp, vp, C.POINTER(RunStats)]
     L.gg_bfs_parent.argtypes = [vp, u32, C.POINTER(RunOpts), vp, vp, C.POINTER(RunStats)]
     L.gg_cc.argtypes = [vp, C.POINTER(RunOpts), vp, vp, C.POINTER(RunStats)]
+    L.gg_kcore.argtypes = [vp, C.POINTER(RunOpts), vp, vp, C.POINTER(u32), C.POINTER(RunStats)]
     L.gg_pagerank.argtypes = [vp, C.POINTER(PrParams), vp, vp, C.POINTER(RunStats)]
     L.gg_tuning_set.argtypes = [C.c_char_p, C.c_int64]
     L.gg_tuning_get.argtypes = [C.c_char_p, C.POINTER(C.c_int64)]
@@ -382,6 +383,18 @@ class Graph:
                                    label.h if label else None, _p(out) if host else None,
                                    C.byref(stats) if stats is not None else None), "gg_cc")
         return out
+
+    def kcore(self, coreness: "Prop" = None, host: bool = True, opts: RunOpts = None,
+              stats: RunStats = None):
+        """k-core decomposition (KC_bucket): (coreness uint32 per vertex or
+        None when host is False, largest coreness)."""
+        out = np.empty(self.n, dtype=np.uint32) if host else None
+        largest = C.c_uint32()
+        self.ctx.check(lib().gg_kcore(self.h, C.byref(opts) if opts else None,
+                                      coreness.h if coreness else None, _p(out) if host else None,
+                                      C.byref(largest), C.byref(stats) if stats is not None else None),
+                       "gg_kcore")
+        return out, int(largest.value)
 
     def pagerank(self, maxiter=20, tol=1e-7, contrib=F32, accum_f64=True, renorm_f32=True,
                  damping=0.85, x: "Prop" = None, host: bool = True, stats: RunStats = None, stages=None,

@@ -195,13 +195,19 @@ typedef enum gg_relax_kind {
     GG_RELAX_AHEAD_CHECK = 6,   /* a[s] < a[d] - 1 on int32          (BFSLVLv.C:299-305) */
     GG_RELAX_OR_U32 = 7,        /* a[d] |= src[s] on uint32 (another property as source;
                                    FMv.C:356-358, its neighbourhood bit masks)          */
-    GG_RELAX_MIS_U8 = 8         /* maximal independent set states on uint8, 0 undecided,
+    GG_RELAX_MIS_U8 = 8,        /* maximal independent set states on uint8, 0 undecided,
                                    1 conditionally in, 2 out, 3 in: over the in-edges
                                    (s, d), s != d, d becomes out when some s is in, else
                                    undecided when it is conditionally in and some s < d
                                    is undecided or conditionally in (MISv.C:235-255,
                                    dsl/ast/dfsaop.h:49-230).  Takes dst filter NONE or
                                    IN_FRONTIER and record NONE or EQ_ZERO. */
+    GG_RELAX_COUNT_DOWN_U32 = 9 /* a[d].count_down_value(_c(k)) on uint32: every active
+                                   in-neighbour s takes one off a[d] while a[d] > k, never
+                                   below the floor k (KC_bucket.C:343-380, the k-core
+                                   peel).  Takes dst filter GT_CONST with k (the floor)
+                                   and record NONE, REDUCTION (every vertex counted down)
+                                   or AT_FLOOR.  Counts must stay below 2^31. */
 } gg_relax_kind;
 
 /* dst filters (api::filter(weak, dst, lambda), api.h:687-706). */
@@ -221,7 +227,10 @@ typedef enum gg_record_kind {
     GG_RECORD_REDUCTION = 1, /* vertices whose relax returned true */
     GG_RECORD_NE_PREV = 2,   /* method a[d] != prev[d]; prev[d] = a[d] afterwards
                                 (record(..., λd: a[d]!=prev[d]) + maintain_copies) */
-    GG_RECORD_EQ_ZERO = 3    /* method a[d] == 0 after the step (MISv.C:246-253) */
+    GG_RECORD_EQ_ZERO = 3,   /* method a[d] == 0 after the step (MISv.C:246-253) */
+    GG_RECORD_AT_FLOOR = 4   /* COUNT_DOWN: the vertices whose count reached the floor k
+                                in this step, each once (the fused k-core step's
+                                old == k + 1 test, KC_bucket.C:353-369) */
 } gg_record_kind;
 
 /* sparse/dense threshold (api.h:130-222) and the learned selector. */
@@ -399,6 +408,19 @@ GG_API gg_status gg_bfs_parent(gg_graph *g, uint32_t root, const gg_run_opts *o,
  * minimum id of each component); otherwise label propagation continues. */
 GG_API gg_status gg_cc(gg_graph *g, const gg_run_opts *o, gg_prop *label, uint32_t *host_label,
                        gg_run_stats *st);
+/* k-core decomposition (KC_bucket, bench/KC_bucket.C:107-420): coreness[v] =
+ * the largest k such that v lies in a subgraph whose every vertex has at
+ * least k neighbours in it (0 for isolated vertices).  The peel: the count
+ * of every vertex starts at its degree; for floors k = 0, 1, 2, ... the
+ * vertices whose count is k are removed and count down their neighbours
+ * (edgemap with GG_RELAX_COUNT_DOWN_U32, floor k, record AT_FLOOR) until no
+ * count reaches k; empty floors are skipped.  o NULL: every step a sparse
+ * push (a count-down pull has no early exit).  Symmetric graphs only
+ * (GG_ERR_UNSUPPORTED otherwise).  coreness: a U32 property of g, or NULL;
+ * host_coreness: n entries of host memory, or NULL; largest_core: the
+ * largest coreness, or NULL.  st: floors, peel steps and device time. */
+GG_API gg_status gg_kcore(gg_graph *g, const gg_run_opts *o, gg_prop *coreness, uint32_t *host_coreness,
+                          uint32_t *largest_core, gg_run_stats *st);
 
 typedef struct gg_pr_params {
     int maxiter;        /* PRv -pr:maxiter (default 100) */

@@ -992,3 +992,64 @@ ORC_API int orc_apr(uint32_t n, const uint64_t *in_off, const uint32_t *in_adj, 
     free(delta); free(z); free(contrib); free(od); free(F); free(act);
     return iter;
 }
+
+/* ------------------------------------------------------------------------
+ * k-core decomposition (reference: bench/KC_bucket.C:107-420, whose peel
+ * counts each vertex down from its degree, removes the vertices whose count
+ * equals the current bucket K and counts their neighbours down, never below
+ * K, KC_bucket.C:343-380).  Restated as the sequential bucket peel of
+ * Batagelj and Zaversnik (2003): vertices sorted by count in bins, always
+ * removing one of smallest count and moving each neighbour with a larger
+ * count one bin down.  Both give every vertex the largest k of a k-core
+ * that holds it (the decomposition is unique), except for isolated vertices
+ * in the case noted at the end.  core[v]: coreness; returns the largest
+ * coreness, or -1 on an allocation failure.
+ * ------------------------------------------------------------------------ */
+ORC_API int64_t orc_kcore(uint32_t n, const uint64_t *off, const uint32_t *adj, uint32_t *core) {
+    if (n == 0) return 0;
+    uint64_t md = 0;
+    for (uint32_t v = 0; v < n; ++v) {
+        const uint64_t d = off[v + 1] - off[v];
+        core[v] = (uint32_t)d;
+        if (d > md) md = d;
+    }
+    uint64_t *bin = (uint64_t *)calloc(md + 2, sizeof(uint64_t));
+    uint64_t *pos = (uint64_t *)malloc((size_t)n * sizeof(uint64_t));
+    uint32_t *vert = (uint32_t *)malloc((size_t)n * sizeof(uint32_t));
+    if (!bin || !pos || !vert) { free(bin); free(pos); free(vert); return -1; }
+    for (uint32_t v = 0; v < n; ++v) bin[core[v]]++;
+    uint64_t start = 0;
+    for (uint64_t d = 0; d <= md; ++d) { const uint64_t c = bin[d]; bin[d] = start; start += c; }
+    for (uint32_t v = 0; v < n; ++v) { pos[v] = bin[core[v]]++; vert[pos[v]] = v; }
+    for (uint64_t d = md; d > 0; --d) bin[d] = bin[d - 1];
+    bin[0] = 0;
+    int64_t largest = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        const uint32_t v = vert[i];
+        if ((int64_t)core[v] > largest) largest = core[v];
+        for (uint64_t e = off[v]; e < off[v + 1]; ++e) {
+            const uint32_t u = adj[e];
+            if (core[u] > core[v]) {   /* u one bin down: swap it with its bin's first */
+                const uint32_t du = core[u];
+                const uint64_t pu = pos[u], pw = bin[du];
+                const uint32_t w = vert[pw];
+                if (u != w) { pos[u] = pw; vert[pu] = w; pos[w] = pu; vert[pw] = u; }
+                bin[du]++;
+                core[u]--;
+            }
+        }
+    }
+    free(bin); free(pos); free(vert);
+    /* The reference's degree-one preprocessing (KC_bucket.C:131-160): when
+     * fewer than n/2 vertices have a degree above one, it counts every
+     * vertex's degree-one neighbours off and raises every count to at least
+     * 1, isolated vertices included, which keep that 1 (they are in no
+     * bucket).  Its output has coreness 1 for them in that case. */
+    uint64_t ngt1 = 0;
+    for (uint32_t v = 0; v < n; ++v) ngt1 += off[v + 1] - off[v] > 1;
+    if (ngt1 < (uint64_t)(n / 2))
+        for (uint32_t v = 0; v < n; ++v)
+            if (off[v + 1] == off[v]) core[v] = 1;
+    if (largest == 0 && ngt1 < (uint64_t)(n / 2)) largest = 1;
+    return largest;
+}

@@ -73,6 +73,8 @@ def lib() -> C.CDLL:
         L.orc_mis.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_mis.restype = C.c_int64
         L.orc_apr.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.orc_kcore.argtypes = [C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_kcore.restype = C.c_int64
         L.orc_free.argtypes = [C.c_void_p]
         _lib = L
     return _lib
@@ -354,6 +356,37 @@ def ref_apr(bin_path: str, out_path: str, maxiter: int = 100, threads: int | Non
         raise PaddedGraph(f"reference padded {n} vertices to {len(x)}")
     its = sum(1 for l in err.splitlines() if l.startswith("Iteration "))
     return x, its
+
+
+def kcore(g: Graph):
+    """k-core decomposition (oracle.c orc_kcore, the KC_bucket restatement):
+    returns (coreness uint32, largest coreness).  g symmetric."""
+    core = np.empty(max(g.n, 1), dtype=np.uint32)
+    k = lib().orc_kcore(g.n, _p(g.off), _p(g.adj), _p(core))
+    if k < 0:
+        raise RuntimeError("orc_kcore failed (allocation)")
+    return core[:g.n], int(k)
+
+
+def ref_kc(bin_path: str, out_path: str, threads: int | None = None):
+    """Reference KC_bucket (its driver, -kc:outfile, KC_bucket.C:496-497):
+    returns (coreness in original order, seconds of its run()).  The build's
+    own validate() stops on an assertion (VL == storedVL, a restriction of
+    its vector-length code) after the output is written: a run that wrote
+    all n values is taken."""
+    args = [ref_prog("KC_bucket"), "-s", "-b", "-rounds", "1", "-c", "256", "-kc:outfile", out_path, bin_path]
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    if os.path.exists(out_path):
+        os.remove(out_path)
+    r = subprocess.run(args, capture_output=True, text=True, env=env, timeout=1800)
+    n = int(np.fromfile(bin_path, dtype=np.uint64, count=3)[2])
+    core = np.fromfile(out_path, dtype=np.int64, sep=" ") if os.path.exists(out_path) else np.zeros(0)
+    if len(core) != n:
+        raise RuntimeError(f"KC_bucket wrote {len(core)} of {n} values, rc={r.returncode}: {r.stderr[-1500:]}")
+    t = _running_times(r.stdout)
+    return core.astype(np.uint32), (t[0] if t else None)
 
 
 def ref_variant() -> str:

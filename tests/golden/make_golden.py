@@ -22,6 +22,8 @@ programs on it, compiled from the reference sources by oracle/Makefile:
                  each vertex (MISv's priorities)
   apr_x        - APRv.C -pr:outfile (to sum |delta| < 1e-7 or 100 iterations),
                  with apr_iters its iteration count
+  kc           - KC_bucket.C -kc:outfile (coreness of every vertex), with
+                 kc_largest the largest
 customfp_sweep.npz holds float bit patterns and, per pattern, the codes and
 decoded floats of the reference's customfp<6,10> and scustomfp<true,8,7>
 conversions (harness oracle/harness/ref_cfp.C).
@@ -33,6 +35,7 @@ Run (needs the reference tree and `make -C oracle ref`):
     python tests/golden/make_golden.py --fm-only  # add / refresh the fm_* keys only
     python tests/golden/make_golden.py --mis-only # add / refresh the mis_* keys only
     python tests/golden/make_golden.py --apr-only # add / refresh the apr_* keys only
+    python tests/golden/make_golden.py --kc-only  # add / refresh the kc* keys only
 """
 import hashlib
 import os
@@ -110,6 +113,15 @@ def apr_reference(g, tmp):
     return dict(apr_x=x, apr_iters=np.int64(its))
 
 
+def kc_reference(g, tmp):
+    p = os.path.join(tmp, "g.bin")
+    O.write_bin(g, p)
+    core, _ = O.ref_kc(p, os.path.join(tmp, "kc.txt"))
+    mine, largest = O.kcore(g)
+    assert np.array_equal(core, mine)  # the restatement must agree
+    return dict(kc=core, kc_largest=np.int64(largest))
+
+
 def add_keys(name, tmp, fn):
     path = os.path.join(HERE, name + ".npz")
     d = dict(np.load(path))
@@ -129,6 +141,7 @@ def save(name, g, roots, pr_iters, tmp, store_csr=True, params=None):
     vary.update(fm_reference(g, tmp))
     vary.update(mis_reference(g, tmp))
     vary.update(apr_reference(g, tmp))
+    vary.update(kc_reference(g, tmp))
     # sanity: the restatement must agree before a fixture is written
     for r, l in zip(roots, levels):
         assert np.array_equal(O.bfs_level(g, r), l), name
@@ -167,7 +180,8 @@ def main():
     if not O.ref_available("ref_bfslvl"):
         raise SystemExit("reference build missing: make -C oracle ref")
     with tempfile.TemporaryDirectory() as tmp:
-        only = {"--fm-only": fm_reference, "--mis-only": mis_reference, "--apr-only": apr_reference}
+        only = {"--fm-only": fm_reference, "--mis-only": mis_reference, "--apr-only": apr_reference,
+                "--kc-only": kc_reference}
         for flag, fn in only.items():
             if flag in sys.argv:
                 for name in ["rmat10_ef8", "rmat12_ef16", "grid20x32_del5pct", "er2000_deg6", "edgecases32",
