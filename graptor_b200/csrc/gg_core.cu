@@ -819,6 +819,8 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "pull_first" && v <= 4) t.pull_first = (int)v;
     else if (k == "pull_stage" && (v == 0 || v == 4 || v == 8 || v == 16 || v == 32)) t.pull_stage = (int)v;
     else if (k == "pull_fresh" && v <= 1) t.pull_fresh = (int)v;
+    else if (k == "pull_ctas" && v >= 4 && v <= 8) t.pull_ctas = (int)v;
+    else if (k == "push_ctas" && v >= 4 && v <= 8) t.push_ctas = (int)v;
     else if (k == "push_k" && v >= 1 && v <= 1024) t.push_k = (int)v;
     else if (k == "heavy_deg" && v >= 32) t.heavy_deg = (uint32_t)v;
     else if (k == "heavy_chunk" && v >= 32) t.heavy_chunk = (uint32_t)v;
@@ -856,6 +858,8 @@ gg_status gg_tuning_get(const char *name, int64_t *v) {
     else if (k == "pull_first") *v = t.pull_first;
     else if (k == "pull_stage") *v = t.pull_stage;
     else if (k == "pull_fresh") *v = t.pull_fresh;
+    else if (k == "pull_ctas") *v = t.pull_ctas;
+    else if (k == "push_ctas") *v = t.push_ctas;
     else if (k == "push_k") *v = t.push_k;
     else if (k == "heavy_deg") *v = t.heavy_deg;
     else if (k == "heavy_chunk") *v = t.heavy_chunk;

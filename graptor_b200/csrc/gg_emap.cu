@@ -2033,7 +2033,8 @@ __device__ __forceinline__ void kspan_end(GCtl *c, int it, unsigned *s_done) {
         atomicMax(&c->kt1[it], g_now());
 }
 
-__global__ void __launch_bounds__(kBlock, 6) k_g_push(GCtl *c) {
+template <int MINB>  // resident CTAs per SM it is compiled for (knob push_ctas)
+__global__ void __launch_bounds__(kBlock, MINB) k_g_push(GCtl *c) {
     chain_enter();
     if (c->variant != GG_VAR_PUSH_SPARSE) return;
     __shared__ EmapArgs sA;
@@ -2164,7 +2165,10 @@ __device__ __forceinline__ void stage_finish(GCtl *c, unsigned long long *bar, b
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBlock, 6) k_g_pull(GCtl *c) {
+// MINB: resident CTAs per SM the kernel is compiled for (knob pull_ctas):
+// 6 caps it at 40 registers, with spills in the row loop; 4 gives 64, none
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_g_pull(GCtl *c) {
     chain_enter();
     if (c->variant != GG_VAR_PULL_DENSE) return;
     extern __shared__ __align__(128) uint32_t s_stage[];
@@ -2200,7 +2204,8 @@ __global__ void __launch_bounds__(kBlock, 6) k_g_pull(GCtl *c) {
 
 // second pass of a split pull: the rows the first pass left open, from
 // their third in-edge
-__global__ void __launch_bounds__(kBlock, 6) k_g_pull2(GCtl *c) {
+template <int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_g_pull2(GCtl *c) {
     chain_enter();
     if (c->variant != GG_VAR_PULL_DENSE || !c->A.rest_out) return;
     extern __shared__ __align__(128) uint32_t s_stage[];
@@ -2368,6 +2373,8 @@ struct GraphBfs {
     int pdl = 0;       // the flat loop body's kernels joined by programmatic edges (knob graph_pdl)
     int pdl_refused = 0;  // the runtime refused programmatic edges here: built without them
     int unroll = 1;       // copies of the flat chain per loop iteration (knob graph_unroll)
+    int pull_ctas = 6;    // the pull kernels' compiled residency (knob pull_ctas)
+    int push_ctas = 6;    // the push kernel's (knob push_ctas)
     // page-locked host copies of the control block: the configuration sent
     // before a run, and the records a kernel writes back after it through the
     // mapping (no copy-engine transfer: a run's records do not queue behind
@@ -2431,15 +2438,32 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb, int pdl) {
     GG_CUDA(ctx, cudaHostAlloc(&gb->h_up, sizeof(GCtl), cudaHostAllocDefault));
     GG_CUDA(ctx, cudaHostAlloc(&gb->h_rec, sizeof(GCtl) + 16, cudaHostAllocMapped));
     GG_CUDA(ctx, cudaHostGetDevicePointer((void **)&gb->d_rec, gb->h_rec, 0));
-    gb->push_grid = (unsigned)(ctx->sm_count * resident_ctas((const void *)k_g_push, kBlock));
+    gb->push_ctas = tuning().push_ctas;
+    const void *fpush = gb->push_ctas == 4   ? (const void *)k_g_push<4>
+                        : gb->push_ctas == 5 ? (const void *)k_g_push<5>
+                        : gb->push_ctas == 7 ? (const void *)k_g_push<7>
+                        : gb->push_ctas == 8 ? (const void *)k_g_push<8>
+                                             : (const void *)k_g_push<6>;
+    gb->push_grid = (unsigned)(ctx->sm_count * resident_ctas(fpush, kBlock));
     // pulls that stage the frontier bitmap's first words take that much
     // dynamic shared memory per CTA (fewer CTAs may then fit on an SM)
     gb->stage_kb = tuning().pull_stage;
     const unsigned stage_bytes = (unsigned)gb->stage_kb * 1024u;
+    gb->pull_ctas = tuning().pull_ctas;
+    const void *fpull = gb->pull_ctas == 4   ? (const void *)k_g_pull<4>
+                        : gb->pull_ctas == 5 ? (const void *)k_g_pull<5>
+                        : gb->pull_ctas == 7 ? (const void *)k_g_pull<7>
+                        : gb->pull_ctas == 8 ? (const void *)k_g_pull<8>
+                                             : (const void *)k_g_pull<6>;
+    const void *fpull2 = gb->pull_ctas == 4   ? (const void *)k_g_pull2<4>
+                         : gb->pull_ctas == 5 ? (const void *)k_g_pull2<5>
+                         : gb->pull_ctas == 7 ? (const void *)k_g_pull2<7>
+                         : gb->pull_ctas == 8 ? (const void *)k_g_pull2<8>
+                                              : (const void *)k_g_pull2<6>;
     int pull_occ = 0;
-    for (const void *fn : {(const void *)k_g_pull, (const void *)k_g_pull2})
+    for (const void *fn : {fpull, fpull2})
         GG_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)stage_bytes));
-    GG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pull_occ, (const void *)k_g_pull, kBlock, stage_bytes));
+    GG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pull_occ, fpull, kBlock, stage_bytes));
     gb->pull_grid = (unsigned)(ctx->sm_count * std::max(pull_occ, 1));
     gb->vgrid = (unsigned)(ctx->sm_count * 8);
     GG_CUDA(ctx, cudaGraphCreate(&gb->graph, 0));
@@ -2463,8 +2487,8 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb, int pdl) {
         // node costs several times an idle kernel's launch inside the loop
         // (measured on B200: SWITCH about 6.7 us, IF about 2.4 us, an idle
         // kernel about 0.9 us per iteration).
-        const void *chain[] = {(const void *)k_g_tolist, (const void *)k_g_chunks, (const void *)k_g_push,
-                               (const void *)k_g_tobitmap, (const void *)k_g_pull, (const void *)k_g_pull2,
+        const void *chain[] = {(const void *)k_g_tolist, (const void *)k_g_chunks, fpush,
+                               (const void *)k_g_tobitmap, fpull, fpull2,
                                (const void *)k_g_next};
         const unsigned grids[] = {gb->vgrid, 1, gb->push_grid, gb->vgrid, gb->pull_grid, gb->pull_grid,
                                   (unsigned)ctx->sm_count * 2};
@@ -2514,12 +2538,12 @@ static gg_status graph_bfs_build(gg_graph *g, GraphBfs *gb, int pdl) {
     cudaGraph_t bc;
     GG_CHECK(add_cond(ctx, bp, &n_ifc, &n_ifl, 1, hc, cudaGraphCondTypeIf, &bc));
     GG_CHECK(add_kernel(ctx, bc, &n_chunks, nullptr, 0, (const void *)k_g_chunks, 1, 1024, arg));
-    GG_CHECK(add_kernel(ctx, bp, &n_push, &n_ifc, 1, (const void *)k_g_push, gb->push_grid, kBlock, arg));
+    GG_CHECK(add_kernel(ctx, bp, &n_push, &n_ifc, 1, fpush, gb->push_grid, kBlock, arg));
     GG_CHECK(add_cond(ctx, bq, &n_ifb, nullptr, 0, hb, cudaGraphCondTypeIf, &bb));
     GG_CHECK(add_kernel(ctx, bb, &n_bits, nullptr, 0, (const void *)k_g_tobitmap, gb->vgrid, 256, arg));
-    GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_ifb, 1, (const void *)k_g_pull, gb->pull_grid, kBlock, arg, stage_bytes));
+    GG_CHECK(add_kernel(ctx, bq, &n_pull, &n_ifb, 1, fpull, gb->pull_grid, kBlock, arg, stage_bytes));
     cudaGraphNode_t n_pull2;
-    GG_CHECK(add_kernel(ctx, bq, &n_pull2, &n_pull, 1, (const void *)k_g_pull2, gb->pull_grid, kBlock, arg,
+    GG_CHECK(add_kernel(ctx, bq, &n_pull2, &n_pull, 1, fpull2, gb->pull_grid, kBlock, arg,
                         stage_bytes));
     GG_CHECK(add_kernel(ctx, body, &n_next, &n_sw, 1, (const void *)k_g_next, (unsigned)ctx->sm_count * 2, 256, arg));
     GG_CUDA(ctx, cudaGraphInstantiate(&gb->exec, G, 0));
@@ -2558,7 +2582,8 @@ gg_status graph_bfs_level(gg_graph *g, uint32_t root, const gg_run_opts &opt, gg
     GraphBfs *gb = (GraphBfs *)g->gbfs;
     if (gb->flat != tuning().graph_flat || gb->stage_kb != tuning().pull_stage ||
         (gb->flat && !gb->pdl_refused && gb->pdl != tuning().graph_pdl) ||
-        (gb->flat && gb->unroll != tuning().graph_unroll)) {  // built for another shape
+        (gb->flat && gb->unroll != tuning().graph_unroll) || gb->pull_ctas != tuning().pull_ctas ||
+        gb->push_ctas != tuning().push_ctas) {  // built for another shape
         graph_bfs_free(g);
         return graph_bfs_level(g, root, opt, level, prev, st, iters_out);
     }

@@ -296,6 +296,10 @@ struct Tuning {
     // pull's unsettled rows, so their levels are known (unvisited) and not
     // loaded
     int pull_fresh = 1;
+    // graph-driven BFS pull kernels compiled for this many resident CTAs per
+    // SM (4 to 8: more CTAs, fewer registers per thread)
+    int pull_ctas = 6;
+    int push_ctas = 6;  // the same for the graph-driven BFS push kernel
     unsigned long long barrier_timeout_ns = 5000000000ull;  // grid-barrier wait limit
 };
 Tuning &tuning();

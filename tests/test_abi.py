@@ -110,16 +110,18 @@ def test_pull_knobs():
     mode (0-4), the KiB of frontier bitmap a CTA stages in shared memory
     (0, 4, 8, 16 or 32) and the skipped level loads after a pull."""
     from graptor_b200 import gg
-    names = ("pull_first", "pull_stage", "pull_fresh", "pull_split", "graph_pdl", "graph_unroll")
+    names = ("pull_first", "pull_stage", "pull_fresh", "pull_split", "graph_pdl", "graph_unroll", "pull_ctas",
+             "push_ctas")
     old = {k: gg.tuning_get(k) for k in names}
     try:
         for k, v in (("pull_first", 3), ("pull_first", 4), ("pull_stage", 4), ("pull_stage", 32),
                      ("pull_stage", 0), ("pull_fresh", 0), ("pull_fresh", 1), ("graph_pdl", 1),
-                     ("graph_unroll", 4), ("graph_unroll", 1)):
+                     ("graph_unroll", 4), ("graph_unroll", 1), ("pull_ctas", 4), ("push_ctas", 5)):
             gg.tuning_set(k, v)
             assert gg.tuning_get(k) == v
         for k, v in (("pull_first", 5), ("pull_stage", 12), ("pull_stage", 64), ("pull_fresh", 2),
-                     ("graph_pdl", 2), ("graph_unroll", 0), ("graph_unroll", 5)):
+                     ("graph_pdl", 2), ("graph_unroll", 0), ("graph_unroll", 5), ("pull_ctas", 3),
+                     ("push_ctas", 9)):
             before = gg.tuning_get(k)
             with pytest.raises(gg.GGError):
                 gg.tuning_set(k, v)

@@ -520,6 +520,29 @@ def test_pull_stage_and_fresh_exact(ctx, stage, gen):
         g.close()
 
 
+@pytest.mark.parametrize("ctas", [(4, 4), (5, 5), (6, 6), (4, 6), (7, 7), (8, 8)])
+def test_graph_bfs_kernel_residency_exact(ctx, ctas):
+    """Graph-driven BFS with its pull and push kernels compiled for 4 to 8
+    resident CTAs per SM (knobs pull_ctas, push_ctas: registers per thread
+    against CTAs per SM): levels identical to the oracle's."""
+    knobs = ("graph", "pull_ctas", "push_ctas")
+    old = {k: gg.tuning_get(k) for k in knobs}
+    try:
+        gg.tuning_set("graph", 1)
+        gg.tuning_set("pull_ctas", ctas[0])
+        gg.tuning_set("push_ctas", ctas[1])
+        for og in (O.rmat(15, 16 << 15, seed=85), O.grid(60, 70, seed=86, del_bp=300)):
+            g = ctx.upload(og.off, og.adj)
+            deg = og.outdeg()
+            nz = np.flatnonzero(deg)
+            for r in (int(np.argmax(deg)), int(nz[len(nz) // 2])):
+                assert np.array_equal(g.bfs_level(r), O.bfs_level(og, r)), (ctas, r)
+            g.close()
+    finally:
+        for k, v in old.items():
+            gg.tuning_set(k, v)
+
+
 @pytest.mark.parametrize("stochastic,avg", [(False, 0), (True, 0), (True, 50)])
 def test_bf16_stochastic_rounding_matches_restatement(ctx, stochastic, avg):
     """BF16 PageRank with rounding to nearest, stochastic rounding (the same
