@@ -222,6 +222,10 @@ def pick_roots(deg: np.ndarray) -> np.ndarray:
 # k_pull with the three-neighbour records (4 launches of R-MAT scale 23 BFS,
 # 245.0 MB each on average) scaled by the vertex count to scale 24
 K_PULL_TRAFFIC_PER_LAUNCH = 490.0e6
+# DRAM bytes of one 128-seed PPR iteration at R-MAT 22 (m = 128,311,324):
+# ncu's 3.03 GB read + 2.08 GB written by k_ppr_light, less the 1.07 GB of
+# rank rows that only the last iteration writes now
+PPR_DRAM_BYTES_PER_ITER = 4.04e9
 
 
 def bfs_bytes(n: int, st, it: int) -> float:
@@ -673,12 +677,23 @@ def batch_eval(ctx, g, roots, hbm_peak, n_small):
         ms.append(st.total_ms / 20)
     t = float(np.median(ms))
     # per iteration: ids + one 256-byte bf16 row per edge, offsets, the new
-    # contribution rows (the ranks are written by the last iteration only)
+    # contribution rows (the ranks are written by the last iteration only).
+    # Most of those row reads hit L2 (R-MAT hubs' rows are read again and
+    # again), so this is a work figure, not DRAM traffic; the DRAM fraction
+    # uses the bytes ncu counted for one light-row launch at this size (3.03
+    # GB read + 2.08 GB written with the ranks written every iteration; 4.0
+    # GB with the ranks written by the last one only)
     ppr_bytes = m * (256.0 + 4.0) + 8.0 * (n + 1) + n * 256.0
+    ppr_dram = PPR_DRAM_BYTES_PER_ITER * m / 128311324.0
     out["ppr128"] = {"ms_per_iter": round(t, 3), "gedges_per_s_per_iter": round(m / (t / 1e3) / 1e9, 3),
                      "seed_edges_per_s": round(128 * m / (t / 1e3) / 1e9, 1),
-                     "frac_of_hbm": round(ppr_bytes / (t / 1e3) / 1e9 / hbm_peak, 4),
-                     "bytes_per_iter": ppr_bytes, "storage": "bf16 rows of 128 seeds, fp32 sums"}
+                     "dram_frac_of_hbm": round(ppr_dram / (t / 1e3) / 1e9 / hbm_peak, 4),
+                     "dram_bytes_per_iter": ppr_dram,
+                     "dram_bytes_source": "ncu dram__bytes_read+write of k_ppr_light at R-MAT 22, less the rank "
+                                          "rows no longer written every iteration, scaled by m",
+                     "work_bytes_per_iter": ppr_bytes,
+                     "work_bytes_over_time_frac": round(ppr_bytes / (t / 1e3) / 1e9 / hbm_peak, 4),
+                     "storage": "bf16 rows of 128 seeds, fp32 sums"}
     # (b) many small graphs: one union; BFS from every part's vertex 0 plus CC,
     # submitted as one CUDA graph launch (gg_batch_bfs_cc), with the knobs the
     # autotuner picks on a 200-graph union of the same family

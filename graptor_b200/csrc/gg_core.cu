@@ -827,6 +827,7 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "large_chunk" && v >= 256) t.large_chunk = (uint32_t)v;
     else if (k == "pr_stream" && v <= 1) t.pr_stream = (int)v;
     else if (k == "blocks_per_sm" && v >= 1 && v <= 32) t.blocks_per_sm = (int)v;
+    else if (k == "pr_blocks_per_sm" && v >= 1 && v <= 32) t.pr_blocks_per_sm = (int)v;
     else if (k == "persistent" && v <= 7) t.persistent = (int)v;
     else if (k == "fusion" && (v == 0 || v == 4)) t.fusion = (int)v;
     else if (k == "fusion_queue" && (v == 0 || v >= 32)) t.fusion_queue = (uint32_t)v;
@@ -866,6 +867,7 @@ gg_status gg_tuning_get(const char *name, int64_t *v) {
     else if (k == "large_chunk") *v = t.large_chunk;
     else if (k == "pr_stream") *v = t.pr_stream;
     else if (k == "blocks_per_sm") *v = t.blocks_per_sm;
+    else if (k == "pr_blocks_per_sm") *v = t.pr_blocks_per_sm;
     else if (k == "persistent") *v = t.persistent;
     else if (k == "fusion") *v = t.fusion;
     else if (k == "fusion_queue") *v = t.fusion_queue;

@@ -521,7 +521,7 @@ constexpr int kBlock = 256;
 
 static unsigned pr_grid(gg_ctx *ctx, uint64_t work) {
     uint64_t b = (work + kBlock - 1) / kBlock;
-    uint64_t cap = (uint64_t)ctx->sm_count * tuning().blocks_per_sm;
+    uint64_t cap = (uint64_t)ctx->sm_count * tuning().pr_blocks_per_sm;
     if (b > cap) b = cap;
     return (unsigned)(b ? b : 1);
 }
@@ -536,7 +536,7 @@ static gg_status gather_launch(gg_graph *g, const typename Store<DT>::T *contrib
     const HeavyRows &H = g->heavy;
     const uint64_t warps = (uint64_t)((g->n + 31) / 32);
     uint64_t blocks = (warps * 32 + 255) / 256;
-    const uint64_t cap = (uint64_t)ctx->sm_count * tuning().blocks_per_sm;
+    const uint64_t cap = (uint64_t)ctx->sm_count * tuning().pr_blocks_per_sm;
     if (blocks > cap) blocks = cap;
     k_pr_gather<DT, ACC64, ADD_OLD, 256><<<(unsigned)(blocks ? blocks : 1), 256, 0, s>>>(
         g->in_off, g->in_adj, contrib, g->n, yf, yd, st, sinv, tuning().pull_k, H.T, tuning().pr_stream,

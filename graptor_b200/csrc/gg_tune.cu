@@ -31,7 +31,10 @@ std::vector<Knob> knob_space(int analytics) {
     };
     if (analytics & (GG_TUNE_BFS | GG_TUNE_CC)) k.push_back({"persistent", {0, 1, 4, 5}, false});
     if (analytics & GG_TUNE_BFS) k.push_back({"pull_split", {0, 1}, false});
-    if (analytics & GG_TUNE_PR) k.push_back({"pr_stream", {0, 1}, false});
+    if (analytics & GG_TUNE_PR) {
+        k.push_back({"pr_stream", {0, 1}, false});
+        k.push_back({"pr_blocks_per_sm", {4, 8, 16, 32}, false});
+    }
     return k;
 }
 

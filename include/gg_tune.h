@@ -13,7 +13,7 @@
  * created afterwards or after gg_graph_retune), large_chunk (push: edges
  * per chunk of a hub row), blocks_per_sm (CTAs per SM of the grid-stride
  * kernels), pr_stream (1: warp-streamed segmented PageRank gather, 0:
- * per-row), persistent (bit mask: 1 BFS levels, 2 BFS parents, 4 CC run as
+ * per-row), pr_blocks_per_sm (the PageRank kernels' grid cap, 16), persistent (bit mask: 1 BFS levels, 2 BFS parents, 4 CC run as
  * one device-driven cooperative launch; otherwise one launch per iteration
  * from the host), graph (1, the default: BFS levels run as one CUDA graph
  * whose conditional nodes take each step's push/pull decision on the

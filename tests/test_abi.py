@@ -111,12 +111,13 @@ def test_pull_knobs():
     (0, 4, 8, 16 or 32) and the skipped level loads after a pull."""
     from graptor_b200 import gg
     names = ("pull_first", "pull_stage", "pull_fresh", "pull_split", "graph_pdl", "graph_unroll", "pull_ctas",
-             "push_ctas")
+             "push_ctas", "pr_blocks_per_sm")
     old = {k: gg.tuning_get(k) for k in names}
     try:
         for k, v in (("pull_first", 3), ("pull_first", 4), ("pull_stage", 4), ("pull_stage", 32),
                      ("pull_stage", 0), ("pull_fresh", 0), ("pull_fresh", 1), ("graph_pdl", 1),
-                     ("graph_unroll", 4), ("graph_unroll", 1), ("pull_ctas", 4), ("push_ctas", 5)):
+                     ("graph_unroll", 4), ("graph_unroll", 1), ("pull_ctas", 4), ("push_ctas", 5),
+                     ("pr_blocks_per_sm", 8)):
             gg.tuning_set(k, v)
             assert gg.tuning_get(k) == v
         for k, v in (("pull_first", 5), ("pull_stage", 12), ("pull_stage", 64), ("pull_fresh", 2),

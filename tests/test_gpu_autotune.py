@@ -9,7 +9,7 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 KNOBS = ["bin_small_max", "bin_medium_max", "pull_k", "push_k", "large_chunk", "blocks_per_sm",
-         "heavy_deg", "heavy_chunk", "persistent", "pr_stream"]
+         "heavy_deg", "heavy_chunk", "persistent", "pr_stream", "pr_blocks_per_sm", "pull_split"]
 
 
 @pytest.fixture
