@@ -831,7 +831,7 @@ gg_status gg_tuning_set(const char *name, int64_t v) {
     else if (k == "persistent" && v <= 7) t.persistent = (int)v;
     else if (k == "fusion" && (v == 0 || v == 4)) t.fusion = (int)v;
     else if (k == "fusion_queue" && (v == 0 || v >= 32)) t.fusion_queue = (uint32_t)v;
-    else if (k == "cc_hook" && v <= 1) t.cc_hook = (int)v;
+    else if (k == "cc_hook" && v <= 2) t.cc_hook = (int)v;
     else if (k == "graph" && v <= 1) t.graph = (int)v;
     else if (k == "graph_handoff" && v <= (1 << 20)) t.graph_handoff = (int)v;
     else if (k == "handoff_ctas" && v <= (1 << 16)) t.handoff_ctas = (int)v;

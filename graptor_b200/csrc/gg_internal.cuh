@@ -280,7 +280,9 @@ struct Tuning {
     uint32_t fusion_queue = 0;  // queue entries (0: 2n + 65536)
     // device-driven CC of a symmetric graph: after the first step, CCv's
     // road-network test (fewer than n/10 zero labels) and, where it holds,
-    // min-id hooking for the rest of the run
+    // min-id hooking for the rest of the run (1); 2: where it fails, hooking
+    // too, of the vertices label 0 has not reached (vertex 0's component is
+    // done)
     int cc_hook = 1;
     // dense pull: each row's first in-neighbours read from a per-vertex
     // record (coalesced with the row's offsets) before the row itself.

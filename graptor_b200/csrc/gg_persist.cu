@@ -583,6 +583,38 @@ __device__ void phase_hook(const PArgs &P) {
     }
 }
 
+// After CCv's first step on a graph that fails the road-network test, vertex
+// 0's label 0 has reached most of its component.  A vertex whose root is 0
+// is in vertex 0's component, whose CCv label is 0, so its row is skipped;
+// every other vertex hooks all its edges (both directions: an edge to a
+// skipped vertex is taken from this side).  A warp per 32 vertices, rows of
+// up to 32 edges by their lane, longer ones by the whole warp in turn.
+__device__ void phase_hook_rest(const PArgs &P) {
+    uint32_t *lab = (uint32_t *)P.a;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t gw = ((uint64_t)blockIdx.x * kPB + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * kPB) >> 5;
+    for (uint64_t w = gw; w * 32 < P.n; w += nw) {
+        const uint32_t u = (uint32_t)(w * 32 + lane);
+        uint64_t beg = 0, end = 0;
+        if (u < P.n && uf_find(lab, u) != 0) {
+            beg = P.off[u];
+            end = P.off[u + 1];
+        }
+        const bool longrow = end - beg > 32;
+        if (!longrow)
+            for (uint64_t e = beg; e < end; ++e) uf_hook(lab, u, __ldg(P.adj + e));
+        unsigned pend = __ballot_sync(FULLP, longrow);
+        while (pend) {
+            const int j = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const uint32_t uj = __shfl_sync(FULLP, u, j);
+            const uint64_t bj = __shfl_sync(FULLP, beg, j), ej = __shfl_sync(FULLP, end, j);
+            for (uint64_t e = bj + lane; e < ej; e += 32) uf_hook(lab, uj, __ldg(P.adj + e));
+        }
+    }
+}
+
 // The root of x without path halving: in the final pass every vertex's
 // entry is written once, by its own thread, with its root; a halving store
 // from another thread's walk could land after it and leave a non-root there.
@@ -1188,8 +1220,10 @@ __global__ void __launch_bounds__(kPB) k_traverse(PArgs P) {
             if (threadIdx.x == 0 && z) atomicAdd(&st->zeros, z);
             if (!grid_barrier(st, P.timeout_ns)) return;
             // (the count includes vertex 0 and its neighbours, CCv's initial_zeros)
-            if (ldcg(&st->zeros) * 10 < (unsigned long long)P.n) {
-                phase_hook(P);
+            const bool road = ldcg(&st->zeros) * 10 < (unsigned long long)P.n;
+            if (road || P.hook == 2) {
+                if (road) phase_hook(P);
+                else phase_hook_rest(P);
                 if (!grid_barrier(st, P.timeout_ns)) return;
                 phase_hook_finish(P);
                 if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -1624,8 +1658,8 @@ gg_status persistent_enqueue(gg_graph *g, const gg_emap_desc &d, int level_k, bo
     P.force_variant = force_iter >= 0 ? force_variant : g->force_variant;
     P.sel_w = (const __nv_bfloat16 *)selector_weights(g);
     // CC of a symmetric graph: road-network test after step 0, then hooking
-    P.hook = t.cc_hook && d.relax == GG_RELAX_MIN_U32 && d.dst_filter == GG_FILTER_NE_ZERO && g->symmetric &&
-             start_all && force_iter < 0 && g->force_iter < 0 && g->n > 0;
+    P.hook = (t.cc_hook && d.relax == GG_RELAX_MIN_U32 && d.dst_filter == GG_FILTER_NE_ZERO && g->symmetric &&
+              start_all && force_iter < 0 && g->force_iter < 0 && g->n > 0) ? t.cc_hook : 0;
     P.rows_sorted = g->rows_sorted ? 1 : 0;
     // fused sparse pushes (CC): the queue holds up to 2n + 64Ki entries, more spill
     P.fusion = (t.fusion & 4) && d.relax == GG_RELAX_MIN_U32 && d.dst_filter == GG_FILTER_NE_ZERO;

@@ -153,18 +153,46 @@ def test_cc_hooking_exact(ctx, fusion_knobs, gen):
     ref = O.cc(og)
     gg.tuning_set("persistent", 4)
     st = {}
-    for h in (0, 1):
+    for h in (0, 1, 2):
         gg.tuning_set("cc_hook", h)
         s = gg.RunStats()
         assert np.array_equal(g.cc(stats=s), ref), (gen, h)
         st[h] = s
-    used = [st[1].variant[i] for i in range(min(st[1].iterations, gg.MAX_ITERS))]
-    zeros_after_first = None
+    used = {h: [st[h].variant[i] for i in range(min(st[h].iterations, gg.MAX_ITERS))] for h in (1, 2)}
     if gen == "rmat":
-        assert gg.VAR_HOOK not in used  # vertex 0 reaches most of an R-MAT graph in one step
+        # vertex 0 reaches most of an R-MAT graph in one step: no road test
+        # pass; with cc_hook 2 the rest of the run is hooking all the same
+        assert gg.VAR_HOOK not in used[1]
+        assert used[2][-1] == gg.VAR_HOOK and st[2].iterations == 2, used[2]
     else:
         # road-like: the run ends with the hooking step
-        assert used[-1] == gg.VAR_HOOK and st[1].iterations == 2, used
+        for h in (1, 2):
+            assert used[h][-1] == gg.VAR_HOOK and st[h].iterations == 2, (h, used[h])
+    g.close()
+
+
+@pytest.mark.parametrize("gen", ["rmat", "er", "union", "two_hubs"])
+def test_cc_hooking_after_first_step_exact(ctx, fusion_knobs, gen):
+    """CC with cc_hook 2 on graphs that fail the road-network test: after
+    the first step, the vertices label 0 has not reached hook all their edges
+    (vertex 0's component is done): the oracle's labels, also for components
+    that label 0 never reaches and for vertex 0 in a small component."""
+    from oracle import batch_oracle as B
+    if gen == "rmat":
+        og = O.rmat(16, 16 << 16, seed=64)
+    elif gen == "er":
+        og = O.er(40000, 3.0, seed=65)
+    elif gen == "union":
+        og, _ = B.union([O.rmat(11, 16 << 11, seed=i) for i in range(6)] + [O.grid(30, 40, seed=3, del_bp=200)])
+    else:
+        # vertex 0 isolated-ish: a small component holding 0, two large ones elsewhere
+        e = [(0, 1), (1, 2)] + [(3, 3 + i) for i in range(1, 500)] + [(600, 600 + i) for i in range(1, 400)] + \
+            [(4 + i, 5 + i) for i in range(0, 450, 3)]
+        og = O.from_edges(1200, e)
+    g = ctx.upload(og.off, og.adj)
+    gg.tuning_set("persistent", 4)
+    gg.tuning_set("cc_hook", 2)
+    assert np.array_equal(g.cc(), O.cc(og)), gen
     g.close()
 
 
