@@ -282,7 +282,8 @@ struct Tuning {
     // road-network test (fewer than n/10 zero labels) and, where it holds,
     // min-id hooking for the rest of the run (1); 2: where it fails, hooking
     // too, of the vertices label 0 has not reached (vertex 0's component is
-    // done)
+    // done).  Measured on R-MAT 24: 1.04 ms with 2 against 0.69 ms with label
+    // propagation after the first step, so 1 stays the default
     int cc_hook = 1;
     // dense pull: each row's first in-neighbours read from a per-vertex
     // record (coalesced with the row's offsets) before the row itself.
